@@ -1,0 +1,392 @@
+"""Benchmark of the Split transport path on the atrium workload.
+
+Workload (one step = one cascade frame): a seeded procedural atrium of
+262,144 FP32 triangles, a 1280x720 camera, screen receivers at 4x4 px
+(cascade-0 spacing), 36 interval rays per receiver (about 2.1 M interval
+rays per frame), 8 cascades with 32 base directions, hit shading with
+emissive next-event estimation, merge of every level, probe packing, and the
+world-space resolve of every pixel.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is interval rays per second of trace+merge with inputs resident in
+HBM (Mrays/s, whole job over all ranks); `e2e` is the same metric through
+lux_view_frame_host with host buffers, copies and the resolve included.
+`--impl reference` times the CPU oracle (the restatement of the reference's
+shader math) on the host cores on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cascade trace+merge ms/frame & Mrays/s @720p: plain vs learned cache, ≤2% RMSE"
+WIDTH, HEIGHT, PROBE_PX = 1280, 720, 4
+RAYS_PER_RECEIVER = 36
+EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
+L2_FLUSH_BYTES = 512 << 20
+LAUNCHES_PER_FRAME_FIXED = 8  # clear, 3 seed, layout, clear entries, trace, pack
+
+
+def settings_for_workload():
+    import bevy_penumbra_b200 as bp
+    return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=8, base_columns=8, base_rows=4,
+                               interval_ratio=2.0, interval_rule=bp.INTERVAL_ENDS_GEOMETRIC,
+                               layout=bp.LAYOUT_SPLIT, rays_per_receiver=RAYS_PER_RECEIVER,
+                               emissive_samples=16).sanitized()
+
+
+def world_normals(packed, hits, dirs):
+    """Geometric normals of hit triangles in world space, facing the ray."""
+    sw = packed.scene_words
+    gw = packed.geometry_words
+    header = sw[0]
+    inst = hits["instance"].astype(np.int64)
+    tri = hits["triangle"].astype(np.int64)
+    base = header[1] + inst * header[3]
+    idx = gw[1 + tri][:, :3].astype(np.int64)
+    vb = int(gw[0][1])
+    verts = gw[vb + idx * 5][:, :, :3].view(np.float32).astype(np.float64)  # (n, 3, 3)
+    rows = np.stack([sw[base + 3 + r].view(np.float32).astype(np.float64) for r in range(3)], axis=1)  # (n,3,4)
+    world = np.einsum("nrc,nvc->nvr", rows[:, :, :3], verts) + rows[:, None, :, 3]
+    n = np.cross(world[:, 1] - world[:, 0], world[:, 2] - world[:, 0])
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-30)
+    flip = np.sum(n * dirs, axis=1) > 0
+    n[flip] = -n[flip]
+    return n.astype(np.float32)
+
+
+def build_workload(device: int = 0, host_only: bool = False):
+    """Scene, receivers and resolve points (primary hits of the camera).
+
+    host_only: the reference arm finds the primary hits with the CPU oracle
+    and touches no GPU code (the hits are bit-identical either way)."""
+    import bevy_penumbra_b200 as bp
+    from bevy_penumbra_b200 import scenes
+
+    t0 = time.time()
+    desc = scenes.atrium(seed=2, triangles=262_144)
+    packed = bp.PackedScene.from_desc(desc)
+    ctx = scene = None
+    if not host_only:
+        import torch
+        stream = torch.cuda.current_stream(device)
+        ctx = bp.LuxContext(device, stream.cuda_stream)
+        scene = bp.GpuScene(ctx, packed)
+
+    def primary(stride):
+        o, d = scenes.camera_rays(WIDTH, HEIGHT, EYE, TARGET, 60.0, stride)
+        rays = np.zeros(len(o), dtype=bp.RAY_DTYPE)
+        rays["origin"] = o
+        rays["direction"] = d
+        rays["limit"] = 1e20
+        if host_only:
+            import oracle
+            hits, _ = oracle.OracleScene.from_packed(packed).trace_rays(rays)
+        else:
+            import torch
+            d_rays = torch.from_numpy(rays.view(np.uint8).copy()).to(f"cuda:{device}")
+            d_hits = torch.zeros(len(rays) * bp.HIT_DTYPE.itemsize, dtype=torch.uint8, device=f"cuda:{device}")
+            bp.trace_rays(ctx, scene, d_rays.data_ptr(), len(rays), d_hits.data_ptr())
+            torch.cuda.synchronize(device)
+            hits = d_hits.cpu().numpy().view(bp.HIT_DTYPE)
+        ok = hits["triangle"] != 0xFFFFFFFF
+        pos = np.zeros((int(ok.sum()), 4), np.float32)
+        pos[:, :3] = o[ok] + d[ok] * hits["distance"][ok, None]
+        nrm = np.zeros_like(pos)
+        nrm[:, :3] = world_normals(packed, hits[ok], d[ok])
+        return pos, nrm
+
+    rpos, rnrm = primary(PROBE_PX)
+    if host_only:
+        ppos, pnrm = rpos[:0], rnrm[:0]
+    else:
+        ppos, pnrm = primary(1)
+    settings = settings_for_workload()
+    # Exact record counts per level (cells holding a receiver x directions).
+    entries = 0
+    cells_max = 0
+    for level in range(settings.levels):
+        s = np.float32(settings.probe_spacing * (1 << level))
+        cells = np.unique(np.floor(rpos[:, :3] / s).astype(np.int64), axis=0).shape[0]
+        cells_max = max(cells_max, cells)
+        entries += cells * settings.direction_count(level)
+    view = None if host_only else bp.SplitView(ctx, max_receivers=len(rpos), max_cells=cells_max,
+                                               max_entries=entries)
+    return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, rpos=rpos,
+                rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, setup_s=time.time() - t0)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_sample(w, fraction_receivers: int, threads: int):
+    """The oracle (CPU restatement) on every `fraction_receivers`-th receiver."""
+    import oracle
+
+    rpos = np.ascontiguousarray(w["rpos"][::fraction_receivers])
+    rnrm = np.ascontiguousarray(w["rnrm"][::fraction_receivers])
+    oscene = oracle.OracleScene.from_packed(w["packed"])
+    settings = w["settings"]
+    t0 = time.perf_counter()
+    frame = oracle.OracleFrame(oscene, settings.to_c(), rpos, rnrm, threads=threads)
+    dt = time.perf_counter() - t0
+    st = frame.stats()
+    rays = int(st.interval_rays)
+    frame.close()
+    return rays, dt, len(rpos)
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the CPU restatement on the host cores."""
+    if rank != 0:
+        return
+    w = build_workload(0, host_only=True)
+    threads = os.cpu_count() or 1
+    stride = 64
+    for _ in range(max(args.warmup, 0) and 1):
+        cpu_sample(w, stride * 4, threads)
+    times, rays_done = [], 0
+    for _ in range(args.steps):
+        rays, dt, n = cpu_sample(w, stride, threads)
+        times.append(dt)
+        rays_done = rays
+    dt = float(np.median(times))
+    full_rays = len(w["rpos"]) * RAYS_PER_RECEIVER
+    mrays = rays_done / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mrays, "unit": "Mrays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 * full_rays / rays_done,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(w),
+        "cpu_baseline": {"value": mrays, "unit": "Mrays/s", "cores": threads, "kind": "port",
+                         "sample": f"every {stride}th receiver ({rays_done} interval rays of {full_rays}) per step"},
+        "e2e": {"value": mrays, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(w):
+    s = w["settings"]
+    return {"workload": "atrium 262144 tris, 1280x720 screen receivers at 4x4 px, 8 cascades",
+            "triangles": w["desc"].world_triangles(), "receivers": int(len(w["rpos"])),
+            "rays_per_receiver": RAYS_PER_RECEIVER, "interval_rays": int(len(w["rpos"]) * RAYS_PER_RECEIVER),
+            "levels": s.levels, "base_directions": s.base_columns * s.base_rows,
+            "emissive_samples": s.emissive_samples, "resolve_points": int(len(w["ppos"])),
+            "records": int(w["entries"]), "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps"}
+
+
+def run_ours(args, rank, world):
+    import torch
+
+    device = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    w = build_workload(device)
+    bp, ctx, scene, view, settings = w["bp"], w["ctx"], w["scene"], w["view"], w["settings"]
+    stream = torch.cuda.current_stream(device)
+    dev = f"cuda:{device}"
+    d_rpos = torch.from_numpy(w["rpos"]).to(dev)
+    d_rnrm = torch.from_numpy(w["rnrm"]).to(dev)
+    d_ppos = torch.from_numpy(w["ppos"]).to(dev)
+    d_pnrm = torch.from_numpy(w["pnrm"]).to(dev)
+    d_out = torch.empty((len(w["ppos"]), 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    n_recv, n_pts = len(w["rpos"]), len(w["ppos"])
+    view.set_timing(True)
+
+    def frame(step):
+        s = settings
+        s.frame_index = step
+        view.trace_merge(scene, s, d_rpos.data_ptr(), d_rnrm.data_ptr(), n_recv)
+
+    for step in range(args.warmup):
+        frame(step)
+        view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
+    torch.cuda.synchronize(device)
+    st = view.stats()
+    if st.error_flags:
+        raise RuntimeError(f"view capacity exceeded: flags {st.error_flags}")
+    interval_rays = int(st.interval_rays)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    step_ms, trace_ms, merge_ms, seed_ms, pack_ms, resolve_ms = [], [], [], [], [], []
+    with ClockSampler(device) as clocks:
+        for step in range(args.steps):
+            flush.fill_(float(step))
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            frame(args.warmup + step)
+            end.record(stream)
+            torch.cuda.synchronize(device)
+            step_ms.append(start.elapsed_time(end))
+            t = view.timings()
+            trace_ms.append(t.trace_ms)
+            merge_ms.append(t.merge_ms)
+            seed_ms.append(t.seed_ms)
+            pack_ms.append(t.pack_ms)
+            view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
+            resolve_ms.append(view.timings().resolve_ms)
+    torch.cuda.synchronize(device)
+    st = view.stats()
+    total_ms = float(np.sum(step_ms))
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * interval_rays * args.steps / (total_ms * 1e-3) / 1e6
+
+    # e2e: host buffers through lux_view_frame_host (copies + trace/merge + resolve).
+    pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
+    h_rpos, h_rnrm, h_ppos, h_pnrm = pin(w["rpos"]), pin(w["rnrm"]), pin(w["ppos"]), pin(w["pnrm"])
+    h_out = torch.empty((n_pts, 4), dtype=torch.float32).pin_memory().numpy()
+    e2e_ms = []
+    for step in range(args.warmup + args.steps):
+        flush.fill_(float(step))
+        torch.cuda.synchronize(device)
+        settings.frame_index = step
+        t0 = time.perf_counter()
+        view.frame_host(scene, settings, h_rpos, h_rnrm, h_ppos, h_pnrm, h_out)
+        dt = (time.perf_counter() - t0) * 1e3
+        if step >= args.warmup:
+            e2e_ms.append(dt)
+    e2e_total = float(np.sum(e2e_ms))
+    if dist:
+        t = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * interval_rays * args.steps / (e2e_total * 1e-3) / 1e6
+
+    if rank == 0:
+        peak, peak_kind = measured_peaks()
+        lay = scene.layout()
+        alg_bytes = (int(st.nodes_visited) * lay["node_bytes"] + int(st.triangles_tested) * lay["triangle_bytes"]
+                     + int(st.instances_visited) * 64)
+        trace_s = float(np.median(trace_ms)) * 1e-3
+        achieved = alg_bytes / trace_s / 1e9
+        cpu_rays, cpu_dt, cpu_recv = cpu_sample(w, 64, os.cpu_count() or 1)
+        line = {
+            "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_config(w),
+            "stages_ms": {"seed": float(np.median(seed_ms)), "trace": float(np.median(trace_ms)),
+                          "merge": float(np.median(merge_ms)), "pack": float(np.median(pack_ms)),
+                          "resolve": float(np.median(resolve_ms))},
+            "rays": {"interval": interval_rays, "shadow": int(st.shadow_rays),
+                     "trace_mrays_s": interval_rays / trace_s / 1e6,
+                     "all_rays_trace_mrays_s": (interval_rays + int(st.shadow_rays)) / trace_s / 1e6},
+            "roofline": {"kernel": "trace_split_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "algorithmic_bytes": alg_bytes},
+            "cpu_baseline": {"value": cpu_rays / cpu_dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
+                             "kind": "port",
+                             "sample": f"every 64th receiver ({cpu_recv} receivers, {cpu_rays} interval rays)"},
+            "e2e": {"value": e2e_value, "unit": "Mrays/s", "ms_per_step": e2e_total / args.steps,
+                    "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
+                    "d2h_bytes_per_step": int(n_pts * 16)},
+            "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
+            "clocks": clocks.summary(),
+            "setup_s": w["setup_s"],
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,401 @@
+"""bevy_penumbra_b200 - B200 Split Radiance Cascades transport for bevy_lux.
+
+Host-side mirror of the reference's settings surface and plugin
+(``RadianceCascades``, ``SamplingSettings``, ``RadianceCascadesPlugin``,
+src/lib.rs:343-900) over the C ABI of liblux.so (include/lux.h).  Every
+compute call goes to the sm_100a kernels of liblux; nothing here computes
+transport on the host.
+
+Typical frame (render(), src/render.rs:9124-9830):
+
+    plugin = RadianceCascadesPlugin()
+    ctx = plugin.build()                       # device context
+    packed = PackedScene.from_desc(scenes.cornell())
+    scene = GpuScene(ctx, packed)               # lux_scene_upload
+    view = SplitView(ctx, max_receivers=4096, max_cells=8192, max_entries=1 << 22)
+    view.trace_merge(scene, settings, receivers_pos, receivers_nrm)
+    irradiance = view.resolve(settings, points_pos, points_nrm)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field, replace
+
+import numpy as np
+
+from . import _native as N
+from ._native import LuxError, check, lib
+
+__all__ = [
+    "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "LuxError", "trace_rays",
+    "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
+]
+
+LAYOUT_SPLIT = N.LUX_LAYOUT_SPLIT
+LAYOUT_DENSE = N.LUX_LAYOUT_DENSE
+INTERVAL_ENDS_GEOMETRIC = N.LUX_INTERVAL_ENDS_GEOMETRIC
+INTERVAL_LENGTHS_GEOMETRIC = N.LUX_INTERVAL_LENGTHS_GEOMETRIC
+
+
+@dataclass
+class SamplingSettings:
+    """SamplingSettings (src/lib.rs:343-413); this path reads resolve_scale."""
+    grid_divisor: int = 0
+    max_receiver_cells: int = 0
+    max_updates_per_frame: int = 0
+    max_cache_entries: int = 0
+    max_traversal_queries: int = 0
+    resolve_scale: int = 1
+
+    @staticmethod
+    def unlimited() -> "SamplingSettings":
+        return SamplingSettings()
+
+    @staticmethod
+    def low_end() -> "SamplingSettings":
+        return SamplingSettings(8, 16_384, 1_024, 16_384, 16_384, 2)
+
+    def sanitized(self) -> "SamplingSettings":
+        def clamp(v, lo, hi):
+            return v if v == 0 else min(max(v, lo), hi)
+        return SamplingSettings(
+            clamp(self.grid_divisor, 1, 256), clamp(self.max_receiver_cells, 1, 131_072),
+            clamp(self.max_updates_per_frame, 1, 131_072), clamp(self.max_cache_entries, 1, 262_144),
+            clamp(self.max_traversal_queries, 1, 131_072), min(max(self.resolve_scale, 1), 8))
+
+
+@dataclass
+class RadianceCascades:
+    """Per-camera settings (RadianceCascades, src/lib.rs:431-518) plus the
+    cascade-shape extensions the reference hard-codes (levels, base direction
+    grid, interval growth) and the probe layout."""
+    probe_spacing: float = 0.25
+    interval_length: float = 0.4
+    normal_bias: float = 0.005
+    intensity: float = 1.0
+    environment: tuple = (0.0, 0.0, 0.0)
+    emissive_samples: int = 16
+    sampling: SamplingSettings = field(default_factory=SamplingSettings)
+    exposure: float = 1.0
+    levels: int = 4
+    base_columns: int = 8
+    base_rows: int = 4
+    interval_ratio: float = 4.0
+    interval_rule: int = INTERVAL_ENDS_GEOMETRIC
+    layout: int = LAYOUT_SPLIT
+    rays_per_receiver: int = 1
+    frame_index: int = 0
+
+    @staticmethod
+    def low_end() -> "RadianceCascades":
+        """RadianceCascades::low_end() (src/lib.rs:700-722), the fields this path reads."""
+        return RadianceCascades(probe_spacing=1.0, interval_length=1.6, emissive_samples=4,
+                                sampling=SamplingSettings.low_end())
+
+    def to_c(self) -> N.LuxSettings:
+        s = N.LuxSettings()
+        s.probe_spacing = self.probe_spacing
+        s.interval_length = self.interval_length
+        s.normal_bias = self.normal_bias
+        s.intensity = self.intensity
+        for i in range(3):
+            s.environment[i] = self.environment[i]
+        s.exposure = self.exposure
+        s.emissive_samples = _u32(self.emissive_samples)
+        s.levels = _u32(self.levels)
+        s.base_columns = _u32(self.base_columns)
+        s.base_rows = _u32(self.base_rows)
+        s.interval_ratio = self.interval_ratio
+        s.interval_rule = _u32(self.interval_rule)
+        s.layout = _u32(self.layout)
+        s.rays_per_receiver = _u32(self.rays_per_receiver)
+        s.frame_index = _u32(self.frame_index)
+        s.resolve_scale = _u32(self.sampling.resolve_scale)
+        return s
+
+    @staticmethod
+    def from_c(s: N.LuxSettings, sampling: SamplingSettings | None = None) -> "RadianceCascades":
+        sampling = replace(sampling or SamplingSettings(), resolve_scale=int(s.resolve_scale))
+        return RadianceCascades(
+            probe_spacing=s.probe_spacing, interval_length=s.interval_length, normal_bias=s.normal_bias,
+            intensity=s.intensity, environment=tuple(s.environment), emissive_samples=int(s.emissive_samples),
+            sampling=sampling, exposure=s.exposure, levels=int(s.levels), base_columns=int(s.base_columns),
+            base_rows=int(s.base_rows), interval_ratio=s.interval_ratio, interval_rule=int(s.interval_rule),
+            layout=int(s.layout), rays_per_receiver=int(s.rays_per_receiver), frame_index=int(s.frame_index))
+
+    def sanitized(self) -> "RadianceCascades":
+        """RadianceCascades::sanitized() (src/lib.rs:731-759), evaluated by liblux."""
+        s = self.to_c()
+        lib().lux_settings_sanitize(C.byref(s))
+        return RadianceCascades.from_c(s, self.sampling.sanitized())
+
+    def interval_end(self, level: int) -> float:
+        s = self.to_c()
+        return float(lib().lux_interval_end(C.byref(s), level))
+
+    def direction_count(self, level: int) -> int:
+        s = self.to_c()
+        return int(lib().lux_direction_count(C.byref(s), level))
+
+
+def _u32(v) -> int:
+    v = int(v)
+    return v & 0xFFFFFFFF if v >= 0 else 0
+
+
+class RadianceCascadesStatus:
+    """Deduplicated failure strings (RadianceCascadesStatus::record_failure,
+    src/lib.rs:225-230)."""
+
+    def __init__(self):
+        self._failures: list[str] = []
+
+    def record_failure(self, message: str) -> None:
+        if message not in self._failures:
+            self._failures.append(message)
+
+    def failures(self) -> list[str]:
+        return list(self._failures)
+
+
+@dataclass
+class RadianceCascadesPlugin:
+    """RadianceCascadesPlugin (src/lib.rs:795-900): budgets, and `build`
+    creates the device context that render() would use."""
+    scene_gpu_budget_bytes: int = 256 * 1024 * 1024
+    view_gpu_budget_bytes: int = 2 * 1024 * 1024 * 1024
+    device: int = 0
+
+    @staticmethod
+    def low_end() -> "RadianceCascadesPlugin":
+        return RadianceCascadesPlugin(scene_gpu_budget_bytes=256 * 1024 * 1024,
+                                      view_gpu_budget_bytes=512 * 1024 * 1024)
+
+    def build(self, stream: int | None = None) -> "LuxContext":
+        return LuxContext(self.device, stream)
+
+
+class LuxContext:
+    """A liblux context on one device (lux_context_create)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        desc = N.LuxDeviceDesc(device, stream or None)
+        handle = C.c_void_p()
+        check(lib().lux_context_create(C.byref(desc), C.byref(handle)))
+        self.handle = handle
+        self.status = RadianceCascadesStatus()
+
+    def check(self, status: int) -> None:
+        if status != N.LUX_OK:
+            raw = lib().lux_last_error_message(self.handle)
+            message = raw.decode() if raw else ""
+            self.status.record_failure(message)
+            raise LuxError(status, message)
+
+    def synchronize(self) -> None:
+        self.check(lib().lux_context_synchronize(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data if a is not None and a.size else 0
+
+
+class PackedScene:
+    """The reference's scene word streams (src/scene.rs:2096-2117, :809-823)
+    produced by liblux's native packer (lux_scene_pack)."""
+
+    def __init__(self, scene_words: np.ndarray, geometry_words: np.ndarray, lights: np.ndarray,
+                 instance_order: np.ndarray | None = None, blas_cost: float = 0.0, max_depth: int = 0,
+                 tlas_nodes: int = 0, blas_nodes: int = 0):
+        self.scene_words = np.ascontiguousarray(scene_words, dtype=np.uint32).reshape(-1, 4)
+        self.geometry_words = np.ascontiguousarray(geometry_words, dtype=np.uint32).reshape(-1, 4)
+        self.lights = np.ascontiguousarray(lights, dtype=np.uint32).reshape(-1, 24)
+        self.instance_order = instance_order
+        self.blas_cost = blas_cost
+        self.max_depth = max_depth
+        self.tlas_nodes = tlas_nodes
+        self.blas_nodes = blas_nodes
+
+    @staticmethod
+    def pack(positions, indices, mesh_first, mesh_count, instance_mesh, instance_transform, instance_flags,
+             instance_material, materials) -> "PackedScene":
+        L = lib()
+        positions = np.ascontiguousarray(positions, dtype=np.float32).reshape(-1, 3)
+        indices = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1, 3)
+        mesh_first = np.ascontiguousarray(mesh_first, dtype=np.uint32)
+        mesh_count = np.ascontiguousarray(mesh_count, dtype=np.uint32)
+        imesh = np.ascontiguousarray(instance_mesh, dtype=np.uint32)
+        ixf = np.ascontiguousarray(instance_transform, dtype=np.float32).reshape(-1, 12)
+        iflags = np.ascontiguousarray(instance_flags, dtype=np.uint32)
+        imat = np.ascontiguousarray(instance_material, dtype=np.uint32)
+        mats = np.ascontiguousarray(materials, dtype=np.uint32).reshape(-1, 32)
+        handle = C.c_void_p()
+        status = L.lux_scene_pack(_ptr(positions), len(positions), _ptr(indices), len(indices), _ptr(mesh_first),
+                                  _ptr(mesh_count), len(mesh_first), _ptr(imesh), _ptr(ixf), _ptr(iflags),
+                                  _ptr(imat), len(imesh), _ptr(mats), len(mats), C.byref(handle))
+        check(status)
+        try:
+            sw, gw, nl = C.c_size_t(), C.c_size_t(), C.c_size_t()
+            tn, bn = C.c_uint32(), C.c_uint32()
+            check(L.lux_packed_scene_sizes(handle, C.byref(sw), C.byref(gw), C.byref(nl), C.byref(tn),
+                                           C.byref(bn)))
+            scene_words = np.zeros((sw.value, 4), dtype=np.uint32)
+            geometry_words = np.zeros((gw.value, 4), dtype=np.uint32)
+            lights = np.zeros((nl.value, 24), dtype=np.uint32)
+            check(L.lux_packed_scene_copy(handle, _ptr(scene_words), _ptr(geometry_words), _ptr(lights)))
+            order = np.zeros(len(imesh), dtype=np.uint32)
+            if len(imesh):
+                check(L.lux_packed_scene_instance_order(handle, _ptr(order)))
+            cost, depth = C.c_double(), C.c_uint32()
+            check(L.lux_packed_scene_quality(handle, C.byref(cost), C.byref(depth)))
+        finally:
+            L.lux_packed_scene_destroy(handle)
+        return PackedScene(scene_words, geometry_words, lights, order, cost.value, depth.value, tn.value, bn.value)
+
+    @staticmethod
+    def from_desc(desc) -> "PackedScene":
+        positions, indices, first, count = desc.arrays()
+        return PackedScene.pack(positions, indices, first, count, desc.instance_mesh,
+                                np.stack(desc.instance_transform), desc.instance_flags, desc.instance_material,
+                                np.stack(desc.materials))
+
+
+class GpuScene:
+    """A scene resident on the device (lux_scene_upload)."""
+
+    def __init__(self, ctx: LuxContext, packed: PackedScene):
+        self.ctx = ctx
+        self.packed = packed
+        handle = C.c_void_p()
+        ctx.check(lib().lux_scene_upload(ctx.handle, _ptr(packed.scene_words), len(packed.scene_words),
+                                         _ptr(packed.geometry_words), len(packed.geometry_words),
+                                         _ptr(packed.lights), len(packed.lights), 0, C.byref(handle)))
+        self.handle = handle
+
+    def layout(self) -> dict:
+        vals = [C.c_uint32() for _ in range(5)]
+        self.ctx.check(lib().lux_scene_layout(self.handle, *[C.byref(v) for v in vals]))
+        keys = ("nodes", "node_bytes", "triangles", "triangle_bytes", "instances")
+        return {k: v.value for k, v in zip(keys, vals)}
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+RAY_DTYPE = np.dtype([("origin", "<f4", 3), ("tmin", "<f4"), ("direction", "<f4", 3), ("limit", "<f4")])
+HIT_DTYPE = np.dtype([("distance", "<f4"), ("triangle", "<u4"), ("instance", "<u4"), ("errors", "<u4"),
+                      ("barycentric", "<f4", 3), ("visited", "<u4")])
+
+
+def trace_rays(ctx: LuxContext, scene: GpuScene, rays_device_ptr: int, count: int, hits_device_ptr: int,
+               any_hit: bool = False) -> None:
+    """lux_trace_rays on device buffers of RAY_DTYPE / HIT_DTYPE records."""
+    ctx.check(lib().lux_trace_rays(ctx.handle, scene.handle, rays_device_ptr, count, 1 if any_hit else 0,
+                                   hits_device_ptr))
+
+
+class SplitView:
+    """Per-view transport state (ViewBuffers) and one frame of
+    seed -> trace -> deposit -> merge -> pack, then resolve."""
+
+    def __init__(self, ctx: LuxContext, max_receivers: int, max_cells: int, max_entries: int):
+        self.ctx = ctx
+        desc = N.LuxViewDesc(max_receivers, max_cells, max_entries)
+        handle = C.c_void_p()
+        ctx.check(lib().lux_view_create(ctx.handle, C.byref(desc), C.byref(handle)))
+        self.handle = handle
+        self.desc = desc
+        self.settings: RadianceCascades | None = None
+
+    def trace_merge(self, scene: GpuScene, settings: RadianceCascades, position_ptr: int, normal_ptr: int,
+                    count: int) -> None:
+        """Device pointers to float4 receiver positions / normals."""
+        s = settings.to_c()
+        rc = N.LuxReceivers(position_ptr, normal_ptr, count)
+        self.ctx.check(lib().lux_view_trace_merge(self.handle, scene.handle, C.byref(s), C.byref(rc)))
+        self.settings = settings
+
+    def resolve(self, settings: RadianceCascades, position_ptr: int, normal_ptr: int, count: int,
+                out_ptr: int) -> None:
+        s = settings.to_c()
+        self.ctx.check(lib().lux_view_resolve(self.handle, C.byref(s), position_ptr, normal_ptr, count, out_ptr))
+
+    def frame_host(self, scene: GpuScene, settings: RadianceCascades, receiver_pos: np.ndarray,
+                   receiver_nrm: np.ndarray, point_pos: np.ndarray, point_nrm: np.ndarray,
+                   out: np.ndarray | None = None) -> np.ndarray:
+        """One frame from host buffers (lux_view_frame_host)."""
+        if out is None:
+            out = np.zeros((len(point_pos), 4), dtype=np.float32)
+        s = settings.to_c()
+        self.ctx.check(lib().lux_view_frame_host(self.handle, scene.handle, C.byref(s), _ptr(receiver_pos),
+                                                 _ptr(receiver_nrm), len(receiver_pos), _ptr(point_pos),
+                                                 _ptr(point_nrm), len(point_pos), _ptr(out)))
+        return out
+
+    def set_timing(self, enable: bool = True) -> None:
+        self.ctx.check(lib().lux_view_set_timing(self.handle, 1 if enable else 0))
+
+    def timings(self) -> N.LuxTimings:
+        t = N.LuxTimings()
+        self.ctx.check(lib().lux_view_timings(self.handle, C.byref(t)))
+        return t
+
+    def stats(self) -> N.LuxStats:
+        st = N.LuxStats()
+        self.ctx.check(lib().lux_view_stats(self.handle, C.byref(st)))
+        return st
+
+    def read_level(self, level: int):
+        """(keys int32[cells,4], merged f32[cells,dirs,4], raw f32[cells,dirs,4], samples u32[cells,dirs])."""
+        st = self.stats()
+        cells = int(st.cells[level])
+        dirs = self.settings.direction_count(level)
+        keys = np.zeros((cells, 4), dtype=np.int32)
+        merged = np.zeros((cells, dirs, 4), dtype=np.float32)
+        raw = np.zeros((cells, dirs, 4), dtype=np.float32)
+        samples = np.zeros((cells, dirs), dtype=np.uint32)
+        if cells:
+            self.ctx.check(lib().lux_view_read_level(self.handle, level, _ptr(keys), _ptr(merged), _ptr(raw),
+                                                     _ptr(samples)))
+        return keys, merged, raw, samples
+
+    def read_probes(self):
+        st = self.stats()
+        cells = int(st.cells[0])
+        keys = np.zeros((cells, 4), dtype=np.int32)
+        tables = np.zeros((cells, 36, 4), dtype=np.float32)
+        if cells:
+            self.ctx.check(lib().lux_view_read_probes(self.handle, _ptr(keys), _ptr(tables)))
+        return keys, tables
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_view_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,74 @@
+// lux_internal.h - host-side structures shared by the library's sources.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/lux.h"
+
+#include <cuda_runtime.h>
+
+// Device BVH4 node: child boxes in structure-of-arrays order so one warp lane
+// reads the node with eight 128-bit loads.  child[i]:
+//   kEmpty                   empty slot
+//   bit 31 clear             inner node index
+//   bit 31 set               leaf: bits 0..26 first element, bits 27..30 count-1
+struct alignas(16) Bvh4Node {
+    float lo_x[4], hi_x[4];
+    float lo_y[4], hi_y[4];
+    float lo_z[4], hi_z[4];
+    uint32_t child[4];
+    uint32_t pad[4];
+};
+static_assert(sizeof(Bvh4Node) == 128, "BVH4 node must be one 128-byte line");
+
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr uint32_t kLeafFirstMask = (1u << 27) - 1u;
+constexpr uint32_t kLeafMaxCount = 16u;
+
+// Device instance record (64 bytes): local_from_world rows, BLAS root node,
+// triangle range and flags (pack_instances rows 0-2 and word 8, word 6.w).
+struct alignas(16) DeviceInstance {
+    float row[3][4];
+    uint32_t root;
+    uint32_t first;
+    uint32_t count;
+    uint32_t flags;
+};
+
+// Scene data as the kernels see it (all device pointers).
+struct SceneView {
+    const Bvh4Node *nodes;
+    const float4 *triangles;        // 3 float4 per triangle (local positions)
+    const DeviceInstance *instances;
+    const uint4 *scene_words;       // verbatim reference words (materials, transforms)
+    const uint4 *geometry_words;    // verbatim reference words (indices, vertices)
+    const LuxLight *lights;
+    uint32_t tlas_root;             // BVH4 node index of the TLAS root
+    uint32_t instance_count;
+    uint32_t triangle_count;
+    uint32_t scene_word_count;
+    uint32_t geometry_word_count;
+    uint32_t conventional_lights;
+    uint32_t emissive_lights;
+    float root_lo[3], root_hi[3];   // binary TLAS root box (root test of traceRayTracked)
+};
+
+struct LuxContext {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool owns_stream = false;
+    std::string last_error;
+    int sm_count = 148;
+};
+
+struct LuxScene {
+    LuxContext *ctx = nullptr;
+    SceneView view{};
+    void *d_nodes = nullptr, *d_tris = nullptr, *d_inst = nullptr, *d_sw = nullptr, *d_gw = nullptr,
+         *d_lights = nullptr;
+    uint32_t node_count = 0;
+};
+
+lux_status lux_fail(LuxContext *ctx, lux_status status, const std::string &message);
+lux_status lux_cuda_check(LuxContext *ctx, int err, const char *what);

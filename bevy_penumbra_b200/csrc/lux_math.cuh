@@ -1,0 +1,226 @@
+// lux_math.cuh - device math of the Split transport path.
+//
+// Evaluation contract: every expression is IEEE binary32, evaluated in the
+// order written, without fused multiply-add contraction (the library is
+// compiled with --fmad=false) and with IEEE division and square root.  The
+// reference computes these on its GPU; the formulas and the order of
+// operations follow the Slang sources cited at each function.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define LUX_HD __host__ __device__ __forceinline__
+#else
+#define LUX_HD inline
+#endif
+
+namespace lux {
+
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr uint32_t kQueryUnsupported = 4u;  // shaders/traversal.slang:16
+constexpr float kPi = 3.14159265358979323846f;
+
+struct f3 {
+    float x, y, z;
+};
+LUX_HD f3 make3(float x, float y, float z) { return f3{x, y, z}; }
+LUX_HD f3 operator+(f3 a, f3 b) { return f3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+LUX_HD f3 operator-(f3 a, f3 b) { return f3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+LUX_HD f3 operator-(f3 a) { return f3{-a.x, -a.y, -a.z}; }
+LUX_HD f3 operator*(f3 a, float s) { return f3{a.x * s, a.y * s, a.z * s}; }
+LUX_HD f3 operator*(f3 a, f3 b) { return f3{a.x * b.x, a.y * b.y, a.z * b.z}; }
+LUX_HD f3 operator/(f3 a, float s) { return f3{a.x / s, a.y / s, a.z / s}; }
+LUX_HD float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+LUX_HD f3 cross(f3 a, f3 b) {
+    return f3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+LUX_HD float comp(f3 v, uint32_t i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+LUX_HD float saturate(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+LUX_HD float fracf(float x) { return x - floorf(x); }
+LUX_HD bool finite3(f3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
+LUX_HD float length(f3 v) { return sqrtf(dot(v, v)); }
+
+LUX_HD float as_float(uint32_t u) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float f;
+    __builtin_memcpy(&f, &u, 4);
+    return f;
+#endif
+}
+LUX_HD uint32_t as_uint(float f) {
+#ifdef __CUDA_ARCH__
+    return __float_as_uint(f);
+#else
+    uint32_t u;
+    __builtin_memcpy(&u, &f, 4);
+    return u;
+#endif
+}
+
+// cos and sin of 2*pi*turns, evaluated identically on host and device:
+// exact reduction to the nearest quarter turn, then the Taylor series of
+// sin(2 pi r) (degree 11) and cos(2 pi r) (degree 10) for |r| <= 1/8
+// (truncation below 3e-8).  Replaces the GPU cos/sin of decodeDirection
+// (shaders/common.slang:376-382).
+LUX_HD void sincos_turns(float turns, float &c, float &s) {
+    float k = floorf(turns * 4.0f + 0.5f);
+    float r = turns - k * 0.25f;
+    int q = ((int)k) & 3;
+    float r2 = r * r;
+    float sp = 42.058693f - r2 * 15.094643f;
+    sp = 76.70586f - r2 * sp;
+    sp = 81.60525f - r2 * sp;
+    sp = 41.3417f - r2 * sp;
+    sp = 6.2831855f - r2 * sp;
+    float sn = r * sp;
+    float cp = 60.24464f - r2 * 26.426256f;
+    cp = 85.45682f - r2 * cp;
+    cp = 64.93939f - r2 * cp;
+    cp = 19.739208f - r2 * cp;
+    float cs = 1.0f - r2 * cp;
+    if (q == 0) {
+        c = cs;
+        s = sn;
+    } else if (q == 1) {
+        c = -sn;
+        s = cs;
+    } else if (q == 2) {
+        c = -cs;
+        s = -sn;
+    } else {
+        c = sn;
+        s = -cs;
+    }
+}
+
+// decodeDirection, shaders/common.slang:376-382.
+LUX_HD f3 decode_direction(float u, float v) {
+    float y = v * 2.0f - 1.0f;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - y * y));
+    float c, s;
+    sincos_turns(u, c, s);
+    return f3{r * c, y, r * s};
+}
+
+// binDirection, shaders/common.slang:395-400 (columns x rows grid).
+LUX_HD f3 bin_direction(uint32_t index, uint32_t columns, uint32_t rows) {
+    float u = ((float)(index % columns) + 0.5f) / (float)columns;
+    float v = ((float)(index / columns) + 0.5f) / (float)rows;
+    return decode_direction(u, v);
+}
+
+// directionIndex, shaders/common.slang:388-394, on the (u, v) of a decoded
+// direction (encodeDirection inverts decodeDirection).
+LUX_HD uint32_t direction_index_uv(float u, float v, uint32_t columns, uint32_t rows) {
+    uint32_t x = (uint32_t)(u * (float)columns);
+    uint32_t y = (uint32_t)(v * (float)rows);
+    x = x > columns - 1u ? columns - 1u : x;
+    y = y > rows - 1u ? rows - 1u : y;
+    return x + y * columns;
+}
+
+// r2, shaders/common.slang:401-406.
+LUX_HD void r2(uint32_t index, float &x, float &y) {
+    uint32_t px = index * 3242174889u;
+    uint32_t py = index * 2447445414u;
+    x = (float)(px >> 8) / 16777216.0f;
+    y = (float)(py >> 8) / 16777216.0f;
+}
+
+// transportHash, shaders/common.slang:281-289.
+LUX_HD uint32_t transport_hash(uint32_t value) {
+    value ^= value >> 16;
+    value *= 0x7feb352du;
+    value ^= value >> 15;
+    value *= 0x846ca68bu;
+    value ^= value >> 16;
+    return value;
+}
+
+// hashKey, shaders/common.slang:423-429.
+LUX_HD uint32_t hash_key(int32_t kx, int32_t ky, int32_t kz, int32_t kw, uint32_t buckets) {
+    uint32_t h = (uint32_t)kx * 0x8da6b343u ^ (uint32_t)ky * 0xd8163841u ^ (uint32_t)kz * 0xcb1ab31fu ^
+                 (uint32_t)kw * 0x165667b1u;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    return h & (buckets - 1u);
+}
+
+// rayOffset, shaders/common.slang:343-359, one axis.
+LUX_HD float ray_offset_axis(float position, float normal, float bias) {
+    float origin = position + normal * bias;
+    int32_t step = (int32_t)(normal * 256.0f);
+    int32_t bits = (int32_t)as_uint(origin);
+    float integer_offset = as_float((uint32_t)(bits + (origin < 0.0f ? -step : step)));
+    float shifted = fabsf(origin) < 0.03125f ? origin + normal / 65536.0f : integer_offset;
+    return isfinite(shifted) ? shifted : position;
+}
+LUX_HD f3 ray_offset(f3 p, f3 n, float bias) {
+    return f3{ray_offset_axis(p.x, n.x, bias), ray_offset_axis(p.y, n.y, bias), ray_offset_axis(p.z, n.z, bias)};
+}
+
+// encodeNormal, shaders/common.slang:360-366.
+LUX_HD void encode_normal(f3 n, float &ox, float &oy) {
+    float d = (fabsf(n.x) + fabsf(n.y)) + fabsf(n.z);
+    n = f3{n.x / d, n.y / d, n.z / d};
+    float px = n.x, py = n.y;
+    if (n.z < 0.0f) {
+        float qx = (1.0f - fabsf(n.y)) * (px >= 0.0f ? 1.0f : -1.0f);
+        float qy = (1.0f - fabsf(n.x)) * (py >= 0.0f ? 1.0f : -1.0f);
+        px = qx;
+        py = qy;
+    }
+    ox = px * 0.5f + 0.5f;
+    oy = py * 0.5f + 0.5f;
+}
+
+// decodeNormal, shaders/common.slang:367-374 (normalize as v / length(v)).
+LUX_HD f3 decode_normal(float ux, float uy) {
+    float px = ux * 2.0f - 1.0f, py = uy * 2.0f - 1.0f;
+    f3 n{px, py, (1.0f - fabsf(px)) - fabsf(py)};
+    float t = saturate(-n.z);
+    n.x = n.x + (n.x >= 0.0f ? -t : t);
+    n.y = n.y + (n.y >= 0.0f ? -t : t);
+    float l = length(n);
+    return f3{n.x / l, n.y / l, n.z / l};
+}
+
+// wrapIrradianceTexel + irradianceTexelIndex, shaders/world_resolve.slang:1-11.
+LUX_HD uint32_t texel_index(int32_t x, int32_t y) {
+    if (x < 0) {
+        int32_t nx = -x - 1, ny = 5 - y;
+        x = nx;
+        y = ny;
+    } else if (x >= 6) {
+        int32_t nx = 11 - x, ny = 5 - y;
+        x = nx;
+        y = ny;
+    }
+    if (y < 0) {
+        int32_t nx = 5 - x, ny = -y - 1;
+        x = nx;
+        y = ny;
+    } else if (y >= 6) {
+        int32_t nx = 5 - x, ny = 11 - y;
+        x = nx;
+        y = ny;
+    }
+    return (uint32_t)(y * 6 + x);
+}
+
+// Cell keys of the world grid: 21 bits per axis, biased by 2^20.
+LUX_HD uint64_t pack_cell(int32_t x, int32_t y, int32_t z) {
+    return ((uint64_t)((uint32_t)(x + (1 << 20)) & 0x1fffffu)) |
+           ((uint64_t)((uint32_t)(y + (1 << 20)) & 0x1fffffu) << 21) |
+           ((uint64_t)((uint32_t)(z + (1 << 20)) & 0x1fffffu) << 42);
+}
+LUX_HD bool cell_in_range(int32_t x, int32_t y, int32_t z) {
+    const int32_t lim = 1 << 20;
+    return x >= -lim && x < lim && y >= -lim && y < lim && z >= -lim && z < lim;
+}
+constexpr uint64_t kEmptyCell = 0xffffffffffffffffull;
+
+}  // namespace lux

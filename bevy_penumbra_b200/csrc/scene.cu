@@ -1,0 +1,376 @@
+// scene.cu - scene upload (reference words -> device BVH4) and the
+// traversal harness entry point lux_trace_rays.
+//
+// Upload validates the reference's word streams (src/scene.rs:2096-2117,
+// :809-823), collapses every binary BVH built by build_tree
+// (src/scene.rs:2398-2554) into a 4-wide BVH whose child boxes are the binary
+// nodes' boxes, gathers triangle positions into leaf order (3 x 16 bytes per
+// triangle), and keeps the verbatim words on the device for hit shading.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "lux_internal.h"
+#include "lux_math.cuh"
+#include "traverse.cuh"
+
+namespace {
+
+struct BinNode {
+    float mn[3], mx[3];
+    uint32_t first, count;
+};
+
+inline float fword(const uint32_t *w, size_t i) {
+    float f;
+    std::memcpy(&f, &w[i], 4);
+    return f;
+}
+
+struct Collapser {
+    const std::vector<BinNode> &bin;
+    std::vector<Bvh4Node> &out;
+    std::string error;
+    uint32_t leaf_limit;  // elements addressable by a leaf (triangles or instances)
+
+    static double area(const BinNode &n) {
+        double sx = (double)n.mx[0] - n.mn[0], sy = (double)n.mx[1] - n.mn[1], sz = (double)n.mx[2] - n.mn[2];
+        return 2.0 * (sx * sy + sy * sz + sz * sx);
+    }
+
+    uint32_t new_node() {
+        Bvh4Node n;
+        for (int i = 0; i < 4; ++i) {
+            n.lo_x[i] = n.lo_y[i] = n.lo_z[i] = INFINITY;
+            n.hi_x[i] = n.hi_y[i] = n.hi_z[i] = -INFINITY;
+            n.child[i] = lux::kEmpty;
+            n.pad[i] = 0;
+        }
+        out.push_back(n);
+        return (uint32_t)out.size() - 1;
+    }
+
+    void set_child(uint32_t node, int slot, const float mn[3], const float mx[3], uint32_t payload) {
+        Bvh4Node &n = out[node];
+        n.lo_x[slot] = mn[0];
+        n.lo_y[slot] = mn[1];
+        n.lo_z[slot] = mn[2];
+        n.hi_x[slot] = mx[0];
+        n.hi_y[slot] = mx[1];
+        n.hi_z[slot] = mx[2];
+        n.child[slot] = payload;
+    }
+
+    // A leaf of `count` elements as one payload; ranges above 16 elements
+    // become a small subtree of 16-element leaves with the leaf's box.
+    uint32_t leaf_payload(uint32_t first, uint32_t count, const float mn[3], const float mx[3]) {
+        if (count <= kLeafMaxCount) return kLeafBit | (first & kLeafFirstMask) | ((count - 1u) << 27);
+        uint32_t per = (count + 3u) / 4u;
+        uint32_t node = new_node();
+        int slot = 0;
+        for (uint32_t start = 0; start < count && slot < 4; start += per, ++slot) {
+            uint32_t c = std::min(per, count - start);
+            uint32_t p = leaf_payload(first + start, c, mn, mx);
+            set_child(node, slot, mn, mx, p);
+        }
+        return node;
+    }
+
+    // Payload of binary subtree `index`.
+    uint32_t collapse(uint32_t index, int depth) {
+        if (index >= bin.size() || depth > 96) {
+            error = "BVH node index out of range or cyclic";
+            return lux::kEmpty;
+        }
+        const BinNode &b = bin[index];
+        if (b.count > 0) {
+            if ((uint64_t)b.first + b.count > leaf_limit || b.first + b.count > kLeafFirstMask) {
+                error = "BVH leaf range exceeds the element array";
+                return lux::kEmpty;
+            }
+            if (b.count > 256u) {
+                error = "BVH leaf holds more than 256 elements";
+                return lux::kEmpty;
+            }
+            return leaf_payload(b.first, b.count, b.mn, b.mx);
+        }
+        if ((size_t)b.first + 1 >= bin.size()) {
+            error = "BVH child index out of range";
+            return lux::kEmpty;
+        }
+        std::vector<uint32_t> kids = {b.first, b.first + 1};
+        while (kids.size() < 4) {
+            int best = -1;
+            double best_area = -1.0;
+            for (size_t k = 0; k < kids.size(); ++k) {
+                const BinNode &c = bin[kids[k]];
+                if (c.count == 0 && (size_t)c.first + 1 < bin.size()) {
+                    double a = area(c);
+                    if (a > best_area) {
+                        best_area = a;
+                        best = (int)k;
+                    }
+                }
+            }
+            if (best < 0) break;
+            uint32_t c = kids[best];
+            kids.erase(kids.begin() + best);
+            kids.push_back(bin[c].first);
+            kids.push_back(bin[c].first + 1);
+        }
+        uint32_t node = new_node();
+        for (size_t k = 0; k < kids.size(); ++k) {
+            uint32_t p = collapse(kids[k], depth + 1);
+            if (!error.empty()) return lux::kEmpty;
+            set_child(node, (int)k, bin[kids[k]].mn, bin[kids[k]].mx, p);
+        }
+        return node;
+    }
+
+    // Payload usable as a traversal start: a node index.
+    uint32_t root(uint32_t index) {
+        uint32_t p = collapse(index, 0);
+        if (!error.empty()) return lux::kEmpty;
+        if ((p & kLeafBit) == 0u) return p;
+        uint32_t node = new_node();
+        set_child(node, 0, bin[index].mn, bin[index].mx, p);
+        return node;
+    }
+};
+
+__global__ void trace_rays_kernel(SceneView S, const LuxRay *__restrict__ rays, uint32_t count, uint32_t any_hit,
+                                  LuxHit *__restrict__ hits, unsigned long long *__restrict__ counters) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    lux::TraceCounters cn{0, 0, 0};
+    if (i < count) {
+        LuxRay r = rays[i];
+        lux::f3 o{r.origin[0], r.origin[1], r.origin[2]};
+        lux::f3 d{r.direction[0], r.direction[1], r.direction[2]};
+        lux::Hit h;
+        if (any_hit)
+            lux::trace<true>(S, o, d, 0.0f, r.limit, h, cn);
+        else
+            lux::trace<false>(S, o, d, r.tmin, r.limit, h, cn);
+        LuxHit out;
+        out.distance = h.t;
+        out.triangle = h.tri;
+        out.instance = h.inst;
+        out.errors = h.errors;
+        out.barycentric[0] = (1.0f - h.b1) - h.b2;
+        out.barycentric[1] = h.b1;
+        out.barycentric[2] = h.b2;
+        out.visited = cn.nodes;
+        hits[i] = out;
+    }
+    if (counters) {
+        unsigned long long n = cn.nodes, t = cn.triangles, in = cn.instances;
+        for (int off = 16; off > 0; off >>= 1) {
+            n += __shfl_down_sync(0xffffffffu, n, off);
+            t += __shfl_down_sync(0xffffffffu, t, off);
+            in += __shfl_down_sync(0xffffffffu, in, off);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&counters[0], n);
+            atomicAdd(&counters[1], t);
+            atomicAdd(&counters[2], in);
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size_t sn, const uint32_t *gw, size_t gn,
+                                       const LuxLight *lights, uint32_t light_count, uint32_t conventional,
+                                       LuxScene **out) {
+    if (!ctx || !out) return LUX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (!sw || sn < 1 || !gw || gn < 1 || (light_count && !lights) || conventional > light_count)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene upload: missing words or lights");
+    if (conventional != 0)
+        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
+                        "scene upload: conventional (punctual/directional) lights are not supported by this build");
+    if (sn > 0xffffffffu || gn > 0xffffffffu)
+        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: word stream exceeds 2^32 words");
+    // Header (src/scene.rs:2103-2110): material end, instance base, count, stride.
+    uint32_t inst_base = sw[1], inst_count = sw[2], stride = sw[3];
+    if (stride != 9u || (uint64_t)inst_base + (uint64_t)inst_count * 9u > sn)
+        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance records outside the scene words");
+    if (inst_count > kLeafFirstMask)
+        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: too many instances");
+    uint32_t node_words = inst_base - 1u;
+    uint32_t node_count = node_words / 2u;
+    std::vector<BinNode> bin(node_count);
+    for (uint32_t i = 0; i < node_count; ++i) {
+        const uint32_t *a = sw + 4 * (size_t)(1 + 2 * i), *b = sw + 4 * (size_t)(2 + 2 * i);
+        for (int k = 0; k < 3; ++k) {
+            std::memcpy(&bin[i].mn[k], &a[k], 4);
+            std::memcpy(&bin[i].mx[k], &b[k], 4);
+        }
+        bin[i].first = a[3];
+        bin[i].count = b[3];
+    }
+    // Geometry header (src/scene.rs:809-823).
+    uint32_t tri_word = gw[0], vertex_base = gw[1], vertex_stride = gw[2], vertex_count = gw[3];
+    if (tri_word != 1u || vertex_stride != 5u || vertex_base < 1u || (uint64_t)vertex_base + (uint64_t)vertex_count * 5u > gn)
+        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: malformed geometry header");
+    uint32_t tri_capacity = vertex_base - 1u;
+    std::vector<DeviceInstance> inst(inst_count);
+    uint32_t tri_count = 0;
+    for (uint32_t i = 0; i < inst_count; ++i) {
+        const uint32_t *w = sw + 4 * (size_t)(inst_base + 9 * i);
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) inst[i].row[r][c] = fword(w, 4 * r + c);
+        inst[i].flags = w[4 * 6 + 3];
+        uint32_t material = w[4 * 7 + 3];
+        inst[i].first = w[4 * 8 + 1];
+        inst[i].count = w[4 * 8 + 2];
+        inst[i].root = w[4 * 8 + 0];
+        if ((uint64_t)inst[i].first + inst[i].count > tri_capacity)
+            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance triangle range outside geometry");
+        if (inst[i].root >= node_count)
+            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance BLAS root outside the node words");
+        if ((uint64_t)material + 8 > sn)
+            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: material record outside the scene words");
+        const uint32_t *m = sw + 4 * (size_t)material;
+        float cutoff;
+        std::memcpy(&cutoff, &m[7], 4);
+        if (cutoff != -1.0f)
+            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
+                            "scene upload: alpha-tested materials are not supported by this build");
+        const uint32_t *tex = m + 4 * 6;
+        if (tex[0] != lux::kEmpty || tex[1] != lux::kEmpty || tex[2] != lux::kEmpty || tex[3] != lux::kEmpty ||
+            m[4 * 7] != lux::kEmpty)
+            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
+                            "scene upload: textured materials are not supported by this build");
+        tri_count = std::max(tri_count, inst[i].first + inst[i].count);
+    }
+    // Collapse: TLAS from node 0, every distinct BLAS root once.
+    std::vector<Bvh4Node> nodes;
+    nodes.reserve(node_count / 2 + 16);
+    uint32_t tlas_root = lux::kEmpty;
+    float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
+    if (inst_count > 0) {
+        if (node_count == 0) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: no TLAS nodes");
+        Collapser tl{bin, nodes, {}, inst_count};
+        tlas_root = tl.root(0);
+        if (!tl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (TLAS): " + tl.error);
+        for (int k = 0; k < 3; ++k) {
+            root_lo[k] = bin[0].mn[k];
+            root_hi[k] = bin[0].mx[k];
+        }
+    }
+    std::unordered_map<uint32_t, uint32_t> blas_root;
+    for (uint32_t i = 0; i < inst_count; ++i) {
+        auto it = blas_root.find(inst[i].root);
+        if (it == blas_root.end()) {
+            Collapser bl{bin, nodes, {}, tri_capacity};
+            uint32_t r = bl.root(inst[i].root);
+            if (!bl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (BLAS): " + bl.error);
+            it = blas_root.emplace(inst[i].root, r).first;
+        }
+        inst[i].root = it->second;
+    }
+    // Triangle positions in packed (leaf) order.
+    std::vector<float4> tris(3 * (size_t)std::max(tri_count, 1u));
+    for (uint32_t t = 0; t < tri_count; ++t) {
+        const uint32_t *idx = gw + 4 * (size_t)(1 + t);
+        for (int v = 0; v < 3; ++v) {
+            uint32_t vi = idx[v];
+            if (vi >= vertex_count) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: vertex index out of range");
+            const uint32_t *p = gw + 4 * ((size_t)vertex_base + (size_t)vi * 5u);
+            float4 f;
+            std::memcpy(&f.x, &p[0], 4);
+            std::memcpy(&f.y, &p[1], 4);
+            std::memcpy(&f.z, &p[2], 4);
+            f.w = 0.0f;
+            tris[3 * (size_t)t + v] = f;
+        }
+    }
+    if (light_count > conventional) {
+        for (uint32_t l = conventional; l < light_count; ++l)
+            if (lights[l].source[0] >= inst_count || lights[l].source[1] >= tri_capacity)
+                return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: emitter record outside the scene");
+    }
+    LuxScene *S = new LuxScene();
+    S->ctx = ctx;
+    auto alloc_copy = [&](void **dst, const void *src, size_t bytes) -> bool {
+        if (bytes == 0) bytes = 16;
+        if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
+        if (src && cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return false;
+        return true;
+    };
+    bool ok = alloc_copy(&S->d_nodes, nodes.data(), nodes.size() * sizeof(Bvh4Node)) &&
+              alloc_copy(&S->d_tris, tris.data(), tris.size() * sizeof(float4)) &&
+              alloc_copy(&S->d_inst, inst.data(), inst.size() * sizeof(DeviceInstance)) &&
+              alloc_copy(&S->d_sw, sw, sn * 16) && alloc_copy(&S->d_gw, gw, gn * 16) &&
+              alloc_copy(&S->d_lights, lights, (size_t)light_count * sizeof(LuxLight));
+    if (!ok) {
+        cudaGetLastError();
+        lux_scene_destroy(S);
+        return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "scene upload: device allocation failed");
+    }
+    SceneView &V = S->view;
+    V.nodes = (const Bvh4Node *)S->d_nodes;
+    V.triangles = (const float4 *)S->d_tris;
+    V.instances = (const DeviceInstance *)S->d_inst;
+    V.scene_words = (const uint4 *)S->d_sw;
+    V.geometry_words = (const uint4 *)S->d_gw;
+    V.lights = (const LuxLight *)S->d_lights;
+    V.tlas_root = tlas_root;
+    V.instance_count = inst_count;
+    V.triangle_count = tri_count;
+    V.scene_word_count = (uint32_t)sn;
+    V.geometry_word_count = (uint32_t)gn;
+    V.conventional_lights = conventional;
+    V.emissive_lights = light_count - conventional;
+    for (int k = 0; k < 3; ++k) {
+        V.root_lo[k] = root_lo[k];
+        V.root_hi[k] = root_hi[k];
+    }
+    S->node_count = (uint32_t)nodes.size();
+    *out = S;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_scene_destroy(LuxScene *S) {
+    if (!S) return LUX_OK;
+    cudaFree(S->d_nodes);
+    cudaFree(S->d_tris);
+    cudaFree(S->d_inst);
+    cudaFree(S->d_sw);
+    cudaFree(S->d_gw);
+    cudaFree(S->d_lights);
+    delete S;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_scene_layout(const LuxScene *S, uint32_t *nodes, uint32_t *node_bytes, uint32_t *triangles,
+                                       uint32_t *triangle_bytes, uint32_t *instances) {
+    if (!S) return LUX_ERR_INVALID_ARGUMENT;
+    if (nodes) *nodes = S->node_count;
+    if (node_bytes) *node_bytes = (uint32_t)sizeof(Bvh4Node);
+    if (triangles) *triangles = S->view.triangle_count;
+    if (triangle_bytes) *triangle_bytes = 48u;
+    if (instances) *instances = S->view.instance_count;
+    return LUX_OK;
+}
+
+lux_status lux_launch_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *rays, uint32_t count,
+                                 uint32_t any_hit, LuxHit *hits, unsigned long long *counters) {
+    if (count == 0) return LUX_OK;
+    uint32_t block = 128;
+    uint32_t grid = (count + block - 1) / block;
+    trace_rays_kernel<<<grid, block, 0, ctx->stream>>>(scene->view, rays, count, any_hit, hits, counters);
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "trace_rays_kernel launch");
+}
+
+extern "C" lux_status lux_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *rays, uint32_t count,
+                                     uint32_t any_hit, LuxHit *hits) {
+    if (!ctx || !scene || (count && (!rays || !hits))) return LUX_ERR_INVALID_ARGUMENT;
+    return lux_launch_trace_rays(ctx, scene, rays, count, any_hit, hits, nullptr);
+}

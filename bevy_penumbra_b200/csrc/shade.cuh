@@ -1,0 +1,271 @@
+// shade.cuh - interval radiance at a hit: outgoingTransportRadianceTracked
+// (shaders/cascades.slang:196-268) with emissive next-event estimation
+// (emissiveResponseTracked, shaders/cascades.slang:57-134).
+//
+// Synthetic-material subset, identical to the CPU oracle: untextured opaque
+// materials (materialSample = 1), no environment map and no conventional
+// lights (rejected at upload), no secondary cache.  All source groups are
+// summed into one radiance.  The scattering response is the diffuse colour
+// times disneyDiffuseMultiplier / pi (shaders/common.slang:298-314 and the
+// non-full branch of scatteringResponse, shaders/environment.slang:2-6).
+#pragma once
+#include "traverse.cuh"
+
+namespace lux {
+
+struct ShadeParams {
+    float probe_spacing;
+    float normal_bias;
+    float exposure;
+    uint32_t emissive_samples;
+    uint32_t frame;
+};
+
+__device__ __forceinline__ uint4 sword(const SceneView &S, uint32_t i) {
+    i = i < S.scene_word_count ? i : S.scene_word_count - 1u;
+    return __ldg(S.scene_words + i);
+}
+__device__ __forceinline__ uint4 gword(const SceneView &S, uint32_t i) {
+    i = i < S.geometry_word_count ? i : S.geometry_word_count - 1u;
+    return __ldg(S.geometry_words + i);
+}
+__device__ __forceinline__ f3 f3w(uint4 w) { return f3{as_float(w.x), as_float(w.y), as_float(w.z)}; }
+
+// unitVector, shaders/traversal.slang:183-190.
+__device__ __forceinline__ f3 unit_vector(f3 v, f3 fallback) {
+    float scale = fmaxf(fabsf(v.x), fmaxf(fabsf(v.y), fabsf(v.z)));
+    if (scale == 0.0f || !isfinite(scale)) return fallback;
+    float div = fmaxf(scale * 0.25f, 1.17549435e-38f);
+    f3 w{v.x / div, v.y / div, v.z / div};
+    float l = length(w);
+    return f3{w.x / l, w.y / l, w.z / l};
+}
+
+// transformDirection, shaders/traversal.slang:229-244 (transpose form).
+__device__ __forceinline__ f3 transform_direction_t(const SceneView &S, uint32_t base, f3 value) {
+    f3 a = f3w(sword(S, base)), b = f3w(sword(S, base + 1)), c = f3w(sword(S, base + 2));
+    f3 mag{fmaxf(fabsf(a.x), fmaxf(fabsf(b.x), fabsf(c.x))), fmaxf(fabsf(a.y), fmaxf(fabsf(b.y), fabsf(c.y))),
+           fmaxf(fabsf(a.z), fmaxf(fabsf(b.z), fabsf(c.z)))};
+    float scale = fmaxf(mag.x, fmaxf(mag.y, mag.z));
+    if (scale == 0.0f) return f3{0.0f, 0.0f, 0.0f};
+    scale = fmaxf(scale * 0.25f, 1.17549435e-38f);
+    a = a / scale;
+    b = b / scale;
+    c = c / scale;
+    f3 v = unit_vector(value, f3{0.0f, 0.0f, 0.0f});
+    return f3{(a.x * v.x + b.x * v.y) + c.x * v.z, (a.y * v.x + b.y * v.y) + c.y * v.z,
+              (a.z * v.x + b.z * v.y) + c.z * v.z};
+}
+
+struct Surface {
+    f3 base_color;
+    f3 emission;
+    float metallic, roughness;
+    uint32_t flags;
+};
+
+__device__ __forceinline__ uint32_t instance_base(const SceneView &S, uint32_t inst) {
+    uint4 h = sword(S, 0);
+    return h.y + inst * h.w;
+}
+
+// materialBaseColor / hitEmission (shaders/material.slang:139-141,
+// shaders/traversal.slang:287-300), untextured.
+__device__ __forceinline__ Surface surface_at(const SceneView &S, const ShadeParams &P, uint32_t inst, uint32_t tri,
+                                              float b0, float b1, float b2) {
+    uint32_t base = instance_base(S, inst);
+    uint32_t flags = sword(S, base + 6).w;
+    uint32_t material = sword(S, base + 7).w;
+    uint4 m0 = sword(S, material), m1 = sword(S, material + 1), m2 = sword(S, material + 2);
+    uint4 header = gword(S, 0);
+    uint4 t = gword(S, header.x + tri);
+    uint4 c0 = gword(S, header.y + t.x * header.z + 4);
+    uint4 c1 = gword(S, header.y + t.y * header.z + 4);
+    uint4 c2 = gword(S, header.y + t.z * header.z + 4);
+    f3 color{(as_float(c0.x) * b0 + as_float(c1.x) * b1) + as_float(c2.x) * b2,
+             (as_float(c0.y) * b0 + as_float(c1.y) * b1) + as_float(c2.y) * b2,
+             (as_float(c0.z) * b0 + as_float(c1.z) * b1) + as_float(c2.z) * b2};
+    Surface sf;
+    sf.base_color = f3{as_float(m0.x) * color.x, as_float(m0.y) * color.y, as_float(m0.z) * color.z};
+    sf.emission = (flags & 16u) != 0u ? sf.base_color : f3{as_float(m1.x), as_float(m1.y), as_float(m1.z)};
+    float weight = (flags & 16u) != 0u ? 0.0f : as_float(m2.w);
+    float exposure = fmaxf(P.exposure, 1e-20f);
+    float inv = 1.0f / exposure;
+    float factor = inv + weight * (1.0f - inv);
+    sf.emission = sf.emission * factor;
+    sf.metallic = as_float(m2.x);
+    sf.roughness = as_float(m2.y);
+    sf.flags = flags;
+    return sf;
+}
+
+// disneyDiffuseMultiplier, shaders/common.slang:298-314.
+__device__ __forceinline__ float disney_multiplier(f3 n, f3 l, f3 v, float pr) {
+    float ndl = saturate(dot(n, l));
+    float ndv = saturate(dot(n, v));
+    f3 h = l + v;
+    float hl2 = dot(h, h);
+    if (ndl <= 0.0f || ndv <= 0.0f || hl2 <= 1e-20f) return 0.0f;
+    float hl = sqrtf(hl2);
+    f3 hv{h.x / hl, h.y / hl, h.z / hl};
+    float rough = fmaxf(saturate(pr), 0.089f);
+    rough = rough * rough;
+    float ldh = saturate(dot(l, hv));
+    float f90 = 0.5f + ((2.0f * rough) * ldh) * ldh;
+    float a = 1.0f - ndl, b = 1.0f - ndv;
+    float a2 = a * a, bb = b * b;
+    float ls = 1.0f + (f90 - 1.0f) * ((a2 * a2) * a);
+    float vs = 1.0f + (f90 - 1.0f) * ((bb * bb) * b);
+    return ls * vs;
+}
+
+// emissiveResponseTracked, shaders/cascades.slang:57-134.  Returns false
+// when a visibility query was unsupported.
+__device__ bool emissive_response(const SceneView &S, const ShadeParams &P, f3 position, f3 normal, f3 gnormal, f3 view,
+                                  float roughness, f3 diffuse, f3 &out, uint32_t &shadow_rays, TraceCounters &cn) {
+    out = f3{0.0f, 0.0f, 0.0f};
+    uint32_t emissive = S.emissive_lights;
+    uint32_t count = P.emissive_samples / 2u;
+    count = count < 1u ? 1u : count;
+    if (emissive == 0u) return true;
+    float cell = P.probe_spacing * 0.05f;
+    uint32_t seed = hash_key((int32_t)floorf(position.x / cell), (int32_t)floorf(position.y / cell),
+                             (int32_t)floorf(position.z / cell), 0, 16777216u);
+    float rot_x, rot_y;
+    r2(seed, rot_x, rot_y);
+    float s0 = P.probe_spacing * 1.0f;
+    uint32_t selection_seed = hash_key((int32_t)floorf(position.x / s0), (int32_t)floorf(position.y / s0),
+                                       (int32_t)floorf(position.z / s0), 0, 65536u);
+    uint32_t sample_frame = P.frame ^ 0xE11E0001u;
+    float ax, ay, bx, by;
+    r2(sample_frame, ax, ay);
+    r2(selection_seed, bx, by);
+    float phase = fracf(ax + bx);
+    f3 sum{0.0f, 0.0f, 0.0f};
+    const float bias = P.normal_bias;
+    const LuxLight *lights = S.lights + S.conventional_lights;
+    for (uint32_t sample = 0; sample < count; ++sample) {
+        float rx, ry;
+        r2(sample + sample_frame * count + 1u, rx, ry);
+        float ux = fracf(rx + rot_x), uy = fracf(ry + rot_y);
+        float selection = fracf(((float)sample + 0.5f) / (float)count + phase);
+        uint32_t low = 0, high = emissive - 1u;
+        while (low < high) {
+            uint32_t middle = (low + high) / 2u;
+            if (__ldg(&lights[middle].direction[3]) < selection)
+                low = middle + 1u;
+            else
+                high = middle;
+        }
+        const LuxLight *L = lights + low;
+        f3 lp{__ldg(&L->position[0]), __ldg(&L->position[1]), __ldg(&L->position[2])};
+        float lpw = __ldg(&L->position[3]);
+        f3 ldir{__ldg(&L->direction[0]), __ldg(&L->direction[1]), __ldg(&L->direction[2])};
+        f3 e1{__ldg(&L->edge1[0]), __ldg(&L->edge1[1]), __ldg(&L->edge1[2])};
+        float e1w = __ldg(&L->edge1[3]);
+        f3 e2{__ldg(&L->edge2[0]), __ldg(&L->edge2[1]), __ldg(&L->edge2[2])};
+        float area = __ldg(&L->color[3]);
+        f3 rel = position - lp;
+        if (e1w <= 0.0f || (lpw != -2.0f && dot(ldir, rel) <= 0.0f)) continue;
+        float root = sqrtf(ux);
+        float w1 = root * (1.0f - uy), w2 = root * uy;
+        f3 target{(lp.x + e1.x * w1) + e2.x * w2, (lp.y + e1.y * w1) + e2.y * w2, (lp.z + e1.z * w1) + e2.z * w2};
+        f3 to_light = target - position;
+        float light_distance = length(to_light);
+        if (light_distance <= bias * 0.25f) continue;
+        f3 ld = to_light / light_distance;
+        float cosine = fmaxf(0.0f, dot(normal, ld));
+        float c_emit = dot(ldir, -ld);
+        if (lpw == -2.0f) c_emit = fabsf(c_emit);
+        float emitter_cosine = fmaxf(0.0f, c_emit);
+        if (cosine <= 0.0f || emitter_cosine <= 0.0f || dot(gnormal, ld) <= 0.0f) continue;
+        Surface es = surface_at(S, P, __ldg(&L->source[0]), __ldg(&L->source[1]), 1.0f - root, w1, w2);
+        f3 emission{fmaxf(es.emission.x, 0.0f), fmaxf(es.emission.y, 0.0f), fmaxf(es.emission.z, 0.0f)};
+        if (!(emission.x > 0.0f || emission.y > 0.0f || emission.z > 0.0f)) continue;
+        float pdf = ((e1w * light_distance) * light_distance) / (area * emitter_cosine);
+        float plane = fabsf(dot(ldir, rel));
+        f3 origin = ray_offset(position, gnormal, fminf(bias, plane * 0.25f));
+        f3 delta = target - origin;
+        float distance = length(delta);
+        if (distance <= bias * 0.25f) continue;
+        f3 dir = delta / distance;
+        Hit sh;
+        ++shadow_rays;
+        trace<true>(S, origin, dir, 0.0f, distance - fminf(bias * 0.25f, distance * 0.001f), sh, cn);
+        if ((sh.errors & kQueryUnsupported) != 0u && sh.tri == kEmpty) {
+            out = f3{0.0f, 0.0f, 0.0f};
+            return false;
+        }
+        if (sh.tri != kEmpty) continue;
+        float factor = disney_multiplier(normal, ld, view, roughness) / kPi;
+        float p = fmaxf(pdf, 1e-20f);
+        sum.x = sum.x + emission.x * (((diffuse.x * factor) * cosine) / p);
+        sum.y = sum.y + emission.y * (((diffuse.y * factor) * cosine) / p);
+        sum.z = sum.z + emission.z * (((diffuse.z * factor) * cosine) / p);
+    }
+    out = f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
+    return true;
+}
+
+// outgoingTransportRadianceTracked, shaders/cascades.slang:196-268.  Returns
+// false when the query is unsupported (no deposit).
+__device__ bool outgoing_radiance(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
+                                  f3 &out, uint32_t &shadow_rays, TraceCounters &cn) {
+    out = f3{0.0f, 0.0f, 0.0f};
+    if ((hit.errors & kQueryUnsupported) != 0u) return false;
+    if (hit.tri == kEmpty) return true;
+    float b0 = (1.0f - hit.b1) - hit.b2;
+    Surface sf = surface_at(S, P, hit.inst, hit.tri, b0, hit.b1, hit.b2);
+    f3 radiance = sf.emission;
+    if ((sf.flags & 16u) == 0u) {
+        uint32_t base = instance_base(S, hit.inst);
+        uint4 header = gword(S, 0);
+        uint4 t = gword(S, header.x + hit.tri);
+        uint32_t idx[3] = {t.x, t.y, t.z};
+        f3 A = f3w(gword(S, header.y + idx[0] * header.z));
+        f3 B = f3w(gword(S, header.y + idx[1] * header.z));
+        f3 C = f3w(gword(S, header.y + idx[2] * header.z));
+        f3 position{origin.x + direction.x * hit.t, origin.y + direction.y * hit.t, origin.z + direction.z * hit.t};
+        f3 gn = unit_vector(transform_direction_t(S, base, cross(B - A, C - A)), f3{0.0f, 1.0f, 0.0f});
+        float sign = (sf.flags & 4u) != 0u ? -1.0f : 1.0f;
+        gn = gn * sign;
+        // hitAttributes world normal, shaders/traversal.slang:258-282.
+        float bary[3] = {b0, hit.b1, hit.b2};
+        f3 world_normal{0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            uint32_t vb = header.y + idx[i] * header.z;
+            f3 nrm = gn;
+            if ((gword(S, vb).w & 1u) != 0u) nrm = unit_vector(transform_direction_t(S, base, f3w(gword(S, vb + 1))), gn);
+            world_normal = f3{world_normal.x + nrm.x * bary[i], world_normal.y + nrm.y * bary[i],
+                              world_normal.z + nrm.z * bary[i]};
+        }
+        // materialNormal without a normal texture, shaders/material.slang:171-177.
+        f3 normal = unit_vector(world_normal, gn);
+        bool back = dot(gn, direction) > 0.0f;
+        if (back && (sf.flags & 8u) != 0u) normal = -normal;
+        f3 flipped = dot(gn, direction) > 0.0f ? -gn : gn;
+        f3 neg = -direction;
+        if (!(dot(normal, neg) <= 0.0f || dot(normal, flipped) <= 0.0f)) {
+            float nl = length(neg);
+            f3 view = neg / nl;
+            float metallic = saturate(sf.metallic);
+            float roughness = saturate(sf.roughness);
+            if (!isfinite(roughness)) roughness = 1.0f;
+            bool bf = finite3(sf.base_color);
+            f3 diffuse{(bf ? saturate(sf.base_color.x) : 0.0f) * (1.0f - metallic),
+                       (bf ? saturate(sf.base_color.y) : 0.0f) * (1.0f - metallic),
+                       (bf ? saturate(sf.base_color.z) : 0.0f) * (1.0f - metallic)};
+            f3 nee;
+            if (!emissive_response(S, P, position, normal, flipped, view, roughness, diffuse, nee, shadow_rays, cn))
+                return false;
+            radiance = radiance + nee;
+        }
+    }
+    // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188.
+    if (!finite3(radiance)) return true;
+    out = f3{fmaxf(radiance.x, 0.0f), fmaxf(radiance.y, 0.0f), fmaxf(radiance.z, 0.0f)};
+    return true;
+}
+
+}  // namespace lux

@@ -1,0 +1,413 @@
+// traverse.cuh - closest-hit and any-hit traversal of the two-level BVH4.
+//
+// Restates traceRayTracked / traceInstance / traceTriangle /
+// intersectTriangle (shaders/traversal.slang:349-811) and traceOccluded /
+// occludedInstance / occludedTriangle (shaders/traversal.slang:826-1046) on
+// a 4-wide BVH whose child boxes are the reference's binary node boxes.
+// Hit distances, triangles and instances are produced by the same watertight
+// triangle test as the reference; equal distances resolve to the smaller
+// (instance, triangle), which makes the answer independent of tree shape.
+#pragma once
+#include "lux_internal.h"
+#include "lux_math.cuh"
+
+namespace lux {
+
+constexpr uint32_t kMaxSteps = 4096u;  // MAX_TRAVERSAL_STEPS, shaders/traversal.slang:8
+constexpr int kStack = 64;
+
+struct Hit {
+    float t;
+    uint32_t tri, inst, errors;
+    float b1, b2;
+};
+
+struct TraceCounters {
+    uint32_t nodes, triangles, instances;
+};
+
+// boxRayInterval, shaders/traversal.slang:349-369, for one box.
+__device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, float lz, float hx, float hy,
+                                             float hz, float limit, float &entry, float &exit) {
+    float near_t = 0.0f, far_t = limit;
+    float lo[3] = {lx, ly, lz}, hi[3] = {hx, hy, hz};
+    float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (dd[a] == 0.0f) {
+            if (oo[a] < lo[a] || oo[a] > hi[a]) {
+                entry = 0.0f;
+                exit = 0.0f;
+                return false;
+            }
+        } else {
+            float ta = (lo[a] - oo[a]) / dd[a];
+            float tb = (hi[a] - oo[a]) / dd[a];
+            float ax = fmaxf(ta, tb);
+            near_t = fmaxf(near_t, fminf(ta, tb));
+            far_t = fminf(far_t, ax + fabsf(ax) * 3.5762791e-7f);
+        }
+    }
+    entry = near_t;
+    exit = far_t;
+    return near_t <= far_t;
+}
+
+// Child tests of one BVH4 node.  Returns the hit mask; entry[i] as in
+// boxEntryDistance.  Children whose padded exit precedes tmin cannot hold a
+// hit with t > tmin and are skipped.
+__device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes, uint32_t index, f3 o, f3 d,
+                                              float limit, float tmin, float entry[4], uint32_t child[4]) {
+    const float4 *p = reinterpret_cast<const float4 *>(nodes + index);
+    float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
+           hz = __ldg(p + 5);
+    uint4 ch = __ldg(reinterpret_cast<const uint4 *>(p + 6));
+    child[0] = ch.x;
+    child[1] = ch.y;
+    child[2] = ch.z;
+    child[3] = ch.w;
+    float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
+    float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
+    float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+    uint32_t mask = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        float e, x;
+        bool h = child[i] != kEmpty && box_interval(o, d, LX[i], LY[i], LZ[i], HX[i], HY[i], HZ[i], limit, e, x);
+        if (h && x >= tmin) {
+            mask |= 1u << i;
+            entry[i] = e;
+        } else {
+            entry[i] = 0.0f;
+        }
+    }
+    return mask;
+}
+
+struct TriRay {
+    uint32_t kx, ky, kz;
+    float sx, sy;
+    bool valid;
+};
+
+// triangleRay, shaders/traversal.slang:399-413.
+__device__ __forceinline__ TriRay triangle_ray(f3 d) {
+    TriRay r{0, 0, 0, 0.0f, 0.0f, false};
+    float mx = fabsf(d.x), my = fabsf(d.y), mz = fabsf(d.z);
+    r.kz = mx > my ? (mx > mz ? 0u : 2u) : (my > mz ? 1u : 2u);
+    float dz = comp(d, r.kz);
+    r.valid = dz != 0.0f;
+    if (!r.valid) return r;
+    r.kx = (r.kz + 1u) % 3u;
+    r.ky = (r.kx + 1u) % 3u;
+    if (dz < 0.0f) {
+        uint32_t t = r.kx;
+        r.kx = r.ky;
+        r.ky = t;
+    }
+    r.sx = comp(d, r.kx) / dz;
+    r.sy = comp(d, r.ky) / dz;
+    return r;
+}
+
+// orientedEdge, shaders/traversal.slang:379-392.
+__device__ __forceinline__ float oriented_edge(float ax, float ay, float bx, float by) {
+    bool reverse = ax > bx || (ax == bx && ay > by);
+    float fx = reverse ? bx : ax, fy = reverse ? by : ay;
+    float sx = reverse ? ax : bx, sy = reverse ? ay : by;
+    float pa = fx * sy;
+    float pb = fy * sx;
+    float edge = pa - pb;
+    float error = (fabsf(pa) + fabsf(pb)) * 2.3841858e-7f;
+    if (fabsf(edge) <= error) edge = 0.0f;
+    return reverse ? -edge : edge;
+}
+
+// intersectTriangle, shaders/traversal.slang:415-443.  Returns distance or -1.
+__device__ __forceinline__ float intersect_triangle(f3 o, f3 d, const TriRay &ray, f3 A, f3 B, f3 C, float &w1,
+                                                    float &w2) {
+    if (!ray.valid) return -1.0f;
+    f3 a = A - o, b = B - o, c = C - o;
+    float akz = comp(a, ray.kz), bkz = comp(b, ray.kz), ckz = comp(c, ray.kz);
+    float pax = comp(a, ray.kx) - ray.sx * akz, pay = comp(a, ray.ky) - ray.sy * akz;
+    float pbx = comp(b, ray.kx) - ray.sx * bkz, pby = comp(b, ray.ky) - ray.sy * bkz;
+    float pcx = comp(c, ray.kx) - ray.sx * ckz, pcy = comp(c, ray.ky) - ray.sy * ckz;
+    float largest = fmaxf(fmaxf(fmaxf(fabsf(pax), fabsf(pay)), fmaxf(fabsf(pbx), fabsf(pby))),
+                          fmaxf(fabsf(pcx), fabsf(pcy)));
+    if (largest == 0.0f || !isfinite(largest)) return -1.0f;
+    uint32_t exponent = (as_uint(largest) >> 23) & 255u;
+    exponent = exponent < 1u ? 1u : (exponent > 253u ? 253u : exponent);
+    float scale = as_float((254u - exponent) << 23);
+    pax *= scale;
+    pay *= scale;
+    pbx *= scale;
+    pby *= scale;
+    pcx *= scale;
+    pcy *= scale;
+    float e0 = oriented_edge(pbx, pby, pcx, pcy);
+    float e1 = oriented_edge(pcx, pcy, pax, pay);
+    float e2 = oriented_edge(pax, pay, pbx, pby);
+    bool any_neg = e0 < 0.0f || e1 < 0.0f || e2 < 0.0f;
+    bool any_pos = e0 > 0.0f || e1 > 0.0f || e2 > 0.0f;
+    if (any_neg && any_pos) return -1.0f;
+    float det = (e0 + e1) + e2;
+    if (det == 0.0f || !isfinite(det)) return -1.0f;
+    float wx = e0 / det, wy = e1 / det, wz = e2 / det;
+    float dist = ((wx * akz + wy * bkz) + wz * ckz) / comp(d, ray.kz);
+    if (!isfinite(dist)) return -1.0f;
+    w1 = wy;
+    w2 = wz;
+    return dist;
+}
+
+__device__ __forceinline__ bool hit_better(float t, uint32_t inst, uint32_t tri, const Hit &h) {
+    if (t < h.t) return true;
+    if (t > h.t || h.tri == kEmpty) return false;
+    if (inst != h.inst) return inst < h.inst;
+    return tri < h.tri;
+}
+
+// Face culling of traceTriangle / occludedTriangle (shaders/traversal.slang:449-453).
+__device__ __forceinline__ bool cull_reject(uint32_t flags, f3 A, f3 B, f3 C, f3 d) {
+    if ((flags & 3u) == 0u) return false;
+    float facing = dot(cross(B - A, C - A), d) * ((flags & 4u) != 0u ? -1.0f : 1.0f);
+    return ((flags & 1u) != 0u && facing >= 0.0f) || ((flags & 2u) != 0u && facing <= 0.0f);
+}
+
+__device__ __forceinline__ void load_triangle(const float4 *__restrict__ tris, uint32_t t, f3 &A, f3 &B, f3 &C) {
+    float4 a = __ldg(tris + 3 * (size_t)t), b = __ldg(tris + 3 * (size_t)t + 1), c = __ldg(tris + 3 * (size_t)t + 2);
+    A = f3{a.x, a.y, a.z};
+    B = f3{b.x, b.y, b.z};
+    C = f3{c.x, c.y, c.z};
+}
+
+// Local ray, shaders/traversal.slang:481-488.
+__device__ __forceinline__ void local_ray(const DeviceInstance &I, f3 o, f3 d, f3 &lo, f3 &ld) {
+    float r[3][4];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) r[k][c] = I.row[k][c];
+    lo = f3{((r[0][0] * o.x + r[0][1] * o.y) + r[0][2] * o.z) + r[0][3] * 1.0f,
+            ((r[1][0] * o.x + r[1][1] * o.y) + r[1][2] * o.z) + r[1][3] * 1.0f,
+            ((r[2][0] * o.x + r[2][1] * o.y) + r[2][2] * o.z) + r[2][3] * 1.0f};
+    ld = f3{((r[0][0] * d.x + r[0][1] * d.y) + r[0][2] * d.z) + r[0][3] * 0.0f,
+            ((r[1][0] * d.x + r[1][1] * d.y) + r[1][2] * d.z) + r[1][3] * 0.0f,
+            ((r[2][0] * d.x + r[2][1] * d.y) + r[2][2] * d.z) + r[2][3] * 0.0f};
+}
+
+__device__ __forceinline__ DeviceInstance load_instance(const DeviceInstance *__restrict__ inst, uint32_t i) {
+    const float4 *p = reinterpret_cast<const float4 *>(inst + i);
+    float4 r0 = __ldg(p), r1 = __ldg(p + 1), r2 = __ldg(p + 2);
+    uint4 w = __ldg(reinterpret_cast<const uint4 *>(p + 3));
+    DeviceInstance I;
+    I.row[0][0] = r0.x; I.row[0][1] = r0.y; I.row[0][2] = r0.z; I.row[0][3] = r0.w;
+    I.row[1][0] = r1.x; I.row[1][1] = r1.y; I.row[1][2] = r1.z; I.row[1][3] = r1.w;
+    I.row[2][0] = r2.x; I.row[2][1] = r2.y; I.row[2][2] = r2.z; I.row[2][3] = r2.w;
+    I.root = w.x;
+    I.first = w.y;
+    I.count = w.z;
+    I.flags = w.w;
+    return I;
+}
+
+// Sort up to four (entry, payload) pairs by entry, ascending.
+__device__ __forceinline__ void sort4(float e[4], uint32_t p[4], int n) {
+#define LUX_CSWAP(i, j)                                          \
+    if (n > (j) && e[j] < e[i]) {                                \
+        float te = e[i]; e[i] = e[j]; e[j] = te;                 \
+        uint32_t tp = p[i]; p[i] = p[j]; p[j] = tp;              \
+    }
+    LUX_CSWAP(0, 1);
+    LUX_CSWAP(2, 3);
+    LUX_CSWAP(0, 2);
+    LUX_CSWAP(1, 3);
+    LUX_CSWAP(1, 2);
+#undef LUX_CSWAP
+}
+
+// BLAS walk of one instance (traceInstance / occludedInstance).  Returns true
+// for an any-hit query that found a blocker.
+template <bool kAnyHit>
+__device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, float tmin, Hit &hit,
+                               TraceCounters &cn) {
+    DeviceInstance I = load_instance(S.instances, inst);
+    f3 lo, ld;
+    local_ray(I, o, d, lo, ld);
+    cn.instances++;
+    TriRay ray = triangle_ray(ld);
+    uint32_t stack_p[kStack];
+    float stack_t[kStack];
+    int sp = 0;
+    uint32_t cur = I.root;
+    bool ready = true;
+    uint32_t steps = 0;
+    const float lower = fmaxf(tmin, 0.000025f);
+    while (true) {
+        if (!ready) {
+            while (sp > 0) {
+                --sp;
+                if (!kAnyHit && stack_t[sp] > hit.t) continue;
+                cur = stack_p[sp];
+                ready = true;
+                break;
+            }
+            if (!ready) break;
+        }
+        ready = false;
+        if (++steps > kMaxSteps) {
+            hit.errors |= kQueryUnsupported;
+            return false;
+        }
+        uint32_t first, count;
+        if (cur & kLeafBit) {
+            first = cur & kLeafFirstMask;
+            count = ((cur >> 27) & 15u) + 1u;
+        } else {
+            float entry[4];
+            uint32_t child[4];
+            cn.nodes++;
+            uint32_t mask = node_test(S.nodes, cur, lo, ld, kAnyHit ? hit.t : hit.t, tmin, entry, child);
+            if (mask == 0u) continue;
+            float e[4];
+            uint32_t p[4];
+            int n = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (mask & (1u << i)) {
+                    e[n] = entry[i];
+                    p[n] = child[i];
+                    ++n;
+                }
+            sort4(e, p, n);
+            if (sp + n - 1 > kStack) {
+                // Stack exhausted: scan the instance's whole range and flag it
+                // (traceInstance fallback, shaders/traversal.slang:512-517).
+                hit.errors |= 1u;
+                sp = 0;
+                first = I.first;
+                count = I.count;
+                goto scan;
+            }
+            for (int k = n - 1; k >= 1; --k) {
+                stack_p[sp] = p[k];
+                stack_t[sp] = e[k];
+                ++sp;
+            }
+            cur = p[0];
+            ready = true;
+            continue;
+        }
+    scan:
+        for (uint32_t t = first; t < first + count; ++t) {
+            f3 A, B, C;
+            load_triangle(S.triangles, t, A, B, C);
+            cn.triangles++;
+            if (cull_reject(I.flags, A, B, C, ld)) continue;
+            float w1 = 0.0f, w2 = 0.0f;
+            float dist = intersect_triangle(lo, ld, ray, A, B, C, w1, w2);
+            if (kAnyHit) {
+                if (dist > 0.000025f && dist < hit.t) {
+                    hit.tri = t;
+                    hit.inst = inst;
+                    return true;
+                }
+            } else if (dist > lower && hit_better(dist, inst, t, hit)) {
+                hit.t = dist;
+                hit.tri = t;
+                hit.inst = inst;
+                hit.b1 = w1;
+                hit.b2 = w2;
+            }
+        }
+    }
+    return false;
+}
+
+// traceRayTracked (kAnyHit = false) / traceOccluded (kAnyHit = true).
+template <bool kAnyHit>
+__device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, Hit &hit, TraceCounters &cn) {
+    hit.t = limit;
+    hit.tri = kEmpty;
+    hit.inst = kEmpty;
+    hit.errors = 0;
+    hit.b1 = 0.0f;
+    hit.b2 = 0.0f;
+    if (S.instance_count == 0) return;
+    float re, rx;
+    if (!box_interval(o, d, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1], S.root_hi[2],
+                      limit, re, rx))
+        return;
+    uint32_t stack_p[kStack];
+    float stack_t[kStack];
+    int sp = 0;
+    uint32_t cur = S.tlas_root;
+    bool ready = true;
+    uint32_t steps = 0;
+    while (true) {
+        if (!ready) {
+            while (sp > 0) {
+                --sp;
+                if (!kAnyHit && stack_t[sp] > hit.t) continue;
+                cur = stack_p[sp];
+                ready = true;
+                break;
+            }
+            if (!ready) break;
+        }
+        ready = false;
+        if (++steps > kMaxSteps) {
+            hit.errors |= kQueryUnsupported;
+            break;
+        }
+        uint32_t first, count;
+        if (cur & kLeafBit) {
+            first = cur & kLeafFirstMask;
+            count = ((cur >> 27) & 15u) + 1u;
+        } else {
+            float entry[4];
+            uint32_t child[4];
+            cn.nodes++;
+            uint32_t mask = node_test(S.nodes, cur, o, d, hit.t, tmin, entry, child);
+            if (mask == 0u) continue;
+            float e[4];
+            uint32_t p[4];
+            int n = 0;
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                if (mask & (1u << i)) {
+                    e[n] = entry[i];
+                    p[n] = child[i];
+                    ++n;
+                }
+            sort4(e, p, n);
+            if (sp + n - 1 > kStack) {
+                // traceRayTracked fallback, shaders/traversal.slang:742-745.
+                hit.errors |= 2u;
+                sp = 0;
+                first = 0;
+                count = S.instance_count;
+                goto scan;
+            }
+            for (int k = n - 1; k >= 1; --k) {
+                stack_p[sp] = p[k];
+                stack_t[sp] = e[k];
+                ++sp;
+            }
+            cur = p[0];
+            ready = true;
+            continue;
+        }
+    scan:
+        for (uint32_t i = first; i < first + count; ++i) {
+            if (trace_instance<kAnyHit>(S, o, d, i, tmin, hit, cn)) {
+                // Any accepted blocker is a complete proof
+                // (shaders/traversal.slang:786-792, :1035-1040).
+                hit.errors &= ~kQueryUnsupported;
+                return;
+            }
+        }
+    }
+}
+
+}  // namespace lux

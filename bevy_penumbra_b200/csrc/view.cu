@@ -1,0 +1,891 @@
+// view.cu - one cascade frame of a view: the Split dispatch sequence of
+// render() (src/render.rs:9553-9801) as CUDA kernels.
+//
+//   seed      world cells of every level that hold a receiver, in per-level
+//             open-addressing directories (seed/rank/insertProbeDescriptor,
+//             shaders/split.slang:292-319, :734-893) with dense cell ids
+//   trace     closest hit + hit shading + deposit in one kernel
+//             (traceTransport/finishTransportVariant/deposit,
+//             shaders/split.slang:1056-1216); the per-key mean of reduce
+//             (shaders/split.slang:1386-1476) is a sum + count per record
+//   merge     levels L-1..0 (mergeEntry, shaders/split.slang:1624-1725)
+//   pack      cascade-0 cells to 6x6 octahedral tables (packProbes,
+//             shaders/split.slang:1786-1918)
+//   resolve   worldResolve (shaders/world_resolve.slang:281-313)
+//
+// Records live in dense per-level arrays indexed [cell][direction] instead of
+// the reference's hashed bucket chains; keys (cell, direction, level) are the
+// reference's world-grid keys (cacheKey, shaders/common.slang:417-422).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lux_internal.h"
+#include "lux_math.cuh"
+#include "shade.cuh"
+#include "traverse.cuh"
+
+namespace {
+
+using lux::f3;
+
+struct FrameParams {
+    uint32_t levels, layout, rays_per_receiver, receivers;
+    uint32_t dir_capacity, cell_capacity;
+    unsigned long long entry_capacity;
+    float spacing[LUX_MAX_LEVELS];
+    float start[LUX_MAX_LEVELS];
+    float end[LUX_MAX_LEVELS];
+    uint32_t columns[LUX_MAX_LEVELS];
+    uint32_t rows[LUX_MAX_LEVELS];
+    uint32_t dirs[LUX_MAX_LEVELS];
+    lux::ShadeParams shade;
+};
+
+// Device state of a view (ViewBuffers, src/render.rs:5077-5160).
+struct ViewDevice {
+    unsigned long long *dir_keys;   // [levels][dir_capacity]
+    uint32_t *dir_ids;              // [levels][dir_capacity]
+    int4 *cell_keys;                // [levels][cell_capacity]
+    uint32_t *cell_count;           // [levels]
+    unsigned long long *level_base; // [levels]
+    uint32_t *receiver_cell;        // [levels][max_receivers]
+    uint32_t *corner_ids;           // [levels][cell_capacity][8] (level+1 ids)
+    float4 *corner_frac;            // [levels][cell_capacity]
+    float4 *accum;                  // [entries] J sum rgb, non-terminating count
+    uint32_t *count;                // [entries]
+    float4 *merged;                 // [entries] I rgb, support
+    float4 *raw;                    // [entries] J mean rgb, beta
+    float4 *tables;                 // [cell_capacity][36]
+    uint32_t *error_flags;
+    unsigned long long *stats;      // 8 counters
+};
+
+constexpr int kStatInterval = 0, kStatShadow = 1, kStatNodes = 2, kStatTris = 3, kStatInst = 4, kStatDeposits = 5,
+              kStatUnsupported = 6;
+
+__device__ __forceinline__ void add_stats(unsigned long long *stats, unsigned long long v[7]) {
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            if (v[k]) atomicAdd(&stats[k], v[k]);
+    }
+}
+
+__device__ __forceinline__ void cell_of(const FrameParams &F, uint32_t level, f3 p, int32_t &x, int32_t &y,
+                                        int32_t &z) {
+    float s = F.spacing[level];
+    x = (int32_t)floorf(p.x / s);
+    y = (int32_t)floorf(p.y / s);
+    z = (int32_t)floorf(p.z / s);
+}
+
+// Probe of a level directory; returns the slot or kEmpty.
+__device__ __forceinline__ uint32_t dir_find(const ViewDevice &V, const FrameParams &F, uint32_t level, int32_t x,
+                                             int32_t y, int32_t z) {
+    if (!lux::cell_in_range(x, y, z)) return lux::kEmpty;
+    unsigned long long key = lux::pack_cell(x, y, z);
+    const unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
+    uint32_t slot = lux::hash_key(x, y, z, (int32_t)level, F.dir_capacity);
+    for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+        unsigned long long k = keys[slot];
+        if (k == key) return slot;
+        if (k == lux::kEmptyCell) return lux::kEmpty;
+        slot = (slot + 1u) & (F.dir_capacity - 1u);
+    }
+    return lux::kEmpty;
+}
+
+__device__ __forceinline__ uint32_t cell_id(const ViewDevice &V, const FrameParams &F, uint32_t level, int32_t x,
+                                            int32_t y, int32_t z) {
+    uint32_t slot = dir_find(V, F, level, x, y, z);
+    return slot == lux::kEmpty ? lux::kEmpty : V.dir_ids[(size_t)level * F.dir_capacity + slot];
+}
+
+__global__ void clear_kernel(ViewDevice V, FrameParams F) {
+    size_t n = (size_t)F.levels * F.dir_capacity;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        V.dir_keys[i] = lux::kEmptyCell;
+        V.dir_ids[i] = lux::kEmpty;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < LUX_MAX_LEVELS) {
+        V.cell_count[threadIdx.x] = 0;
+        V.level_base[threadIdx.x] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 8) V.stats[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *V.error_flags = 0;
+}
+
+// seed: insert every receiver's cell of every level (insertProbeDescriptor,
+// shaders/split.slang:292-319, with a 64-bit key compare-and-swap).
+__global__ void seed_insert_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
+    size_t n = (size_t)F.receivers * F.levels;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
+        float4 p = pos[r];
+        int32_t x, y, z;
+        cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
+        if (!lux::cell_in_range(x, y, z)) {
+            atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+            continue;
+        }
+        unsigned long long key = lux::pack_cell(x, y, z);
+        unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
+        uint32_t slot = lux::hash_key(x, y, z, (int32_t)level, F.dir_capacity);
+        bool placed = false;
+        for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+            unsigned long long prev = atomicCAS(&keys[slot], lux::kEmptyCell, key);
+            if (prev == lux::kEmptyCell || prev == key) {
+                placed = true;
+                break;
+            }
+            slot = (slot + 1u) & (F.dir_capacity - 1u);
+        }
+        if (!placed) atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+    }
+}
+
+// rank: dense ids for occupied directory slots.
+__global__ void seed_assign_kernel(ViewDevice V, FrameParams F) {
+    size_t n = (size_t)F.levels * F.dir_capacity;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        unsigned long long key = V.dir_keys[i];
+        if (key == lux::kEmptyCell) continue;
+        uint32_t level = (uint32_t)(i / F.dir_capacity);
+        uint32_t id = atomicAdd(&V.cell_count[level], 1u);
+        if (id >= F.cell_capacity) {
+            atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+            V.dir_ids[i] = lux::kEmpty;
+            continue;
+        }
+        V.dir_ids[i] = id;
+        int32_t x = (int32_t)(key & 0x1fffffull) - (1 << 20);
+        int32_t y = (int32_t)((key >> 21) & 0x1fffffull) - (1 << 20);
+        int32_t z = (int32_t)((key >> 42) & 0x1fffffull) - (1 << 20);
+        V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)(level << 12));
+    }
+}
+
+__global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
+    size_t n = (size_t)F.receivers * F.levels;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
+        float4 p = pos[r];
+        int32_t x, y, z;
+        cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
+        V.receiver_cell[(size_t)level * F.receivers + r] = cell_id(V, F, level, x, y, z);
+    }
+}
+
+// Per-level record offsets; the entry capacity bounds the whole frame.
+__global__ void layout_kernel(ViewDevice V, FrameParams F) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long base = 0;
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        uint32_t cells = min(V.cell_count[l], F.cell_capacity);
+        V.cell_count[l] = cells;
+        V.level_base[l] = base;
+        base += (unsigned long long)cells * F.dirs[l];
+    }
+    if (base > F.entry_capacity) atomicOr(V.error_flags, LUX_VIEW_ERR_ENTRY_CAPACITY);
+}
+
+__device__ __forceinline__ unsigned long long total_entries(const ViewDevice &V, const FrameParams &F) {
+    unsigned long long base = 0;
+    for (uint32_t l = 0; l < F.levels; ++l) base += (unsigned long long)V.cell_count[l] * F.dirs[l];
+    return base;
+}
+
+__global__ void clear_entries_kernel(ViewDevice V, FrameParams F) {
+    if (*V.error_flags) return;
+    unsigned long long n = total_entries(V, F);
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        V.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        V.count[i] = 0u;
+    }
+}
+
+// Split layout: one thread per (receiver, ray).  traceTransport +
+// finishTransportVariant + deposit (shaders/split.slang:1056-1216).
+__global__ void __launch_bounds__(128) trace_split_kernel(ViewDevice V, FrameParams F, SceneView S,
+                                                          const float4 *__restrict__ pos,
+                                                          const float4 *__restrict__ nrm, uint32_t ray_count) {
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    bool ok = *V.error_flags == 0u;
+    uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ok && ray < ray_count) {
+        uint32_t R = F.rays_per_receiver;
+        uint32_t i = ray / R, k = ray % R;
+        float4 p4 = pos[i], n4 = nrm[i];
+        f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+        float jx, jy, rx, ry;
+        lux::r2(lux::transport_hash(F.shade.frame ^ 0x5a17c9e3u), jx, jy);
+        lux::r2(i * R + k + 1u, rx, ry);
+        float u = lux::fracf((0.5f + rx) + jx);
+        float v = lux::fracf((0.5f + ry) + jy);
+        f3 dir = lux::decode_direction(u, v);
+        if (lux::dot(dir, n) < 0.0f) {
+            dir = -dir;
+            u = lux::fracf(u + 0.5f);
+            v = 1.0f - v;
+        }
+        f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
+        lux::TraceCounters cn{0, 0, 0};
+        lux::Hit hit;
+        lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
+        f3 radiance;
+        uint32_t shadow = 0;
+        bool supported = lux::outgoing_radiance(S, F.shade, origin, dir, hit, radiance, shadow, cn);
+        st[kStatInterval] = 1;
+        st[kStatShadow] = shadow;
+        st[kStatNodes] = cn.nodes;
+        st[kStatTris] = cn.triangles;
+        st[kStatInst] = cn.instances;
+        if (!supported) {
+            st[kStatUnsupported] = 1;
+        } else {
+            uint32_t term = F.levels - 1u;
+            for (uint32_t l = 0; l + 1u < F.levels; ++l)
+                if (hit.t > F.start[l] && hit.t <= F.end[l]) {
+                    term = l;
+                    break;
+                }
+            for (uint32_t l = 0; l <= term; ++l) {
+                uint32_t cell = V.receiver_cell[(size_t)l * F.receivers + i];
+                if (cell == lux::kEmpty) continue;
+                uint32_t bin = lux::direction_index_uv(u, v, F.columns[l], F.rows[l]);
+                unsigned long long e = V.level_base[l] + (unsigned long long)cell * F.dirs[l] + bin;
+                atomicAdd(&V.count[e], 1u);
+                if (l == term) {
+                    atomicAdd(&V.accum[e].x, radiance.x);
+                    atomicAdd(&V.accum[e].y, radiance.y);
+                    atomicAdd(&V.accum[e].z, radiance.z);
+                } else {
+                    atomicAdd(&V.accum[e].w, 1.0f);
+                }
+                st[kStatDeposits] += 1;
+            }
+        }
+    }
+    add_stats(V.stats, st);
+}
+
+// Dense layout: one thread per (cell, direction) record of one level; the
+// ray starts at the cell centre and covers the level's interval (the dense
+// reference of src/transport_tests.rs:179-248 with BVH geometry).
+__global__ void __launch_bounds__(128) trace_dense_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t level) {
+    if (*V.error_flags) return;
+    unsigned long long n = (unsigned long long)V.cell_count[level] * F.dirs[level];
+    unsigned long long base = V.level_base[level];
+    const bool terminal = level + 1u == F.levels;
+    const float tmin = F.start[level];
+    const float limit = terminal ? 1e20f : nextafterf(F.end[level], INFINITY);
+    const float sp = F.spacing[level];
+    const uint32_t dirs = F.dirs[level];
+    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+         e < ((n + 31ull) & ~31ull); e += (unsigned long long)gridDim.x * blockDim.x) {
+        unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (e < n) {
+            uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
+            int4 key = V.cell_keys[(size_t)level * F.cell_capacity + cell];
+            f3 origin{((float)key.x + 0.5f) * sp, ((float)key.y + 0.5f) * sp, ((float)key.z + 0.5f) * sp};
+            f3 dir = lux::bin_direction(d, F.columns[level], F.rows[level]);
+            lux::TraceCounters cn{0, 0, 0};
+            lux::Hit hit;
+            lux::trace<false>(S, origin, dir, tmin, limit, hit, cn);
+            f3 radiance;
+            uint32_t shadow = 0;
+            bool supported = lux::outgoing_radiance(S, F.shade, origin, dir, hit, radiance, shadow, cn);
+            st[kStatInterval] = 1;
+            st[kStatShadow] = shadow;
+            st[kStatNodes] = cn.nodes;
+            st[kStatTris] = cn.triangles;
+            st[kStatInst] = cn.instances;
+            if (supported) {
+                bool terminates = terminal || hit.tri != lux::kEmpty;
+                V.count[base + e] = 1u;
+                V.accum[base + e] = terminates ? make_float4(radiance.x, radiance.y, radiance.z, 0.0f)
+                                               : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+                st[kStatDeposits] = 1;
+            } else {
+                st[kStatUnsupported] = 1;
+            }
+        }
+        add_stats(V.stats, st);
+    }
+}
+
+// Spatial corners of every cell of `level` in level + 1 (mergeRadianceGroups
+// grid, shaders/split.slang:1590-1596).
+__global__ void corners_kernel(ViewDevice V, FrameParams F, uint32_t level) {
+    if (*V.error_flags) return;
+    uint32_t cells = V.cell_count[level];
+    float sp = F.spacing[level], sp1 = F.spacing[level + 1];
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+        int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+        float ox = ((float)key.x + 0.5f) * sp, oy = ((float)key.y + 0.5f) * sp, oz = ((float)key.z + 0.5f) * sp;
+        float gx = ox / sp1 - 0.5f, gy = oy / sp1 - 0.5f, gz = oz / sp1 - 0.5f;
+        float fx = floorf(gx), fy = floorf(gy), fz = floorf(gz);
+        int32_t bx = (int32_t)fx, by = (int32_t)fy, bz = (int32_t)fz;
+        V.corner_frac[(size_t)level * F.cell_capacity + c] = make_float4(gx - fx, gy - fy, gz - fz, 0.0f);
+        uint32_t *ids = V.corner_ids + ((size_t)level * F.cell_capacity + c) * 8;
+#pragma unroll
+        for (uint32_t corner = 0; corner < 8u; ++corner)
+            ids[corner] = cell_id(V, F, level + 1, bx + (int32_t)(corner & 1u), by + (int32_t)((corner >> 1) & 1u),
+                                  bz + (int32_t)(corner >> 2));
+    }
+}
+
+// interpolateMergedChildSources, shaders/split.slang:389-479 (one group).
+__device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FrameParams &F, uint32_t child_level,
+                                              const uint32_t ids[8], float4 frac, uint32_t dir) {
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f, total = 0.0f, potential = 0.0f;
+    unsigned long long base = V.level_base[child_level];
+    uint32_t dirs = F.dirs[child_level];
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        float ax = (corner & 1u) == 0u ? 1.0f - frac.x : frac.x;
+        float ay = ((corner >> 1) & 1u) == 0u ? 1.0f - frac.y : frac.y;
+        float az = (corner >> 2) == 0u ? 1.0f - frac.z : frac.z;
+        float w = (ax * ay) * az;
+        if (!(w > 0.0f)) continue;
+        potential += w;
+        if (ids[corner] == lux::kEmpty) continue;
+        float4 s = __ldg(V.merged + base + (unsigned long long)ids[corner] * dirs + dir);
+        if (s.w > 0.0f && isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w)) {
+            float sw = w * lux::saturate(s.w);
+            sx = sx + s.x * sw;
+            sy = sy + s.y * sw;
+            sz = sz + s.z * sw;
+            total += sw;
+        }
+    }
+    if (total > 0.0f) return make_float4(sx / total, sy / total, sz / total, lux::saturate(total / fmaxf(potential, 1e-8f)));
+    return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// mergeEntry without history, shaders/split.slang:1523-1725.
+__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, uint32_t level) {
+    if (*V.error_flags) return;
+    uint32_t dirs = F.dirs[level];
+    unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
+    unsigned long long base = V.level_base[level];
+    bool has_children = level + 1u < F.levels;
+    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
+         e += (unsigned long long)gridDim.x * blockDim.x) {
+        uint32_t cnt = V.count[base + e];
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float4 raw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (cnt) {
+            float4 acc = V.accum[base + e];
+            float fn = (float)cnt;
+            raw = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
+            float transmittance = lux::saturate(raw.w);
+            float support = 1.0f - transmittance;
+            float rx = 0.0f, ry = 0.0f, rz = 0.0f;
+            if (support > 0.0f) {
+                rx = raw.x;
+                ry = raw.y;
+                rz = raw.z;
+            }
+            float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
+            if (transmittance > 0.0f && has_children) {
+                uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
+                size_t ci = (size_t)level * F.cell_capacity + cell;
+                uint32_t ids[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) ids[k] = __ldg(V.corner_ids + ci * 8 + k);
+                float4 frac = __ldg(V.corner_frac + ci);
+                uint32_t x = d % F.columns[level], y = d / F.columns[level];
+                uint32_t fine_columns = F.columns[level + 1];
+#pragma unroll
+                for (uint32_t child = 0; child < 4u; ++child) {
+                    uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
+                    float4 v = interpolate(V, F, level + 1, ids, frac, fine);
+                    if (!(v.w > 0.0f)) continue;
+                    cx = cx + v.x * v.w;
+                    cy = cy + v.y * v.w;
+                    cz = cz + v.z * v.w;
+                    csup += v.w;
+                }
+            }
+            if (csup > 0.0f) {
+                rx = rx + (transmittance * cx) * 0.25f;
+                ry = ry + (transmittance * cy) * 0.25f;
+                rz = rz + (transmittance * cz) * 0.25f;
+                support = support + (transmittance * csup) * 0.25f;
+            }
+            if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
+        }
+        V.merged[base + e] = out;
+        V.raw[base + e] = raw;
+    }
+}
+
+// packProbes, shaders/split.slang:1786-1918: one block per cascade-0 cell.
+__global__ void __launch_bounds__(64) pack_kernel(ViewDevice V, FrameParams F) {
+    if (*V.error_flags) return;
+    extern __shared__ float4 smem[];
+    const uint32_t dirs = F.dirs[0];
+    float4 *val = smem;                                   // [dirs]
+    float4 *dir = smem + dirs;                            // [dirs] xyz
+    uint32_t cells = V.cell_count[0];
+    for (uint32_t d = threadIdx.x; d < dirs; d += blockDim.x) {
+        f3 b = lux::bin_direction(d, F.columns[0], F.rows[0]);
+        dir[d] = make_float4(b.x, b.y, b.z, 0.0f);
+    }
+    for (uint32_t cell = blockIdx.x; cell < cells; cell += gridDim.x) {
+        __syncthreads();
+        for (uint32_t d = threadIdx.x; d < dirs; d += blockDim.x) {
+            float4 m = V.merged[V.level_base[0] + (unsigned long long)cell * dirs + d];
+            bool ok = m.w > 0.0f && isfinite(m.x) && isfinite(m.y) && isfinite(m.z) && isfinite(m.w);
+            val[d] = ok ? m : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        __syncthreads();
+        if (threadIdx.x < 36u) {
+            uint32_t texel = threadIdx.x;
+            f3 normal = lux::decode_normal(((float)(texel % 6u) + 0.5f) / 6.0f, ((float)(texel / 6u) + 0.5f) / 6.0f);
+            float sx = 0.0f, sy = 0.0f, sz = 0.0f, nominal = 0.0f, observed = 0.0f;
+            for (uint32_t d = 0; d < dirs; ++d) {
+                float4 dv = dir[d];
+                float cosine = fmaxf(lux::dot(normal, f3{dv.x, dv.y, dv.z}), 0.0f);
+                nominal += cosine;
+                if (cosine <= 0.0f) continue;
+                float4 v = val[d];
+                if (v.w > 0.0f) {
+                    float w = cosine * lux::saturate(v.w);
+                    sx = sx + v.x * w;
+                    sy = sy + v.y * w;
+                    sz = sz + v.z * w;
+                    observed += w;
+                }
+            }
+            float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (nominal > 0.0f) {
+                float scale = nominal * (4.0f / (float)dirs);
+                if (observed > 0.0f)
+                    out = make_float4((sx / observed) * scale, (sy / observed) * scale, (sz / observed) * scale,
+                                      lux::saturate(observed / nominal));
+            }
+            V.tables[(size_t)cell * 36 + texel] = out;
+        }
+    }
+}
+
+// worldResolve at LOD 0, shaders/world_resolve.slang:96-196, :281-313.
+__global__ void __launch_bounds__(128) resolve_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos,
+                                                      const float4 *__restrict__ nrm, uint32_t count,
+                                                      float4 *__restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float4 p = pos[i], n4 = nrm[i];
+    f3 n3{n4.x, n4.y, n4.z};
+    float dx = 0.0f, dy = 0.0f, dz = 0.0f, coverage = 0.0f;
+    bool supported = false;
+    if (*V.error_flags == 0u && lux::finite3(n3) && lux::dot(n3, n3) > 0.01f) {
+        float l = lux::length(n3);
+        f3 normal{n3.x / l, n3.y / l, n3.z / l};
+        float ex, ey;
+        lux::encode_normal(normal, ex, ey);
+        float gx = ex * 6.0f - 0.5f, gy = ey * 6.0f - 0.5f;
+        float bxf = floorf(gx), byf = floorf(gy);
+        float fx = gx - bxf, fy = gy - byf;
+        float cx = 1.0f - fx, cy = 1.0f - fy;
+        float weight[4] = {cx * cy, fx * cy, cx * fy, fx * fy};
+        int32_t ix = (int32_t)bxf, iy = (int32_t)byf;
+        uint32_t texel[4] = {lux::texel_index(ix, iy), lux::texel_index(ix + 1, iy), lux::texel_index(ix, iy + 1),
+                             lux::texel_index(ix + 1, iy + 1)};
+        float s0 = F.spacing[0];
+        float g[3] = {p.x / s0 - 0.5f, p.y / s0 - 0.5f, p.z / s0 - 0.5f};
+        float b[3] = {floorf(g[0]), floorf(g[1]), floorf(g[2])};
+        float fr[3] = {g[0] - b[0], g[1] - b[1], g[2] - b[2]};
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, observed = 0.0f, potential = 0.0f;
+        for (uint32_t corner = 0; corner < 8u; ++corner) {
+            float ax = (corner & 1u) == 0u ? 1.0f - fr[0] : fr[0];
+            float ay = ((corner >> 1) & 1u) == 0u ? 1.0f - fr[1] : fr[1];
+            float az = (corner >> 2) == 0u ? 1.0f - fr[2] : fr[2];
+            float w = (ax * ay) * az;
+            if (!(w > 0.0f)) continue;
+            potential += w;
+            uint32_t cell = cell_id(V, F, 0, (int32_t)b[0] + (int32_t)(corner & 1u),
+                                    (int32_t)b[1] + (int32_t)((corner >> 1) & 1u), (int32_t)b[2] + (int32_t)(corner >> 2));
+            if (cell == lux::kEmpty) continue;
+            // diffuseProbePage, shaders/world_resolve.slang:51-89.
+            float px = 0.0f, py = 0.0f, pz = 0.0f, pobs = 0.0f;
+            for (int c = 0; c < 4; ++c) {
+                float bw = weight[c];
+                if (!(bw > 0.0f)) continue;
+                float4 s = __ldg(V.tables + (size_t)cell * 36 + texel[c]);
+                if (!(s.w > 0.0f) || !(isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w))) continue;
+                float ww = bw * lux::saturate(s.w);
+                px = px + s.x * ww;
+                py = py + s.y * ww;
+                pz = pz + s.z * ww;
+                pobs += ww;
+            }
+            float qx = pobs > 0.0f ? px / pobs : 0.0f, qy = pobs > 0.0f ? py / pobs : 0.0f,
+                  qz = pobs > 0.0f ? pz / pobs : 0.0f;
+            float support = lux::saturate(pobs);
+            if (!(support > 0.0f)) continue;
+            float weight_s = w * support;
+            sx = sx + qx * weight_s;
+            sy = sy + qy * weight_s;
+            sz = sz + qz * weight_s;
+            observed += weight_s;
+        }
+        float lx = 0.0f, ly = 0.0f, lz = 0.0f, low_cov = 0.0f;
+        if (potential > 0.0f) {
+            low_cov = lux::saturate(observed / potential);
+            if (observed > 0.0f) {
+                lx = sx / observed;
+                ly = sy / observed;
+                lz = sz / observed;
+            }
+        }
+        // resolveLodSource with one LOD (blend 0, high coverage 1).
+        float low_weight = low_cov * (1.0f - 0.0f);
+        float high_weight = 1.0f * 0.0f;
+        float total = low_weight + high_weight;
+        coverage = lux::saturate(total);
+        dx = total > 0.0f ? (lx * low_weight + 0.0f * high_weight) / total : 0.0f;
+        dy = total > 0.0f ? (ly * low_weight + 0.0f * high_weight) / total : 0.0f;
+        dz = total > 0.0f ? (lz * low_weight + 0.0f * high_weight) / total : 0.0f;
+        supported = coverage > 0.0f && isfinite(dx) && isfinite(dy) && isfinite(dz);
+    }
+    // rawGiSupportAlpha, shaders/common.slang:323-326.
+    out[i] = make_float4(dx, dy, dz, supported ? 1.0f + 0.25f * coverage : -1.0f);
+}
+
+uint32_t next_pow2(uint64_t v) {
+    uint64_t p = 64;
+    while (p < v) p <<= 1;
+    return (uint32_t)p;
+}
+
+}  // namespace
+
+constexpr int kTimingEvents = 7;
+
+struct LuxView {
+    LuxContext *ctx = nullptr;
+    bool timing = false;
+    cudaEvent_t ev[kTimingEvents] = {};
+    LuxViewDesc desc{};
+    ViewDevice dev{};
+    uint32_t dir_capacity = 0;
+    void *stage_pos = nullptr, *stage_nrm = nullptr, *stage_ppos = nullptr, *stage_pnrm = nullptr, *stage_out = nullptr;
+    uint32_t stage_receivers = 0, stage_points = 0;
+    FrameParams last{};
+    bool has_frame = false;
+};
+
+static lux_status view_alloc(LuxView *v) {
+    LuxContext *ctx = v->ctx;
+    const LuxViewDesc &d = v->desc;
+    ViewDevice &D = v->dev;
+    v->dir_capacity = next_pow2(2ull * d.max_cells);
+    size_t L = LUX_MAX_LEVELS;
+    struct A {
+        void **p;
+        size_t bytes;
+    } allocs[] = {
+        {(void **)&D.dir_keys, L * v->dir_capacity * sizeof(unsigned long long)},
+        {(void **)&D.dir_ids, L * v->dir_capacity * sizeof(uint32_t)},
+        {(void **)&D.cell_keys, L * d.max_cells * sizeof(int4)},
+        {(void **)&D.cell_count, L * sizeof(uint32_t)},
+        {(void **)&D.level_base, L * sizeof(unsigned long long)},
+        {(void **)&D.receiver_cell, L * (size_t)d.max_receivers * sizeof(uint32_t)},
+        {(void **)&D.corner_ids, L * (size_t)d.max_cells * 8 * sizeof(uint32_t)},
+        {(void **)&D.corner_frac, L * (size_t)d.max_cells * sizeof(float4)},
+        {(void **)&D.accum, (size_t)d.max_entries * sizeof(float4)},
+        {(void **)&D.count, (size_t)d.max_entries * sizeof(uint32_t)},
+        {(void **)&D.merged, (size_t)d.max_entries * sizeof(float4)},
+        {(void **)&D.raw, (size_t)d.max_entries * sizeof(float4)},
+        {(void **)&D.tables, (size_t)d.max_cells * 36 * sizeof(float4)},
+        {(void **)&D.error_flags, sizeof(uint32_t) * 4},
+        {(void **)&D.stats, 8 * sizeof(unsigned long long)},
+    };
+    for (auto &a : allocs) {
+        if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "view: device allocation failed");
+        }
+    }
+    cudaMemsetAsync(D.error_flags, 0, 16, ctx->stream);
+    cudaMemsetAsync(D.stats, 0, 64, ctx->stream);
+    cudaMemsetAsync(D.cell_count, 0, L * 4, ctx->stream);
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "view allocation");
+}
+
+extern "C" lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out) {
+    if (!ctx || !desc || !out) return LUX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    if (desc->max_receivers == 0 || desc->max_cells == 0 || desc->max_entries == 0)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: capacities must be positive");
+    if (desc->max_cells > (1u << 30))
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_cells above 2^30");
+    LuxView *v = new LuxView();
+    v->ctx = ctx;
+    v->desc = *desc;
+    lux_status s = view_alloc(v);
+    if (s != LUX_OK) {
+        lux_view_destroy(v);
+        return s;
+    }
+    *out = v;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_destroy(LuxView *v) {
+    if (!v) return LUX_OK;
+    ViewDevice &D = v->dev;
+    void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
+                    D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
+                    v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    for (int i = 0; i < kTimingEvents; ++i)
+        if (v->ev[i]) cudaEventDestroy(v->ev[i]);
+    delete v;
+    return LUX_OK;
+}
+
+static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32_t receivers, FrameParams &F) {
+    LuxSettings s = *settings_in;
+    lux_settings_sanitize(&s);
+    std::memset(&F, 0, sizeof F);
+    F.levels = s.levels;
+    F.layout = s.layout;
+    F.rays_per_receiver = s.rays_per_receiver;
+    F.receivers = receivers;
+    F.dir_capacity = v->dir_capacity;
+    F.cell_capacity = v->desc.max_cells;
+    F.entry_capacity = v->desc.max_entries;
+    for (uint32_t l = 0; l < s.levels; ++l) {
+        F.spacing[l] = s.probe_spacing * (float)(1u << l);
+        F.end[l] = lux_interval_end(&s, l);
+        F.start[l] = l == 0 ? 0.0f : lux_interval_end(&s, l - 1);
+        F.columns[l] = s.base_columns << l;
+        F.rows[l] = s.base_rows << l;
+        F.dirs[l] = F.columns[l] * F.rows[l];
+    }
+    F.shade.probe_spacing = s.probe_spacing;
+    F.shade.normal_bias = s.normal_bias;
+    F.shade.exposure = s.exposure;
+    F.shade.emissive_samples = s.emissive_samples;
+    F.shade.frame = s.frame_index;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, const LuxSettings *settings,
+                                           const LuxReceivers *rc) {
+    if (!v || !scene || !settings || !rc) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = v->ctx;
+    if (rc->count > v->desc.max_receivers)
+        return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: more receivers than the view's max_receivers");
+    if (rc->count && (!rc->position || (!rc->normal && settings->layout == LUX_LAYOUT_SPLIT)))
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: missing receiver buffers");
+    FrameParams F;
+    make_params(v, settings, rc->count, F);
+    if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > 0xffffffffull)
+        return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: ray count exceeds 2^32");
+    const ViewDevice &D = v->dev;
+    cudaStream_t st = ctx->stream;
+    const int grid = ctx->sm_count * 8;
+    const float4 *pos = (const float4 *)rc->position;
+    const float4 *nrm = (const float4 *)rc->normal;
+    auto mark = [&](int i) {
+        if (v->timing) cudaEventRecord(v->ev[i], st);
+    };
+    mark(0);
+    clear_kernel<<<grid, 256, 0, st>>>(D, F);
+    if (rc->count) {
+        seed_insert_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+        seed_assign_kernel<<<grid, 256, 0, st>>>(D, F);
+        seed_lookup_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+    }
+    layout_kernel<<<1, 32, 0, st>>>(D, F);
+    clear_entries_kernel<<<grid, 256, 0, st>>>(D, F);
+    mark(1);
+    if (F.layout == LUX_LAYOUT_SPLIT) {
+        uint32_t rays = rc->count * F.rays_per_receiver;
+        if (rays) trace_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, pos, nrm, rays);
+    } else {
+        for (uint32_t l = 0; l < F.levels; ++l) trace_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
+    }
+    mark(2);
+    for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
+    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, (uint32_t)l);
+    mark(3);
+    size_t smem = (size_t)F.dirs[0] * 2 * sizeof(float4);
+    if (smem > 48 * 1024) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: too many cascade-0 directions");
+    pack_kernel<<<grid, 64, smem, st>>>(D, F);
+    mark(4);
+    v->last = F;
+    v->has_frame = true;
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "trace_merge launch");
+}
+
+extern "C" lux_status lux_view_resolve(LuxView *v, const LuxSettings *settings, const float *ppos, const float *pnrm,
+                                       uint32_t count, float *out) {
+    if (!v || !settings || (count && (!ppos || !pnrm || !out))) return LUX_ERR_INVALID_ARGUMENT;
+    if (!v->has_frame) return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "resolve: no frame traced yet");
+    if (count == 0) return LUX_OK;
+    if (v->timing) cudaEventRecord(v->ev[5], v->ctx->stream);
+    resolve_kernel<<<(count + 127) / 128, 128, 0, v->ctx->stream>>>(v->dev, v->last, (const float4 *)ppos,
+                                                                      (const float4 *)pnrm, count, (float4 *)out);
+    if (v->timing) cudaEventRecord(v->ev[6], v->ctx->stream);
+    return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "resolve launch");
+}
+
+static lux_status ensure_stage(LuxView *v, uint32_t receivers, uint32_t points) {
+    if (receivers > v->stage_receivers) {
+        cudaFree(v->stage_pos);
+        cudaFree(v->stage_nrm);
+        v->stage_pos = v->stage_nrm = nullptr;
+        if (cudaMalloc(&v->stage_pos, (size_t)receivers * 16) != cudaSuccess ||
+            cudaMalloc(&v->stage_nrm, (size_t)receivers * 16) != cudaSuccess) {
+            cudaGetLastError();
+            v->stage_receivers = 0;
+            return lux_fail(v->ctx, LUX_ERR_OUT_OF_MEMORY, "frame_host: staging allocation failed");
+        }
+        v->stage_receivers = receivers;
+    }
+    if (points > v->stage_points) {
+        cudaFree(v->stage_ppos);
+        cudaFree(v->stage_pnrm);
+        cudaFree(v->stage_out);
+        v->stage_ppos = v->stage_pnrm = v->stage_out = nullptr;
+        if (cudaMalloc(&v->stage_ppos, (size_t)points * 16) != cudaSuccess ||
+            cudaMalloc(&v->stage_pnrm, (size_t)points * 16) != cudaSuccess ||
+            cudaMalloc(&v->stage_out, (size_t)points * 16) != cudaSuccess) {
+            cudaGetLastError();
+            v->stage_points = 0;
+            return lux_fail(v->ctx, LUX_ERR_OUT_OF_MEMORY, "frame_host: staging allocation failed");
+        }
+        v->stage_points = points;
+    }
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_frame_host(LuxView *v, const LuxScene *scene, const LuxSettings *settings,
+                                          const float *rpos, const float *rnrm, uint32_t receivers, const float *ppos,
+                                          const float *pnrm, uint32_t points, float *out) {
+    if (!v || !scene || !settings || (receivers && (!rpos || !rnrm)) || (points && (!ppos || !pnrm || !out)))
+        return LUX_ERR_INVALID_ARGUMENT;
+    lux_status s = ensure_stage(v, receivers, points);
+    if (s != LUX_OK) return s;
+    cudaStream_t st = v->ctx->stream;
+    cudaMemcpyAsync(v->stage_pos, rpos, (size_t)receivers * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(v->stage_nrm, rnrm, (size_t)receivers * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(v->stage_ppos, ppos, (size_t)points * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(v->stage_pnrm, pnrm, (size_t)points * 16, cudaMemcpyHostToDevice, st);
+    LuxReceivers rc{(const float *)v->stage_pos, (const float *)v->stage_nrm, receivers};
+    s = lux_view_trace_merge(v, scene, settings, &rc);
+    if (s != LUX_OK) return s;
+    s = lux_view_resolve(v, settings, (const float *)v->stage_ppos, (const float *)v->stage_pnrm, points,
+                         (float *)v->stage_out);
+    if (s != LUX_OK) return s;
+    cudaMemcpyAsync(out, v->stage_out, (size_t)points * 16, cudaMemcpyDeviceToHost, st);
+    s = lux_cuda_check(v->ctx, (int)cudaStreamSynchronize(st), "frame_host");
+    if (s != LUX_OK) return s;
+    uint32_t flags = 0;
+    cudaMemcpy(&flags, v->dev.error_flags, 4, cudaMemcpyDeviceToHost);
+    if (flags) return lux_fail(v->ctx, LUX_ERR_CAPACITY, "frame_host: view capacity exceeded (see lux_view_stats)");
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_stats(LuxView *v, LuxStats *out) {
+    if (!v || !out) return LUX_ERR_INVALID_ARGUMENT;
+    cudaStream_t st = v->ctx->stream;
+    lux_status s = lux_cuda_check(v->ctx, (int)cudaStreamSynchronize(st), "stats");
+    if (s != LUX_OK) return s;
+    unsigned long long stats[8];
+    uint32_t counts[LUX_MAX_LEVELS];
+    uint32_t flags = 0;
+    cudaMemcpy(stats, v->dev.stats, sizeof stats, cudaMemcpyDeviceToHost);
+    cudaMemcpy(counts, v->dev.cell_count, sizeof counts, cudaMemcpyDeviceToHost);
+    cudaMemcpy(&flags, v->dev.error_flags, 4, cudaMemcpyDeviceToHost);
+    std::memset(out, 0, sizeof *out);
+    out->interval_rays = stats[kStatInterval];
+    out->shadow_rays = stats[kStatShadow];
+    out->nodes_visited = stats[kStatNodes];
+    out->triangles_tested = stats[kStatTris];
+    out->instances_visited = stats[kStatInst];
+    out->deposits = stats[kStatDeposits];
+    out->unsupported = stats[kStatUnsupported];
+    out->levels = v->last.levels;
+    for (uint32_t l = 0; l < v->last.levels; ++l) {
+        out->cells[l] = counts[l];
+        out->entries[l] = (uint64_t)counts[l] * v->last.dirs[l];
+    }
+    out->error_flags = flags;
+    return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "stats copy");
+}
+
+extern "C" lux_status lux_view_read_level(LuxView *v, uint32_t level, int32_t *keys, float *merged, float *raw,
+                                          uint32_t *samples) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    if (!v->has_frame || level >= v->last.levels) return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "read_level: bad level");
+    cudaStreamSynchronize(v->ctx->stream);
+    uint32_t counts[LUX_MAX_LEVELS];
+    unsigned long long bases[LUX_MAX_LEVELS];
+    cudaMemcpy(counts, v->dev.cell_count, sizeof counts, cudaMemcpyDeviceToHost);
+    cudaMemcpy(bases, v->dev.level_base, sizeof bases, cudaMemcpyDeviceToHost);
+    uint32_t cells = counts[level];
+    size_t entries = (size_t)cells * v->last.dirs[level];
+    if (keys) cudaMemcpy(keys, v->dev.cell_keys + (size_t)level * v->desc.max_cells, (size_t)cells * 16, cudaMemcpyDeviceToHost);
+    if (merged) cudaMemcpy(merged, v->dev.merged + bases[level], entries * 16, cudaMemcpyDeviceToHost);
+    if (raw) cudaMemcpy(raw, v->dev.raw + bases[level], entries * 16, cudaMemcpyDeviceToHost);
+    if (samples) cudaMemcpy(samples, v->dev.count + bases[level], entries * 4, cudaMemcpyDeviceToHost);
+    return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "read_level");
+}
+
+extern "C" lux_status lux_view_read_probes(LuxView *v, int32_t *keys, float *tables) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    if (!v->has_frame) return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "read_probes: no frame");
+    cudaStreamSynchronize(v->ctx->stream);
+    uint32_t cells = 0;
+    cudaMemcpy(&cells, v->dev.cell_count, 4, cudaMemcpyDeviceToHost);
+    if (keys) cudaMemcpy(keys, v->dev.cell_keys, (size_t)cells * 16, cudaMemcpyDeviceToHost);
+    if (tables) cudaMemcpy(tables, v->dev.tables, (size_t)cells * 36 * 16, cudaMemcpyDeviceToHost);
+    return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "read_probes");
+}
+
+extern "C" lux_status lux_view_set_timing(LuxView *v, uint32_t enable) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    if (enable && !v->ev[0]) {
+        for (int i = 0; i < kTimingEvents; ++i)
+            if (cudaEventCreate(&v->ev[i]) != cudaSuccess)
+                return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "timing events");
+    }
+    v->timing = enable != 0;
+    return LUX_OK;
+}
+
+// Per-stage device times of the last frame in milliseconds (the reference's
+// per-pass timestamp spans, src/render.rs:9323-9333): seed, trace, merge,
+// pack, resolve.
+extern "C" lux_status lux_view_timings(LuxView *v, LuxTimings *out) {
+    if (!v || !out) return LUX_ERR_INVALID_ARGUMENT;
+    if (!v->timing) return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "timings: timing is disabled");
+    lux_status s = lux_cuda_check(v->ctx, (int)cudaStreamSynchronize(v->ctx->stream), "timings");
+    if (s != LUX_OK) return s;
+    float ms[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&ms[i], v->ev[i], v->ev[i + 1]);
+    cudaEventElapsedTime(&ms[4], v->ev[5], v->ev[6]);
+    cudaGetLastError();
+    out->seed_ms = ms[0];
+    out->trace_ms = ms[1];
+    out->merge_ms = ms[2];
+    out->pack_ms = ms[3];
+    out->resolve_ms = ms[4];
+    return LUX_OK;
+}

@@ -1,0 +1,287 @@
+/*
+ * lux.h - C ABI of the B200 Split Radiance Cascades transport library (liblux).
+ *
+ * This is the drop-in boundary for the Split transport hot path of bevy_lux
+ * (HyperExtendedReality/bevy_penumbra): closest-hit BVH traversal of cascade
+ * interval rays, interval deposit, the split cascade merge, probe packing and
+ * the world-space probe resolve.  In the reference these run as Slang compute
+ * dispatches issued by `render` (src/render.rs:9553-9801); here each call
+ * below replaces one group of those dispatches.
+ *
+ * Conventions
+ *  - Every function returns lux_status; 0 (LUX_OK) is success.  No C++
+ *    exception crosses this boundary.  The text of the last failure of a
+ *    context is available from lux_last_error_message (the reference records
+ *    failures as strings: RadianceCascadesStatus::record_failure,
+ *    src/lib.rs:225-230).
+ *  - Handles are opaque and owned by the library.  Calls on one context must
+ *    be serialised by the caller; distinct contexts may run on distinct host
+ *    threads.
+ *  - Pointers documented as "device" are CUDA device pointers on the
+ *    context's device; all device work is ordered on the context's stream.
+ *  - Scene inputs are the reference's own packed word streams (uint4 words,
+ *    little endian), so src/scene.rs output can be passed unchanged.
+ */
+#ifndef LUX_H
+#define LUX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LUX_ABI_VERSION 1u
+
+typedef enum lux_status {
+    LUX_OK = 0,
+    LUX_ERR_INVALID_ARGUMENT = 1,
+    LUX_ERR_CUDA = 2,
+    LUX_ERR_OUT_OF_MEMORY = 3,
+    LUX_ERR_CAPACITY = 4,        /* a view's fixed capacity was exceeded */
+    LUX_ERR_MALFORMED_SCENE = 5, /* scene words failed validation */
+    LUX_ERR_NO_DEVICE = 6,
+    LUX_ERR_TIMEOUT = 7,         /* a bounded device wait gave up */
+    LUX_ERR_INTERNAL = 8
+} lux_status;
+
+/* Hit.errors bits, same values as shaders/traversal.slang:16 and :500,:743. */
+#define LUX_HIT_BLAS_FALLBACK 1u
+#define LUX_HIT_TLAS_FALLBACK 2u
+#define LUX_HIT_QUERY_UNSUPPORTED 4u
+#define LUX_EMPTY 0xffffffffu
+
+typedef struct LuxContext LuxContext;
+typedef struct LuxScene LuxScene;
+typedef struct LuxView LuxView;
+
+typedef struct LuxDeviceDesc {
+    int32_t device;  /* CUDA ordinal */
+    void *stream;    /* cudaStream_t to order work on; NULL = library-owned stream */
+} LuxDeviceDesc;
+
+/* One ray of the traversal harness: the reference's `Ray` of
+ * src/traversal_tests.rs (origin, direction, limit, any_hit). */
+typedef struct LuxRay {
+    float origin[3];
+    float tmin;       /* hits must satisfy t > max(tmin, 2.5e-5) */
+    float direction[3];
+    float limit;      /* hits must satisfy t < limit */
+} LuxRay;
+
+/* Closest-hit record: the reference's Hit (shaders/traversal.slang:1). */
+typedef struct LuxHit {
+    float distance;
+    uint32_t triangle;
+    uint32_t instance;
+    uint32_t errors;
+    float barycentric[3];
+    uint32_t visited;  /* nodes visited (statistics) */
+} LuxHit;
+
+/* Emitter / light record, the reference's `Light`
+ * (shaders/common.slang:110): position, color, direction, edge1, edge2 as
+ * float4 then source as uint4; 24 words.  Emissive triangle records follow
+ * the conventional ones exactly as build_emissive_lights writes them
+ * (src/scene.rs:2311-2372). */
+typedef struct LuxLight {
+    float position[4];
+    float color[4];
+    float direction[4];
+    float edge1[4];
+    float edge2[4];
+    uint32_t source[4];
+} LuxLight;
+
+/* Probe layouts. */
+#define LUX_LAYOUT_SPLIT 0u      /* receivers trace rays and deposit into every level (the reference's Split) */
+#define LUX_LAYOUT_DENSE 1u      /* every (probe, direction) of every level traces its own interval */
+
+/* Interval growth rules. */
+#define LUX_INTERVAL_ENDS_GEOMETRIC 0u   /* end_L = length * ratio^L (reference: ratio 4, shaders/split.slang:224-227) */
+#define LUX_INTERVAL_LENGTHS_GEOMETRIC 1u /* length_L = length * ratio^L, end_L = sum of lengths */
+
+#define LUX_MAX_LEVELS 12u
+
+/* Per-view transport settings.  Field names and clamps follow
+ * RadianceCascades / SamplingSettings (src/lib.rs:343-518, sanitized at
+ * src/lib.rs:731-759); the fields marked "extension" parameterise what the
+ * reference hard-codes (CASCADES = 4, BASE_THETA = 4 and the x4 interval rule,
+ * shaders/common.slang:10-11, shaders/split.slang:224-231). */
+typedef struct LuxSettings {
+    float probe_spacing;            /* RadianceCascades::probe_spacing (tuning.x) */
+    float interval_length;          /* RadianceCascades::interval_length (tuning.y) */
+    float normal_bias;              /* RadianceCascades::normal_bias (tuning.z) */
+    float intensity;                /* RadianceCascades::intensity (tuning.w) */
+    float environment[3];           /* RadianceCascades::environment (escape radiance of hit-surface NEE; primary escapes are supported zero) */
+    float exposure;                 /* camera exposure (params.environment.w) */
+    uint32_t emissive_samples;      /* RadianceCascades::emissive_samples, 1..=32; NEE draws max(1, n/2) */
+    uint32_t levels;                /* extension: cascade count, 1..=LUX_MAX_LEVELS (reference 4) */
+    uint32_t base_columns;          /* extension: azimuth bins at cascade 0 (reference 2*BASE_THETA = 8) */
+    uint32_t base_rows;             /* extension: polar bins at cascade 0 (reference BASE_THETA = 4) */
+    float interval_ratio;           /* extension: growth ratio (reference 4) */
+    uint32_t interval_rule;         /* extension: LUX_INTERVAL_* (reference ENDS_GEOMETRIC) */
+    uint32_t layout;                /* LUX_LAYOUT_* */
+    uint32_t rays_per_receiver;     /* Split layout: rays traced per receiver per frame (reference 1) */
+    uint32_t frame_index;           /* params.frame.x */
+    uint32_t resolve_scale;         /* SamplingSettings::resolve_scale, 1..=8 */
+} LuxSettings;
+
+/* Receivers (Split) or the cascade-0 probe set (Dense), device pointers.
+ * position[i] = (x, y, z, unused), normal[i] = (geometric normal, unused).
+ * For the dense layout normals are ignored and positions are cascade-0
+ * probe centres. */
+typedef struct LuxReceivers {
+    const float *position;  /* device float4[count] */
+    const float *normal;    /* device float4[count] */
+    uint32_t count;
+} LuxReceivers;
+
+/* Device-side statistics of the last frame (the reference's head counters,
+ * shaders/split.slang:517-533). */
+typedef struct LuxStats {
+    uint64_t interval_rays;     /* closest-hit interval rays traced */
+    uint64_t shadow_rays;       /* NEE visibility rays traced */
+    uint64_t nodes_visited;     /* BVH4 nodes visited by all rays */
+    uint64_t triangles_tested;  /* triangle tests by all rays */
+    uint64_t instances_visited; /* instance transforms applied */
+    uint64_t deposits;          /* (level, entry) samples deposited */
+    uint64_t unsupported;       /* rays whose query was unsupported */
+    uint32_t cells[LUX_MAX_LEVELS];
+    uint64_t entries[LUX_MAX_LEVELS];
+    uint32_t levels;
+    uint32_t error_flags;       /* LUX_VIEW_ERR_* bits raised on the device */
+} LuxStats;
+
+#define LUX_VIEW_ERR_CELL_CAPACITY 1u
+#define LUX_VIEW_ERR_ENTRY_CAPACITY 2u
+#define LUX_VIEW_ERR_PROBE_LOOKUP 4u
+
+/* Capacities of a view (ViewBuffers, src/render.rs:5077-5160). */
+typedef struct LuxViewDesc {
+    uint32_t max_receivers;  /* receivers (Split) or cascade-0 probes (Dense) */
+    uint32_t max_cells;      /* distinct world cells per level */
+    uint64_t max_entries;    /* (cell, direction) records summed over levels */
+} LuxViewDesc;
+
+/* ---- library / context ---------------------------------------------- */
+uint32_t lux_abi_version(void);
+lux_status lux_context_create(const LuxDeviceDesc *desc, LuxContext **out);
+lux_status lux_context_destroy(LuxContext *ctx);
+const char *lux_last_error_message(const LuxContext *ctx);
+lux_status lux_context_synchronize(LuxContext *ctx);
+
+/* ---- settings (RadianceCascades mirror, src/lib.rs:671-759) ----------- */
+void lux_settings_default(LuxSettings *out);   /* RadianceCascades::default() */
+void lux_settings_low_end(LuxSettings *out);   /* RadianceCascades::low_end() */
+void lux_settings_sanitize(LuxSettings *s);    /* RadianceCascades::sanitized() */
+/* Interval end of `level` (shaders/split.slang:224-227 generalised). */
+float lux_interval_end(const LuxSettings *s, uint32_t level);
+uint32_t lux_direction_count(const LuxSettings *s, uint32_t level);
+
+/* ---- scene (GiScene words, src/scene.rs:2096-2117, :809-823) ---------- */
+/* Packs meshes and instances into the reference's word streams.  Restates
+ * build_tree (binned SAH, 12 bins, leaves <= 4, depth <= 48,
+ * src/scene.rs:2398-2554), node_words (src/scene.rs:1025-1038),
+ * pack_instances (src/scene.rs:1071-1122), geometry_words
+ * (src/scene.rs:809-823) and build_emissive_lights (src/scene.rs:2311-2372).
+ * Inputs (host):
+ *   positions[3*vertex_count], indices[3*triangle_count] (global vertex ids)
+ *   mesh_first_triangle[mesh_count], mesh_triangle_count[mesh_count]
+ *   per instance (host): mesh id, world_from_local 3x4 row-major (12 floats),
+ *   flags (bits 0-1 cull mode, 2 mirror), material id
+ *   materials: 8 uint4 words each (MATERIAL_WORDS, src/material.rs:16)
+ * The library keeps the packed words; query sizes then copy them out. */
+typedef struct LuxPackedScene LuxPackedScene;
+lux_status lux_scene_pack(const float *positions, uint32_t vertex_count,
+                          const uint32_t *indices, uint32_t triangle_count,
+                          const uint32_t *mesh_first_triangle, const uint32_t *mesh_triangle_count,
+                          uint32_t mesh_count,
+                          const uint32_t *instance_mesh, const float *instance_world_from_local,
+                          const uint32_t *instance_flags, const uint32_t *instance_material,
+                          uint32_t instance_count,
+                          const uint32_t *material_words, uint32_t material_count,
+                          LuxPackedScene **out);
+/* Word counts are in uint4 units; light count in LuxLight records. */
+lux_status lux_packed_scene_sizes(const LuxPackedScene *p, size_t *scene_words,
+                                  size_t *geometry_words, size_t *lights,
+                                  uint32_t *tlas_nodes, uint32_t *blas_nodes);
+lux_status lux_packed_scene_copy(const LuxPackedScene *p, uint32_t *scene_words,
+                                 uint32_t *geometry_words, LuxLight *lights);
+/* Packed instance i is caller instance order[i] (the TLAS build permutes
+ * instances into leaf order, src/scene.rs:2052). */
+lux_status lux_packed_scene_instance_order(const LuxPackedScene *p, uint32_t *order);
+/* SAH cost of the packed TLAS and of all BLASes (tree_cost, src/scene.rs:2383-2396)
+ * and the maximum leaf depth. */
+lux_status lux_packed_scene_quality(const LuxPackedScene *p, double *blas_cost,
+                                    uint32_t *max_depth);
+void lux_packed_scene_destroy(LuxPackedScene *p);
+
+/* Uploads word streams (host pointers) and builds the device BVH4 layout.
+ * scene_words = [header, TLAS node words, BLAS node words, instance words,
+ * materials...]; conventional_lights = how many leading light records are
+ * conventional (lightCounts.x); the rest are emissive (lightCounts.y). */
+lux_status lux_scene_upload(LuxContext *ctx,
+                            const uint32_t *scene_words, size_t scene_word_count,
+                            const uint32_t *geometry_words, size_t geometry_word_count,
+                            const LuxLight *lights, uint32_t light_count,
+                            uint32_t conventional_lights,
+                            LuxScene **out);
+lux_status lux_scene_destroy(LuxScene *scene);
+/* Device BVH4 size facts: nodes (TLAS+BLAS) and node/triangle record bytes. */
+lux_status lux_scene_layout(const LuxScene *scene, uint32_t *nodes, uint32_t *node_bytes,
+                            uint32_t *triangles, uint32_t *triangle_bytes,
+                            uint32_t *instances);
+
+/* ---- traversal (traceRay / traceOccluded, shaders/traversal.slang:696-1046) -- */
+/* Closest hit (any_hit = 0) or occlusion (any_hit = 1) for `count` rays.
+ * rays: device LuxRay[count]; hits: device LuxHit[count].  For any-hit rays
+ * hits[i].triangle != LUX_EMPTY means blocked. */
+lux_status lux_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *rays,
+                          uint32_t count, uint32_t any_hit, LuxHit *hits);
+
+/* ---- cascade view (render(), src/render.rs:9124-9830) ------------------ */
+lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out);
+lux_status lux_view_destroy(LuxView *view);
+/* seed -> trace (+NEE) -> deposit -> merge (levels L-1..0) -> pack.
+ * Replaces the dispatch sequence clear..packProbes (src/render.rs:9553-9801). */
+lux_status lux_view_trace_merge(LuxView *view, const LuxScene *scene, const LuxSettings *settings,
+                                const LuxReceivers *receivers);
+/* worldResolve (shaders/world_resolve.slang:281-313): for each point
+ * (device float4 position, float4 shading normal) writes device float4
+ * (irradiance / pi, alpha = 1 + 0.25 coverage | -1 | 0). */
+lux_status lux_view_resolve(LuxView *view, const LuxSettings *settings, const float *points_position,
+                            const float *points_normal, uint32_t count, float *out_irradiance);
+/* The same frame with HOST buffers: copies receivers and resolve points to
+ * the device, runs trace_merge and resolve, copies irradiance back, and
+ * synchronises.  This is the call a host engine makes per frame. */
+lux_status lux_view_frame_host(LuxView *view, const LuxScene *scene, const LuxSettings *settings,
+                               const float *receiver_position, const float *receiver_normal,
+                               uint32_t receiver_count, const float *points_position,
+                               const float *points_normal, uint32_t point_count,
+                               float *out_irradiance);
+lux_status lux_view_stats(LuxView *view, LuxStats *out);
+/* Per-stage CUDA-event timing of a view's frames (the reference's per-pass
+ * timestamp spans, src/render.rs:9323-9333). */
+typedef struct LuxTimings {
+    float seed_ms;     /* clear + seed + record layout */
+    float trace_ms;    /* closest hit + hit shading + deposit */
+    float merge_ms;    /* corner tables + merge of every level */
+    float pack_ms;     /* cascade-0 probe tables */
+    float resolve_ms;  /* last lux_view_resolve */
+} LuxTimings;
+lux_status lux_view_set_timing(LuxView *view, uint32_t enable);
+lux_status lux_view_timings(LuxView *view, LuxTimings *out);
+/* Copies one level's records to host memory (tests): cell keys int4[cells],
+ * merged float4[cells*dirs] (I.rgb, support), raw float4[cells*dirs]
+ * (J.rgb, beta) and sample counts uint32[cells*dirs].  Any pointer may be NULL. */
+lux_status lux_view_read_level(LuxView *view, uint32_t level, int32_t *cell_keys,
+                               float *merged, float *raw, uint32_t *samples);
+/* Copies packed cascade-0 probe tables: keys int4[cells], tables float4[cells*36]. */
+lux_status lux_view_read_probes(LuxView *view, int32_t *cell_keys, float *tables);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LUX_H */

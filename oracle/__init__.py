@@ -1,0 +1,184 @@
+"""CPU oracle of bevy_lux's Split transport path (test infrastructure only).
+
+Loaded by the tests, the smoke check and the CPU-baseline leg of bench.py as
+the parity checker; the product (bevy_penumbra_b200) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liblux_oracle.so")
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "lux_oracle.c")
+    hdr = os.path.join(HERE, "lux_oracle.h")
+    if force or not os.path.exists(LIB) or max(os.path.getmtime(src), os.path.getmtime(hdr)) > os.path.getmtime(LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "liblux_oracle.so"], check=True)
+    return LIB
+
+
+class Counters(C.Structure):
+    _fields_ = [("nodes", C.c_uint64), ("triangles", C.c_uint64), ("instances", C.c_uint64)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        h = C.CDLL(LIB)
+        P = C.c_void_p
+        U = C.c_uint32
+        F = C.c_float
+        sig = {
+            "orc_sincos_turns": (None, [F, P, P]),
+            "orc_decode_direction": (None, [F, F, P]),
+            "orc_bin_direction": (None, [U, U, U, P]),
+            "orc_direction_index_uv": (U, [F, F, U, U]),
+            "orc_r2": (None, [U, P]),
+            "orc_transport_hash": (U, [U]),
+            "orc_hash_key": (U, [P, U]),
+            "orc_ray_offset": (None, [P, P, F, P]),
+            "orc_encode_normal": (None, [P, P]),
+            "orc_decode_normal": (None, [P, P]),
+            "orc_interval_end": (F, [P, U]),
+            "orc_spacing": (F, [P, U]),
+            "orc_scene_create": (P, [P, C.c_size_t, P, C.c_size_t, P, U, U]),
+            "orc_scene_destroy": (None, [P]),
+            "orc_trace_closest": (None, [P, P, P, F, F, P, P]),
+            "orc_trace_occluded": (C.c_int, [P, P, P, F, P, P]),
+            "orc_brute_closest": (None, [P, P, P, F, F, P]),
+            "orc_brute_f64": (U, [P, P, P, F, P, P, P, U]),
+            "orc_trace_rays": (None, [P, P, U, C.c_int, P, C.c_int, P]),
+            "orc_outgoing_radiance": (C.c_int, [P, P, P, P, P, P, P, P]),
+            "orc_frame_run": (P, [P, P, P, P, U, C.c_int]),
+            "orc_frame_destroy": (None, [P]),
+            "orc_frame_cells": (U, [P, U]),
+            "orc_frame_read_level": (None, [P, U, P, P, P, P]),
+            "orc_frame_read_probes": (None, [P, P]),
+            "orc_frame_stats": (None, [P, P]),
+            "orc_frame_resolve": (None, [P, P, P, U, P]),
+            "orc_deposit_levels": (U, [P, F, C.c_int, C.c_int, P, P]),
+            "orc_merge_entry": (None, [P, U, P, P, C.c_int, P]),
+            "orc_interpolate_children": (None, [P, P, P]),
+            "orc_pack_table": (None, [P, U, U, P]),
+            "orc_probe_lookup": (None, [P, P, P]),
+            "orc_dense_sdf_record": (None, [U, P, P]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(h, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = h
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data if a is not None and a.size else 0
+
+
+def f32(*v) -> np.ndarray:
+    return np.ascontiguousarray(np.array(v, dtype=np.float32).ravel())
+
+
+class OracleScene:
+    """Oracle view of the reference word streams."""
+
+    def __init__(self, scene_words: np.ndarray, geometry_words: np.ndarray, lights: np.ndarray):
+        self._keep = (np.ascontiguousarray(scene_words, np.uint32), np.ascontiguousarray(geometry_words, np.uint32),
+                      np.ascontiguousarray(lights, np.uint32))
+        sw, gw, lt = self._keep
+        self.handle = lib().orc_scene_create(_p(sw), sw.size // 4, _p(gw), gw.size // 4, _p(lt), lt.size // 24, 0)
+
+    @staticmethod
+    def from_packed(packed) -> "OracleScene":
+        return OracleScene(packed.scene_words, packed.geometry_words, packed.lights)
+
+    def trace_rays(self, rays: np.ndarray, any_hit: bool = False, threads: int = 0):
+        """rays: structured RAY_DTYPE array -> HIT_DTYPE array, counters."""
+        from bevy_penumbra_b200 import HIT_DTYPE  # record layout only
+        rays = np.ascontiguousarray(rays)
+        hits = np.zeros(len(rays), dtype=HIT_DTYPE)
+        cn = Counters()
+        lib().orc_trace_rays(self.handle, _p(rays), len(rays), 1 if any_hit else 0, _p(hits),
+                             threads or os.cpu_count() or 1, C.byref(cn))
+        return hits, cn
+
+    def brute_f64(self, origin, direction, limit, capacity: int = 64):
+        t = np.zeros(capacity, np.float64)
+        tri = np.zeros(capacity, np.uint32)
+        inst = np.zeros(capacity, np.uint32)
+        o = f32(*origin)
+        d = f32(*direction)
+        n = lib().orc_brute_f64(self.handle, _p(o), _p(d), float(limit), _p(t), _p(tri), _p(inst), capacity)
+        n = min(int(n), capacity)
+        return t[:n], tri[:n], inst[:n]
+
+    def close(self):
+        if self.handle:
+            lib().orc_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class OracleFrame:
+    def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0):
+        self.settings = settings_c
+        pos = np.ascontiguousarray(pos, np.float32)
+        nrm = np.ascontiguousarray(nrm, np.float32)
+        self.handle = lib().orc_frame_run(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
+                                          threads or os.cpu_count() or 1)
+
+    def level(self, level: int, dirs: int):
+        cells = lib().orc_frame_cells(self.handle, level)
+        keys = np.zeros((cells, 4), np.int32)
+        merged = np.zeros((cells, dirs, 4), np.float32)
+        raw = np.zeros((cells, dirs, 4), np.float32)
+        samples = np.zeros((cells, dirs), np.uint32)
+        if cells:
+            lib().orc_frame_read_level(self.handle, level, _p(keys), _p(merged), _p(raw), _p(samples))
+        return keys, merged, raw, samples
+
+    def probes(self):
+        cells = lib().orc_frame_cells(self.handle, 0)
+        tables = np.zeros((cells, 36, 4), np.float32)
+        if cells:
+            lib().orc_frame_read_probes(self.handle, _p(tables))
+        return tables
+
+    def stats(self):
+        from bevy_penumbra_b200._native import LuxStats
+        st = LuxStats()
+        lib().orc_frame_stats(self.handle, C.byref(st))
+        return st
+
+    def resolve(self, pos: np.ndarray, nrm: np.ndarray) -> np.ndarray:
+        pos = np.ascontiguousarray(pos, np.float32)
+        nrm = np.ascontiguousarray(nrm, np.float32)
+        out = np.zeros((len(pos), 4), np.float32)
+        lib().orc_frame_resolve(self.handle, _p(pos), _p(nrm), len(pos), _p(out))
+        return out
+
+    def close(self):
+        if self.handle:
+            lib().orc_frame_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

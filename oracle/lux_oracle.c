@@ -1,0 +1,1913 @@
+/*
+ * lux_oracle.c - CPU restatement of bevy_lux's Split transport path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see lux_oracle.h).  Build: oracle/Makefile
+ * (gcc -O2 -ffp-contract=off -fno-fast-math): every floating-point expression
+ * below is evaluated in IEEE single precision in the order written, without
+ * contraction, which is the evaluation contract liblux's kernels follow too
+ * (nvcc --fmad=false).  Citations are paths inside the reference project.
+ */
+#define _GNU_SOURCE
+#include "lux_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define EMPTY 0xffffffffu
+#define MAX_TRAVERSAL_STEPS 4096u   /* shaders/traversal.slang:8 */
+#define MAX_LEAF_TRIANGLES 256u     /* shaders/traversal.slang:9 */
+#define MAX_LEAF_INSTANCES 4096u    /* shaders/traversal.slang:10 */
+#define HIT_QUERY_UNSUPPORTED 4u    /* shaders/traversal.slang:16 */
+#define STACK 49u                   /* shaders/traversal.slang:490, :712 */
+#define PI_F 3.14159265358979323846f
+
+static inline float saturatef(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+static inline float fracf(float x) { return x - floorf(x); }
+static inline float asf(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+static inline uint32_t asu(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline int finite3(const float v[3]) { return isfinite(v[0]) && isfinite(v[1]) && isfinite(v[2]); }
+static inline float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static inline void cross3(const float a[3], const float b[3], float o[3]) {
+    float x = a[1] * b[2] - a[2] * b[1];
+    float y = a[2] * b[0] - a[0] * b[2];
+    float z = a[0] * b[1] - a[1] * b[0];
+    o[0] = x; o[1] = y; o[2] = z;
+}
+static inline float length3(const float v[3]) { return sqrtf(dot3(v, v)); }
+
+/* ======================================================================
+ * Direction and key math (shaders/common.slang)
+ * ==================================================================== */
+
+/* cos and sin of 2*pi*turns.  The reference calls the GPU's cos/sin on
+ * phi = uv.x * 2 * PI (decodeDirection, shaders/common.slang:376-382).  The
+ * restatement reduces exactly to the nearest quarter turn and evaluates the
+ * Taylor series of sin(2 pi r) and cos(2 pi r), |r| <= 1/8, to degree 11/10
+ * (truncation error < 3e-8), so CPU and GPU agree bit for bit. */
+#define SC_S1 6.2831855f
+#define SC_S3 41.3417f
+#define SC_S5 81.60525f
+#define SC_S7 76.70586f
+#define SC_S9 42.058693f
+#define SC_S11 15.094643f
+#define SC_C2 19.739208f
+#define SC_C4 64.93939f
+#define SC_C6 85.45682f
+#define SC_C8 60.24464f
+#define SC_C10 26.426256f
+void orc_sincos_turns(float turns, float *c, float *s) {
+    float k = floorf(turns * 4.0f + 0.5f);
+    float r = turns - k * 0.25f;
+    int q = ((int)k) & 3;
+    float r2 = r * r;
+    float sp = SC_S9 - r2 * SC_S11;
+    sp = SC_S7 - r2 * sp;
+    sp = SC_S5 - r2 * sp;
+    sp = SC_S3 - r2 * sp;
+    sp = SC_S1 - r2 * sp;
+    float sn = r * sp;
+    float cp = SC_C8 - r2 * SC_C10;
+    cp = SC_C6 - r2 * cp;
+    cp = SC_C4 - r2 * cp;
+    cp = SC_C2 - r2 * cp;
+    float cs = 1.0f - r2 * cp;
+    switch (q) {
+    case 0: *c = cs; *s = sn; break;
+    case 1: *c = -sn; *s = cs; break;
+    case 2: *c = -cs; *s = -sn; break;
+    default: *c = sn; *s = -cs; break;
+    }
+}
+
+/* decodeDirection, shaders/common.slang:376-382 (+Y is the polar axis). */
+void orc_decode_direction(float u, float v, float out[3]) {
+    float y = v * 2.0f - 1.0f;
+    float r = sqrtf(fmaxf(0.0f, 1.0f - y * y));
+    float c, s;
+    orc_sincos_turns(u, &c, &s);
+    out[0] = r * c;
+    out[1] = y;
+    out[2] = r * s;
+}
+
+/* binDirection, shaders/common.slang:395-400, for a columns x rows grid. */
+void orc_bin_direction(uint32_t index, uint32_t columns, uint32_t rows, float out[3]) {
+    float u = ((float)(index % columns) + 0.5f) / (float)columns;
+    float v = ((float)(index / columns) + 0.5f) / (float)rows;
+    orc_decode_direction(u, v, out);
+}
+
+/* directionIndex, shaders/common.slang:388-394, applied to the (u, v) that
+ * encodeDirection returns for a direction decoded from (u, v). */
+uint32_t orc_direction_index_uv(float u, float v, uint32_t columns, uint32_t rows) {
+    uint32_t x = (uint32_t)(u * (float)columns);
+    uint32_t y = (uint32_t)(v * (float)rows);
+    if (x > columns - 1u) x = columns - 1u;
+    if (y > rows - 1u) y = rows - 1u;
+    return x + y * columns;
+}
+
+/* r2, shaders/common.slang:401-406. */
+void orc_r2(uint32_t index, float out[2]) {
+    uint32_t px = index * 3242174889u;
+    uint32_t py = index * 2447445414u;
+    out[0] = (float)(px >> 8) / 16777216.0f;
+    out[1] = (float)(py >> 8) / 16777216.0f;
+}
+
+/* transportHash, shaders/common.slang:281-289. */
+uint32_t orc_transport_hash(uint32_t value) {
+    value ^= value >> 16;
+    value *= 0x7feb352du;
+    value ^= value >> 15;
+    value *= 0x846ca68bu;
+    value ^= value >> 16;
+    return value;
+}
+
+/* hashKey, shaders/common.slang:423-429. */
+uint32_t orc_hash_key(const int32_t key[4], uint32_t bucket_count) {
+    uint32_t h = (uint32_t)key[0] * 0x8da6b343u ^ (uint32_t)key[1] * 0xd8163841u ^
+                 (uint32_t)key[2] * 0xcb1ab31fu ^ (uint32_t)key[3] * 0x165667b1u;
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    return h & (bucket_count - 1u);
+}
+
+/* rayOffset, shaders/common.slang:343-359. */
+void orc_ray_offset(const float position[3], const float normal[3], float bias, float out[3]) {
+    for (int i = 0; i < 3; ++i) {
+        float origin = position[i] + normal[i] * bias;
+        int32_t step = (int32_t)(normal[i] * 256.0f);
+        int32_t bits;
+        memcpy(&bits, &origin, 4);
+        int32_t moved = bits + (origin < 0.0f ? -step : step);
+        float integer_offset;
+        memcpy(&integer_offset, &moved, 4);
+        float shifted = fabsf(origin) < 0.03125f ? origin + normal[i] / 65536.0f : integer_offset;
+        out[i] = isfinite(shifted) ? shifted : position[i];
+    }
+}
+
+/* encodeNormal, shaders/common.slang:360-366. */
+void orc_encode_normal(const float n_in[3], float out[2]) {
+    float d = (fabsf(n_in[0]) + fabsf(n_in[1])) + fabsf(n_in[2]);
+    float n[3] = {n_in[0] / d, n_in[1] / d, n_in[2] / d};
+    float p[2] = {n[0], n[1]};
+    if (n[2] < 0.0f) {
+        float px = (1.0f - fabsf(n[1])) * (p[0] >= 0.0f ? 1.0f : -1.0f);
+        float py = (1.0f - fabsf(n[0])) * (p[1] >= 0.0f ? 1.0f : -1.0f);
+        p[0] = px;
+        p[1] = py;
+    }
+    out[0] = p[0] * 0.5f + 0.5f;
+    out[1] = p[1] * 0.5f + 0.5f;
+}
+
+/* decodeNormal, shaders/common.slang:367-374 (normalize = v / length(v)). */
+void orc_decode_normal(const float p_in[2], float out[3]) {
+    float p[2] = {p_in[0] * 2.0f - 1.0f, p_in[1] * 2.0f - 1.0f};
+    float n[3] = {p[0], p[1], (1.0f - fabsf(p[0])) - fabsf(p[1])};
+    float t = saturatef(-n[2]);
+    n[0] = n[0] + (n[0] >= 0.0f ? -t : t);
+    n[1] = n[1] + (n[1] >= 0.0f ? -t : t);
+    float l = length3(n);
+    out[0] = n[0] / l;
+    out[1] = n[1] / l;
+    out[2] = n[2] / l;
+}
+
+/* splitIntervalEnd, shaders/split.slang:224-227, with the growth ratio and
+ * rule as parameters (reference: end_L = length * 4^L). */
+float orc_interval_end(const LuxSettings *s, uint32_t level) {
+    if (s->interval_rule == LUX_INTERVAL_LENGTHS_GEOMETRIC) {
+        float sum = 0.0f, term = 1.0f;
+        for (uint32_t k = 0; k <= level; ++k) {
+            sum += term;
+            term *= s->interval_ratio;
+        }
+        return s->interval_length * sum;
+    }
+    float scale = 1.0f;
+    for (uint32_t k = 0; k < level; ++k) scale *= s->interval_ratio;
+    return s->interval_length * scale;
+}
+
+static float interval_start(const LuxSettings *s, uint32_t level) {
+    return level == 0u ? 0.0f : orc_interval_end(s, level - 1u);
+}
+
+/* spacing, shaders/common.slang:413-416 (LOD 0). */
+float orc_spacing(const LuxSettings *s, uint32_t level) {
+    return s->probe_spacing * (float)(1u << level);
+}
+
+static inline uint32_t level_columns(const LuxSettings *s, uint32_t level) { return s->base_columns << level; }
+static inline uint32_t level_rows(const LuxSettings *s, uint32_t level) { return s->base_rows << level; }
+
+/* ======================================================================
+ * Scene words (src/scene.rs:809-823, :1025-1122, :2096-2117)
+ * ==================================================================== */
+struct OrcScene {
+    uint32_t *sw;
+    size_t sn;
+    uint32_t *gw;
+    size_t gn;
+    LuxLight *lights;
+    uint32_t light_count;
+    uint32_t conventional;
+};
+
+typedef struct { uint32_t x, y, z, w; } U4;
+
+/* sceneInlineWord / geometryInlineWord: clamped reads
+ * (shaders/traversal.slang:58-62, :114-118). */
+static inline U4 sword(const OrcScene *S, uint32_t index) {
+    U4 r = {0, 0, 0, 0};
+    if (S->sn == 0) return r;
+    if (index > S->sn - 1) index = (uint32_t)(S->sn - 1);
+    memcpy(&r, S->sw + 4 * (size_t)index, 16);
+    return r;
+}
+static inline U4 gword(const OrcScene *S, uint32_t index) {
+    U4 r = {0, 0, 0, 0};
+    if (S->gn == 0) return r;
+    if (index > S->gn - 1) index = (uint32_t)(S->gn - 1);
+    memcpy(&r, S->gw + 4 * (size_t)index, 16);
+    return r;
+}
+
+OrcScene *orc_scene_create(const uint32_t *scene_words, size_t scene_word_count,
+                           const uint32_t *geometry_words, size_t geometry_word_count,
+                           const LuxLight *lights, uint32_t light_count, uint32_t conventional) {
+    OrcScene *S = (OrcScene *)calloc(1, sizeof(OrcScene));
+    S->sn = scene_word_count;
+    S->gn = geometry_word_count;
+    S->sw = (uint32_t *)malloc(16 * (scene_word_count ? scene_word_count : 1));
+    S->gw = (uint32_t *)malloc(16 * (geometry_word_count ? geometry_word_count : 1));
+    if (scene_word_count) memcpy(S->sw, scene_words, 16 * scene_word_count);
+    if (geometry_word_count) memcpy(S->gw, geometry_words, 16 * geometry_word_count);
+    S->light_count = light_count;
+    S->conventional = conventional;
+    S->lights = (LuxLight *)malloc(sizeof(LuxLight) * (light_count ? light_count : 1));
+    if (light_count) memcpy(S->lights, lights, sizeof(LuxLight) * light_count);
+    return S;
+}
+
+void orc_scene_destroy(OrcScene *S) {
+    if (!S) return;
+    free(S->sw);
+    free(S->gw);
+    free(S->lights);
+    free(S);
+}
+
+typedef struct { float mn[3]; uint32_t first; float mx[3]; uint32_t count; } Node;
+
+/* sceneNode, shaders/traversal.slang:192-196. */
+static inline Node scene_node(const OrcScene *S, uint32_t index) {
+    U4 a = sword(S, 1 + index * 2), b = sword(S, 2 + index * 2);
+    Node n;
+    n.mn[0] = asf(a.x); n.mn[1] = asf(a.y); n.mn[2] = asf(a.z); n.first = a.w;
+    n.mx[0] = asf(b.x); n.mx[1] = asf(b.y); n.mx[2] = asf(b.z); n.count = b.w;
+    return n;
+}
+static inline uint32_t instance_count(const OrcScene *S) { return sword(S, 0).z; }
+/* instanceBase, shaders/traversal.slang:197-201. */
+static inline uint32_t instance_base(const OrcScene *S, uint32_t instance) {
+    U4 h = sword(S, 0);
+    return h.y + instance * h.w;
+}
+
+/* localTriangle, shaders/traversal.slang:158-173. */
+static void local_triangle(const OrcScene *S, uint32_t triangle, U4 header, float a[3], float b[3],
+                           float c[3], uint32_t idx[3]) {
+    U4 t = gword(S, header.x + triangle);
+    idx[0] = t.x; idx[1] = t.y; idx[2] = t.z;
+    U4 va = gword(S, header.y + t.x * header.z);
+    U4 vb = gword(S, header.y + t.y * header.z);
+    U4 vc = gword(S, header.y + t.z * header.z);
+    a[0] = asf(va.x); a[1] = asf(va.y); a[2] = asf(va.z);
+    b[0] = asf(vb.x); b[1] = asf(vb.y); b[2] = asf(vb.z);
+    c[0] = asf(vc.x); c[1] = asf(vc.y); c[2] = asf(vc.z);
+}
+
+/* ======================================================================
+ * Traversal (shaders/traversal.slang)
+ * ==================================================================== */
+
+/* boxRayInterval, shaders/traversal.slang:349-369. */
+static int box_interval(const float o[3], const float d[3], const Node *n, float limit, float *entry,
+                        float *exit) {
+    float near_t = 0.0f, far_t = limit;
+    for (int axis = 0; axis < 3; ++axis) {
+        if (d[axis] == 0.0f) {
+            if (o[axis] < n->mn[axis] || o[axis] > n->mx[axis]) {
+                *entry = 0.0f;
+                *exit = 0.0f;
+                return 0;
+            }
+        } else {
+            float a = (n->mn[axis] - o[axis]) / d[axis];
+            float b = (n->mx[axis] - o[axis]) / d[axis];
+            float axis_exit = fmaxf(a, b);
+            near_t = fmaxf(near_t, fminf(a, b));
+            far_t = fminf(far_t, axis_exit + fabsf(axis_exit) * 3.5762791e-7f);
+        }
+    }
+    *entry = near_t;
+    *exit = far_t;
+    return near_t <= far_t;
+}
+static inline float box_entry(const float o[3], const float d[3], const Node *n, float limit) {
+    float e, x;
+    return box_interval(o, d, n, limit, &e, &x) ? e : -1.0f;
+}
+
+/* orientedEdge, shaders/traversal.slang:379-392. */
+static inline float oriented_edge(const float a[2], const float b[2]) {
+    int reverse = a[0] > b[0] || (a[0] == b[0] && a[1] > b[1]);
+    const float *first = reverse ? b : a, *second = reverse ? a : b;
+    float pa = first[0] * second[1];
+    float pb = first[1] * second[0];
+    float edge = pa - pb;
+    float error = (fabsf(pa) + fabsf(pb)) * 2.3841858e-7f;
+    if (fabsf(edge) <= error) edge = 0.0f;
+    return reverse ? -edge : edge;
+}
+
+typedef struct { uint32_t kx, ky, kz; float sx, sy; int valid; } TriRay;
+
+/* triangleRay, shaders/traversal.slang:399-413. */
+static TriRay triangle_ray(const float d[3]) {
+    TriRay r;
+    memset(&r, 0, sizeof r);
+    float m[3] = {fabsf(d[0]), fabsf(d[1]), fabsf(d[2])};
+    r.kz = m[0] > m[1] ? (m[0] > m[2] ? 0 : 2) : (m[1] > m[2] ? 1 : 2);
+    r.valid = d[r.kz] != 0.0f;
+    if (!r.valid) return r;
+    r.kx = (r.kz + 1) % 3;
+    r.ky = (r.kx + 1) % 3;
+    if (d[r.kz] < 0.0f) {
+        uint32_t t = r.kx;
+        r.kx = r.ky;
+        r.ky = t;
+    }
+    r.sx = d[r.kx] / d[r.kz];
+    r.sy = d[r.ky] / d[r.kz];
+    return r;
+}
+
+/* intersectTriangle, shaders/traversal.slang:415-443.  Returns distance or
+ * -1; w1, w2 = barycentric y, z. */
+static float intersect_triangle(const float o[3], const float d[3], const TriRay *ray, const float A[3],
+                                const float B[3], const float C[3], float *w1, float *w2) {
+    if (!ray->valid) return -1.0f;
+    uint32_t kx = ray->kx, ky = ray->ky, kz = ray->kz;
+    float a[3] = {A[0] - o[0], A[1] - o[1], A[2] - o[2]};
+    float b[3] = {B[0] - o[0], B[1] - o[1], B[2] - o[2]};
+    float c[3] = {C[0] - o[0], C[1] - o[1], C[2] - o[2]};
+    float pa[2] = {a[kx] - ray->sx * a[kz], a[ky] - ray->sy * a[kz]};
+    float pb[2] = {b[kx] - ray->sx * b[kz], b[ky] - ray->sy * b[kz]};
+    float pc[2] = {c[kx] - ray->sx * c[kz], c[ky] - ray->sy * c[kz]};
+    float largest = fmaxf(fmaxf(fmaxf(fabsf(pa[0]), fabsf(pa[1])), fmaxf(fabsf(pb[0]), fabsf(pb[1]))),
+                          fmaxf(fabsf(pc[0]), fabsf(pc[1])));
+    if (largest == 0.0f || !isfinite(largest)) return -1.0f;
+    uint32_t exponent = (asu(largest) >> 23) & 255u;
+    if (exponent < 1u) exponent = 1u;
+    if (exponent > 253u) exponent = 253u;
+    float scale = asf((254u - exponent) << 23);
+    pa[0] *= scale; pa[1] *= scale;
+    pb[0] *= scale; pb[1] *= scale;
+    pc[0] *= scale; pc[1] *= scale;
+    float e0 = oriented_edge(pb, pc), e1 = oriented_edge(pc, pa), e2 = oriented_edge(pa, pb);
+    int any_neg = e0 < 0.0f || e1 < 0.0f || e2 < 0.0f;
+    int any_pos = e0 > 0.0f || e1 > 0.0f || e2 > 0.0f;
+    if (any_neg && any_pos) return -1.0f;
+    float det = (e0 + e1) + e2;
+    if (det == 0.0f || !isfinite(det)) return -1.0f;
+    float wx = e0 / det, wy = e1 / det, wz = e2 / det;
+    float dist = ((wx * a[kz] + wy * b[kz]) + wz * c[kz]) / d[kz];
+    if (!isfinite(dist)) return -1.0f;
+    *w1 = wy;
+    *w2 = wz;
+    return dist;
+}
+
+/* Deterministic closest-hit order: smaller distance, then (instance,
+ * triangle).  The reference keeps the first of equal distances found by its
+ * depth-first order (strict `<`, shaders/traversal.slang:457); an explicit
+ * key makes the answer independent of the BVH shape. */
+static inline int hit_better(float t, uint32_t instance, uint32_t triangle, const LuxHit *h) {
+    if (t < h->distance) return 1;
+    if (t > h->distance || h->triangle == EMPTY) return 0;
+    if (instance != h->instance) return instance < h->instance;
+    return triangle < h->triangle;
+}
+
+static inline int cull_reject(uint32_t flags, const float A[3], const float B[3], const float C[3],
+                              const float d[3]) {
+    if ((flags & 3u) == 0u) return 0;
+    float e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+    float e2[3] = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+    float cr[3];
+    cross3(e1, e2, cr);
+    float facing = dot3(cr, d) * ((flags & 4u) != 0u ? -1.0f : 1.0f);
+    return ((flags & 1u) != 0u && facing >= 0.0f) || ((flags & 2u) != 0u && facing <= 0.0f);
+}
+
+/* traceTriangle, shaders/traversal.slang:445-473 (opaque materials). */
+static void trace_triangle(const OrcScene *S, const float lo[3], const float ld[3], const TriRay *ray,
+                           uint32_t tri, uint32_t instance, uint32_t flags, U4 header, float tmin,
+                           LuxHit *hit, OrcCounters *cn) {
+    float A[3], B[3], C[3];
+    uint32_t idx[3];
+    local_triangle(S, tri, header, A, B, C, idx);
+    if (cn) cn->triangles++;
+    if (cull_reject(flags, A, B, C, ld)) return;
+    float w1 = 0, w2 = 0;
+    float t = intersect_triangle(lo, ld, ray, A, B, C, &w1, &w2);
+    if (t > 0.000025f && t > tmin && hit_better(t, instance, tri, hit)) {
+        hit->distance = t;
+        hit->triangle = tri;
+        hit->instance = instance;
+        hit->barycentric[0] = (1.0f - w1) - w2;
+        hit->barycentric[1] = w1;
+        hit->barycentric[2] = w2;
+    }
+}
+
+/* Local ray of an instance: rows 0-2 of the record (local_from_world),
+ * shaders/traversal.slang:481-488. */
+static void local_ray(const OrcScene *S, uint32_t base, const float o[3], const float d[3], float lo[3],
+                      float ld[3]) {
+    for (int r = 0; r < 3; ++r) {
+        U4 w = sword(S, base + (uint32_t)r);
+        float x = asf(w.x), y = asf(w.y), z = asf(w.z), t = asf(w.w);
+        lo[r] = ((x * o[0] + y * o[1]) + z * o[2]) + t * 1.0f;
+        ld[r] = ((x * d[0] + y * d[1]) + z * d[2]) + t * 0.0f;
+    }
+}
+
+/* traceInstance, shaders/traversal.slang:474-566 (closest hit). */
+static void trace_instance(const OrcScene *S, const float o[3], const float d[3], uint32_t instance,
+                           U4 header, float tmin, LuxHit *hit, OrcCounters *cn) {
+    uint32_t base = instance_base(S, instance);
+    U4 record = sword(S, base + 6);
+    float lo[3], ld[3];
+    local_ray(S, base, o, d, lo, ld);
+    if (cn) cn->instances++;
+    uint32_t flags = record.w;
+    uint32_t stack_node[STACK];
+    float stack_t[STACK];
+    uint32_t count = 0;
+    U4 geometry = sword(S, base + 8);
+    Node node = scene_node(S, geometry.x);
+    if (cn) cn->nodes++;
+    int ready = box_entry(lo, ld, &node, hit->distance) >= 0.0f;
+    TriRay ray;
+    memset(&ray, 0, sizeof ray);
+    if (ready) ray = triangle_ray(ld);
+    uint32_t steps = 0;
+    while (ready || count != 0) {
+        if (++steps > MAX_TRAVERSAL_STEPS) {
+            hit->errors |= HIT_QUERY_UNSUPPORTED;
+            break;
+        }
+        if (!ready) {
+            --count;
+            if (stack_t[count] > hit->distance) continue;
+            node = scene_node(S, stack_node[count]);
+        }
+        ready = 0;
+        if (node.count == 0) {
+            if (count + 2 > STACK) {
+                hit->errors |= 1u;
+                node.first = geometry.y;
+                node.count = geometry.z;
+                count = 0;
+            } else {
+                uint32_t li = node.first, ri = li + 1;
+                Node ln = scene_node(S, li), rn = scene_node(S, ri);
+                if (cn) cn->nodes += 2;
+                float le = box_entry(lo, ld, &ln, hit->distance);
+                float re = box_entry(lo, ld, &rn, hit->distance);
+                if (le >= 0.0f && re >= 0.0f) {
+                    if (le <= re) {
+                        stack_node[count] = ri; stack_t[count] = re; ++count;
+                        node = ln;
+                    } else {
+                        stack_node[count] = li; stack_t[count] = le; ++count;
+                        node = rn;
+                    }
+                    ready = 1;
+                } else if (le >= 0.0f) {
+                    node = ln;
+                    ready = 1;
+                } else if (re >= 0.0f) {
+                    node = rn;
+                    ready = 1;
+                }
+                continue;
+            }
+        }
+        uint32_t begin = node.first > geometry.y ? node.first : geometry.y;
+        uint32_t limit_tri = geometry.y + geometry.z;
+        uint32_t requested_end = node.first + node.count;
+        uint32_t end = requested_end < limit_tri ? requested_end : limit_tri;
+        int truncated = node.first < geometry.y || requested_end < node.first ||
+                        requested_end > limit_tri || node.count > MAX_LEAF_TRIANGLES;
+        uint32_t bounded = end < begin + MAX_LEAF_TRIANGLES ? end : begin + MAX_LEAF_TRIANGLES;
+        truncated = truncated || bounded < end;
+        if (truncated) hit->errors |= HIT_QUERY_UNSUPPORTED;
+        for (uint32_t i = begin; i < bounded; ++i)
+            trace_triangle(S, lo, ld, &ray, i, instance, flags, header, tmin, hit, cn);
+    }
+}
+
+/* traceRayTracked, shaders/traversal.slang:696-811 (software path, no
+ * admission budget).  `tmin` extends the reference: hits must also satisfy
+ * t > tmin (dense-layout intervals start there). */
+void orc_trace_closest(const OrcScene *S, const float o[3], const float d[3], float tmin, float limit,
+                       LuxHit *hit, OrcCounters *cn) {
+    memset(hit, 0, sizeof *hit);
+    hit->distance = limit;
+    hit->triangle = EMPTY;
+    hit->instance = EMPTY;
+    uint32_t instances = instance_count(S);
+    if (instances == 0) return;
+    uint32_t stack_node[STACK];
+    float stack_t[STACK];
+    uint32_t count = 0;
+    Node node = scene_node(S, 0);
+    if (cn) cn->nodes++;
+    float root_entry, root_exit;
+    if (!box_interval(o, d, &node, hit->distance, &root_entry, &root_exit)) return;
+    U4 header = gword(S, 0);
+    int ready = root_entry >= 0.0f;
+    uint32_t steps = 0;
+    while (ready || count != 0) {
+        if (++steps > MAX_TRAVERSAL_STEPS) {
+            hit->errors |= HIT_QUERY_UNSUPPORTED;
+            break;
+        }
+        if (!ready) {
+            --count;
+            if (stack_t[count] > hit->distance) continue;
+            node = scene_node(S, stack_node[count]);
+        }
+        ready = 0;
+        if (node.count == 0) {
+            if (count + 2 > STACK) {
+                hit->errors |= 2u;
+                node.first = 0;
+                node.count = instances;
+                count = 0;
+            } else {
+                uint32_t li = node.first, ri = li + 1;
+                Node ln = scene_node(S, li), rn = scene_node(S, ri);
+                if (cn) cn->nodes += 2;
+                float le = box_entry(o, d, &ln, hit->distance);
+                float re = box_entry(o, d, &rn, hit->distance);
+                if (le >= 0.0f && re >= 0.0f) {
+                    if (le <= re) {
+                        stack_node[count] = ri; stack_t[count] = re; ++count;
+                        node = ln;
+                    } else {
+                        stack_node[count] = li; stack_t[count] = le; ++count;
+                        node = rn;
+                    }
+                    ready = 1;
+                } else if (le >= 0.0f) {
+                    node = ln;
+                    ready = 1;
+                } else if (re >= 0.0f) {
+                    node = rn;
+                    ready = 1;
+                }
+                continue;
+            }
+        }
+        uint32_t requested_end = node.first + node.count;
+        int truncated = requested_end < node.first || node.first > instances || requested_end > instances ||
+                        node.count > MAX_LEAF_INSTANCES;
+        uint32_t begin = node.first < instances ? node.first : instances;
+        uint32_t end = requested_end < instances ? requested_end : instances;
+        uint32_t bounded = end < begin + MAX_LEAF_INSTANCES ? end : begin + MAX_LEAF_INSTANCES;
+        truncated = truncated || bounded < end;
+        if (truncated) hit->errors |= HIT_QUERY_UNSUPPORTED;
+        for (uint32_t i = begin; i < bounded; ++i) trace_instance(S, o, d, i, header, tmin, hit, cn);
+    }
+}
+
+/* occludedTriangle, shaders/traversal.slang:826-843 (opaque materials). */
+static int occluded_triangle(const OrcScene *S, const float lo[3], const float ld[3], const TriRay *ray,
+                             uint32_t tri, uint32_t flags, float limit, U4 header, OrcCounters *cn) {
+    float A[3], B[3], C[3];
+    uint32_t idx[3];
+    local_triangle(S, tri, header, A, B, C, idx);
+    if (cn) cn->triangles++;
+    if (cull_reject(flags, A, B, C, ld)) return 0;
+    float w1, w2;
+    float t = intersect_triangle(lo, ld, ray, A, B, C, &w1, &w2);
+    return t > 0.000025f && t < limit;
+}
+
+/* occludedInstance, shaders/traversal.slang:845-932. */
+static int occluded_instance(const OrcScene *S, const float o[3], const float d[3], uint32_t instance,
+                             float limit, U4 header, int *supported, OrcCounters *cn) {
+    *supported = 1;
+    uint32_t base = instance_base(S, instance);
+    U4 record = sword(S, base + 6);
+    float lo[3], ld[3];
+    local_ray(S, base, o, d, lo, ld);
+    if (cn) cn->instances++;
+    uint32_t flags = record.w;
+    uint32_t stack_node[STACK];
+    uint32_t count = 0;
+    U4 geometry = sword(S, base + 8);
+    Node node = scene_node(S, geometry.x);
+    if (cn) cn->nodes++;
+    int ready = box_entry(lo, ld, &node, limit) >= 0.0f;
+    TriRay ray;
+    memset(&ray, 0, sizeof ray);
+    if (ready) ray = triangle_ray(ld);
+    uint32_t steps = 0;
+    int incomplete = 0;
+    while (ready || count != 0) {
+        if (++steps > MAX_TRAVERSAL_STEPS) {
+            *supported = 0;
+            return 0;
+        }
+        if (!ready) node = scene_node(S, stack_node[--count]);
+        ready = 0;
+        if (node.count == 0) {
+            if (count + 2 > STACK) {
+                node.first = geometry.y;
+                node.count = geometry.z;
+                count = 0;
+            } else {
+                uint32_t li = node.first, ri = li + 1;
+                Node ln = scene_node(S, li), rn = scene_node(S, ri);
+                if (cn) cn->nodes += 2;
+                float le = box_entry(lo, ld, &ln, limit);
+                float re = box_entry(lo, ld, &rn, limit);
+                if (le >= 0.0f && re >= 0.0f) {
+                    if (le <= re) {
+                        stack_node[count++] = ri;
+                        node = ln;
+                    } else {
+                        stack_node[count++] = li;
+                        node = rn;
+                    }
+                    ready = 1;
+                } else if (le >= 0.0f) {
+                    node = ln;
+                    ready = 1;
+                } else if (re >= 0.0f) {
+                    node = rn;
+                    ready = 1;
+                }
+                continue;
+            }
+        }
+        uint32_t begin = node.first > geometry.y ? node.first : geometry.y;
+        uint32_t limit_tri = geometry.y + geometry.z;
+        uint32_t requested_end = node.first + node.count;
+        uint32_t end = requested_end < limit_tri ? requested_end : limit_tri;
+        int truncated = node.first < geometry.y || requested_end < node.first ||
+                        requested_end > limit_tri || node.count > MAX_LEAF_TRIANGLES;
+        uint32_t bounded = end < begin + MAX_LEAF_TRIANGLES ? end : begin + MAX_LEAF_TRIANGLES;
+        truncated = truncated || bounded < end;
+        incomplete = incomplete || truncated;
+        for (uint32_t i = begin; i < bounded; ++i)
+            if (occluded_triangle(S, lo, ld, &ray, i, flags, limit, header, cn)) return 1;
+    }
+    *supported = !incomplete;
+    return 0;
+}
+
+/* traceOccluded, shaders/traversal.slang:955-1046. */
+int orc_trace_occluded(const OrcScene *S, const float o[3], const float d[3], float limit, int *supported,
+                       OrcCounters *cn) {
+    *supported = 1;
+    uint32_t instances = instance_count(S);
+    if (instances == 0) return 0;
+    uint32_t stack_node[STACK];
+    uint32_t count = 0;
+    Node node = scene_node(S, 0);
+    if (cn) cn->nodes++;
+    float root_entry, root_exit;
+    int intersects = box_interval(o, d, &node, limit, &root_entry, &root_exit);
+    int ready = intersects && root_entry >= 0.0f;
+    if (!ready) return 0;
+    U4 header = gword(S, 0);
+    uint32_t steps = 0;
+    int incomplete = 0;
+    while (ready || count != 0) {
+        if (++steps > MAX_TRAVERSAL_STEPS) {
+            *supported = 0;
+            return 0;
+        }
+        if (!ready) node = scene_node(S, stack_node[--count]);
+        ready = 0;
+        if (node.count == 0) {
+            if (count + 2 > STACK) {
+                node.first = 0;
+                node.count = instances;
+                count = 0;
+            } else {
+                uint32_t li = node.first, ri = li + 1;
+                Node ln = scene_node(S, li), rn = scene_node(S, ri);
+                if (cn) cn->nodes += 2;
+                float le = box_entry(o, d, &ln, limit);
+                float re = box_entry(o, d, &rn, limit);
+                if (le >= 0.0f && re >= 0.0f) {
+                    if (le <= re) {
+                        stack_node[count++] = ri;
+                        node = ln;
+                    } else {
+                        stack_node[count++] = li;
+                        node = rn;
+                    }
+                    ready = 1;
+                } else if (le >= 0.0f) {
+                    node = ln;
+                    ready = 1;
+                } else if (re >= 0.0f) {
+                    node = rn;
+                    ready = 1;
+                }
+                continue;
+            }
+        }
+        uint32_t requested_end = node.first + node.count;
+        int truncated = requested_end < node.first || node.first > instances || requested_end > instances ||
+                        node.count > MAX_LEAF_INSTANCES;
+        uint32_t begin = node.first < instances ? node.first : instances;
+        uint32_t end = requested_end < instances ? requested_end : instances;
+        uint32_t bounded = end < begin + MAX_LEAF_INSTANCES ? end : begin + MAX_LEAF_INSTANCES;
+        incomplete = incomplete || truncated || bounded < end;
+        for (uint32_t i = begin; i < bounded; ++i) {
+            int inst_supported;
+            int blocked = occluded_instance(S, o, d, i, limit, header, &inst_supported, cn);
+            incomplete = incomplete || !inst_supported;
+            if (blocked) {
+                *supported = 1;
+                return 1;
+            }
+        }
+    }
+    *supported = !incomplete;
+    return 0;
+}
+
+void orc_brute_closest(const OrcScene *S, const float o[3], const float d[3], float tmin, float limit,
+                       LuxHit *hit) {
+    memset(hit, 0, sizeof *hit);
+    hit->distance = limit;
+    hit->triangle = EMPTY;
+    hit->instance = EMPTY;
+    U4 header = gword(S, 0);
+    uint32_t instances = instance_count(S);
+    for (uint32_t inst = 0; inst < instances; ++inst) {
+        uint32_t base = instance_base(S, inst);
+        U4 record = sword(S, base + 6);
+        U4 geometry = sword(S, base + 8);
+        float lo[3], ld[3];
+        local_ray(S, base, o, d, lo, ld);
+        TriRay ray = triangle_ray(ld);
+        for (uint32_t tri = geometry.y; tri < geometry.y + geometry.z; ++tri)
+            trace_triangle(S, lo, ld, &ray, tri, inst, record.w, header, tmin, hit, NULL);
+    }
+}
+
+/* brute_force, src/traversal_tests.rs:978-1038 (Moller-Trumbore in world
+ * space, f64, componentwise f32 uncertainty band). */
+typedef struct { double t; uint32_t tri, inst; } F64Hit;
+static int f64_cmp(const void *a, const void *b) {
+    double x = ((const F64Hit *)a)->t, y = ((const F64Hit *)b)->t;
+    return x < y ? -1 : (x > y ? 1 : 0);
+}
+uint32_t orc_brute_f64(const OrcScene *S, const float o[3], const float d[3], float limit, double *t_out,
+                       uint32_t *tri_out, uint32_t *inst_out, uint32_t capacity) {
+    U4 header = gword(S, 0);
+    uint32_t instances = instance_count(S);
+    size_t cap = 64, n = 0;
+    F64Hit *hits = (F64Hit *)malloc(cap * sizeof(F64Hit));
+    const double eps = 8.0 * (double)FLT_EPSILON;
+    for (uint32_t inst = 0; inst < instances; ++inst) {
+        uint32_t base = instance_base(S, inst);
+        U4 record = sword(S, base + 6);
+        U4 geometry = sword(S, base + 8);
+        double m[3][4];
+        for (int r = 0; r < 3; ++r) {
+            U4 w = sword(S, base + 3 + (uint32_t)r);
+            m[r][0] = asf(w.x); m[r][1] = asf(w.y); m[r][2] = asf(w.z); m[r][3] = asf(w.w);
+        }
+        for (uint32_t tri = geometry.y; tri < geometry.y + geometry.z; ++tri) {
+            float A[3], B[3], C[3];
+            uint32_t idx[3];
+            local_triangle(S, tri, header, A, B, C, idx);
+            const float *lv[3] = {A, B, C};
+            double w[3][3];
+            for (int v = 0; v < 3; ++v)
+                for (int r = 0; r < 3; ++r)
+                    w[v][r] = m[r][0] * lv[v][0] + m[r][1] * lv[v][1] + m[r][2] * lv[v][2] + m[r][3];
+            double dir[3] = {d[0], d[1], d[2]}, org[3] = {o[0], o[1], o[2]};
+            double e1[3], e2[3], nrm[3], p[3], q[3], rel[3];
+            for (int k = 0; k < 3; ++k) {
+                e1[k] = w[1][k] - w[0][k];
+                e2[k] = w[2][k] - w[0][k];
+                rel[k] = org[k] - w[0][k];
+            }
+#define DCROSS(a, b, o_) do { o_[0] = a[1]*b[2]-a[2]*b[1]; o_[1] = a[2]*b[0]-a[0]*b[2]; o_[2] = a[0]*b[1]-a[1]*b[0]; } while (0)
+#define DDOT(a, b) (a[0]*b[0]+a[1]*b[1]+a[2]*b[2])
+            DCROSS(e1, e2, nrm);
+            double facing = DDOT(nrm, dir);
+            uint32_t cull = record.w & 3u;
+            if ((cull == 1 && facing >= 0.0) || (cull == 2 && facing <= 0.0)) continue;
+            DCROSS(dir, e2, p);
+            double det = DDOT(e1, p);
+            if (det == 0.0) continue;
+            double u = DDOT(rel, p) / det;
+            DCROSS(rel, e1, q);
+            double v = DDOT(dir, q) / det;
+            double t = DDOT(e2, q) / det;
+            double nl2 = DDOT(nrm, nrm);
+            double gu[3], gv[3];
+            DCROSS(e2, nrm, gu);
+            DCROSS(nrm, e1, gv);
+            for (int k = 0; k < 3; ++k) { gu[k] /= nl2; gv[k] /= nl2; }
+            double err[3];
+            for (int k = 0; k < 3; ++k)
+                err[k] = (fabs(org[k]) + fabs(dir[k]) * fabs(t) + fabs(w[0][k]) + fabs(w[1][k]) + fabs(w[2][k])) * eps;
+            double bu = fabs(gu[0]) * err[0] + fabs(gu[1]) * err[1] + fabs(gu[2]) * err[2];
+            double bv = fabs(gv[0]) * err[0] + fabs(gv[1]) * err[1] + fabs(gv[2]) * err[2];
+            double buv = fabs(gu[0] + gv[0]) * err[0] + fabs(gu[1] + gv[1]) * err[1] + fabs(gu[2] + gv[2]) * err[2];
+            if (u < -bu || v < -bv || u + v > 1.0 + buv) continue;
+            if (t > 0.000025 && t < (double)limit) {
+                if (n == cap) {
+                    cap *= 2;
+                    hits = (F64Hit *)realloc(hits, cap * sizeof(F64Hit));
+                }
+                hits[n].t = t;
+                hits[n].tri = tri;
+                hits[n].inst = inst;
+                ++n;
+            }
+#undef DCROSS
+#undef DDOT
+        }
+    }
+    qsort(hits, n, sizeof(F64Hit), f64_cmp);
+    for (size_t i = 0; i < n && i < capacity; ++i) {
+        t_out[i] = hits[i].t;
+        tri_out[i] = hits[i].tri;
+        inst_out[i] = hits[i].inst;
+    }
+    free(hits);
+    return (uint32_t)n;
+}
+
+/* ---- threaded batch harness ---- */
+typedef struct {
+    const OrcScene *S;
+    const LuxRay *rays;
+    LuxHit *hits;
+    uint32_t begin, end;
+    int any_hit;
+    OrcCounters cn;
+} RayJob;
+
+static void *ray_job(void *arg) {
+    RayJob *j = (RayJob *)arg;
+    for (uint32_t i = j->begin; i < j->end; ++i) {
+        const LuxRay *r = &j->rays[i];
+        LuxHit *h = &j->hits[i];
+        if (j->any_hit) {
+            int supported;
+            int blocked = orc_trace_occluded(j->S, r->origin, r->direction, r->limit, &supported, &j->cn);
+            memset(h, 0, sizeof *h);
+            h->distance = r->limit;
+            h->triangle = blocked ? 0u : EMPTY;
+            h->instance = blocked ? 0u : EMPTY;
+            h->errors = supported ? 0u : HIT_QUERY_UNSUPPORTED;
+        } else {
+            orc_trace_closest(j->S, r->origin, r->direction, r->tmin, r->limit, h, &j->cn);
+        }
+    }
+    return NULL;
+}
+
+void orc_trace_rays(const OrcScene *S, const LuxRay *rays, uint32_t count, int any_hit, LuxHit *hits,
+                    int threads, OrcCounters *counters) {
+    if (threads < 1) threads = 1;
+    if ((uint32_t)threads > count) threads = count ? (int)count : 1;
+    RayJob *jobs = (RayJob *)calloc((size_t)threads, sizeof(RayJob));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int t = 0; t < threads; ++t) {
+        jobs[t].S = S;
+        jobs[t].rays = rays;
+        jobs[t].hits = hits;
+        jobs[t].any_hit = any_hit;
+        jobs[t].begin = (uint32_t)((uint64_t)count * t / threads);
+        jobs[t].end = (uint32_t)((uint64_t)count * (t + 1) / threads);
+        pthread_create(&tid[t], NULL, ray_job, &jobs[t]);
+    }
+    for (int t = 0; t < threads; ++t) {
+        pthread_join(tid[t], NULL);
+        if (counters) {
+            counters->nodes += jobs[t].cn.nodes;
+            counters->triangles += jobs[t].cn.triangles;
+            counters->instances += jobs[t].cn.instances;
+        }
+    }
+    free(jobs);
+    free(tid);
+}
+
+/* ======================================================================
+ * Hit shading (shaders/cascades.slang:57-268, shaders/traversal.slang:174-316)
+ * ==================================================================== */
+
+/* unitVector, shaders/traversal.slang:183-190. */
+static void unit_vector(const float v[3], const float fallback[3], float out[3]) {
+    float scale = fmaxf(fabsf(v[0]), fmaxf(fabsf(v[1]), fabsf(v[2])));
+    if (scale == 0.0f || !isfinite(scale)) {
+        out[0] = fallback[0]; out[1] = fallback[1]; out[2] = fallback[2];
+        return;
+    }
+    float div = fmaxf(scale * 0.25f, FLT_MIN);
+    float w[3] = {v[0] / div, v[1] / div, v[2] / div};
+    float l = length3(w);
+    out[0] = w[0] / l; out[1] = w[1] / l; out[2] = w[2] / l;
+}
+
+/* transformDirection, shaders/traversal.slang:229-244. */
+static void transform_direction(const OrcScene *S, uint32_t base, const float value[3], int transpose,
+                                float out[3]) {
+    float r[3][3];
+    for (int k = 0; k < 3; ++k) {
+        U4 w = sword(S, base + (uint32_t)k);
+        r[k][0] = asf(w.x); r[k][1] = asf(w.y); r[k][2] = asf(w.z);
+    }
+    float mag[3];
+    for (int k = 0; k < 3; ++k) mag[k] = fmaxf(fabsf(r[0][k]), fmaxf(fabsf(r[1][k]), fabsf(r[2][k])));
+    float scale = fmaxf(mag[0], fmaxf(mag[1], mag[2]));
+    if (scale == 0.0f) {
+        out[0] = out[1] = out[2] = 0.0f;
+        return;
+    }
+    scale = fmaxf(scale * 0.25f, FLT_MIN);
+    for (int k = 0; k < 3; ++k)
+        for (int c = 0; c < 3; ++c) r[k][c] = r[k][c] / scale;
+    static const float zero[3] = {0, 0, 0};
+    float v[3];
+    unit_vector(value, zero, v);
+    if (transpose) {
+        for (int c = 0; c < 3; ++c) out[c] = (r[0][c] * v[0] + r[1][c] * v[1]) + r[2][c] * v[2];
+    } else {
+        for (int k = 0; k < 3; ++k) out[k] = dot3(r[k], v);
+    }
+}
+
+/* triangleGeometricNormal, shaders/traversal.slang:250-253. */
+static void geometric_normal(const OrcScene *S, uint32_t base, uint32_t flags, const float A[3],
+                             const float B[3], const float C[3], float out[3]) {
+    float e1[3] = {B[0] - A[0], B[1] - A[1], B[2] - A[2]};
+    float e2[3] = {C[0] - A[0], C[1] - A[1], C[2] - A[2]};
+    float cr[3], t[3];
+    cross3(e1, e2, cr);
+    transform_direction(S, base, cr, 1, t);
+    static const float up[3] = {0.0f, 1.0f, 0.0f};
+    unit_vector(t, up, out);
+    float sign = (flags & 4u) != 0u ? -1.0f : 1.0f;
+    out[0] *= sign; out[1] *= sign; out[2] *= sign;
+}
+
+/* hitVertexAttribute, shaders/traversal.slang:174-182. */
+static void vertex_attribute(const OrcScene *S, U4 header, const uint32_t idx[3], const float bary[3],
+                             uint32_t attribute, float out[4]) {
+    float acc[4] = {0, 0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        U4 w = gword(S, header.y + idx[i] * header.z + attribute);
+        float v[4] = {asf(w.x), asf(w.y), asf(w.z), asf(w.w)};
+        for (int c = 0; c < 4; ++c) acc[c] = i == 0 ? v[c] * bary[i] : acc[c] + v[c] * bary[i];
+    }
+    memcpy(out, acc, sizeof acc);
+}
+
+typedef struct {
+    float base_color[3];
+    float emission[3];
+    float metallic, roughness;
+    uint32_t flags;
+} Surface;
+
+/* materialBaseColor / hitEmission (shaders/material.slang:139-141,
+ * shaders/traversal.slang:287-300) for untextured materials. */
+static void surface_at(const OrcScene *S, const LuxSettings *st, uint32_t instance, uint32_t triangle,
+                       const float bary[3], Surface *sf) {
+    uint32_t base = instance_base(S, instance);
+    uint32_t flags = sword(S, base + 6).w;
+    uint32_t material = sword(S, base + 7).w;
+    U4 m0 = sword(S, material), m1 = sword(S, material + 1), m2 = sword(S, material + 2);
+    U4 header = gword(S, 0);
+    U4 t = gword(S, header.x + triangle);
+    uint32_t idx[3] = {t.x, t.y, t.z};
+    float color[4];
+    vertex_attribute(S, header, idx, bary, 4, color);
+    sf->base_color[0] = asf(m0.x) * color[0];
+    sf->base_color[1] = asf(m0.y) * color[1];
+    sf->base_color[2] = asf(m0.z) * color[2];
+    if ((flags & 16u) != 0u) {
+        memcpy(sf->emission, sf->base_color, sizeof sf->emission);
+    } else {
+        sf->emission[0] = asf(m1.x);
+        sf->emission[1] = asf(m1.y);
+        sf->emission[2] = asf(m1.z);
+    }
+    float weight = (flags & 16u) != 0u ? 0.0f : asf(m2.w);
+    float exposure = fmaxf(st->exposure, 1e-20f);
+    float inv = 1.0f / exposure;
+    float factor = inv + weight * (1.0f - inv);
+    for (int c = 0; c < 3; ++c) sf->emission[c] = sf->emission[c] * factor;
+    sf->metallic = asf(m2.x);
+    sf->roughness = asf(m2.y);
+    sf->flags = flags;
+}
+
+/* disneyDiffuseMultiplier, shaders/common.slang:298-314 (rsqrt written as
+ * 1/sqrt, pow(x, 5) as bsdfPow5). */
+static float disney_multiplier(const float n[3], const float l[3], const float v[3], float pr) {
+    float ndl = saturatef(dot3(n, l));
+    float ndv = saturatef(dot3(n, v));
+    float h[3] = {l[0] + v[0], l[1] + v[1], l[2] + v[2]};
+    float hl2 = dot3(h, h);
+    if (ndl <= 0.0f || ndv <= 0.0f || hl2 <= 1e-20f) return 0.0f;
+    float hl = sqrtf(hl2);
+    float hv[3] = {h[0] / hl, h[1] / hl, h[2] / hl};
+    float rough = fmaxf(saturatef(pr), 0.089f);
+    rough = rough * rough;
+    float ldh = saturatef(dot3(l, hv));
+    float f90 = 0.5f + ((2.0f * rough) * ldh) * ldh;
+    float a = 1.0f - ndl, b = 1.0f - ndv;
+    float a2 = a * a, b2 = b * b;
+    float light_scatter = 1.0f + (f90 - 1.0f) * ((a2 * a2) * a);
+    float view_scatter = 1.0f + (f90 - 1.0f) * ((b2 * b2) * b);
+    return light_scatter * view_scatter;
+}
+
+/* emissiveResponseTracked, shaders/cascades.slang:57-134; the scattering
+ * response is the diffuse colour times the Disney diffuse factor / pi
+ * (shaders/environment.slang:2-6 non-full branch, times bsdfDiffuseColor). */
+static int emissive_response(const OrcScene *S, const LuxSettings *st, const float position[3],
+                             const float normal[3], const float gnormal[3], const float view[3],
+                             float roughness, const float diffuse[3], float out[3], uint64_t *shadow_rays,
+                             OrcCounters *cn) {
+    out[0] = out[1] = out[2] = 0.0f;
+    uint32_t emissive = S->light_count - S->conventional;
+    uint32_t count = st->emissive_samples / 2u;
+    if (count < 1u) count = 1u;
+    if (emissive == 0u) return 1;
+    float cell = st->probe_spacing * 0.05f;
+    int32_t k1[4] = {(int32_t)floorf(position[0] / cell), (int32_t)floorf(position[1] / cell),
+                     (int32_t)floorf(position[2] / cell), 0};
+    uint32_t seed = orc_hash_key(k1, 16777216u);
+    float rotation[2];
+    orc_r2(seed, rotation);
+    float s0 = orc_spacing(st, 0);
+    int32_t k2[4] = {(int32_t)floorf(position[0] / s0), (int32_t)floorf(position[1] / s0),
+                     (int32_t)floorf(position[2] / s0), 0};
+    uint32_t selection_seed = orc_hash_key(k2, 65536u);
+    uint32_t sample_frame = st->frame_index ^ 0xE11E0001u;
+    float ra[2], rb[2];
+    orc_r2(sample_frame, ra);
+    orc_r2(selection_seed, rb);
+    float phase = fracf(ra[0] + rb[0]);
+    float sum[3] = {0, 0, 0};
+    const float bias = st->normal_bias;
+    for (uint32_t sample = 0; sample < count; ++sample) {
+        float rr[2];
+        orc_r2(sample + sample_frame * count + 1u, rr);
+        float uv[2] = {fracf(rr[0] + rotation[0]), fracf(rr[1] + rotation[1])};
+        float selection = fracf(((float)sample + 0.5f) / (float)count + phase);
+        uint32_t low = 0, high = emissive - 1u;
+        while (low < high) {
+            uint32_t middle = (low + high) / 2u;
+            if (S->lights[S->conventional + middle].direction[3] < selection)
+                low = middle + 1u;
+            else
+                high = middle;
+        }
+        const LuxLight *L = &S->lights[S->conventional + low];
+        float rel[3] = {position[0] - L->position[0], position[1] - L->position[1], position[2] - L->position[2]};
+        if (L->edge1[3] <= 0.0f || (L->position[3] != -2.0f && dot3(L->direction, rel) <= 0.0f)) continue;
+        float root = sqrtf(uv[0]);
+        float w1 = root * (1.0f - uv[1]), w2 = root * uv[1];
+        float target[3];
+        for (int c = 0; c < 3; ++c) target[c] = (L->position[c] + L->edge1[c] * w1) + L->edge2[c] * w2;
+        float to_light[3] = {target[0] - position[0], target[1] - position[1], target[2] - position[2]};
+        float light_distance = length3(to_light);
+        if (light_distance <= bias * 0.25f) continue;
+        float ldir[3] = {to_light[0] / light_distance, to_light[1] / light_distance, to_light[2] / light_distance};
+        float cosine = fmaxf(0.0f, dot3(normal, ldir));
+        float neg[3] = {-ldir[0], -ldir[1], -ldir[2]};
+        float c_emit = dot3(L->direction, neg);
+        if (L->position[3] == -2.0f) c_emit = fabsf(c_emit);
+        float emitter_cosine = fmaxf(0.0f, c_emit);
+        if (cosine <= 0.0f || emitter_cosine <= 0.0f || dot3(gnormal, ldir) <= 0.0f) continue;
+        float bary[3] = {1.0f - root, w1, w2};
+        Surface es;
+        surface_at(S, st, L->source[0], L->source[1], bary, &es);
+        float emission[3] = {fmaxf(es.emission[0], 0.0f), fmaxf(es.emission[1], 0.0f), fmaxf(es.emission[2], 0.0f)};
+        if (!(emission[0] > 0.0f || emission[1] > 0.0f || emission[2] > 0.0f)) continue;
+        float pdf = ((L->edge1[3] * light_distance) * light_distance) / (L->color[3] * emitter_cosine);
+        float plane = fabsf(dot3(L->direction, rel));
+        float origin[3];
+        orc_ray_offset(position, gnormal, fminf(bias, plane * 0.25f), origin);
+        float delta[3] = {target[0] - origin[0], target[1] - origin[1], target[2] - origin[2]};
+        float distance = length3(delta);
+        if (distance <= bias * 0.25f) continue;
+        float dir[3] = {delta[0] / distance, delta[1] / distance, delta[2] / distance};
+        int supported;
+        if (shadow_rays) (*shadow_rays)++;
+        int blocked = orc_trace_occluded(S, origin, dir, distance - fminf(bias * 0.25f, distance * 0.001f),
+                                         &supported, cn);
+        if (!supported) {
+            out[0] = out[1] = out[2] = 0.0f;
+            return 0;
+        }
+        if (blocked) continue;
+        float factor = disney_multiplier(normal, ldir, view, roughness) / PI_F;
+        float p = fmaxf(pdf, 1e-20f);
+        for (int c = 0; c < 3; ++c) {
+            float response = diffuse[c] * factor;
+            sum[c] = sum[c] + emission[c] * ((response * cosine) / p);
+        }
+    }
+    for (int c = 0; c < 3; ++c) out[c] = sum[c] / (float)count;
+    return 1;
+}
+
+/* outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, with
+ * every active source group summed into one radiance (no environment, no
+ * conventional lights, no secondary cache: the synthetic-scene subset). */
+int orc_outgoing_radiance(const OrcScene *S, const LuxSettings *st, const float origin[3],
+                          const float direction[3], const LuxHit *hit, float out[3], uint64_t *shadow_rays,
+                          OrcCounters *cn) {
+    out[0] = out[1] = out[2] = 0.0f;
+    if ((hit->errors & HIT_QUERY_UNSUPPORTED) != 0u) return 0;
+    if (hit->triangle == EMPTY) return 1;
+    Surface sf;
+    surface_at(S, st, hit->instance, hit->triangle, hit->barycentric, &sf);
+    float radiance[3] = {sf.emission[0], sf.emission[1], sf.emission[2]};
+    if ((sf.flags & 16u) == 0u) {
+        uint32_t base = instance_base(S, hit->instance);
+        U4 header = gword(S, 0);
+        float A[3], B[3], C[3];
+        uint32_t idx[3];
+        local_triangle(S, hit->triangle, header, A, B, C, idx);
+        float position[3];
+        for (int c = 0; c < 3; ++c) position[c] = origin[c] + direction[c] * hit->distance;
+        float gn[3];
+        geometric_normal(S, base, sf.flags, A, B, C, gn);
+        /* hitAttributes world normal, shaders/traversal.slang:258-282. */
+        float world_normal[3] = {0, 0, 0};
+        for (int i = 0; i < 3; ++i) {
+            U4 vw = gword(S, header.y + idx[i] * header.z);
+            float nrm[3] = {gn[0], gn[1], gn[2]};
+            if ((vw.w & 1u) != 0u) {
+                U4 nw = gword(S, header.y + idx[i] * header.z + 1);
+                float vn[3] = {asf(nw.x), asf(nw.y), asf(nw.z)}, tn[3];
+                transform_direction(S, base, vn, 1, tn);
+                unit_vector(tn, gn, nrm);
+            }
+            for (int c = 0; c < 3; ++c) world_normal[c] = world_normal[c] + nrm[c] * hit->barycentric[i];
+        }
+        /* materialNormal without a normal texture, shaders/material.slang:171-177. */
+        float normal[3];
+        unit_vector(world_normal, gn, normal);
+        int back = dot3(gn, direction) > 0.0f;
+        if (back && (sf.flags & 8u) != 0u) {
+            normal[0] = -normal[0]; normal[1] = -normal[1]; normal[2] = -normal[2];
+        }
+        float flipped[3] = {gn[0], gn[1], gn[2]};
+        if (dot3(flipped, direction) > 0.0f) {
+            flipped[0] = -flipped[0]; flipped[1] = -flipped[1]; flipped[2] = -flipped[2];
+        }
+        float neg[3] = {-direction[0], -direction[1], -direction[2]};
+        if (!(dot3(normal, neg) <= 0.0f || dot3(normal, flipped) <= 0.0f)) {
+            float nl = length3(neg);
+            float view[3] = {neg[0] / nl, neg[1] / nl, neg[2] / nl};
+            float metallic = saturatef(sf.metallic);
+            float roughness = saturatef(sf.roughness);
+            if (!isfinite(roughness)) roughness = 1.0f;
+            float diffuse[3];
+            int base_finite = finite3(sf.base_color);
+            for (int c = 0; c < 3; ++c)
+                diffuse[c] = (base_finite ? saturatef(sf.base_color[c]) : 0.0f) * (1.0f - metallic);
+            float nee[3];
+            if (!emissive_response(S, st, position, normal, flipped, view, roughness, diffuse, nee, shadow_rays, cn)) {
+                out[0] = out[1] = out[2] = 0.0f;
+                return 0;
+            }
+            for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + nee[c];
+        }
+    }
+    /* clampOutgoingTransportRadiance, shaders/cascades.slang:179-188. */
+    if (!finite3(radiance)) return 1;
+    for (int c = 0; c < 3; ++c) out[c] = fmaxf(radiance[c], 0.0f);
+    return 1;
+}
+
+/* ======================================================================
+ * Cascade frame: deposit, reduce, merge, pack, resolve (shaders/split.slang,
+ * shaders/world_resolve.slang)
+ * ==================================================================== */
+typedef struct { int32_t k[4]; } Key;
+
+static int key_cmp(const void *a, const void *b) {
+    const int32_t *x = ((const Key *)a)->k, *y = ((const Key *)b)->k;
+    for (int i = 0; i < 3; ++i)
+        if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+    return 0;
+}
+
+typedef struct {
+    uint32_t cells, dirs, columns, rows;
+    Key *keys;
+    float *jsum;     /* float4: J sum rgb, non-terminating count */
+    uint32_t *count;
+    float *merged;   /* float4 */
+    float *raw;      /* float4 J mean, beta */
+} Level;
+
+struct OrcFrame {
+    LuxSettings st;
+    uint32_t levels;
+    Level level[LUX_MAX_LEVELS];
+    float *tables;  /* c0 cells * 36 float4 */
+    LuxStats stats;
+};
+
+static int64_t find_cell(const Level *L, const int32_t key[3]) {
+    int64_t lo = 0, hi = (int64_t)L->cells - 1;
+    while (lo <= hi) {
+        int64_t mid = (lo + hi) / 2;
+        const int32_t *m = L->keys[mid].k;
+        int c = 0;
+        for (int i = 0; i < 3 && c == 0; ++i)
+            if (m[i] != key[i]) c = m[i] < key[i] ? -1 : 1;
+        if (c == 0) return mid;
+        if (c < 0) lo = mid + 1;
+        else hi = mid - 1;
+    }
+    return -1;
+}
+
+/* cacheKey cell, shaders/common.slang:417-422 (LOD 0). */
+static void cell_key(const LuxSettings *st, uint32_t level, const float p[3], int32_t out[3]) {
+    float s = orc_spacing(st, level);
+    for (int i = 0; i < 3; ++i) out[i] = (int32_t)floorf(p[i] / s);
+}
+
+typedef struct {
+    const OrcScene *S;
+    const LuxSettings *st;
+    const float *pos, *nrm;
+    uint32_t n;
+    /* split: per ray outputs */
+    int32_t *term_level;  /* -1 = unsupported */
+    float *radiance;      /* rgb per ray */
+    uint32_t *ubin;       /* flipped (u, v) stored as bits */
+    float *uv;
+    /* dense */
+    Level *levels;
+    uint32_t level;
+    uint64_t begin, end;
+    uint64_t shadow;
+    OrcCounters cn;
+} FrameJob;
+
+static void split_ray(const OrcScene *S, const LuxSettings *st, const float p[3], const float n[3], uint32_t sequence,
+                      float uv_out[2], LuxHit *hit, float origin[3], float dir[3]) {
+    float jitter[2], r[2];
+    orc_r2(orc_transport_hash(st->frame_index ^ 0x5a17c9e3u), jitter);
+    orc_r2(sequence + 1u, r);
+    float u = fracf((0.5f + r[0]) + jitter[0]);
+    float v = fracf((0.5f + r[1]) + jitter[1]);
+    orc_decode_direction(u, v, dir);
+    if (dot3(dir, n) < 0.0f) {
+        dir[0] = -dir[0]; dir[1] = -dir[1]; dir[2] = -dir[2];
+        u = fracf(u + 0.5f);
+        v = 1.0f - v;
+    }
+    uv_out[0] = u;
+    uv_out[1] = v;
+    orc_ray_offset(p, n, st->normal_bias, origin);
+    (void)S;
+    (void)hit;
+}
+
+static void *split_job(void *arg) {
+    FrameJob *j = (FrameJob *)arg;
+    const LuxSettings *st = j->st;
+    uint32_t R = st->rays_per_receiver;
+    for (uint64_t ray = j->begin; ray < j->end; ++ray) {
+        uint32_t i = (uint32_t)(ray / R), k = (uint32_t)(ray % R);
+        const float *p = j->pos + 4 * (size_t)i, *n = j->nrm + 4 * (size_t)i;
+        float uv[2], origin[3], dir[3];
+        LuxHit hit;
+        split_ray(j->S, st, p, n, i * R + k, uv, &hit, origin, dir);
+        orc_trace_closest(j->S, origin, dir, 0.0f, 1e20f, &hit, &j->cn);
+        float rad[3];
+        int supported = orc_outgoing_radiance(j->S, st, origin, dir, &hit, rad, &j->shadow, &j->cn);
+        j->uv[2 * ray] = uv[0];
+        j->uv[2 * ray + 1] = uv[1];
+        memcpy(&j->radiance[3 * ray], rad, sizeof rad);
+        if (!supported || (hit.errors & HIT_QUERY_UNSUPPORTED)) {
+            j->term_level[ray] = -1;
+            continue;
+        }
+        int32_t term = (int32_t)st->levels - 1;
+        for (uint32_t l = 0; l + 1 < st->levels; ++l) {
+            if (hit.distance > interval_start(st, l) && hit.distance <= orc_interval_end(st, l)) {
+                term = (int32_t)l;
+                break;
+            }
+        }
+        j->term_level[ray] = term;
+    }
+    return NULL;
+}
+
+static void *dense_job(void *arg) {
+    FrameJob *j = (FrameJob *)arg;
+    const LuxSettings *st = j->st;
+    Level *L = &j->levels[j->level];
+    uint32_t l = j->level;
+    int terminal = l + 1 == st->levels;
+    float start = interval_start(st, l), end = orc_interval_end(st, l);
+    float limit = terminal ? 1e20f : nextafterf(end, INFINITY);
+    float sp = orc_spacing(st, l);
+    for (uint64_t e = j->begin; e < j->end; ++e) {
+        uint32_t cell = (uint32_t)(e / L->dirs), d = (uint32_t)(e % L->dirs);
+        float origin[3], dir[3];
+        for (int c = 0; c < 3; ++c) origin[c] = ((float)L->keys[cell].k[c] + 0.5f) * sp;
+        orc_bin_direction(d, L->columns, L->rows, dir);
+        LuxHit hit;
+        orc_trace_closest(j->S, origin, dir, start, limit, &hit, &j->cn);
+        float rad[3];
+        int supported = orc_outgoing_radiance(j->S, st, origin, dir, &hit, rad, &j->shadow, &j->cn);
+        if (!supported || (hit.errors & HIT_QUERY_UNSUPPORTED)) continue;
+        int terminates = terminal || hit.triangle != EMPTY;
+        float *js = &L->jsum[4 * e];
+        L->count[e] = 1;
+        if (terminates) {
+            js[0] = rad[0]; js[1] = rad[1]; js[2] = rad[2];
+        } else {
+            js[3] = 1.0f;
+        }
+    }
+    return NULL;
+}
+
+static void run_jobs(FrameJob *proto, uint64_t total, int threads, void *(*fn)(void *), uint64_t *shadow,
+                     OrcCounters *cn) {
+    if (threads < 1) threads = 1;
+    if ((uint64_t)threads > total) threads = total ? (int)total : 1;
+    FrameJob *jobs = (FrameJob *)calloc((size_t)threads, sizeof(FrameJob));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int t = 0; t < threads; ++t) {
+        jobs[t] = *proto;
+        jobs[t].begin = total * (uint64_t)t / (uint64_t)threads;
+        jobs[t].end = total * (uint64_t)(t + 1) / (uint64_t)threads;
+        pthread_create(&tid[t], NULL, fn, &jobs[t]);
+    }
+    for (int t = 0; t < threads; ++t) {
+        pthread_join(tid[t], NULL);
+        *shadow += jobs[t].shadow;
+        cn->nodes += jobs[t].cn.nodes;
+        cn->triangles += jobs[t].cn.triangles;
+        cn->instances += jobs[t].cn.instances;
+    }
+    free(jobs);
+    free(tid);
+}
+
+/* interpolateMergedChildSources, shaders/split.slang:389-479, one source
+ * group; corner_merged = float4[8] (w <= 0 or NaN: unsupported / missing). */
+void orc_interpolate_children(const float fraction[3], const float *corner_merged, float out[4]) {
+    float sum[3] = {0, 0, 0}, total = 0.0f, potential = 0.0f;
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        uint32_t bx = corner & 1u, by = (corner >> 1) & 1u, bz = corner >> 2;
+        float ax = bx == 0u ? 1.0f - fraction[0] : fraction[0];
+        float ay = by == 0u ? 1.0f - fraction[1] : fraction[1];
+        float az = bz == 0u ? 1.0f - fraction[2] : fraction[2];
+        float weight = (ax * ay) * az;
+        if (!(weight > 0.0f)) continue;
+        potential += weight;
+        const float *s = corner_merged + 4 * corner;
+        if (s[3] > 0.0f && isfinite(s[0]) && isfinite(s[1]) && isfinite(s[2]) && isfinite(s[3])) {
+            float sw = weight * saturatef(s[3]);
+            for (int c = 0; c < 3; ++c) sum[c] = sum[c] + s[c] * sw;
+            total += sw;
+        }
+    }
+    if (total > 0.0f) {
+        for (int c = 0; c < 3; ++c) out[c] = sum[c] / total;
+        out[3] = saturatef(total / fmaxf(potential, 1e-8f));
+    } else {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+    }
+}
+
+/* mergeEntry + mergeRadianceGroups + finishMergeGroup without history
+ * (shaders/split.slang:1523-1725): interval = (J.rgb, beta) of the reduced
+ * entry, child values = the 4 angular children already interpolated. */
+static void merge_values(const float interval[4], uint32_t samples, const float *children, int has_children,
+                         float out[4]) {
+    if (samples == 0u) {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+        return;
+    }
+    float transmittance = saturatef(interval[3]);
+    float support = 1.0f - transmittance;
+    float radiance[3] = {0, 0, 0};
+    if (support > 0.0f) {
+        radiance[0] = interval[0]; radiance[1] = interval[1]; radiance[2] = interval[2];
+    }
+    float child_sum[3] = {0, 0, 0}, child_support = 0.0f;
+    if (transmittance > 0.0f && has_children) {
+        for (int c = 0; c < 4; ++c) {
+            const float *v = children + 4 * c;
+            if (!(v[3] > 0.0f)) continue;
+            for (int k = 0; k < 3; ++k) child_sum[k] = child_sum[k] + v[k] * v[3];
+            child_support += v[3];
+        }
+    }
+    if (child_support > 0.0f) {
+        for (int k = 0; k < 3; ++k) radiance[k] = radiance[k] + (transmittance * child_sum[k]) * 0.25f;
+        support = support + (transmittance * child_support) * 0.25f;
+    }
+    if (support > 0.0f) {
+        for (int k = 0; k < 3; ++k) out[k] = radiance[k] / support;
+        out[3] = saturatef(support);
+    } else {
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+    }
+}
+
+void orc_merge_entry(const float interval[4], uint32_t samples, const float fraction[3], const float *child_merged,
+                     int has_children, float out[4]) {
+    float children[16];
+    for (int c = 0; c < 4; ++c) orc_interpolate_children(fraction, child_merged + 32 * c, children + 4 * c);
+    merge_values(interval, samples, children, has_children, out);
+}
+
+static void merge_level(OrcFrame *F, uint32_t l) {
+    const LuxSettings *st = &F->st;
+    Level *L = &F->level[l];
+    int has_children = l + 1 < F->levels;
+    Level *P = has_children ? &F->level[l + 1] : NULL;
+    float sp = orc_spacing(st, l);
+    float sp1 = has_children ? orc_spacing(st, l + 1) : 1.0f;
+    for (uint32_t cell = 0; cell < L->cells; ++cell) {
+        int64_t corner_cell[8];
+        float fraction[3];
+        if (has_children) {
+            int32_t base[3];
+            for (int c = 0; c < 3; ++c) {
+                float origin = ((float)L->keys[cell].k[c] + 0.5f) * sp;
+                float grid = origin / sp1 - 0.5f;
+                float fl = floorf(grid);
+                base[c] = (int32_t)fl;
+                fraction[c] = grid - fl;
+            }
+            for (uint32_t corner = 0; corner < 8u; ++corner) {
+                int32_t k[3] = {base[0] + (int32_t)(corner & 1u), base[1] + (int32_t)((corner >> 1) & 1u),
+                                base[2] + (int32_t)(corner >> 2)};
+                corner_cell[corner] = find_cell(P, k);
+            }
+        }
+        for (uint32_t d = 0; d < L->dirs; ++d) {
+            uint64_t e = (uint64_t)cell * L->dirs + d;
+            uint32_t n = L->count[e];
+            float interval[4] = {0, 0, 0, 0};
+            if (n) {
+                float fn = (float)n;
+                for (int c = 0; c < 4; ++c) interval[c] = L->jsum[4 * e + c] / fn;
+            }
+            memcpy(&L->raw[4 * e], interval, sizeof interval);
+            float children[16];
+            memset(children, 0, sizeof children);
+            if (has_children && n) {
+                uint32_t x = d % L->columns, y = d / L->columns;
+                for (uint32_t child = 0; child < 4u; ++child) {
+                    uint32_t fx = x * 2u + (child & 1u), fy = y * 2u + (child >> 1);
+                    uint32_t fine = fx + fy * P->columns;
+                    float corners[32];
+                    for (uint32_t corner = 0; corner < 8u; ++corner) {
+                        if (corner_cell[corner] < 0) {
+                            memset(corners + 4 * corner, 0, 16);
+                        } else {
+                            memcpy(corners + 4 * corner, &P->merged[4 * ((uint64_t)corner_cell[corner] * P->dirs + fine)], 16);
+                        }
+                    }
+                    orc_interpolate_children(fraction, corners, children + 4 * child);
+                }
+            }
+            merge_values(interval, n, children, has_children, &L->merged[4 * e]);
+        }
+    }
+}
+
+/* packProbes, shaders/split.slang:1786-1918 (one source group; D0 base
+ * directions with scale nominal * 4 / D0). */
+void orc_pack_table(const float *merged, uint32_t columns, uint32_t rows, float *table) {
+    uint32_t dirs = columns * rows;
+    float *dir = (float *)malloc(sizeof(float) * 3 * dirs);
+    float *val = (float *)malloc(sizeof(float) * 4 * dirs);
+    for (uint32_t d = 0; d < dirs; ++d) {
+        orc_bin_direction(d, columns, rows, dir + 3 * d);
+        const float *m = merged + 4 * d;
+        int ok = m[3] > 0.0f && isfinite(m[0]) && isfinite(m[1]) && isfinite(m[2]) && isfinite(m[3]);
+        for (int c = 0; c < 4; ++c) val[4 * d + c] = ok ? m[c] : 0.0f;
+    }
+    for (uint32_t texel = 0; texel < 36u; ++texel) {
+        float p[2] = {((float)(texel % 6u) + 0.5f) / 6.0f, ((float)(texel / 6u) + 0.5f) / 6.0f};
+        float normal[3];
+        orc_decode_normal(p, normal);
+        float sum[3] = {0, 0, 0}, nominal = 0.0f, observed = 0.0f;
+        for (uint32_t d = 0; d < dirs; ++d) {
+            float cosine = fmaxf(dot3(normal, dir + 3 * d), 0.0f);
+            nominal += cosine;
+            if (cosine <= 0.0f) continue;
+            const float *v = val + 4 * d;
+            if (v[3] > 0.0f) {
+                float w = cosine * saturatef(v[3]);
+                for (int c = 0; c < 3; ++c) sum[c] = sum[c] + v[c] * w;
+                observed += w;
+            }
+        }
+        float *out = table + 4 * texel;
+        out[0] = out[1] = out[2] = out[3] = 0.0f;
+        if (nominal > 0.0f) {
+            float scale = nominal * (4.0f / (float)dirs);
+            if (observed > 0.0f) {
+                for (int c = 0; c < 3; ++c) out[c] = (sum[c] / observed) * scale;
+                out[3] = saturatef(observed / nominal);
+            }
+        }
+    }
+    free(dir);
+    free(val);
+}
+
+/* wrapIrradianceTexel / irradianceTexelIndex, shaders/world_resolve.slang:1-11. */
+static uint32_t texel_index(int32_t x, int32_t y) {
+    if (x < 0) { int32_t nx = -x - 1, ny = 5 - y; x = nx; y = ny; }
+    else if (x >= 6) { int32_t nx = 11 - x, ny = 5 - y; x = nx; y = ny; }
+    if (y < 0) { int32_t nx = 5 - x, ny = -y - 1; x = nx; y = ny; }
+    else if (y >= 6) { int32_t nx = 5 - x, ny = 11 - y; x = nx; y = ny; }
+    return (uint32_t)(y * 6 + x);
+}
+
+typedef struct { uint32_t texel[4]; float weight[4]; } Lookup;
+
+/* irradianceLookup, shaders/world_resolve.slang:27-40. */
+static Lookup irradiance_lookup(const float normal[3]) {
+    Lookup lk;
+    float e[2];
+    orc_encode_normal(normal, e);
+    float gx = e[0] * 6.0f - 0.5f, gy = e[1] * 6.0f - 0.5f;
+    float bx = floorf(gx), by = floorf(gy);
+    float fx = gx - bx, fy = gy - by;
+    float cx = 1.0f - fx, cy = 1.0f - fy;
+    lk.weight[0] = cx * cy;
+    lk.weight[1] = fx * cy;
+    lk.weight[2] = cx * fy;
+    lk.weight[3] = fx * fy;
+    int32_t ix = (int32_t)bx, iy = (int32_t)by;
+    lk.texel[0] = texel_index(ix, iy);
+    lk.texel[1] = texel_index(ix + 1, iy);
+    lk.texel[2] = texel_index(ix, iy + 1);
+    lk.texel[3] = texel_index(ix + 1, iy + 1);
+    return lk;
+}
+
+/* diffuseProbePage, shaders/world_resolve.slang:51-89: out = rgb, coverage. */
+static void probe_page(const float *table, const Lookup *lk, float out[4]) {
+    float sum[3] = {0, 0, 0}, observed = 0.0f;
+    for (int c = 0; c < 4; ++c) {
+        float bw = lk->weight[c];
+        if (!(bw > 0.0f)) continue;
+        const float *s = table + 4 * lk->texel[c];
+        if (!(s[3] > 0.0f) || !(isfinite(s[0]) && isfinite(s[1]) && isfinite(s[2]) && isfinite(s[3]))) continue;
+        float w = bw * saturatef(s[3]);
+        for (int k = 0; k < 3; ++k) sum[k] = sum[k] + s[k] * w;
+        observed += w;
+    }
+    for (int k = 0; k < 3; ++k) out[k] = observed > 0.0f ? sum[k] / observed : 0.0f;
+    out[3] = saturatef(observed);
+}
+
+void orc_probe_lookup(const float *table36, const float normal[3], float out[4]) {
+    Lookup lk = irradiance_lookup(normal);
+    probe_page(table36, &lk, out);
+}
+
+OrcFrame *orc_frame_run(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm, uint32_t n,
+                        int threads) {
+    OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
+    F->st = *st_in;
+    const LuxSettings *st = &F->st;
+    F->levels = st->levels;
+    /* seed: the cells of every level that hold a receiver. */
+    Key *tmp = (Key *)malloc(sizeof(Key) * (n ? n : 1));
+    for (uint32_t l = 0; l < F->levels; ++l) {
+        Level *L = &F->level[l];
+        L->columns = level_columns(st, l);
+        L->rows = level_rows(st, l);
+        L->dirs = L->columns * L->rows;
+        for (uint32_t i = 0; i < n; ++i) {
+            cell_key(st, l, pos + 4 * (size_t)i, tmp[i].k);
+            tmp[i].k[3] = 0;
+        }
+        qsort(tmp, n, sizeof(Key), key_cmp);
+        uint32_t cells = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (cells == 0 || key_cmp(&tmp[i], &tmp[cells - 1]) != 0) tmp[cells++] = tmp[i];
+        L->cells = cells;
+        L->keys = (Key *)malloc(sizeof(Key) * (cells ? cells : 1));
+        memcpy(L->keys, tmp, sizeof(Key) * cells);
+        uint64_t entries = (uint64_t)cells * L->dirs;
+        L->jsum = (float *)calloc(4 * entries + 4, sizeof(float));
+        L->count = (uint32_t *)calloc(entries + 1, sizeof(uint32_t));
+        L->merged = (float *)calloc(4 * entries + 4, sizeof(float));
+        L->raw = (float *)calloc(4 * entries + 4, sizeof(float));
+        F->stats.cells[l] = cells;
+        F->stats.entries[l] = entries;
+    }
+    free(tmp);
+    F->stats.levels = F->levels;
+    uint64_t shadow = 0;
+    OrcCounters cn = {0, 0, 0};
+    if (st->layout == LUX_LAYOUT_SPLIT) {
+        uint64_t rays = (uint64_t)n * st->rays_per_receiver;
+        FrameJob proto;
+        memset(&proto, 0, sizeof proto);
+        proto.S = S;
+        proto.st = st;
+        proto.pos = pos;
+        proto.nrm = nrm;
+        proto.n = n;
+        proto.term_level = (int32_t *)malloc(sizeof(int32_t) * (rays ? rays : 1));
+        proto.radiance = (float *)malloc(sizeof(float) * 3 * (rays ? rays : 1));
+        proto.uv = (float *)malloc(sizeof(float) * 2 * (rays ? rays : 1));
+        run_jobs(&proto, rays, threads, split_job, &shadow, &cn);
+        /* deposit, shaders/split.slang:1056-1117, then the per-key mean of
+         * reduce (shaders/split.slang:1386-1476), in ray order. */
+        for (uint64_t ray = 0; ray < rays; ++ray) {
+            int32_t term = proto.term_level[ray];
+            if (term < 0) {
+                F->stats.unsupported++;
+                continue;
+            }
+            uint32_t i = (uint32_t)(ray / st->rays_per_receiver);
+            for (uint32_t l = 0; l <= (uint32_t)term; ++l) {
+                Level *L = &F->level[l];
+                int32_t key[3];
+                cell_key(st, l, pos + 4 * (size_t)i, key);
+                int64_t cell = find_cell(L, key);
+                uint32_t bin = orc_direction_index_uv(proto.uv[2 * ray], proto.uv[2 * ray + 1], L->columns, L->rows);
+                uint64_t e = (uint64_t)cell * L->dirs + bin;
+                L->count[e] += 1;
+                if (l == (uint32_t)term) {
+                    for (int c = 0; c < 3; ++c) L->jsum[4 * e + c] += proto.radiance[3 * ray + c];
+                } else {
+                    L->jsum[4 * e + 3] += 1.0f;
+                }
+                F->stats.deposits++;
+            }
+        }
+        F->stats.interval_rays = rays;
+        free(proto.term_level);
+        free(proto.radiance);
+        free(proto.uv);
+    } else {
+        for (uint32_t l = 0; l < F->levels; ++l) {
+            FrameJob proto;
+            memset(&proto, 0, sizeof proto);
+            proto.S = S;
+            proto.st = st;
+            proto.levels = F->level;
+            proto.level = l;
+            uint64_t total = (uint64_t)F->level[l].cells * F->level[l].dirs;
+            run_jobs(&proto, total, threads, dense_job, &shadow, &cn);
+            F->stats.interval_rays += total;
+            for (uint64_t e = 0; e < total; ++e) {
+                if (F->level[l].count[e]) F->stats.deposits++;
+                else F->stats.unsupported++;
+            }
+        }
+    }
+    F->stats.shadow_rays = shadow;
+    F->stats.nodes_visited = cn.nodes;
+    F->stats.triangles_tested = cn.triangles;
+    F->stats.instances_visited = cn.instances;
+    /* merge, levels L-1 .. 0 (src/render.rs:9767-9777). */
+    for (int l = (int)F->levels - 1; l >= 0; --l) merge_level(F, (uint32_t)l);
+    /* pack every cascade-0 cell. */
+    Level *L0 = &F->level[0];
+    F->tables = (float *)calloc((size_t)L0->cells * 36 * 4 + 4, sizeof(float));
+    for (uint32_t cell = 0; cell < L0->cells; ++cell)
+        orc_pack_table(&L0->merged[4 * (uint64_t)cell * L0->dirs], L0->columns, L0->rows, &F->tables[(size_t)cell * 144]);
+    return F;
+}
+
+void orc_frame_destroy(OrcFrame *F) {
+    if (!F) return;
+    for (uint32_t l = 0; l < F->levels; ++l) {
+        free(F->level[l].keys);
+        free(F->level[l].jsum);
+        free(F->level[l].count);
+        free(F->level[l].merged);
+        free(F->level[l].raw);
+    }
+    free(F->tables);
+    free(F);
+}
+
+uint32_t orc_frame_cells(const OrcFrame *F, uint32_t level) { return level < F->levels ? F->level[level].cells : 0; }
+
+void orc_frame_read_level(const OrcFrame *F, uint32_t level, int32_t *keys, float *merged, float *raw,
+                          uint32_t *samples) {
+    if (level >= F->levels) return;
+    const Level *L = &F->level[level];
+    uint64_t entries = (uint64_t)L->cells * L->dirs;
+    if (keys) memcpy(keys, L->keys, sizeof(Key) * L->cells);
+    if (merged) memcpy(merged, L->merged, sizeof(float) * 4 * entries);
+    if (raw) memcpy(raw, L->raw, sizeof(float) * 4 * entries);
+    if (samples) memcpy(samples, L->count, sizeof(uint32_t) * entries);
+}
+
+void orc_frame_read_probes(const OrcFrame *F, float *tables) {
+    memcpy(tables, F->tables, sizeof(float) * 144 * F->level[0].cells);
+}
+
+void orc_frame_stats(const OrcFrame *F, LuxStats *stats) { *stats = F->stats; }
+
+/* worldResolve -> resolveSplitDiffuse -> diffuseAtLod at LOD 0
+ * (shaders/world_resolve.slang:96-196, :281-313). */
+void orc_frame_resolve(const OrcFrame *F, const float *position, const float *normal_in, uint32_t count, float *out) {
+    const LuxSettings *st = &F->st;
+    const Level *L0 = &F->level[0];
+    float s0 = orc_spacing(st, 0);
+    for (uint32_t i = 0; i < count; ++i) {
+        const float *p = position + 4 * (size_t)i, *nn = normal_in + 4 * (size_t)i;
+        float *o = out + 4 * (size_t)i;
+        float diffuse[3] = {0, 0, 0}, coverage = 0.0f;
+        int supported = 0;
+        float n3[3] = {nn[0], nn[1], nn[2]};
+        if (finite3(n3) && dot3(n3, n3) > 0.01f) {
+            float l = length3(n3);
+            float normal[3] = {n3[0] / l, n3[1] / l, n3[2] / l};
+            Lookup lk = irradiance_lookup(normal);
+            float grid[3], base[3], fr[3];
+            for (int c = 0; c < 3; ++c) {
+                grid[c] = p[c] / s0 - 0.5f;
+                base[c] = floorf(grid[c]);
+                fr[c] = grid[c] - base[c];
+            }
+            float sum[3] = {0, 0, 0}, observed = 0.0f, potential = 0.0f;
+            for (uint32_t corner = 0; corner < 8u; ++corner) {
+                uint32_t bx = corner & 1u, by = (corner >> 1) & 1u, bz = corner >> 2;
+                float ax = bx == 0u ? 1.0f - fr[0] : fr[0];
+                float ay = by == 0u ? 1.0f - fr[1] : fr[1];
+                float az = bz == 0u ? 1.0f - fr[2] : fr[2];
+                float w = (ax * ay) * az;
+                if (!(w > 0.0f)) continue;
+                potential += w;
+                int32_t key[3] = {(int32_t)base[0] + (int32_t)bx, (int32_t)base[1] + (int32_t)by,
+                                  (int32_t)base[2] + (int32_t)bz};
+                int64_t cell = find_cell(L0, key);
+                if (cell < 0) continue;
+                float probe[4];
+                probe_page(&F->tables[(size_t)cell * 144], &lk, probe);
+                float support = probe[3];
+                if (!(support > 0.0f)) continue;
+                float weight = w * support;
+                for (int c = 0; c < 3; ++c) sum[c] = sum[c] + probe[c] * weight;
+                observed += weight;
+            }
+            float low[3] = {0, 0, 0}, low_cov = 0.0f;
+            if (potential > 0.0f) {
+                low_cov = saturatef(observed / potential);
+                if (observed > 0.0f)
+                    for (int c = 0; c < 3; ++c) low[c] = sum[c] / observed;
+            }
+            /* resolveLodSource with one LOD (blend 0, high coverage 1). */
+            float low_weight = low_cov * (1.0f - 0.0f);
+            float high_weight = 1.0f * 0.0f;
+            float total = low_weight + high_weight;
+            coverage = saturatef(total);
+            for (int c = 0; c < 3; ++c)
+                diffuse[c] = total > 0.0f ? (low[c] * low_weight + 0.0f * high_weight) / total : 0.0f;
+            supported = coverage > 0.0f && finite3(diffuse);
+        }
+        o[0] = diffuse[0];
+        o[1] = diffuse[1];
+        o[2] = diffuse[2];
+        /* rawGiSupportAlpha, shaders/common.slang:323-326. */
+        o[3] = supported ? 1.0f + 0.25f * coverage : -1.0f;
+    }
+}
+
+/* ---- KAT helpers ---- */
+uint32_t orc_deposit_levels(const LuxSettings *s, float distance, int hit, int unsupported, const float radiance[3],
+                            float *out) {
+    if (unsupported) return 0;
+    uint32_t written = 0;
+    for (uint32_t l = 0; l < s->levels; ++l) {
+        int terminal = l + 1 == s->levels;
+        int terminates = terminal || (distance > interval_start(s, l) && distance <= orc_interval_end(s, l));
+        float *o = out + 4 * l;
+        o[0] = terminates ? radiance[0] : 0.0f;
+        o[1] = terminates ? radiance[1] : 0.0f;
+        o[2] = terminates ? radiance[2] : 0.0f;
+        o[3] = terminates ? 0.0f : 1.0f;
+        ++written;
+        if (terminates) break;
+    }
+    (void)hit;
+    return written;
+}
+
+/* checkDenseSdf, src/transport_tests.rs:179-248, on the CPU. */
+static float dense_box(const float p[3], const float c[3], const float h[3]) {
+    float q[3] = {fabsf(p[0] - c[0]) - h[0], fabsf(p[1] - c[1]) - h[1], fabsf(p[2] - c[2]) - h[2]};
+    float m[3] = {fmaxf(q[0], 0.0f), fmaxf(q[1], 0.0f), fmaxf(q[2], 0.0f)};
+    return length3(m) + fminf(fmaxf(q[0], fmaxf(q[1], q[2])), 0.0f);
+}
+static float dense_scene(const float p[3], uint32_t *material) {
+    static const float c1[3] = {-3, 0, 0}, h1[3] = {0.9f, 0.9f, 0.9f};
+    static const float c3[3] = {0, 3, 0}, h3[3] = {2, 0.04f, 2};
+    static const float c4[3] = {0, 0, 4}, h4[3] = {2, 0.5f, 0.03f};
+    float d = dense_box(p, c1, h1);
+    *material = 1;
+    float q[3] = {p[0] - 3.0f, p[1] - 1.0f, p[2]};
+    float sphere = length3(q) - 1.0f;
+    if (sphere < d) { d = sphere; *material = 2; }
+    float f = dense_box(p, c3, h3);
+    if (f < d) { d = f; *material = 3; }
+    float b = dense_box(p, c4, h4);
+    if (b < d) { d = b; *material = 4; }
+    return d;
+}
+void orc_dense_sdf_record(uint32_t index, float interval[4], float direction[4]) {
+    uint32_t level = 0, offset = 0, dimension = 1, dcount = 1;
+    for (uint32_t c = 0; c < 4; ++c) {
+        dimension = 16u >> c;
+        dcount = 32u << (2u * c);
+        uint32_t count = dimension * dimension * dimension * dcount;
+        if (index < offset + count) { level = c; break; }
+        offset += count;
+    }
+    uint32_t local = index - offset;
+    uint32_t di = local % dcount, probe = local / dcount;
+    uint32_t x = probe % dimension, y = (probe / dimension) % dimension, z = probe / (dimension * dimension);
+    float cell = (float)(1u << level);
+    float origin[3] = {-8.0f + ((float)x + 0.5f) * cell, -8.0f + ((float)y + 0.5f) * cell,
+                       -8.0f + ((float)z + 0.5f) * cell};
+    float dir[3];
+    orc_bin_direction(di, 8u << level, 4u << level, dir);
+    float start = (float)((1u << level) - 1u) + 0.001f;
+    float end = (float)((1u << (level + 1u)) - 1u);
+    interval[0] = interval[1] = interval[2] = 0.0f;
+    interval[3] = 1.0f;
+    for (uint32_t step = 0; step < 96u && start <= end; ++step) {
+        uint32_t material;
+        float p[3] = {origin[0] + dir[0] * start, origin[1] + dir[1] * start, origin[2] + dir[2] * start};
+        float d = dense_scene(p, &material);
+        if (d < 0.001f) {
+            if (material == 3u) {
+                interval[0] = 6.0f; interval[1] = 2.0f; interval[2] = 0.5f; interval[3] = 0.0f;
+            } else {
+                interval[0] = interval[1] = interval[2] = interval[3] = 0.0f;
+            }
+            break;
+        }
+        start += fmaxf(d, 0.005f);
+    }
+    direction[0] = dir[0];
+    direction[1] = dir[1];
+    direction[2] = dir[2];
+    direction[3] = (float)di;
+}

@@ -1,0 +1,125 @@
+/*
+ * lux_oracle.h - CPU restatement of the Split Radiance Cascades transport
+ * path of bevy_lux (HyperExtendedReality/bevy_penumbra).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the parity checker for liblux:
+ * only the tests, the smoke check and the CPU-baseline leg of the benchmark
+ * load it.  The product never links, loads or calls it.
+ *
+ * Every function restates a reference function; the citation is given at the
+ * definition in lux_oracle.c.  Parity is pinned against the reference's own
+ * known-answer tests (tests/test_oracle_golden.py): the deposit KAT
+ * (src/transport_tests.rs:3637-3829), the merge / support KATs
+ * (src/split_merge_tests.rs:13-305, 1298-1430), the resolve references
+ * (src/world_resolve_tests.rs:31-309), the dense-SDF direction mapping
+ * (src/transport_tests.rs:179-248, 3830-4107) and the traversal brute force
+ * (src/traversal_tests.rs:978-1125).
+ *
+ * Record layouts are the ones of include/lux.h (LuxRay, LuxHit, LuxLight,
+ * LuxSettings), so a test can hand the same bytes to both libraries.
+ */
+#ifndef LUX_ORACLE_H
+#define LUX_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+#include "../include/lux.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* --- direction / key math (shaders/common.slang) --------------------- */
+void orc_sincos_turns(float turns, float *c, float *s);
+void orc_decode_direction(float u, float v, float out[3]);
+void orc_bin_direction(uint32_t index, uint32_t columns, uint32_t rows, float out[3]);
+uint32_t orc_direction_index_uv(float u, float v, uint32_t columns, uint32_t rows);
+void orc_r2(uint32_t index, float out[2]);
+uint32_t orc_transport_hash(uint32_t value);
+uint32_t orc_hash_key(const int32_t key[4], uint32_t bucket_count);
+void orc_ray_offset(const float position[3], const float normal[3], float bias, float out[3]);
+void orc_encode_normal(const float n[3], float out[2]);
+void orc_decode_normal(const float p[2], float out[3]);
+float orc_interval_end(const LuxSettings *s, uint32_t level);
+float orc_spacing(const LuxSettings *s, uint32_t level);
+
+/* --- scene over the reference word streams ---------------------------- */
+typedef struct OrcScene OrcScene;
+OrcScene *orc_scene_create(const uint32_t *scene_words, size_t scene_word_count,
+                           const uint32_t *geometry_words, size_t geometry_word_count,
+                           const LuxLight *lights, uint32_t light_count,
+                           uint32_t conventional_lights);
+void orc_scene_destroy(OrcScene *scene);
+
+typedef struct OrcCounters {
+    uint64_t nodes;      /* binary BVH nodes whose box was tested */
+    uint64_t triangles;  /* triangle tests */
+    uint64_t instances;  /* instance transforms */
+} OrcCounters;
+
+/* traceRayTracked / traceRay (shaders/traversal.slang:696-819), closest hit. */
+void orc_trace_closest(const OrcScene *scene, const float origin[3], const float direction[3],
+                       float tmin, float limit, LuxHit *hit, OrcCounters *counters);
+/* traceOccluded (shaders/traversal.slang:955-1046). Returns blocked; *supported. */
+int orc_trace_occluded(const OrcScene *scene, const float origin[3], const float direction[3],
+                       float limit, int *supported, OrcCounters *counters);
+/* Same triangle test as the traversal, applied to every triangle (no BVH). */
+void orc_brute_closest(const OrcScene *scene, const float origin[3], const float direction[3],
+                       float tmin, float limit, LuxHit *hit);
+/* The f64 Moller-Trumbore brute force of src/traversal_tests.rs:978-1038:
+ * writes up to `capacity` (t, triangle, instance) candidates sorted by t and
+ * returns how many exist. */
+uint32_t orc_brute_f64(const OrcScene *scene, const float origin[3], const float direction[3],
+                       float limit, double *t, uint32_t *triangle, uint32_t *instance,
+                       uint32_t capacity);
+/* Batched harness: one LuxHit per LuxRay, `threads` host threads. */
+void orc_trace_rays(const OrcScene *scene, const LuxRay *rays, uint32_t count, int any_hit,
+                    LuxHit *hits, int threads, OrcCounters *counters);
+
+/* outgoingTransportRadianceTracked (shaders/cascades.slang:196-268) for the
+ * synthetic-material subset.  Returns supported. */
+int orc_outgoing_radiance(const OrcScene *scene, const LuxSettings *settings,
+                          const float origin[3], const float direction[3], const LuxHit *hit,
+                          float out[3], uint64_t *shadow_rays, OrcCounters *counters);
+
+/* --- one cascade frame ---------------------------------------------------- */
+typedef struct OrcFrame OrcFrame;
+OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
+                        const float *receiver_position, const float *receiver_normal,
+                        uint32_t receiver_count, int threads);
+void orc_frame_destroy(OrcFrame *frame);
+uint32_t orc_frame_cells(const OrcFrame *frame, uint32_t level);
+/* cell keys int4[cells] sorted ascending; merged/raw float4[cells*dirs];
+ * samples uint32[cells*dirs]; any pointer may be NULL. */
+void orc_frame_read_level(const OrcFrame *frame, uint32_t level, int32_t *keys, float *merged,
+                          float *raw, uint32_t *samples);
+/* packed cascade-0 tables float4[cells*36], same cell order as level 0. */
+void orc_frame_read_probes(const OrcFrame *frame, float *tables);
+void orc_frame_stats(const OrcFrame *frame, LuxStats *stats);
+void orc_frame_resolve(const OrcFrame *frame, const float *position, const float *normal,
+                       uint32_t count, float *out);
+
+/* --- stand-alone KAT entry points ------------------------------------ */
+/* deposit (shaders/split.slang:1056-1117) of one ray at `distance` with
+ * radiance rgb into `levels` (J.rgb, beta) records; returns the number of
+ * levels written (later levels untouched). */
+uint32_t orc_deposit_levels(const LuxSettings *s, float distance, int hit, int unsupported,
+                            const float radiance[3], float *out_interval);
+/* mergeEntry without history (shaders/split.slang:1624-1725): J, beta of one
+ * entry at `level` with its 4 children x 8 corners merged records supplied
+ * as child_merged[4][8] float4 (w <= 0 = missing) and the spatial fraction. */
+void orc_merge_entry(const float interval[4], uint32_t samples, const float fraction[3],
+                     const float *child_merged, int has_children, float out[4]);
+/* interpolateMergedChildSources, one source (shaders/split.slang:389-479). */
+void orc_interpolate_children(const float fraction[3], const float *corner_merged, float out[4]);
+/* packProbes texel table from base-direction merged values float4[dirs]. */
+void orc_pack_table(const float *merged, uint32_t columns, uint32_t rows, float *table36);
+/* irradianceLookup + diffuseProbePage on one table (shaders/world_resolve.slang:27-89). */
+void orc_probe_lookup(const float *table36, const float normal[3], float out[4]);
+/* Dense 16^3 SDF interval reference (src/transport_tests.rs:179-248) record i:
+ * interval float4 and direction float4 (xyz, index). */
+void orc_dense_sdf_record(uint32_t index, float interval[4], float direction[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,142 @@
+"""GPU cascade frame parity: trace + deposit + merge + pack + resolve of
+liblux against the CPU oracle on identical seeded inputs."""
+import numpy as np
+import pytest
+
+import bevy_penumbra_b200 as bp
+from bevy_penumbra_b200 import scenes
+import oracle
+from tests.helpers import cornell_dense_settings, empty_device, from_device, packed, to_device
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-4   # merged cascade radiance: relative tolerance
+ATOL = 1e-6
+
+
+def by_key(keys):
+    return {tuple(k[:3]): i for i, k in enumerate(keys)}
+
+
+def run_frame(name, settings, pos, nrm, max_cells=1 << 16, max_entries=1 << 24):
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed(name))
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=max_cells, max_entries=max_entries)
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    view.trace_merge(scene, settings, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+    st = view.stats()
+    assert st.error_flags == 0
+    levels = [view.read_level(l) for l in range(settings.levels)]
+    probes = view.read_probes()
+    return ctx, scene, view, st, levels, probes
+
+
+def oracle_frame(name, settings, pos, nrm):
+    return oracle.OracleFrame(oracle.OracleScene.from_packed(packed(name)), settings.to_c(), pos, nrm)
+
+
+def compare_levels(settings, gpu_levels, ofr, exact):
+    for level in range(settings.levels):
+        keys, merged, raw, samples = gpu_levels[level]
+        okeys, omerged, oraw, osamples = ofr.level(level, settings.direction_count(level))
+        assert len(keys) == len(okeys), f"level {level}: cell count"
+        index = by_key(okeys)
+        order = np.array([index[tuple(k[:3])] for k in keys])
+        np.testing.assert_array_equal(samples, osamples[order], err_msg=f"level {level} samples")
+        if exact:
+            np.testing.assert_array_equal(raw.view(np.uint32), oraw[order].view(np.uint32))
+            np.testing.assert_array_equal(merged.view(np.uint32), omerged[order].view(np.uint32))
+        else:
+            np.testing.assert_allclose(raw, oraw[order], rtol=RTOL, atol=ATOL, err_msg=f"level {level} raw")
+            np.testing.assert_allclose(merged, omerged[order], rtol=RTOL, atol=ATOL, err_msg=f"level {level} merged")
+    return order
+
+
+def test_dense_cornell_frame_matches_oracle():
+    settings = cornell_dense_settings()
+    pos, nrm = scenes.dense_plane_probes(64, 0.1, 10)
+    ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm)
+    assert st.interval_rays == 262_144
+    assert [st.cells[l] for l in range(4)] == [4096, 1024, 256, 64]
+    ofr = oracle_frame("cornell", settings, pos, nrm)
+    ost = ofr.stats()
+    assert st.shadow_rays == ost.shadow_rays
+    assert st.deposits == ost.deposits
+    compare_levels(settings, levels, ofr, exact=True)
+    index = by_key(levels[0][0])
+    otables = ofr.probes()
+    okeys = ofr.level(0, 16)[0]
+    order = np.array([by_key(pkeys)[tuple(k[:3])] for k in okeys])
+    np.testing.assert_allclose(tables[order], otables, rtol=RTOL, atol=ATOL)
+    # Some probes see lit surfaces and some see the emitter.
+    assert np.mean(levels[0][1][..., 3] > 0) > 0.2
+    assert float(np.max(tables[..., :3])) > 0.0
+
+
+def test_dense_cornell_resolve_matches_oracle():
+    settings = cornell_dense_settings()
+    pos, nrm = scenes.dense_plane_probes(64, 0.1, 10)
+    ctx, scene, view, st, levels, probes = run_frame("cornell", settings, pos, nrm)
+    rng = np.random.default_rng(3)
+    n = 8192
+    ppos = np.zeros((n, 4), np.float32)
+    ppos[:, 0] = rng.uniform(-3.0, 3.0, n)
+    ppos[:, 1] = rng.uniform(0.95, 1.15, n)
+    ppos[:, 2] = rng.uniform(-3.0, 3.0, n)
+    pn = rng.normal(size=(n, 3))
+    pn /= np.linalg.norm(pn, axis=1, keepdims=True)
+    pnrm = np.zeros((n, 4), np.float32)
+    pnrm[:, :3] = pn
+    d_p, d_n, d_o = to_device(ppos), to_device(pnrm), empty_device(n * 16)
+    view.resolve(settings, d_p.data_ptr(), d_n.data_ptr(), n, d_o.data_ptr())
+    ctx.synchronize()
+    out = from_device(d_o, np.float32, (n, 4))
+    expected = oracle_frame("cornell", settings, pos, nrm).resolve(ppos, pnrm)
+    np.testing.assert_allclose(out, expected, rtol=RTOL, atol=ATOL)
+    assert np.mean(out[:, 3] >= 1.0) > 0.5
+    # frame_host gives the same irradiance from host buffers.
+    host = view.frame_host(scene, settings, pos, nrm, ppos, pnrm)
+    np.testing.assert_allclose(host, expected, rtol=RTOL, atol=ATOL)
+
+
+def cornell_floor_receivers(n=32):
+    k = (np.arange(n, dtype=np.float32) + np.float32(0.5)) / np.float32(n) * np.float32(1.9) - np.float32(0.95)
+    x, z = np.meshgrid(k, k, indexing="ij")
+    pos = np.zeros((n * n, 4), np.float32)
+    pos[:, 0] = x.ravel()
+    pos[:, 2] = z.ravel()
+    nrm = np.zeros_like(pos)
+    nrm[:, 1] = 1.0
+    return pos, nrm
+
+
+@pytest.mark.parametrize("rays", [1, 8])
+def test_split_cornell_frame_matches_oracle(rays):
+    settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=rays,
+                                   frame_index=3).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm)
+    ofr = oracle_frame("cornell", settings, pos, nrm)
+    ost = ofr.stats()
+    assert st.interval_rays == len(pos) * rays
+    assert st.deposits == ost.deposits and st.shadow_rays == ost.shadow_rays
+    compare_levels(settings, levels, ofr, exact=False)
+    okeys = ofr.level(0, 32)[0]
+    order = np.array([by_key(pkeys)[tuple(k[:3])] for k in okeys])
+    np.testing.assert_allclose(tables[order], ofr.probes(), rtol=RTOL, atol=ATOL)
+
+
+def test_split_atrium_frame_matches_oracle():
+    settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=8, interval_ratio=2.0,
+                                   rays_per_receiver=4, emissive_samples=4, frame_index=1).sanitized()
+    rng = np.random.default_rng(9)
+    n = 2048
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, 0] = rng.uniform(-18, 18, n)
+    pos[:, 2] = rng.uniform(-18, 18, n)
+    pos[:, 1] = 0.0
+    nrm = np.zeros_like(pos)
+    nrm[:, 1] = 1.0
+    ctx, scene, view, st, levels, probes = run_frame("atrium65536", settings, pos, nrm, max_entries=1 << 26)
+    ofr = oracle_frame("atrium65536", settings, pos, nrm)
+    compare_levels(settings, levels, ofr, exact=False)
