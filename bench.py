@@ -32,10 +32,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cascade trace+merge ms/frame & Mrays/s @720p: plain vs learned cache, ≤2% RMSE"
 WIDTH, HEIGHT, PROBE_PX = 1280, 720, 4
+TRIANGLES = 262_144
 RAYS_PER_RECEIVER = 36
 EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
-LAUNCHES_PER_FRAME_FIXED = 8  # clear, 3 seed, layout, clear entries, trace, pack
+LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
 
 
 def settings_for_workload():
@@ -75,7 +76,7 @@ def build_workload(device: int = 0, host_only: bool = False):
     from bevy_penumbra_b200 import scenes
 
     t0 = time.time()
-    desc = scenes.atrium(seed=2, triangles=262_144)
+    desc = scenes.atrium(seed=2, triangles=TRIANGLES)
     packed = bp.PackedScene.from_desc(desc)
     ctx = scene = None
     if not host_only:
@@ -122,7 +123,8 @@ def build_workload(device: int = 0, host_only: bool = False):
         cells_max = max(cells_max, cells)
         entries += cells * settings.direction_count(level)
     view = None if host_only else bp.SplitView(ctx, max_receivers=len(rpos), max_cells=cells_max,
-                                               max_entries=entries)
+                                               max_entries=entries,
+                                               max_rays=len(rpos) * settings.rays_per_receiver)
     return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, rpos=rpos,
                 rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, setup_s=time.time() - t0)
 
@@ -240,7 +242,7 @@ def run_reference(args, rank, world):
 
 def workload_config(w):
     s = w["settings"]
-    return {"workload": "atrium 262144 tris, 1280x720 screen receivers at 4x4 px, 8 cascades",
+    return {"workload": f"atrium {TRIANGLES} tris, {WIDTH}x{HEIGHT} screen receivers at 4x4 px, 8 cascades",
             "triangles": w["desc"].world_triangles(), "receivers": int(len(w["rpos"])),
             "rays_per_receiver": RAYS_PER_RECEIVER, "interval_rays": int(len(w["rpos"]) * RAYS_PER_RECEIVER),
             "levels": s.levels, "base_directions": s.base_columns * s.base_rows,
@@ -253,6 +255,10 @@ def run_ours(args, rank, world):
 
     device = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(device)
+    # A real stream (not the legacy default) so the library orders its work on
+    # the same stream the CUDA events are recorded on.
+    work_stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(work_stream)
     dist = None
     if world > 1:
         import datetime
@@ -379,7 +385,13 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true",
+                    help="profiling case: 65,536-triangle atrium at 640x360 (not a benchmark line)")
     args = ap.parse_args()
+    if args.small:
+        global WIDTH, HEIGHT, TRIANGLES, EYE, TARGET
+        WIDTH, HEIGHT, TRIANGLES = 640, 360, 65_536
+        EYE, TARGET = (-7.0, 3.0, -6.0), (2.0, 4.0, 3.0)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":

@@ -319,9 +319,12 @@ class SplitView:
     """Per-view transport state (ViewBuffers) and one frame of
     seed -> trace -> deposit -> merge -> pack, then resolve."""
 
-    def __init__(self, ctx: LuxContext, max_receivers: int, max_cells: int, max_entries: int):
+    def __init__(self, ctx: LuxContext, max_receivers: int, max_cells: int, max_entries: int,
+                 max_rays: int | None = None):
         self.ctx = ctx
-        desc = N.LuxViewDesc(max_receivers, max_cells, max_entries)
+        if max_rays is None:
+            max_rays = max(max_receivers, min(max_entries, 1 << 24))
+        desc = N.LuxViewDesc(max_receivers, max_cells, max_entries, max_rays, 0)
         handle = C.c_void_p()
         ctx.check(lib().lux_view_create(ctx.handle, C.byref(desc), C.byref(handle)))
         self.handle = handle

@@ -81,7 +81,8 @@ class LuxStats(C.Structure):
 
 
 class LuxViewDesc(C.Structure):
-    _fields_ = [("max_receivers", C.c_uint32), ("max_cells", C.c_uint32), ("max_entries", C.c_uint64)]
+    _fields_ = [("max_receivers", C.c_uint32), ("max_cells", C.c_uint32), ("max_entries", C.c_uint64),
+                ("max_rays", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class LuxTimings(C.Structure):

@@ -268,7 +268,7 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     for (uint32_t i = 0; i < inst_count; ++i) {
         auto it = blas_root.find(inst[i].root);
         if (it == blas_root.end()) {
-            Collapser bl{bin, nodes, {}, tri_capacity};
+            Collapser bl{bin, nodes, {}, tri_count};
             uint32_t r = bl.root(inst[i].root);
             if (!bl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (BLAS): " + bl.error);
             it = blas_root.emplace(inst[i].root, r).first;

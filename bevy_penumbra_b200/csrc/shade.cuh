@@ -119,15 +119,27 @@ __device__ __forceinline__ float disney_multiplier(f3 n, f3 l, f3 v, float pr) {
     return ls * vs;
 }
 
-// emissiveResponseTracked, shaders/cascades.slang:57-134.  Returns false
-// when a visibility query was unsupported.
-__device__ bool emissive_response(const SceneView &S, const ShadeParams &P, f3 position, f3 normal, f3 gnormal, f3 view,
-                                  float roughness, f3 diffuse, f3 &out, uint32_t &shadow_rays, TraceCounters &cn) {
-    out = f3{0.0f, 0.0f, 0.0f};
+constexpr uint32_t kMaxNeeSamples = 16u;  // max(1, emissive_samples / 2) with emissive_samples <= 32
+
+// One next-event sample of emissiveResponseTracked whose visibility query is
+// still to be traced: the query ray and the sample's contribution if visible.
+struct NeeQuery {
+    f3 origin, direction;
+    float limit;
+    f3 contribution;
+};
+
+// emissiveResponseTracked, shaders/cascades.slang:57-134, up to (but not
+// including) the visibility trace: every sample that survives the geometric
+// tests becomes a query with its contribution emission * (response * cos / pdf).
+// Samples are emitted in sample order; `count` is the estimator's divisor.
+template <typename Emit>
+__device__ void emissive_queries(const SceneView &S, const ShadeParams &P, f3 position, f3 normal, f3 gnormal,
+                                 f3 view, float roughness, f3 diffuse, uint32_t &count, Emit &&emit) {
     uint32_t emissive = S.emissive_lights;
-    uint32_t count = P.emissive_samples / 2u;
+    count = P.emissive_samples / 2u;
     count = count < 1u ? 1u : count;
-    if (emissive == 0u) return true;
+    if (emissive == 0u) return;
     float cell = P.probe_spacing * 0.05f;
     uint32_t seed = hash_key((int32_t)floorf(position.x / cell), (int32_t)floorf(position.y / cell),
                              (int32_t)floorf(position.z / cell), 0, 16777216u);
@@ -141,7 +153,6 @@ __device__ bool emissive_response(const SceneView &S, const ShadeParams &P, f3 p
     r2(sample_frame, ax, ay);
     r2(selection_seed, bx, by);
     float phase = fracf(ax + bx);
-    f3 sum{0.0f, 0.0f, 0.0f};
     const float bias = P.normal_bias;
     const LuxLight *lights = S.lights + S.conventional_lights;
     for (uint32_t sample = 0; sample < count; ++sample) {
@@ -188,84 +199,83 @@ __device__ bool emissive_response(const SceneView &S, const ShadeParams &P, f3 p
         f3 delta = target - origin;
         float distance = length(delta);
         if (distance <= bias * 0.25f) continue;
-        f3 dir = delta / distance;
-        Hit sh;
-        ++shadow_rays;
-        trace<true>(S, origin, dir, 0.0f, distance - fminf(bias * 0.25f, distance * 0.001f), sh, cn);
-        if ((sh.errors & kQueryUnsupported) != 0u && sh.tri == kEmpty) {
-            out = f3{0.0f, 0.0f, 0.0f};
-            return false;
-        }
-        if (sh.tri != kEmpty) continue;
+        NeeQuery q;
+        q.origin = origin;
+        q.direction = delta / distance;
+        q.limit = distance - fminf(bias * 0.25f, distance * 0.001f);
         float factor = disney_multiplier(normal, ld, view, roughness) / kPi;
         float p = fmaxf(pdf, 1e-20f);
-        sum.x = sum.x + emission.x * (((diffuse.x * factor) * cosine) / p);
-        sum.y = sum.y + emission.y * (((diffuse.y * factor) * cosine) / p);
-        sum.z = sum.z + emission.z * (((diffuse.z * factor) * cosine) / p);
+        q.contribution = f3{emission.x * (((diffuse.x * factor) * cosine) / p),
+                            emission.y * (((diffuse.y * factor) * cosine) / p),
+                            emission.z * (((diffuse.z * factor) * cosine) / p)};
+        emit(sample, q);
     }
-    out = f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
-    return true;
 }
 
-// outgoingTransportRadianceTracked, shaders/cascades.slang:196-268.  Returns
-// false when the query is unsupported (no deposit).
-__device__ bool outgoing_radiance(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
-                                  f3 &out, uint32_t &shadow_rays, TraceCounters &cn) {
-    out = f3{0.0f, 0.0f, 0.0f};
+// outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, up to the
+// visibility traces.  Writes the hit's own emission to `base` and emits the
+// next-event queries; returns false when the query is unsupported (no
+// deposit).  `count` = 0 when no next-event estimate applies.
+template <typename Emit>
+__device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
+                                f3 &base, uint32_t &count, Emit &&emit) {
+    base = f3{0.0f, 0.0f, 0.0f};
+    count = 0;
     if ((hit.errors & kQueryUnsupported) != 0u) return false;
     if (hit.tri == kEmpty) return true;
     float b0 = (1.0f - hit.b1) - hit.b2;
     Surface sf = surface_at(S, P, hit.inst, hit.tri, b0, hit.b1, hit.b2);
-    f3 radiance = sf.emission;
-    if ((sf.flags & 16u) == 0u) {
-        uint32_t base = instance_base(S, hit.inst);
-        uint4 header = gword(S, 0);
-        uint4 t = gword(S, header.x + hit.tri);
-        uint32_t idx[3] = {t.x, t.y, t.z};
-        f3 A = f3w(gword(S, header.y + idx[0] * header.z));
-        f3 B = f3w(gword(S, header.y + idx[1] * header.z));
-        f3 C = f3w(gword(S, header.y + idx[2] * header.z));
-        f3 position{origin.x + direction.x * hit.t, origin.y + direction.y * hit.t, origin.z + direction.z * hit.t};
-        f3 gn = unit_vector(transform_direction_t(S, base, cross(B - A, C - A)), f3{0.0f, 1.0f, 0.0f});
-        float sign = (sf.flags & 4u) != 0u ? -1.0f : 1.0f;
-        gn = gn * sign;
-        // hitAttributes world normal, shaders/traversal.slang:258-282.
-        float bary[3] = {b0, hit.b1, hit.b2};
-        f3 world_normal{0.0f, 0.0f, 0.0f};
+    base = sf.emission;
+    if ((sf.flags & 16u) != 0u) return true;
+    uint32_t ibase = instance_base(S, hit.inst);
+    uint4 header = gword(S, 0);
+    uint4 t = gword(S, header.x + hit.tri);
+    uint32_t idx[3] = {t.x, t.y, t.z};
+    f3 A = f3w(gword(S, header.y + idx[0] * header.z));
+    f3 B = f3w(gword(S, header.y + idx[1] * header.z));
+    f3 C = f3w(gword(S, header.y + idx[2] * header.z));
+    f3 position{origin.x + direction.x * hit.t, origin.y + direction.y * hit.t, origin.z + direction.z * hit.t};
+    f3 gn = unit_vector(transform_direction_t(S, ibase, cross(B - A, C - A)), f3{0.0f, 1.0f, 0.0f});
+    float sign = (sf.flags & 4u) != 0u ? -1.0f : 1.0f;
+    gn = gn * sign;
+    // hitAttributes world normal, shaders/traversal.slang:258-282.
+    float bary[3] = {b0, hit.b1, hit.b2};
+    f3 world_normal{0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int i = 0; i < 3; ++i) {
-            uint32_t vb = header.y + idx[i] * header.z;
-            f3 nrm = gn;
-            if ((gword(S, vb).w & 1u) != 0u) nrm = unit_vector(transform_direction_t(S, base, f3w(gword(S, vb + 1))), gn);
-            world_normal = f3{world_normal.x + nrm.x * bary[i], world_normal.y + nrm.y * bary[i],
-                              world_normal.z + nrm.z * bary[i]};
-        }
-        // materialNormal without a normal texture, shaders/material.slang:171-177.
-        f3 normal = unit_vector(world_normal, gn);
-        bool back = dot(gn, direction) > 0.0f;
-        if (back && (sf.flags & 8u) != 0u) normal = -normal;
-        f3 flipped = dot(gn, direction) > 0.0f ? -gn : gn;
-        f3 neg = -direction;
-        if (!(dot(normal, neg) <= 0.0f || dot(normal, flipped) <= 0.0f)) {
-            float nl = length(neg);
-            f3 view = neg / nl;
-            float metallic = saturate(sf.metallic);
-            float roughness = saturate(sf.roughness);
-            if (!isfinite(roughness)) roughness = 1.0f;
-            bool bf = finite3(sf.base_color);
-            f3 diffuse{(bf ? saturate(sf.base_color.x) : 0.0f) * (1.0f - metallic),
-                       (bf ? saturate(sf.base_color.y) : 0.0f) * (1.0f - metallic),
-                       (bf ? saturate(sf.base_color.z) : 0.0f) * (1.0f - metallic)};
-            f3 nee;
-            if (!emissive_response(S, P, position, normal, flipped, view, roughness, diffuse, nee, shadow_rays, cn))
-                return false;
-            radiance = radiance + nee;
-        }
+    for (int i = 0; i < 3; ++i) {
+        uint32_t vb = header.y + idx[i] * header.z;
+        f3 nrm = gn;
+        if ((gword(S, vb).w & 1u) != 0u) nrm = unit_vector(transform_direction_t(S, ibase, f3w(gword(S, vb + 1))), gn);
+        world_normal = f3{world_normal.x + nrm.x * bary[i], world_normal.y + nrm.y * bary[i],
+                          world_normal.z + nrm.z * bary[i]};
     }
-    // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188.
-    if (!finite3(radiance)) return true;
-    out = f3{fmaxf(radiance.x, 0.0f), fmaxf(radiance.y, 0.0f), fmaxf(radiance.z, 0.0f)};
+    // materialNormal without a normal texture, shaders/material.slang:171-177.
+    f3 normal = unit_vector(world_normal, gn);
+    bool back = dot(gn, direction) > 0.0f;
+    if (back && (sf.flags & 8u) != 0u) normal = -normal;
+    f3 flipped = dot(gn, direction) > 0.0f ? -gn : gn;
+    f3 neg = -direction;
+    if (dot(normal, neg) <= 0.0f || dot(normal, flipped) <= 0.0f) return true;
+    float nl = length(neg);
+    f3 view = neg / nl;
+    float metallic = saturate(sf.metallic);
+    float roughness = saturate(sf.roughness);
+    if (!isfinite(roughness)) roughness = 1.0f;
+    bool bf = finite3(sf.base_color);
+    f3 diffuse{(bf ? saturate(sf.base_color.x) : 0.0f) * (1.0f - metallic),
+               (bf ? saturate(sf.base_color.y) : 0.0f) * (1.0f - metallic),
+               (bf ? saturate(sf.base_color.z) : 0.0f) * (1.0f - metallic)};
+    emissive_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
     return true;
+}
+
+// clampOutgoingTransportRadiance, shaders/cascades.slang:179-188, after the
+// next-event sum: radiance = base + sum / count.
+__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count) {
+    f3 radiance = base;
+    if (count) radiance = radiance + f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
+    if (!finite3(radiance)) return f3{0.0f, 0.0f, 0.0f};
+    return f3{fmaxf(radiance.x, 0.0f), fmaxf(radiance.y, 0.0f), fmaxf(radiance.z, 0.0f)};
 }
 
 }  // namespace lux

@@ -53,10 +53,48 @@ __device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, flo
     return near_t <= far_t;
 }
 
-// Child tests of one BVH4 node.  Returns the hit mask; entry[i] as in
-// boxEntryDistance.  Children whose padded exit precedes tmin cannot hold a
-// hit with t > tmin and are skipped.
-__device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes, uint32_t index, f3 o, f3 d,
+// Per-ray slab constants for the BVH4 child tests.  The reference divides
+// by the direction for every slab (shaders/traversal.slang:360-361); the
+// child tests here multiply by the reciprocal and widen the interval so the
+// test stays conservative: t = (lo - o) * inv carries at most three roundings
+// (gamma_3 < 1.8e-7 relative), and the interval grows by 7.2e-7 relative on
+// both ends, twice the reference's exit padding.  Culling only decides which
+// triangles are tested; hit distances come from the exact triangle test.
+struct SlabRay {
+    float ox, oy, oz;
+    float ix, iy, iz;  // 1 / d (unused on zero axes)
+    bool zx, zy, zz;   // zero direction components (the reference's inside test)
+};
+
+__device__ __forceinline__ SlabRay slab_ray(f3 o, f3 d) {
+    SlabRay r;
+    r.ox = o.x;
+    r.oy = o.y;
+    r.oz = o.z;
+    r.zx = d.x == 0.0f;
+    r.zy = d.y == 0.0f;
+    r.zz = d.z == 0.0f;
+    r.ix = r.zx ? 0.0f : 1.0f / d.x;
+    r.iy = r.zy ? 0.0f : 1.0f / d.y;
+    r.iz = r.zz ? 0.0f : 1.0f / d.z;
+    return r;
+}
+
+__device__ __forceinline__ void slab_axis(bool zero, float o, float inv, float lo, float hi, float &near_t,
+                                          float &far_t) {
+    if (zero) {
+        if (o < lo || o > hi) far_t = -INFINITY;
+    } else {
+        float ta = (lo - o) * inv;
+        float tb = (hi - o) * inv;
+        near_t = fmaxf(near_t, fminf(ta, tb));
+        far_t = fminf(far_t, fmaxf(ta, tb));
+    }
+}
+
+// Child tests of one BVH4 node.  Returns the hit mask and conservative entry
+// distances; children that end before tmin or start after `limit` are culled.
+__device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes, uint32_t index, const SlabRay &r,
                                               float limit, float tmin, float entry[4], uint32_t child[4]) {
     const float4 *p = reinterpret_cast<const float4 *>(nodes + index);
     float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
@@ -72,14 +110,15 @@ __device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        float e, x;
-        bool h = child[i] != kEmpty && box_interval(o, d, LX[i], LY[i], LZ[i], HX[i], HY[i], HZ[i], limit, e, x);
-        if (h && x >= tmin) {
-            mask |= 1u << i;
-            entry[i] = e;
-        } else {
-            entry[i] = 0.0f;
-        }
+        float near_t = 0.0f, far_t = INFINITY;
+        slab_axis(r.zx, r.ox, r.ix, LX[i], HX[i], near_t, far_t);
+        slab_axis(r.zy, r.oy, r.iy, LY[i], HY[i], near_t, far_t);
+        slab_axis(r.zz, r.oz, r.iz, LZ[i], HZ[i], near_t, far_t);
+        near_t = near_t - fabsf(near_t) * 7.2e-7f;
+        far_t = far_t + fabsf(far_t) * 7.2e-7f;
+        bool h = child[i] != kEmpty && near_t <= far_t && near_t <= limit && far_t >= tmin;
+        entry[i] = h ? near_t : 0.0f;
+        mask |= h ? (1u << i) : 0u;
     }
     return mask;
 }
@@ -236,6 +275,7 @@ __device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, fl
     local_ray(I, o, d, lo, ld);
     cn.instances++;
     TriRay ray = triangle_ray(ld);
+    SlabRay sr = slab_ray(lo, ld);
     uint32_t stack_p[kStack];
     float stack_t[kStack];
     int sp = 0;
@@ -267,7 +307,7 @@ __device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, fl
             float entry[4];
             uint32_t child[4];
             cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, lo, ld, kAnyHit ? hit.t : hit.t, tmin, entry, child);
+            uint32_t mask = node_test(S.nodes, cur, sr, hit.t, tmin, entry, child);
             if (mask == 0u) continue;
             float e[4];
             uint32_t p[4];
@@ -338,6 +378,7 @@ __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, H
     if (!box_interval(o, d, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1], S.root_hi[2],
                       limit, re, rx))
         return;
+    SlabRay sr = slab_ray(o, d);
     uint32_t stack_p[kStack];
     float stack_t[kStack];
     int sp = 0;
@@ -368,7 +409,7 @@ __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, H
             float entry[4];
             uint32_t child[4];
             cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, o, d, hit.t, tmin, entry, child);
+            uint32_t mask = node_test(S.nodes, cur, sr, hit.t, tmin, entry, child);
             if (mask == 0u) continue;
             float e[4];
             uint32_t p[4];

@@ -34,7 +34,7 @@ using lux::f3;
 
 struct FrameParams {
     uint32_t levels, layout, rays_per_receiver, receivers;
-    uint32_t dir_capacity, cell_capacity;
+    uint32_t dir_capacity, cell_capacity, ray_capacity, queue_capacity;
     unsigned long long entry_capacity;
     float spacing[LUX_MAX_LEVELS];
     float start[LUX_MAX_LEVELS];
@@ -62,6 +62,17 @@ struct ViewDevice {
     float4 *tables;                 // [cell_capacity][36]
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
+    // Wavefront trace state, [max_rays] and [max_rays * kMaxNeeSamples].
+    float4 *ray_o;                  // origin, hit t
+    float4 *ray_d;                  // direction, barycentric 1
+    uint4 *ray_h;                   // triangle, instance, errors, barycentric 2 bits
+    float4 *ray_base;               // hit emission, next-event count (kEmpty: unsupported)
+    uint32_t *slot_query;           // per (ray, sample): queue index or kEmpty
+    float4 *slot_contrib;           // per (ray, sample): contribution if visible
+    float4 *queue_o;                // query origin, limit
+    float4 *queue_d;                // query direction
+    uint8_t *queue_result;          // 0 visible, 1 blocked, 2 unsupported
+    uint32_t *queue_count;
 };
 
 constexpr int kStatInterval = 0, kStatShadow = 1, kStatNodes = 2, kStatTris = 3, kStatInst = 4, kStatDeposits = 5,
@@ -119,7 +130,10 @@ __global__ void clear_kernel(ViewDevice V, FrameParams F) {
         V.level_base[threadIdx.x] = 0;
     }
     if (blockIdx.x == 0 && threadIdx.x < 8) V.stats[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *V.error_flags = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *V.error_flags = 0;
+        *V.queue_count = 0;
+    }
 }
 
 // seed: insert every receiver's cell of every level (insertProbeDescriptor,
@@ -194,6 +208,7 @@ __global__ void layout_kernel(ViewDevice V, FrameParams F) {
         base += (unsigned long long)cells * F.dirs[l];
     }
     if (base > F.entry_capacity) atomicOr(V.error_flags, LUX_VIEW_ERR_ENTRY_CAPACITY);
+    if (F.layout == LUX_LAYOUT_DENSE && base > F.ray_capacity) atomicOr(V.error_flags, LUX_VIEW_ERR_RAY_CAPACITY);
 }
 
 __device__ __forceinline__ unsigned long long total_entries(const ViewDevice &V, const FrameParams &F) {
@@ -212,48 +227,240 @@ __global__ void clear_entries_kernel(ViewDevice V, FrameParams F) {
     }
 }
 
-// Split layout: one thread per (receiver, ray).  traceTransport +
-// finishTransportVariant + deposit (shaders/split.slang:1056-1216).
-__global__ void __launch_bounds__(128) trace_split_kernel(ViewDevice V, FrameParams F, SceneView S,
-                                                          const float4 *__restrict__ pos,
-                                                          const float4 *__restrict__ nrm, uint32_t ray_count) {
+// ---------------------------------------------------------------------------
+// Trace stage as a wavefront (the reference's deferred trace: traceDeferred,
+// traceRecord, traceVisibility, traceResolve, shaders/split.slang:1276-1384):
+//   closest   interval rays -> closest hits (lean traversal kernel)
+//   shade     hit shading; next-event queries appended to one queue
+//   shadow    every queued visibility query in its own lane (any hit)
+//   deposit   next-event sum in sample order, then deposit into the levels
+// ---------------------------------------------------------------------------
+
+// Split ray of receiver i, ray k: direction decodeDirection(frac(0.5 +
+// r2(sequence + 1) + jitter)) flipped into the normal's hemisphere
+// (traceTransport, shaders/split.slang:1135-1146); (u, v) of the flipped
+// direction give its bin at every level.
+__device__ __forceinline__ void split_direction(const FrameParams &F, uint32_t i, uint32_t k, f3 n, f3 &dir, float &u,
+                                                float &v) {
+    float jx, jy, rx, ry;
+    lux::r2(lux::transport_hash(F.shade.frame ^ 0x5a17c9e3u), jx, jy);
+    lux::r2(i * F.rays_per_receiver + k + 1u, rx, ry);
+    u = lux::fracf((0.5f + rx) + jx);
+    v = lux::fracf((0.5f + ry) + jy);
+    dir = lux::decode_direction(u, v);
+    if (lux::dot(dir, n) < 0.0f) {
+        dir = -dir;
+        u = lux::fracf(u + 0.5f);
+        v = 1.0f - v;
+    }
+}
+
+__device__ __forceinline__ void store_ray(const ViewDevice &V, uint32_t ray, f3 o, f3 d, const lux::Hit &h) {
+    V.ray_o[ray] = make_float4(o.x, o.y, o.z, h.t);
+    V.ray_d[ray] = make_float4(d.x, d.y, d.z, h.b1);
+    V.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
+}
+
+__device__ __forceinline__ void load_ray(const ViewDevice &V, uint32_t ray, f3 &o, f3 &d, lux::Hit &h) {
+    float4 a = V.ray_o[ray], b = V.ray_d[ray];
+    uint4 c = V.ray_h[ray];
+    o = f3{a.x, a.y, a.z};
+    d = f3{b.x, b.y, b.z};
+    h.t = a.w;
+    h.b1 = b.w;
+    h.tri = c.x;
+    h.inst = c.y;
+    h.errors = c.z;
+    h.b2 = lux::as_float(c.w);
+}
+
+__global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
+                                                            const float4 *__restrict__ pos,
+                                                            const float4 *__restrict__ nrm, uint32_t ray_count) {
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
-    bool ok = *V.error_flags == 0u;
     uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x;
-    if (ok && ray < ray_count) {
-        uint32_t R = F.rays_per_receiver;
-        uint32_t i = ray / R, k = ray % R;
+    if (*V.error_flags == 0u && ray < ray_count) {
+        uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
         float4 p4 = pos[i], n4 = nrm[i];
         f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
-        float jx, jy, rx, ry;
-        lux::r2(lux::transport_hash(F.shade.frame ^ 0x5a17c9e3u), jx, jy);
-        lux::r2(i * R + k + 1u, rx, ry);
-        float u = lux::fracf((0.5f + rx) + jx);
-        float v = lux::fracf((0.5f + ry) + jy);
-        f3 dir = lux::decode_direction(u, v);
-        if (lux::dot(dir, n) < 0.0f) {
-            dir = -dir;
-            u = lux::fracf(u + 0.5f);
-            v = 1.0f - v;
-        }
+        f3 dir;
+        float u, v;
+        split_direction(F, i, k, n, dir, u, v);
         f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
         lux::TraceCounters cn{0, 0, 0};
         lux::Hit hit;
         lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
-        f3 radiance;
-        uint32_t shadow = 0;
-        bool supported = lux::outgoing_radiance(S, F.shade, origin, dir, hit, radiance, shadow, cn);
+        store_ray(V, ray, origin, dir, hit);
         st[kStatInterval] = 1;
-        st[kStatShadow] = shadow;
         st[kStatNodes] = cn.nodes;
         st[kStatTris] = cn.triangles;
         st[kStatInst] = cn.instances;
-        if (!supported) {
+    }
+    add_stats(V.stats, st);
+}
+
+// Dense layout: one ray per (cell, direction) record of one level; the ray
+// starts at the cell centre and covers the level's interval (the dense
+// reference of src/transport_tests.rs:179-248 with BVH geometry).  The ray
+// index is the record index.
+__global__ void __launch_bounds__(128) closest_dense_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t level) {
+    if (*V.error_flags) return;
+    unsigned long long n = (unsigned long long)V.cell_count[level] * F.dirs[level];
+    unsigned long long base = V.level_base[level];
+    const bool terminal = level + 1u == F.levels;
+    const float tmin = F.start[level];
+    const float limit = terminal ? 1e20f : nextafterf(F.end[level], INFINITY);
+    const float sp = F.spacing[level];
+    const uint32_t dirs = F.dirs[level];
+    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
+         e < ((n + 31ull) & ~31ull); e += (unsigned long long)gridDim.x * blockDim.x) {
+        unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (e < n) {
+            uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
+            int4 key = V.cell_keys[(size_t)level * F.cell_capacity + cell];
+            f3 origin{((float)key.x + 0.5f) * sp, ((float)key.y + 0.5f) * sp, ((float)key.z + 0.5f) * sp};
+            f3 dir = lux::bin_direction(d, F.columns[level], F.rows[level]);
+            lux::TraceCounters cn{0, 0, 0};
+            lux::Hit hit;
+            lux::trace<false>(S, origin, dir, tmin, limit, hit, cn);
+            store_ray(V, (uint32_t)(base + e), origin, dir, hit);
+            st[kStatInterval] = 1;
+            st[kStatNodes] = cn.nodes;
+            st[kStatTris] = cn.triangles;
+            st[kStatInst] = cn.instances;
+        }
+        add_stats(V.stats, st);
+    }
+}
+
+// Hit shading up to the visibility traces; queries are appended to the
+// queue with one atomic per warp.
+__global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t ray_count,
+                                                    bool dense) {
+    if (*V.error_flags) return;
+    uint32_t rays = dense ? (uint32_t)min(total_entries(V, F), (unsigned long long)ray_count) : ray_count;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base_ray = blockIdx.x * blockDim.x; base_ray < rays; base_ray += gridDim.x * blockDim.x) {
+        uint32_t ray = base_ray + threadIdx.x;
+        lux::NeeQuery q[lux::kMaxNeeSamples];
+        uint32_t slot_of[lux::kMaxNeeSamples];
+        uint32_t nq = 0, count = 0;
+        bool supported = false;
+        f3 base{0.0f, 0.0f, 0.0f};
+        if (ray < rays) {
+            f3 o, d;
+            lux::Hit hit;
+            load_ray(V, ray, o, d, hit);
+            supported = lux::outgoing_record(S, F.shade, o, d, hit, base, count,
+                                             [&](uint32_t sample, const lux::NeeQuery &query) {
+                                                 q[nq] = query;
+                                                 slot_of[nq] = sample;
+                                                 ++nq;
+                                             });
+            V.ray_base[ray] = make_float4(base.x, base.y, base.z,
+                                          lux::as_float(supported ? count : lux::kEmpty));
+        }
+        // Warp-aggregated append of this warp's queries.
+        uint32_t prefix = nq;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, prefix, off);
+            if (lane >= (uint32_t)off) prefix += t;
+        }
+        uint32_t total = __shfl_sync(0xffffffffu, prefix, 31);
+        uint32_t first = 0;
+        if (lane == 31 && total) first = atomicAdd(V.queue_count, total);
+        first = __shfl_sync(0xffffffffu, first, 31);
+        uint32_t at = first + prefix - nq;
+        if (ray < rays) {
+            uint32_t k = 0;
+            for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
+                uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
+                if (k < nq && slot_of[k] == s) {
+                    uint32_t qi = at + k;
+                    if (qi < F.queue_capacity) {
+                        V.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
+                        V.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
+                        V.slot_query[slot] = qi;
+                        V.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
+                                                           q[k].contribution.z, 0.0f);
+                    } else {
+                        V.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
+                    }
+                    ++k;
+                } else {
+                    V.slot_query[slot] = lux::kEmpty;
+                }
+            }
+        }
+    }
+}
+
+// Visibility queries, one per lane (traceVisibility, shaders/split.slang:1326-1339).
+// result: 0 visible, 1 blocked, 2 unsupported.
+__global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
+    if (*V.error_flags) return;
+    uint32_t n = min(*V.queue_count, F.queue_capacity);
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        uint32_t qi = base + threadIdx.x;
+        unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (qi < n) {
+            float4 a = V.queue_o[qi], b = V.queue_d[qi];
+            lux::TraceCounters cn{0, 0, 0};
+            lux::Hit sh;
+            lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
+            uint8_t r = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            V.queue_result[qi] = r;
+            st[kStatShadow] = 1;
+            st[kStatNodes] = cn.nodes;
+            st[kStatTris] = cn.triangles;
+            st[kStatInst] = cn.instances;
+        }
+        add_stats(V.stats, st);
+    }
+}
+
+// Next-event sum in sample order; false when the ray's query is unsupported.
+__device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, f3 &radiance) {
+    float4 b = V.ray_base[ray];
+    uint32_t count = lux::as_uint(b.w);
+    if (count == lux::kEmpty) return false;
+    f3 sum{0.0f, 0.0f, 0.0f};
+    for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
+        size_t slot = (size_t)ray * lux::kMaxNeeSamples + s;
+        uint32_t qi = V.slot_query[slot];
+        if (qi == lux::kEmpty) continue;
+        if (qi == lux::kEmpty - 1u) return false;
+        uint8_t r = V.queue_result[qi];
+        if (r == 2) return false;
+        if (r == 1) continue;
+        float4 c = V.slot_contrib[slot];
+        sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
+    }
+    radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count);
+    return true;
+}
+
+// deposit, shaders/split.slang:1056-1117: every level up to and including
+// the one whose interval holds the hit; the last level owns the tail.
+__global__ void __launch_bounds__(128) deposit_split_kernel(ViewDevice V, FrameParams F,
+                                                            const float4 *__restrict__ nrm, uint32_t ray_count) {
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x;
+    if (*V.error_flags == 0u && ray < ray_count) {
+        f3 radiance;
+        if (!ray_radiance(V, ray, radiance)) {
             st[kStatUnsupported] = 1;
         } else {
+            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+            float4 n4 = nrm[i];
+            f3 dir;
+            float u, v;
+            split_direction(F, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+            float t = V.ray_o[ray].w;
             uint32_t term = F.levels - 1u;
             for (uint32_t l = 0; l + 1u < F.levels; ++l)
-                if (hit.t > F.start[l] && hit.t <= F.end[l]) {
+                if (t > F.start[l] && t <= F.end[l]) {
                     term = l;
                     break;
                 }
@@ -277,42 +484,22 @@ __global__ void __launch_bounds__(128) trace_split_kernel(ViewDevice V, FramePar
     add_stats(V.stats, st);
 }
 
-// Dense layout: one thread per (cell, direction) record of one level; the
-// ray starts at the cell centre and covers the level's interval (the dense
-// reference of src/transport_tests.rs:179-248 with BVH geometry).
-__global__ void __launch_bounds__(128) trace_dense_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t level) {
+__global__ void __launch_bounds__(128) deposit_dense_kernel(ViewDevice V, FrameParams F) {
     if (*V.error_flags) return;
-    unsigned long long n = (unsigned long long)V.cell_count[level] * F.dirs[level];
-    unsigned long long base = V.level_base[level];
-    const bool terminal = level + 1u == F.levels;
-    const float tmin = F.start[level];
-    const float limit = terminal ? 1e20f : nextafterf(F.end[level], INFINITY);
-    const float sp = F.spacing[level];
-    const uint32_t dirs = F.dirs[level];
+    unsigned long long n = total_entries(V, F);
     for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x;
          e < ((n + 31ull) & ~31ull); e += (unsigned long long)gridDim.x * blockDim.x) {
         unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
         if (e < n) {
-            uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
-            int4 key = V.cell_keys[(size_t)level * F.cell_capacity + cell];
-            f3 origin{((float)key.x + 0.5f) * sp, ((float)key.y + 0.5f) * sp, ((float)key.z + 0.5f) * sp};
-            f3 dir = lux::bin_direction(d, F.columns[level], F.rows[level]);
-            lux::TraceCounters cn{0, 0, 0};
-            lux::Hit hit;
-            lux::trace<false>(S, origin, dir, tmin, limit, hit, cn);
+            uint32_t level = 0;
+            while (level + 1u < F.levels && e >= V.level_base[level + 1u]) ++level;
+            bool terminal = level + 1u == F.levels;
             f3 radiance;
-            uint32_t shadow = 0;
-            bool supported = lux::outgoing_radiance(S, F.shade, origin, dir, hit, radiance, shadow, cn);
-            st[kStatInterval] = 1;
-            st[kStatShadow] = shadow;
-            st[kStatNodes] = cn.nodes;
-            st[kStatTris] = cn.triangles;
-            st[kStatInst] = cn.instances;
-            if (supported) {
-                bool terminates = terminal || hit.tri != lux::kEmpty;
-                V.count[base + e] = 1u;
-                V.accum[base + e] = terminates ? make_float4(radiance.x, radiance.y, radiance.z, 0.0f)
-                                               : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
+            if (ray_radiance(V, (uint32_t)e, radiance)) {
+                bool terminates = terminal || V.ray_h[e].x != lux::kEmpty;
+                V.count[e] = 1u;
+                V.accum[e] = terminates ? make_float4(radiance.x, radiance.y, radiance.z, 0.0f)
+                                        : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
                 st[kStatDeposits] = 1;
             } else {
                 st[kStatUnsupported] = 1;
@@ -611,6 +798,16 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.tables, (size_t)d.max_cells * 36 * sizeof(float4)},
         {(void **)&D.error_flags, sizeof(uint32_t) * 4},
         {(void **)&D.stats, 8 * sizeof(unsigned long long)},
+        {(void **)&D.ray_o, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ray_d, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ray_h, (size_t)d.max_rays * sizeof(uint4)},
+        {(void **)&D.ray_base, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.slot_query, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
+        {(void **)&D.slot_contrib, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.queue_o, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.queue_d, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
+        {(void **)&D.queue_count, 16},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
@@ -627,8 +824,10 @@ static lux_status view_alloc(LuxView *v) {
 extern "C" lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out) {
     if (!ctx || !desc || !out) return LUX_ERR_INVALID_ARGUMENT;
     *out = nullptr;
-    if (desc->max_receivers == 0 || desc->max_cells == 0 || desc->max_entries == 0)
+    if (desc->max_receivers == 0 || desc->max_cells == 0 || desc->max_entries == 0 || desc->max_rays == 0)
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: capacities must be positive");
+    if ((uint64_t)desc->max_rays * lux::kMaxNeeSamples > 0xffffffffull)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_rays above 2^28");
     if (desc->max_cells > (1u << 30))
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_cells above 2^30");
     LuxView *v = new LuxView();
@@ -648,6 +847,8 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     ViewDevice &D = v->dev;
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
+                    D.ray_o, D.ray_d, D.ray_h, D.ray_base, D.slot_query, D.slot_contrib, D.queue_o, D.queue_d,
+                    D.queue_result, D.queue_count,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -667,6 +868,8 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
     F.receivers = receivers;
     F.dir_capacity = v->dir_capacity;
     F.cell_capacity = v->desc.max_cells;
+    F.ray_capacity = v->desc.max_rays;
+    F.queue_capacity = v->desc.max_rays * lux::kMaxNeeSamples;
     F.entry_capacity = v->desc.max_entries;
     for (uint32_t l = 0; l < s.levels; ++l) {
         F.spacing[l] = s.probe_spacing * (float)(1u << l);
@@ -694,8 +897,8 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: missing receiver buffers");
     FrameParams F;
     make_params(v, settings, rc->count, F);
-    if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > 0xffffffffull)
-        return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: ray count exceeds 2^32");
+    if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > v->desc.max_rays)
+        return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: receivers x rays_per_receiver exceeds max_rays");
     const ViewDevice &D = v->dev;
     cudaStream_t st = ctx->stream;
     const int grid = ctx->sm_count * 8;
@@ -716,9 +919,18 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     mark(1);
     if (F.layout == LUX_LAYOUT_SPLIT) {
         uint32_t rays = rc->count * F.rays_per_receiver;
-        if (rays) trace_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, pos, nrm, rays);
+        if (rays) {
+            closest_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, pos, nrm, rays);
+            shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, rays, false);
+            shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view);
+            deposit_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, nrm, rays);
+        }
     } else {
-        for (uint32_t l = 0; l < F.levels; ++l) trace_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
+        for (uint32_t l = 0; l < F.levels; ++l)
+            closest_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
+        shade_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, F.ray_capacity, true);
+        shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view);
+        deposit_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F);
     }
     mark(2);
     for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);

@@ -192,17 +192,21 @@ def arch_mesh(span: float, thickness: float, depth: float, segments: int) -> Mes
     return Mesh(np.array(v, dtype=np.float32), np.array(tri, dtype=np.uint32))
 
 
-def grid_mesh(nx: int, nz: int, size_x: float, size_z: float, y: float, rng, jitter: float) -> Mesh:
+def grid_mesh(quads: int, size_x: float, size_z: float, y: float, rng, jitter: float) -> Mesh:
+    """`quads` quads of a near-square row-major grid (the last row may be
+    partial), facing -y, vertex heights jittered by U[-jitter, jitter]."""
+    nx = max(1, int(math.ceil(math.sqrt(quads))))
+    nz = (quads + nx - 1) // nx
     xs = np.linspace(-size_x * 0.5, size_x * 0.5, nx + 1)
     zs = np.linspace(-size_z * 0.5, size_z * 0.5, nz + 1)
     v = np.array([(x, y, z) for z in zs for x in xs], dtype=np.float64)
     v[:, 1] += rng.uniform(-jitter, jitter, size=len(v))
     tri = []
-    for j in range(nz):
-        for i in range(nx):
-            a = j * (nx + 1) + i
-            b, c, d = a + 1, a + nx + 2, a + nx + 1
-            tri += [[a, c, b], [a, d, c]]  # normal -y (ceiling seen from below)
+    for q in range(quads):
+        j, i = divmod(q, nx)
+        a = j * (nx + 1) + i
+        b, c, d = a + 1, a + nx + 2, a + nx + 1
+        tri += [[a, c, b], [a, d, c]]  # normal -y (ceiling seen from below)
     return Mesh(v.astype(np.float32), np.array(tri, dtype=np.uint32))
 
 
@@ -219,8 +223,10 @@ def atrium(seed: int = 2, triangles: int = 262_144) -> SceneDesc:
     arch = sc.add_mesh(arch_mesh(4.0, 0.4, 0.6, 60))               # 60*4*2 = 480
     tile = sc.add_mesh(box_mesh((0.98, 0.05, 0.98), bottom=False))  # 10
     emitter_mesh = sc.add_mesh(quad((-1.0, 0.0, -1.0), (1.0, 0.0, -1.0), (1.0, 0.0, 1.0), (-1.0, 0.0, 1.0)))
-    # Columns on a 10 x 10 grid with 4 m pitch.
-    pitch, n = 4.0, 10
+    # Columns on an n x n grid with 4 m pitch (10 x 10 at full size).
+    large = triangles >= 200_000
+    pitch, n = 4.0, (10 if large else 4)
+    tiles = 40 if large else 16
     for i in range(n):
         for j in range(n):
             t = np.eye(3, 4, dtype=np.float64)
@@ -233,29 +239,25 @@ def atrium(seed: int = 2, triangles: int = 262_144) -> SceneDesc:
             cz = (j - (n - 1) / 2) * pitch
             sc.add_instance(arch, rotation_y(0.0, (cx, 6.0, cz)) + _jit3(jit), material=albedo_material())
             sc.add_instance(arch, rotation_y(math.pi / 2, (cz, 6.0, cx)) + _jit3(jit), material=albedo_material())
-    # Floor tiles, 1 m pitch over 40 x 40 m.
-    for i in range(40):
-        for j in range(40):
+    # Floor tiles, 1 m pitch (40 x 40 m at full size).
+    for i in range(tiles):
+        for j in range(tiles):
             t = np.eye(3, 4, dtype=np.float64)
-            t[:, 3] = (i - 19.5, -0.05, j - 19.5) + jit()
+            t[:, 3] = (i - (tiles - 1) / 2, -0.05, j - (tiles - 1) / 2) + jit()
             sc.add_instance(tile, t, material=albedo_material())
     # Three emitters under the ceiling, radiance U[5, 20].
     for k in range(3):
         radiance = float(rng.uniform(5.0, 20.0))
         mat = sc.add_material(material_words((0.0, 0.0, 0.0), emission=(radiance, radiance, radiance)))
         t = np.eye(3, 4, dtype=np.float64)  # the quad faces -y
-        t[:, 3] = ((k - 1) * 12.0, 9.5, rng.uniform(-6.0, 6.0))
+        t[:, 3] = ((k - 1) * pitch * n * 0.3, 9.5, rng.uniform(-0.15, 0.15) * pitch * n)
         sc.add_instance(emitter_mesh, t, material=mat)
     # Coffered ceiling fills the remaining triangle budget exactly.
     remaining = triangles - sc.world_triangles()
     if remaining < 2 or remaining % 2:
         raise ValueError(f"atrium triangle budget {triangles} cannot be met (remaining {remaining})")
-    quads = remaining // 2
-    nx = int(math.sqrt(quads))
-    while quads % nx:
-        nx -= 1
-    nz = quads // nx
-    ceiling = sc.add_mesh(grid_mesh(nx, nz, 44.0, 44.0, 10.0, rng, 0.02))
+    extent = pitch * n + 4.0
+    ceiling = sc.add_mesh(grid_mesh(remaining // 2, extent, extent, 10.0, rng, 0.02))
     sc.add_instance(ceiling, material=albedo_material())
     assert sc.world_triangles() == triangles, (sc.world_triangles(), triangles)
     return sc

@@ -157,12 +157,15 @@ typedef struct LuxStats {
 #define LUX_VIEW_ERR_CELL_CAPACITY 1u
 #define LUX_VIEW_ERR_ENTRY_CAPACITY 2u
 #define LUX_VIEW_ERR_PROBE_LOOKUP 4u
+#define LUX_VIEW_ERR_RAY_CAPACITY 8u
 
 /* Capacities of a view (ViewBuffers, src/render.rs:5077-5160). */
 typedef struct LuxViewDesc {
     uint32_t max_receivers;  /* receivers (Split) or cascade-0 probes (Dense) */
     uint32_t max_cells;      /* distinct world cells per level */
     uint64_t max_entries;    /* (cell, direction) records summed over levels */
+    uint32_t max_rays;       /* interval rays per frame: receivers x rays_per_receiver (Split) or records (Dense) */
+    uint32_t reserved;
 } LuxViewDesc;
 
 /* ---- library / context ---------------------------------------------- */

@@ -66,6 +66,7 @@ def lib():
             "orc_frame_read_probes": (None, [P, P]),
             "orc_frame_stats": (None, [P, P]),
             "orc_frame_resolve": (None, [P, P, P, U, P]),
+            "orc_resolve_tables": (None, [P, U, P, F, P, P, U, P]),
             "orc_deposit_levels": (U, [P, F, C.c_int, C.c_int, P, P]),
             "orc_merge_entry": (None, [P, U, P, P, C.c_int, P]),
             "orc_interpolate_children": (None, [P, P, P]),

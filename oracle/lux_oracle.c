@@ -1765,11 +1765,14 @@ void orc_frame_read_probes(const OrcFrame *F, float *tables) {
 void orc_frame_stats(const OrcFrame *F, LuxStats *stats) { *stats = F->stats; }
 
 /* worldResolve -> resolveSplitDiffuse -> diffuseAtLod at LOD 0
- * (shaders/world_resolve.slang:96-196, :281-313). */
-void orc_frame_resolve(const OrcFrame *F, const float *position, const float *normal_in, uint32_t count, float *out) {
-    const LuxSettings *st = &F->st;
-    const Level *L0 = &F->level[0];
-    float s0 = orc_spacing(st, 0);
+ * (shaders/world_resolve.slang:96-196, :281-313) over cascade-0 probe
+ * tables: keys int4[cells] sorted ascending, tables float4[cells*36]. */
+static void resolve_tables(const Key *keys, uint32_t cells, const float *tables, float s0, const float *position,
+                           const float *normal_in, uint32_t count, float *out) {
+    Level L0;
+    memset(&L0, 0, sizeof L0);
+    L0.cells = cells;
+    L0.keys = (Key *)keys;
     for (uint32_t i = 0; i < count; ++i) {
         const float *p = position + 4 * (size_t)i, *nn = normal_in + 4 * (size_t)i;
         float *o = out + 4 * (size_t)i;
@@ -1797,10 +1800,10 @@ void orc_frame_resolve(const OrcFrame *F, const float *position, const float *no
                 potential += w;
                 int32_t key[3] = {(int32_t)base[0] + (int32_t)bx, (int32_t)base[1] + (int32_t)by,
                                   (int32_t)base[2] + (int32_t)bz};
-                int64_t cell = find_cell(L0, key);
+                int64_t cell = find_cell(&L0, key);
                 if (cell < 0) continue;
                 float probe[4];
-                probe_page(&F->tables[(size_t)cell * 144], &lk, probe);
+                probe_page(&tables[(size_t)cell * 144], &lk, probe);
                 float support = probe[3];
                 if (!(support > 0.0f)) continue;
                 float weight = w * support;
@@ -1828,6 +1831,30 @@ void orc_frame_resolve(const OrcFrame *F, const float *position, const float *no
         /* rawGiSupportAlpha, shaders/common.slang:323-326. */
         o[3] = supported ? 1.0f + 0.25f * coverage : -1.0f;
     }
+}
+
+void orc_frame_resolve(const OrcFrame *F, const float *position, const float *normal_in, uint32_t count, float *out) {
+    resolve_tables(F->level[0].keys, F->level[0].cells, F->tables, orc_spacing(&F->st, 0), position, normal_in, count,
+                   out);
+}
+
+void orc_resolve_tables(const int32_t *keys, uint32_t cells, const float *tables, float spacing, const float *position,
+                        const float *normal, uint32_t count, float *out) {
+    Key *sorted = (Key *)malloc(sizeof(Key) * (cells ? cells : 1));
+    uint32_t *order = (uint32_t *)malloc(sizeof(uint32_t) * (cells ? cells : 1));
+    memcpy(sorted, keys, sizeof(Key) * cells);
+    for (uint32_t i = 0; i < cells; ++i) sorted[i].k[3] = (int32_t)i;
+    qsort(sorted, cells, sizeof(Key), key_cmp);
+    float *tab = (float *)malloc(sizeof(float) * 144 * (cells ? cells : 1));
+    for (uint32_t i = 0; i < cells; ++i) {
+        order[i] = (uint32_t)sorted[i].k[3];
+        memcpy(&tab[(size_t)i * 144], &tables[(size_t)order[i] * 144], sizeof(float) * 144);
+        sorted[i].k[3] = 0;
+    }
+    resolve_tables(sorted, cells, tab, spacing, position, normal, count, out);
+    free(sorted);
+    free(order);
+    free(tab);
 }
 
 /* ---- KAT helpers ---- */

@@ -98,6 +98,11 @@ void orc_frame_stats(const OrcFrame *frame, LuxStats *stats);
 void orc_frame_resolve(const OrcFrame *frame, const float *position, const float *normal,
                        uint32_t count, float *out);
 
+/* Resolve over given cascade-0 tables: keys int4[cells] (any order), tables
+ * float4[cells*36], cascade-0 spacing. */
+void orc_resolve_tables(const int32_t *keys, uint32_t cells, const float *tables, float spacing,
+                        const float *position, const float *normal, uint32_t count, float *out);
+
 /* --- stand-alone KAT entry points ------------------------------------ */
 /* deposit (shaders/split.slang:1056-1117) of one ray at `distance` with
  * radiance rgb into `levels` (J.rgb, beta) records; returns the number of

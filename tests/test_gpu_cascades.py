@@ -21,7 +21,8 @@ def by_key(keys):
 def run_frame(name, settings, pos, nrm, max_cells=1 << 16, max_entries=1 << 24):
     ctx = bp.LuxContext()
     scene = bp.GpuScene(ctx, packed(name))
-    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=max_cells, max_entries=max_entries)
+    rays = len(pos) * settings.rays_per_receiver if settings.layout == bp.LAYOUT_SPLIT else 1 << 20
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=max_cells, max_entries=max_entries, max_rays=rays)
     d_pos, d_nrm = to_device(pos), to_device(nrm)
     view.trace_merge(scene, settings, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
     st = view.stats()

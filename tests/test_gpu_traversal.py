@@ -60,7 +60,7 @@ def test_atrium_random_rays_match_oracle():
     rng = np.random.default_rng(11)
     n = 20000
     rays = np.zeros(n, dtype=bp.RAY_DTYPE)
-    rays["origin"] = rng.uniform((-19, 0.2, -19), (19, 9.5, 19), size=(n, 3)).astype(np.float32)
+    rays["origin"] = rng.uniform((-7, 0.2, -7), (7, 9.5, 7), size=(n, 3)).astype(np.float32)
     d = rng.normal(size=(n, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     rays["direction"] = d.astype(np.float32)
@@ -69,7 +69,7 @@ def test_atrium_random_rays_match_oracle():
     oscene = oracle.OracleScene.from_packed(packed(name))
     cpu, _ = oscene.trace_rays(rays)
     hit = cpu["triangle"] != EMPTY
-    assert hit.mean() > 0.9
+    assert hit.mean() > 0.5
     np.testing.assert_array_equal(gpu["triangle"], cpu["triangle"])
     np.testing.assert_array_equal(gpu["instance"], cpu["instance"])
     np.testing.assert_array_equal(gpu["distance"][hit].view(np.uint32), cpu["distance"][hit].view(np.uint32))
