@@ -283,6 +283,8 @@ def run_ours(args, rank, world):
         s.frame_index = step
         view.trace_merge(scene, s, d_rpos.data_ptr(), d_rnrm.data_ptr(), n_recv)
 
+    from bevy_penumbra_b200.autotune import autotune
+    tuned = autotune(view, lambda: frame(0))
     for step in range(args.warmup):
         frame(step)
         view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
@@ -358,6 +360,14 @@ def run_ours(args, rank, world):
                           "merge": float(np.median(merge_ms)), "pack": float(np.median(pack_ms)),
                           "resolve": float(np.median(resolve_ms))},
             "rays": {"interval": interval_rays, "shadow": int(st.shadow_rays),
+                     "per_interval_ray": {
+                         "nodes": (int(st.nodes_visited) - int(st.shadow_nodes)) / interval_rays,
+                         "triangles": (int(st.triangles_tested) - int(st.shadow_triangles)) / interval_rays,
+                         "instances": (int(st.instances_visited) - int(st.shadow_instances)) / interval_rays},
+                     "per_shadow_ray": {
+                         "nodes": int(st.shadow_nodes) / max(int(st.shadow_rays), 1),
+                         "triangles": int(st.shadow_triangles) / max(int(st.shadow_rays), 1),
+                         "instances": int(st.shadow_instances) / max(int(st.shadow_rays), 1)},
                      "trace_mrays_s": interval_rays / trace_s / 1e6,
                      "all_rays_trace_mrays_s": (interval_rays + int(st.shadow_rays)) / trace_s / 1e6},
             "roofline": {"kernel": "trace_split_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -370,6 +380,8 @@ def run_ours(args, rank, world):
                     "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
                     "d2h_bytes_per_step": int(n_pts * 16)},
             "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
+            "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
+                         "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
             "clocks": clocks.summary(),
             "setup_s": w["setup_s"],
         }

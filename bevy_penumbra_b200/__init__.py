@@ -359,6 +359,17 @@ class SplitView:
     def set_timing(self, enable: bool = True) -> None:
         self.ctx.check(lib().lux_view_set_timing(self.handle, 1 if enable else 0))
 
+    def tuning(self) -> N.LuxTuning:
+        t = N.LuxTuning()
+        self.ctx.check(lib().lux_view_get_tuning(self.handle, C.byref(t)))
+        return t
+
+    def set_tuning(self, **fields) -> None:
+        t = self.tuning()
+        for k, val in fields.items():
+            setattr(t, k, int(val))
+        self.ctx.check(lib().lux_view_set_tuning(self.handle, C.byref(t)))
+
     def timings(self) -> N.LuxTimings:
         t = N.LuxTimings()
         self.ctx.check(lib().lux_view_timings(self.handle, C.byref(t)))

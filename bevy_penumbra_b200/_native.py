@@ -75,7 +75,8 @@ class LuxStats(C.Structure):
     _fields_ = [
         ("interval_rays", C.c_uint64), ("shadow_rays", C.c_uint64), ("nodes_visited", C.c_uint64),
         ("triangles_tested", C.c_uint64), ("instances_visited", C.c_uint64), ("deposits", C.c_uint64),
-        ("unsupported", C.c_uint64), ("cells", C.c_uint32 * LUX_MAX_LEVELS),
+        ("unsupported", C.c_uint64), ("shadow_nodes", C.c_uint64), ("shadow_triangles", C.c_uint64),
+        ("shadow_instances", C.c_uint64), ("cells", C.c_uint32 * LUX_MAX_LEVELS),
         ("entries", C.c_uint64 * LUX_MAX_LEVELS), ("levels", C.c_uint32), ("error_flags", C.c_uint32),
     ]
 
@@ -88,6 +89,11 @@ class LuxViewDesc(C.Structure):
 class LuxTimings(C.Structure):
     _fields_ = [("seed_ms", C.c_float), ("trace_ms", C.c_float), ("merge_ms", C.c_float),
                 ("pack_ms", C.c_float), ("resolve_ms", C.c_float)]
+
+
+class LuxTuning(C.Structure):
+    _fields_ = [("closest_mode", C.c_uint32), ("shadow_mode", C.c_uint32), ("closest_blocks_per_sm", C.c_uint32),
+                ("shadow_blocks_per_sm", C.c_uint32), ("sort_queries", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 P = C.c_void_p
@@ -126,6 +132,8 @@ SIGNATURES = {
     "lux_view_stats": (C.c_int, [P, C.POINTER(LuxStats)]),
     "lux_view_set_timing": (C.c_int, [P, U32]),
     "lux_view_timings": (C.c_int, [P, C.POINTER(LuxTimings)]),
+    "lux_view_set_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
+    "lux_view_get_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
     "lux_view_read_level": (C.c_int, [P, U32, P, P, P, P]),
     "lux_view_read_probes": (C.c_int, [P, P, P]),
 }

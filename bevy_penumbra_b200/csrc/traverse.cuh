@@ -55,11 +55,12 @@ __device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, flo
 
 // Per-ray slab constants for the BVH4 child tests.  The reference divides
 // by the direction for every slab (shaders/traversal.slang:360-361); the
-// child tests here multiply by the reciprocal and widen the interval so the
-// test stays conservative: t = (lo - o) * inv carries at most three roundings
-// (gamma_3 < 1.8e-7 relative), and the interval grows by 7.2e-7 relative on
-// both ends, twice the reference's exit padding.  Culling only decides which
-// triangles are tested; hit distances come from the exact triangle test.
+// child tests here multiply by an approximate reciprocal (at most 2 ulp,
+// __fdividef) and widen the interval so the test stays conservative:
+// t = (lo - o) * inv then carries under 5 ulp of relative error, and the
+// interval grows by 7.2e-7 (about 6 ulp) relative on both ends.  Culling only
+// decides which triangles are tested; hit distances come from the exact
+// triangle test.
 struct SlabRay {
     float ox, oy, oz;
     float ix, iy, iz;  // 1 / d (unused on zero axes)
@@ -74,9 +75,9 @@ __device__ __forceinline__ SlabRay slab_ray(f3 o, f3 d) {
     r.zx = d.x == 0.0f;
     r.zy = d.y == 0.0f;
     r.zz = d.z == 0.0f;
-    r.ix = r.zx ? 0.0f : 1.0f / d.x;
-    r.iy = r.zy ? 0.0f : 1.0f / d.y;
-    r.iz = r.zz ? 0.0f : 1.0f / d.z;
+    r.ix = r.zx ? 0.0f : __fdividef(1.0f, d.x);
+    r.iy = r.zy ? 0.0f : __fdividef(1.0f, d.y);
+    r.iz = r.zz ? 0.0f : __fdividef(1.0f, d.z);
     return r;
 }
 
@@ -265,50 +266,93 @@ __device__ __forceinline__ void sort4(float e[4], uint32_t p[4], int n) {
 #undef LUX_CSWAP
 }
 
-// BLAS walk of one instance (traceInstance / occludedInstance).  Returns true
-// for an any-hit query that found a blocker.
+// traceRayTracked + traceInstance (kAnyHit = false) and traceOccluded +
+// occludedInstance (kAnyHit = true) as one resumable walk over one stack.  A
+// TLAS leaf enters its first instance (the rest of the leaf is pushed back);
+// the BLAS walk runs on the same stack above `blas_base` in the instance's
+// local space and returns to world space when the stack drops back to it.
+// Each step traverses inner nodes until a leaf is reached, then processes
+// that leaf (the while-while order), so the lanes of a warp stay in step and
+// a lane whose ray finished can take a new ray between steps.
+//
+// Error bits follow the reference: 4 when a walk exceeds MAX_TRAVERSAL_STEPS
+// (per TLAS walk and per instance walk), 2 / 1 when the stack is exhausted in
+// the TLAS / a BLAS, after which the walk continues over every instance / every
+// triangle of the instance in order (shaders/traversal.slang:498-517, :729-745).
 template <bool kAnyHit>
-__device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, float tmin, Hit &hit,
-                               TraceCounters &cn) {
-    DeviceInstance I = load_instance(S.instances, inst);
-    f3 lo, ld;
-    local_ray(I, o, d, lo, ld);
-    cn.instances++;
-    TriRay ray = triangle_ray(ld);
-    SlabRay sr = slab_ray(lo, ld);
+struct Walker {
+    Hit hit;
+    f3 o, d, lo, ld;
+    float tmin, lower;
+    SlabRay world, r;
+    TriRay world_tri, tri_ray;
+    uint32_t inst, inst_flags, inst_first, inst_count;
+    int blas_base;        // stack depth at instance entry; -1 = TLAS space
+    uint32_t tlas_next;   // TLAS fallback: next instance to scan in order
+    uint32_t blas_next;   // BLAS fallback: next triangle to scan in order
+    uint32_t tlas_steps, blas_steps;
     uint32_t stack_p[kStack];
     float stack_t[kStack];
-    int sp = 0;
-    uint32_t cur = I.root;
-    bool ready = true;
-    uint32_t steps = 0;
-    const float lower = fmaxf(tmin, 0.000025f);
-    while (true) {
-        if (!ready) {
-            while (sp > 0) {
-                --sp;
-                if (!kAnyHit && stack_t[sp] > hit.t) continue;
-                cur = stack_p[sp];
-                ready = true;
+    int sp;
+    uint32_t cur;
+    float cur_t;
+    bool have;
+
+    // Returns false when the query is already complete (no instances, or the
+    // ray misses the TLAS root box: traceRayTracked's early exits).
+    __device__ __forceinline__ bool start(const SceneView &S, f3 origin, f3 direction, float t_min, float limit) {
+        hit.t = limit;
+        hit.tri = kEmpty;
+        hit.inst = kEmpty;
+        hit.errors = 0;
+        hit.b1 = 0.0f;
+        hit.b2 = 0.0f;
+        if (S.instance_count == 0) return false;
+        float re, rx;
+        if (!box_interval(origin, direction, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1],
+                          S.root_hi[2], limit, re, rx))
+            return false;
+        o = origin;
+        d = direction;
+        tmin = t_min;
+        lower = fmaxf(t_min, 0.000025f);
+        world = slab_ray(o, d);
+        r = world;
+        world_tri = triangle_ray(d);
+        lo = o;
+        ld = d;
+        inst = kEmpty;
+        inst_flags = inst_first = inst_count = 0;
+        blas_base = -1;
+        tlas_next = blas_next = kEmpty;
+        tlas_steps = blas_steps = 0;
+        sp = 0;
+        cur = S.tlas_root;
+        cur_t = 0.0f;
+        have = true;
+        return true;
+    }
+
+    // One step: inner nodes down to a leaf, that leaf, then the next pending
+    // entry.  Returns true when the query is complete.
+    __device__ __forceinline__ bool step(const SceneView &S, TraceCounters &cn) {
+        while (have && (cur & kLeafBit) == 0u) {
+            uint32_t &steps = blas_base < 0 ? tlas_steps : blas_steps;
+            if (++steps > kMaxSteps) {
+                hit.errors |= kQueryUnsupported;
+                if (blas_base < 0) return true;  // abandon the whole query
+                sp = blas_base;                  // abandon this instance
+                have = false;
                 break;
             }
-            if (!ready) break;
-        }
-        ready = false;
-        if (++steps > kMaxSteps) {
-            hit.errors |= kQueryUnsupported;
-            return false;
-        }
-        uint32_t first, count;
-        if (cur & kLeafBit) {
-            first = cur & kLeafFirstMask;
-            count = ((cur >> 27) & 15u) + 1u;
-        } else {
             float entry[4];
             uint32_t child[4];
             cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, sr, hit.t, tmin, entry, child);
-            if (mask == 0u) continue;
+            uint32_t mask = node_test(S.nodes, cur, r, hit.t, tmin, entry, child);
+            if (mask == 0u) {
+                have = false;
+                break;
+            }
             float e[4];
             uint32_t p[4];
             int n = 0;
@@ -321,13 +365,17 @@ __device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, fl
                 }
             sort4(e, p, n);
             if (sp + n - 1 > kStack) {
-                // Stack exhausted: scan the instance's whole range and flag it
-                // (traceInstance fallback, shaders/traversal.slang:512-517).
-                hit.errors |= 1u;
-                sp = 0;
-                first = I.first;
-                count = I.count;
-                goto scan;
+                if (blas_base < 0) {
+                    hit.errors |= 2u;
+                    sp = 0;
+                    tlas_next = 0;
+                } else {
+                    hit.errors |= 1u;
+                    sp = blas_base;
+                    blas_next = inst_first;
+                }
+                have = false;
+                break;
             }
             for (int k = n - 1; k >= 1; --k) {
                 stack_p[sp] = p[k];
@@ -335,118 +383,165 @@ __device__ bool trace_instance(const SceneView &S, f3 o, f3 d, uint32_t inst, fl
                 ++sp;
             }
             cur = p[0];
-            ready = true;
-            continue;
+            cur_t = e[0];
         }
-    scan:
-        for (uint32_t t = first; t < first + count; ++t) {
-            f3 A, B, C;
-            load_triangle(S.triangles, t, A, B, C);
-            cn.triangles++;
-            if (cull_reject(I.flags, A, B, C, ld)) continue;
-            float w1 = 0.0f, w2 = 0.0f;
-            float dist = intersect_triangle(lo, ld, ray, A, B, C, w1, w2);
-            if (kAnyHit) {
-                if (dist > 0.000025f && dist < hit.t) {
-                    hit.tri = t;
-                    hit.inst = inst;
-                    return true;
+        if (have) {
+            uint32_t first = cur & kLeafFirstMask;
+            uint32_t count = ((cur >> 27) & 15u) + 1u;
+            have = false;
+            if (blas_base < 0) {
+                // TLAS leaf: enter its first instance; the rest waits on the stack.
+                if (count > 1u) {
+                    if (sp < kStack) {
+                        stack_p[sp] = kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27);
+                        stack_t[sp] = cur_t;
+                        ++sp;
+                    } else {
+                        // Stack exhausted: after this instance, scan every instance.
+                        hit.errors |= 2u;
+                        sp = 0;
+                        tlas_next = 0;
+                    }
                 }
-            } else if (dist > lower && hit_better(dist, inst, t, hit)) {
-                hit.t = dist;
-                hit.tri = t;
-                hit.inst = inst;
-                hit.b1 = w1;
-                hit.b2 = w2;
+                DeviceInstance I = load_instance(S.instances, first);
+                local_ray(I, o, d, lo, ld);
+                cn.instances++;
+                // A local direction bit-identical to the world direction
+                // (translation-only instances) reuses the world constants.
+                if (as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) && as_uint(ld.z) == as_uint(d.z)) {
+                    r = world;
+                    r.ox = lo.x;
+                    r.oy = lo.y;
+                    r.oz = lo.z;
+                    tri_ray = world_tri;
+                } else {
+                    r = slab_ray(lo, ld);
+                    tri_ray = triangle_ray(ld);
+                }
+                inst = first;
+                inst_flags = I.flags;
+                inst_first = I.first;
+                inst_count = I.count;
+                blas_base = sp;
+                blas_steps = 0;
+                cur = I.root;
+                cur_t = 0.0f;
+                have = true;
+                return false;
+            }
+            // BLAS leaf (traceTriangle / occludedTriangle).
+            if (++blas_steps > kMaxSteps) {
+                hit.errors |= kQueryUnsupported;
+                sp = blas_base;
+            } else {
+                for (uint32_t t = first; t < first + count; ++t) {
+                    f3 A, B, C;
+                    load_triangle(S.triangles, t, A, B, C);
+                    cn.triangles++;
+                    if (cull_reject(inst_flags, A, B, C, ld)) continue;
+                    float w1 = 0.0f, w2 = 0.0f;
+                    float dist = intersect_triangle(lo, ld, tri_ray, A, B, C, w1, w2);
+                    if (kAnyHit) {
+                        if (dist > 0.000025f && dist < hit.t) {
+                            // Any accepted blocker is a complete proof
+                            // (shaders/traversal.slang:786-792, :1035-1040).
+                            hit.tri = t;
+                            hit.inst = inst;
+                            hit.errors &= ~kQueryUnsupported;
+                            return true;
+                        }
+                    } else if (dist > lower && hit_better(dist, inst, t, hit)) {
+                        hit.t = dist;
+                        hit.tri = t;
+                        hit.inst = inst;
+                        hit.b1 = w1;
+                        hit.b2 = w2;
+                    }
+                }
             }
         }
+        // The next pending entry, leaving instances and fallbacks as needed.
+        while (!have) {
+            if (blas_base >= 0 && sp == blas_base) {
+                if (blas_next != kEmpty && blas_next < inst_first + inst_count) {
+                    uint32_t c = min(kLeafMaxCount, inst_first + inst_count - blas_next);
+                    cur = kLeafBit | (blas_next & kLeafFirstMask) | ((c - 1u) << 27);
+                    blas_next += c;
+                    have = true;
+                    break;
+                }
+                blas_next = kEmpty;
+                blas_base = -1;
+                r = world;
+                inst = kEmpty;
+                continue;
+            }
+            if (sp == 0) {
+                if (tlas_next != kEmpty && tlas_next < S.instance_count) {
+                    cur = kLeafBit | (tlas_next & kLeafFirstMask);
+                    ++tlas_next;
+                    have = true;
+                    break;
+                }
+                return true;
+            }
+            --sp;
+            if (!kAnyHit && stack_t[sp] > hit.t) continue;
+            cur = stack_p[sp];
+            cur_t = stack_t[sp];
+            have = true;
+        }
+        return false;
     }
-    return false;
-}
+};
 
-// traceRayTracked (kAnyHit = false) / traceOccluded (kAnyHit = true).
 template <bool kAnyHit>
 __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, Hit &hit, TraceCounters &cn) {
-    hit.t = limit;
-    hit.tri = kEmpty;
-    hit.inst = kEmpty;
-    hit.errors = 0;
-    hit.b1 = 0.0f;
-    hit.b2 = 0.0f;
-    if (S.instance_count == 0) return;
-    float re, rx;
-    if (!box_interval(o, d, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1], S.root_hi[2],
-                      limit, re, rx))
-        return;
-    SlabRay sr = slab_ray(o, d);
-    uint32_t stack_p[kStack];
-    float stack_t[kStack];
-    int sp = 0;
-    uint32_t cur = S.tlas_root;
-    bool ready = true;
-    uint32_t steps = 0;
+    Walker<kAnyHit> w;
+    if (w.start(S, o, d, tmin, limit))
+        while (!w.step(S, cn)) {
+        }
+    hit = w.hit;
+}
+
+// Persistent warp loop with per-lane refill: whenever lanes are idle, the
+// warp takes that many new rays from `counter` (one atomic per refill) and
+// keeps stepping until the counter passes `n` and every lane is done.
+// gen(id, o, d, tmin, limit) produces ray `id`; done(id, hit) consumes it.
+template <bool kAnyHit, typename Gen, typename Done>
+__device__ void trace_persistent(const SceneView &S, uint32_t *counter, uint32_t n, Gen &&gen, Done &&done,
+                                 TraceCounters &cn) {
+    const uint32_t lane = threadIdx.x & 31u;
+    Walker<kAnyHit> w;
+    bool active = false;
+    bool exhausted = false;  // the counter passed n: no further rays for this warp
+    uint32_t id = 0;
     while (true) {
-        if (!ready) {
-            while (sp > 0) {
-                --sp;
-                if (!kAnyHit && stack_t[sp] > hit.t) continue;
-                cur = stack_p[sp];
-                ready = true;
-                break;
-            }
-            if (!ready) break;
-        }
-        ready = false;
-        if (++steps > kMaxSteps) {
-            hit.errors |= kQueryUnsupported;
-            break;
-        }
-        uint32_t first, count;
-        if (cur & kLeafBit) {
-            first = cur & kLeafFirstMask;
-            count = ((cur >> 27) & 15u) + 1u;
-        } else {
-            float entry[4];
-            uint32_t child[4];
-            cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, sr, hit.t, tmin, entry, child);
-            if (mask == 0u) continue;
-            float e[4];
-            uint32_t p[4];
-            int n = 0;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (mask & (1u << i)) {
-                    e[n] = entry[i];
-                    p[n] = child[i];
-                    ++n;
+        uint32_t need = __ballot_sync(0xffffffffu, !active && !exhausted);
+        if (need) {
+            uint32_t leader = __ffs(need) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base + (uint32_t)__popc(need) > n) exhausted = true;  // uniform across the warp
+            if (!active && (need & (1u << lane))) {
+                id = base + (uint32_t)__popc(need & ((1u << lane) - 1u));
+                if (id < n) {
+                    f3 o, d;
+                    float tmin, limit;
+                    gen(id, o, d, tmin, limit);
+                    active = w.start(S, o, d, tmin, limit);
+                    if (!active) done(id, w.hit);
                 }
-            sort4(e, p, n);
-            if (sp + n - 1 > kStack) {
-                // traceRayTracked fallback, shaders/traversal.slang:742-745.
-                hit.errors |= 2u;
-                sp = 0;
-                first = 0;
-                count = S.instance_count;
-                goto scan;
             }
-            for (int k = n - 1; k >= 1; --k) {
-                stack_p[sp] = p[k];
-                stack_t[sp] = e[k];
-                ++sp;
-            }
-            cur = p[0];
-            ready = true;
+        }
+        if (!__any_sync(0xffffffffu, active)) {
+            if (exhausted) break;
             continue;
         }
-    scan:
-        for (uint32_t i = first; i < first + count; ++i) {
-            if (trace_instance<kAnyHit>(S, o, d, i, tmin, hit, cn)) {
-                // Any accepted blocker is a complete proof
-                // (shaders/traversal.slang:786-792, :1035-1040).
-                hit.errors &= ~kQueryUnsupported;
-                return;
-            }
+        if (active && w.step(S, cn)) {
+            done(id, w.hit);
+            active = false;
         }
     }
 }

@@ -73,19 +73,25 @@ struct ViewDevice {
     float4 *queue_d;                // query direction
     uint8_t *queue_result;          // 0 visible, 1 blocked, 2 unsupported
     uint32_t *queue_count;
+    uint32_t *work_counter;         // [2] persistent-warp ray fetch: closest, shadow
 };
 
 constexpr int kStatInterval = 0, kStatShadow = 1, kStatNodes = 2, kStatTris = 3, kStatInst = 4, kStatDeposits = 5,
-              kStatUnsupported = 6;
+              kStatUnsupported = 6, kStatShadowNodes = 7, kStatShadowTris = 8, kStatShadowInst = 9;
+constexpr int kStats = 10;
 
-__device__ __forceinline__ void add_stats(unsigned long long *stats, unsigned long long v[7]) {
+__device__ __forceinline__ void add_stats(unsigned long long *stats, unsigned long long v[7],
+                                          const unsigned long long *extra = nullptr) {
+    unsigned long long w[kStats];
 #pragma unroll
-    for (int k = 0; k < 7; ++k)
-        for (int off = 16; off > 0; off >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], off);
+    for (int k = 0; k < kStats; ++k) w[k] = k < 7 ? v[k] : (extra ? extra[k - 7] : 0ull);
+#pragma unroll
+    for (int k = 0; k < kStats; ++k)
+        for (int off = 16; off > 0; off >>= 1) w[k] += __shfl_down_sync(0xffffffffu, w[k], off);
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-        for (int k = 0; k < 7; ++k)
-            if (v[k]) atomicAdd(&stats[k], v[k]);
+        for (int k = 0; k < kStats; ++k)
+            if (w[k]) atomicAdd(&stats[k], w[k]);
     }
 }
 
@@ -129,10 +135,12 @@ __global__ void clear_kernel(ViewDevice V, FrameParams F) {
         V.cell_count[threadIdx.x] = 0;
         V.level_base[threadIdx.x] = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x < 8) V.stats[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 16) V.stats[threadIdx.x] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *V.error_flags = 0;
         *V.queue_count = 0;
+        V.work_counter[0] = 0;
+        V.work_counter[1] = 0;
     }
 }
 
@@ -274,28 +282,74 @@ __device__ __forceinline__ void load_ray(const ViewDevice &V, uint32_t ray, f3 &
     h.b2 = lux::as_float(c.w);
 }
 
+// Persistent warps with per-lane refill (lux::trace_persistent).
+__global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V, FrameParams F, SceneView S,
+                                                            const float4 *__restrict__ pos,
+                                                            const float4 *__restrict__ nrm, uint32_t ray_count) {
+    if (*V.error_flags) return;
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    lux::trace_persistent<false>(
+        S, &V.work_counter[0], ray_count,
+        [&](uint32_t ray, f3 &o, f3 &d, float &tmin, float &limit) {
+            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+            float4 p4 = pos[i], n4 = nrm[i];
+            f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+            float u, v;
+            split_direction(F, i, k, n, d, u, v);
+            o = lux::ray_offset(p, n, F.shade.normal_bias);
+            tmin = 0.0f;
+            limit = 1e20f;
+            V.ray_o[ray] = make_float4(o.x, o.y, o.z, 0.0f);
+            V.ray_d[ray] = make_float4(d.x, d.y, d.z, 0.0f);
+        },
+        [&](uint32_t ray, const lux::Hit &h) {
+            V.ray_o[ray].w = h.t;
+            V.ray_d[ray].w = h.b1;
+            V.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
+            st[kStatInterval] += 1;
+        },
+        cn);
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
+    add_stats(V.stats, st);
+}
+
+// Persistent warps, 32 consecutive rays per fetch (one atomic per warp).
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter) {
+    uint32_t base = 0;
+    if ((threadIdx.x & 31u) == 0u) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
 __global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                             const float4 *__restrict__ pos,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
+    if (*V.error_flags) return;
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
-    uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x;
-    if (*V.error_flags == 0u && ray < ray_count) {
-        uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
-        float4 p4 = pos[i], n4 = nrm[i];
-        f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
-        f3 dir;
-        float u, v;
-        split_direction(F, i, k, n, dir, u, v);
-        f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
-        lux::TraceCounters cn{0, 0, 0};
-        lux::Hit hit;
-        lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
-        store_ray(V, ray, origin, dir, hit);
-        st[kStatInterval] = 1;
-        st[kStatNodes] = cn.nodes;
-        st[kStatTris] = cn.triangles;
-        st[kStatInst] = cn.instances;
+    lux::TraceCounters cn{0, 0, 0};
+    while (true) {
+        uint32_t base = warp_fetch(&V.work_counter[0]);
+        if (base >= ray_count) break;
+        uint32_t ray = base + (threadIdx.x & 31u);
+        if (ray < ray_count) {
+            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+            float4 p4 = pos[i], n4 = nrm[i];
+            f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+            f3 dir;
+            float u, v;
+            split_direction(F, i, k, n, dir, u, v);
+            f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
+            lux::Hit hit;
+            lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
+            store_ray(V, ray, origin, dir, hit);
+            st[kStatInterval] += 1;
+        }
     }
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
     add_stats(V.stats, st);
 }
 
@@ -398,26 +452,54 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
 
 // Visibility queries, one per lane (traceVisibility, shaders/split.slang:1326-1339).
 // result: 0 visible, 1 blocked, 2 unsupported.
+__global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameParams F, SceneView S) {
+    if (*V.error_flags) return;
+    uint32_t n = min(*V.queue_count, F.queue_capacity);
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    lux::trace_persistent<true>(
+        S, &V.work_counter[1], n,
+        [&](uint32_t qi, f3 &o, f3 &d, float &tmin, float &limit) {
+            float4 a = V.queue_o[qi], b = V.queue_d[qi];
+            o = f3{a.x, a.y, a.z};
+            d = f3{b.x, b.y, b.z};
+            tmin = 0.0f;
+            limit = a.w;
+        },
+        [&](uint32_t qi, const lux::Hit &sh) {
+            V.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            st[kStatShadow] += 1;
+        },
+        cn);
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
+    unsigned long long extra[3] = {cn.nodes, cn.triangles, cn.instances};
+    add_stats(V.stats, st, extra);
+}
+
 __global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
     uint32_t n = min(*V.queue_count, F.queue_capacity);
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        uint32_t qi = base + threadIdx.x;
-        unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    while (true) {
+        uint32_t base = warp_fetch(&V.work_counter[1]);
+        if (base >= n) break;
+        uint32_t qi = base + (threadIdx.x & 31u);
         if (qi < n) {
             float4 a = V.queue_o[qi], b = V.queue_d[qi];
-            lux::TraceCounters cn{0, 0, 0};
             lux::Hit sh;
             lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
-            uint8_t r = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
-            V.queue_result[qi] = r;
-            st[kStatShadow] = 1;
-            st[kStatNodes] = cn.nodes;
-            st[kStatTris] = cn.triangles;
-            st[kStatInst] = cn.instances;
+            V.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            st[kStatShadow] += 1;
         }
-        add_stats(V.stats, st);
     }
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
+    unsigned long long extra[3] = {cn.nodes, cn.triangles, cn.instances};
+    add_stats(V.stats, st, extra);
 }
 
 // Next-event sum in sample order; false when the ray's query is unsupported.
@@ -762,6 +844,7 @@ constexpr int kTimingEvents = 7;
 
 struct LuxView {
     LuxContext *ctx = nullptr;
+    LuxTuning tuning{0, 0, 8, 8, 0, {0, 0, 0}};
     bool timing = false;
     cudaEvent_t ev[kTimingEvents] = {};
     LuxViewDesc desc{};
@@ -797,7 +880,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.raw, (size_t)d.max_entries * sizeof(float4)},
         {(void **)&D.tables, (size_t)d.max_cells * 36 * sizeof(float4)},
         {(void **)&D.error_flags, sizeof(uint32_t) * 4},
-        {(void **)&D.stats, 8 * sizeof(unsigned long long)},
+        {(void **)&D.stats, 16 * sizeof(unsigned long long)},
         {(void **)&D.ray_o, (size_t)d.max_rays * sizeof(float4)},
         {(void **)&D.ray_d, (size_t)d.max_rays * sizeof(float4)},
         {(void **)&D.ray_h, (size_t)d.max_rays * sizeof(uint4)},
@@ -808,6 +891,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.queue_d, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
         {(void **)&D.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
         {(void **)&D.queue_count, 16},
+        {(void **)&D.work_counter, 16},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
@@ -816,7 +900,7 @@ static lux_status view_alloc(LuxView *v) {
         }
     }
     cudaMemsetAsync(D.error_flags, 0, 16, ctx->stream);
-    cudaMemsetAsync(D.stats, 0, 64, ctx->stream);
+    cudaMemsetAsync(D.stats, 0, 128, ctx->stream);
     cudaMemsetAsync(D.cell_count, 0, L * 4, ctx->stream);
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "view allocation");
 }
@@ -848,7 +932,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
                     D.ray_o, D.ray_d, D.ray_h, D.ray_base, D.slot_query, D.slot_contrib, D.queue_o, D.queue_d,
-                    D.queue_result, D.queue_count,
+                    D.queue_result, D.queue_count, D.work_counter,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -920,16 +1004,25 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     if (F.layout == LUX_LAYOUT_SPLIT) {
         uint32_t rays = rc->count * F.rays_per_receiver;
         if (rays) {
-            closest_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, pos, nrm, rays);
+            const LuxTuning &T = v->tuning;
+            if (T.closest_mode == 1)
+                closest_split_refill_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
+                    D, F, scene->view, pos, nrm, rays);
+            else
+                closest_split_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(D, F, scene->view, pos,
+                                                                                             nrm, rays);
             shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, rays, false);
-            shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view);
+            if (T.shadow_mode == 1)
+                shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
+            else
+                shadow_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
             deposit_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, nrm, rays);
         }
     } else {
         for (uint32_t l = 0; l < F.levels; ++l)
             closest_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
         shade_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, F.ray_capacity, true);
-        shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view);
+        shadow_kernel<<<ctx->sm_count * v->tuning.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
         deposit_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F);
     }
     mark(2);
@@ -1019,7 +1112,7 @@ extern "C" lux_status lux_view_stats(LuxView *v, LuxStats *out) {
     cudaStream_t st = v->ctx->stream;
     lux_status s = lux_cuda_check(v->ctx, (int)cudaStreamSynchronize(st), "stats");
     if (s != LUX_OK) return s;
-    unsigned long long stats[8];
+    unsigned long long stats[16];
     uint32_t counts[LUX_MAX_LEVELS];
     uint32_t flags = 0;
     cudaMemcpy(stats, v->dev.stats, sizeof stats, cudaMemcpyDeviceToHost);
@@ -1033,6 +1126,9 @@ extern "C" lux_status lux_view_stats(LuxView *v, LuxStats *out) {
     out->instances_visited = stats[kStatInst];
     out->deposits = stats[kStatDeposits];
     out->unsupported = stats[kStatUnsupported];
+    out->shadow_nodes = stats[kStatShadowNodes];
+    out->shadow_triangles = stats[kStatShadowTris];
+    out->shadow_instances = stats[kStatShadowInst];
     out->levels = v->last.levels;
     for (uint32_t l = 0; l < v->last.levels; ++l) {
         out->cells[l] = counts[l];
@@ -1099,5 +1195,20 @@ extern "C" lux_status lux_view_timings(LuxView *v, LuxTimings *out) {
     out->merge_ms = ms[2];
     out->pack_ms = ms[3];
     out->resolve_ms = ms[4];
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_set_tuning(LuxView *v, const LuxTuning *t) {
+    if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
+    if (t->closest_mode > 1 || t->shadow_mode > 1 || t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 ||
+        t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64)
+        return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_tuning: value out of range");
+    v->tuning = *t;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_get_tuning(const LuxView *v, LuxTuning *t) {
+    if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
+    *t = v->tuning;
     return LUX_OK;
 }

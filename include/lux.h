@@ -148,6 +148,9 @@ typedef struct LuxStats {
     uint64_t instances_visited; /* instance transforms applied */
     uint64_t deposits;          /* (level, entry) samples deposited */
     uint64_t unsupported;       /* rays whose query was unsupported */
+    uint64_t shadow_nodes;      /* of nodes_visited: by visibility queries */
+    uint64_t shadow_triangles;  /* of triangles_tested: by visibility queries */
+    uint64_t shadow_instances;  /* of instances_visited: by visibility queries */
     uint32_t cells[LUX_MAX_LEVELS];
     uint64_t entries[LUX_MAX_LEVELS];
     uint32_t levels;
@@ -275,6 +278,21 @@ typedef struct LuxTimings {
     float resolve_ms;  /* last lux_view_resolve */
 } LuxTimings;
 lux_status lux_view_set_timing(LuxView *view, uint32_t enable);
+
+/* Launch-shape choices of a view's trace kernels (the autotuner's knobs).
+ * closest_mode / shadow_mode: 0 = persistent warps taking 32 rays per fetch,
+ * 1 = persistent warps refilling idle lanes between traversal steps.
+ * *_blocks_per_sm: persistent blocks of 128 threads per SM (1..64). */
+typedef struct LuxTuning {
+    uint32_t closest_mode;
+    uint32_t shadow_mode;
+    uint32_t closest_blocks_per_sm;
+    uint32_t shadow_blocks_per_sm;
+    uint32_t sort_queries;        /* reserved */
+    uint32_t reserved[3];
+} LuxTuning;
+lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
+lux_status lux_view_get_tuning(const LuxView *view, LuxTuning *tuning);
 lux_status lux_view_timings(LuxView *view, LuxTimings *out);
 /* Copies one level's records to host memory (tests): cell keys int4[cells],
  * merged float4[cells*dirs] (I.rgb, support), raw float4[cells*dirs]
