@@ -29,7 +29,7 @@ from ._native import LuxError, check, lib
 
 __all__ = [
     "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
-    "LuxContext", "PackedScene", "GpuScene", "SplitView", "LuxError", "trace_rays",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "LuxError", "trace_rays", "interval_radiance",
     "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
 ]
 
@@ -313,6 +313,14 @@ def trace_rays(ctx: LuxContext, scene: GpuScene, rays_device_ptr: int, count: in
     """lux_trace_rays on device buffers of RAY_DTYPE / HIT_DTYPE records."""
     ctx.check(lib().lux_trace_rays(ctx.handle, scene.handle, rays_device_ptr, count, 1 if any_hit else 0,
                                    hits_device_ptr))
+
+
+def interval_radiance(ctx: LuxContext, scene: GpuScene, settings: RadianceCascades, rays_device_ptr: int,
+                      count: int, out_device_ptr: int) -> None:
+    """lux_interval_radiance: float4 (radiance rgb, hit distance | -1) per ray."""
+    s = settings.to_c()
+    ctx.check(lib().lux_interval_radiance(ctx.handle, scene.handle, C.byref(s), rays_device_ptr, count,
+                                          out_device_ptr))
 
 
 class SplitView:

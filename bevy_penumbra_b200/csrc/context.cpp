@@ -52,6 +52,7 @@ extern "C" lux_status lux_context_create(const LuxDeviceDesc *desc, LuxContext *
 
 extern "C" lux_status lux_context_destroy(LuxContext *ctx) {
     if (!ctx) return LUX_OK;
+    if (ctx->scratch_mem) cudaFree(ctx->scratch_mem);
     if (ctx->owns_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return LUX_OK;

@@ -54,13 +54,66 @@ struct SceneView {
     float root_lo[3], root_hi[3];   // binary TLAS root box (root test of traceRayTracked)
 };
 
+// Wavefront trace scratch (the reference's deferred-trace slots and query
+// list, shaders/common.slang:501-533): [rays] and [rays * 16] records.
+struct TraceScratch {
+    float4 *ray_o;          // origin, hit t
+    float4 *ray_d;          // direction, barycentric 1
+    uint4 *ray_h;           // triangle, instance, errors, barycentric 2 bits
+    float4 *ray_base;       // hit emission, next-event count (kEmpty: unsupported)
+    uint32_t *slot_query;   // per (ray, sample): queue index or kEmpty
+    float4 *slot_contrib;   // per (ray, sample): contribution if visible
+    float4 *queue_o;        // query origin, limit
+    float4 *queue_d;        // query direction
+    uint8_t *queue_result;  // 0 visible, 1 blocked, 2 unsupported
+    uint32_t *queue_count;
+    uint32_t *work_counter; // [2] persistent-warp ray fetch: closest, shadow
+};
+
 struct LuxContext {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool owns_stream = false;
     std::string last_error;
     int sm_count = 148;
+    // Trace scratch of lux_interval_radiance, grown on demand.
+    void *scratch_mem = nullptr;
+    uint32_t scratch_rays = 0;
 };
+
+// Carves trace scratch for `rays` rays, plus an error word and 16 statistics
+// counters, out of one 256-byte-aligned block of trace_scratch_bytes(rays) +
+// 256 bytes.  Returns the end of the carved range.
+inline unsigned char *carve_trace_scratch(unsigned char *base, uint32_t rays, TraceScratch &t, uint32_t *&error_flags,
+                                          unsigned long long *&stats) {
+    auto take = [&](size_t bytes) {
+        unsigned char *p = base;
+        base += (bytes + 255) & ~(size_t)255;
+        return p;
+    };
+    size_t r = rays, q = (size_t)rays * 16u;
+    t.ray_o = (float4 *)take(r * 16);
+    t.ray_d = (float4 *)take(r * 16);
+    t.ray_h = (uint4 *)take(r * 16);
+    t.ray_base = (float4 *)take(r * 16);
+    t.slot_query = (uint32_t *)take(q * 4);
+    t.slot_contrib = (float4 *)take(q * 16);
+    t.queue_o = (float4 *)take(q * 16);
+    t.queue_d = (float4 *)take(q * 16);
+    t.queue_result = (uint8_t *)take(q);
+    t.queue_count = (uint32_t *)take(16);
+    t.work_counter = (uint32_t *)take(16);
+    error_flags = (uint32_t *)take(16);
+    stats = (unsigned long long *)take(16 * 8);
+    return base;
+}
+
+// Bytes carve_trace_scratch consumes for `rays` rays.
+inline size_t carved_scratch_bytes(uint32_t rays) {
+    auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+    size_t r = rays, q = (size_t)rays * 16u;
+    return 4 * up(r * 16) + up(q * 4) + 3 * up(q * 16) + up(q) + 3 * up(16) + up(128);
+}
 
 struct LuxScene {
     LuxContext *ctx = nullptr;

@@ -62,18 +62,7 @@ struct ViewDevice {
     float4 *tables;                 // [cell_capacity][36]
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
-    // Wavefront trace state, [max_rays] and [max_rays * kMaxNeeSamples].
-    float4 *ray_o;                  // origin, hit t
-    float4 *ray_d;                  // direction, barycentric 1
-    uint4 *ray_h;                   // triangle, instance, errors, barycentric 2 bits
-    float4 *ray_base;               // hit emission, next-event count (kEmpty: unsupported)
-    uint32_t *slot_query;           // per (ray, sample): queue index or kEmpty
-    float4 *slot_contrib;           // per (ray, sample): contribution if visible
-    float4 *queue_o;                // query origin, limit
-    float4 *queue_d;                // query direction
-    uint8_t *queue_result;          // 0 visible, 1 blocked, 2 unsupported
-    uint32_t *queue_count;
-    uint32_t *work_counter;         // [2] persistent-warp ray fetch: closest, shadow
+    TraceScratch ts;                // wavefront trace state
 };
 
 constexpr int kStatInterval = 0, kStatShadow = 1, kStatNodes = 2, kStatTris = 3, kStatInst = 4, kStatDeposits = 5,
@@ -138,9 +127,9 @@ __global__ void clear_kernel(ViewDevice V, FrameParams F) {
     if (blockIdx.x == 0 && threadIdx.x < 16) V.stats[threadIdx.x] = 0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         *V.error_flags = 0;
-        *V.queue_count = 0;
-        V.work_counter[0] = 0;
-        V.work_counter[1] = 0;
+        *V.ts.queue_count = 0;
+        V.ts.work_counter[0] = 0;
+        V.ts.work_counter[1] = 0;
     }
 }
 
@@ -264,14 +253,14 @@ __device__ __forceinline__ void split_direction(const FrameParams &F, uint32_t i
 }
 
 __device__ __forceinline__ void store_ray(const ViewDevice &V, uint32_t ray, f3 o, f3 d, const lux::Hit &h) {
-    V.ray_o[ray] = make_float4(o.x, o.y, o.z, h.t);
-    V.ray_d[ray] = make_float4(d.x, d.y, d.z, h.b1);
-    V.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
+    V.ts.ray_o[ray] = make_float4(o.x, o.y, o.z, h.t);
+    V.ts.ray_d[ray] = make_float4(d.x, d.y, d.z, h.b1);
+    V.ts.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
 }
 
 __device__ __forceinline__ void load_ray(const ViewDevice &V, uint32_t ray, f3 &o, f3 &d, lux::Hit &h) {
-    float4 a = V.ray_o[ray], b = V.ray_d[ray];
-    uint4 c = V.ray_h[ray];
+    float4 a = V.ts.ray_o[ray], b = V.ts.ray_d[ray];
+    uint4 c = V.ts.ray_h[ray];
     o = f3{a.x, a.y, a.z};
     d = f3{b.x, b.y, b.z};
     h.t = a.w;
@@ -290,7 +279,7 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     lux::trace_persistent<false>(
-        S, &V.work_counter[0], ray_count,
+        S, &V.ts.work_counter[0], ray_count,
         [&](uint32_t ray, f3 &o, f3 &d, float &tmin, float &limit) {
             uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
             float4 p4 = pos[i], n4 = nrm[i];
@@ -300,13 +289,13 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
             o = lux::ray_offset(p, n, F.shade.normal_bias);
             tmin = 0.0f;
             limit = 1e20f;
-            V.ray_o[ray] = make_float4(o.x, o.y, o.z, 0.0f);
-            V.ray_d[ray] = make_float4(d.x, d.y, d.z, 0.0f);
+            V.ts.ray_o[ray] = make_float4(o.x, o.y, o.z, 0.0f);
+            V.ts.ray_d[ray] = make_float4(d.x, d.y, d.z, 0.0f);
         },
         [&](uint32_t ray, const lux::Hit &h) {
-            V.ray_o[ray].w = h.t;
-            V.ray_d[ray].w = h.b1;
-            V.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
+            V.ts.ray_o[ray].w = h.t;
+            V.ts.ray_d[ray].w = h.b1;
+            V.ts.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
             st[kStatInterval] += 1;
         },
         cn);
@@ -330,7 +319,7 @@ __global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameP
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(&V.work_counter[0]);
+        uint32_t base = warp_fetch(&V.ts.work_counter[0]);
         if (base >= ray_count) break;
         uint32_t ray = base + (threadIdx.x & 31u);
         if (ray < ray_count) {
@@ -411,7 +400,7 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
                                                  slot_of[nq] = sample;
                                                  ++nq;
                                              });
-            V.ray_base[ray] = make_float4(base.x, base.y, base.z,
+            V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z,
                                           lux::as_float(supported ? count : lux::kEmpty));
         }
         // Warp-aggregated append of this warp's queries.
@@ -423,7 +412,7 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
         }
         uint32_t total = __shfl_sync(0xffffffffu, prefix, 31);
         uint32_t first = 0;
-        if (lane == 31 && total) first = atomicAdd(V.queue_count, total);
+        if (lane == 31 && total) first = atomicAdd(V.ts.queue_count, total);
         first = __shfl_sync(0xffffffffu, first, 31);
         uint32_t at = first + prefix - nq;
         if (ray < rays) {
@@ -433,17 +422,17 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
                 if (k < nq && slot_of[k] == s) {
                     uint32_t qi = at + k;
                     if (qi < F.queue_capacity) {
-                        V.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
-                        V.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
-                        V.slot_query[slot] = qi;
-                        V.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
+                        V.ts.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
+                        V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
+                        V.ts.slot_query[slot] = qi;
+                        V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
                                                            q[k].contribution.z, 0.0f);
                     } else {
-                        V.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
+                        V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
                     }
                     ++k;
                 } else {
-                    V.slot_query[slot] = lux::kEmpty;
+                    V.ts.slot_query[slot] = lux::kEmpty;
                 }
             }
         }
@@ -454,20 +443,20 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
 // result: 0 visible, 1 blocked, 2 unsupported.
 __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
-    uint32_t n = min(*V.queue_count, F.queue_capacity);
+    uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     lux::trace_persistent<true>(
-        S, &V.work_counter[1], n,
+        S, &V.ts.work_counter[1], n,
         [&](uint32_t qi, f3 &o, f3 &d, float &tmin, float &limit) {
-            float4 a = V.queue_o[qi], b = V.queue_d[qi];
+            float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
             o = f3{a.x, a.y, a.z};
             d = f3{b.x, b.y, b.z};
             tmin = 0.0f;
             limit = a.w;
         },
         [&](uint32_t qi, const lux::Hit &sh) {
-            V.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
             st[kStatShadow] += 1;
         },
         cn);
@@ -480,18 +469,18 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
 
 __global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
-    uint32_t n = min(*V.queue_count, F.queue_capacity);
+    uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(&V.work_counter[1]);
+        uint32_t base = warp_fetch(&V.ts.work_counter[1]);
         if (base >= n) break;
         uint32_t qi = base + (threadIdx.x & 31u);
         if (qi < n) {
-            float4 a = V.queue_o[qi], b = V.queue_d[qi];
+            float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
             lux::Hit sh;
             lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
-            V.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
             st[kStatShadow] += 1;
         }
     }
@@ -504,19 +493,19 @@ __global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F
 
 // Next-event sum in sample order; false when the ray's query is unsupported.
 __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, f3 &radiance) {
-    float4 b = V.ray_base[ray];
+    float4 b = V.ts.ray_base[ray];
     uint32_t count = lux::as_uint(b.w);
     if (count == lux::kEmpty) return false;
     f3 sum{0.0f, 0.0f, 0.0f};
     for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
         size_t slot = (size_t)ray * lux::kMaxNeeSamples + s;
-        uint32_t qi = V.slot_query[slot];
+        uint32_t qi = V.ts.slot_query[slot];
         if (qi == lux::kEmpty) continue;
         if (qi == lux::kEmpty - 1u) return false;
-        uint8_t r = V.queue_result[qi];
+        uint8_t r = V.ts.queue_result[qi];
         if (r == 2) return false;
         if (r == 1) continue;
-        float4 c = V.slot_contrib[slot];
+        float4 c = V.ts.slot_contrib[slot];
         sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
     }
     radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count);
@@ -539,7 +528,7 @@ __global__ void __launch_bounds__(128) deposit_split_kernel(ViewDevice V, FrameP
             f3 dir;
             float u, v;
             split_direction(F, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
-            float t = V.ray_o[ray].w;
+            float t = V.ts.ray_o[ray].w;
             uint32_t term = F.levels - 1u;
             for (uint32_t l = 0; l + 1u < F.levels; ++l)
                 if (t > F.start[l] && t <= F.end[l]) {
@@ -578,7 +567,7 @@ __global__ void __launch_bounds__(128) deposit_dense_kernel(ViewDevice V, FrameP
             bool terminal = level + 1u == F.levels;
             f3 radiance;
             if (ray_radiance(V, (uint32_t)e, radiance)) {
-                bool terminates = terminal || V.ray_h[e].x != lux::kEmpty;
+                bool terminates = terminal || V.ts.ray_h[e].x != lux::kEmpty;
                 V.count[e] = 1u;
                 V.accum[e] = terminates ? make_float4(radiance.x, radiance.y, radiance.z, 0.0f)
                                         : make_float4(0.0f, 0.0f, 0.0f, 1.0f);
@@ -881,17 +870,17 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.tables, (size_t)d.max_cells * 36 * sizeof(float4)},
         {(void **)&D.error_flags, sizeof(uint32_t) * 4},
         {(void **)&D.stats, 16 * sizeof(unsigned long long)},
-        {(void **)&D.ray_o, (size_t)d.max_rays * sizeof(float4)},
-        {(void **)&D.ray_d, (size_t)d.max_rays * sizeof(float4)},
-        {(void **)&D.ray_h, (size_t)d.max_rays * sizeof(uint4)},
-        {(void **)&D.ray_base, (size_t)d.max_rays * sizeof(float4)},
-        {(void **)&D.slot_query, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
-        {(void **)&D.slot_contrib, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
-        {(void **)&D.queue_o, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
-        {(void **)&D.queue_d, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
-        {(void **)&D.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
-        {(void **)&D.queue_count, 16},
-        {(void **)&D.work_counter, 16},
+        {(void **)&D.ts.ray_o, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ts.ray_d, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ts.ray_h, (size_t)d.max_rays * sizeof(uint4)},
+        {(void **)&D.ts.ray_base, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ts.slot_query, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
+        {(void **)&D.ts.slot_contrib, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.ts.queue_o, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.ts.queue_d, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
+        {(void **)&D.ts.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
+        {(void **)&D.ts.queue_count, 16},
+        {(void **)&D.ts.work_counter, 16},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
@@ -931,8 +920,8 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     ViewDevice &D = v->dev;
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
-                    D.ray_o, D.ray_d, D.ray_h, D.ray_base, D.slot_query, D.slot_contrib, D.queue_o, D.queue_d,
-                    D.queue_result, D.queue_count, D.work_counter,
+                    D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
+                    D.ts.queue_result, D.ts.queue_count, D.ts.work_counter,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -1211,4 +1200,105 @@ extern "C" lux_status lux_view_get_tuning(const LuxView *v, LuxTuning *t) {
     if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
     *t = v->tuning;
     return LUX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Interval radiance of caller rays: traceTransport's closest hit followed by
+// finishTransportVariant's outgoing radiance (shaders/split.slang:1122-1216,
+// shaders/cascades.slang:196-268) without the deposit.  Uses the same
+// wavefront kernels as a view's trace stage on trace scratch of the context.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void scratch_clear_kernel(ViewDevice V) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        *V.error_flags = 0;
+        *V.ts.queue_count = 0;
+        V.ts.work_counter[0] = 0;
+        V.ts.work_counter[1] = 0;
+    }
+    if (blockIdx.x == 0 && threadIdx.x < 16) V.stats[threadIdx.x] = 0;
+}
+
+__global__ void __launch_bounds__(128) closest_rays_kernel(ViewDevice V, SceneView S, const LuxRay *__restrict__ rays,
+                                                           uint32_t count) {
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    while (true) {
+        uint32_t base = warp_fetch(&V.ts.work_counter[0]);
+        if (base >= count) break;
+        uint32_t i = base + (threadIdx.x & 31u);
+        if (i < count) {
+            LuxRay r = rays[i];
+            f3 o{r.origin[0], r.origin[1], r.origin[2]}, d{r.direction[0], r.direction[1], r.direction[2]};
+            lux::Hit hit;
+            lux::trace<false>(S, o, d, r.tmin, r.limit, hit, cn);
+            store_ray(V, i, o, d, hit);
+            st[kStatInterval] += 1;
+        }
+    }
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
+    add_stats(V.stats, st);
+}
+
+// out[i] = (radiance rgb, hit distance) or (0, 0, 0, -1) when unsupported.
+__global__ void radiance_out_kernel(ViewDevice V, uint32_t count, float4 *__restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    f3 radiance;
+    if (ray_radiance(V, i, radiance))
+        out[i] = make_float4(radiance.x, radiance.y, radiance.z, V.ts.ray_o[i].w);
+    else
+        out[i] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+}
+
+lux_status launch_interval_radiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings_in,
+                                    const LuxRay *rays, uint32_t count, float *out, const ViewDevice &V,
+                                    uint32_t capacity) {
+    LuxSettings s = *settings_in;
+    lux_settings_sanitize(&s);
+    FrameParams F;
+    std::memset(&F, 0, sizeof F);
+    F.ray_capacity = capacity;
+    F.queue_capacity = capacity * lux::kMaxNeeSamples;
+    F.shade.probe_spacing = s.probe_spacing;
+    F.shade.normal_bias = s.normal_bias;
+    F.shade.exposure = s.exposure;
+    F.shade.emissive_samples = s.emissive_samples;
+    F.shade.frame = s.frame_index;
+    cudaStream_t st = ctx->stream;
+    scratch_clear_kernel<<<1, 32, 0, st>>>(V);
+    if (count) {
+        closest_rays_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(V, scene->view, rays, count);
+        shade_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, F, scene->view, count, false);
+        shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(V, F, scene->view);
+        radiance_out_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, count, (float4 *)out);
+    }
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "interval_radiance launch");
+}
+
+}  // namespace
+
+extern "C" lux_status lux_interval_radiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
+                                           const LuxRay *rays, uint32_t count, float *out) {
+    if (!ctx || !scene || !settings || (count && (!rays || !out))) return LUX_ERR_INVALID_ARGUMENT;
+    if ((uint64_t)count * lux::kMaxNeeSamples > 0xffffffffull)
+        return lux_fail(ctx, LUX_ERR_CAPACITY, "interval_radiance: more than 2^28 rays");
+    if (count > ctx->scratch_rays) {
+        cudaStreamSynchronize(ctx->stream);
+        if (ctx->scratch_mem) cudaFree(ctx->scratch_mem);
+        ctx->scratch_mem = nullptr;
+        ctx->scratch_rays = 0;
+        if (cudaMalloc(&ctx->scratch_mem, carved_scratch_bytes(count)) != cudaSuccess) {
+            cudaGetLastError();
+            return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "interval_radiance: scratch allocation failed");
+        }
+        ctx->scratch_rays = count;
+    }
+    ViewDevice V;
+    std::memset(&V, 0, sizeof V);
+    carve_trace_scratch((unsigned char *)ctx->scratch_mem, ctx->scratch_rays, V.ts, V.error_flags, V.stats);
+    return launch_interval_radiance(ctx, scene, settings, rays, count, out, V, ctx->scratch_rays);
 }

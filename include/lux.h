@@ -247,6 +247,16 @@ lux_status lux_scene_layout(const LuxScene *scene, uint32_t *nodes, uint32_t *no
 lux_status lux_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *rays,
                           uint32_t count, uint32_t any_hit, LuxHit *hits);
 
+/* Interval radiance of caller rays: the closest hit of each ray and the
+ * outgoing radiance there (hit emission + emissive next-event estimation with
+ * visibility rays), the value traceTransport deposits
+ * (shaders/split.slang:1122-1216, shaders/cascades.slang:196-268).
+ * rays: device LuxRay[count]; out: device float4[count] = (radiance rgb, hit
+ * distance, or the ray's limit on a miss), or (0, 0, 0, -1) when the query is
+ * unsupported.  Trace scratch is owned by the context and grows with count. */
+lux_status lux_interval_radiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
+                                 const LuxRay *rays, uint32_t count, float *out);
+
 /* ---- cascade view (render(), src/render.rs:9124-9830) ------------------ */
 lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out);
 lux_status lux_view_destroy(LuxView *view);

@@ -1,0 +1,60 @@
+"""lux_interval_radiance against the oracle's traceRayTracked +
+outgoingTransportRadianceTracked restatement on identical rays."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import bevy_penumbra_b200 as bp
+import oracle
+from tests.helpers import EMPTY, empty_device, from_device, packed, to_device
+
+pytestmark = pytest.mark.gpu
+
+
+def random_rays(n, lo, hi, seed):
+    rng = np.random.default_rng(seed)
+    rays = np.zeros(n, dtype=bp.RAY_DTYPE)
+    rays["origin"] = rng.uniform(lo, hi, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays["direction"] = d.astype(np.float32)
+    rays["limit"] = 1e20
+    return rays
+
+
+def oracle_radiance(name, settings, rays):
+    osc = oracle.OracleScene.from_packed(packed(name))
+    s = settings.to_c()
+    out = np.zeros((len(rays), 4), np.float32)
+    hit = np.zeros(1, dtype=bp.HIT_DTYPE)
+    rad = np.zeros(3, np.float32)
+    for i in range(len(rays)):
+        o = np.ascontiguousarray(rays["origin"][i])
+        d = np.ascontiguousarray(rays["direction"][i])
+        oracle.lib().orc_trace_closest(osc.handle, o.ctypes.data, d.ctypes.data, float(rays["tmin"][i]),
+                                       float(rays["limit"][i]), hit.ctypes.data, None)
+        ok = oracle.lib().orc_outgoing_radiance(osc.handle, C.byref(s), o.ctypes.data, d.ctypes.data, hit.ctypes.data,
+                                                rad.ctypes.data, None, None)
+        out[i] = (*rad, hit["distance"][0]) if ok else (0, 0, 0, -1)
+    return out
+
+
+@pytest.mark.parametrize("name,lo,hi,samples", [
+    ("cornell", (-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), 16),
+    ("cornell", (-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), 3),
+    ("atrium65536", (-7, 0.2, -7), (7, 9.0, 7), 8),
+])
+def test_interval_radiance_bit_exact(name, lo, hi, samples):
+    settings = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=samples, frame_index=5).sanitized()
+    rays = random_rays(4096, lo, hi, seed=samples)
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed(name))
+    d_rays = to_device(rays)
+    d_out = empty_device(len(rays) * 16)
+    bp.interval_radiance(ctx, scene, settings, d_rays.data_ptr(), len(rays), d_out.data_ptr())
+    ctx.synchronize()
+    gpu = from_device(d_out, np.float32, (len(rays), 4))
+    cpu = oracle_radiance(name, settings, rays)
+    np.testing.assert_array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+    assert np.mean(gpu[:, :3].sum(1) > 0) > 0.2, "many rays must see lit surfaces or emitters"
