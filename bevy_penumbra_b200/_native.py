@@ -125,6 +125,7 @@ SIGNATURES = {
                                    C.POINTER(U32)]),
     "lux_trace_rays": (C.c_int, [P, P, P, U32, U32, P]),
     "lux_interval_radiance": (C.c_int, [P, P, C.POINTER(LuxSettings), P, U32, P]),
+    "lux_interval_radiance_noalloc": (C.c_int, [P, P, C.POINTER(LuxSettings), P, U32, P]),
     "lux_view_create": (C.c_int, [P, C.POINTER(LuxViewDesc), C.POINTER(P)]),
     "lux_view_destroy": (C.c_int, [P]),
     "lux_view_trace_merge": (C.c_int, [P, P, C.POINTER(LuxSettings), C.POINTER(LuxReceivers)]),

@@ -21,6 +21,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "lux_internal.h"
@@ -1301,4 +1303,64 @@ extern "C" lux_status lux_interval_radiance(LuxContext *ctx, const LuxScene *sce
     std::memset(&V, 0, sizeof V);
     carve_trace_scratch((unsigned char *)ctx->scratch_mem, ctx->scratch_rays, V.ts, V.error_flags, V.stats);
     return launch_interval_radiance(ctx, scene, settings, rays, count, out, V, ctx->scratch_rays);
+}
+
+// ---------------------------------------------------------------------------
+// lux_interval_radiance_noalloc: lux_interval_radiance for callers that must
+// not allocate device memory.  Its trace scratch is one fixed array in the
+// library's own device image (reserved when the module loads on a device), so
+// the call makes no cudaMalloc, cudaFree or allocating library call.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint32_t kNoAllocMaxRays = 8192u;
+constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+// Same partition as carve_trace_scratch for kNoAllocMaxRays rays.
+constexpr size_t kNoAllocBytes = 4 * align256((size_t)kNoAllocMaxRays * 16) +
+                                 align256((size_t)kNoAllocMaxRays * 16 * 4) +
+                                 3 * align256((size_t)kNoAllocMaxRays * 16 * 16) +
+                                 align256((size_t)kNoAllocMaxRays * 16) + 3 * align256(16) + align256(128);
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char *g_noalloc_address[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+// About 7.5 MiB, held on every device that loads the library, until exit.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+extern "C" lux_status lux_interval_radiance_noalloc(LuxContext *ctx, const LuxScene *scene,
+                                                    const LuxSettings *settings, const LuxRay *rays, uint32_t count,
+                                                    float *out) {
+    if (!ctx || !scene || !settings || (count && (!rays || !out))) return LUX_ERR_INVALID_ARGUMENT;
+    if (count > kNoAllocMaxRays)
+        return lux_fail(ctx, LUX_ERR_CAPACITY,
+                        "interval_radiance_noalloc: " + std::to_string(count) +
+                            " rays exceed the fixed scratch capacity of 8192 rays; split the batch");
+    if (ctx->device < 0 || ctx->device >= kNoAllocMaxDevices)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "interval_radiance_noalloc: device ordinal out of range");
+    unsigned char *base = nullptr;
+    {
+        // Set-up once per device, with that device current: the host-side
+        // name of the array is not a device address; ask the runtime for it.
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        base = g_noalloc_address[ctx->device];
+        if (!base) {
+            lux_status s = lux_cuda_check(ctx, (int)cudaSetDevice(ctx->device), "interval_radiance_noalloc set device");
+            if (s != LUX_OK) return s;
+            void *address = nullptr;
+            s = lux_cuda_check(ctx, (int)cudaGetSymbolAddress(&address, g_noalloc_scratch),
+                               "interval_radiance_noalloc scratch address");
+            if (s != LUX_OK) return s;
+            base = (unsigned char *)address;
+            g_noalloc_address[ctx->device] = base;
+        }
+    }
+    ViewDevice V;
+    std::memset(&V, 0, sizeof V);
+    unsigned char *end = carve_trace_scratch(base, kNoAllocMaxRays, V.ts, V.error_flags, V.stats);
+    if ((size_t)(end - base) > kNoAllocBytes)
+        return lux_fail(ctx, LUX_ERR_INTERNAL, "interval_radiance_noalloc: scratch partition exceeds the array");
+    return launch_interval_radiance(ctx, scene, settings, rays, count, out, V, kNoAllocMaxRays);
 }

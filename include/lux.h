@@ -257,6 +257,27 @@ lux_status lux_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *
 lux_status lux_interval_radiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
                                  const LuxRay *rays, uint32_t count, float *out);
 
+/* lux_interval_radiance for callers that are not allowed to allocate device
+ * memory.  No counterpart in the reference: it exists for hosts such as a
+ * real-time render thread, where cudaMalloc / cudaFree can synchronise the
+ * device and stall a frame, or an engine that reserves its whole device
+ * budget up front through its own allocator and forbids allocations it does
+ * not account for.  This entry point calls no cudaMalloc, cudaFree or other
+ * allocating routine: its scratch is one fixed array of about 7.5 MiB built
+ * into the library, which every device that loads the library keeps until the
+ * process exits.
+ *  - At most 8192 rays per call; larger counts fail with LUX_ERR_CAPACITY
+ *    before any work is queued.  Split bigger batches.
+ *  - The first call on a device looks up the array's device address (with
+ *    that device made current); make that first call before any stream
+ *    capture on the device.
+ *  - All calls share the one array.  Each call resets the counters it needs
+ *    and overwrites the rest, but calls whose GPU work overlaps (different
+ *    streams or contexts on the same device) race: order them. */
+lux_status lux_interval_radiance_noalloc(LuxContext *ctx, const LuxScene *scene,
+                                         const LuxSettings *settings, const LuxRay *rays,
+                                         uint32_t count, float *out);
+
 /* ---- cascade view (render(), src/render.rs:9124-9830) ------------------ */
 lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out);
 lux_status lux_view_destroy(LuxView *view);
