@@ -93,7 +93,8 @@ class LuxTimings(C.Structure):
 
 class LuxTuning(C.Structure):
     _fields_ = [("closest_mode", C.c_uint32), ("shadow_mode", C.c_uint32), ("closest_blocks_per_sm", C.c_uint32),
-                ("shadow_blocks_per_sm", C.c_uint32), ("sort_queries", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("shadow_blocks_per_sm", C.c_uint32), ("sort_queries", C.c_uint32), ("sort_rays", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 P = C.c_void_p

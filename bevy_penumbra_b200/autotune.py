@@ -1,35 +1,43 @@
 """Launch-shape autotuner for a view's trace kernels.
 
-Times each candidate LuxTuning (traversal scheduling mode and persistent
-blocks per SM for the closest-hit and visibility kernels) on the caller's
-own frame with the library's per-stage CUDA-event timings, and keeps the
-fastest.  The winner is a property of the scene, receivers and settings, so
-a host engine runs this once per view configuration (untimed), like a
-convolution-algorithm search.
+Times each candidate LuxTuning (traversal scheduling mode, persistent blocks
+per SM, and whether interval rays / visibility queries are put in coherence
+order before tracing) on the caller's own frame with the library's per-stage
+CUDA-event timings, and keeps the fastest.  The winner depends on the scene,
+receivers and settings, so a host engine runs this once per view
+configuration (untimed), like a convolution-algorithm search.
 """
 from __future__ import annotations
 
 import itertools
 
-
 DEFAULT_SPACE = {
-    "closest_mode": (0, 1),
-    "shadow_mode": (0, 1),
-    "blocks_per_sm": (4, 8, 16),
+    "closest_mode": (0,),
+    "shadow_mode": (0,),
+    "blocks_per_sm": (16, 32),
+    "sort_rays": (0, 1),
+    "sort_queries": (0, 1),
 }
+
+
+def candidates(space=None):
+    space = space or DEFAULT_SPACE
+    for cm, sm, bps, sr, sq in itertools.product(space["closest_mode"], space["shadow_mode"],
+                                                 space["blocks_per_sm"], space["sort_rays"],
+                                                 space["sort_queries"]):
+        yield dict(closest_mode=cm, shadow_mode=sm, closest_blocks_per_sm=bps, shadow_blocks_per_sm=bps,
+                   sort_rays=sr, sort_queries=sq)
 
 
 def autotune(view, run_frame, space=None, repeats: int = 2) -> dict:
     """run_frame() must issue one lux_view_trace_merge on `view`.
 
     Returns {"best": {...}, "trace_ms": best time, "trials": [(tuning, ms), ...]}."""
-    space = space or DEFAULT_SPACE
     view.set_timing(True)
     trials = []
-    for cm, sm, bps in itertools.product(space["closest_mode"], space["shadow_mode"], space["blocks_per_sm"]):
-        cand = dict(closest_mode=cm, shadow_mode=sm, closest_blocks_per_sm=bps, shadow_blocks_per_sm=bps)
+    for cand in candidates(space):
         view.set_tuning(**cand)
-        run_frame()  # first frame with a new shape is not timed
+        run_frame()  # the first frame with a new shape is not timed
         times = []
         for _ in range(repeats):
             run_frame()

@@ -127,6 +127,7 @@ struct NeeQuery {
     f3 origin, direction;
     float limit;
     f3 contribution;
+    uint32_t light;  // emitter record index (coherence sort key)
 };
 
 // emissiveResponseTracked, shaders/cascades.slang:57-134, up to (but not
@@ -208,6 +209,7 @@ __device__ void emissive_queries(const SceneView &S, const ShadeParams &P, f3 po
         q.contribution = f3{emission.x * (((diffuse.x * factor) * cosine) / p),
                             emission.y * (((diffuse.y * factor) * cosine) / p),
                             emission.z * (((diffuse.z * factor) * cosine) / p)};
+        q.light = low;
         emit(sample, q);
     }
 }

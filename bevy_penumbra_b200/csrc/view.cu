@@ -65,7 +65,34 @@ struct ViewDevice {
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
     TraceScratch ts;                // wavefront trace state
+    // Coherence ordering of rays / visibility queries (counting sort by bin).
+    uint32_t *sort_keys;            // [max(rays, queries)]
+    uint32_t *sort_perm;            // [max(rays, queries)] processing order -> item
+    uint32_t *sort_hist;            // [kSortBins]
+    const uint32_t *ray_order;      // closest-hit processing order (nullptr: identity)
+    const uint32_t *query_order;    // visibility processing order (nullptr: identity)
 };
+
+constexpr uint32_t kSortCells = 4096;           // 16^3 origin cells over the TLAS root box
+constexpr uint32_t kSortBins = 64 * kSortCells; // x 64 emitter buckets or 32 direction bins
+
+// Morton index of a point's cell in a 16^3 grid over the scene box.
+__device__ __forceinline__ uint32_t cell16(const SceneView &S, lux::f3 p) {
+    float e[3] = {p.x, p.y, p.z};
+    uint32_t c[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float span = S.root_hi[a] - S.root_lo[a];
+        float t = span > 0.0f ? (e[a] - S.root_lo[a]) / span : 0.0f;
+        int q = (int)(t * 16.0f);
+        c[a] = (uint32_t)(q < 0 ? 0 : (q > 15 ? 15 : q));
+    }
+    uint32_t m = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        m |= (((c[0] >> b) & 1u) << (3 * b)) | (((c[1] >> b) & 1u) << (3 * b + 1)) | (((c[2] >> b) & 1u) << (3 * b + 2));
+    return m;
+}
 
 constexpr int kStatInterval = 0, kStatShadow = 1, kStatNodes = 2, kStatTris = 3, kStatInst = 4, kStatDeposits = 5,
               kStatUnsupported = 6, kStatShadowNodes = 7, kStatShadowTris = 8, kStatShadowInst = 9;
@@ -282,7 +309,8 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
     lux::TraceCounters cn{0, 0, 0};
     lux::trace_persistent<false>(
         S, &V.ts.work_counter[0], ray_count,
-        [&](uint32_t ray, f3 &o, f3 &d, float &tmin, float &limit) {
+        [&](uint32_t slot, f3 &o, f3 &d, float &tmin, float &limit) {
+            uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
             uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
             float4 p4 = pos[i], n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
@@ -294,7 +322,8 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
             V.ts.ray_o[ray] = make_float4(o.x, o.y, o.z, 0.0f);
             V.ts.ray_d[ray] = make_float4(d.x, d.y, d.z, 0.0f);
         },
-        [&](uint32_t ray, const lux::Hit &h) {
+        [&](uint32_t slot, const lux::Hit &h) {
+            uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
             V.ts.ray_o[ray].w = h.t;
             V.ts.ray_d[ray].w = h.b1;
             V.ts.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
@@ -323,8 +352,9 @@ __global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameP
     while (true) {
         uint32_t base = warp_fetch(&V.ts.work_counter[0]);
         if (base >= ray_count) break;
-        uint32_t ray = base + (threadIdx.x & 31u);
-        if (ray < ray_count) {
+        uint32_t slot = base + (threadIdx.x & 31u);
+        if (slot < ray_count) {
+            uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
             uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
             float4 p4 = pos[i], n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
@@ -378,6 +408,58 @@ __global__ void __launch_bounds__(128) closest_dense_kernel(ViewDevice V, FrameP
     }
 }
 
+// Coherence keys of split interval rays: (direction bin of an 8 x 4 grid,
+// origin cell).
+__global__ void ray_keys_kernel(ViewDevice V, FrameParams F, SceneView S, const float4 *__restrict__ pos,
+                                const float4 *__restrict__ nrm, uint32_t ray_count) {
+    for (uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x; ray < ray_count; ray += gridDim.x * blockDim.x) {
+        uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+        float4 p4 = pos[i], n4 = nrm[i];
+        f3 dir;
+        float u, v;
+        split_direction(F, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+        uint32_t bin = lux::direction_index_uv(u, v, 8u, 4u);
+        V.sort_keys[ray] = bin * kSortCells + cell16(S, f3{p4.x, p4.y, p4.z});
+    }
+}
+
+// Counting sort of keys in [0, kSortBins): histogram, exclusive scan, scatter.
+// Order within a bin is arbitrary; every item is processed exactly once and
+// its result is written to its own slot, so the outputs do not depend on it.
+__global__ void sort_hist_kernel(ViewDevice V, const uint32_t *count_ptr, uint32_t cap) {
+    uint32_t n = count_ptr ? min(*count_ptr, cap) : cap;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        atomicAdd(&V.sort_hist[V.sort_keys[i]], 1u);
+}
+
+__global__ void __launch_bounds__(1024) sort_scan_kernel(ViewDevice V) {
+    __shared__ uint32_t part[1024];
+    constexpr uint32_t per = kSortBins / 1024;
+    uint32_t t = threadIdx.x;
+    uint32_t sum = 0;
+    for (uint32_t j = 0; j < per; ++j) sum += V.sort_hist[t * per + j];
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {
+        uint32_t add = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += add;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;  // exclusive prefix of this thread's range
+    for (uint32_t j = 0; j < per; ++j) {
+        uint32_t c = V.sort_hist[t * per + j];
+        V.sort_hist[t * per + j] = run;
+        run += c;
+    }
+}
+
+__global__ void sort_scatter_kernel(ViewDevice V, const uint32_t *count_ptr, uint32_t cap) {
+    uint32_t n = count_ptr ? min(*count_ptr, cap) : cap;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        V.sort_perm[atomicAdd(&V.sort_hist[V.sort_keys[i]], 1u)] = i;
+}
+
 // Hit shading up to the visibility traces; queries are appended to the
 // queue with one atomic per warp.
 __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t ray_count,
@@ -429,6 +511,7 @@ __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F,
                         V.ts.slot_query[slot] = qi;
                         V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
                                                            q[k].contribution.z, 0.0f);
+                        if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
                     } else {
                         V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
                     }
@@ -450,14 +533,16 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
     lux::TraceCounters cn{0, 0, 0};
     lux::trace_persistent<true>(
         S, &V.ts.work_counter[1], n,
-        [&](uint32_t qi, f3 &o, f3 &d, float &tmin, float &limit) {
+        [&](uint32_t i, f3 &o, f3 &d, float &tmin, float &limit) {
+            uint32_t qi = V.query_order ? V.query_order[i] : i;
             float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
             o = f3{a.x, a.y, a.z};
             d = f3{b.x, b.y, b.z};
             tmin = 0.0f;
             limit = a.w;
         },
-        [&](uint32_t qi, const lux::Hit &sh) {
+        [&](uint32_t i, const lux::Hit &sh) {
+            uint32_t qi = V.query_order ? V.query_order[i] : i;
             V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
             st[kStatShadow] += 1;
         },
@@ -477,8 +562,9 @@ __global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F
     while (true) {
         uint32_t base = warp_fetch(&V.ts.work_counter[1]);
         if (base >= n) break;
-        uint32_t qi = base + (threadIdx.x & 31u);
-        if (qi < n) {
+        uint32_t i = base + (threadIdx.x & 31u);
+        if (i < n) {
+            uint32_t qi = V.query_order ? V.query_order[i] : i;
             float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
             lux::Hit sh;
             lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
@@ -835,7 +921,7 @@ constexpr int kTimingEvents = 7;
 
 struct LuxView {
     LuxContext *ctx = nullptr;
-    LuxTuning tuning{0, 0, 8, 8, 0, {0, 0, 0}};
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, {0, 0}};
     bool timing = false;
     cudaEvent_t ev[kTimingEvents] = {};
     LuxViewDesc desc{};
@@ -883,6 +969,9 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.ts.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
         {(void **)&D.ts.queue_count, 16},
         {(void **)&D.ts.work_counter, 16},
+        {(void **)&D.sort_keys, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
+        {(void **)&D.sort_perm, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
+        {(void **)&D.sort_hist, (size_t)kSortBins * sizeof(uint32_t)},
     };
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
@@ -923,7 +1012,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
                     D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
-                    D.ts.queue_result, D.ts.queue_count, D.ts.work_counter,
+                    D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
@@ -996,17 +1085,36 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
         uint32_t rays = rc->count * F.rays_per_receiver;
         if (rays) {
             const LuxTuning &T = v->tuning;
+            ViewDevice Dr = D;  // ray pass view: optional coherence order of interval rays
+            Dr.sort_keys = nullptr;
+            if (T.sort_rays) {
+                cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
+                ray_keys_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, F, scene->view, pos, nrm, rays);
+                sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
+                sort_scan_kernel<<<1, 1024, 0, st>>>(D);
+                sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
+                Dr.ray_order = D.sort_perm;
+            }
             if (T.closest_mode == 1)
                 closest_split_refill_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
-                    D, F, scene->view, pos, nrm, rays);
+                    Dr, F, scene->view, pos, nrm, rays);
             else
-                closest_split_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(D, F, scene->view, pos,
-                                                                                             nrm, rays);
-            shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, scene->view, rays, false);
+                closest_split_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(Dr, F, scene->view,
+                                                                                             pos, nrm, rays);
+            ViewDevice Dq = D;  // query pass view: keys written by shade, optional order
+            if (!T.sort_queries) Dq.sort_keys = nullptr;
+            shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(Dq, F, scene->view, rays, false);
+            if (T.sort_queries) {
+                cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
+                sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
+                sort_scan_kernel<<<1, 1024, 0, st>>>(D);
+                sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
+                Dq.query_order = D.sort_perm;
+            }
             if (T.shadow_mode == 1)
-                shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
+                shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             else
-                shadow_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
+                shadow_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             deposit_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, nrm, rays);
         }
     } else {
@@ -1192,7 +1300,7 @@ extern "C" lux_status lux_view_timings(LuxView *v, LuxTimings *out) {
 extern "C" lux_status lux_view_set_tuning(LuxView *v, const LuxTuning *t) {
     if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
     if (t->closest_mode > 1 || t->shadow_mode > 1 || t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 ||
-        t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64)
+        t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64 || t->sort_queries > 1 || t->sort_rays > 1)
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_tuning: value out of range");
     v->tuning = *t;
     return LUX_OK;

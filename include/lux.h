@@ -319,8 +319,9 @@ typedef struct LuxTuning {
     uint32_t shadow_mode;
     uint32_t closest_blocks_per_sm;
     uint32_t shadow_blocks_per_sm;
-    uint32_t sort_queries;        /* reserved */
-    uint32_t reserved[3];
+    uint32_t sort_queries;        /* 1: order visibility queries by (emitter, origin cell) before tracing */
+    uint32_t sort_rays;           /* 1: order interval rays by (direction bin, origin cell) before tracing */
+    uint32_t reserved[2];
 } LuxTuning;
 lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
 lux_status lux_view_get_tuning(const LuxView *view, LuxTuning *tuning);

@@ -18,11 +18,13 @@ def by_key(keys):
     return {tuple(k[:3]): i for i, k in enumerate(keys)}
 
 
-def run_frame(name, settings, pos, nrm, max_cells=1 << 16, max_entries=1 << 24):
+def run_frame(name, settings, pos, nrm, max_cells=1 << 16, max_entries=1 << 24, tuning=None):
     ctx = bp.LuxContext()
     scene = bp.GpuScene(ctx, packed(name))
     rays = len(pos) * settings.rays_per_receiver if settings.layout == bp.LAYOUT_SPLIT else 1 << 20
     view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=max_cells, max_entries=max_entries, max_rays=rays)
+    if tuning:
+        view.set_tuning(**tuning)
     d_pos, d_nrm = to_device(pos), to_device(nrm)
     view.trace_merge(scene, settings, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
     st = view.stats()
@@ -111,12 +113,13 @@ def cornell_floor_receivers(n=32):
     return pos, nrm
 
 
-@pytest.mark.parametrize("rays", [1, 8])
-def test_split_cornell_frame_matches_oracle(rays):
+@pytest.mark.parametrize("rays,sort", [(1, 0), (8, 0), (8, 1)])
+def test_split_cornell_frame_matches_oracle(rays, sort):
     settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=rays,
                                    frame_index=3).sanitized()
     pos, nrm = cornell_floor_receivers()
-    ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm)
+    ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm,
+                                                              tuning=dict(sort_rays=sort, sort_queries=sort))
     ofr = oracle_frame("cornell", settings, pos, nrm)
     ost = ofr.stats()
     assert st.interval_rays == len(pos) * rays
@@ -138,6 +141,7 @@ def test_split_atrium_frame_matches_oracle():
     pos[:, 1] = 0.0
     nrm = np.zeros_like(pos)
     nrm[:, 1] = 1.0
-    ctx, scene, view, st, levels, probes = run_frame("atrium65536", settings, pos, nrm, max_entries=1 << 26)
+    ctx, scene, view, st, levels, probes = run_frame("atrium65536", settings, pos, nrm, max_entries=1 << 26,
+                                                     tuning=dict(sort_rays=1, sort_queries=1))
     ofr = oracle_frame("atrium65536", settings, pos, nrm)
     compare_levels(settings, levels, ofr, exact=False)
