@@ -37,6 +37,11 @@ struct Collapser {
     std::vector<Bvh4Node> &out;
     std::string error;
     uint32_t leaf_limit;  // elements addressable by a leaf (triangles or instances)
+    // Per-element world boxes (TLAS only): a leaf of 2-4 instances becomes a
+    // node whose children are single instances with their own boxes, so an
+    // instance is entered (ray transform, BLAS root test) only when the ray
+    // meets that instance's box rather than the whole leaf's.
+    const std::vector<BinNode> *element_box = nullptr;
 
     static double area(const BinNode &n) {
         double sx = (double)n.mx[0] - n.mn[0], sy = (double)n.mx[1] - n.mn[1], sz = (double)n.mx[2] - n.mn[2];
@@ -96,6 +101,19 @@ struct Collapser {
             if (b.count > 256u) {
                 error = "BVH leaf holds more than 256 elements";
                 return lux::kEmpty;
+            }
+            if (element_box && b.count >= 2u && b.count <= 4u) {
+                uint32_t node = new_node();
+                for (uint32_t k = 0; k < b.count; ++k) {
+                    const BinNode &e = (*element_box)[b.first + k];
+                    float mn[3], mx[3];
+                    for (int a = 0; a < 3; ++a) {
+                        mn[a] = std::max(e.mn[a], b.mn[a]);
+                        mx[a] = std::min(e.mx[a], b.mx[a]);
+                    }
+                    set_child(node, (int)k, mn, mx, kLeafBit | ((b.first + k) & kLeafFirstMask));
+                }
+                return node;
             }
             return leaf_payload(b.first, b.count, b.mn, b.mx);
         }
@@ -249,6 +267,41 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
                             "scene upload: textured materials are not supported by this build");
         tri_count = std::max(tri_count, inst[i].first + inst[i].count);
     }
+    // World box of every instance: the eight corners of its BLAS root box
+    // through world_from_local (instance rows 3-5) in f64, padded by 2^-17
+    // of the coordinate magnitude plus the box extent.  The reference's
+    // instance box (src/scene.rs:1911-1924) is the same transformed box padded
+    // by 8 f32 epsilons of the magnitudes, so this box contains it, and the
+    // child box (this box cut by the TLAS leaf's box, which is a union of
+    // reference instance boxes) never culls more than the reference's own
+    // box for that instance would.
+    std::vector<BinNode> inst_box(inst_count);
+    for (uint32_t i = 0; i < inst_count; ++i) {
+        const uint32_t *w = sw + 4 * (size_t)(inst_base + 9 * i);
+        double m[3][4];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) m[r][c] = (double)fword(w, 12 + 4 * r + c);
+        const BinNode &rb = bin[inst[i].root];
+        double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int corner = 0; corner < 8; ++corner) {
+            double q[3] = {(corner & 1) ? rb.mx[0] : rb.mn[0], (corner & 2) ? rb.mx[1] : rb.mn[1],
+                           (corner & 4) ? rb.mx[2] : rb.mn[2]};
+            for (int r = 0; r < 3; ++r) {
+                double v = m[r][0] * q[0] + m[r][1] * q[1] + m[r][2] * q[2] + m[r][3];
+                mn[r] = std::min(mn[r], v);
+                mx[r] = std::max(mx[r], v);
+            }
+        }
+        BinNode &b = inst_box[i];
+        for (int r = 0; r < 3; ++r) {
+            double pad = (std::max(std::fabs(mn[r]), std::fabs(mx[r])) + (mx[r] - mn[r])) * 7.62939453125e-6 + 1e-30;
+            bool finite = std::isfinite(mn[r]) && std::isfinite(mx[r]);
+            b.mn[r] = finite ? (float)(mn[r] - pad) : -INFINITY;
+            b.mx[r] = finite ? (float)(mx[r] + pad) : INFINITY;
+        }
+        b.first = i;
+        b.count = 1;
+    }
     // Collapse: TLAS from node 0, every distinct BLAS root once.
     std::vector<Bvh4Node> nodes;
     nodes.reserve(node_count / 2 + 16);
@@ -256,7 +309,7 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
     if (inst_count > 0) {
         if (node_count == 0) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: no TLAS nodes");
-        Collapser tl{bin, nodes, {}, inst_count};
+        Collapser tl{bin, nodes, {}, inst_count, &inst_box};
         tlas_root = tl.root(0);
         if (!tl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (TLAS): " + tl.error);
         for (int k = 0; k < 3; ++k) {

@@ -55,16 +55,24 @@ __device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, flo
 
 // Per-ray slab constants for the BVH4 child tests.  The reference divides
 // by the direction for every slab (shaders/traversal.slang:360-361); the
-// child tests here multiply by an approximate reciprocal (at most 2 ulp,
-// __fdividef) and widen the interval so the test stays conservative:
-// t = (lo - o) * inv then carries under 5 ulp of relative error, and the
-// interval grows by 7.2e-7 (about 6 ulp) relative on both ends.  Culling only
-// decides which triangles are tested; hit distances come from the exact
-// triangle test.
+// child tests here multiply by the correctly rounded reciprocal and widen the
+// interval so the test stays conservative: t = (plane - o) * inv carries
+// under 2 ulp of relative error, and the interval grows by 7.2e-7 (about 6
+// ulp) relative on both ends.  Culling only decides which triangles are
+// tested; hit distances come from the exact triangle test.
+//
+// The sign of each reciprocal picks the near and far plane of every axis
+// once per ray (s = 1 selects the high plane as near), so a child costs two
+// subtracts, two multiplies and no min/max per axis.  A zero direction
+// component gives an infinite reciprocal: planes on either side of the
+// origin give -inf/+inf (no constraint), a box wholly on one side gives an
+// infinite near or -inf far (miss), and a plane through the origin gives
+// NaN, which fmaxf/fminf ignore -- the reference's inside test for a zero
+// component.
 struct SlabRay {
     float ox, oy, oz;
-    float ix, iy, iz;  // 1 / d (unused on zero axes)
-    bool zx, zy, zz;   // zero direction components (the reference's inside test)
+    float ix, iy, iz;     // 1 / d, correctly rounded (+-inf on zero axes)
+    uint32_t sx, sy, sz;  // sign bits of ix, iy, iz
 };
 
 __device__ __forceinline__ SlabRay slab_ray(f3 o, f3 d) {
@@ -72,49 +80,40 @@ __device__ __forceinline__ SlabRay slab_ray(f3 o, f3 d) {
     r.ox = o.x;
     r.oy = o.y;
     r.oz = o.z;
-    r.zx = d.x == 0.0f;
-    r.zy = d.y == 0.0f;
-    r.zz = d.z == 0.0f;
-    r.ix = r.zx ? 0.0f : __fdividef(1.0f, d.x);
-    r.iy = r.zy ? 0.0f : __fdividef(1.0f, d.y);
-    r.iz = r.zz ? 0.0f : __fdividef(1.0f, d.z);
+    r.ix = __frcp_rn(d.x);
+    r.iy = __frcp_rn(d.y);
+    r.iz = __frcp_rn(d.z);
+    r.sx = as_uint(r.ix) >> 31;
+    r.sy = as_uint(r.iy) >> 31;
+    r.sz = as_uint(r.iz) >> 31;
     return r;
-}
-
-__device__ __forceinline__ void slab_axis(bool zero, float o, float inv, float lo, float hi, float &near_t,
-                                          float &far_t) {
-    if (zero) {
-        if (o < lo || o > hi) far_t = -INFINITY;
-    } else {
-        float ta = (lo - o) * inv;
-        float tb = (hi - o) * inv;
-        near_t = fmaxf(near_t, fminf(ta, tb));
-        far_t = fminf(far_t, fmaxf(ta, tb));
-    }
 }
 
 // Child tests of one BVH4 node.  Returns the hit mask and conservative entry
 // distances; children that end before tmin or start after `limit` are culled.
 __device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes, uint32_t index, const SlabRay &r,
                                               float limit, float tmin, float entry[4], uint32_t child[4]) {
+    // Node rows: lo_x, hi_x, lo_y, hi_y, lo_z, hi_z, child.
     const float4 *p = reinterpret_cast<const float4 *>(nodes + index);
-    float4 lx = __ldg(p + 0), hx = __ldg(p + 1), ly = __ldg(p + 2), hy = __ldg(p + 3), lz = __ldg(p + 4),
-           hz = __ldg(p + 5);
+    float4 nx = __ldg(p + r.sx), fx = __ldg(p + (1u - r.sx));
+    float4 ny = __ldg(p + 2u + r.sy), fy = __ldg(p + (3u - r.sy));
+    float4 nz = __ldg(p + 4u + r.sz), fz = __ldg(p + (5u - r.sz));
     uint4 ch = __ldg(reinterpret_cast<const uint4 *>(p + 6));
     child[0] = ch.x;
     child[1] = ch.y;
     child[2] = ch.z;
     child[3] = ch.w;
-    float LX[4] = {lx.x, lx.y, lx.z, lx.w}, HX[4] = {hx.x, hx.y, hx.z, hx.w};
-    float LY[4] = {ly.x, ly.y, ly.z, ly.w}, HY[4] = {hy.x, hy.y, hy.z, hy.w};
-    float LZ[4] = {lz.x, lz.y, lz.z, lz.w}, HZ[4] = {hz.x, hz.y, hz.z, hz.w};
+    float NX[4] = {nx.x, nx.y, nx.z, nx.w}, FX[4] = {fx.x, fx.y, fx.z, fx.w};
+    float NY[4] = {ny.x, ny.y, ny.z, ny.w}, FY[4] = {fy.x, fy.y, fy.z, fy.w};
+    float NZ[4] = {nz.x, nz.y, nz.z, nz.w}, FZ[4] = {fz.x, fz.y, fz.z, fz.w};
     uint32_t mask = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        float near_t = 0.0f, far_t = INFINITY;
-        slab_axis(r.zx, r.ox, r.ix, LX[i], HX[i], near_t, far_t);
-        slab_axis(r.zy, r.oy, r.iy, LY[i], HY[i], near_t, far_t);
-        slab_axis(r.zz, r.oz, r.iz, LZ[i], HZ[i], near_t, far_t);
+        float ax = (NX[i] - r.ox) * r.ix, bx = (FX[i] - r.ox) * r.ix;
+        float ay = (NY[i] - r.oy) * r.iy, by = (FY[i] - r.oy) * r.iy;
+        float az = (NZ[i] - r.oz) * r.iz, bz = (FZ[i] - r.oz) * r.iz;
+        float near_t = fmaxf(fmaxf(ax, ay), fmaxf(az, 0.0f));
+        float far_t = fminf(fminf(bx, by), bz);
         near_t = near_t - fabsf(near_t) * 7.2e-7f;
         far_t = far_t + fabsf(far_t) * 7.2e-7f;
         bool h = child[i] != kEmpty && near_t <= far_t && near_t <= limit && far_t >= tmin;
@@ -251,20 +250,27 @@ __device__ __forceinline__ DeviceInstance load_instance(const DeviceInstance *__
     return I;
 }
 
-// Sort up to four (entry, payload) pairs by entry, ascending.
-__device__ __forceinline__ void sort4(float e[4], uint32_t p[4], int n) {
-#define LUX_CSWAP(i, j)                                          \
-    if (n > (j) && e[j] < e[i]) {                                \
-        float te = e[i]; e[i] = e[j]; e[j] = te;                 \
-        uint32_t tp = p[i]; p[i] = p[j]; p[j] = tp;              \
-    }
-    LUX_CSWAP(0, 1);
-    LUX_CSWAP(2, 3);
-    LUX_CSWAP(0, 2);
-    LUX_CSWAP(1, 3);
-    LUX_CSWAP(1, 2);
-#undef LUX_CSWAP
+// Child ordering keys: the entry distance's bits (entries are >= 0, so the
+// bits order like the values) with the low two bits replaced by the child
+// slot; missed children get ~0 and sort last.  Truncating two mantissa bits
+// only lowers a stored entry, which keeps the closest-hit pop test
+// (skip when entry > best distance) conservative.
+__device__ __forceinline__ uint32_t child_key(uint32_t mask, const float entry[4], int i) {
+    return (mask & (1u << i)) ? ((as_uint(entry[i]) & ~3u) | (uint32_t)i) : 0xffffffffu;
 }
+
+__device__ __forceinline__ void key_swap(uint32_t &a, uint32_t &b) {
+    uint32_t lo = min(a, b), hi = max(a, b);
+    a = lo;
+    b = hi;
+}
+
+__device__ __forceinline__ uint32_t key_child(uint32_t key, const uint32_t child[4]) {
+    uint32_t s = key & 3u;
+    return s == 0u ? child[0] : (s == 1u ? child[1] : (s == 2u ? child[2] : child[3]));
+}
+
+__device__ __forceinline__ float key_entry(uint32_t key) { return as_float(key & ~3u); }
 
 // traceRayTracked + traceInstance (kAnyHit = false) and traceOccluded +
 // occludedInstance (kAnyHit = true) as one resumable walk over one stack.  A
@@ -291,9 +297,7 @@ struct Walker {
     uint32_t tlas_next;   // TLAS fallback: next instance to scan in order
     uint32_t blas_next;   // BLAS fallback: next triangle to scan in order
     uint32_t tlas_steps, blas_steps;
-    uint32_t stack_p[kStack];
-    float stack_t[kStack];
-    int sp;
+    int sp;  // depth of the caller's stack: kStack entries of (payload, entry distance bits)
     uint32_t cur;
     float cur_t;
     bool have;
@@ -335,13 +339,20 @@ struct Walker {
 
     // One step: inner nodes down to a leaf, that leaf, then the next pending
     // entry.  Returns true when the query is complete.
-    __device__ __forceinline__ bool step(const SceneView &S, TraceCounters &cn) {
+    // The stack lives outside the walker so the walker's fields stay in
+    // registers; only the stack itself is addressed dynamically.
+    __device__ __forceinline__ bool step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
         while (have && (cur & kLeafBit) == 0u) {
-            uint32_t &steps = blas_base < 0 ? tlas_steps : blas_steps;
-            if (++steps > kMaxSteps) {
+            bool in_tlas = blas_base < 0;
+            uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
+            if (in_tlas)
+                tlas_steps = steps;
+            else
+                blas_steps = steps;
+            if (steps > kMaxSteps) {
                 hit.errors |= kQueryUnsupported;
-                if (blas_base < 0) return true;  // abandon the whole query
-                sp = blas_base;                  // abandon this instance
+                if (in_tlas) return true;  // abandon the whole query
+                sp = blas_base;            // abandon this instance
                 have = false;
                 break;
             }
@@ -353,19 +364,16 @@ struct Walker {
                 have = false;
                 break;
             }
-            float e[4];
-            uint32_t p[4];
-            int n = 0;
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-                if (mask & (1u << i)) {
-                    e[n] = entry[i];
-                    p[n] = child[i];
-                    ++n;
-                }
-            sort4(e, p, n);
+            uint32_t k0 = child_key(mask, entry, 0), k1 = child_key(mask, entry, 1);
+            uint32_t k2 = child_key(mask, entry, 2), k3 = child_key(mask, entry, 3);
+            key_swap(k0, k1);
+            key_swap(k2, k3);
+            key_swap(k0, k2);
+            key_swap(k1, k3);
+            key_swap(k1, k2);
+            int n = __popc(mask);
             if (sp + n - 1 > kStack) {
-                if (blas_base < 0) {
+                if (in_tlas) {
                     hit.errors |= 2u;
                     sp = 0;
                     tlas_next = 0;
@@ -377,13 +385,11 @@ struct Walker {
                 have = false;
                 break;
             }
-            for (int k = n - 1; k >= 1; --k) {
-                stack_p[sp] = p[k];
-                stack_t[sp] = e[k];
-                ++sp;
-            }
-            cur = p[0];
-            cur_t = e[0];
+            if (n > 3) stack[sp++] = make_uint2(key_child(k3, child), k3 & ~3u);
+            if (n > 2) stack[sp++] = make_uint2(key_child(k2, child), k2 & ~3u);
+            if (n > 1) stack[sp++] = make_uint2(key_child(k1, child), k1 & ~3u);
+            cur = key_child(k0, child);
+            cur_t = key_entry(k0);
         }
         if (have) {
             uint32_t first = cur & kLeafFirstMask;
@@ -393,9 +399,8 @@ struct Walker {
                 // TLAS leaf: enter its first instance; the rest waits on the stack.
                 if (count > 1u) {
                     if (sp < kStack) {
-                        stack_p[sp] = kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27);
-                        stack_t[sp] = cur_t;
-                        ++sp;
+                        stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
+                                                 as_uint(cur_t));
                     } else {
                         // Stack exhausted: after this instance, scan every instance.
                         hit.errors |= 2u;
@@ -485,10 +490,10 @@ struct Walker {
                 }
                 return true;
             }
-            --sp;
-            if (!kAnyHit && stack_t[sp] > hit.t) continue;
-            cur = stack_p[sp];
-            cur_t = stack_t[sp];
+            uint2 top = stack[--sp];
+            if (!kAnyHit && as_float(top.y) > hit.t) continue;
+            cur = top.x;
+            cur_t = as_float(top.y);
             have = true;
         }
         return false;
@@ -498,8 +503,9 @@ struct Walker {
 template <bool kAnyHit>
 __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, Hit &hit, TraceCounters &cn) {
     Walker<kAnyHit> w;
+    uint2 stack[kStack];
     if (w.start(S, o, d, tmin, limit))
-        while (!w.step(S, cn)) {
+        while (!w.step(S, stack, cn)) {
         }
     hit = w.hit;
 }
@@ -513,6 +519,7 @@ __device__ void trace_persistent(const SceneView &S, uint32_t *counter, uint32_t
                                  TraceCounters &cn) {
     const uint32_t lane = threadIdx.x & 31u;
     Walker<kAnyHit> w;
+    uint2 stack[kStack];
     bool active = false;
     bool exhausted = false;  // the counter passed n: no further rays for this warp
     uint32_t id = 0;
@@ -539,7 +546,7 @@ __device__ void trace_persistent(const SceneView &S, uint32_t *counter, uint32_t
             if (exhausted) break;
             continue;
         }
-        if (active && w.step(S, cn)) {
+        if (active && w.step(S, stack, cn)) {
             done(id, w.hit);
             active = false;
         }
