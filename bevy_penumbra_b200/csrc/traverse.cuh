@@ -290,8 +290,9 @@ struct Walker {
     Hit hit;
     f3 o, d, lo, ld;
     float tmin, lower;
-    SlabRay world, r;
-    TriRay world_tri, tri_ray;
+    SlabRay r;       // slab constants of the current space's ray
+    TriRay tri_ray;  // world ray's constants in the TLAS; the local ray's inside an instance
+    bool rotated;    // the current instance changed the direction (r, tri_ray are local)
     uint32_t inst, inst_flags, inst_first, inst_count;
     int blas_base;        // stack depth at instance entry; -1 = TLAS space
     uint32_t tlas_next;   // TLAS fallback: next instance to scan in order
@@ -320,9 +321,9 @@ struct Walker {
         d = direction;
         tmin = t_min;
         lower = fmaxf(t_min, 0.000025f);
-        world = slab_ray(o, d);
-        r = world;
-        world_tri = triangle_ray(d);
+        r = slab_ray(o, d);
+        tri_ray = triangle_ray(d);
+        rotated = false;
         lo = o;
         ld = d;
         inst = kEmpty;
@@ -412,16 +413,17 @@ struct Walker {
                 local_ray(I, o, d, lo, ld);
                 cn.instances++;
                 // A local direction bit-identical to the world direction
-                // (translation-only instances) reuses the world constants.
-                if (as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) && as_uint(ld.z) == as_uint(d.z)) {
-                    r = world;
+                // (translation-only instances) keeps the world constants;
+                // only the origin moves.
+                rotated = !(as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) &&
+                            as_uint(ld.z) == as_uint(d.z));
+                if (rotated) {
+                    r = slab_ray(lo, ld);
+                    tri_ray = triangle_ray(ld);
+                } else {
                     r.ox = lo.x;
                     r.oy = lo.y;
                     r.oz = lo.z;
-                    tri_ray = world_tri;
-                } else {
-                    r = slab_ray(lo, ld);
-                    tri_ray = triangle_ray(ld);
                 }
                 inst = first;
                 inst_flags = I.flags;
@@ -477,7 +479,15 @@ struct Walker {
                 }
                 blas_next = kEmpty;
                 blas_base = -1;
-                r = world;
+                if (rotated) {
+                    r = slab_ray(o, d);
+                    tri_ray = triangle_ray(d);
+                    rotated = false;
+                } else {
+                    r.ox = o.x;
+                    r.oy = o.y;
+                    r.oz = o.z;
+                }
                 inst = kEmpty;
                 continue;
             }

@@ -30,6 +30,16 @@
 #include "shade.cuh"
 #include "traverse.cuh"
 
+// Resident 128-thread blocks per SM the trace kernels are compiled for: the
+// register cap that trades walker state kept in registers against warps in
+// flight (6 blocks = 80 registers per thread).
+#ifndef LUX_CLOSEST_MIN_BLOCKS
+#define LUX_CLOSEST_MIN_BLOCKS 6
+#endif
+#ifndef LUX_SHADOW_MIN_BLOCKS
+#define LUX_SHADOW_MIN_BLOCKS 6
+#endif
+
 namespace {
 
 using lux::f3;
@@ -343,7 +353,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter) {
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
-__global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
+__global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                             const float4 *__restrict__ pos,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
     if (*V.error_flags) return;
@@ -378,7 +388,7 @@ __global__ void __launch_bounds__(128) closest_split_kernel(ViewDevice V, FrameP
 // starts at the cell centre and covers the level's interval (the dense
 // reference of src/transport_tests.rs:179-248 with BVH geometry).  The ray
 // index is the record index.
-__global__ void __launch_bounds__(128) closest_dense_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t level) {
+__global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_dense_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t level) {
     if (*V.error_flags) return;
     unsigned long long n = (unsigned long long)V.cell_count[level] * F.dirs[level];
     unsigned long long base = V.level_base[level];
@@ -554,7 +564,7 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
     add_stats(V.stats, st, extra);
 }
 
-__global__ void __launch_bounds__(128) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
+__global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -1330,7 +1340,7 @@ __global__ void scratch_clear_kernel(ViewDevice V) {
     if (blockIdx.x == 0 && threadIdx.x < 16) V.stats[threadIdx.x] = 0;
 }
 
-__global__ void __launch_bounds__(128) closest_rays_kernel(ViewDevice V, SceneView S, const LuxRay *__restrict__ rays,
+__global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_rays_kernel(ViewDevice V, SceneView S, const LuxRay *__restrict__ rays,
                                                            uint32_t count) {
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
