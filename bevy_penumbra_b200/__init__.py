@@ -291,6 +291,22 @@ class GpuScene:
         keys = ("nodes", "node_bytes", "triangles", "triangle_bytes", "instances")
         return {k: v.value for k, v in zip(keys, vals)}
 
+    def refit(self, world_from_local, lights=None) -> None:
+        """lux_scene_refit: new float[instances, 3, 4] poses in instance-record
+        (slot) order; optional replacement light records (LuxLight dtype)."""
+        m = np.ascontiguousarray(world_from_local, dtype=np.float32).reshape(-1, 12)
+        lp, ln = (None, 0)
+        if lights is not None:
+            lights = np.ascontiguousarray(lights)
+            lp, ln = _ptr(lights), len(lights)
+        self.ctx.check(lib().lux_scene_refit(self.handle, _ptr(m), len(m), lp, ln))
+
+    def read_words(self) -> np.ndarray:
+        """lux_scene_read_words: the device scene words (uint32[words, 4])."""
+        out = np.zeros((len(self.packed.scene_words), 4), dtype=np.uint32)
+        self.ctx.check(lib().lux_scene_read_words(self.handle, _ptr(out), len(out)))
+        return out
+
     def close(self) -> None:
         if self.handle:
             lib().lux_scene_destroy(self.handle)
@@ -310,17 +326,24 @@ HIT_DTYPE = np.dtype([("distance", "<f4"), ("triangle", "<u4"), ("instance", "<u
 
 def trace_rays(ctx: LuxContext, scene: GpuScene, rays_device_ptr: int, count: int, hits_device_ptr: int,
                any_hit: bool = False) -> None:
-    """lux_trace_rays on device buffers of RAY_DTYPE / HIT_DTYPE records."""
+    """lux_trace_rays on device buffers of RAY_DTYPE / HIT_DTYPE records.
+
+    The launch is ordered on the context's stream; this wrapper waits for it,
+    so the hits can be read from any stream when it returns.  The rays must
+    be complete in device memory before the call."""
     ctx.check(lib().lux_trace_rays(ctx.handle, scene.handle, rays_device_ptr, count, 1 if any_hit else 0,
                                    hits_device_ptr))
+    ctx.synchronize()
 
 
 def interval_radiance(ctx: LuxContext, scene: GpuScene, settings: RadianceCascades, rays_device_ptr: int,
                       count: int, out_device_ptr: int) -> None:
-    """lux_interval_radiance: float4 (radiance rgb, hit distance | -1) per ray."""
+    """lux_interval_radiance: float4 (radiance rgb, hit distance | -1) per ray.
+    Waits for the context's stream before returning (see trace_rays)."""
     s = settings.to_c()
     ctx.check(lib().lux_interval_radiance(ctx.handle, scene.handle, C.byref(s), rays_device_ptr, count,
                                           out_device_ptr))
+    ctx.synchronize()
 
 
 class SplitView:

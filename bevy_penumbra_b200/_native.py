@@ -122,6 +122,8 @@ SIGNATURES = {
     "lux_packed_scene_destroy": (None, [P]),
     "lux_scene_upload": (C.c_int, [P, P, SZ, P, SZ, P, U32, U32, C.POINTER(P)]),
     "lux_scene_destroy": (C.c_int, [P]),
+    "lux_scene_refit": (C.c_int, [P, P, U32, P, U32]),
+    "lux_scene_read_words": (C.c_int, [P, P, SZ]),
     "lux_scene_layout": (C.c_int, [P, C.POINTER(U32), C.POINTER(U32), C.POINTER(U32), C.POINTER(U32),
                                    C.POINTER(U32)]),
     "lux_trace_rays": (C.c_int, [P, P, P, U32, U32, P]),

@@ -51,7 +51,7 @@ struct SceneView {
     uint32_t geometry_word_count;
     uint32_t conventional_lights;
     uint32_t emissive_lights;
-    float root_lo[3], root_hi[3];   // binary TLAS root box (root test of traceRayTracked)
+    float root_lo[3], root_hi[3];   // TLAS root box at upload (quantises coherence sort keys only)
 };
 
 // Wavefront trace scratch (the reference's deferred-trace slots and query
@@ -121,7 +121,25 @@ struct LuxScene {
     void *d_nodes = nullptr, *d_tris = nullptr, *d_inst = nullptr, *d_sw = nullptr, *d_gw = nullptr,
          *d_lights = nullptr;
     uint32_t node_count = 0;
+    // Refit state (lux_scene_refit): host copies of the instance records and
+    // device instances, the TLAS binary nodes by depth, and where every TLAS
+    // BVH4 child slot takes its box from.
+    uint32_t instance_base = 0;                 // first instance word
+    std::vector<uint32_t> instance_words;       // inst_count * 9 uint4 words
+    std::vector<DeviceInstance> instances;
+    std::vector<uint32_t> depth_start;          // refit order offsets, one per depth + 1
+    uint32_t slot_count = 0;                    // TLAS BVH4 nodes * 4
+    uint32_t *d_refit_order = nullptr;          // binary TLAS nodes, deepest depth first
+    uint32_t *d_depth_start = nullptr;
+    uint2 *d_slot_source = nullptr;             // (binary node, instance or kEmpty) per slot
+    uint32_t light_count = 0;
 };
+
+// local_from_world of a 3x4 world_from_local (row-major), inverted in f64
+// and rounded to f32; false when the linear part is singular or not finite.
+// Shared by the packer and lux_scene_refit so a refit to a pose writes the
+// same instance rows as packing the scene at that pose.
+bool lux_affine_inverse(const float world_from_local[12], float local_from_world[12]);
 
 lux_status lux_fail(LuxContext *ctx, lux_status status, const std::string &message);
 lux_status lux_cuda_check(LuxContext *ctx, int err, const char *what);

@@ -42,6 +42,10 @@ struct Collapser {
     // instance is entered (ray transform, BLAS root test) only when the ray
     // meets that instance's box rather than the whole leaf's.
     const std::vector<BinNode> *element_box = nullptr;
+    // Where each child slot's box comes from (TLAS only, for refit):
+    // (binary node, instance) -- the instance is kEmpty unless the slot is a
+    // single-instance child cut from binary leaf `x`.
+    std::vector<uint2> *sources = nullptr;
 
     static double area(const BinNode &n) {
         double sx = (double)n.mx[0] - n.mn[0], sy = (double)n.mx[1] - n.mn[1], sz = (double)n.mx[2] - n.mn[2];
@@ -57,10 +61,14 @@ struct Collapser {
             n.pad[i] = 0;
         }
         out.push_back(n);
+        if (sources)
+            for (int i = 0; i < 4; ++i) sources->push_back(make_uint2(lux::kEmpty, lux::kEmpty));
         return (uint32_t)out.size() - 1;
     }
 
-    void set_child(uint32_t node, int slot, const float mn[3], const float mx[3], uint32_t payload) {
+    void set_child(uint32_t node, int slot, const float mn[3], const float mx[3], uint32_t payload,
+                   uint32_t bin_index, uint32_t instance = lux::kEmpty) {
+        if (sources) (*sources)[4 * (size_t)node + slot] = make_uint2(bin_index, instance);
         Bvh4Node &n = out[node];
         n.lo_x[slot] = mn[0];
         n.lo_y[slot] = mn[1];
@@ -73,15 +81,15 @@ struct Collapser {
 
     // A leaf of `count` elements as one payload; ranges above 16 elements
     // become a small subtree of 16-element leaves with the leaf's box.
-    uint32_t leaf_payload(uint32_t first, uint32_t count, const float mn[3], const float mx[3]) {
+    uint32_t leaf_payload(uint32_t first, uint32_t count, const float mn[3], const float mx[3], uint32_t bin_index) {
         if (count <= kLeafMaxCount) return kLeafBit | (first & kLeafFirstMask) | ((count - 1u) << 27);
         uint32_t per = (count + 3u) / 4u;
         uint32_t node = new_node();
         int slot = 0;
         for (uint32_t start = 0; start < count && slot < 4; start += per, ++slot) {
             uint32_t c = std::min(per, count - start);
-            uint32_t p = leaf_payload(first + start, c, mn, mx);
-            set_child(node, slot, mn, mx, p);
+            uint32_t p = leaf_payload(first + start, c, mn, mx, bin_index);
+            set_child(node, slot, mn, mx, p, bin_index);
         }
         return node;
     }
@@ -111,11 +119,11 @@ struct Collapser {
                         mn[a] = std::max(e.mn[a], b.mn[a]);
                         mx[a] = std::min(e.mx[a], b.mx[a]);
                     }
-                    set_child(node, (int)k, mn, mx, kLeafBit | ((b.first + k) & kLeafFirstMask));
+                    set_child(node, (int)k, mn, mx, kLeafBit | ((b.first + k) & kLeafFirstMask), index, b.first + k);
                 }
                 return node;
             }
-            return leaf_payload(b.first, b.count, b.mn, b.mx);
+            return leaf_payload(b.first, b.count, b.mn, b.mx, index);
         }
         if ((size_t)b.first + 1 >= bin.size()) {
             error = "BVH child index out of range";
@@ -145,7 +153,7 @@ struct Collapser {
         for (size_t k = 0; k < kids.size(); ++k) {
             uint32_t p = collapse(kids[k], depth + 1);
             if (!error.empty()) return lux::kEmpty;
-            set_child(node, (int)k, bin[kids[k]].mn, bin[kids[k]].mx, p);
+            set_child(node, (int)k, bin[kids[k]].mn, bin[kids[k]].mx, p, kids[k]);
         }
         return node;
     }
@@ -156,7 +164,7 @@ struct Collapser {
         if (!error.empty()) return lux::kEmpty;
         if ((p & kLeafBit) == 0u) return p;
         uint32_t node = new_node();
-        set_child(node, 0, bin[index].mn, bin[index].mx, p);
+        set_child(node, 0, bin[index].mn, bin[index].mx, p, index);
         return node;
     }
 };
@@ -197,6 +205,107 @@ __global__ void trace_rays_kernel(SceneView S, const LuxRay *__restrict__ rays, 
             atomicAdd(&counters[1], t);
             atomicAdd(&counters[2], in);
         }
+    }
+}
+
+__device__ __forceinline__ float4 word_f4(const uint4 w) {
+    return make_float4(lux::as_float(w.x), lux::as_float(w.y), lux::as_float(w.z), lux::as_float(w.w));
+}
+
+// Conservative world box of one instance (refitTlas's leaf loop,
+// shaders/acceleration.slang:73-84), its error term scaled by `pad`: the
+// BLAS root box's centre and half extent through world_from_local (rows
+// 3-5), widened by (|t| + |M| max(|lo|, |hi|)) * 9.536743164e-7 * pad.
+__device__ void instance_world_box(const uint4 *__restrict__ sw, uint32_t inst_base, uint32_t instance, float pad,
+                                   float mn[3], float mx[3]) {
+    uint32_t base = inst_base + instance * 9u;
+    uint32_t root = sw[base + 8].x;
+    uint4 la = sw[1 + root * 2], ub = sw[2 + root * 2];
+    float a[3] = {lux::as_float(la.x), lux::as_float(la.y), lux::as_float(la.z)};
+    float b[3] = {lux::as_float(ub.x), lux::as_float(ub.y), lux::as_float(ub.z)};
+    float center[3], extent[3], absolute[3];
+    for (int k = 0; k < 3; ++k) {
+        center[k] = a[k] * 0.5f + b[k] * 0.5f;
+        extent[k] = b[k] * 0.5f - a[k] * 0.5f;
+        absolute[k] = fmaxf(fabsf(a[k]), fabsf(b[k]));
+    }
+    for (int r = 0; r < 3; ++r) {
+        float4 row = word_f4(sw[base + 3 + r]);
+        float wc = ((row.x * center[0] + row.y * center[1]) + row.z * center[2]) + row.w * 1.0f;
+        float we = (fabsf(row.x) * extent[0] + fabsf(row.y) * extent[1]) + fabsf(row.z) * extent[2];
+        float err = (fabsf(row.w) + ((fabsf(row.x) * absolute[0] + fabsf(row.y) * absolute[1]) +
+                                     fabsf(row.z) * absolute[2])) * 9.536743164e-7f;
+        err = err * pad;
+        mn[r] = (wc - we) - err;
+        mx[r] = (wc + we) + err;
+    }
+}
+
+// refitTlas (shaders/acceleration.slang:61-88) for every depth in one block:
+// `order` lists the binary TLAS nodes deepest depth first, so each pass
+// reads children written by the previous one (a block barrier between
+// depths).  Then every TLAS BVH4 child slot takes the refit box of the
+// binary node it was collapsed from; single-instance slots take the
+// instance's own box (error term x8, so it contains refitTlas's) cut by the
+// refit leaf box.
+__global__ void __launch_bounds__(1024) refit_kernel(uint4 *__restrict__ sw, uint32_t inst_base,
+                                                     const uint32_t *__restrict__ order,
+                                                     const uint32_t *__restrict__ depth_start, uint32_t depths,
+                                                     Bvh4Node *__restrict__ nodes, const uint2 *__restrict__ source,
+                                                     uint32_t slots) {
+    for (uint32_t d = 0; d < depths; ++d) {
+        for (uint32_t k = depth_start[d] + threadIdx.x; k < depth_start[d + 1]; k += blockDim.x) {
+            uint32_t node = order[k];
+            uint4 lower = sw[1 + node * 2], upper = sw[2 + node * 2];
+            float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+            float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+            if (upper.w == 0u) {
+                uint32_t child = lower.w;
+                uint4 a0 = sw[1 + child * 2], a1 = sw[1 + (child + 1) * 2];
+                uint4 b0 = sw[2 + child * 2], b1 = sw[2 + (child + 1) * 2];
+                mn[0] = fminf(lux::as_float(a0.x), lux::as_float(a1.x));
+                mn[1] = fminf(lux::as_float(a0.y), lux::as_float(a1.y));
+                mn[2] = fminf(lux::as_float(a0.z), lux::as_float(a1.z));
+                mx[0] = fmaxf(lux::as_float(b0.x), lux::as_float(b1.x));
+                mx[1] = fmaxf(lux::as_float(b0.y), lux::as_float(b1.y));
+                mx[2] = fmaxf(lux::as_float(b0.z), lux::as_float(b1.z));
+            } else {
+                for (uint32_t i = lower.w; i < lower.w + upper.w; ++i) {
+                    float a[3], b[3];
+                    instance_world_box(sw, inst_base, i, 1.0f, a, b);
+                    for (int r = 0; r < 3; ++r) {
+                        mn[r] = fminf(mn[r], a[r]);
+                        mx[r] = fmaxf(mx[r], b[r]);
+                    }
+                }
+            }
+            sw[1 + node * 2] = make_uint4(lux::as_uint(mn[0]), lux::as_uint(mn[1]), lux::as_uint(mn[2]), lower.w);
+            sw[2 + node * 2] = make_uint4(lux::as_uint(mx[0]), lux::as_uint(mx[1]), lux::as_uint(mx[2]), upper.w);
+        }
+        __syncthreads();
+    }
+    for (uint32_t slot = threadIdx.x; slot < slots; slot += blockDim.x) {
+        uint2 src = source[slot];
+        if (src.x == lux::kEmpty) continue;
+        uint4 la = sw[1 + src.x * 2], ub = sw[2 + src.x * 2];
+        float mn[3] = {lux::as_float(la.x), lux::as_float(la.y), lux::as_float(la.z)};
+        float mx[3] = {lux::as_float(ub.x), lux::as_float(ub.y), lux::as_float(ub.z)};
+        if (src.y != lux::kEmpty) {
+            float a[3], b[3];
+            instance_world_box(sw, inst_base, src.y, 8.0f, a, b);
+            for (int r = 0; r < 3; ++r) {
+                mn[r] = fmaxf(mn[r], a[r]);
+                mx[r] = fminf(mx[r], b[r]);
+            }
+        }
+        Bvh4Node &n = nodes[slot / 4];
+        uint32_t c = slot % 4;
+        n.lo_x[c] = mn[0];
+        n.lo_y[c] = mn[1];
+        n.lo_z[c] = mn[2];
+        n.hi_x[c] = mx[0];
+        n.hi_y[c] = mx[1];
+        n.hi_z[c] = mx[2];
     }
 }
 
@@ -307,16 +416,39 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     nodes.reserve(node_count / 2 + 16);
     uint32_t tlas_root = lux::kEmpty;
     float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
+    std::vector<uint2> slot_source;
+    std::vector<uint32_t> refit_order, depth_start;
     if (inst_count > 0) {
         if (node_count == 0) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: no TLAS nodes");
-        Collapser tl{bin, nodes, {}, inst_count, &inst_box};
+        Collapser tl{bin, nodes, {}, inst_count, &inst_box, &slot_source};
         tlas_root = tl.root(0);
         if (!tl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (TLAS): " + tl.error);
         for (int k = 0; k < 3; ++k) {
             root_lo[k] = bin[0].mn[k];
             root_hi[k] = bin[0].mx[k];
         }
+        // Binary TLAS nodes grouped by depth, deepest first: the pass order
+        // of refitTlas (shaders/acceleration.slang:61), where each depth's
+        // children are final before their parents read them.
+        std::vector<std::vector<uint32_t>> by_depth;
+        std::vector<std::pair<uint32_t, uint32_t>> todo = {{0u, 0u}};
+        while (!todo.empty()) {
+            auto [index, depth] = todo.back();
+            todo.pop_back();
+            if (by_depth.size() <= depth) by_depth.resize(depth + 1);
+            by_depth[depth].push_back(index);
+            if (bin[index].count == 0) {
+                todo.push_back({bin[index].first, depth + 1});
+                todo.push_back({bin[index].first + 1, depth + 1});
+            }
+        }
+        for (size_t d = by_depth.size(); d-- > 0;) {
+            depth_start.push_back((uint32_t)refit_order.size());
+            refit_order.insert(refit_order.end(), by_depth[d].begin(), by_depth[d].end());
+        }
+        depth_start.push_back((uint32_t)refit_order.size());
     }
+    uint32_t tlas_slots = (uint32_t)slot_source.size();
     std::unordered_map<uint32_t, uint32_t> blas_root;
     for (uint32_t i = 0; i < inst_count; ++i) {
         auto it = blas_root.find(inst[i].root);
@@ -352,7 +484,10 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     LuxScene *S = new LuxScene();
     S->ctx = ctx;
     auto alloc_copy = [&](void **dst, const void *src, size_t bytes) -> bool {
-        if (bytes == 0) bytes = 16;
+        if (bytes == 0) {
+            bytes = 16;
+            src = nullptr;
+        }
         if (cudaMalloc(dst, bytes) != cudaSuccess) return false;
         if (src && cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice) != cudaSuccess) return false;
         return true;
@@ -361,7 +496,10 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
               alloc_copy(&S->d_tris, tris.data(), tris.size() * sizeof(float4)) &&
               alloc_copy(&S->d_inst, inst.data(), inst.size() * sizeof(DeviceInstance)) &&
               alloc_copy(&S->d_sw, sw, sn * 16) && alloc_copy(&S->d_gw, gw, gn * 16) &&
-              alloc_copy(&S->d_lights, lights, (size_t)light_count * sizeof(LuxLight));
+              alloc_copy(&S->d_lights, lights, (size_t)light_count * sizeof(LuxLight)) &&
+              alloc_copy((void **)&S->d_refit_order, refit_order.data(), refit_order.size() * 4) &&
+              alloc_copy((void **)&S->d_depth_start, depth_start.data(), depth_start.size() * 4) &&
+              alloc_copy((void **)&S->d_slot_source, slot_source.data(), slot_source.size() * sizeof(uint2));
     if (!ok) {
         cudaGetLastError();
         lux_scene_destroy(S);
@@ -386,6 +524,12 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
         V.root_hi[k] = root_hi[k];
     }
     S->node_count = (uint32_t)nodes.size();
+    S->instance_base = inst_base;
+    S->instance_words.assign(sw + 4 * (size_t)inst_base, sw + 4 * ((size_t)inst_base + 9 * (size_t)inst_count));
+    S->instances = inst;
+    S->depth_start = depth_start;
+    S->slot_count = tlas_slots;
+    S->light_count = light_count;
     *out = S;
     return LUX_OK;
 }
@@ -398,6 +542,9 @@ extern "C" lux_status lux_scene_destroy(LuxScene *S) {
     cudaFree(S->d_sw);
     cudaFree(S->d_gw);
     cudaFree(S->d_lights);
+    cudaFree(S->d_refit_order);
+    cudaFree(S->d_depth_start);
+    cudaFree(S->d_slot_source);
     delete S;
     return LUX_OK;
 }
@@ -411,6 +558,86 @@ extern "C" lux_status lux_scene_layout(const LuxScene *S, uint32_t *nodes, uint3
     if (triangle_bytes) *triangle_bytes = 48u;
     if (instances) *instances = S->view.instance_count;
     return LUX_OK;
+}
+
+extern "C" lux_status lux_scene_refit(LuxScene *S, const float *wfl, uint32_t count, const LuxLight *lights,
+                                      uint32_t light_count) {
+    if (!S) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = S->ctx;
+    uint32_t n = S->view.instance_count;
+    if (count != n || (n && !wfl))
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene refit: need one world_from_local per instance");
+    if (lights && light_count != S->light_count)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene refit: light count differs from the upload");
+    if (lights)
+        for (uint32_t l = S->view.conventional_lights; l < light_count; ++l)
+            if (lights[l].source[0] >= n)
+                return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene refit: emitter record outside the scene");
+    if (n == 0 && !lights) return LUX_OK;
+    // Host half: instance rows 0-5 and the device instances' local_from_world.
+    std::vector<uint32_t> words = S->instance_words;
+    std::vector<DeviceInstance> inst = S->instances;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *m = wfl + 12 * (size_t)i;
+        for (int k = 0; k < 12; ++k)
+            if (!std::isfinite(m[k]))
+                return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene refit: non-finite transform");
+        float lfw[12];
+        if (!lux_affine_inverse(m, lfw))
+            return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene refit: singular transform");
+        uint32_t *w = words.data() + 36 * (size_t)i;
+        for (int k = 0; k < 12; ++k) {
+            std::memcpy(&w[k], &lfw[k], 4);
+            std::memcpy(&w[12 + k], &m[k], 4);
+        }
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) inst[i].row[r][c] = lfw[4 * r + c];
+    }
+    cudaStream_t st = ctx->stream;
+    cudaSetDevice(ctx->device);
+    uint4 *sw = (uint4 *)S->d_sw;
+    lux_status rc = LUX_OK;
+    if (n) {
+        rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(sw + S->instance_base, words.data(), words.size() * 4,
+                                                      cudaMemcpyHostToDevice, st),
+                            "scene refit: instance words");
+        if (rc == LUX_OK)
+            rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(S->d_inst, inst.data(), inst.size() * sizeof(DeviceInstance),
+                                                          cudaMemcpyHostToDevice, st),
+                                "scene refit: instances");
+    }
+    if (rc == LUX_OK && lights)
+        rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(S->d_lights, lights, (size_t)light_count * sizeof(LuxLight),
+                                                      cudaMemcpyHostToDevice, st),
+                            "scene refit: lights");
+    if (rc != LUX_OK) return rc;
+    if (n) {
+        uint32_t depths = S->depth_start.empty() ? 0u : (uint32_t)S->depth_start.size() - 1u;
+        refit_kernel<<<1, 1024, 0, st>>>(sw, S->instance_base, S->d_refit_order, S->d_depth_start, depths,
+                                         (Bvh4Node *)S->d_nodes, S->d_slot_source, S->slot_count);
+        rc = lux_cuda_check(ctx, (int)cudaGetLastError(), "scene refit: launch");
+        if (rc != LUX_OK) return rc;
+    }
+    // The pageable copies above may return before the transfer completes;
+    // keep the staging vectors alive until the stream has consumed them.
+    rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "scene refit");
+    if (rc != LUX_OK) return rc;
+    S->instance_words.swap(words);
+    S->instances.swap(inst);
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_scene_read_words(const LuxScene *S, uint32_t *out, size_t word_count) {
+    if (!S || !out) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = S->ctx;
+    if (word_count != S->view.scene_word_count)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene words: count differs from the upload");
+    cudaSetDevice(ctx->device);
+    lux_status rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(out, S->d_sw, word_count * 16, cudaMemcpyDeviceToHost,
+                                                             ctx->stream),
+                                   "scene words: copy");
+    if (rc != LUX_OK) return rc;
+    return lux_cuda_check(ctx, (int)cudaStreamSynchronize(ctx->stream), "scene words: synchronize");
 }
 
 lux_status lux_launch_trace_rays(LuxContext *ctx, const LuxScene *scene, const LuxRay *rays, uint32_t count,

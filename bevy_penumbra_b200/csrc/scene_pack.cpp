@@ -297,22 +297,13 @@ extern "C" lux_status lux_scene_pack(const float *positions, uint32_t vertex_cou
                     I.w[r][c] = m[4 * r + c];
                     I.wfl[r][c] = m[4 * r + c];
                 }
-            // Affine inverse in f64.
-            double a = I.w[0][0], b = I.w[0][1], c = I.w[0][2], d = I.w[1][0], e = I.w[1][1], f = I.w[1][2],
-                   g = I.w[2][0], h = I.w[2][1], k = I.w[2][2];
-            double det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
-            if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) {
+            float lfw[12];
+            if (!lux_affine_inverse(m, lfw)) {
                 delete P;
                 return LUX_ERR_INVALID_ARGUMENT;
             }
-            double inv[3][3] = {{(e * k - f * h) / det, (c * h - b * k) / det, (b * f - c * e) / det},
-                                {(f * g - d * k) / det, (a * k - c * g) / det, (c * d - a * f) / det},
-                                {(d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det}};
-            for (int r = 0; r < 3; ++r) {
-                double t = -(inv[r][0] * I.w[0][3] + inv[r][1] * I.w[1][3] + inv[r][2] * I.w[2][3]);
-                for (int cc = 0; cc < 3; ++cc) I.lfw[r][cc] = (float)inv[r][cc];
-                I.lfw[r][3] = (float)t;
-            }
+            for (int r = 0; r < 3; ++r)
+                for (int cc = 0; cc < 4; ++cc) I.lfw[r][cc] = lfw[4 * r + cc];
             const Box &mb = mesh_box[instance_mesh[i]];
             Box wb;
             for (int r = 0; r < 3; ++r) {
@@ -517,3 +508,22 @@ extern "C" lux_status lux_packed_scene_quality(const LuxPackedScene *p, double *
 }
 
 extern "C" void lux_packed_scene_destroy(LuxPackedScene *p) { delete p; }
+
+bool lux_affine_inverse(const float m[12], float out[12]) {
+    double w[3][4];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) w[r][c] = m[4 * r + c];
+    double a = w[0][0], b = w[0][1], c = w[0][2], d = w[1][0], e = w[1][1], f = w[1][2], g = w[2][0], h = w[2][1],
+           k = w[2][2];
+    double det = a * (e * k - f * h) - b * (d * k - f * g) + c * (d * h - e * g);
+    if (!(std::fabs(det) > 0.0) || !std::isfinite(det)) return false;
+    double inv[3][3] = {{(e * k - f * h) / det, (c * h - b * k) / det, (b * f - c * e) / det},
+                        {(f * g - d * k) / det, (a * k - c * g) / det, (c * d - a * f) / det},
+                        {(d * h - e * g) / det, (b * g - a * h) / det, (a * e - b * d) / det}};
+    for (int r = 0; r < 3; ++r) {
+        double t = -(inv[r][0] * w[0][3] + inv[r][1] * w[1][3] + inv[r][2] * w[2][3]);
+        for (int cc = 0; cc < 3; ++cc) out[4 * r + cc] = (float)inv[r][cc];
+        out[4 * r + 3] = (float)t;
+    }
+    return true;
+}

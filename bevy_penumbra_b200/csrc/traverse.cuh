@@ -313,9 +313,12 @@ struct Walker {
         hit.b1 = 0.0f;
         hit.b2 = 0.0f;
         if (S.instance_count == 0) return false;
+        // The TLAS root box is read from the live scene words (node 0), so a
+        // device-side refit takes effect without a host round trip.
         float re, rx;
-        if (!box_interval(origin, direction, S.root_lo[0], S.root_lo[1], S.root_lo[2], S.root_hi[0], S.root_hi[1],
-                          S.root_hi[2], limit, re, rx))
+        uint4 ra = __ldg(S.scene_words + 1), rb = __ldg(S.scene_words + 2);
+        if (!box_interval(origin, direction, as_float(ra.x), as_float(ra.y), as_float(ra.z), as_float(rb.x),
+                          as_float(rb.y), as_float(rb.z), limit, re, rx))
             return false;
         o = origin;
         d = direction;

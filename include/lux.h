@@ -240,6 +240,24 @@ lux_status lux_scene_layout(const LuxScene *scene, uint32_t *nodes, uint32_t *no
                             uint32_t *triangles, uint32_t *triangle_bytes,
                             uint32_t *instances);
 
+/* Rigid pose update of every instance: the host half writes each instance's
+ * rows 0-5 (local_from_world, inverted in f64 like the packer, and
+ * world_from_local) as the reference's instance upload does
+ * (src/render.rs:3819-3915), then one device launch refits the TLAS bottom-up
+ * by depth with refitTlas's conservative transformed boxes
+ * (shaders/acceleration.slang:61-88) and rewrites the BVH4 child boxes.  The
+ * tree topology is kept.  world_from_local: host float[count * 12], row-major
+ * 3x4, in instance-record order (the packed scene's slot order); count must
+ * equal the scene's instance count.  lights: NULL to keep the uploaded
+ * records, else light_count (= the uploaded count) replacement records
+ * (moved emitters).  Stream-ordered on the context stream. */
+lux_status lux_scene_refit(LuxScene *scene, const float *world_from_local, uint32_t count,
+                           const LuxLight *lights, uint32_t light_count);
+/* Copies the scene's device words (scene_words as uploaded, with refit boxes
+ * and instance rows) to host memory: out[word_count * 4]; word_count must
+ * equal the uploaded scene word count.  Synchronises the context stream. */
+lux_status lux_scene_read_words(const LuxScene *scene, uint32_t *out, size_t word_count);
+
 /* ---- traversal (traceRay / traceOccluded, shaders/traversal.slang:696-1046) -- */
 /* Closest hit (any_hit = 0) or occlusion (any_hit = 1) for `count` rays.
  * rays: device LuxRay[count]; hits: device LuxHit[count].  For any-hit rays

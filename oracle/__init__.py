@@ -53,6 +53,8 @@ def lib():
             "orc_spacing": (F, [P, U]),
             "orc_scene_create": (P, [P, C.c_size_t, P, C.c_size_t, P, U, U]),
             "orc_scene_destroy": (None, [P]),
+            "orc_scene_refit": (C.c_int, [P, P, C.c_uint32]),
+            "orc_scene_words": (None, [P, P]),
             "orc_trace_closest": (None, [P, P, P, F, F, P, P]),
             "orc_trace_occluded": (C.c_int, [P, P, P, F, P, P]),
             "orc_brute_closest": (None, [P, P, P, F, F, P]),
@@ -122,6 +124,18 @@ class OracleScene:
         n = lib().orc_brute_f64(self.handle, _p(o), _p(d), float(limit), _p(t), _p(tri), _p(inst), capacity)
         n = min(int(n), capacity)
         return t[:n], tri[:n], inst[:n]
+
+    def refit(self, world_from_local) -> None:
+        """Pose update + TLAS refit (float[instances, 3, 4], slot order)."""
+        m = np.ascontiguousarray(world_from_local, dtype=np.float32).reshape(-1, 12)
+        rc = lib().orc_scene_refit(self.handle, _p(m), len(m))
+        if rc != 0:
+            raise ValueError("oracle refit: instance count mismatch or singular transform")
+
+    def words(self) -> np.ndarray:
+        out = np.zeros(self._keep[0].shape, dtype=np.uint32).reshape(-1, 4)
+        lib().orc_scene_words(self.handle, _p(out))
+        return out
 
     def close(self):
         if self.handle:

@@ -268,6 +268,7 @@ void orc_scene_destroy(OrcScene *S) {
 
 typedef struct { float mn[3]; uint32_t first; float mx[3]; uint32_t count; } Node;
 
+
 /* sceneNode, shaders/traversal.slang:192-196. */
 static inline Node scene_node(const OrcScene *S, uint32_t index) {
     U4 a = sword(S, 1 + index * 2), b = sword(S, 2 + index * 2);
@@ -282,6 +283,126 @@ static inline uint32_t instance_base(const OrcScene *S, uint32_t instance) {
     U4 h = sword(S, 0);
     return h.y + instance * h.w;
 }
+
+static inline float word_f(uint32_t w) { return asf(w); }
+
+/* refitTlas's transformed box for one instance (shaders/acceleration.slang:
+ * 73-84): BLAS root box centre/extent through world_from_local (rows 3-5),
+ * error (|t| + |M| max(|a|,|b|)) * 9.536743164e-7. */
+static void refit_instance_box(const OrcScene *S, uint32_t instance, float mn[3], float mx[3]) {
+    uint32_t base = sword(S, 0).y + instance * sword(S, 0).w;
+    uint32_t root = sword(S, base + 8).x;
+    U4 la = sword(S, 1 + root * 2), ub = sword(S, 2 + root * 2);
+    float a[3] = {word_f(la.x), word_f(la.y), word_f(la.z)};
+    float b[3] = {word_f(ub.x), word_f(ub.y), word_f(ub.z)};
+    float center[3], extent[3], absolute[3];
+    for (int k = 0; k < 3; ++k) {
+        center[k] = a[k] * 0.5f + b[k] * 0.5f;
+        extent[k] = b[k] * 0.5f - a[k] * 0.5f;
+        absolute[k] = fmaxf(fabsf(a[k]), fabsf(b[k]));
+    }
+    for (int r = 0; r < 3; ++r) {
+        U4 w = sword(S, base + 3 + r);
+        float x = word_f(w.x), y = word_f(w.y), z = word_f(w.z), t = word_f(w.w);
+        float wc = ((x * center[0] + y * center[1]) + z * center[2]) + t * 1.0f;
+        float we = (fabsf(x) * extent[0] + fabsf(y) * extent[1]) + fabsf(z) * extent[2];
+        float err = (fabsf(t) + ((fabsf(x) * absolute[0] + fabsf(y) * absolute[1]) + fabsf(z) * absolute[2])) *
+                    9.536743164e-7f;
+        mn[r] = (wc - we) - err;
+        mx[r] = (wc + we) + err;
+    }
+}
+
+static void put_word(OrcScene *S, uint32_t index, uint32_t x, uint32_t y, uint32_t z, uint32_t w) {
+    uint32_t *p = S->sw + 4 * (size_t)index;
+    p[0] = x; p[1] = y; p[2] = z; p[3] = w;
+}
+
+static uint32_t fbits_u(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+
+/* Rigid pose update (host instance upload, src/render.rs:3819-3915, then
+ * refitTlas by depth, shaders/acceleration.slang:61-88).  Rows 0-2 get
+ * local_from_world (f64 inverse rounded to f32), rows 3-5 world_from_local;
+ * TLAS nodes are refit deepest depth first.  Returns 0, or -1 for a count
+ * mismatch / singular transform. */
+int orc_scene_refit(OrcScene *S, const float *wfl, uint32_t count) {
+    uint32_t n = instance_count(S);
+    if (count != n) return -1;
+    U4 h = sword(S, 0);
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *m = wfl + 12 * (size_t)i;
+        double w[3][4];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) w[r][c] = m[4 * r + c];
+        double a = w[0][0], b = w[0][1], c = w[0][2], d = w[1][0], e = w[1][1], f = w[1][2], g = w[2][0],
+               hh = w[2][1], k = w[2][2];
+        double det = a * (e * k - f * hh) - b * (d * k - f * g) + c * (d * hh - e * g);
+        if (!(fabs(det) > 0.0) || !isfinite(det)) return -1;
+        double inv[3][3] = {{(e * k - f * hh) / det, (c * hh - b * k) / det, (b * f - c * e) / det},
+                            {(f * g - d * k) / det, (a * k - c * g) / det, (c * d - a * f) / det},
+                            {(d * hh - e * g) / det, (b * g - a * hh) / det, (a * e - b * d) / det}};
+        uint32_t base = h.y + i * h.w;
+        for (int r = 0; r < 3; ++r) {
+            double t = -(inv[r][0] * w[0][3] + inv[r][1] * w[1][3] + inv[r][2] * w[2][3]);
+            put_word(S, base + r, fbits_u((float)inv[r][0]), fbits_u((float)inv[r][1]), fbits_u((float)inv[r][2]),
+                     fbits_u((float)t));
+            put_word(S, base + 3 + r, fbits_u(m[4 * r]), fbits_u(m[4 * r + 1]), fbits_u(m[4 * r + 2]),
+                     fbits_u(m[4 * r + 3]));
+        }
+    }
+    if (n == 0) return 0;
+    /* Depth of every TLAS node (DFS from node 0), then passes deepest first. */
+    uint32_t node_total = (h.y - 1u) / 2u;
+    uint32_t *depth = (uint32_t *)malloc(sizeof(uint32_t) * (node_total ? node_total : 1));
+    uint8_t *in_tlas = (uint8_t *)calloc(node_total ? node_total : 1, 1);
+    uint32_t *todo = (uint32_t *)malloc(sizeof(uint32_t) * (2 * (size_t)node_total + 2));
+    uint32_t top = 0, max_depth = 0;
+    todo[top++] = 0;
+    depth[0] = 0;
+    while (top) {
+        uint32_t i = todo[--top];
+        in_tlas[i] = 1;
+        Node nd = scene_node(S, i);
+        if (depth[i] > max_depth) max_depth = depth[i];
+        if (nd.count == 0 && nd.first + 1 < node_total) {
+            depth[nd.first] = depth[nd.first + 1] = depth[i] + 1;
+            todo[top++] = nd.first;
+            todo[top++] = nd.first + 1;
+        }
+    }
+    for (int64_t dd = max_depth; dd >= 0; --dd)
+        for (uint32_t i = 0; i < node_total; ++i) {
+            if (!in_tlas[i] || depth[i] != (uint32_t)dd) continue;
+            U4 lower = sword(S, 1 + i * 2), upper = sword(S, 2 + i * 2);
+            float mn[3] = {3.402823466e+38f, 3.402823466e+38f, 3.402823466e+38f};
+            float mx[3] = {-3.402823466e+38f, -3.402823466e+38f, -3.402823466e+38f};
+            if (upper.w == 0) {
+                Node c0 = scene_node(S, lower.w), c1 = scene_node(S, lower.w + 1);
+                for (int k = 0; k < 3; ++k) {
+                    mn[k] = fminf(c0.mn[k], c1.mn[k]);
+                    mx[k] = fmaxf(c0.mx[k], c1.mx[k]);
+                }
+            } else {
+                for (uint32_t inst = lower.w; inst < lower.w + upper.w; ++inst) {
+                    float a[3], b[3];
+                    refit_instance_box(S, inst, a, b);
+                    for (int k = 0; k < 3; ++k) {
+                        mn[k] = fminf(mn[k], a[k]);
+                        mx[k] = fmaxf(mx[k], b[k]);
+                    }
+                }
+            }
+            put_word(S, 1 + i * 2, fbits_u(mn[0]), fbits_u(mn[1]), fbits_u(mn[2]), lower.w);
+            put_word(S, 2 + i * 2, fbits_u(mx[0]), fbits_u(mx[1]), fbits_u(mx[2]), upper.w);
+        }
+    free(depth);
+    free(in_tlas);
+    free(todo);
+    return 0;
+}
+
+/* The scene words (after refits): out[sn * 4]. */
+void orc_scene_words(const OrcScene *S, uint32_t *out) { memcpy(out, S->sw, 16 * S->sn); }
 
 /* localTriangle, shaders/traversal.slang:158-173. */
 static void local_triangle(const OrcScene *S, uint32_t triangle, U4 header, float a[3], float b[3],

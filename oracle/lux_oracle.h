@@ -49,6 +49,8 @@ OrcScene *orc_scene_create(const uint32_t *scene_words, size_t scene_word_count,
                            const LuxLight *lights, uint32_t light_count,
                            uint32_t conventional_lights);
 void orc_scene_destroy(OrcScene *scene);
+int orc_scene_refit(OrcScene *scene, const float *world_from_local, uint32_t count);
+void orc_scene_words(const OrcScene *scene, uint32_t *out);
 
 typedef struct OrcCounters {
     uint64_t nodes;      /* binary BVH nodes whose box was tested */

@@ -186,6 +186,7 @@ def to_device(arr: np.ndarray):
     import torch
     a = np.ascontiguousarray(arr)
     t = torch.from_numpy(a.view(np.uint8).reshape(-1).copy()).cuda()
+    torch.cuda.synchronize()  # the library's stream does not order after torch's
     return t
 
 
@@ -195,7 +196,9 @@ def from_device(t, dtype, shape) -> np.ndarray:
 
 def empty_device(nbytes: int):
     import torch
-    return torch.zeros(max(nbytes, 16), dtype=torch.uint8, device="cuda")
+    t = torch.zeros(max(nbytes, 16), dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()  # the fill must land before the library writes
+    return t
 
 
 def cornell_dense_settings(**kw) -> bp.RadianceCascades:
