@@ -391,12 +391,148 @@ def run_ours(args, rank, world):
         dist.destroy_process_group()
 
 
+def build_batch_workload(device: int):
+    """The batched configuration: 64 seeded scenes (triangles log-uniform in
+    [1k, 200k]), each seen by one camera at 320x180, 640x360 or 1280x720 with
+    screen receivers at 4x4 px and the atrium's cascade settings."""
+    import torch
+
+    import bevy_penumbra_b200 as bp
+    from bevy_penumbra_b200 import scenes
+
+    t0 = time.time()
+    stream = torch.cuda.current_stream(device)
+    ctx = bp.LuxContext(device, stream.cuda_stream)
+    settings = settings_for_workload()
+    dev = f"cuda:{device}"
+    jobs, tris, res_counts = [], 0, {}
+    for seed, triangles, (width, height) in scenes.batch_workload(seed=3, scenes=64):
+        desc = scenes.batch_scene(seed, triangles)
+        packed = bp.PackedScene.from_desc(desc)
+        scene = bp.GpuScene(ctx, packed)
+        size = 6.0 + 18.0 * np.log(triangles / 1000.0 + 1.0) / np.log(201.0)
+        room_h = 3.0 + 0.25 * size
+        eye = (0.05 * size, 0.45 * room_h, -0.45 * size)
+        target = (-0.05 * size, 0.2 * room_h, 0.3 * size)
+        o, d = scenes.camera_rays(width, height, eye, target, 60.0, PROBE_PX)
+        rays = np.zeros(len(o), dtype=bp.RAY_DTYPE)
+        rays["origin"], rays["direction"], rays["limit"] = o, d, 1e20
+        d_rays = torch.from_numpy(rays.view(np.uint8).copy()).to(dev)
+        d_hits = torch.zeros(len(rays) * bp.HIT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+        torch.cuda.synchronize(device)
+        bp.trace_rays(ctx, scene, d_rays.data_ptr(), len(rays), d_hits.data_ptr())
+        hits = d_hits.cpu().numpy().view(bp.HIT_DTYPE)
+        ok = hits["triangle"] != 0xFFFFFFFF
+        pos = np.zeros((int(ok.sum()), 4), np.float32)
+        pos[:, :3] = o[ok] + d[ok] * hits["distance"][ok, None]
+        nrm = np.zeros_like(pos)
+        nrm[:, :3] = world_normals(packed, hits[ok], d[ok])
+        entries, cells_max = 0, 1
+        for level in range(settings.levels):
+            sp = np.float32(settings.probe_spacing * (1 << level))
+            cells = np.unique(np.floor(pos[:, :3] / sp).astype(np.int64), axis=0).shape[0] if len(pos) else 0
+            cells_max = max(cells_max, cells)
+            entries += cells * settings.direction_count(level)
+        n = len(pos)
+        view = bp.SplitView(ctx, max_receivers=max(n, 1), max_cells=cells_max, max_entries=max(entries, 1),
+                            max_rays=max(n, 1) * settings.rays_per_receiver)
+        jobs.append(dict(scene=scene, view=view, pos=torch.from_numpy(pos).to(dev), nrm=torch.from_numpy(nrm).to(dev),
+                         n=n, triangles=triangles, res=(width, height)))
+        tris += triangles
+        res_counts[f"{width}x{height}"] = res_counts.get(f"{width}x{height}", 0) + 1
+    torch.cuda.synchronize(device)
+    return dict(bp=bp, ctx=ctx, settings=settings, jobs=jobs, triangles=tris, resolutions=res_counts,
+                setup_s=time.time() - t0)
+
+
+def run_batched(args, rank, world):
+    """--workload batched: 64 scenes per step through lux_batch_trace_merge
+    (one persistent launch per trace stage, the frame replayed as a CUDA
+    graph), beside the same views traced one lux_view_trace_merge at a time."""
+    import torch
+
+    device = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(device)
+    work_stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(work_stream)
+    w = build_batch_workload(device)
+    bp, ctx, settings, jobs = w["bp"], w["ctx"], w["settings"], w["jobs"]
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{device}")
+    batch = bp.Batch(ctx)
+    args_jobs = [(j["view"], j["scene"], j["pos"].data_ptr(), j["nrm"].data_ptr(), j["n"]) for j in jobs]
+
+    def batched(step):
+        settings.frame_index = step
+        batch.trace_merge(args_jobs, settings)
+
+    def one_by_one(step):
+        settings.frame_index = step
+        for j in jobs:
+            j["view"].trace_merge(j["scene"], settings, j["pos"].data_ptr(), j["nrm"].data_ptr(), j["n"])
+
+    # Batch launch shape: the project autotuner's blocks-per-SM axis.
+    trials = []
+    for bps in (8, 16, 32):
+        batch.set_tuning(bps, bps)
+        batched(0)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        batched(1)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+        trials.append((bps, start.elapsed_time(end)))
+    best_bps = min(trials, key=lambda t: t[1])[0]
+    batch.set_tuning(best_bps, best_bps)
+
+    def timed(fn):
+        for step in range(args.warmup):
+            fn(step)
+        torch.cuda.synchronize(device)
+        ms = []
+        for step in range(args.steps):
+            flush.fill_(float(step))
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            fn(args.warmup + step)
+            end.record(stream)
+            torch.cuda.synchronize(device)
+            ms.append(start.elapsed_time(end))
+        return float(np.sum(ms)) / args.steps
+
+    with ClockSampler(device) as clocks:
+        batch_ms = timed(batched)
+    sequential_ms = timed(one_by_one)
+    rays = sum(j["n"] for j in jobs) * settings.rays_per_receiver
+    info = batch.info()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * rays / (batch_ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched: 64 seeded scenes, triangles log-uniform in [1k, 200k], views from "
+                                   "{320x180, 640x360, 1280x720}, receivers at 4x4 px, 8 cascades",
+                       "scenes": len(jobs), "triangles": w["triangles"], "resolutions": w["resolutions"],
+                       "interval_rays": rays, "rays_per_receiver": settings.rays_per_receiver,
+                       "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps"},
+            "batch": {"graph_captures": info.graph_captures, "graph_launches": int(info.graph_launches),
+                      "kernels_per_frame": info.kernels_per_frame, "blocks_per_sm": best_bps,
+                      "tuning_trials_ms": [[b, round(t, 3)] for b, t in trials]},
+            "sequential_views": {"ms_per_step": sequential_ms, "value": rays / (sequential_ms * 1e-3) / 1e6},
+            "gpu_launches": args.steps * info.kernels_per_frame,
+            "clocks": clocks.summary(), "setup_s": w["setup_s"],
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="atrium", choices=["atrium", "batched"],
+                    help="atrium: the headline frame; batched: 64 scenes per step through lux_batch_trace_merge")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 65,536-triangle atrium at 640x360 (not a benchmark line)")
     args = ap.parse_args()
@@ -408,6 +544,8 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "batched":
+        run_batched(args, rank, world)
     else:
         run_ours(args, rank, world)
 

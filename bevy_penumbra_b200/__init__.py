@@ -29,7 +29,7 @@ from ._native import LuxError, check, lib
 
 __all__ = [
     "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
-    "LuxContext", "PackedScene", "GpuScene", "SplitView", "LuxError", "trace_rays", "interval_radiance",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance",
     "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
 ]
 
@@ -434,9 +434,63 @@ class SplitView:
             self.ctx.check(lib().lux_view_read_probes(self.handle, _ptr(keys), _ptr(tables)))
         return keys, tables
 
+    def read_hits(self, count: int) -> np.ndarray:
+        """lux_view_read_hits: the last Split frame's first `count` interval-ray hits."""
+        out = np.zeros(count, dtype=HIT_DTYPE)
+        self.ctx.check(lib().lux_view_read_hits(self.handle, _ptr(out), count))
+        return out
+
     def close(self) -> None:
         if self.handle:
             lib().lux_view_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many (view, scene, receivers) jobs per frame: one launch per trace
+    stage over all jobs, the whole frame captured once as a CUDA graph and
+    replayed (lux_batch_*)."""
+
+    def __init__(self, ctx: LuxContext):
+        self.ctx = ctx
+        handle = C.c_void_p()
+        ctx.check(lib().lux_batch_create(ctx.handle, C.byref(handle)))
+        self.handle = handle
+
+    def set_graph(self, enable: bool) -> None:
+        self.ctx.check(lib().lux_batch_set_graph(self.handle, 1 if enable else 0))
+
+    def set_tuning(self, closest_blocks_per_sm: int = 16, shadow_blocks_per_sm: int = 16) -> None:
+        t = N.LuxTuning()
+        t.closest_blocks_per_sm = closest_blocks_per_sm
+        t.shadow_blocks_per_sm = shadow_blocks_per_sm
+        self.ctx.check(lib().lux_batch_set_tuning(self.handle, C.byref(t)))
+
+    def trace_merge(self, jobs, settings: RadianceCascades) -> None:
+        """jobs: sequence of (SplitView, GpuScene, position_ptr, normal_ptr, count)."""
+        arr = (N.LuxBatchJob * len(jobs))()
+        for k, (view, scene, pos, nrm, count) in enumerate(jobs):
+            arr[k].view = view.handle
+            arr[k].scene = scene.handle
+            arr[k].receivers = N.LuxReceivers(pos, nrm, count)
+            view.settings = settings
+        s = settings.to_c()
+        self.ctx.check(lib().lux_batch_trace_merge(self.handle, arr, len(jobs), C.byref(s)))
+
+    def info(self) -> N.LuxBatchInfo:
+        out = N.LuxBatchInfo()
+        self.ctx.check(lib().lux_batch_info(self.handle, C.byref(out)))
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -97,6 +97,15 @@ class LuxTuning(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
 
+class LuxBatchJob(C.Structure):
+    _fields_ = [("view", C.c_void_p), ("scene", C.c_void_p), ("receivers", LuxReceivers)]
+
+
+class LuxBatchInfo(C.Structure):
+    _fields_ = [("jobs", C.c_uint32), ("graph_captures", C.c_uint32), ("graph_launches", C.c_uint64),
+                ("interval_rays", C.c_uint64), ("kernels_per_frame", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 P = C.c_void_p
 U32 = C.c_uint32
 SZ = C.c_size_t
@@ -141,6 +150,13 @@ SIGNATURES = {
     "lux_view_get_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
     "lux_view_read_level": (C.c_int, [P, U32, P, P, P, P]),
     "lux_view_read_probes": (C.c_int, [P, P, P]),
+    "lux_view_read_hits": (C.c_int, [P, P, U32]),
+    "lux_batch_create": (C.c_int, [P, C.POINTER(P)]),
+    "lux_batch_destroy": (C.c_int, [P]),
+    "lux_batch_set_graph": (C.c_int, [P, U32]),
+    "lux_batch_set_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
+    "lux_batch_trace_merge": (C.c_int, [P, P, U32, P]),
+    "lux_batch_info": (C.c_int, [P, C.POINTER(LuxBatchInfo)]),
 }
 
 _lib = None

@@ -39,6 +39,10 @@
 #ifndef LUX_SHADOW_MIN_BLOCKS
 #define LUX_SHADOW_MIN_BLOCKS 6
 #endif
+// The batched trace kernels keep a job's scene pointers per warp as well.
+#ifndef LUX_BATCH_MIN_BLOCKS
+#define LUX_BATCH_MIN_BLOCKS 6
+#endif
 
 namespace {
 
@@ -276,10 +280,10 @@ __global__ void clear_entries_kernel(ViewDevice V, FrameParams F) {
 // r2(sequence + 1) + jitter)) flipped into the normal's hemisphere
 // (traceTransport, shaders/split.slang:1135-1146); (u, v) of the flipped
 // direction give its bin at every level.
-__device__ __forceinline__ void split_direction(const FrameParams &F, uint32_t i, uint32_t k, f3 n, f3 &dir, float &u,
-                                                float &v) {
+__device__ __forceinline__ void split_direction(const FrameParams &F, uint32_t frame, uint32_t i, uint32_t k, f3 n,
+                                                f3 &dir, float &u, float &v) {
     float jx, jy, rx, ry;
-    lux::r2(lux::transport_hash(F.shade.frame ^ 0x5a17c9e3u), jx, jy);
+    lux::r2(lux::transport_hash(frame ^ 0x5a17c9e3u), jx, jy);
     lux::r2(i * F.rays_per_receiver + k + 1u, rx, ry);
     u = lux::fracf((0.5f + rx) + jx);
     v = lux::fracf((0.5f + ry) + jy);
@@ -325,7 +329,7 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
             float4 p4 = pos[i], n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
             float u, v;
-            split_direction(F, i, k, n, d, u, v);
+            split_direction(F, F.shade.frame, i, k, n, d, u, v);
             o = lux::ray_offset(p, n, F.shade.normal_bias);
             tmin = 0.0f;
             limit = 1e20f;
@@ -346,6 +350,26 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
     add_stats(V.stats, st);
 }
 
+// One Split interval ray (traceTransport, shaders/split.slang:1122-1163):
+// receiver i = ray / R, sample k = ray % R, from the biased receiver position
+// to 1e20; the hit is stored for shading.
+__device__ __forceinline__ void closest_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
+                                                  const SceneView &S, const float4 *__restrict__ pos,
+                                                  const float4 *__restrict__ nrm, uint32_t slot,
+                                                  lux::TraceCounters &cn) {
+    uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
+    uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+    float4 p4 = pos[i], n4 = nrm[i];
+    f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+    f3 dir;
+    float u, v;
+    split_direction(F, frame, i, k, n, dir, u, v);
+    f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
+    lux::Hit hit;
+    lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
+    store_ray(V, ray, origin, dir, hit);
+}
+
 // Persistent warps, 32 consecutive rays per fetch (one atomic per warp).
 __device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter) {
     uint32_t base = 0;
@@ -364,17 +388,7 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_ker
         if (base >= ray_count) break;
         uint32_t slot = base + (threadIdx.x & 31u);
         if (slot < ray_count) {
-            uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
-            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
-            float4 p4 = pos[i], n4 = nrm[i];
-            f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
-            f3 dir;
-            float u, v;
-            split_direction(F, i, k, n, dir, u, v);
-            f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
-            lux::Hit hit;
-            lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
-            store_ray(V, ray, origin, dir, hit);
+            closest_split_ray(V, F, F.shade.frame, S, pos, nrm, slot, cn);
             st[kStatInterval] += 1;
         }
     }
@@ -427,7 +441,7 @@ __global__ void ray_keys_kernel(ViewDevice V, FrameParams F, SceneView S, const 
         float4 p4 = pos[i], n4 = nrm[i];
         f3 dir;
         float u, v;
-        split_direction(F, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+        split_direction(F, F.shade.frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
         uint32_t bin = lux::direction_index_uv(u, v, 8u, 4u);
         V.sort_keys[ray] = bin * kSortCells + cell16(S, f3{p4.x, p4.y, p4.z});
     }
@@ -472,66 +486,72 @@ __global__ void sort_scatter_kernel(ViewDevice V, const uint32_t *count_ptr, uin
 
 // Hit shading up to the visibility traces; queries are appended to the
 // queue with one atomic per warp.
+// Hit shading of one warp's rays (one ray per lane, `ray` < `rays` active):
+// base emission and next-event queries (outgoingTransportRadianceTracked,
+// shaders/cascades.slang:196-268); the warp's queries are appended to the
+// view's queue with one atomic.  Every lane of the warp belongs to one view.
+__device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParams &F, const lux::ShadeParams &P,
+                                           const SceneView &S, uint32_t ray, uint32_t rays) {
+    const uint32_t lane = threadIdx.x & 31u;
+    lux::NeeQuery q[lux::kMaxNeeSamples];
+    uint32_t slot_of[lux::kMaxNeeSamples];
+    uint32_t nq = 0, count = 0;
+    bool supported = false;
+    f3 base{0.0f, 0.0f, 0.0f};
+    if (ray < rays) {
+        f3 o, d;
+        lux::Hit hit;
+        load_ray(V, ray, o, d, hit);
+        supported = lux::outgoing_record(S, P, o, d, hit, base, count,
+                                         [&](uint32_t sample, const lux::NeeQuery &query) {
+                                             q[nq] = query;
+                                             slot_of[nq] = sample;
+                                             ++nq;
+                                         });
+        V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? count : lux::kEmpty));
+    }
+    // Warp-aggregated append of this warp's queries.
+    uint32_t prefix = nq;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, prefix, off);
+        if (lane >= (uint32_t)off) prefix += t;
+    }
+    uint32_t total = __shfl_sync(0xffffffffu, prefix, 31);
+    uint32_t first = 0;
+    if (lane == 31 && total) first = atomicAdd(V.ts.queue_count, total);
+    first = __shfl_sync(0xffffffffu, first, 31);
+    uint32_t at = first + prefix - nq;
+    if (ray < rays) {
+        uint32_t k = 0;
+        for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
+            uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
+            if (k < nq && slot_of[k] == s) {
+                uint32_t qi = at + k;
+                if (qi < F.queue_capacity) {
+                    V.ts.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
+                    V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
+                    V.ts.slot_query[slot] = qi;
+                    V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
+                                                          q[k].contribution.z, 0.0f);
+                    if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
+                } else {
+                    V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
+                }
+                ++k;
+            } else {
+                V.ts.slot_query[slot] = lux::kEmpty;
+            }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t ray_count,
                                                     bool dense) {
     if (*V.error_flags) return;
     uint32_t rays = dense ? (uint32_t)min(total_entries(V, F), (unsigned long long)ray_count) : ray_count;
-    const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base_ray = blockIdx.x * blockDim.x; base_ray < rays; base_ray += gridDim.x * blockDim.x) {
-        uint32_t ray = base_ray + threadIdx.x;
-        lux::NeeQuery q[lux::kMaxNeeSamples];
-        uint32_t slot_of[lux::kMaxNeeSamples];
-        uint32_t nq = 0, count = 0;
-        bool supported = false;
-        f3 base{0.0f, 0.0f, 0.0f};
-        if (ray < rays) {
-            f3 o, d;
-            lux::Hit hit;
-            load_ray(V, ray, o, d, hit);
-            supported = lux::outgoing_record(S, F.shade, o, d, hit, base, count,
-                                             [&](uint32_t sample, const lux::NeeQuery &query) {
-                                                 q[nq] = query;
-                                                 slot_of[nq] = sample;
-                                                 ++nq;
-                                             });
-            V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z,
-                                          lux::as_float(supported ? count : lux::kEmpty));
-        }
-        // Warp-aggregated append of this warp's queries.
-        uint32_t prefix = nq;
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, prefix, off);
-            if (lane >= (uint32_t)off) prefix += t;
-        }
-        uint32_t total = __shfl_sync(0xffffffffu, prefix, 31);
-        uint32_t first = 0;
-        if (lane == 31 && total) first = atomicAdd(V.ts.queue_count, total);
-        first = __shfl_sync(0xffffffffu, first, 31);
-        uint32_t at = first + prefix - nq;
-        if (ray < rays) {
-            uint32_t k = 0;
-            for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
-                uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
-                if (k < nq && slot_of[k] == s) {
-                    uint32_t qi = at + k;
-                    if (qi < F.queue_capacity) {
-                        V.ts.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
-                        V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
-                        V.ts.slot_query[slot] = qi;
-                        V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
-                                                           q[k].contribution.z, 0.0f);
-                        if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
-                    } else {
-                        V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
-                    }
-                    ++k;
-                } else {
-                    V.ts.slot_query[slot] = lux::kEmpty;
-                }
-            }
-        }
-    }
+    for (uint32_t base_ray = blockIdx.x * blockDim.x; base_ray < rays; base_ray += gridDim.x * blockDim.x)
+        shade_warp(V, F, F.shade, S, base_ray + threadIdx.x, rays);
 }
 
 // Visibility queries, one per lane (traceVisibility, shaders/split.slang:1326-1339).
@@ -564,6 +584,17 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
     add_stats(V.stats, st, extra);
 }
 
+// One visibility query (traceVisibility, shaders/split.slang:1326-1339):
+// result 0 visible, 1 blocked, 2 unsupported.
+__device__ __forceinline__ void shadow_query(const ViewDevice &V, const SceneView &S, uint32_t i,
+                                             lux::TraceCounters &cn) {
+    uint32_t qi = V.query_order ? V.query_order[i] : i;
+    float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
+    lux::Hit sh;
+    lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
+    V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+}
+
 __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
@@ -574,11 +605,7 @@ __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(View
         if (base >= n) break;
         uint32_t i = base + (threadIdx.x & 31u);
         if (i < n) {
-            uint32_t qi = V.query_order ? V.query_order[i] : i;
-            float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
-            lux::Hit sh;
-            lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
-            V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+            shadow_query(V, S, i, cn);
             st[kStatShadow] += 1;
         }
     }
@@ -612,44 +639,48 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
 
 // deposit, shaders/split.slang:1056-1117: every level up to and including
 // the one whose interval holds the hit; the last level owns the tail.
+__device__ __forceinline__ void deposit_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
+                                                  const float4 *__restrict__ nrm, uint32_t ray,
+                                                  unsigned long long st[7]) {
+    f3 radiance;
+    if (!ray_radiance(V, ray, radiance)) {
+        st[kStatUnsupported] += 1;
+        return;
+    }
+    uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+    float4 n4 = nrm[i];
+    f3 dir;
+    float u, v;
+    split_direction(F, frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+    float t = V.ts.ray_o[ray].w;
+    uint32_t term = F.levels - 1u;
+    for (uint32_t l = 0; l + 1u < F.levels; ++l)
+        if (t > F.start[l] && t <= F.end[l]) {
+            term = l;
+            break;
+        }
+    for (uint32_t l = 0; l <= term; ++l) {
+        uint32_t cell = V.receiver_cell[(size_t)l * F.receivers + i];
+        if (cell == lux::kEmpty) continue;
+        uint32_t bin = lux::direction_index_uv(u, v, F.columns[l], F.rows[l]);
+        unsigned long long e = V.level_base[l] + (unsigned long long)cell * F.dirs[l] + bin;
+        atomicAdd(&V.count[e], 1u);
+        if (l == term) {
+            atomicAdd(&V.accum[e].x, radiance.x);
+            atomicAdd(&V.accum[e].y, radiance.y);
+            atomicAdd(&V.accum[e].z, radiance.z);
+        } else {
+            atomicAdd(&V.accum[e].w, 1.0f);
+        }
+        st[kStatDeposits] += 1;
+    }
+}
+
 __global__ void __launch_bounds__(128) deposit_split_kernel(ViewDevice V, FrameParams F,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x;
-    if (*V.error_flags == 0u && ray < ray_count) {
-        f3 radiance;
-        if (!ray_radiance(V, ray, radiance)) {
-            st[kStatUnsupported] = 1;
-        } else {
-            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
-            float4 n4 = nrm[i];
-            f3 dir;
-            float u, v;
-            split_direction(F, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
-            float t = V.ts.ray_o[ray].w;
-            uint32_t term = F.levels - 1u;
-            for (uint32_t l = 0; l + 1u < F.levels; ++l)
-                if (t > F.start[l] && t <= F.end[l]) {
-                    term = l;
-                    break;
-                }
-            for (uint32_t l = 0; l <= term; ++l) {
-                uint32_t cell = V.receiver_cell[(size_t)l * F.receivers + i];
-                if (cell == lux::kEmpty) continue;
-                uint32_t bin = lux::direction_index_uv(u, v, F.columns[l], F.rows[l]);
-                unsigned long long e = V.level_base[l] + (unsigned long long)cell * F.dirs[l] + bin;
-                atomicAdd(&V.count[e], 1u);
-                if (l == term) {
-                    atomicAdd(&V.accum[e].x, radiance.x);
-                    atomicAdd(&V.accum[e].y, radiance.y);
-                    atomicAdd(&V.accum[e].z, radiance.z);
-                } else {
-                    atomicAdd(&V.accum[e].w, 1.0f);
-                }
-                st[kStatDeposits] += 1;
-            }
-        }
-    }
+    if (*V.error_flags == 0u && ray < ray_count) deposit_split_ray(V, F, F.shade.frame, nrm, ray, st);
     add_stats(V.stats, st);
 }
 
@@ -925,6 +956,171 @@ uint32_t next_pow2(uint64_t v) {
     return (uint32_t)p;
 }
 
+// ---- batched trace stages ----------------------------------------------
+// One job = one view's frame: its device state, parameters, scene and
+// receivers.  Ray (and visibility-query) indices of all jobs are
+// concatenated with every job's range padded to a multiple of 32, so each
+// warp-sized chunk lies inside one job: the job is warp-uniform, per-view
+// warp aggregation (query append, stats) works unchanged, and a warp reads
+// its job's parameters as broadcasts.
+struct BatchJob {
+    ViewDevice V;
+    FrameParams F;
+    SceneView S;
+    const float4 *pos, *nrm;
+    uint32_t rays;
+    uint32_t pad;
+};
+
+// Largest j < n with begin[j] <= x (begin[0] = 0, non-decreasing).
+__device__ __forceinline__ uint32_t find_job(const uint32_t *__restrict__ begin, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(begin + mid) <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void flush_stats(unsigned long long *stats, unsigned long long st[7],
+                                            lux::TraceCounters &cn, bool shadow) {
+    st[kStatNodes] += cn.nodes;
+    st[kStatTris] += cn.triangles;
+    st[kStatInst] += cn.instances;
+    unsigned long long extra[3] = {cn.nodes, cn.triangles, cn.instances};
+    add_stats(stats, st, shadow ? extra : nullptr);
+#pragma unroll
+    for (int k = 0; k < 7; ++k) st[k] = 0;
+    cn = lux::TraceCounters{0, 0, 0};
+}
+
+__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
+    closest_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
+                         uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counter) {
+    const uint32_t fr = *frame;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t cur = lux::kEmpty;
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    while (true) {
+        uint32_t base = warp_fetch(counter);
+        if (base >= total) break;
+        uint32_t j = find_job(begin, n, base);
+        const BatchJob &J = jobs[j];
+        if (j != cur) {
+            if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
+            cur = j;
+        }
+        if (*J.V.error_flags) continue;
+        uint32_t slot = base - __ldg(begin + j) + lane;
+        if (slot < J.rays) {
+            SceneView S = J.S;
+            closest_split_ray(J.V, J.F, fr, S, J.pos, J.nrm, slot, cn);
+            st[kStatInterval] += 1;
+        }
+    }
+    if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
+}
+
+__global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__restrict__ jobs,
+                                                          const uint32_t *__restrict__ begin, uint32_t n,
+                                                          uint32_t total, const uint32_t *__restrict__ frame) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total / 32u; w += warps) {
+        uint32_t base = w * 32u;
+        uint32_t j = find_job(begin, n, base);
+        const BatchJob &J = jobs[j];
+        if (*J.V.error_flags) continue;
+        lux::ShadeParams P = J.F.shade;
+        P.frame = *frame;
+        SceneView S = J.S;
+        shade_warp(J.V, J.F, P, S, base - __ldg(begin + j) + lane, J.rays);
+    }
+}
+
+__device__ __forceinline__ uint32_t job_queries(const BatchJob &J) {
+    return *J.V.error_flags ? 0u : min(*J.V.ts.queue_count, J.F.queue_capacity);
+}
+
+// Padded prefix of every job's visibility-query count (known only on the
+// device after shading); qbegin[n] is the padded total.
+__global__ void query_prefix_kernel(const BatchJob *__restrict__ jobs, uint32_t n, uint32_t *__restrict__ qbegin) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    uint32_t sum = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        qbegin[j] = sum;
+        sum += (job_queries(jobs[j]) + 31u) & ~31u;
+    }
+    qbegin[n] = sum;
+}
+
+__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
+    shadow_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ qbegin, uint32_t n,
+                        uint32_t *counter) {
+    const uint32_t total = qbegin[n];
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t cur = lux::kEmpty;
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    while (true) {
+        uint32_t base = warp_fetch(counter);
+        if (base >= total) break;
+        uint32_t j = find_job(qbegin, n, base);
+        const BatchJob &J = jobs[j];
+        if (j != cur) {
+            if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
+            cur = j;
+        }
+        uint32_t i = base - qbegin[j] + lane;
+        if (i < job_queries(J)) {
+            SceneView S = J.S;
+            shadow_query(J.V, S, i, cn);
+            st[kStatShadow] += 1;
+        }
+    }
+    if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
+}
+
+__global__ void __launch_bounds__(128) deposit_batch_kernel(const BatchJob *__restrict__ jobs,
+                                                            const uint32_t *__restrict__ begin, uint32_t n,
+                                                            uint32_t total, const uint32_t *__restrict__ frame) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total / 32u; w += warps) {
+        uint32_t base = w * 32u;
+        uint32_t j = find_job(begin, n, base);
+        const BatchJob &J = jobs[j];
+        if (*J.V.error_flags) continue;
+        unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+        uint32_t ray = base - __ldg(begin + j) + lane;
+        if (ray < J.rays) deposit_split_ray(J.V, J.F, *frame, J.nrm, ray, st);
+        add_stats(J.V.stats, st);
+    }
+}
+
+// Interval-ray hits of a Split frame as LuxHit records.
+__global__ void read_hits_kernel(ViewDevice V, uint32_t count, LuxHit *__restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    f3 o, d;
+    lux::Hit h;
+    load_ray(V, i, o, d, h);
+    LuxHit r;
+    r.distance = h.t;
+    r.triangle = h.tri;
+    r.instance = h.inst;
+    r.errors = h.errors;
+    r.barycentric[0] = (1.0f - h.b1) - h.b2;
+    r.barycentric[1] = h.b1;
+    r.barycentric[2] = h.b2;
+    r.visited = 0;
+    out[i] = r;
+}
+
 }  // namespace
 
 constexpr int kTimingEvents = 7;
@@ -1058,7 +1254,40 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
     F.shade.exposure = s.exposure;
     F.shade.emissive_samples = s.emissive_samples;
     F.shade.frame = s.frame_index;
+    if ((size_t)F.dirs[0] * 2 * sizeof(float4) > 48 * 1024)
+        return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: too many cascade-0 directions");
     return LUX_OK;
+}
+
+// seed -> layout: the receivers' cells of every level, dense ids, record
+// offsets, cleared records (clear .. prefix, shaders/split.slang:734-983).
+static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, cudaStream_t st) {
+    const ViewDevice &D = v->dev;
+    const int grid = v->ctx->sm_count * 8;
+    clear_kernel<<<grid, 256, 0, st>>>(D, F);
+    if (F.receivers) {
+        seed_insert_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+        seed_assign_kernel<<<grid, 256, 0, st>>>(D, F);
+        seed_lookup_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+    }
+    layout_kernel<<<1, 32, 0, st>>>(D, F);
+    clear_entries_kernel<<<grid, 256, 0, st>>>(D, F);
+}
+
+// Corners then the merge of every level, coarsest first (mergeEntry over
+// levels n-1 .. 0, shaders/split.slang:1624-1725).
+static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
+    const ViewDevice &D = v->dev;
+    const int grid = v->ctx->sm_count * 8;
+    for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
+    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, (uint32_t)l);
+}
+
+// packProbes (shaders/split.slang:1786-1918); the direction count is
+// checked by make_params.
+static void enqueue_pack(LuxView *v, const FrameParams &F, cudaStream_t st) {
+    size_t smem = (size_t)F.dirs[0] * 2 * sizeof(float4);
+    pack_kernel<<<v->ctx->sm_count * 8, 64, smem, st>>>(v->dev, F);
 }
 
 extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, const LuxSettings *settings,
@@ -1070,26 +1299,19 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     if (rc->count && (!rc->position || (!rc->normal && settings->layout == LUX_LAYOUT_SPLIT)))
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: missing receiver buffers");
     FrameParams F;
-    make_params(v, settings, rc->count, F);
+    lux_status ps = make_params(v, settings, rc->count, F);
+    if (ps != LUX_OK) return ps;
     if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > v->desc.max_rays)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: receivers x rays_per_receiver exceeds max_rays");
     const ViewDevice &D = v->dev;
     cudaStream_t st = ctx->stream;
-    const int grid = ctx->sm_count * 8;
     const float4 *pos = (const float4 *)rc->position;
     const float4 *nrm = (const float4 *)rc->normal;
     auto mark = [&](int i) {
         if (v->timing) cudaEventRecord(v->ev[i], st);
     };
     mark(0);
-    clear_kernel<<<grid, 256, 0, st>>>(D, F);
-    if (rc->count) {
-        seed_insert_kernel<<<grid, 256, 0, st>>>(D, F, pos);
-        seed_assign_kernel<<<grid, 256, 0, st>>>(D, F);
-        seed_lookup_kernel<<<grid, 256, 0, st>>>(D, F, pos);
-    }
-    layout_kernel<<<1, 32, 0, st>>>(D, F);
-    clear_entries_kernel<<<grid, 256, 0, st>>>(D, F);
+    enqueue_setup(v, F, pos, st);
     mark(1);
     if (F.layout == LUX_LAYOUT_SPLIT) {
         uint32_t rays = rc->count * F.rays_per_receiver;
@@ -1135,12 +1357,9 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
         deposit_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F);
     }
     mark(2);
-    for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
-    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, (uint32_t)l);
+    enqueue_merge(v, F, st);
     mark(3);
-    size_t smem = (size_t)F.dirs[0] * 2 * sizeof(float4);
-    if (smem > 48 * 1024) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: too many cascade-0 directions");
-    pack_kernel<<<grid, 64, smem, st>>>(D, F);
+    enqueue_pack(v, F, st);
     mark(4);
     v->last = F;
     v->has_frame = true;
@@ -1481,4 +1700,290 @@ extern "C" lux_status lux_interval_radiance_noalloc(LuxContext *ctx, const LuxSc
     if ((size_t)(end - base) > kNoAllocBytes)
         return lux_fail(ctx, LUX_ERR_INTERNAL, "interval_radiance_noalloc: scratch partition exceeds the array");
     return launch_interval_radiance(ctx, scene, settings, rays, count, out, V, kNoAllocMaxRays);
+}
+
+// ---- lux_view_read_hits ----------------------------------------------------
+
+extern "C" lux_status lux_view_read_hits(LuxView *v, LuxHit *out, uint32_t count) {
+    if (!v || (count && !out)) return LUX_ERR_INVALID_ARGUMENT;
+    if (!v->has_frame || v->last.layout != LUX_LAYOUT_SPLIT)
+        return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "read_hits: no Split frame traced yet");
+    if ((uint64_t)count > (uint64_t)v->last.receivers * v->last.rays_per_receiver)
+        return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "read_hits: more hits than the frame's interval rays");
+    if (count == 0) return LUX_OK;
+    LuxContext *ctx = v->ctx;
+    cudaStream_t st = ctx->stream;
+    LuxHit *d = nullptr;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaMallocAsync((void **)&d, (size_t)count * sizeof(LuxHit), st),
+                                   "read_hits: staging");
+    if (rc != LUX_OK) return rc;
+    read_hits_kernel<<<(count + 255) / 256, 256, 0, st>>>(v->dev, count, d);
+    cudaMemcpyAsync(out, d, (size_t)count * sizeof(LuxHit), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "read_hits");
+    if (rc != LUX_OK) return rc;
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "read_hits launch");
+}
+
+// ---- batches ---------------------------------------------------------------
+
+struct LuxBatch {
+    LuxContext *ctx = nullptr;
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, {0, 0}};
+    bool use_graph = true;
+    // Configuration the device tables and graph were built for.
+    std::vector<LuxBatchJob> jobs;
+    LuxSettings settings{};  // frame_index zeroed
+    std::vector<FrameParams> params;
+    uint32_t total = 0;      // padded interval rays
+    uint64_t rays = 0;
+    bool built = false;
+    BatchJob *d_jobs = nullptr;
+    uint32_t *d_begin = nullptr, *d_qbegin = nullptr, *d_counters = nullptr, *d_frame = nullptr;
+    size_t job_capacity = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint32_t captures = 0;
+    uint64_t replays = 0;
+    uint32_t kernels = 0;
+};
+
+static void batch_release_graph(LuxBatch *b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+}
+
+static void batch_release_tables(LuxBatch *b) {
+    cudaFree(b->d_jobs);
+    cudaFree(b->d_begin);
+    cudaFree(b->d_qbegin);
+    b->d_jobs = nullptr;
+    b->d_begin = b->d_qbegin = nullptr;
+    b->job_capacity = 0;
+}
+
+extern "C" lux_status lux_batch_create(LuxContext *ctx, LuxBatch **out) {
+    if (!ctx || !out) return LUX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    LuxBatch *b = new (std::nothrow) LuxBatch();
+    if (!b) return LUX_ERR_OUT_OF_MEMORY;
+    b->ctx = ctx;
+    cudaSetDevice(ctx->device);
+    if (cudaMalloc((void **)&b->d_counters, 16) != cudaSuccess || cudaMalloc((void **)&b->d_frame, 16) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(b->d_counters);
+        delete b;
+        return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
+    }
+    *out = b;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_destroy(LuxBatch *b) {
+    if (!b) return LUX_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    batch_release_graph(b);
+    batch_release_tables(b);
+    cudaFree(b->d_counters);
+    cudaFree(b->d_frame);
+    delete b;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_set_graph(LuxBatch *b, uint32_t enable) {
+    if (!b) return LUX_ERR_INVALID_ARGUMENT;
+    b->use_graph = enable != 0;
+    b->built = false;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_set_tuning(LuxBatch *b, const LuxTuning *t) {
+    if (!b || !t) return LUX_ERR_INVALID_ARGUMENT;
+    if (t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 || t->shadow_blocks_per_sm < 1 ||
+        t->shadow_blocks_per_sm > 64)
+        return lux_fail(b->ctx, LUX_ERR_INVALID_ARGUMENT, "batch tuning: blocks per SM must be 1..64");
+    b->tuning = *t;
+    b->built = false;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_info(const LuxBatch *b, LuxBatchInfo *out) {
+    if (!b || !out) return LUX_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    out->jobs = (uint32_t)b->jobs.size();
+    out->graph_captures = b->captures;
+    out->graph_launches = b->replays;
+    out->interval_rays = b->rays;
+    out->kernels_per_frame = b->kernels;
+    return LUX_OK;
+}
+
+static bool same_jobs(const std::vector<LuxBatchJob> &a, const LuxBatchJob *b, uint32_t n) {
+    if (a.size() != n) return false;
+    for (uint32_t j = 0; j < n; ++j)
+        if (a[j].view != b[j].view || a[j].scene != b[j].scene || a[j].receivers.position != b[j].receivers.position ||
+            a[j].receivers.normal != b[j].receivers.normal || a[j].receivers.count != b[j].receivers.count)
+            return false;
+    return true;
+}
+
+// Every kernel of one batched frame, in order, on `st` (captured or direct).
+static uint32_t batch_enqueue(LuxBatch *b, cudaStream_t st) {
+    LuxContext *ctx = b->ctx;
+    const uint32_t n = (uint32_t)b->jobs.size();
+    uint32_t kernels = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        enqueue_setup(b->jobs[j].view, b->params[j], (const float4 *)b->jobs[j].receivers.position, st);
+        kernels += b->params[j].receivers ? 6u : 3u;
+    }
+    cudaMemsetAsync(b->d_counters, 0, 8, st);
+    const int grid = ctx->sm_count * 8;
+    if (b->total) {
+        closest_batch_kernel<<<ctx->sm_count * b->tuning.closest_blocks_per_sm, 128, 0, st>>>(
+            b->d_jobs, b->d_begin, n, b->total, b->d_frame, b->d_counters);
+        shade_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
+        query_prefix_kernel<<<1, 32, 0, st>>>(b->d_jobs, n, b->d_qbegin);
+        shadow_batch_kernel<<<ctx->sm_count * b->tuning.shadow_blocks_per_sm, 128, 0, st>>>(
+            b->d_jobs, b->d_qbegin, n, b->d_counters + 1);
+        deposit_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
+        kernels += 5;
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+        enqueue_merge(b->jobs[j].view, b->params[j], st);
+        enqueue_pack(b->jobs[j].view, b->params[j], st);
+        kernels += 2u * b->params[j].levels;
+    }
+    return kernels;
+}
+
+static lux_status batch_build(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n, const LuxSettings &s,
+                              std::vector<FrameParams> &params) {
+    LuxContext *ctx = b->ctx;
+    cudaStream_t st = ctx->stream;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "batch: synchronize");
+    if (rc != LUX_OK) return rc;
+    batch_release_graph(b);
+    b->built = false;
+    if (n > b->job_capacity) {
+        batch_release_tables(b);
+        if (cudaMalloc((void **)&b->d_jobs, n * sizeof(BatchJob)) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_begin, (n + 1) * 4) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_qbegin, (n + 1) * 4) != cudaSuccess) {
+            cudaGetLastError();
+            batch_release_tables(b);
+            return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
+        }
+        b->job_capacity = n;
+    }
+    std::vector<BatchJob> h(n);
+    std::vector<uint32_t> begin(n + 1, 0);
+    uint64_t padded = 0, rays = 0;
+    for (uint32_t j = 0; j < n; ++j) {
+        const FrameParams &F = params[j];
+        uint32_t r = F.receivers * F.rays_per_receiver;
+        BatchJob &J = h[j];
+        std::memset(&J, 0, sizeof J);
+        J.V = jobs[j].view->dev;
+        J.V.sort_keys = nullptr;
+        J.V.ray_order = nullptr;
+        J.V.query_order = nullptr;
+        J.F = F;
+        J.S = jobs[j].scene->view;
+        J.pos = (const float4 *)jobs[j].receivers.position;
+        J.nrm = (const float4 *)jobs[j].receivers.normal;
+        J.rays = r;
+        begin[j] = (uint32_t)padded;
+        padded += (r + 31u) & ~31u;
+        rays += r;
+    }
+    if (padded > 0xffffffe0ull) return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: more than 2^32 interval rays");
+    begin[n] = (uint32_t)padded;
+    rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_jobs, h.data(), n * sizeof(BatchJob), cudaMemcpyHostToDevice),
+                        "batch: job table");
+    if (rc == LUX_OK)
+        rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_begin, begin.data(), (n + 1) * 4, cudaMemcpyHostToDevice),
+                            "batch: ray offsets");
+    if (rc != LUX_OK) return rc;
+    b->jobs.assign(jobs, jobs + n);
+    b->settings = s;
+    b->settings.frame_index = 0;
+    b->params = params;
+    b->total = (uint32_t)padded;
+    b->rays = rays;
+    if (b->use_graph) {
+        rc = lux_cuda_check(ctx, (int)cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "batch: capture");
+        if (rc != LUX_OK) return rc;
+        b->kernels = batch_enqueue(b, st);
+        cudaGraph_t g = nullptr;
+        rc = lux_cuda_check(ctx, (int)cudaStreamEndCapture(st, &g), "batch: end capture");
+        if (rc != LUX_OK) return rc;
+        b->graph = g;
+        rc = lux_cuda_check(ctx, (int)cudaGraphInstantiate(&b->exec, g, 0), "batch: instantiate");
+        if (rc != LUX_OK) {
+            batch_release_graph(b);
+            return rc;
+        }
+        ++b->captures;
+    }
+    b->built = true;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n,
+                                            const LuxSettings *settings) {
+    if (!b || !settings || (n && !jobs)) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = b->ctx;
+    if (n == 0 || n > 65536) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: need 1..65536 jobs");
+    LuxSettings s = *settings;
+    lux_settings_sanitize(&s);
+    if (s.layout != LUX_LAYOUT_SPLIT) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: layout must be Split");
+    std::vector<FrameParams> params(n);
+    for (uint32_t j = 0; j < n; ++j) {
+        const LuxBatchJob &J = jobs[j];
+        if (!J.view || !J.scene || J.view->ctx != ctx || J.scene->ctx != ctx)
+            return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: job view/scene missing or on another context");
+        for (uint32_t k = 0; k < j; ++k)
+            if (jobs[k].view == J.view) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: a view appears twice");
+        const LuxReceivers &rc = J.receivers;
+        if (rc.count > J.view->desc.max_receivers)
+            return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: more receivers than a view's max_receivers");
+        if (rc.count && (!rc.position || !rc.normal))
+            return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: missing receiver buffers");
+        lux_status ps = make_params(J.view, &s, rc.count, params[j]);
+        if (ps != LUX_OK) return ps;
+        if ((uint64_t)rc.count * params[j].rays_per_receiver > J.view->desc.max_rays)
+            return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: receivers x rays_per_receiver exceeds a view's max_rays");
+    }
+    cudaSetDevice(ctx->device);
+    LuxSettings key = s;
+    key.frame_index = 0;
+    bool same = b->built && same_jobs(b->jobs, jobs, n) && std::memcmp(&key, &b->settings, sizeof key) == 0;
+    if (!same) {
+        lux_status rc = batch_build(b, jobs, n, s, params);
+        if (rc != LUX_OK) return rc;
+    }
+    cudaStream_t st = ctx->stream;
+    // Pageable source: the copy is staged before the call returns, so the
+    // local may go out of scope; it orders before the frame's kernels.
+    uint32_t frame = s.frame_index;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(b->d_frame, &frame, 4, cudaMemcpyHostToDevice, st),
+                                   "batch: frame index");
+    if (rc != LUX_OK) return rc;
+    if (b->use_graph) {
+        rc = lux_cuda_check(ctx, (int)cudaGraphLaunch(b->exec, st), "batch: graph launch");
+        if (rc != LUX_OK) return rc;
+        ++b->replays;
+    } else {
+        b->kernels = batch_enqueue(b, st);
+    }
+    for (uint32_t j = 0; j < n; ++j) {
+        FrameParams F = b->params[j];
+        F.shade.frame = s.frame_index;
+        jobs[j].view->last = F;
+        jobs[j].view->has_frame = true;
+    }
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "batch launch");
 }

@@ -263,6 +263,72 @@ def atrium(seed: int = 2, triangles: int = 262_144) -> SceneDesc:
     return sc
 
 
+def batch_scene(seed: int, triangles: int) -> SceneDesc:
+    """One scene of the batched workload: a floor, 1-3 downward emitters
+    (radiance U[5, 20]), seeded boxes and columns on the floor and a jittered
+    ceiling grid that makes the world triangle count exactly ``triangles``
+    (>= 200).  The room grows with the triangle count (about 6 m at 1k, 24 m
+    at 200k)."""
+    if triangles < 200:
+        raise ValueError("batch scene needs at least 200 triangles")
+    rng = np.random.default_rng(seed)
+    sc = SceneDesc(name=f"batch{seed}")
+    size = 6.0 + 18.0 * math.log(triangles / 1000.0 + 1.0) / math.log(201.0)
+    height = 3.0 + 0.25 * size
+    half = size * 0.5
+
+    def albedo_material():
+        return sc.add_material(material_words(tuple(rng.uniform(0.2, 0.8, size=3))))
+
+    floor = sc.add_mesh(quad((-half, 0.0, -half), (-half, 0.0, half), (half, 0.0, half), (half, 0.0, -half)))
+    sc.add_instance(floor, material=albedo_material())
+    emitter = sc.add_mesh(quad((-0.5, 0.0, -0.5), (0.5, 0.0, -0.5), (0.5, 0.0, 0.5), (-0.5, 0.0, 0.5)))
+    for _ in range(int(rng.integers(1, 4))):
+        radiance = float(rng.uniform(5.0, 20.0))
+        mat = sc.add_material(material_words((0.0, 0.0, 0.0), emission=(radiance, radiance, radiance)))
+        t = np.eye(3, 4, dtype=np.float64)
+        t[:, 3] = (rng.uniform(-0.3, 0.3) * size, height - 0.3, rng.uniform(-0.3, 0.3) * size)
+        sc.add_instance(emitter, t, material=mat)
+    budget = triangles - sc.world_triangles() - 2
+    box = sc.add_mesh(box_mesh((1.0, 1.0, 1.0), bottom=False))  # 10 triangles
+    column = sc.add_mesh(cylinder_mesh(0.25, 1.0, 12, 2))
+    column_tris = len(sc.meshes[column].indices)
+    spend = int(budget * 0.3)
+    while spend >= column_tris:
+        use_column = rng.uniform() < 0.4
+        mesh, tris = (column, column_tris) if use_column else (box, 10)
+        if tris > spend:
+            break
+        m = rotation_y(float(rng.uniform(0.0, 2.0 * math.pi)),
+                       (float(rng.uniform(-0.45, 0.45) * size), 0.0, float(rng.uniform(-0.45, 0.45) * size)))
+        m = m.astype(np.float64)
+        m[:, :3] = m[:, :3] @ np.diag((rng.uniform(0.3, 1.5), rng.uniform(0.3, height * 0.6), rng.uniform(0.3, 1.5)))
+        sc.add_instance(mesh, m.astype(np.float32), material=albedo_material())
+        spend -= tris
+    remaining = triangles - sc.world_triangles()
+    if remaining % 2:
+        sc.add_instance(sc.add_mesh(Mesh(np.array([[-half, 0.01, -half], [-half + 0.2, 0.01, -half],
+                                                   [-half, 0.01, -half + 0.2]], np.float32),
+                                         np.array([[0, 2, 1]], np.uint32))), material=albedo_material())
+        remaining -= 1
+    ceiling = sc.add_mesh(grid_mesh(remaining // 2, size, size, height, rng, 0.02))
+    sc.add_instance(ceiling, material=albedo_material())
+    assert sc.world_triangles() == triangles, (sc.world_triangles(), triangles)
+    return sc
+
+
+def batch_workload(seed: int = 3, scenes: int = 64):
+    """The batched configuration: per scene (seed, triangle count log-uniform
+    in [1k, 200k], view resolution from {320x180, 640x360, 1280x720})."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(scenes):
+        tris = int(round(math.exp(rng.uniform(math.log(1000.0), math.log(200000.0)))))
+        res = [(320, 180), (640, 360), (1280, 720)][int(rng.integers(0, 3))]
+        out.append((seed * 1000 + k, tris, res))
+    return out
+
+
 def _jit3(jit):
     t = np.zeros((3, 4), dtype=np.float32)
     t[:, 3] = jit()

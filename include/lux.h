@@ -352,6 +352,50 @@ lux_status lux_view_read_level(LuxView *view, uint32_t level, int32_t *cell_keys
 /* Copies packed cascade-0 probe tables: keys int4[cells], tables float4[cells*36]. */
 lux_status lux_view_read_probes(LuxView *view, int32_t *cell_keys, float *tables);
 
+/* Interval-ray hits of the view's last Split frame, in ray order
+ * (ray = receiver * rays_per_receiver + sample): out[count] LuxHit, count <=
+ * the frame's interval rays.  visited is 0.  For comparing runs. */
+lux_status lux_view_read_hits(LuxView *view, LuxHit *out, uint32_t count);
+
+/* ---- batching: many scenes and views in one launch per trace stage -------
+ * No reference counterpart (the reference renders one view per dispatch
+ * sequence).  One lux_batch_trace_merge runs the Split frame of every job:
+ * each view's seed/layout and merge/pack kernels, and for all jobs together
+ * ONE persistent closest-hit launch, one shading launch, one visibility launch
+ * and one deposit launch over the concatenated rays (every warp works on
+ * one job; uneven ray counts balance across the GPU).  With graphs enabled
+ * (the default) the whole multi-view frame is captured once per job
+ * configuration as a CUDA graph and replayed; only frame_index may change
+ * between replays.  Results per view are read with the lux_view_* calls and
+ * equal an unbatched lux_view_trace_merge of the same view bit for bit on hit
+ * ids (queue order, and so float sums, may differ).  Sorting tuning flags do
+ * not apply to batched frames. */
+typedef struct LuxBatch LuxBatch;
+typedef struct LuxBatchJob {
+    LuxView *view;            /* distinct per job, created on the batch's context */
+    const LuxScene *scene;    /* may be shared between jobs */
+    LuxReceivers receivers;   /* device pointers, as lux_view_trace_merge */
+} LuxBatchJob;
+typedef struct LuxBatchInfo {
+    uint32_t jobs;
+    uint32_t graph_captures;  /* CUDA graphs captured so far */
+    uint64_t graph_launches;  /* frames replayed from a graph */
+    uint64_t interval_rays;   /* interval rays of one frame */
+    uint32_t kernels_per_frame; /* kernel launches one frame enqueues */
+    uint32_t reserved;
+} LuxBatchInfo;
+lux_status lux_batch_create(LuxContext *ctx, LuxBatch **out);
+lux_status lux_batch_destroy(LuxBatch *batch);
+/* 1 (default): capture/replay a CUDA graph; 0: direct launches. */
+lux_status lux_batch_set_graph(LuxBatch *batch, uint32_t enable);
+/* closest/shadow blocks per SM of the batched persistent launches (modes and
+ * sort flags are ignored). */
+lux_status lux_batch_set_tuning(LuxBatch *batch, const LuxTuning *tuning);
+/* One frame of every job with shared settings (layout must be Split). */
+lux_status lux_batch_trace_merge(LuxBatch *batch, const LuxBatchJob *jobs, uint32_t job_count,
+                                 const LuxSettings *settings);
+lux_status lux_batch_info(const LuxBatch *batch, LuxBatchInfo *out);
+
 #ifdef __cplusplus
 }
 #endif
