@@ -36,6 +36,7 @@ TRIANGLES = 262_144
 RAYS_PER_RECEIVER = 36
 EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
+REFERENCE_SPP = 1024
 LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
 
 
@@ -344,6 +345,21 @@ def run_ours(args, rank, world):
         e2e_total = float(t.item())
     e2e_value = world * interval_rays * args.steps / (e2e_total * 1e-3) / 1e6
 
+    # FP32 error of the resolved irradiance against the FP64 path-traced
+    # reference on every 97th resolve point (not timed).
+    view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
+    sub = torch.arange(0, n_pts, 97, device=dev)
+    s_pos, s_nrm, s_est = d_ppos[sub].contiguous(), d_pnrm[sub].contiguous(), d_out[sub].contiguous()
+    s_ref = torch.zeros((len(sub), 4), dtype=torch.float64, device=dev)
+    torch.cuda.synchronize(device)
+    t0 = time.perf_counter()
+    bp.reference_irradiance(ctx, scene, settings, s_pos.data_ptr(), s_nrm.data_ptr(), len(sub), REFERENCE_SPP, 99,
+                            s_ref.data_ptr())
+    ref_s = time.perf_counter() - t0
+    error = bp.error_stats(ctx, s_est.data_ptr(), s_ref.data_ptr(), len(sub))
+    error.update({"spp": REFERENCE_SPP, "sample": f"every 97th resolve point ({len(sub)})",
+                  "reference_s": ref_s, "oracle": "FP64-accumulated path-traced interval radiance"})
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         lay = scene.layout()
@@ -379,6 +395,7 @@ def run_ours(args, rank, world):
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "ms_per_step": e2e_total / args.steps,
                     "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
                     "d2h_bytes_per_step": int(n_pts * 16)},
+            "error_vs_fp64": error,
             "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},

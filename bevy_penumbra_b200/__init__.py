@@ -29,7 +29,7 @@ from ._native import LuxError, check, lib
 
 __all__ = [
     "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
-    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance", "reference_irradiance", "error_stats",
     "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
 ]
 
@@ -344,6 +344,28 @@ def interval_radiance(ctx: LuxContext, scene: GpuScene, settings: RadianceCascad
     ctx.check(lib().lux_interval_radiance(ctx.handle, scene.handle, C.byref(s), rays_device_ptr, count,
                                           out_device_ptr))
     ctx.synchronize()
+
+
+def reference_irradiance(ctx: LuxContext, scene: GpuScene, settings: RadianceCascades, position_ptr: int,
+                         normal_ptr: int, count: int, spp: int, seed: int, out_ptr: int) -> None:
+    """lux_reference_irradiance: FP64 Monte Carlo reference (device double4[count]:
+    mean rgb, supported samples) at device float4 points / unit normals."""
+    s = settings.to_c()
+    ctx.check(lib().lux_reference_irradiance(ctx.handle, scene.handle, C.byref(s), position_ptr, normal_ptr, count,
+                                             spp, seed, out_ptr))
+    ctx.synchronize()
+
+
+def error_stats(ctx: LuxContext, estimate_ptr: int, reference_ptr: int, count: int) -> dict:
+    """lux_error_stats: FP64 error of a float4 estimate against a double4 reference."""
+    out = (C.c_double * 4)()
+    ctx.check(lib().lux_error_stats(ctx.handle, estimate_ptr, reference_ptr, count, out))
+    sq, ref_sum, used, mx = out[0], out[1], out[2], out[3]
+    n = max(used, 1.0) * 3.0
+    rmse = (sq / n) ** 0.5
+    mean = ref_sum / n
+    return {"rmse": rmse, "mean_reference": mean, "relative_rmse": rmse / mean if mean > 0 else float("inf"),
+            "points": int(used), "max_abs_error": mx}
 
 
 class SplitView:

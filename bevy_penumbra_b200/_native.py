@@ -151,6 +151,9 @@ SIGNATURES = {
     "lux_view_read_level": (C.c_int, [P, U32, P, P, P, P]),
     "lux_view_read_probes": (C.c_int, [P, P, P]),
     "lux_view_read_hits": (C.c_int, [P, P, U32]),
+    "lux_reference_round_samples": (U32, [U32, U32]),
+    "lux_reference_irradiance": (C.c_int, [P, P, C.POINTER(LuxSettings), P, P, U32, U32, U32, P]),
+    "lux_error_stats": (C.c_int, [P, P, P, U32, C.POINTER(C.c_double)]),
     "lux_batch_create": (C.c_int, [P, C.POINTER(P)]),
     "lux_batch_destroy": (C.c_int, [P]),
     "lux_batch_set_graph": (C.c_int, [P, U32]),

@@ -139,6 +139,16 @@ LUX_HD uint32_t transport_hash(uint32_t value) {
     return value;
 }
 
+// Sample (u1, u2) in [0, 1)^2 of hemisphere sample `s` at reference point
+// `p` (the FP64 reference irradiance; no reference counterpart): two chained
+// transportHash values, 24 bits each.
+LUX_HD void reference_sample(uint32_t p, uint32_t s, uint32_t seed, float &u1, float &u2) {
+    uint32_t h1 = transport_hash(p ^ transport_hash(s ^ transport_hash(seed + 0x2545f491u)));
+    uint32_t h2 = transport_hash(h1 ^ 0x68bc21ebu);
+    u1 = (float)(h1 >> 8) / 16777216.0f;
+    u2 = (float)(h2 >> 8) / 16777216.0f;
+}
+
 // hashKey, shaders/common.slang:423-429.
 LUX_HD uint32_t hash_key(int32_t kx, int32_t ky, int32_t kz, int32_t kw, uint32_t buckets) {
     uint32_t h = (uint32_t)kx * 0x8da6b343u ^ (uint32_t)ky * 0xd8163841u ^ (uint32_t)kz * 0xcb1ab31fu ^
@@ -222,5 +232,22 @@ LUX_HD bool cell_in_range(int32_t x, int32_t y, int32_t z) {
     return x >= -lim && x < lim && y >= -lim && y < lim && z >= -lim && z < lim;
 }
 constexpr uint64_t kEmptyCell = 0xffffffffffffffffull;
+
+// Cosine-weighted direction about the unit normal n: radius sqrt(u1) at
+// u2 turns in the tangent plane, height sqrt(1 - u1), in the orthonormal
+// frame of Duff et al., "Building an Orthonormal Basis, Revisited" (2017).
+LUX_HD f3 cosine_direction(f3 n, float u1, float u2) {
+    float sign = n.z >= 0.0f ? 1.0f : -1.0f;
+    float a = -1.0f / (sign + n.z);
+    float b = n.x * n.y * a;
+    f3 t{1.0f + sign * n.x * n.x * a, sign * b, -sign * n.x};
+    f3 bt{b, sign + n.y * n.y * a, -n.y};
+    float c, s;
+    sincos_turns(u2, c, s);
+    float r = sqrtf(u1);
+    float z = sqrtf(fmaxf(1.0f - u1, 0.0f));
+    float x = r * c, y = r * s;
+    return f3{(t.x * x + bt.x * y) + n.x * z, (t.y * x + bt.y * y) + n.y * z, (t.z * x + bt.z * y) + n.z * z};
+}
 
 }  // namespace lux

@@ -1987,3 +1987,159 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
     }
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "batch launch");
 }
+
+// ---- FP64 reference irradiance and error reductions --------------------------
+// The oracle of the error reports (no reference counterpart): Monte Carlo
+// over cosine-weighted hemisphere rays of the same interval radiance the
+// cascades resolve (emission seen + one-bounce next-event estimation), each
+// ray traced and shaded in FP32 by the library's kernels, the per-point means
+// accumulated in FP64.
+namespace {
+
+constexpr uint32_t kReferenceRoundRays = 1u << 21;
+
+__global__ void reference_rays_kernel(const float4 *__restrict__ pos, const float4 *__restrict__ nrm, uint32_t count,
+                                      uint32_t sample0, uint32_t samples, uint32_t seed, float bias,
+                                      LuxRay *__restrict__ rays) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count * samples) return;
+    uint32_t p = i / samples, s = sample0 + i % samples;
+    float4 p4 = pos[p], n4 = nrm[p];
+    f3 P{p4.x, p4.y, p4.z}, N{n4.x, n4.y, n4.z};
+    float u1, u2;
+    lux::reference_sample(p, s, seed, u1, u2);
+    f3 d = lux::cosine_direction(N, u1, u2);
+    f3 o = lux::ray_offset(P, N, bias);
+    LuxRay r;
+    r.origin[0] = o.x;
+    r.origin[1] = o.y;
+    r.origin[2] = o.z;
+    r.tmin = 0.0f;
+    r.direction[0] = d.x;
+    r.direction[1] = d.y;
+    r.direction[2] = d.z;
+    r.limit = 1e20f;
+    rays[i] = r;
+}
+
+// acc[p] += (sum of supported sample radiance, supported samples), in
+// sample order.
+__global__ void reference_accumulate_kernel(const float4 *__restrict__ radiance, uint32_t count, uint32_t samples,
+                                            double4 *__restrict__ acc) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    double4 a = acc[p];
+    for (uint32_t s = 0; s < samples; ++s) {
+        float4 v = radiance[(size_t)p * samples + s];
+        if (v.w < 0.0f) continue;
+        a.x += (double)v.x;
+        a.y += (double)v.y;
+        a.z += (double)v.z;
+        a.w += 1.0;
+    }
+    acc[p] = a;
+}
+
+__global__ void reference_finish_kernel(double4 *__restrict__ acc, uint32_t count) {
+    uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    double4 a = acc[p];
+    acc[p] = a.w > 0.0 ? make_double4(a.x / a.w, a.y / a.w, a.z / a.w, a.w) : make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+// out[0] += sum of squared rgb error, out[1] += sum of reference rgb,
+// out[2] += points used, out[3] = max |error| (as ordered bits): points with
+// estimate alpha > 0 and at least one reference sample.
+__global__ void error_stats_kernel(const float4 *__restrict__ est, const double4 *__restrict__ ref, uint32_t count,
+                                   double *__restrict__ out) {
+    double sq = 0.0, sum = 0.0, used = 0.0, mx = 0.0;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+        float4 e = est[p];
+        double4 r = ref[p];
+        if (!(e.w > 0.0f) || !(r.w > 0.0)) continue;
+        double dx = (double)e.x - r.x, dy = (double)e.y - r.y, dz = (double)e.z - r.z;
+        sq += dx * dx + dy * dy + dz * dz;
+        sum += r.x + r.y + r.z;
+        used += 1.0;
+        mx = fmax(mx, fmax(fabs(dx), fmax(fabs(dy), fabs(dz))));
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+        sq += __shfl_down_sync(0xffffffffu, sq, off);
+        sum += __shfl_down_sync(0xffffffffu, sum, off);
+        used += __shfl_down_sync(0xffffffffu, used, off);
+        mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    }
+    if ((threadIdx.x & 31u) == 0u) {
+        atomicAdd(&out[0], sq);
+        atomicAdd(&out[1], sum);
+        atomicAdd(&out[2], used);
+        atomicMax((unsigned long long *)&out[3], (unsigned long long)__double_as_longlong(mx));
+    }
+}
+
+}  // namespace
+
+extern "C" uint32_t lux_reference_round_samples(uint32_t count, uint32_t spp) {
+    if (count == 0 || spp == 0) return 0;
+    uint32_t r = kReferenceRoundRays / count;
+    r = r < 1u ? 1u : r;
+    return r < spp ? r : spp;
+}
+
+extern "C" lux_status lux_reference_irradiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
+                                               const float *position, const float *normal, uint32_t count,
+                                               uint32_t spp, uint32_t seed, double *out) {
+    if (!ctx || !scene || !settings || (count && (!position || !normal || !out))) return LUX_ERR_INVALID_ARGUMENT;
+    if (count == 0) return LUX_OK;
+    if (spp == 0) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "reference: spp must be positive");
+    LuxSettings s = *settings;
+    lux_settings_sanitize(&s);
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    const uint32_t round = lux_reference_round_samples(count, spp);
+    const uint32_t rays = count * round;
+    LuxRay *d_rays = nullptr;
+    float4 *d_rad = nullptr;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaMallocAsync((void **)&d_rays, (size_t)rays * sizeof(LuxRay), st),
+                                   "reference: rays");
+    if (rc == LUX_OK)
+        rc = lux_cuda_check(ctx, (int)cudaMallocAsync((void **)&d_rad, (size_t)rays * sizeof(float4), st),
+                            "reference: radiance");
+    if (rc == LUX_OK)
+        rc = lux_cuda_check(ctx, (int)cudaMemsetAsync(out, 0, (size_t)count * sizeof(double4), st), "reference: clear");
+    for (uint32_t k = 0, s0 = 0; rc == LUX_OK && s0 < spp; ++k, s0 += round) {
+        uint32_t samples = std::min(round, spp - s0);
+        uint32_t n = count * samples;
+        reference_rays_kernel<<<(n + 255) / 256, 256, 0, st>>>((const float4 *)position, (const float4 *)normal,
+                                                                count, s0, samples, seed, s.normal_bias, d_rays);
+        LuxSettings fs = s;
+        fs.frame_index = seed + k;
+        rc = lux_interval_radiance(ctx, scene, &fs, d_rays, n, (float *)d_rad);
+        if (rc != LUX_OK) break;
+        reference_accumulate_kernel<<<(count + 127) / 128, 128, 0, st>>>(d_rad, count, samples, (double4 *)out);
+    }
+    if (rc == LUX_OK) reference_finish_kernel<<<(count + 127) / 128, 128, 0, st>>>((double4 *)out, count);
+    if (d_rays) cudaFreeAsync(d_rays, st);
+    if (d_rad) cudaFreeAsync(d_rad, st);
+    if (rc != LUX_OK) return rc;
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "reference launch");
+}
+
+extern "C" lux_status lux_error_stats(LuxContext *ctx, const float *estimate, const double *reference, uint32_t count,
+                                      double out[4]) {
+    if (!ctx || !out || (count && (!estimate || !reference))) return LUX_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    double *d = nullptr;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaMallocAsync((void **)&d, 4 * sizeof(double), st), "error: sums");
+    if (rc != LUX_OK) return rc;
+    cudaMemsetAsync(d, 0, 4 * sizeof(double), st);
+    if (count)
+        error_stats_kernel<<<std::min((count + 255) / 256, (uint32_t)ctx->sm_count * 4), 256, 0, st>>>(
+            (const float4 *)estimate, (const double4 *)reference, count, d);
+    cudaMemcpyAsync(out, d, 4 * sizeof(double), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d, st);
+    rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "error stats");
+    if (rc != LUX_OK) return rc;
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "error stats launch");
+}

@@ -357,6 +357,30 @@ lux_status lux_view_read_probes(LuxView *view, int32_t *cell_keys, float *tables
  * the frame's interval rays.  visited is 0.  For comparing runs. */
 lux_status lux_view_read_hits(LuxView *view, LuxHit *out, uint32_t count);
 
+/* ---- FP64 reference and error reductions ----------------------------------
+ * No reference counterpart: the oracle of the error reports.  For every point
+ * (device float4 position, float4 unit normal) the mean over `spp`
+ * cosine-weighted hemisphere rays from rayOffset(point, normal, normal_bias)
+ * of the interval radiance the cascades resolve (emission seen plus
+ * one-bounce next-event estimation; irradiance / pi before receiver albedo,
+ * the raw output's units).  Rays are traced and shaded in FP32 by the same
+ * kernels as lux_interval_radiance; only the per-point accumulation is FP64.
+ * Samples run in rounds of lux_reference_round_samples(count, spp) per point
+ * (frame index seed + round for the next-event samples).  out: device
+ * double4[count] = (mean r, g, b, supported samples).  Allocates temporary
+ * device memory; ordered on the context stream. */
+uint32_t lux_reference_round_samples(uint32_t count, uint32_t spp);
+lux_status lux_reference_irradiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
+                                    const float *position, const float *normal, uint32_t count,
+                                    uint32_t spp, uint32_t seed, double *out);
+/* FP64 error of an FP32 estimate (device float4[count], alpha > 0 =
+ * resolved) against a reference (device double4[count], w > 0 = sampled):
+ * out[4] (host) = {sum of squared rgb error, sum of reference rgb, points
+ * used, max |error|}; relative RMSE = sqrt(out[0] / (3 out[2])) /
+ * (out[1] / (3 out[2])).  Synchronises the context stream. */
+lux_status lux_error_stats(LuxContext *ctx, const float *estimate, const double *reference, uint32_t count,
+                           double out[4]);
+
 /* ---- batching: many scenes and views in one launch per trace stage -------
  * No reference counterpart (the reference renders one view per dispatch
  * sequence).  One lux_batch_trace_merge runs the Split frame of every job:

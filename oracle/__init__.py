@@ -54,6 +54,7 @@ def lib():
             "orc_scene_create": (P, [P, C.c_size_t, P, C.c_size_t, P, U, U]),
             "orc_scene_destroy": (None, [P]),
             "orc_scene_refit": (C.c_int, [P, P, C.c_uint32]),
+            "orc_reference_irradiance": (None, [P, P, P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, P]),
             "orc_scene_words": (None, [P, P]),
             "orc_trace_closest": (None, [P, P, P, F, F, P, P]),
             "orc_trace_occluded": (C.c_int, [P, P, P, F, P, P]),
@@ -131,6 +132,15 @@ class OracleScene:
         rc = lib().orc_scene_refit(self.handle, _p(m), len(m))
         if rc != 0:
             raise ValueError("oracle refit: instance count mismatch or singular transform")
+
+    def reference_irradiance(self, settings_c, position, normal, spp: int, seed: int, round_samples: int):
+        """FP64 reference irradiance (double[count, 4]) at float4 points / normals."""
+        pos = np.ascontiguousarray(position, np.float32)
+        nrm = np.ascontiguousarray(normal, np.float32)
+        out = np.zeros((len(pos), 4), np.float64)
+        lib().orc_reference_irradiance(self.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos), spp, seed,
+                                       round_samples, _p(out))
+        return out
 
     def words(self) -> np.ndarray:
         out = np.zeros(self._keep[0].shape, dtype=np.uint32).reshape(-1, 4)

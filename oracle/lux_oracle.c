@@ -2059,3 +2059,70 @@ void orc_dense_sdf_record(uint32_t index, float interval[4], float direction[4])
     direction[2] = dir[2];
     direction[3] = (float)di;
 }
+
+/* --- FP64 reference irradiance (the error-report oracle; no reference
+ * counterpart).  Restates lux_reference_irradiance: cosine-weighted rays,
+ * interval radiance per ray, per-point means accumulated in double in
+ * sample order, rounds of `round` samples with frame index seed + round. */
+
+static uint32_t orc_hash(uint32_t value) { return orc_transport_hash(value); }
+
+void orc_reference_sample(uint32_t p, uint32_t s, uint32_t seed, float *u1, float *u2) {
+    uint32_t h1 = orc_hash(p ^ orc_hash(s ^ orc_hash(seed + 0x2545f491u)));
+    uint32_t h2 = orc_hash(h1 ^ 0x68bc21ebu);
+    *u1 = (float)(h1 >> 8) / 16777216.0f;
+    *u2 = (float)(h2 >> 8) / 16777216.0f;
+}
+
+/* Cosine-weighted direction in the orthonormal frame of Duff et al. (2017). */
+void orc_cosine_direction(const float n[3], float u1, float u2, float out[3]) {
+    float sign = n[2] >= 0.0f ? 1.0f : -1.0f;
+    float a = -1.0f / (sign + n[2]);
+    float b = n[0] * n[1] * a;
+    float t[3] = {1.0f + sign * n[0] * n[0] * a, sign * b, -sign * n[0]};
+    float bt[3] = {b, sign + n[1] * n[1] * a, -n[1]};
+    float c, s;
+    orc_sincos_turns(u2, &c, &s);
+    float r = sqrtf(u1);
+    float z = sqrtf(fmaxf(1.0f - u1, 0.0f));
+    float x = r * c, y = r * s;
+    for (int k = 0; k < 3; ++k) out[k] = (t[k] * x + bt[k] * y) + n[k] * z;
+}
+
+void orc_reference_irradiance(const OrcScene *S, const LuxSettings *settings_in, const float *position,
+                              const float *normal, uint32_t count, uint32_t spp, uint32_t seed, uint32_t round,
+                              double *out) {
+    LuxSettings st = *settings_in;
+    for (uint32_t p = 0; p < count; ++p) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        const float *P = position + 4 * (size_t)p, *N = normal + 4 * (size_t)p;
+        for (uint32_t k = 0, s0 = 0; s0 < spp; ++k, s0 += round) {
+            uint32_t samples = round < spp - s0 ? round : spp - s0;
+            st.frame_index = seed + k;
+            for (uint32_t s = s0; s < s0 + samples; ++s) {
+                float u1, u2, d[3], o[3];
+                orc_reference_sample(p, s, seed, &u1, &u2);
+                orc_cosine_direction(N, u1, u2, d);
+                orc_ray_offset(P, N, st.normal_bias, o);
+                LuxHit hit;
+                orc_trace_closest(S, o, d, 0.0f, 1e20f, &hit, NULL);
+                float rad[3];
+                uint64_t shadow = 0;
+                if (!orc_outgoing_radiance(S, &st, o, d, &hit, rad, &shadow, NULL)) continue;
+                acc[0] += (double)rad[0];
+                acc[1] += (double)rad[1];
+                acc[2] += (double)rad[2];
+                acc[3] += 1.0;
+            }
+        }
+        double *q = out + 4 * (size_t)p;
+        if (acc[3] > 0.0) {
+            q[0] = acc[0] / acc[3];
+            q[1] = acc[1] / acc[3];
+            q[2] = acc[2] / acc[3];
+            q[3] = acc[3];
+        } else {
+            q[0] = q[1] = q[2] = q[3] = 0.0;
+        }
+    }
+}

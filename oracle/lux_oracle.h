@@ -83,6 +83,14 @@ int orc_outgoing_radiance(const OrcScene *scene, const LuxSettings *settings,
                           const float origin[3], const float direction[3], const LuxHit *hit,
                           float out[3], uint64_t *shadow_rays, OrcCounters *counters);
 
+/* FP64 reference irradiance (lux_reference_irradiance restated; `round` =
+ * lux_reference_round_samples(count, spp)); out double4[count]. */
+void orc_reference_sample(uint32_t p, uint32_t s, uint32_t seed, float *u1, float *u2);
+void orc_cosine_direction(const float n[3], float u1, float u2, float out[3]);
+void orc_reference_irradiance(const OrcScene *scene, const LuxSettings *settings, const float *position,
+                              const float *normal, uint32_t count, uint32_t spp, uint32_t seed, uint32_t round,
+                              double *out);
+
 /* --- one cascade frame ---------------------------------------------------- */
 typedef struct OrcFrame OrcFrame;
 OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
