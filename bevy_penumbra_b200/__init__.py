@@ -29,7 +29,7 @@ from ._native import LuxError, check, lib
 
 __all__ = [
     "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
-    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance", "reference_irradiance", "error_stats",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance", "reference_irradiance", "error_stats", "LearnedCache", "CACHE_SAMPLE_DTYPE",
     "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
 ]
 
@@ -456,6 +456,26 @@ class SplitView:
             self.ctx.check(lib().lux_view_read_probes(self.handle, _ptr(keys), _ptr(tables)))
         return keys, tables
 
+    def set_cache(self, cache, cutoff_level: int = 3, validate_period: int = 16, error_bound: float = 0.25,
+                  train_samples: int = 65536, fallback_frames: int = 32) -> None:
+        """lux_view_set_cache: the learned-cache form (cache=None: plain)."""
+        if cache is None:
+            self.ctx.check(lib().lux_view_set_cache(self.handle, None))
+            return
+        m = N.LuxCacheMode()
+        m.cache = cache.handle
+        m.cutoff_level = cutoff_level
+        m.validate_period = validate_period
+        m.error_bound = error_bound
+        m.train_samples = train_samples
+        m.fallback_frames = fallback_frames
+        self.ctx.check(lib().lux_view_set_cache(self.handle, C.byref(m)))
+
+    def cache_stats(self) -> N.LuxCacheFrameStats:
+        out = N.LuxCacheFrameStats()
+        self.ctx.check(lib().lux_view_cache_stats(self.handle, C.byref(out)))
+        return out
+
     def read_hits(self, count: int) -> np.ndarray:
         """lux_view_read_hits: the last Split frame's first `count` interval-ray hits."""
         out = np.zeros(count, dtype=HIT_DTYPE)
@@ -513,6 +533,67 @@ class Batch:
     def close(self) -> None:
         if self.handle:
             lib().lux_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+CACHE_SAMPLE_DTYPE = np.dtype([("position", "<f4", 3), ("weight", "<f4"), ("direction", "<f4", 3), ("pad0", "<f4"),
+                               ("normal", "<f4", 3), ("pad1", "<f4"), ("albedo", "<f4", 3), ("pad2", "<f4")])
+CACHE_WEIGHTS = 4 * 64 * 64 + 16 * 64
+
+
+class LearnedCache:
+    """lux_cache_*: hash-grid encoded MLP radiance cache (tcgen05 BF16 MLP)."""
+
+    def __init__(self, ctx: LuxContext, **desc):
+        self.ctx = ctx
+        d = N.LuxCacheDesc()
+        lib().lux_cache_desc_default(C.byref(d))
+        for k, v in desc.items():
+            setattr(d, k, v)
+        handle = C.c_void_p()
+        ctx.check(lib().lux_cache_create(ctx.handle, C.byref(d), C.byref(handle)))
+        self.handle = handle
+        self.desc = d
+
+    def set_bounds(self, lo, hi) -> None:
+        lo = np.asarray(lo, np.float32)
+        hi = np.asarray(hi, np.float32)
+        self.ctx.check(lib().lux_cache_set_bounds(self.handle, _ptr(lo), _ptr(hi)))
+
+    def train(self, samples_ptr: int, targets_ptr: int, count: int) -> None:
+        self.ctx.check(lib().lux_cache_train(self.handle, samples_ptr, targets_ptr, count))
+
+    def query(self, queries_ptr: int, count: int, out_ptr: int) -> None:
+        self.ctx.check(lib().lux_cache_query(self.handle, queries_ptr, count, out_ptr))
+
+    def encode(self, samples_ptr: int, count: int, out_ptr: int) -> None:
+        self.ctx.check(lib().lux_cache_encode(self.handle, samples_ptr, count, out_ptr))
+
+    def forward(self, encoded_ptr: int, count: int, out_ptr: int) -> None:
+        self.ctx.check(lib().lux_cache_forward(self.handle, encoded_ptr, count, out_ptr))
+
+    def weights(self) -> list:
+        """FP32 master weights: 4 x [64, 64] hidden layers and the [16, 64] output layer ([out, in])."""
+        w = np.zeros(CACHE_WEIGHTS, np.float32)
+        self.ctx.check(lib().lux_cache_read_weights(self.handle, _ptr(w)))
+        layers = [w[k * 4096:(k + 1) * 4096].reshape(64, 64) for k in range(4)]
+        layers.append(w[4 * 4096:].reshape(16, 64))
+        return layers
+
+    def stats(self) -> N.LuxCacheStats:
+        out = N.LuxCacheStats()
+        self.ctx.check(lib().lux_cache_stats(self.handle, C.byref(out)))
+        return out
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_cache_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -97,6 +97,29 @@ class LuxTuning(C.Structure):
                 ("reserved", C.c_uint32 * 2)]
 
 
+class LuxCacheDesc(C.Structure):
+    _fields_ = [("levels", C.c_uint32), ("log2_table", C.c_uint32), ("base_resolution", C.c_uint32),
+                ("growth", C.c_float), ("learning_rate", C.c_float), ("batch", C.c_uint32), ("seed", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class LuxCacheStats(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("samples", C.c_uint64), ("last_loss", C.c_float),
+                ("error_flags", C.c_uint32)]
+
+
+class LuxCacheMode(C.Structure):
+    _fields_ = [("cache", C.c_void_p), ("cutoff_level", C.c_uint32), ("validate_period", C.c_uint32),
+                ("error_bound", C.c_float), ("train_samples", C.c_uint32), ("fallback_frames", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
+class LuxCacheFrameStats(C.Structure):
+    _fields_ = [("cached_rays", C.c_uint64), ("validated_rays", C.c_uint64), ("train_candidates", C.c_uint64),
+                ("trained_samples", C.c_uint64), ("validated_cells", C.c_uint32), ("failed_cells", C.c_uint32),
+                ("fallback_rays", C.c_uint32), ("validated_bias", C.c_float)]
+
+
 class LuxBatchJob(C.Structure):
     _fields_ = [("view", C.c_void_p), ("scene", C.c_void_p), ("receivers", LuxReceivers)]
 
@@ -151,9 +174,21 @@ SIGNATURES = {
     "lux_view_read_level": (C.c_int, [P, U32, P, P, P, P]),
     "lux_view_read_probes": (C.c_int, [P, P, P]),
     "lux_view_read_hits": (C.c_int, [P, P, U32]),
+    "lux_view_set_cache": (C.c_int, [P, C.POINTER(LuxCacheMode)]),
+    "lux_view_cache_stats": (C.c_int, [P, C.POINTER(LuxCacheFrameStats)]),
     "lux_reference_round_samples": (U32, [U32, U32]),
     "lux_reference_irradiance": (C.c_int, [P, P, C.POINTER(LuxSettings), P, P, U32, U32, U32, P]),
     "lux_error_stats": (C.c_int, [P, P, P, U32, C.POINTER(C.c_double)]),
+    "lux_cache_desc_default": (None, [C.POINTER(LuxCacheDesc)]),
+    "lux_cache_create": (C.c_int, [P, C.POINTER(LuxCacheDesc), C.POINTER(P)]),
+    "lux_cache_destroy": (C.c_int, [P]),
+    "lux_cache_set_bounds": (C.c_int, [P, P, P]),
+    "lux_cache_train": (C.c_int, [P, P, P, U32]),
+    "lux_cache_query": (C.c_int, [P, P, U32, P]),
+    "lux_cache_stats": (C.c_int, [P, C.POINTER(LuxCacheStats)]),
+    "lux_cache_encode": (C.c_int, [P, P, U32, P]),
+    "lux_cache_read_weights": (C.c_int, [P, P]),
+    "lux_cache_forward": (C.c_int, [P, P, U32, P]),
     "lux_batch_create": (C.c_int, [P, C.POINTER(P)]),
     "lux_batch_destroy": (C.c_int, [P]),
     "lux_batch_set_graph": (C.c_int, [P, U32]),

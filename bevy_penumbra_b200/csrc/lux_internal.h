@@ -141,5 +141,11 @@ struct LuxScene {
 // same instance rows as packing the scene at that pose.
 bool lux_affine_inverse(const float world_from_local[12], float local_from_world[12]);
 
+// Cache query over a compacted list whose length is on the device
+// (count <= max_count); ordered on the cache's context stream.
+LuxContext *lux_cache_context(const LuxCache *cache);
+lux_status lux_cache_query_device_count(LuxCache *cache, const LuxCacheSample *queries, const uint32_t *count,
+                                        uint32_t max_count, float *out);
+
 lux_status lux_fail(LuxContext *ctx, lux_status status, const std::string &message);
 lux_status lux_cuda_check(LuxContext *ctx, int err, const char *what);

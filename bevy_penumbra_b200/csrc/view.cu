@@ -1121,6 +1121,253 @@ __global__ void read_hits_kernel(ViewDevice V, uint32_t count, LuxHit *__restric
     out[i] = r;
 }
 
+// ---- learned-cache form ----------------------------------------------------
+constexpr uint32_t kFallbackSlots = 1u << 17;
+constexpr uint32_t kFallbackProbes = 16;
+enum CacheCounter : uint32_t {
+    kCntQueries = 0, kCntCandidates = 1, kCntTrain = 2, kCntCached = 3, kCntValidated = 4, kCntValidatedCells = 5,
+    kCntFailedCells = 6, kCntFallbackRays = 7, kCntCount = 8
+};
+constexpr uint8_t kRayPlain = 0, kRayCached = 1, kRayValidated = 2;
+
+struct CacheDevice {
+    uint8_t *flags;                // per ray
+    LuxCacheSample *queries;       // per ray (compacted)
+    uint32_t *query_ray;           // per compacted query: ray index
+    float4 *pred;                  // per compacted query
+    LuxCacheSample *train;         // [train_cap]
+    float4 *target;                // [train_cap]
+    float4 *cell_error;            // per cascade-0 cell: sums of (cache - traced), traced, traced^2; rgb summed
+    float *global_error;           // [2]: the same sums over every validated cell
+    unsigned long long *fb_key;    // fallback table
+    uint32_t *fb_expiry;
+    uint32_t *counters;            // CacheCounter
+    uint32_t cutoff, period, frame, fallback_frames, train_cap;
+    float near_limit, far_t, bound;
+};
+
+__device__ __forceinline__ uint32_t cell_hash(unsigned long long key) {
+    return lux::transport_hash((uint32_t)key ^ lux::transport_hash((uint32_t)(key >> 32)));
+}
+
+__device__ __forceinline__ bool fallback_active(const CacheDevice &C, unsigned long long key) {
+    uint32_t h = cell_hash(key) & (kFallbackSlots - 1u);
+    for (uint32_t p = 0; p < kFallbackProbes; ++p) {
+        uint32_t slot = (h + p) & (kFallbackSlots - 1u);
+        unsigned long long k = C.fb_key[slot];
+        if (k == key) return C.fb_expiry[slot] > C.frame;
+        if (k == lux::kEmptyCell) return false;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void fallback_insert(const CacheDevice &C, unsigned long long key, uint32_t expiry) {
+    uint32_t h = cell_hash(key) & (kFallbackSlots - 1u);
+    for (uint32_t p = 0; p < kFallbackProbes; ++p) {
+        uint32_t slot = (h + p) & (kFallbackSlots - 1u);
+        unsigned long long prev = atomicCAS(&C.fb_key[slot], lux::kEmptyCell, key);
+        if (prev == lux::kEmptyCell || prev == key) {
+            atomicMax(&C.fb_expiry[slot], expiry);
+            return;
+        }
+    }
+}
+
+__device__ __forceinline__ unsigned long long receiver_key(const FrameParams &F, f3 p) {
+    int32_t x, y, z;
+    cell_of(F, 0, p, x, y, z);
+    return lux::pack_cell(x, y, z);
+}
+
+// Interval rays of the learned-cache form: full traces for validated and
+// fallback cells, otherwise up to the cutoff; a truncated ray that meets
+// nothing is answered by the cache at level `cutoff` (its stored distance
+// is that level's interval end, so the deposit terminates there).
+__global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
+    closest_cache_kernel(ViewDevice V, FrameParams F, SceneView S, const float4 *__restrict__ pos,
+                         const float4 *__restrict__ nrm, uint32_t ray_count, CacheDevice C) {
+    if (*V.error_flags) return;
+    unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
+    lux::TraceCounters cn{0, 0, 0};
+    uint32_t fallback_rays = 0;
+    while (true) {
+        uint32_t base = warp_fetch(&V.ts.work_counter[0]);
+        if (base >= ray_count) break;
+        uint32_t ray = base + (threadIdx.x & 31u);
+        if (ray < ray_count) {
+            uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+            float4 p4 = pos[i], n4 = nrm[i];
+            f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+            unsigned long long key = receiver_key(F, p);
+            bool validate = cell_hash(key) % C.period == C.frame % C.period;
+            bool fallback = !validate && fallback_active(C, key);
+            bool full = validate || fallback;
+            f3 dir;
+            float u, v;
+            split_direction(F, F.shade.frame, i, k, n, dir, u, v);
+            f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
+            lux::Hit hit;
+            lux::trace<false>(S, origin, dir, 0.0f, full ? 1e20f : C.near_limit, hit, cn);
+            uint8_t flag = kRayPlain;
+            if (!full && hit.tri == lux::kEmpty) {
+                flag = kRayCached;
+                hit.t = C.far_t;
+            } else if (validate && hit.t > F.end[C.cutoff - 1u]) {
+                flag = kRayValidated;
+            }
+            fallback_rays += fallback ? 1u : 0u;
+            C.flags[ray] = flag;
+            store_ray(V, ray, origin, dir, hit);
+            st[kStatInterval] += 1;
+        }
+    }
+    st[kStatNodes] = cn.nodes;
+    st[kStatTris] = cn.triangles;
+    st[kStatInst] = cn.instances;
+    add_stats(V.stats, st);
+    for (int off = 16; off > 0; off >>= 1) fallback_rays += __shfl_down_sync(0xffffffffu, fallback_rays, off);
+    if ((threadIdx.x & 31u) == 0u && fallback_rays) atomicAdd(&C.counters[kCntFallbackRays], fallback_rays);
+}
+
+// Compacted cache queries: every cached or validated ray, keyed by its
+// origin and direction at its receiver's normal (albedo unknown: zero).
+__global__ void cache_queries_kernel(ViewDevice V, const float4 *__restrict__ nrm, uint32_t ray_count,
+                                     uint32_t rays_per_receiver, CacheDevice C) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < ray_count; base += gridDim.x * blockDim.x) {
+        uint32_t ray = base + threadIdx.x;
+        bool want = ray < ray_count && C.flags[ray] != kRayPlain;
+        uint32_t mask = __ballot_sync(0xffffffffu, want);
+        uint32_t first = 0;
+        if (lane == 0 && mask) first = atomicAdd(&C.counters[kCntQueries], (uint32_t)__popc(mask));
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (!want) continue;
+        uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+        float4 o = V.ts.ray_o[ray], d = V.ts.ray_d[ray], n = nrm[ray / rays_per_receiver];
+        LuxCacheSample q;
+        q.position[0] = o.x;
+        q.position[1] = o.y;
+        q.position[2] = o.z;
+        q.weight = 1.0f;
+        q.direction[0] = d.x;
+        q.direction[1] = d.y;
+        q.direction[2] = d.z;
+        q.pad0 = 0.0f;
+        q.normal[0] = n.x;
+        q.normal[1] = n.y;
+        q.normal[2] = n.z;
+        q.pad1 = 0.0f;
+        q.albedo[0] = q.albedo[1] = q.albedo[2] = 0.0f;
+        q.pad2 = 0.0f;
+        C.queries[slot] = q;
+        C.query_ray[slot] = ray;
+    }
+}
+
+// Cached rays take the prediction as their hit radiance (no next-event
+// samples); validated rays compare it with what they traced, per cell.
+__global__ void cache_apply_kernel(ViewDevice V, FrameParams F, uint32_t ray_count, CacheDevice C) {
+    uint32_t n = min(C.counters[kCntQueries], ray_count);
+    for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += gridDim.x * blockDim.x) {
+        uint32_t ray = C.query_ray[q];
+        float4 pr = C.pred[q];
+        if (C.flags[ray] == kRayCached) {
+            V.ts.ray_base[ray] = make_float4(pr.x, pr.y, pr.z, lux::as_float(0u));
+            atomicAdd(&C.counters[kCntCached], 1u);
+        } else {
+            f3 traced;
+            if (!ray_radiance(V, ray, traced)) continue;
+            uint32_t cell = V.receiver_cell[ray / F.rays_per_receiver];
+            if (cell == lux::kEmpty) continue;
+            // Signed: the per-ray traced radiance carries next-event noise,
+            // so the cell's summed difference measures the cache's bias.
+            float err = (pr.x - traced.x) + (pr.y - traced.y) + (pr.z - traced.z);
+            float t = traced.x + traced.y + traced.z;
+            atomicAdd(&C.cell_error[cell].x, err);
+            atomicAdd(&C.cell_error[cell].y, t);
+            atomicAdd(&C.cell_error[cell].z, t * t);
+            atomicAdd(&C.counters[kCntValidated], 1u);
+        }
+    }
+}
+
+__device__ __forceinline__ bool train_candidate(const ViewDevice &V, const FrameParams &F, const CacheDevice &C,
+                                                uint32_t ray, f3 &radiance) {
+    uint8_t flag = C.flags[ray];
+    if (flag == kRayCached) return false;
+    if (flag != kRayValidated) {
+        uint4 h = V.ts.ray_h[ray];
+        if (h.x == lux::kEmpty || V.ts.ray_o[ray].w > F.end[F.levels > 1u ? 1u : 0u]) return false;
+    }
+    return ray_radiance(V, ray, radiance);
+}
+
+__global__ void cache_count_kernel(ViewDevice V, FrameParams F, uint32_t ray_count, CacheDevice C) {
+    uint32_t count = 0;
+    for (uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x; ray < ray_count; ray += gridDim.x * blockDim.x) {
+        f3 r;
+        count += train_candidate(V, F, C, ray, r) ? 1u : 0u;
+    }
+    for (int off = 16; off > 0; off >>= 1) count += __shfl_down_sync(0xffffffffu, count, off);
+    if ((threadIdx.x & 31u) == 0u && count) atomicAdd(&C.counters[kCntCandidates], count);
+}
+
+// Training samples: each candidate is kept with probability cap / candidates
+// (a hash of ray and frame), up to cap.
+__global__ void cache_select_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ nrm, uint32_t ray_count,
+                                    CacheDevice C) {
+    uint32_t candidates = C.counters[kCntCandidates];
+    float keep = candidates > C.train_cap ? (float)C.train_cap / (float)candidates : 1.0f;
+    for (uint32_t ray = blockIdx.x * blockDim.x + threadIdx.x; ray < ray_count; ray += gridDim.x * blockDim.x) {
+        f3 r;
+        if (!train_candidate(V, F, C, ray, r)) continue;
+        float u = (float)(lux::transport_hash(ray * 0x9E3779B9u ^ lux::transport_hash(C.frame)) >> 8) / 16777216.0f;
+        if (u >= keep) continue;
+        uint32_t slot = atomicAdd(&C.counters[kCntTrain], 1u);
+        if (slot >= C.train_cap) continue;
+        float4 o = V.ts.ray_o[ray], d = V.ts.ray_d[ray], n = nrm[ray / F.rays_per_receiver];
+        LuxCacheSample s;
+        s.position[0] = o.x;
+        s.position[1] = o.y;
+        s.position[2] = o.z;
+        s.weight = 1.0f;
+        s.direction[0] = d.x;
+        s.direction[1] = d.y;
+        s.direction[2] = d.z;
+        s.pad0 = 0.0f;
+        s.normal[0] = n.x;
+        s.normal[1] = n.y;
+        s.normal[2] = n.z;
+        s.pad1 = 0.0f;
+        s.albedo[0] = s.albedo[1] = s.albedo[2] = 0.0f;
+        s.pad2 = 0.0f;
+        C.train[slot] = s;
+        C.target[slot] = make_float4(r.x, r.y, r.z, 0.0f);
+    }
+}
+
+// Validated cells whose cache error exceeds the bound fall back to full
+// tracing for the next frames.
+__global__ void cache_fallback_kernel(ViewDevice V, FrameParams F, CacheDevice C) {
+    uint32_t cells = min(V.cell_count[0], F.cell_capacity);
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+        float4 e = C.cell_error[c];
+        C.cell_error[c] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (!(e.y > 0.0f) && e.x == 0.0f) continue;
+        atomicAdd(&C.counters[kCntValidatedCells], 1u);
+        atomicAdd(&C.global_error[0], e.x);
+        atomicAdd(&C.global_error[1], e.y);
+        // Fail when the bias is both large (bound x traced) and significant:
+        // beyond three standard deviations of a sum of per-ray values whose
+        // second moment is sum t^2.
+        if (fabsf(e.x) > C.bound * e.y + 3.0f * sqrtf(e.z) + 1e-6f) {
+            int4 key = V.cell_keys[c];
+            fallback_insert(C, lux::pack_cell(key.x, key.y, key.z), C.frame + C.fallback_frames);
+            atomicAdd(&C.counters[kCntFailedCells], 1u);
+        }
+    }
+}
+
 }  // namespace
 
 constexpr int kTimingEvents = 7;
@@ -1137,7 +1384,21 @@ struct LuxView {
     uint32_t stage_receivers = 0, stage_points = 0;
     FrameParams last{};
     bool has_frame = false;
+    // Learned-cache form (lux_view_set_cache).
+    LuxCacheMode cache{};
+    CacheDevice cdev{};
+    bool cache_alloc = false;
 };
+
+static void cache_buffers_free(LuxView *v) {
+    CacheDevice &C = v->cdev;
+    void *ptrs[] = {C.flags, C.queries, C.query_ray, C.pred, C.train, C.target, C.cell_error, C.global_error,
+                    C.fb_key, C.fb_expiry, C.counters};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    C = CacheDevice{};
+    v->cache_alloc = false;
+}
 
 static lux_status view_alloc(LuxView *v) {
     LuxContext *ctx = v->ctx;
@@ -1224,8 +1485,74 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
         if (p) cudaFree(p);
     for (int i = 0; i < kTimingEvents; ++i)
         if (v->ev[i]) cudaEventDestroy(v->ev[i]);
+    cache_buffers_free(v);
     delete v;
     return LUX_OK;
+}
+
+extern "C" lux_status lux_view_set_cache(LuxView *v, const LuxCacheMode *mode) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = v->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (!mode || !mode->cache) {
+        cache_buffers_free(v);
+        v->cache = LuxCacheMode{};
+        return LUX_OK;
+    }
+    LuxCacheMode m = *mode;
+    if (lux_cache_context(m.cache) != ctx)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "set_cache: the cache belongs to another context");
+    if (m.cutoff_level < 1 || m.cutoff_level >= LUX_MAX_LEVELS || m.validate_period < 1 || m.train_samples < 128 ||
+        m.train_samples > (1u << 22) || !(m.error_bound > 0.0f) || m.fallback_frames < 1)
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "set_cache: mode out of range");
+    cache_buffers_free(v);
+    CacheDevice &C = v->cdev;
+    size_t rays = v->desc.max_rays, cells = v->desc.max_cells;
+    bool ok = cudaMalloc((void **)&C.flags, rays) == cudaSuccess &&
+              cudaMalloc((void **)&C.queries, rays * sizeof(LuxCacheSample)) == cudaSuccess &&
+              cudaMalloc((void **)&C.query_ray, rays * 4) == cudaSuccess &&
+              cudaMalloc((void **)&C.pred, rays * sizeof(float4)) == cudaSuccess &&
+              cudaMalloc((void **)&C.train, (size_t)m.train_samples * sizeof(LuxCacheSample)) == cudaSuccess &&
+              cudaMalloc((void **)&C.target, (size_t)m.train_samples * sizeof(float4)) == cudaSuccess &&
+              cudaMalloc((void **)&C.cell_error, cells * sizeof(float4)) == cudaSuccess &&
+              cudaMalloc((void **)&C.global_error, 16) == cudaSuccess &&
+              cudaMalloc((void **)&C.fb_key, (size_t)kFallbackSlots * 8) == cudaSuccess &&
+              cudaMalloc((void **)&C.fb_expiry, (size_t)kFallbackSlots * 4) == cudaSuccess &&
+              cudaMalloc((void **)&C.counters, kCntCount * 4) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        cache_buffers_free(v);
+        return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "set_cache: device allocation failed");
+    }
+    cudaMemset(C.cell_error, 0, cells * sizeof(float4));
+    cudaMemset(C.fb_key, 0xff, (size_t)kFallbackSlots * 8);
+    cudaMemset(C.fb_expiry, 0, (size_t)kFallbackSlots * 4);
+    cudaMemset(C.counters, 0, kCntCount * 4);
+    v->cache_alloc = true;
+    v->cache = m;
+    return lux_cuda_check(ctx, (int)cudaDeviceSynchronize(), "set_cache");
+}
+
+extern "C" lux_status lux_view_cache_stats(LuxView *v, LuxCacheFrameStats *out) {
+    if (!v || !out) return LUX_ERR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof *out);
+    if (!v->cache_alloc) return LUX_OK;
+    lux_status rc = lux_cuda_check(v->ctx, (int)cudaStreamSynchronize(v->ctx->stream), "cache stats");
+    if (rc != LUX_OK) return rc;
+    uint32_t c[kCntCount];
+    float g[2];
+    cudaMemcpy(c, v->cdev.counters, sizeof c, cudaMemcpyDeviceToHost);
+    cudaMemcpy(g, v->cdev.global_error, sizeof g, cudaMemcpyDeviceToHost);
+    out->validated_bias = g[1] > 0.0f ? g[0] / g[1] : 0.0f;
+    out->cached_rays = c[kCntCached];
+    out->validated_rays = c[kCntValidated];
+    out->train_candidates = c[kCntCandidates];
+    out->trained_samples = std::min(c[kCntTrain], v->cache.train_samples);
+    out->validated_cells = c[kCntValidatedCells];
+    out->failed_cells = c[kCntFailedCells];
+    out->fallback_rays = c[kCntFallbackRays];
+    return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "cache stats copy");
 }
 
 static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32_t receivers, FrameParams &F) {
@@ -1327,7 +1654,22 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
                 sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
                 Dr.ray_order = D.sort_perm;
             }
-            if (T.closest_mode == 1)
+            const bool cached = v->cache_alloc && v->cache.cutoff_level < F.levels;
+            CacheDevice C = v->cdev;
+            if (cached) {
+                C.cutoff = v->cache.cutoff_level;
+                C.period = v->cache.validate_period;
+                C.frame = F.shade.frame;
+                C.fallback_frames = v->cache.fallback_frames;
+                C.train_cap = v->cache.train_samples;
+                C.near_limit = nextafterf(F.end[C.cutoff - 1u], INFINITY);
+                C.far_t = F.end[C.cutoff];
+                C.bound = v->cache.error_bound;
+                cudaMemsetAsync(C.counters, 0, kCntCount * 4, st);
+                cudaMemsetAsync(C.global_error, 0, 8, st);
+                closest_cache_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(D, F, scene->view, pos,
+                                                                                             nrm, rays, C);
+            } else if (T.closest_mode == 1)
                 closest_split_refill_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
                     Dr, F, scene->view, pos, nrm, rays);
             else
@@ -1347,7 +1689,24 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
                 shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             else
                 shadow_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
+            if (cached) {
+                const int g = ctx->sm_count * 8;
+                cache_queries_kernel<<<g, 256, 0, st>>>(D, nrm, rays, F.rays_per_receiver, C);
+                lux_status qrc = lux_cache_query_device_count(v->cache.cache, C.queries, C.counters + kCntQueries, rays,
+                                                              (float *)C.pred);
+                if (qrc != LUX_OK) return qrc;
+                cache_apply_kernel<<<g, 256, 0, st>>>(D, F, rays, C);
+            }
             deposit_split_kernel<<<(rays + 127) / 128, 128, 0, st>>>(D, F, nrm, rays);
+            if (cached) {
+                const int g = ctx->sm_count * 8;
+                cache_count_kernel<<<g, 256, 0, st>>>(D, F, rays, C);
+                cudaMemsetAsync(C.train, 0, (size_t)C.train_cap * sizeof(LuxCacheSample), st);
+                cache_select_kernel<<<g, 256, 0, st>>>(D, F, nrm, rays, C);
+                lux_status trc = lux_cache_train(v->cache.cache, C.train, (const float *)C.target, C.train_cap);
+                if (trc != LUX_OK) return trc;
+                cache_fallback_kernel<<<g, 256, 0, st>>>(D, F, C);
+            }
         }
     } else {
         for (uint32_t l = 0; l < F.levels; ++l)

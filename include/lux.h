@@ -381,6 +381,103 @@ lux_status lux_reference_irradiance(LuxContext *ctx, const LuxScene *scene, cons
 lux_status lux_error_stats(LuxContext *ctx, const float *estimate, const double *reference, uint32_t count,
                            double out[4]);
 
+/* ---- learned radiance cache ------------------------------------------------
+ * No reference counterpart (the reference's README defers neural caching).
+ * A multiresolution hash encoding (levels x 2 BF16 features, 2^log2_table
+ * entries per level, base resolution x growth^level over the scene box)
+ * feeding a fused MLP: 64 inputs (32 hash features, 16 spherical-harmonic
+ * coefficients of the direction, normal, albedo, a constant 1, zeros), 4
+ * hidden layers of 64 ReLU units, 3 linear outputs; BF16
+ * weights and FP32 accumulation on the 5th-generation tensor cores
+ * (tcgen05.mma with TMEM accumulators) for the forward pass and the
+ * backward data gradients; Adam (FP32 master copies) for the table and the
+ * weights.  Loss: relative L2, (y - t)^2 / (y^2 + 0.01).  Trained online on
+ * interval radiance samples the transport produces and queried for the
+ * radiance arriving at a point from a direction. */
+typedef struct LuxCache LuxCache;
+typedef struct LuxCacheDesc {
+    uint32_t levels;          /* 16 */
+    uint32_t log2_table;      /* 19 */
+    uint32_t base_resolution; /* 16 */
+    float growth;             /* 1.5 */
+    float learning_rate;      /* 1e-3 */
+    uint32_t batch;           /* samples per Adam step: 16384 */
+    uint32_t seed;
+    uint32_t reserved;
+} LuxCacheDesc;
+/* One training sample or query: the radiance arriving at `position` from
+ * `direction` (unit; the ray's direction), at a receiver with `normal` and
+ * `albedo`; radiance = target (samples) and weight (0 = ignore). 64 bytes. */
+typedef struct LuxCacheSample {
+    float position[3];
+    float weight;
+    float direction[3];
+    float pad0;
+    float normal[3];
+    float pad1;
+    float albedo[3];
+    float pad2;
+} LuxCacheSample;
+typedef struct LuxCacheStats {
+    uint64_t steps;           /* Adam steps taken */
+    uint64_t samples;         /* training samples consumed */
+    float last_loss;          /* mean relative L2 loss of the last step */
+    uint32_t error_flags;     /* 1: a tensor-core wait gave up */
+} LuxCacheStats;
+void lux_cache_desc_default(LuxCacheDesc *desc);
+lux_status lux_cache_create(LuxContext *ctx, const LuxCacheDesc *desc, LuxCache **out);
+lux_status lux_cache_destroy(LuxCache *cache);
+/* Scene box the hash grid covers (positions outside are clamped). */
+lux_status lux_cache_set_bounds(LuxCache *cache, const float lo[3], const float hi[3]);
+/* Trains on `count` device samples with device targets rgb (float4 per
+ * sample, .w unused): ceil(count / batch) Adam steps in order. */
+lux_status lux_cache_train(LuxCache *cache, const LuxCacheSample *samples, const float *targets, uint32_t count);
+/* Predicts radiance (device float4 per query: rgb >= 0, w = 1). */
+lux_status lux_cache_query(LuxCache *cache, const LuxCacheSample *queries, uint32_t count, float *out);
+lux_status lux_cache_stats(LuxCache *cache, LuxCacheStats *out);
+/* Tests: the 64-wide BF16 input encoding of `count` device samples
+ * (device uint16 bf16 bits [count][64]), the MLP weights as FP32
+ * (host float[64*64*4 + 16*64], layer-major, each [out][in]), and the raw
+ * MLP output of given encodings (device float4 per row; no clamping). */
+lux_status lux_cache_encode(LuxCache *cache, const LuxCacheSample *samples, uint32_t count, uint16_t *out);
+lux_status lux_cache_read_weights(LuxCache *cache, float *out);
+lux_status lux_cache_forward(LuxCache *cache, const uint16_t *encoded, uint32_t count, float *out);
+
+/* Learned-cache form of a view's Split frame (no reference counterpart).
+ * Interval rays of cascade-0 cells that are neither validated this frame nor
+ * falling back trace only up to the end of level cutoff_level - 1; a ray
+ * that meets nothing there takes the cache's radiance for its (origin,
+ * direction) as its hit radiance at level cutoff_level, so the levels from
+ * cutoff_level on are answered by the cache instead of traced.  Each frame
+ * 1/validate_period of the cascade-0 cells (rotating) trace fully; their
+ * rays past the cutoff are compared with the cache and a cell whose bias
+ * |sum cache - sum traced| exceeds error_bound x its summed traced radiance
+ * plus three standard deviations of that sum (single traced rays carry
+ * next-event noise) traces fully for the next fallback_frames frames.  Up to train_samples rays per frame
+ * (validated rays and rays that hit within cascade 1) train the cache, one
+ * lux_cache_train inside the frame.  mode NULL or mode->cache NULL: plain. */
+typedef struct LuxCacheMode {
+    LuxCache *cache;
+    uint32_t cutoff_level;     /* 3 */
+    uint32_t validate_period;  /* 16 */
+    float error_bound;         /* 0.25 */
+    uint32_t train_samples;    /* 65536 */
+    uint32_t fallback_frames;  /* 32 */
+    uint32_t reserved[3];
+} LuxCacheMode;
+typedef struct LuxCacheFrameStats {
+    uint64_t cached_rays;      /* rays answered by the cache */
+    uint64_t validated_rays;   /* fully traced rays past the cutoff compared with the cache */
+    uint64_t train_candidates; /* rays eligible as training samples */
+    uint64_t trained_samples;  /* samples given to lux_cache_train */
+    uint32_t validated_cells;
+    uint32_t failed_cells;     /* cells sent to fallback this frame */
+    uint32_t fallback_rays;    /* rays traced fully because their cell falls back */
+    float validated_bias;      /* (sum cache - sum traced) / sum traced over the validated rays */
+} LuxCacheFrameStats;
+lux_status lux_view_set_cache(LuxView *view, const LuxCacheMode *mode);
+lux_status lux_view_cache_stats(LuxView *view, LuxCacheFrameStats *out);
+
 /* ---- batching: many scenes and views in one launch per trace stage -------
  * No reference counterpart (the reference renders one view per dispatch
  * sequence).  One lux_batch_trace_merge runs the Split frame of every job:
