@@ -37,6 +37,8 @@ RAYS_PER_RECEIVER = 36
 EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
 REFERENCE_SPP = 1024
+LEARNED_CUTOFF = 2
+LEARNED_WARMUP = 200
 LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
 
 
@@ -127,7 +129,7 @@ def build_workload(device: int = 0, host_only: bool = False):
                                                max_entries=entries,
                                                max_rays=len(rpos) * settings.rays_per_receiver)
     return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, rpos=rpos,
-                rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, setup_s=time.time() - t0)
+                rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, cells_max=cells_max, setup_s=time.time() - t0)
 
 
 class ClockSampler:
@@ -251,6 +253,66 @@ def workload_config(w):
             "records": int(w["entries"]), "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps"}
 
 
+def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref, plain_ms,
+                plain_error, interval_rays, device):
+    """The learned-cache form of the same frame: levels from LEARNED_CUTOFF on
+    answered by the hash-grid MLP cache (trained online inside each frame),
+    1/16 of the cascade-0 cells validated per frame with per-cell fallback.
+    The cache warms up for LEARNED_WARMUP untimed frames first."""
+    import torch
+
+    bp, ctx, scene, settings = w["bp"], w["ctx"], w["scene"], w["settings"]
+    n_recv, n_pts = len(w["rpos"]), len(w["ppos"])
+    lview = bp.SplitView(ctx, max_receivers=n_recv, max_cells=int(w["cells_max"]),
+                         max_entries=int(w["entries"]), max_rays=n_recv * settings.rays_per_receiver)
+    cache = bp.LearnedCache(ctx)
+    lo = w["rpos"][:, :3].min(0) - 1.0
+    hi = w["rpos"][:, :3].max(0) + 1.0
+    cache.set_bounds(lo, hi)
+    lview.set_cache(cache, cutoff_level=LEARNED_CUTOFF, validate_period=16, error_bound=4.0, train_samples=65536,
+                    fallback_frames=16)
+    lview.set_timing(True)
+
+    def frame(step):
+        settings.frame_index = step
+        lview.trace_merge(scene, settings, d_rpos.data_ptr(), d_rnrm.data_ptr(), n_recv)
+
+    for step in range(LEARNED_WARMUP):
+        frame(step)
+    torch.cuda.synchronize(device)
+    ms = []
+    for step in range(args.steps):
+        flush.fill_(float(step))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        frame(LEARNED_WARMUP + step)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+        ms.append(start.elapsed_time(end))
+    learned_ms = float(np.sum(ms)) / args.steps
+    cs = lview.cache_stats()
+    st = lview.stats()
+    if st.error_flags or cache.stats().error_flags:
+        raise RuntimeError("learned-cache frame reported an error")
+    lview.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
+    s_est = d_out[sub].contiguous()
+    err = bp.error_stats(ctx, s_est.data_ptr(), s_ref.data_ptr(), len(sub))
+    return {
+        "ms_per_step": learned_ms, "value": interval_rays / (learned_ms * 1e-3) / 1e6, "unit": "Mrays/s",
+        "speedup_vs_plain": plain_ms / learned_ms,
+        "relative_rmse": err["relative_rmse"], "plain_relative_rmse": plain_error["relative_rmse"],
+        "rmse_change": err["relative_rmse"] / plain_error["relative_rmse"] - 1.0,
+        "rays": {"cached": int(cs.cached_rays), "fallback": int(cs.fallback_rays),
+                 "validated": int(cs.validated_rays), "trained_samples": int(cs.trained_samples),
+                 "failed_cells": int(cs.failed_cells), "validated_cells": int(cs.validated_cells),
+                 "validated_bias": float(cs.validated_bias)},
+        "cache": {"levels": 16, "table": "2^19 x 2 BF16 per level", "base_resolution": 16, "growth": 1.5,
+                  "mlp": "64 -> 4 x 64 ReLU -> 3, BF16 tcgen05", "learning_rate": 1e-3, "batch": 16384,
+                  "samples_per_frame": 65536, "cutoff_level": LEARNED_CUTOFF, "validate_period": 16,
+                  "error_bound": 4.0, "fallback_frames": 16, "warmup_frames": LEARNED_WARMUP},
+    }
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -360,6 +422,9 @@ def run_ours(args, rank, world):
     error.update({"spp": REFERENCE_SPP, "sample": f"every 97th resolve point ({len(sub)})",
                   "reference_s": ref_s, "oracle": "FP64-accumulated path-traced interval radiance"})
 
+    learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref,
+                          ms_per_step, error, interval_rays, device)
+
     if rank == 0:
         peak, peak_kind = measured_peaks()
         lay = scene.layout()
@@ -396,6 +461,7 @@ def run_ours(args, rank, world):
                     "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
                     "d2h_bytes_per_step": int(n_pts * 16)},
             "error_vs_fp64": error,
+            "learned": learned,
             "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
