@@ -313,6 +313,22 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     }
 
 
+def max_over_ranks(value, dist, device):
+    """Replicas: the job's time is the slowest rank's (a MAX all-reduce;
+    the identity without a process group)."""
+    if not dist:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mrays(world, rays_per_rank, steps, total_ms):
+    """Whole-job throughput: every rank traces its own replica of the frame."""
+    return world * rays_per_rank * steps / (total_ms * 1e-3) / 1e6
+
+
 def run_ours(args, rank, world):
     import torch
 
@@ -378,13 +394,9 @@ def run_ours(args, rank, world):
             resolve_ms.append(view.timings().resolve_ms)
     torch.cuda.synchronize(device)
     st = view.stats()
-    total_ms = float(np.sum(step_ms))
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(step_ms)), dist, dev)
     ms_per_step = total_ms / args.steps
-    value = world * interval_rays * args.steps / (total_ms * 1e-3) / 1e6
+    value = job_mrays(world, interval_rays, args.steps, total_ms)
 
     # e2e: host buffers through lux_view_frame_host (copies + trace/merge + resolve).
     pin = lambda a: torch.from_numpy(a).pin_memory().numpy()
@@ -400,12 +412,8 @@ def run_ours(args, rank, world):
         dt = (time.perf_counter() - t0) * 1e3
         if step >= args.warmup:
             e2e_ms.append(dt)
-    e2e_total = float(np.sum(e2e_ms))
-    if dist:
-        t = torch.tensor([e2e_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * interval_rays * args.steps / (e2e_total * 1e-3) / 1e6
+    e2e_total = max_over_ranks(float(np.sum(e2e_ms)), dist, dev)
+    e2e_value = job_mrays(world, interval_rays, args.steps, e2e_total)
 
     # FP32 error of the resolved irradiance against the FP64 path-traced
     # reference on every 97th resolve point (not timed).
