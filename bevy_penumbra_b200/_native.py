@@ -94,7 +94,7 @@ class LuxTimings(C.Structure):
 class LuxTuning(C.Structure):
     _fields_ = [("closest_mode", C.c_uint32), ("shadow_mode", C.c_uint32), ("closest_blocks_per_sm", C.c_uint32),
                 ("shadow_blocks_per_sm", C.c_uint32), ("sort_queries", C.c_uint32), ("sort_rays", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("stack_depth", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class LuxCacheDesc(C.Structure):

@@ -14,7 +14,7 @@
 namespace lux {
 
 constexpr uint32_t kMaxSteps = 4096u;  // MAX_TRAVERSAL_STEPS, shaders/traversal.slang:8
-constexpr int kStack = 64;
+constexpr int kStack = 64;  // default traversal stack depth (entries)
 
 struct Hit {
     float t;
@@ -285,7 +285,7 @@ __device__ __forceinline__ float key_entry(uint32_t key) { return as_float(key &
 // (per TLAS walk and per instance walk), 2 / 1 when the stack is exhausted in
 // the TLAS / a BLAS, after which the walk continues over every instance / every
 // triangle of the instance in order (shaders/traversal.slang:498-517, :729-745).
-template <bool kAnyHit>
+template <bool kAnyHit, int kDepth = kStack>
 struct Walker {
     Hit hit;
     f3 o, d, lo, ld;
@@ -298,7 +298,7 @@ struct Walker {
     uint32_t tlas_next;   // TLAS fallback: next instance to scan in order
     uint32_t blas_next;   // BLAS fallback: next triangle to scan in order
     uint32_t tlas_steps, blas_steps;
-    int sp;  // depth of the caller's stack: kStack entries of (payload, entry distance bits)
+    int sp;  // depth of the caller's stack: kDepth entries of (payload, entry distance bits)
     uint32_t cur;
     float cur_t;
     bool have;
@@ -376,7 +376,7 @@ struct Walker {
             key_swap(k1, k3);
             key_swap(k1, k2);
             int n = __popc(mask);
-            if (sp + n - 1 > kStack) {
+            if (sp + n - 1 > kDepth) {
                 if (in_tlas) {
                     hit.errors |= 2u;
                     sp = 0;
@@ -402,7 +402,7 @@ struct Walker {
             if (blas_base < 0) {
                 // TLAS leaf: enter its first instance; the rest waits on the stack.
                 if (count > 1u) {
-                    if (sp < kStack) {
+                    if (sp < kDepth) {
                         stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
                                                  as_uint(cur_t));
                     } else {
@@ -513,10 +513,13 @@ struct Walker {
     }
 };
 
-template <bool kAnyHit>
+// Closest hit (kAnyHit = false) or any hit of one ray.  kDepth is the stack
+// depth: a shallower stack uses less local memory per thread, and a walk that
+// overflows it continues with the reference's ordered scan (same answers).
+template <bool kAnyHit, int kDepth = kStack>
 __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, Hit &hit, TraceCounters &cn) {
-    Walker<kAnyHit> w;
-    uint2 stack[kStack];
+    Walker<kAnyHit, kDepth> w;
+    uint2 stack[kDepth];
     if (w.start(S, o, d, tmin, limit))
         while (!w.step(S, stack, cn)) {
         }

@@ -353,6 +353,7 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
 // One Split interval ray (traceTransport, shaders/split.slang:1122-1163):
 // receiver i = ray / R, sample k = ray % R, from the biased receiver position
 // to 1e20; the hit is stored for shading.
+template <int kDepth = lux::kStack>
 __device__ __forceinline__ void closest_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
                                                   const SceneView &S, const float4 *__restrict__ pos,
                                                   const float4 *__restrict__ nrm, uint32_t slot,
@@ -366,7 +367,7 @@ __device__ __forceinline__ void closest_split_ray(const ViewDevice &V, const Fra
     split_direction(F, frame, i, k, n, dir, u, v);
     f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
     lux::Hit hit;
-    lux::trace<false>(S, origin, dir, 0.0f, 1e20f, hit, cn);
+    lux::trace<false, kDepth>(S, origin, dir, 0.0f, 1e20f, hit, cn);
     store_ray(V, ray, origin, dir, hit);
 }
 
@@ -377,6 +378,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter) {
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
+template <int kDepth>
 __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                             const float4 *__restrict__ pos,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
@@ -388,7 +390,7 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_ker
         if (base >= ray_count) break;
         uint32_t slot = base + (threadIdx.x & 31u);
         if (slot < ray_count) {
-            closest_split_ray(V, F, F.shade.frame, S, pos, nrm, slot, cn);
+            closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn);
             st[kStatInterval] += 1;
         }
     }
@@ -586,15 +588,17 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
 
 // One visibility query (traceVisibility, shaders/split.slang:1326-1339):
 // result 0 visible, 1 blocked, 2 unsupported.
+template <int kDepth = lux::kStack>
 __device__ __forceinline__ void shadow_query(const ViewDevice &V, const SceneView &S, uint32_t i,
                                              lux::TraceCounters &cn) {
     uint32_t qi = V.query_order ? V.query_order[i] : i;
     float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
     lux::Hit sh;
-    lux::trace<true>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
+    lux::trace<true, kDepth>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
     V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
 }
 
+template <int kDepth>
 __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
@@ -605,7 +609,7 @@ __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(View
         if (base >= n) break;
         uint32_t i = base + (threadIdx.x & 31u);
         if (i < n) {
-            shadow_query(V, S, i, cn);
+            shadow_query<kDepth>(V, S, i, cn);
             st[kStatShadow] += 1;
         }
     }
@@ -1374,7 +1378,7 @@ constexpr int kTimingEvents = 7;
 
 struct LuxView {
     LuxContext *ctx = nullptr;
-    LuxTuning tuning{0, 0, 16, 16, 0, 0, {0, 0}};
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0};
     bool timing = false;
     cudaEvent_t ev[kTimingEvents] = {};
     LuxViewDesc desc{};
@@ -1672,9 +1676,12 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
             } else if (T.closest_mode == 1)
                 closest_split_refill_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
                     Dr, F, scene->view, pos, nrm, rays);
+            else if (T.stack_depth == 32)
+                closest_split_kernel<32><<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
+                    Dr, F, scene->view, pos, nrm, rays);
             else
-                closest_split_kernel<<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(Dr, F, scene->view,
-                                                                                             pos, nrm, rays);
+                closest_split_kernel<64><<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
+                    Dr, F, scene->view, pos, nrm, rays);
             ViewDevice Dq = D;  // query pass view: keys written by shade, optional order
             if (!T.sort_queries) Dq.sort_keys = nullptr;
             shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(Dq, F, scene->view, rays, false);
@@ -1687,8 +1694,10 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
             }
             if (T.shadow_mode == 1)
                 shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
+            else if (T.stack_depth == 32)
+                shadow_kernel<32><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             else
-                shadow_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
+                shadow_kernel<64><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             if (cached) {
                 const int g = ctx->sm_count * 8;
                 cache_queries_kernel<<<g, 256, 0, st>>>(D, nrm, rays, F.rays_per_receiver, C);
@@ -1712,7 +1721,7 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
         for (uint32_t l = 0; l < F.levels; ++l)
             closest_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
         shade_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, F.ray_capacity, true);
-        shadow_kernel<<<ctx->sm_count * v->tuning.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
+        shadow_kernel<64><<<ctx->sm_count * v->tuning.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
         deposit_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F);
     }
     mark(2);
@@ -1888,7 +1897,8 @@ extern "C" lux_status lux_view_timings(LuxView *v, LuxTimings *out) {
 extern "C" lux_status lux_view_set_tuning(LuxView *v, const LuxTuning *t) {
     if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
     if (t->closest_mode > 1 || t->shadow_mode > 1 || t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 ||
-        t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64 || t->sort_queries > 1 || t->sort_rays > 1)
+        t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64 || t->sort_queries > 1 || t->sort_rays > 1 ||
+        (t->stack_depth != 0 && t->stack_depth != 32 && t->stack_depth != 64))
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_tuning: value out of range");
     v->tuning = *t;
     return LUX_OK;
@@ -1971,7 +1981,7 @@ lux_status launch_interval_radiance(LuxContext *ctx, const LuxScene *scene, cons
     if (count) {
         closest_rays_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(V, scene->view, rays, count);
         shade_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, F, scene->view, count, false);
-        shadow_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(V, F, scene->view);
+        shadow_kernel<64><<<ctx->sm_count * 16, 128, 0, st>>>(V, F, scene->view);
         radiance_out_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, count, (float4 *)out);
     }
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "interval_radiance launch");
@@ -2088,7 +2098,7 @@ extern "C" lux_status lux_view_read_hits(LuxView *v, LuxHit *out, uint32_t count
 
 struct LuxBatch {
     LuxContext *ctx = nullptr;
-    LuxTuning tuning{0, 0, 16, 16, 0, 0, {0, 0}};
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0};
     bool use_graph = true;
     // Configuration the device tables and graph were built for.
     std::vector<LuxBatchJob> jobs;

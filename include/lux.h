@@ -339,7 +339,9 @@ typedef struct LuxTuning {
     uint32_t shadow_blocks_per_sm;
     uint32_t sort_queries;        /* 1: order visibility queries by (emitter, origin cell) before tracing */
     uint32_t sort_rays;           /* 1: order interval rays by (direction bin, origin cell) before tracing */
-    uint32_t reserved[2];
+    uint32_t stack_depth;         /* traversal stack entries per thread: 32 or 64 (0 = 64); an overflowing
+                                     walk continues with the reference's ordered scan, same answers */
+    uint32_t reserved;
 } LuxTuning;
 lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
 lux_status lux_view_get_tuning(const LuxView *view, LuxTuning *tuning);

@@ -113,13 +113,14 @@ def cornell_floor_receivers(n=32):
     return pos, nrm
 
 
-@pytest.mark.parametrize("rays,sort", [(1, 0), (8, 0), (8, 1)])
-def test_split_cornell_frame_matches_oracle(rays, sort):
+@pytest.mark.parametrize("rays,sort,depth", [(1, 0, 64), (8, 0, 64), (8, 1, 64), (8, 1, 32)])
+def test_split_cornell_frame_matches_oracle(rays, sort, depth):
     settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=rays,
                                    frame_index=3).sanitized()
     pos, nrm = cornell_floor_receivers()
     ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm,
-                                                              tuning=dict(sort_rays=sort, sort_queries=sort))
+                                                              tuning=dict(sort_rays=sort, sort_queries=sort,
+                                                                          stack_depth=depth))
     ofr = oracle_frame("cornell", settings, pos, nrm)
     ost = ofr.stats()
     assert st.interval_rays == len(pos) * rays
