@@ -37,6 +37,12 @@ RAYS_PER_RECEIVER = 36
 EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
 REFERENCE_SPP = 1024
+# DRAM bytes per ray of the traversal kernels from one ncu capture of the
+# small atrium case (profiles/closest_split_kernel_shadow_kernel_atrium65536_640x360.md:
+# dram read + write per launch / rays of that launch); the full frame's traffic
+# is scaled from it by its ray counts.
+DRAM_BYTES_PER_INTERVAL_RAY = (3.781632e6 + 0.268544e6) / 421344
+DRAM_BYTES_PER_SHADOW_RAY = (42.74688e6 + 0.385536e6) / 1236328
 LEARNED_CUTOFF = 2
 LEARNED_WARMUP = 200
 LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
@@ -459,8 +465,13 @@ def run_ours(args, rank, world):
                          "instances": int(st.shadow_instances) / max(int(st.shadow_rays), 1)},
                      "trace_mrays_s": interval_rays / trace_s / 1e6,
                      "all_rays_trace_mrays_s": (interval_rays + int(st.shadow_rays)) / trace_s / 1e6},
-            "roofline": {"kernel": "trace_split_kernel", "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "roofline": {"kernel": "trace stage (closest_split_kernel, shade, shadow_kernel, deposit)", "bound": "hbm",
+                         "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_INTERVAL_RAY * interval_rays
+                         + DRAM_BYTES_PER_SHADOW_RAY * int(st.shadow_rays),
+                         "traffic_note": "ncu dram bytes of the traversal kernels per frame, scaled by rays from "
+                                         "the 65,536-triangle capture; the scene stays in L2",
                          "algorithmic_bytes": alg_bytes},
             "cpu_baseline": {"value": cpu_rays / cpu_dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
                              "kind": "port",
