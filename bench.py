@@ -43,7 +43,7 @@ REFERENCE_SPP = 1024
 # is scaled from it by its ray counts.
 DRAM_BYTES_PER_INTERVAL_RAY = (3.781632e6 + 0.268544e6) / 421344
 DRAM_BYTES_PER_SHADOW_RAY = (42.74688e6 + 0.385536e6) / 1236328
-LEARNED_CUTOFF = 2
+LEARNED_CUTOFF = 1
 LEARNED_WARMUP = 200
 LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
 
@@ -261,7 +261,7 @@ def workload_config(w):
 
 def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref, plain_ms,
                 plain_error, interval_rays, device):
-    """The learned-cache form of the same frame: levels from LEARNED_CUTOFF on
+    """The learned-cache form of the same frame: levels from the cutoff on
     answered by the hash-grid MLP cache (trained online inside each frame),
     1/16 of the cascade-0 cells validated per frame with per-cell fallback.
     The cache warms up for LEARNED_WARMUP untimed frames first."""
@@ -275,7 +275,8 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     lo = w["rpos"][:, :3].min(0) - 1.0
     hi = w["rpos"][:, :3].max(0) + 1.0
     cache.set_bounds(lo, hi)
-    lview.set_cache(cache, cutoff_level=LEARNED_CUTOFF, validate_period=16, error_bound=4.0, train_samples=65536,
+    lview.set_cache(cache, cutoff_level=args.cache_cutoff, validate_period=16, error_bound=args.cache_bound,
+                    train_samples=65536,
                     fallback_frames=16)
     lview.set_timing(True)
 
@@ -314,8 +315,8 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
                  "validated_bias": float(cs.validated_bias)},
         "cache": {"levels": 16, "table": "2^19 x 2 BF16 per level", "base_resolution": 16, "growth": 1.5,
                   "mlp": "64 -> 4 x 64 ReLU -> 3, BF16 tcgen05", "learning_rate": 1e-3, "batch": 16384,
-                  "samples_per_frame": 65536, "cutoff_level": LEARNED_CUTOFF, "validate_period": 16,
-                  "error_bound": 4.0, "fallback_frames": 16, "warmup_frames": LEARNED_WARMUP},
+                  "samples_per_frame": 65536, "cutoff_level": args.cache_cutoff, "validate_period": 16,
+                  "error_bound": args.cache_bound, "fallback_frames": 16, "warmup_frames": LEARNED_WARMUP},
     }
 
 
@@ -635,6 +636,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="atrium", choices=["atrium", "batched"],
                     help="atrium: the headline frame; batched: 64 scenes per step through lux_batch_trace_merge")
+    ap.add_argument("--cache-cutoff", type=int, default=LEARNED_CUTOFF,
+                    help="learned-cache form: first cascade answered by the cache")
+    ap.add_argument("--cache-bound", type=float, default=8.0,
+                    help="learned-cache form: relative bias above which a validated cell falls back")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 65,536-triangle atrium at 640x360 (not a benchmark line)")
     args = ap.parse_args()

@@ -87,12 +87,15 @@ class RadianceCascades:
     layout: int = LAYOUT_SPLIT
     rays_per_receiver: int = 1
     frame_index: int = 0
+    temporal_blend: float = 0.88
+    split_transmittance_blend: float = 0.98
+    history_frames: int = 24
 
     @staticmethod
     def low_end() -> "RadianceCascades":
         """RadianceCascades::low_end() (src/lib.rs:700-722), the fields this path reads."""
         return RadianceCascades(probe_spacing=1.0, interval_length=1.6, emissive_samples=4,
-                                sampling=SamplingSettings.low_end())
+                                sampling=SamplingSettings.low_end(), temporal_blend=0.95)
 
     def to_c(self) -> N.LuxSettings:
         s = N.LuxSettings()
@@ -113,6 +116,9 @@ class RadianceCascades:
         s.rays_per_receiver = _u32(self.rays_per_receiver)
         s.frame_index = _u32(self.frame_index)
         s.resolve_scale = _u32(self.sampling.resolve_scale)
+        s.temporal_blend = self.temporal_blend
+        s.transmittance_blend = self.split_transmittance_blend
+        s.history_frames = _u32(self.history_frames)
         return s
 
     @staticmethod
@@ -123,7 +129,9 @@ class RadianceCascades:
             intensity=s.intensity, environment=tuple(s.environment), emissive_samples=int(s.emissive_samples),
             sampling=sampling, exposure=s.exposure, levels=int(s.levels), base_columns=int(s.base_columns),
             base_rows=int(s.base_rows), interval_ratio=s.interval_ratio, interval_rule=int(s.interval_rule),
-            layout=int(s.layout), rays_per_receiver=int(s.rays_per_receiver), frame_index=int(s.frame_index))
+            layout=int(s.layout), rays_per_receiver=int(s.rays_per_receiver), frame_index=int(s.frame_index),
+            temporal_blend=s.temporal_blend, split_transmittance_blend=s.transmittance_blend,
+            history_frames=int(s.history_frames))
 
     def sanitized(self) -> "RadianceCascades":
         """RadianceCascades::sanitized() (src/lib.rs:731-759), evaluated by liblux."""
@@ -475,6 +483,16 @@ class SplitView:
         out = N.LuxCacheFrameStats()
         self.ctx.check(lib().lux_view_cache_stats(self.handle, C.byref(out)))
         return out
+
+    def reset_history(self) -> None:
+        """lux_view_reset_history: the next frame starts without history."""
+        self.ctx.check(lib().lux_view_reset_history(self.handle))
+
+    def invalidate_bounds(self, lo, hi) -> None:
+        """lux_view_invalidate_bounds: records near this box take no history next frame."""
+        lo = np.asarray(lo, np.float32)
+        hi = np.asarray(hi, np.float32)
+        self.ctx.check(lib().lux_view_invalidate_bounds(self.handle, _ptr(lo), _ptr(hi)))
 
     def read_hits(self, count: int) -> np.ndarray:
         """lux_view_read_hits: the last Split frame's first `count` interval-ray hits."""

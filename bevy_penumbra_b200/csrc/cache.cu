@@ -265,7 +265,10 @@ __global__ void encode_kernel(GridParams G, const LuxCacheSample *__restrict__ s
     float v[kIn];
 #pragma unroll
     for (int k = 0; k < kIn; ++k) v[k] = 0.0f;
-    for (uint32_t level = 0; level < G.levels; ++level) {
+    // Unrolled over the maximum level count so v[] stays in registers.
+#pragma unroll
+    for (uint32_t level = 0; level < (uint32_t)kLevelsMax; ++level) {
+        if (level >= G.levels) break;
         Corner c;
         level_corners(G, level, u, c);
         float f0 = 0.0f, f1 = 0.0f;
@@ -602,6 +605,32 @@ __global__ void adam_kernel(AdamParams P, float *__restrict__ param, float *__re
     }
 }
 
+// adam_kernel on four consecutive parameters per thread (the hash table:
+// n is a multiple of 4), with the BF16 copy written as one 8-byte store.
+__global__ void adam4_kernel(AdamParams P, float4 *__restrict__ param, float4 *__restrict__ grad,
+                             float4 *__restrict__ m, float4 *__restrict__ v, size_t n4, uint2 *__restrict__ out) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
+        float4 g = grad[i], mi = m[i];
+        if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f && mi.x == 0.0f && mi.y == 0.0f &&
+            mi.z == 0.0f && mi.w == 0.0f)
+            continue;  // never touched: nothing to move
+        grad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float4 vi = v[i], p = param[i];
+        float gs[4] = {g.x, g.y, g.z, g.w}, ms[4] = {mi.x, mi.y, mi.z, mi.w}, vs[4] = {vi.x, vi.y, vi.z, vi.w};
+        float ps[4] = {p.x, p.y, p.z, p.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            ms[k] = P.beta1 * ms[k] + (1.0f - P.beta1) * gs[k];
+            vs[k] = P.beta2 * vs[k] + (1.0f - P.beta2) * gs[k] * gs[k];
+            ps[k] = ps[k] - P.lr * (ms[k] / P.correction1) / (sqrtf(vs[k] / P.correction2) + P.eps);
+        }
+        m[i] = make_float4(ms[0], ms[1], ms[2], ms[3]);
+        v[i] = make_float4(vs[0], vs[1], vs[2], vs[3]);
+        param[i] = make_float4(ps[0], ps[1], ps[2], ps[3]);
+        out[i] = make_uint2(pack_bf16x2(ps[0], ps[1]), pack_bf16x2(ps[2], ps[3]));
+    }
+}
+
 // Packs the FP32 master weights into the forward (W) and backward (W^T)
 // shared-memory tile layouts.
 __global__ void pack_weights_kernel(const float *__restrict__ w, bf16 *__restrict__ out) {
@@ -864,8 +893,9 @@ extern "C" lux_status lux_cache_train(LuxCache *c, const LuxCacheSample *samples
         P.eps = 1e-10f;
         P.correction1 = 1.0f - (float)std::pow(0.9, (double)c->steps);
         P.correction2 = 1.0f - (float)std::pow(0.99, (double)c->steps);
-        adam_kernel<<<grid, 256, 0, st>>>(P, c->table_master, c->table_grad, c->table_m, c->table_v, c->table_params,
-                                          c->table);
+        adam4_kernel<<<grid, 256, 0, st>>>(P, (float4 *)c->table_master, (float4 *)c->table_grad,
+                                           (float4 *)c->table_m, (float4 *)c->table_v, c->table_params / 4,
+                                           (uint2 *)c->table);
         adam_kernel<<<(kWTotal + 255) / 256, 256, 0, st>>>(P, c->w_master, c->w_grad, c->w_m, c->w_v, kWTotal,
                                                            nullptr);
         pack_weights_kernel<<<(kWTotal + 255) / 256, 256, 0, st>>>(c->w_master, c->w_packed);

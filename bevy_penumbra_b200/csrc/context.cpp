@@ -67,7 +67,8 @@ extern "C" lux_status lux_context_synchronize(LuxContext *ctx) {
     return lux_cuda_check(ctx, (int)cudaStreamSynchronize(ctx->stream), "stream synchronize");
 }
 
-// RadianceCascades::default(), src/lib.rs:671-698, plus the extension fields
+// RadianceCascades::default(), src/lib.rs:671-698 (temporal_blend 0.88,
+// split_transmittance_blend 0.98, history_frames 24), plus the extension fields
 // at the reference's fixed values (CASCADES = 4, BASE_THETA = 4, x4 ends).
 extern "C" void lux_settings_default(LuxSettings *s) {
     if (!s) return;
@@ -87,6 +88,9 @@ extern "C" void lux_settings_default(LuxSettings *s) {
     s->rays_per_receiver = 1;
     s->frame_index = 0;
     s->resolve_scale = 1;
+    s->temporal_blend = 0.88f;
+    s->transmittance_blend = 0.98f;
+    s->history_frames = 24;
 }
 
 // RadianceCascades::low_end(), src/lib.rs:700-722 (the fields this path reads).
@@ -97,6 +101,7 @@ extern "C" void lux_settings_low_end(LuxSettings *s) {
     s->interval_length = 1.6f;
     s->emissive_samples = 4;
     s->resolve_scale = 2;
+    s->temporal_blend = 0.95f;
 }
 
 static float finite_clamp(float value, float fallback, float lo, float hi) {
@@ -106,7 +111,8 @@ static float finite_clamp(float value, float fallback, float lo, float hi) {
 
 static uint32_t clamp_u(uint32_t v, uint32_t lo, uint32_t hi) { return v < lo ? lo : (v > hi ? hi : v); }
 
-// RadianceCascades::sanitized(), src/lib.rs:731-759; SamplingSettings
+// RadianceCascades::sanitized(), src/lib.rs:731-759 (blends clamped to
+// 0.99 / 0.999, history_frames to 64); SamplingSettings
 // resolve_scale clamp, src/lib.rs:388-407.
 extern "C" void lux_settings_sanitize(LuxSettings *s) {
     if (!s) return;
@@ -128,6 +134,9 @@ extern "C" void lux_settings_sanitize(LuxSettings *s) {
     if (s->interval_rule > LUX_INTERVAL_LENGTHS_GEOMETRIC) s->interval_rule = LUX_INTERVAL_ENDS_GEOMETRIC;
     if (s->layout > LUX_LAYOUT_DENSE) s->layout = LUX_LAYOUT_SPLIT;
     s->rays_per_receiver = clamp_u(s->rays_per_receiver, 1, 4096);
+    s->temporal_blend = finite_clamp(s->temporal_blend, 0.88f, 0.0f, 0.99f);
+    s->transmittance_blend = finite_clamp(s->transmittance_blend, 0.98f, 0.0f, 0.999f);
+    s->history_frames = s->history_frames > 64u ? 64u : s->history_frames;
 }
 
 // splitIntervalEnd, shaders/split.slang:224-227, generalised to a ratio and

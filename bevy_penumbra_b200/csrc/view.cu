@@ -19,6 +19,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -48,6 +49,20 @@ namespace {
 
 using lux::f3;
 
+constexpr int kMaxDirty = 8;  // invalidation boxes per frame (more are merged into their union)
+
+// The previous frame's records: its cell directories, record offsets, and
+// blended raw records with their masses (swapped with the current frame's
+// buffers at the start of each frame).
+struct HistoryDevice {
+    const unsigned long long *dir_keys;
+    const uint32_t *dir_ids;
+    const unsigned long long *level_base;
+    const uint32_t *cell_count;
+    const float4 *raw;
+    const float2 *mass;
+};
+
 struct FrameParams {
     uint32_t levels, layout, rays_per_receiver, receivers;
     uint32_t dir_capacity, cell_capacity, ray_capacity, queue_capacity;
@@ -59,6 +74,11 @@ struct FrameParams {
     uint32_t rows[LUX_MAX_LEVELS];
     uint32_t dirs[LUX_MAX_LEVELS];
     lux::ShadeParams shade;
+    // World history (mergeEntry, shaders/split.slang:1624-1725).
+    float radiance_blend, transmittance_blend;  // 0 disables that quantity's history
+    uint32_t history;                           // 1: the previous frame's records may be reused
+    uint32_t dirty_count;                       // boxes whose records do not reuse history
+    float dirty_lo[kMaxDirty][3], dirty_hi[kMaxDirty][3];
 };
 
 // Device state of a view (ViewBuffers, src/render.rs:5077-5160).
@@ -74,7 +94,9 @@ struct ViewDevice {
     float4 *accum;                  // [entries] J sum rgb, non-terminating count
     uint32_t *count;                // [entries]
     float4 *merged;                 // [entries] I rgb, support
-    float4 *raw;                    // [entries] J mean rgb, beta
+    float4 *raw;                    // [entries] J rgb, beta (history-blended)
+    float2 *mass;                   // [entries] radiance mass, transmittance mass
+    uint32_t *hist_cell;            // [levels][cell_capacity] the previous frame's id of each cell, or kEmpty
     float4 *tables;                 // [cell_capacity][36]
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
@@ -763,60 +785,180 @@ __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FramePa
 }
 
 // mergeEntry without history, shaders/split.slang:1523-1725.
-__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, uint32_t level) {
+// base^n by squaring and multiplying in a fixed order (the CPU restatement
+// rounds identically); pow(blend, observations) of mergeRawRadianceGroup.
+__device__ __forceinline__ float pow_count(float base, uint32_t n) {
+    float r = 1.0f, b = base;
+    while (n) {
+        if (n & 1u) r = r * b;
+        b = b * b;
+        n >>= 1;
+    }
+    return r;
+}
+
+// The previous frame's dense id of every cell of `level` (kEmpty when the
+// cell was not there or its history is invalidated), one directory probe per
+// cell instead of one per record.
+__device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t level, int4 key);
+
+__global__ void history_map_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
+    uint32_t cells = min(V.cell_count[level], F.cell_capacity);
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+        uint32_t id = lux::kEmpty;
+        int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+        if (lux::cell_in_range(key.x, key.y, key.z) && !record_dirty(F, level, key)) {
+            unsigned long long packed = lux::pack_cell(key.x, key.y, key.z);
+            const unsigned long long *keys = H.dir_keys + (size_t)level * F.dir_capacity;
+            uint32_t slot = lux::hash_key(key.x, key.y, key.z, (int32_t)level, F.dir_capacity);
+            for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+                unsigned long long k = keys[slot];
+                if (k == packed) {
+                    uint32_t prev = H.dir_ids[(size_t)level * F.dir_capacity + slot];
+                    if (prev != lux::kEmpty && prev < H.cell_count[level]) id = prev;
+                    break;
+                }
+                if (k == lux::kEmptyCell) break;
+                slot = (slot + 1u) & (F.dir_capacity - 1u);
+            }
+        }
+        V.hist_cell[(size_t)level * F.cell_capacity + c] = id;
+    }
+}
+
+// A record's history is invalid when the region its rays may have crossed
+// (the cell grown by the level's interval end; unbounded at the last level)
+// meets an invalidation box (dirtyRawCacheEntry / betaHistoryEligible,
+// shaders/split.slang:123-132, :201-203, with a box dependency).
+__device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t level, int4 key) {
+    if (F.dirty_count == 0u) return false;
+    if (level + 1u >= F.levels) return true;
+    float s = F.spacing[level], reach = F.end[level];
+    float lo[3] = {(float)key.x * s - reach, (float)key.y * s - reach, (float)key.z * s - reach};
+    float hi[3] = {(float)(key.x + 1) * s + reach, (float)(key.y + 1) * s + reach, (float)(key.z + 1) * s + reach};
+    for (uint32_t b = 0; b < F.dirty_count && b < (uint32_t)kMaxDirty; ++b) {
+        bool meet = true;
+        for (int a = 0; a < 3; ++a) meet = meet && lo[a] <= F.dirty_hi[b][a] && hi[a] >= F.dirty_lo[b][a];
+        if (meet) return true;
+    }
+    return false;
+}
+
+// mergeEntry (shaders/split.slang:1624-1725) for one record: the fresh mean
+// (J, beta) of this frame's observations blended with the previous frame's
+// record by mergeRawRadianceGroup's masses (retention blend^n, mass limit
+// 1 / (1 - blend); :1478-1521) for the summed radiance group and for the
+// transmittance, then Eq. 7 with the children: I = [J (1 - beta) + beta
+// mean_4(trilerp_8(I_child) support)] / support.
+__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
     if (*V.error_flags) return;
     uint32_t dirs = F.dirs[level];
     unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
     unsigned long long base = V.level_base[level];
     bool has_children = level + 1u < F.levels;
+    const float jb = F.radiance_blend, tb = F.transmittance_blend;
+    const float jlimit = 1.0f / (1.0f - jb), tlimit = 1.0f / (1.0f - tb);
     for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
          e += (unsigned long long)gridDim.x * blockDim.x) {
         uint32_t cnt = V.count[base + e];
-        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float4 raw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
+        float4 fresh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (cnt) {
             float4 acc = V.accum[base + e];
             float fn = (float)cnt;
-            raw = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
-            float transmittance = lux::saturate(raw.w);
-            float support = 1.0f - transmittance;
-            float rx = 0.0f, ry = 0.0f, rz = 0.0f;
-            if (support > 0.0f) {
-                rx = raw.x;
-                ry = raw.y;
-                rz = raw.z;
-            }
-            float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
-            if (transmittance > 0.0f && has_children) {
-                uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
-                size_t ci = (size_t)level * F.cell_capacity + cell;
-                uint32_t ids[8];
-#pragma unroll
-                for (int k = 0; k < 8; ++k) ids[k] = __ldg(V.corner_ids + ci * 8 + k);
-                float4 frac = __ldg(V.corner_frac + ci);
-                uint32_t x = d % F.columns[level], y = d / F.columns[level];
-                uint32_t fine_columns = F.columns[level + 1];
-#pragma unroll
-                for (uint32_t child = 0; child < 4u; ++child) {
-                    uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
-                    float4 v = interpolate(V, F, level + 1, ids, frac, fine);
-                    if (!(v.w > 0.0f)) continue;
-                    cx = cx + v.x * v.w;
-                    cy = cy + v.y * v.w;
-                    cz = cz + v.z * v.w;
-                    csup += v.w;
-                }
-            }
-            if (csup > 0.0f) {
-                rx = rx + (transmittance * cx) * 0.25f;
-                ry = ry + (transmittance * cy) * 0.25f;
-                rz = rz + (transmittance * cz) * 0.25f;
-                support = support + (transmittance * csup) * 0.25f;
-            }
-            if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
+            fresh = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
         }
+        // History of this record.
+        bool reuse = false;
+        float4 old = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        float2 old_mass = make_float2(0.0f, 0.0f);
+        if (F.history) {
+            uint32_t prev = V.hist_cell[(size_t)level * F.cell_capacity + cell];
+            if (prev != lux::kEmpty) {
+                unsigned long long r = H.level_base[level] + (unsigned long long)prev * dirs + d;
+                old = H.raw[r];
+                old_mass = H.mass[r];
+                reuse = true;
+            }
+        }
+        float rm = old_mass.x, tm = old_mass.y;
+        if (!isfinite(rm) || rm < 0.0f) rm = 0.0f;
+        if (!isfinite(tm) || tm < 0.0f) tm = 0.0f;
+        const bool reuse_r = reuse && jb > 0.0f, reuse_t = reuse && tb > 0.0f;
+        float jx = 0.0f, jy = 0.0f, jz = 0.0f, beta = 1.0f, rmass = 0.0f, tmass = 0.0f;
+        if (cnt) {
+            float ret = pow_count(jb, cnt);
+            rmass = (1.0f - ret) * jlimit;
+            jx = fresh.x;
+            jy = fresh.y;
+            jz = fresh.z;
+            float om = fminf(rm, jlimit) * ret;
+            if (reuse_r && om > 0.0f) {
+                jx = (jx * rmass + old.x * om) / (rmass + om);
+                jy = (jy * rmass + old.y * om) / (rmass + om);
+                jz = (jz * rmass + old.z * om) / (rmass + om);
+                rmass = rmass + om;
+            }
+            float tret = pow_count(tb, cnt);
+            tmass = (1.0f - tret) * tlimit;
+            beta = fresh.w;
+            float otm = fminf(tm, tlimit) * tret;
+            if (reuse_t && otm > 0.0f) {
+                beta = (beta * tmass + old.w * otm) / (tmass + otm);
+                tmass = tmass + otm;
+            }
+        } else {
+            if (reuse_r && rm > 0.0f) {
+                jx = old.x;
+                jy = old.y;
+                jz = old.z;
+                rmass = rm;
+            }
+            if (reuse_t && tm > 0.0f) {
+                beta = old.w;
+                tmass = tm;
+            }
+        }
+        float transmittance = tmass > 0.0f ? lux::saturate(beta) : 0.0f;
+        float support = rmass > 0.0f && tmass > 0.0f ? 1.0f - transmittance : 0.0f;
+        float rx = 0.0f, ry = 0.0f, rz = 0.0f;
+        if (support > 0.0f) {
+            rx = jx;
+            ry = jy;
+            rz = jz;
+        }
+        float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
+        if (transmittance > 0.0f && has_children) {
+            size_t ci = (size_t)level * F.cell_capacity + cell;
+            uint32_t ids[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) ids[k] = __ldg(V.corner_ids + ci * 8 + k);
+            float4 frac = __ldg(V.corner_frac + ci);
+            uint32_t x = d % F.columns[level], y = d / F.columns[level];
+            uint32_t fine_columns = F.columns[level + 1];
+#pragma unroll
+            for (uint32_t child = 0; child < 4u; ++child) {
+                uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
+                float4 v = interpolate(V, F, level + 1, ids, frac, fine);
+                if (!(v.w > 0.0f)) continue;
+                cx = cx + v.x * v.w;
+                cy = cy + v.y * v.w;
+                cz = cz + v.z * v.w;
+                csup += v.w;
+            }
+        }
+        if (csup > 0.0f) {
+            rx = rx + (transmittance * cx) * 0.25f;
+            ry = ry + (transmittance * cy) * 0.25f;
+            rz = rz + (transmittance * cz) * 0.25f;
+            support = support + (transmittance * csup) * 0.25f;
+        }
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
         V.merged[base + e] = out;
-        V.raw[base + e] = raw;
+        V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
+                                                                 : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        V.mass[base + e] = make_float2(rmass, tmass);
     }
 }
 
@@ -1388,6 +1530,22 @@ struct LuxView {
     uint32_t stage_receivers = 0, stage_points = 0;
     FrameParams last{};
     bool has_frame = false;
+    // World history: the other buffer set (swapped with dev's at each
+    // frame start), whether it holds a usable previous frame, and the
+    // invalidation boxes queued for the next frame.
+    struct {
+        unsigned long long *dir_keys = nullptr;
+        uint32_t *dir_ids = nullptr;
+        unsigned long long *level_base = nullptr;
+        uint32_t *cell_count = nullptr;
+        float4 *raw = nullptr;
+        float2 *mass = nullptr;
+    } hist;
+    bool hist_valid = false;
+    uint32_t hist_levels = 0;
+    uint32_t hist_dirs[LUX_MAX_LEVELS] = {};
+    uint64_t generation = 0;  // bumped at every buffer swap (batch job tables hold pointers)
+    std::vector<std::array<float, 6>> dirty;
     // Learned-cache form (lux_view_set_cache).
     LuxCacheMode cache{};
     CacheDevice cdev{};
@@ -1426,6 +1584,14 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.count, (size_t)d.max_entries * sizeof(uint32_t)},
         {(void **)&D.merged, (size_t)d.max_entries * sizeof(float4)},
         {(void **)&D.raw, (size_t)d.max_entries * sizeof(float4)},
+        {(void **)&D.mass, (size_t)d.max_entries * sizeof(float2)},
+        {(void **)&D.hist_cell, L * (size_t)d.max_cells * sizeof(uint32_t)},
+        {(void **)&v->hist.dir_keys, L * v->dir_capacity * sizeof(unsigned long long)},
+        {(void **)&v->hist.dir_ids, L * v->dir_capacity * sizeof(uint32_t)},
+        {(void **)&v->hist.level_base, L * sizeof(unsigned long long)},
+        {(void **)&v->hist.cell_count, L * sizeof(uint32_t)},
+        {(void **)&v->hist.raw, (size_t)d.max_entries * sizeof(float4)},
+        {(void **)&v->hist.mass, (size_t)d.max_entries * sizeof(float2)},
         {(void **)&D.tables, (size_t)d.max_cells * 36 * sizeof(float4)},
         {(void **)&D.error_flags, sizeof(uint32_t) * 4},
         {(void **)&D.stats, 16 * sizeof(unsigned long long)},
@@ -1481,7 +1647,10 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     if (!v) return LUX_OK;
     ViewDevice &D = v->dev;
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
-                    D.corner_frac, D.accum, D.count, D.merged, D.raw, D.tables, D.error_flags, D.stats,
+                    D.corner_frac, D.accum, D.count, D.merged, D.raw, D.mass, D.hist_cell, D.tables, D.error_flags,
+                    D.stats,
+                    v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
+                    v->hist.mass,
                     D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
                     D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
@@ -1585,6 +1754,10 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
     F.shade.exposure = s.exposure;
     F.shade.emissive_samples = s.emissive_samples;
     F.shade.frame = s.frame_index;
+    F.radiance_blend = s.temporal_blend;
+    F.transmittance_blend = s.transmittance_blend;
+    F.history = 0;
+    F.dirty_count = 0;
     if ((size_t)F.dirs[0] * 2 * sizeof(float4) > 48 * 1024)
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: too many cascade-0 directions");
     return LUX_OK;
@@ -1610,8 +1783,49 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
 static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     const ViewDevice &D = v->dev;
     const int grid = v->ctx->sm_count * 8;
+    HistoryDevice H{v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
+                    v->hist.mass};
     for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
-    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, (uint32_t)l);
+    if (F.history)
+        for (uint32_t l = 0; l < F.levels; ++l) history_map_kernel<<<grid, 128, 0, st>>>(D, F, H, l);
+    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, H, (uint32_t)l);
+}
+
+// Start of an unbatched frame: the last frame's records become the history
+// (a pointer swap, no copy); history is used when enabled and the previous
+// frame had the same cascade shape.  Queued invalidation boxes apply now.
+static void begin_history(LuxView *v, FrameParams &F, const LuxSettings &s) {
+    const bool enabled = s.history_frames > 0 && (s.temporal_blend > 0.0f || s.transmittance_blend > 0.0f);
+    bool same_shape = v->hist_valid && v->hist_levels == F.levels;
+    for (uint32_t l = 0; same_shape && l < F.levels; ++l) same_shape = v->hist_dirs[l] == F.dirs[l];
+    F.history = enabled && same_shape ? 1u : 0u;
+    if (enabled) {  // without history the current buffers are simply reused
+        ViewDevice &D = v->dev;
+        std::swap(D.dir_keys, v->hist.dir_keys);
+        std::swap(D.dir_ids, v->hist.dir_ids);
+        std::swap(D.level_base, v->hist.level_base);
+        std::swap(D.cell_count, v->hist.cell_count);
+        std::swap(D.raw, v->hist.raw);
+        std::swap(D.mass, v->hist.mass);
+        ++v->generation;
+    }
+    F.dirty_count = 0;
+    for (size_t i = 0; i < v->dirty.size(); ++i) {
+        const auto &box = v->dirty[i];
+        uint32_t slot = i < (size_t)kMaxDirty ? (uint32_t)i : (uint32_t)kMaxDirty - 1u;
+        for (int a = 0; a < 3; ++a) {
+            F.dirty_lo[slot][a] = i < (size_t)kMaxDirty ? box[a] : std::min(F.dirty_lo[slot][a], box[a]);
+            F.dirty_hi[slot][a] = i < (size_t)kMaxDirty ? box[3 + a] : std::max(F.dirty_hi[slot][a], box[3 + a]);
+        }
+        F.dirty_count = std::max(F.dirty_count, slot + 1u);
+    }
+    v->dirty.clear();
+}
+
+static void end_history(LuxView *v, const FrameParams &F) {
+    v->hist_valid = true;
+    v->hist_levels = F.levels;
+    for (uint32_t l = 0; l < F.levels; ++l) v->hist_dirs[l] = F.dirs[l];
 }
 
 // packProbes (shaders/split.slang:1786-1918); the direction count is
@@ -1641,6 +1855,9 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     auto mark = [&](int i) {
         if (v->timing) cudaEventRecord(v->ev[i], st);
     };
+    LuxSettings sanitized = *settings;
+    lux_settings_sanitize(&sanitized);
+    begin_history(v, F, sanitized);
     mark(0);
     enqueue_setup(v, F, pos, st);
     mark(1);
@@ -1729,9 +1946,30 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     mark(3);
     enqueue_pack(v, F, st);
     mark(4);
+    end_history(v, F);
     v->last = F;
     v->has_frame = true;
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "trace_merge launch");
+}
+
+extern "C" lux_status lux_view_reset_history(LuxView *v) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    v->hist_valid = false;
+    v->dirty.clear();
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_view_invalidate_bounds(LuxView *v, const float lo[3], const float hi[3]) {
+    if (!v || !lo || !hi) return LUX_ERR_INVALID_ARGUMENT;
+    std::array<float, 6> box;
+    for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(lo[a]) || !std::isfinite(hi[a]) || lo[a] > hi[a])
+            return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "invalidate_bounds: need finite lo <= hi");
+        box[a] = lo[a];
+        box[3 + a] = hi[a];
+    }
+    v->dirty.push_back(box);
+    return LUX_OK;
 }
 
 extern "C" lux_status lux_view_resolve(LuxView *v, const LuxSettings *settings, const float *ppos, const float *pnrm,
@@ -2102,6 +2340,7 @@ struct LuxBatch {
     bool use_graph = true;
     // Configuration the device tables and graph were built for.
     std::vector<LuxBatchJob> jobs;
+    std::vector<uint64_t> generations;  // each view's buffer generation the job table holds
     LuxSettings settings{};  // frame_index zeroed
     std::vector<FrameParams> params;
     uint32_t total = 0;      // padded interval rays
@@ -2277,6 +2516,8 @@ static lux_status batch_build(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n, 
                             "batch: ray offsets");
     if (rc != LUX_OK) return rc;
     b->jobs.assign(jobs, jobs + n);
+    b->generations.resize(n);
+    for (uint32_t j = 0; j < n; ++j) b->generations[j] = jobs[j].view->generation;
     b->settings = s;
     b->settings.frame_index = 0;
     b->params = params;
@@ -2330,6 +2571,7 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
     LuxSettings key = s;
     key.frame_index = 0;
     bool same = b->built && same_jobs(b->jobs, jobs, n) && std::memcmp(&key, &b->settings, sizeof key) == 0;
+    for (uint32_t j = 0; same && j < n; ++j) same = b->generations[j] == jobs[j].view->generation;
     if (!same) {
         lux_status rc = batch_build(b, jobs, n, s, params);
         if (rc != LUX_OK) return rc;
@@ -2353,6 +2595,7 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
         F.shade.frame = s.frame_index;
         jobs[j].view->last = F;
         jobs[j].view->has_frame = true;
+        end_history(jobs[j].view, F);
     }
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "batch launch");
 }

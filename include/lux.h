@@ -126,6 +126,10 @@ typedef struct LuxSettings {
     uint32_t rays_per_receiver;     /* Split layout: rays traced per receiver per frame (reference 1) */
     uint32_t frame_index;           /* params.frame.x */
     uint32_t resolve_scale;         /* SamplingSettings::resolve_scale, 1..=8 */
+    float temporal_blend;           /* RadianceCascades::temporal_blend (history.x): per-observation retention of
+                                       interval radiance, 0..=0.99; mass limit 1 / (1 - blend) */
+    float transmittance_blend;      /* RadianceCascades::split_transmittance_blend (intervalHistory.x), 0..=0.999 */
+    uint32_t history_frames;        /* RadianceCascades::history_frames (history.w), 0..=64; 0 disables history */
 } LuxSettings;
 
 /* Receivers (Split) or the cascade-0 probe set (Dense), device pointers.
@@ -353,6 +357,23 @@ lux_status lux_view_read_level(LuxView *view, uint32_t level, int32_t *cell_keys
                                float *merged, float *raw, uint32_t *samples);
 /* Copies packed cascade-0 probe tables: keys int4[cells], tables float4[cells*36]. */
 lux_status lux_view_read_probes(LuxView *view, int32_t *cell_keys, float *tables);
+
+/* World history (mergeEntry, shaders/split.slang:1624-1725).  Each
+ * unbatched lux_view_trace_merge blends every record's fresh observations
+ * with the same record (cell key, direction, level) of the view's previous
+ * frame: retention temporal_blend^n of the old radiance mass (limit
+ * 1 / (1 - blend)), likewise the transmittance with transmittance_blend;
+ * records without observations keep their history.  History applies when
+ * history_frames > 0 and the previous frame had the same cascade shape.
+ * Cells seen in neither frame carry no history (records live as long as
+ * receivers keep seeding their cell).  Batched frames do not blend, but
+ * their records serve as the next unbatched frame's history. */
+/* Forgets the view's history (RadianceCascades::reset_history). */
+lux_status lux_view_reset_history(LuxView *view);
+/* Queues a world box for the next frame: records whose rays may have crossed
+ * it (the cell grown by its level's interval end; any record of the last
+ * level) take no history (dirty-bounds invalidation; moved geometry). */
+lux_status lux_view_invalidate_bounds(LuxView *view, const float lo[3], const float hi[3]);
 
 /* Interval-ray hits of the view's last Split frame, in ray order
  * (ray = receiver * rays_per_receiver + sample): out[count] LuxHit, count <=

@@ -63,6 +63,8 @@ def lib():
             "orc_trace_rays": (None, [P, P, U, C.c_int, P, C.c_int, P]),
             "orc_outgoing_radiance": (C.c_int, [P, P, P, P, P, P, P, P]),
             "orc_frame_run": (P, [P, P, P, P, U, C.c_int]),
+            "orc_frame_run_history": (P, [P, P, P, P, U, C.c_int, P, P, U]),
+            "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
             "orc_frame_read_level": (None, [P, U, P, P, P, P]),
@@ -160,12 +162,19 @@ class OracleScene:
 
 
 class OracleFrame:
-    def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0):
+    def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0,
+                 previous: "OracleFrame | None" = None, dirty=None):
+        """previous: the frame whose records serve as history; dirty: boxes
+        (n, 6) = (lo xyz, hi xyz) whose nearby records take no history."""
         self.settings = settings_c
         pos = np.ascontiguousarray(pos, np.float32)
         nrm = np.ascontiguousarray(nrm, np.float32)
-        self.handle = lib().orc_frame_run(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
-                                          threads or os.cpu_count() or 1)
+        self._previous = previous  # keeps the history frame alive
+        boxes = np.ascontiguousarray(dirty if dirty is not None else np.zeros((0, 6)), np.float32).reshape(-1, 6)
+        self.handle = lib().orc_frame_run_history(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
+                                                  threads or os.cpu_count() or 1,
+                                                  previous.handle if previous is not None else None, _p(boxes),
+                                                  len(boxes))
 
     def level(self, level: int, dirs: int):
         cells = lib().orc_frame_cells(self.handle, level)
@@ -207,3 +216,15 @@ class OracleFrame:
             self.close()
         except Exception:
             pass
+
+
+def history_blend(settings_c, samples: int, fresh, old=None, old_mass=None):
+    """mergeEntry's history blend of one record: (J rgb, beta), (radiance mass, transmittance mass)."""
+    fresh = f32(*fresh)
+    out = np.zeros(4, np.float32)
+    mass = np.zeros(2, np.float32)
+    o = f32(*old) if old is not None else None
+    om = f32(*old_mass) if old_mass is not None else None
+    lib().orc_history_blend(C.byref(settings_c), samples, _p(fresh), _p(o) if o is not None else None,
+                            _p(om) if om is not None else None, _p(out), _p(mass))
+    return out, mass

@@ -1366,7 +1366,8 @@ typedef struct {
     float *jsum;     /* float4: J sum rgb, non-terminating count */
     uint32_t *count;
     float *merged;   /* float4 */
-    float *raw;      /* float4 J mean, beta */
+    float *raw;      /* float4 J, beta (history-blended) */
+    float *mass;     /* float2 radiance mass, transmittance mass */
 } Level;
 
 struct OrcFrame {
@@ -1375,6 +1376,9 @@ struct OrcFrame {
     Level level[LUX_MAX_LEVELS];
     float *tables;  /* c0 cells * 36 float4 */
     LuxStats stats;
+    const struct OrcFrame *previous;  /* history source (NULL: none) */
+    const float *dirty;               /* invalidation boxes, 6 floats each */
+    uint32_t dirty_count;
 };
 
 static int64_t find_cell(const Level *L, const int32_t key[3]) {
@@ -1552,17 +1556,78 @@ void orc_interpolate_children(const float fraction[3], const float *corner_merge
 /* mergeEntry + mergeRadianceGroups + finishMergeGroup without history
  * (shaders/split.slang:1523-1725): interval = (J.rgb, beta) of the reduced
  * entry, child values = the 4 angular children already interpolated. */
-static void merge_values(const float interval[4], uint32_t samples, const float *children, int has_children,
-                         float out[4]) {
-    if (samples == 0u) {
-        out[0] = out[1] = out[2] = out[3] = 0.0f;
-        return;
+/* base^n by squaring and multiplying (the GPU kernel rounds identically). */
+static float pow_count(float base, uint32_t n) {
+    float r = 1.0f, b = base;
+    while (n) {
+        if (n & 1u) r = r * b;
+        b = b * b;
+        n >>= 1;
     }
-    float transmittance = saturatef(interval[3]);
-    float support = 1.0f - transmittance;
+    return r;
+}
+
+/* mergeEntry's history blend (shaders/split.slang:1624-1725 with
+ * mergeRawRadianceGroup, :1478-1521) of one record, for the summed radiance
+ * group (blend temporal_blend) and the transmittance (transmittance_blend):
+ * n fresh observations with mean `fresh` (J rgb, beta); `old` / `old_mass`
+ * the previous frame's record (NULL: none).  With n > 0 the new mass is
+ * (1 - blend^n) / (1 - blend) and the old mass is min(old, limit) * blend^n;
+ * with n == 0 the old record is kept as it is; without either, J = 0,
+ * beta = 1 and both masses are 0. */
+void orc_history_blend(const LuxSettings *st, uint32_t n, const float fresh[4], const float *old,
+                       const float *old_mass, float out[4], float mass[2]) {
+    float jb = st->temporal_blend, tb = st->transmittance_blend;
+    float jlimit = 1.0f / (1.0f - jb), tlimit = 1.0f / (1.0f - tb);
+    float rm = old_mass ? old_mass[0] : 0.0f, tm = old_mass ? old_mass[1] : 0.0f;
+    if (!isfinite(rm) || rm < 0.0f) rm = 0.0f;
+    if (!isfinite(tm) || tm < 0.0f) tm = 0.0f;
+    int reuse_r = old && jb > 0.0f, reuse_t = old && tb > 0.0f;
+    float j[3] = {0.0f, 0.0f, 0.0f}, beta = 1.0f, rmass = 0.0f, tmass = 0.0f;
+    if (n) {
+        float ret = pow_count(jb, n);
+        rmass = (1.0f - ret) * jlimit;
+        for (int c = 0; c < 3; ++c) j[c] = fresh[c];
+        float om = fminf(rm, jlimit) * ret;
+        if (reuse_r && om > 0.0f) {
+            for (int c = 0; c < 3; ++c) j[c] = (j[c] * rmass + old[c] * om) / (rmass + om);
+            rmass = rmass + om;
+        }
+        float tret = pow_count(tb, n);
+        tmass = (1.0f - tret) * tlimit;
+        beta = fresh[3];
+        float otm = fminf(tm, tlimit) * tret;
+        if (reuse_t && otm > 0.0f) {
+            beta = (beta * tmass + old[3] * otm) / (tmass + otm);
+            tmass = tmass + otm;
+        }
+    } else {
+        if (reuse_r && rm > 0.0f) {
+            for (int c = 0; c < 3; ++c) j[c] = old[c];
+            rmass = rm;
+        }
+        if (reuse_t && tm > 0.0f) {
+            beta = old[3];
+            tmass = tm;
+        }
+    }
+    out[0] = j[0];
+    out[1] = j[1];
+    out[2] = j[2];
+    out[3] = beta;
+    mass[0] = rmass;
+    mass[1] = tmass;
+}
+
+/* Eq. 7 on a blended record (mergeRadianceGroups / finishMergeGroup,
+ * shaders/split.slang:1523-1622). */
+static void merge_blended(const float raw[4], const float mass[2], const float *children, int has_children,
+                          float out[4]) {
+    float transmittance = mass[1] > 0.0f ? saturatef(raw[3]) : 0.0f;
+    float support = mass[0] > 0.0f && mass[1] > 0.0f ? 1.0f - transmittance : 0.0f;
     float radiance[3] = {0, 0, 0};
     if (support > 0.0f) {
-        radiance[0] = interval[0]; radiance[1] = interval[1]; radiance[2] = interval[2];
+        radiance[0] = raw[0]; radiance[1] = raw[1]; radiance[2] = raw[2];
     }
     float child_sum[3] = {0, 0, 0}, child_support = 0.0f;
     if (transmittance > 0.0f && has_children) {
@@ -1585,11 +1650,38 @@ static void merge_values(const float interval[4], uint32_t samples, const float 
     }
 }
 
+static void merge_values(const LuxSettings *st, const float interval[4], uint32_t samples, const float *children,
+                         int has_children, float out[4]) {
+    float raw[4], mass[2];
+    orc_history_blend(st, samples, interval, NULL, NULL, raw, mass);
+    merge_blended(raw, mass, children, has_children, out);
+}
+
 void orc_merge_entry(const float interval[4], uint32_t samples, const float fraction[3], const float *child_merged,
                      int has_children, float out[4]) {
     float children[16];
     for (int c = 0; c < 4; ++c) orc_interpolate_children(fraction, child_merged + 32 * c, children + 4 * c);
-    merge_values(interval, samples, children, has_children, out);
+    LuxSettings st;
+    memset(&st, 0, sizeof st);  /* no history: blends 0 */
+    merge_values(&st, interval, samples, children, has_children, out);
+}
+
+/* A record's history is invalid when its cell grown by the level's
+ * interval end (unbounded at the last level) meets an invalidation box. */
+static int record_dirty(const OrcFrame *F, uint32_t level, const int32_t key[3]) {
+    if (F->dirty_count == 0) return 0;
+    if (level + 1 >= F->levels) return 1;
+    float s = orc_spacing(&F->st, level), reach = orc_interval_end(&F->st, level);
+    for (uint32_t b = 0; b < F->dirty_count; ++b) {
+        const float *box = F->dirty + 6 * (size_t)b;
+        int meet = 1;
+        for (int a = 0; a < 3; ++a) {
+            float lo = (float)key[a] * s - reach, hi = (float)(key[a] + 1) * s + reach;
+            meet = meet && lo <= box[3 + a] && hi >= box[a];
+        }
+        if (meet) return 1;
+    }
+    return 0;
 }
 
 static void merge_level(OrcFrame *F, uint32_t l) {
@@ -1617,6 +1709,15 @@ static void merge_level(OrcFrame *F, uint32_t l) {
                 corner_cell[corner] = find_cell(P, k);
             }
         }
+        /* The previous frame's cell of this key (history), unless an
+         * invalidation box meets the region its rays may have crossed. */
+        const Level *H = NULL;
+        int64_t hcell = -1;
+        if (F->previous && l < F->previous->levels && F->previous->level[l].dirs == L->dirs &&
+            !record_dirty(F, l, L->keys[cell].k)) {
+            H = &F->previous->level[l];
+            hcell = find_cell(H, L->keys[cell].k);
+        }
         for (uint32_t d = 0; d < L->dirs; ++d) {
             uint64_t e = (uint64_t)cell * L->dirs + d;
             uint32_t n = L->count[e];
@@ -1625,10 +1726,23 @@ static void merge_level(OrcFrame *F, uint32_t l) {
                 float fn = (float)n;
                 for (int c = 0; c < 4; ++c) interval[c] = L->jsum[4 * e + c] / fn;
             }
-            memcpy(&L->raw[4 * e], interval, sizeof interval);
+            const float *old = NULL, *old_mass = NULL;
+            if (hcell >= 0) {
+                uint64_t he = (uint64_t)hcell * H->dirs + d;
+                old = &H->raw[4 * he];
+                old_mass = &H->mass[2 * he];
+            }
+            float raw[4], mass[2];
+            orc_history_blend(st, n, interval, old, old_mass, raw, mass);
+            if (n || mass[0] > 0.0f || mass[1] > 0.0f)
+                memcpy(&L->raw[4 * e], raw, sizeof raw);
+            else
+                memset(&L->raw[4 * e], 0, sizeof raw);
+            memcpy(&L->mass[2 * e], mass, sizeof mass);
+            float transmittance = mass[1] > 0.0f ? saturatef(raw[3]) : 0.0f;
             float children[16];
             memset(children, 0, sizeof children);
-            if (has_children && n) {
+            if (has_children && transmittance > 0.0f) {
                 uint32_t x = d % L->columns, y = d / L->columns;
                 for (uint32_t child = 0; child < 4u; ++child) {
                     uint32_t fx = x * 2u + (child & 1u), fy = y * 2u + (child >> 1);
@@ -1644,7 +1758,7 @@ static void merge_level(OrcFrame *F, uint32_t l) {
                     orc_interpolate_children(fraction, corners, children + 4 * child);
                 }
             }
-            merge_values(interval, n, children, has_children, &L->merged[4 * e]);
+            merge_blended(raw, mass, children, has_children, &L->merged[4 * e]);
         }
     }
 }
@@ -1746,8 +1860,22 @@ void orc_probe_lookup(const float *table36, const float normal[3], float out[4])
 
 OrcFrame *orc_frame_run(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm, uint32_t n,
                         int threads) {
+    return orc_frame_run_history(S, st_in, pos, nrm, n, threads, NULL, NULL, 0);
+}
+
+OrcFrame *orc_frame_run_history(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
+                                uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
+                                uint32_t dirty_count) {
     OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
     F->st = *st_in;
+    /* History applies with history_frames > 0, a blend above zero and a
+     * previous frame of the same cascade count. */
+    if (previous && st_in->history_frames > 0 && (st_in->temporal_blend > 0.0f || st_in->transmittance_blend > 0.0f) &&
+        previous->levels == st_in->levels) {
+        F->previous = previous;
+        F->dirty = dirty;
+        F->dirty_count = dirty ? dirty_count : 0;
+    }
     const LuxSettings *st = &F->st;
     F->levels = st->levels;
     /* seed: the cells of every level that hold a receiver. */
@@ -1773,6 +1901,7 @@ OrcFrame *orc_frame_run(const OrcScene *S, const LuxSettings *st_in, const float
         L->count = (uint32_t *)calloc(entries + 1, sizeof(uint32_t));
         L->merged = (float *)calloc(4 * entries + 4, sizeof(float));
         L->raw = (float *)calloc(4 * entries + 4, sizeof(float));
+        L->mass = (float *)calloc(2 * entries + 2, sizeof(float));
         F->stats.cells[l] = cells;
         F->stats.entries[l] = entries;
     }
@@ -1861,6 +1990,7 @@ void orc_frame_destroy(OrcFrame *F) {
         free(F->level[l].count);
         free(F->level[l].merged);
         free(F->level[l].raw);
+        free(F->level[l].mass);
     }
     free(F->tables);
     free(F);

@@ -93,6 +93,15 @@ void orc_reference_irradiance(const OrcScene *scene, const LuxSettings *settings
 
 /* --- one cascade frame ---------------------------------------------------- */
 typedef struct OrcFrame OrcFrame;
+/* A frame that takes history from `previous` (NULL: none; settings must be
+ * sanitized): records of the previous frame with the same key blend in as
+ * lux_view_trace_merge does; `dirty` holds dirty_count boxes (lo xyz, hi xyz)
+ * whose nearby records take no history. */
+OrcFrame *orc_frame_run_history(const OrcScene *scene, const LuxSettings *settings, const float *receiver_position,
+                                const float *receiver_normal, uint32_t receiver_count, int threads,
+                                const OrcFrame *previous, const float *dirty, uint32_t dirty_count);
+void orc_history_blend(const LuxSettings *settings, uint32_t samples, const float fresh[4], const float *old,
+                       const float *old_mass, float out[4], float mass[2]);
 OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
                         const float *receiver_position, const float *receiver_normal,
                         uint32_t receiver_count, int threads);

@@ -67,6 +67,10 @@ def test_invalid_settings_are_bounded():
     assert 1 <= s.levels <= N.LUX_MAX_LEVELS
     assert s.rays_per_receiver == 1
     assert s.sampling.resolve_scale == 8
+    h = bp.RadianceCascades(temporal_blend=math.inf, split_transmittance_blend=5.0, history_frames=1000).sanitized()
+    assert h.temporal_blend == np.float32(0.88)        # non-finite: the default
+    assert h.split_transmittance_blend == np.float32(0.999)
+    assert h.history_frames == 64
 
 
 def test_low_end_preset_fields():
@@ -78,6 +82,8 @@ def test_low_end_preset_fields():
     N.lib().lux_settings_default(C.byref(d))
     assert d.probe_spacing == np.float32(0.25) and d.emissive_samples == 16 and d.levels == 4
     assert (d.base_columns, d.base_rows) == (8, 4)  # 2*BASE_THETA x BASE_THETA
+    assert d.temporal_blend == np.float32(0.88) and d.transmittance_blend == np.float32(0.98)
+    assert d.history_frames == 24 and c.temporal_blend == np.float32(0.95)
     lo = bp.RadianceCascades.low_end()
     assert lo.sampling.grid_divisor == 8 and lo.sampling.max_receiver_cells == 16_384
 

@@ -146,3 +146,54 @@ def test_split_atrium_frame_matches_oracle():
                                                      tuning=dict(sort_rays=1, sort_queries=1))
     ofr = oracle_frame("atrium65536", settings, pos, nrm)
     compare_levels(settings, levels, ofr, exact=False)
+
+
+def test_dense_cornell_history_matches_oracle():
+    """Two frames on one view: the second blends the first's records
+    (mergeEntry's history); dense records are bit-exact."""
+    settings = cornell_dense_settings(frame_index=0)
+    pos, nrm = scenes.dense_plane_probes(64, 0.1, 10)
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=1 << 16, max_entries=1 << 24, max_rays=1 << 20)
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    view.trace_merge(scene, settings, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+    second = cornell_dense_settings(frame_index=1)
+    view.trace_merge(scene, second, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+    levels = [view.read_level(l) for l in range(second.levels)]
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    first = oracle.OracleFrame(oscene, settings.to_c(), pos, nrm)
+    ofr = oracle.OracleFrame(oscene, second.to_c(), pos, nrm, previous=first)
+    compare_levels(second, levels, ofr, exact=True)
+    # History changed something against a fresh second frame.
+    fresh = oracle.OracleFrame(oscene, second.to_c(), pos, nrm)
+    assert np.any(fresh.level(0, 16)[1] != ofr.level(0, 16)[1])
+
+
+def test_split_history_and_invalidation_match_oracle():
+    settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   frame_index=0).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    ctx, scene, view, st, levels, _ = run_frame("cornell", settings, pos, nrm)
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    prev = oracle.OracleFrame(oscene, settings.to_c(), pos, nrm)
+    box = np.array([-0.3, -0.1, -0.3, 0.3, 0.5, 0.3], np.float32)
+    for frame, dirty in ((1, None), (2, box)):
+        s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                frame_index=frame).sanitized()
+        if dirty is not None:
+            view.invalidate_bounds(dirty[:3], dirty[3:])
+        view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+        assert view.stats().error_flags == 0
+        cur = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prev,
+                                 dirty=None if dirty is None else dirty[None])
+        compare_levels(s, [view.read_level(l) for l in range(4)], cur, exact=False)
+        prev = cur
+    # reset_history: the next frame is fresh.
+    view.reset_history()
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                            frame_index=3).sanitized()
+    view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+    compare_levels(s, [view.read_level(l) for l in range(4)], oracle.OracleFrame(oscene, s.to_c(), pos, nrm),
+                   exact=False)

@@ -1,0 +1,129 @@
+"""World history (mergeEntry's bounded interval history,
+shaders/split.slang:1478-1521, :1624-1725) in the oracle: the temporal cases
+of gpu_split_merge_bounds_history_and_preserves_fractional_support
+(src/split_merge_tests.rs:36-70, asserted at :1306-1360, tolerance 2e-4),
+and history across oracle frames."""
+import numpy as np
+import pytest
+
+import bevy_penumbra_b200 as bp
+import oracle
+from tests.helpers import packed
+
+TOL = 2e-4
+
+
+def settings(radiance_blend, beta_blend):
+    s = bp.RadianceCascades(temporal_blend=radiance_blend, split_transmittance_blend=beta_blend,
+                            history_frames=30).to_c()
+    return s
+
+
+class Record:
+    """One cache entry advanced frame by frame (the KAT's advance())."""
+
+    def __init__(self, st):
+        self.st = st
+        self.raw = np.zeros(4, np.float32)
+        self.mass = np.zeros(2, np.float32)
+
+    def advance(self, radiance, beta, count):
+        self.raw, self.mass = oracle.history_blend(self.st, count, (radiance, radiance, radiance, beta),
+                                                   self.raw, self.mass)
+
+
+@pytest.mark.parametrize("j,beta", [(0.5, 0.75), (0.9, 0.95)])
+def test_temporal_cases(j, beta):
+    r = Record(settings(j, beta))
+    for _ in range(512):
+        r.advance(2.0, 0.0, 1)
+    # Masses saturate at 1 / (1 - blend).
+    assert abs(r.mass[0] - 1.0 / (1.0 - j)) < TOL
+    assert abs(r.mass[1] - 1.0 / (1.0 - beta)) < TOL
+    r.advance(0.0, 1.0, 1)
+    assert abs(r.raw[0] - 2.0 * j) < TOL
+    assert abs(r.raw[3] - (1.0 - beta)) < TOL
+    raw2, mass2 = r.raw.copy(), r.mass.copy()
+    for _ in range(200):
+        r.advance(0.0, 1.0, 0)
+    # Zero observations must not decay world state, mass or support.
+    np.testing.assert_array_equal(r.raw, raw2)
+    np.testing.assert_array_equal(r.mass, mass2)
+    # Batched observations consume retention per observation.
+    for _ in range(512):
+        r.advance(2.0, 0.0, 1)
+    r.advance(0.0, 1.0, 4)
+    assert abs(r.raw[0] - 2.0 * j ** 4) < TOL
+    assert abs(r.raw[3] - (1.0 - beta ** 4)) < TOL
+    assert abs(r.mass[0] - 1.0 / (1.0 - j)) < TOL
+    assert abs(r.mass[1] - 1.0 / (1.0 - beta)) < TOL
+
+
+def test_beta_only_and_radiance_only_history():
+    r = Record(settings(0.0, 0.9))
+    for _ in range(512):
+        r.advance(2.0, 0.0, 1)
+    r.advance(0.0, 1.0, 1)
+    assert abs(r.raw[0] - 0.0) < TOL and abs(r.raw[3] - 0.1) < TOL
+    for _ in range(200):
+        r.advance(0.0, 1.0, 0)
+    assert abs(r.mass[0] - 0.0) < TOL and abs(r.mass[1] - 10.0) < TOL
+    r = Record(settings(0.9, 0.0))
+    for _ in range(512):
+        r.advance(2.0, 0.0, 1)
+    r.advance(0.0, 1.0, 1)
+    assert abs(r.raw[0] - 1.8) < TOL and abs(r.raw[3] - 1.0) < TOL
+    for _ in range(200):
+        r.advance(0.0, 1.0, 0)
+    assert abs(r.mass[0] - 10.0) < TOL and abs(r.mass[1] - 0.0) < TOL
+
+
+def test_disabled_history_is_the_fresh_mean():
+    r = Record(settings(0.0, 0.0))
+    r.advance(2.0, 0.25, 3)
+    r.advance(1.0, 0.5, 2)
+    np.testing.assert_allclose(r.raw, [1.0, 1.0, 1.0, 0.5], rtol=0, atol=0)
+
+
+def cornell_receivers(n=24):
+    k = (np.arange(n, dtype=np.float32) + np.float32(0.5)) / np.float32(n) * np.float32(1.9) - np.float32(0.95)
+    x, z = np.meshgrid(k, k, indexing="ij")
+    pos = np.zeros((n * n, 4), np.float32)
+    pos[:, 0], pos[:, 2] = x.ravel(), z.ravel()
+    nrm = np.zeros_like(pos)
+    nrm[:, 1] = 1.0
+    return pos, nrm
+
+
+def test_oracle_frames_accumulate_history():
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=2,
+                            emissive_samples=4, temporal_blend=0.88, split_transmittance_blend=0.98,
+                            history_frames=24)
+    pos, nrm = cornell_receivers()
+    scene = oracle.OracleScene.from_packed(packed("cornell"))
+    f1 = oracle.OracleFrame(scene, s.sanitized().to_c(), pos, nrm)
+    s2 = s.sanitized()
+    s2.frame_index = 1
+    fresh = oracle.OracleFrame(scene, s2.to_c(), pos, nrm)
+    blended = oracle.OracleFrame(scene, s2.to_c(), pos, nrm, previous=f1)
+    dirs = s.direction_count(0)
+    k1, m1, r1, c1 = f1.level(0, dirs)
+    kf, mf, rf, cf = fresh.level(0, dirs)
+    kb, mb, rb, cb = blended.level(0, dirs)
+    np.testing.assert_array_equal(kf, kb)
+    np.testing.assert_array_equal(cf, cb)  # samples are this frame's
+    seen = (c1 > 0) & (cf > 0)
+    # Records observed in both frames mix the two frames' means.
+    lo = np.minimum(r1[seen][:, :3], rf[seen][:, :3]) - 1e-6
+    hi = np.maximum(r1[seen][:, :3], rf[seen][:, :3]) + 1e-6
+    assert np.all((rb[seen][:, :3] >= lo) & (rb[seen][:, :3] <= hi))
+    assert np.any(np.abs(rb[seen][:, :3] - rf[seen][:, :3]) > 1e-4)
+    # Records seen only before keep their history in the blended frame.
+    kept = (c1 > 0) & (cf == 0)
+    if kept.any():
+        np.testing.assert_array_equal(rb[kept], r1[kept])
+    # An invalidation box over the whole scene leaves only fresh data.
+    reset = oracle.OracleFrame(scene, s2.to_c(), pos, nrm, previous=f1, dirty=[[-10, -10, -10, 10, 10, 10]])
+    kr, mr, rr, cr = reset.level(0, dirs)
+    np.testing.assert_array_equal(rr, rf)
+    np.testing.assert_array_equal(mr, mf)
