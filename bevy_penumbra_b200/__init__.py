@@ -273,6 +273,15 @@ class PackedScene:
             L.lux_packed_scene_destroy(handle)
         return PackedScene(scene_words, geometry_words, lights, order, cost.value, depth.value, tn.value, bn.value)
 
+    def lights_at(self, world_from_local_slots) -> np.ndarray:
+        """lux_emissive_lights_at: this scene's emissive light records at new
+        rigid poses (float[instances, 3, 4] in instance-record order)."""
+        m = np.ascontiguousarray(world_from_local_slots, dtype=np.float32).reshape(-1, 12)
+        out = np.zeros_like(self.lights)
+        check(lib().lux_emissive_lights_at(_ptr(self.geometry_words), len(self.geometry_words), _ptr(self.lights),
+                                           len(self.lights), _ptr(m), len(m), _ptr(out)))
+        return out
+
     @staticmethod
     def from_desc(desc) -> "PackedScene":
         positions, indices, first, count = desc.arrays()

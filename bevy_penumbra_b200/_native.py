@@ -156,6 +156,7 @@ SIGNATURES = {
     "lux_scene_upload": (C.c_int, [P, P, SZ, P, SZ, P, U32, U32, C.POINTER(P)]),
     "lux_scene_destroy": (C.c_int, [P]),
     "lux_scene_refit": (C.c_int, [P, P, U32, P, U32]),
+    "lux_emissive_lights_at": (C.c_int, [P, SZ, P, U32, P, U32, P]),
     "lux_scene_read_words": (C.c_int, [P, P, SZ]),
     "lux_scene_layout": (C.c_int, [P, C.POINTER(U32), C.POINTER(U32), C.POINTER(U32), C.POINTER(U32),
                                    C.POINTER(U32)]),

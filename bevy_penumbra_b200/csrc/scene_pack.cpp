@@ -527,3 +527,62 @@ bool lux_affine_inverse(const float m[12], float out[12]) {
     }
     return true;
 }
+
+// Emissive light records of a rigidly moved scene (build_emissive_lights,
+// src/scene.rs:2311-2372, at new instance poses): each record's triangle
+// (source.y, packed order) is re-transformed by its instance's new
+// world_from_local (source.x, slot order) with the packer's arithmetic;
+// position, edges and the facing normal change, while the area, power and
+// CDF fields stay those of the given records (rigid motion keeps areas).
+extern "C" lux_status lux_emissive_lights_at(const uint32_t *gw, size_t gn, const LuxLight *lights,
+                                             uint32_t light_count, const float *world_from_local,
+                                             uint32_t instance_count, LuxLight *out) {
+    if ((light_count && (!lights || !out)) || !gw || gn < 1 || (instance_count && !world_from_local))
+        return LUX_ERR_INVALID_ARGUMENT;
+    uint32_t vertex_base = gw[1], vertex_stride = gw[2], vertex_count = gw[3];
+    if (gw[0] != 1u || vertex_stride != 5u || (uint64_t)vertex_base + (uint64_t)vertex_count * 5u > gn)
+        return LUX_ERR_MALFORMED_SCENE;
+    for (uint32_t k = 0; k < light_count; ++k) {
+        const LuxLight &L = lights[k];
+        uint32_t slot = L.source[0], t = L.source[1];
+        if (slot >= instance_count || 1u + (uint64_t)t >= vertex_base) return LUX_ERR_MALFORMED_SCENE;
+        const float *m = world_from_local + 12 * (size_t)slot;
+        double w64[3][4];
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) w64[r][c] = m[4 * r + c];
+        const uint32_t *idx = gw + 4 * (size_t)(1 + t);
+        float w[3][3];
+        for (int v = 0; v < 3; ++v) {
+            if (idx[v] >= vertex_count) return LUX_ERR_MALFORMED_SCENE;
+            const uint32_t *pw = gw + 4 * ((size_t)vertex_base + (size_t)idx[v] * 5u);
+            float p[3];
+            std::memcpy(p, pw, 12);
+            for (int r = 0; r < 3; ++r)
+                w[v][r] = (float)(w64[r][0] * p[0] + w64[r][1] * p[1] + w64[r][2] * p[2] + w64[r][3]);
+        }
+        double e1[3], e2[3];
+        for (int r = 0; r < 3; ++r) {
+            e1[r] = (double)w[1][r] - w[0][r];
+            e2[r] = (double)w[2][r] - w[0][r];
+        }
+        double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+        double len = std::sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        LuxLight o = L;
+        // The facing sign the packer chose: the old normal's orientation
+        // relative to the old edges' cross product.
+        double old_cr[3] = {(double)L.edge1[1] * L.edge2[2] - (double)L.edge1[2] * L.edge2[1],
+                            (double)L.edge1[2] * L.edge2[0] - (double)L.edge1[0] * L.edge2[2],
+                            (double)L.edge1[0] * L.edge2[1] - (double)L.edge1[1] * L.edge2[0]};
+        double sign = old_cr[0] * L.direction[0] + old_cr[1] * L.direction[1] + old_cr[2] * L.direction[2] < 0.0
+                          ? -1.0
+                          : 1.0;
+        for (int r = 0; r < 3; ++r) {
+            o.position[r] = w[0][r];
+            o.direction[r] = len > 0.0 ? (float)(cr[r] / len * sign) : L.direction[r];
+            o.edge1[r] = (float)e1[r];
+            o.edge2[r] = (float)e2[r];
+        }
+        out[k] = o;
+    }
+    return LUX_OK;
+}

@@ -227,6 +227,15 @@ lux_status lux_packed_scene_instance_order(const LuxPackedScene *p, uint32_t *or
 lux_status lux_packed_scene_quality(const LuxPackedScene *p, double *blas_cost,
                                     uint32_t *max_depth);
 void lux_packed_scene_destroy(LuxPackedScene *p);
+/* Emissive light records after a rigid pose update (moving emitters, for
+ * lux_scene_refit's `lights`): every record's triangle is re-transformed by
+ * its instance's new world_from_local (host float[instance_count * 12] in
+ * instance-record order) exactly as the packer transforms it
+ * (build_emissive_lights, src/scene.rs:2311-2372); areas, power and the CDF
+ * stay those of `lights`.  out: host LuxLight[light_count]. */
+lux_status lux_emissive_lights_at(const uint32_t *geometry_words, size_t geometry_word_count,
+                                  const LuxLight *lights, uint32_t light_count,
+                                  const float *world_from_local, uint32_t instance_count, LuxLight *out);
 
 /* Uploads word streams (host pointers) and builds the device BVH4 layout.
  * scene_words = [header, TLAS node words, BLAS node words, instance words,

@@ -81,3 +81,30 @@ def test_oracle_refit_round_trip_restores_words():
     lo1, hi1 = words[1, :3].view(np.float32), words[2, :3].view(np.float32)
     assert n_tlas > 2
     assert np.all(lo1 <= lo0 + 1e-4) and np.all(hi1 >= hi0 - 1e-4)
+
+
+def test_emissive_lights_follow_moved_emitters():
+    """lux_emissive_lights_at at a new pose gives the records a fresh pack at
+    that pose builds (position, normal, edges), keeping the CDF."""
+    name = "atrium65536"
+    desc = scene_desc(name)
+    p0 = packed(name)
+    emitters = [i for i in range(len(desc.instance_mesh)) if desc.instance_mesh[i] == 3]
+    assert len(emitters) == 3
+    moved = move_instances(desc, seed=31, select=lambda i: i in emitters)
+    lights = p0.lights_at(slot_transforms(moved, p0))
+    p1 = bp.PackedScene.from_desc(moved)
+    def records(p, lt):
+        flat = np.ascontiguousarray(lt).view(np.float32).reshape(len(lt), 24)
+        src = np.ascontiguousarray(lt).view(np.uint32).reshape(len(lt), 24)[:, 20:22]
+        return {(int(p.instance_order[s]), int(t)): flat[k] for k, (s, t) in enumerate(src)}
+    a, b = records(p0, lights), records(p1, p1.lights)
+    assert set(a) == set(b) and len(a) > 0
+    for key in a:
+        np.testing.assert_array_equal(a[key][0:3], b[key][0:3])      # position
+        np.testing.assert_array_equal(a[key][8:11], b[key][8:11])    # direction (facing normal)
+        np.testing.assert_array_equal(a[key][12:15], b[key][12:15])  # edge1
+        np.testing.assert_array_equal(a[key][16:19], b[key][16:19])  # edge2
+    # Unmoved records (and every CDF field) are unchanged.
+    np.testing.assert_array_equal(np.ascontiguousarray(lights).view(np.float32).reshape(-1, 24)[:, [11, 15, 7]],
+                                  np.ascontiguousarray(p0.lights).view(np.float32).reshape(-1, 24)[:, [11, 15, 7]])
