@@ -19,6 +19,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -628,14 +629,209 @@ def run_batched(args, rank, world):
         print(json.dumps(line), flush=True)
 
 
+FULL_VIEWS = [((-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)), ((17.0, 3.5, -15.0), (-4.0, 4.0, 6.0)),
+              ((-17.0, 4.0, 15.0), (4.0, 3.0, -6.0)), ((17.0, 3.0, 15.0), (-4.0, 4.0, -6.0))]
+FULL_WIDTH, FULL_HEIGHT, FULL_FPS = 1920, 1080, 60.0
+
+
+def primary_receivers(bp, ctx, scene, packed, eye, target, width, height, stride, device):
+    """World-space primary hits (position, facing normal) through every
+    stride-th pixel block of a camera (the G-buffer receivers)."""
+    import torch
+
+    from bevy_penumbra_b200 import scenes
+    o, d = scenes.camera_rays(width, height, eye, target, 60.0, stride)
+    rays = np.zeros(len(o), dtype=bp.RAY_DTYPE)
+    rays["origin"], rays["direction"], rays["limit"] = o, d, 1e20
+    dev = f"cuda:{device}"
+    d_rays = torch.from_numpy(rays.view(np.uint8).copy()).to(dev)
+    d_hits = torch.zeros(len(rays) * bp.HIT_DTYPE.itemsize, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(device)
+    bp.trace_rays(ctx, scene, d_rays.data_ptr(), len(rays), d_hits.data_ptr())
+    hits = d_hits.cpu().numpy().view(bp.HIT_DTYPE)
+    ok = hits["triangle"] != 0xFFFFFFFF
+    pos = np.zeros((int(ok.sum()), 4), np.float32)
+    pos[:, :3] = o[ok] + d[ok] * hits["distance"][ok, None]
+    nrm = np.zeros_like(pos)
+    nrm[:, :3] = world_normals(packed, hits[ok], d[ok])
+    return pos, nrm
+
+
+def run_full(args, rank, world):
+    """--workload full: a 1,048,576-triangle scene whose 4 emitters move on
+    circles at 0.5 m/s (60 frames per second) and whose 8 rigid boxes move in
+    turn every 30 frames, seen by 4 views at 1920x1080 (receivers at 4x4 px);
+    every frame refits the TLAS with the new poses and emitter records, the
+    views invalidate history around what moved, and trace+merge runs per
+    view.  The plain form runs all frames, then the learned-cache form replays
+    the same motion; the final frame of each is compared with a 4096-spp FP64
+    reference on every 64th receiver of every view."""
+    import torch
+
+    import bevy_penumbra_b200 as bp
+    from bevy_penumbra_b200 import scenes
+
+    device = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(device)
+    work_stream = torch.cuda.Stream(device)
+    torch.cuda.set_stream(work_stream)
+    stream = torch.cuda.current_stream(device)
+    dev = f"cuda:{device}"
+    t0 = time.time()
+    desc, emitters, boxes = scenes.full_scene(5, 1 << 20)
+    packed = bp.PackedScene.from_desc(desc)
+    ctx = bp.LuxContext(device, stream.cuda_stream)
+    scene = bp.GpuScene(ctx, packed)
+    slot_of = np.empty(len(packed.instance_order), np.int64)
+    slot_of[packed.instance_order.astype(np.int64)] = np.arange(len(packed.instance_order))
+    base = np.stack([desc.instance_transform[int(i)] for i in packed.instance_order]).astype(np.float64)
+    orbits = scenes.emitter_orbits(desc, emitters)
+    box_rng = np.random.default_rng(55)
+    box_steps = [box_rng.uniform(-0.6, 0.6, size=3) * (1.0, 0.0, 1.0) for _ in range(64)]
+    settings = settings_for_workload()
+    mesh_lo = {m: desc.meshes[m].positions.min(0) for m in set(desc.instance_mesh)}
+    mesh_hi = {m: desc.meshes[m].positions.max(0) for m in set(desc.instance_mesh)}
+
+    def world_box(inst, m):
+        lo, hi = mesh_lo[desc.instance_mesh[inst]], mesh_hi[desc.instance_mesh[inst]]
+        corners = np.array([[x, y, z] for x in (lo[0], hi[0]) for y in (lo[1], hi[1]) for z in (lo[2], hi[2])])
+        w = corners @ m[:, :3].T + m[:, 3]
+        return w.min(0), w.max(0)
+
+    def poses(frame):
+        """Slot-ordered poses at `frame`, and the (instance, old, new) moves."""
+        cur = base.copy()
+        t = frame / FULL_FPS
+        for (c, r, phase, sign), inst in zip(orbits, emitters):
+            a = phase + sign * 0.5 * t / r
+            cur[slot_of[inst], :, 3] = c + r * np.array([math.cos(a), 0.0, math.sin(a)])
+        for k in range(frame // 30):
+            inst = boxes[k % len(boxes)]
+            cur[slot_of[inst], :, 3] += box_steps[k % len(box_steps)]
+        return cur
+
+    stride = PROBE_PX
+    # Views sized for the receivers of the first frame with headroom (moved
+    # boxes change the receiver set a little).
+    recv = [primary_receivers(bp, ctx, scene, packed, e, tgt, FULL_WIDTH, FULL_HEIGHT, stride, device)
+            for e, tgt in FULL_VIEWS]
+    views = []
+    for pos, _ in recv:
+        entries, cells_max = 0, 1
+        for level in range(settings.levels):
+            sp = np.float32(settings.probe_spacing * (1 << level))
+            cells = np.unique(np.floor(pos[:, :3] / sp).astype(np.int64), axis=0).shape[0]
+            cells_max = max(cells_max, int(cells * 1.25) + 64)
+            entries += int(cells * 1.25 + 64) * settings.direction_count(level)
+        views.append(bp.SplitView(ctx, max_receivers=int(len(pos) * 1.1), max_cells=cells_max,
+                                  max_entries=entries, max_rays=int(len(pos) * 1.1) * settings.rays_per_receiver))
+    setup_s = time.time() - t0
+
+    def receivers_now():
+        rec = [primary_receivers(bp, ctx, scene, packed, e, tgt, FULL_WIDTH, FULL_HEIGHT, stride, device)
+               for e, tgt in FULL_VIEWS]
+        out = []
+        for v, (p, nm) in zip(views, rec):
+            n = min(len(p), int(v.desc.max_receivers))
+            out.append((torch.from_numpy(p[:n]).to(dev), torch.from_numpy(nm[:n]).to(dev), n))
+        return out
+
+    def run_form(cache):
+        for v in views:
+            v.reset_history()
+            if cache is None:
+                v.set_cache(None)
+            else:
+                v.set_cache(cache, cutoff_level=args.cache_cutoff, validate_period=16, error_bound=args.cache_bound,
+                            train_samples=65536, fallback_frames=16)
+        prev = poses(0)
+        scene.refit(prev, lights=packed.lights_at(prev))
+        d_rec = receivers_now()
+        ms, rays = [], 0
+        for frame in range(args.frames):
+            cur = poses(frame)
+            moved = [i for i in range(len(cur)) if not np.array_equal(cur[i], prev[i])]
+            box_moved = any(int(packed.instance_order[sl]) in boxes for sl in moved)
+            if box_moved:
+                # A rigid box moved: refit, then the G-buffer (receivers) changes.
+                scene.refit(cur, lights=packed.lights_at(cur))
+                d_rec = receivers_now()
+            start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            if moved and not box_moved:
+                scene.refit(cur, lights=packed.lights_at(cur))
+            for slot in moved:
+                inst = int(packed.instance_order[slot])
+                lo0, hi0 = world_box(inst, prev[slot])
+                lo1, hi1 = world_box(inst, cur[slot])
+                for v in views:
+                    v.invalidate_bounds(np.minimum(lo0, lo1), np.maximum(hi0, hi1))
+            settings.frame_index = frame
+            for v, (p, nm, n) in zip(views, d_rec):
+                v.trace_merge(scene, settings, p.data_ptr(), nm.data_ptr(), n)
+            end.record(stream)
+            torch.cuda.synchronize(device)
+            if frame >= 10:
+                ms.append(start.elapsed_time(end))
+            rays = sum(n for _, _, n in d_rec) * settings.rays_per_receiver
+            prev = cur
+        for v in views:
+            if v.stats().error_flags:
+                raise RuntimeError("full form: a view's capacity was exceeded")
+        # FP64 reference on every 64th receiver of every view (final pose).
+        errs = []
+        for v, (p, nm, n) in zip(views, d_rec):
+            sub = torch.arange(0, n, 64, device=dev)
+            s_pos, s_nrm = p[sub].contiguous(), nm[sub].contiguous()
+            out = torch.empty((len(sub), 4), dtype=torch.float32, device=dev)
+            v.resolve(settings, s_pos.data_ptr(), s_nrm.data_ptr(), len(sub), out.data_ptr())
+            ref = torch.zeros((len(sub), 4), dtype=torch.float64, device=dev)
+            bp.reference_irradiance(ctx, scene, settings, s_pos.data_ptr(), s_nrm.data_ptr(), len(sub), 4096, 7,
+                                    ref.data_ptr())
+            errs.append((out, ref))
+        est = torch.cat([e for e, _ in errs]).contiguous()
+        ref = torch.cat([r for _, r in errs]).contiguous()
+        err = bp.error_stats(ctx, est.data_ptr(), ref.data_ptr(), len(est))
+        frame_ms = float(np.mean(ms))
+        return {"ms_per_frame": frame_ms, "value": rays / (frame_ms * 1e-3) / 1e6, "interval_rays_per_frame": rays,
+                "relative_rmse": err["relative_rmse"], "rmse": err["rmse"], "points": err["points"]}
+
+    with ClockSampler(device) as clocks:
+        plain = run_form(None)
+        cache = bp.LearnedCache(ctx)
+        lo = np.min([p[:, :3].min(0) for p, _ in recv], axis=0) - 1.0
+        hi = np.max([p[:, :3].max(0) for p, _ in recv], axis=0) + 1.0
+        cache.set_bounds(lo, hi)
+        learned = run_form(cache)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": world * plain["value"], "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.frames, "warmup": 10, "ms_per_step": plain["ms_per_frame"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "full: 1,048,576 tris, 4 emitters on circles at 0.5 m/s, 8 rigid boxes moved in "
+                                   "turn every 30 frames, 4 views at 1920x1080 (receivers at 4x4 px), 8 cascades",
+                       "frames": args.frames, "fps": FULL_FPS, "views": len(views),
+                       "interval_rays_per_frame": plain["interval_rays_per_frame"],
+                       "reference": "4096-spp FP64 reference on every 64th receiver, final frame"},
+            "plain": plain,
+            "learned": dict(learned, speedup_vs_plain=plain["ms_per_frame"] / learned["ms_per_frame"],
+                            rmse_change=learned["relative_rmse"] / plain["relative_rmse"] - 1.0,
+                            cutoff_level=args.cache_cutoff, error_bound=args.cache_bound),
+            "clocks": clocks.summary(), "setup_s": setup_s,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="atrium", choices=["atrium", "batched"],
-                    help="atrium: the headline frame; batched: 64 scenes per step through lux_batch_trace_merge")
+    ap.add_argument("--workload", default="atrium", choices=["atrium", "batched", "full"],
+                    help="atrium: the headline frame; batched: 64 scenes per step through lux_batch_trace_merge; "
+                         "full: moving emitters and boxes, 4 views at 1080p, plain and learned forms")
+    ap.add_argument("--frames", type=int, default=600, help="full workload: frames of motion")
     ap.add_argument("--cache-cutoff", type=int, default=LEARNED_CUTOFF,
                     help="learned-cache form: first cascade answered by the cache")
     ap.add_argument("--cache-bound", type=float, default=8.0,
@@ -653,6 +849,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "batched":
         run_batched(args, rank, world)
+    elif args.workload == "full":
+        run_full(args, rank, world)
     else:
         run_ours(args, rank, world)
 

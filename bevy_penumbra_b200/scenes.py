@@ -263,6 +263,76 @@ def atrium(seed: int = 2, triangles: int = 262_144) -> SceneDesc:
     return sc
 
 
+def full_scene(seed: int = 5, triangles: int = 1_048_576):
+    """The full-form scene: the atrium layout at ``triangles`` world triangles
+    with four emitters (radiance U[5, 20]) and eight rigid boxes on the floor.
+    Returns (desc, emitter instances, box instances)."""
+    rng = np.random.default_rng(seed)
+    sc = SceneDesc(name="full")
+    jit = lambda: rng.uniform(-0.02, 0.02, size=3)
+
+    def albedo_material():
+        return sc.add_material(material_words(tuple(rng.uniform(0.2, 0.8, size=3))))
+
+    column = sc.add_mesh(cylinder_mesh(0.3, 6.0, 32, 16))
+    arch = sc.add_mesh(arch_mesh(4.0, 0.4, 0.6, 60))
+    tile = sc.add_mesh(box_mesh((0.98, 0.05, 0.98), bottom=False))
+    emitter_mesh = sc.add_mesh(quad((-1.0, 0.0, -1.0), (1.0, 0.0, -1.0), (1.0, 0.0, 1.0), (-1.0, 0.0, 1.0)))
+    box = sc.add_mesh(box_mesh((1.2, 1.2, 1.2), bottom=False))
+    pitch, n, tiles = 4.0, 10, 40
+    for i in range(n):
+        for j in range(n):
+            t = np.eye(3, 4, dtype=np.float64)
+            t[:, 3] = ((i - (n - 1) / 2) * pitch, 0.0, (j - (n - 1) / 2) * pitch) + jit()
+            sc.add_instance(column, t, material=albedo_material())
+    for i in range(n - 1):
+        for j in range(n):
+            cx = (i + 0.5 - (n - 1) / 2) * pitch
+            cz = (j - (n - 1) / 2) * pitch
+            sc.add_instance(arch, rotation_y(0.0, (cx, 6.0, cz)) + _jit3(jit), material=albedo_material())
+            sc.add_instance(arch, rotation_y(math.pi / 2, (cz, 6.0, cx)) + _jit3(jit), material=albedo_material())
+    for i in range(tiles):
+        for j in range(tiles):
+            t = np.eye(3, 4, dtype=np.float64)
+            t[:, 3] = (i - (tiles - 1) / 2, -0.05, j - (tiles - 1) / 2) + jit()
+            sc.add_instance(tile, t, material=albedo_material())
+    emitters = []
+    for k in range(4):
+        radiance = float(rng.uniform(5.0, 20.0))
+        mat = sc.add_material(material_words((0.0, 0.0, 0.0), emission=(radiance, radiance, radiance)))
+        t = np.eye(3, 4, dtype=np.float64)
+        t[:, 3] = (rng.uniform(-12.0, 12.0), 9.5, rng.uniform(-12.0, 12.0))
+        emitters.append(len(sc.instance_mesh))
+        sc.add_instance(emitter_mesh, t, material=mat)
+    boxes = []
+    for k in range(8):
+        boxes.append(len(sc.instance_mesh))
+        sc.add_instance(box, rotation_y(float(rng.uniform(0, 2 * math.pi)),
+                                        (float(rng.uniform(-16, 16)), 0.0, float(rng.uniform(-16, 16)))),
+                        material=albedo_material())
+    remaining = triangles - sc.world_triangles()
+    if remaining < 2 or remaining % 2:
+        raise ValueError(f"full scene triangle budget {triangles} cannot be met (remaining {remaining})")
+    extent = pitch * n + 4.0
+    ceiling = sc.add_mesh(grid_mesh(remaining // 2, extent, extent, 10.0, rng, 0.02))
+    sc.add_instance(ceiling, material=albedo_material())
+    assert sc.world_triangles() == triangles, (sc.world_triangles(), triangles)
+    return sc, emitters, boxes
+
+
+def emitter_orbits(desc: SceneDesc, emitters, seed: int = 5):
+    """Seeded circular paths of the emitters at 0.5 m/s: (centre, radius,
+    phase, direction) per emitter; the pose at time t is
+    centre + radius (cos, 0, sin)(phase + direction 0.5 t / radius)."""
+    rng = np.random.default_rng(seed + 1000)
+    orbits = []
+    for i in emitters:
+        c = desc.instance_transform[i][:, 3].astype(np.float64)
+        r = float(rng.uniform(2.0, 5.0))
+        orbits.append((c, r, float(rng.uniform(0, 2 * math.pi)), 1.0 if rng.uniform() < 0.5 else -1.0))
+    return orbits
+
+
 def batch_scene(seed: int, triangles: int) -> SceneDesc:
     """One scene of the batched workload: a floor, 1-3 downward emitters
     (radiance U[5, 20]), seeded boxes and columns on the floor and a jittered
