@@ -227,6 +227,11 @@ LUX_HD uint64_t pack_cell(int32_t x, int32_t y, int32_t z) {
            ((uint64_t)((uint32_t)(y + (1 << 20)) & 0x1fffffu) << 21) |
            ((uint64_t)((uint32_t)(z + (1 << 20)) & 0x1fffffu) << 42);
 }
+LUX_HD void unpack_cell(uint64_t key, int32_t &x, int32_t &y, int32_t &z) {
+    x = (int32_t)(key & 0x1fffffull) - (1 << 20);
+    y = (int32_t)((key >> 21) & 0x1fffffull) - (1 << 20);
+    z = (int32_t)((key >> 42) & 0x1fffffull) - (1 << 20);
+}
 LUX_HD bool cell_in_range(int32_t x, int32_t y, int32_t z) {
     const int32_t lim = 1 << 20;
     return x >= -lim && x < lim && y >= -lim && y < lim && z >= -lim && z < lim;

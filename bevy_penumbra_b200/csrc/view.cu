@@ -50,6 +50,7 @@ namespace {
 using lux::f3;
 
 constexpr int kMaxDirty = 8;  // invalidation boxes per frame (more are merged into their union)
+constexpr uint32_t kRetainBins = 256;  // age classes of retained cells (older cells share the last)
 
 // The previous frame's records: its cell directories, record offsets, and
 // blended raw records with their masses (swapped with the current frame's
@@ -61,6 +62,8 @@ struct HistoryDevice {
     const uint32_t *cell_count;
     const float4 *raw;
     const float2 *mass;
+    const uint32_t *cell_last;  // [levels][cell_capacity] frame of each cell's last receiver
+    const int4 *cell_keys;      // [levels][cell_capacity]
 };
 
 struct FrameParams {
@@ -97,6 +100,9 @@ struct ViewDevice {
     float4 *raw;                    // [entries] J rgb, beta (history-blended)
     float2 *mass;                   // [entries] radiance mass, transmittance mass
     uint32_t *hist_cell;            // [levels][cell_capacity] the previous frame's id of each cell, or kEmpty
+    uint32_t *cell_last;            // [levels][cell_capacity] frame index of the cell's last receiver
+    uint32_t *retain_hist;          // [levels][kRetainBins] retain candidates per age class
+    uint32_t *retain_limit;         // [levels] age classes below this are retained
     float4 *tables;                 // [cell_capacity][36]
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
@@ -241,10 +247,10 @@ __global__ void seed_assign_kernel(ViewDevice V, FrameParams F) {
             continue;
         }
         V.dir_ids[i] = id;
-        int32_t x = (int32_t)(key & 0x1fffffull) - (1 << 20);
-        int32_t y = (int32_t)((key >> 21) & 0x1fffffull) - (1 << 20);
-        int32_t z = (int32_t)((key >> 42) & 0x1fffffull) - (1 << 20);
+        int32_t x, y, z;
+        lux::unpack_cell(key, x, y, z);
         V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)(level << 12));
+        V.cell_last[(size_t)level * F.cell_capacity + id] = F.shade.frame;
     }
 }
 
@@ -842,6 +848,90 @@ __device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t leve
         if (meet) return true;
     }
     return false;
+}
+
+// retain (shaders/split.slang:991-1054): with history on, the world cache is
+// persistent (persistentWorldIntervals, shaders/common.slang:82-89, is set
+// for the Split method at src/render.rs:8470), so every cell of the previous
+// frame that no receiver seeded this frame stays in the cache with its
+// records, which the merge carries forward unchanged (no fresh samples) and
+// which parents and the resolve keep reading.  A cell whose history an
+// invalidation box voids is dropped (betaHistoryEligible).  Capacity bounds
+// the cache as commitCache's per-bucket quota does (youngest kept,
+// :1919-1961): levels in order, whole age classes (frames since the cell's
+// last receiver) youngest first, while the cells fit max_cells and all
+// records the view's max_entries.
+// Age class of the previous frame's cell `prev` of `level`, or kRetainBins
+// when it is not retained (seeded this frame, or its history voided).
+__device__ __forceinline__ uint32_t retain_bin(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                               uint32_t level, uint32_t prev, int4 &key) {
+    key = H.cell_keys[(size_t)level * F.cell_capacity + prev];
+    if (dir_find(V, F, level, key.x, key.y, key.z) != lux::kEmpty) return kRetainBins;  // seeded this frame
+    if (record_dirty(F, level, key)) return kRetainBins;
+    uint32_t age = F.shade.frame - H.cell_last[(size_t)level * F.cell_capacity + prev];
+    return min(age, kRetainBins - 1u);
+}
+
+__global__ void retain_count_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        uint32_t cells = min(H.cell_count[l], F.cell_capacity);
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+            int4 key;
+            uint32_t bin = retain_bin(V, F, H, l, c, key);
+            if (bin < kRetainBins) atomicAdd(&V.retain_hist[l * kRetainBins + bin], 1u);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) retain_limit_kernel(ViewDevice V, FrameParams F) {
+    __shared__ uint32_t hist[LUX_MAX_LEVELS * kRetainBins];
+    for (uint32_t i = threadIdx.x; i < F.levels * kRetainBins; i += blockDim.x) hist[i] = V.retain_hist[i];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    unsigned long long used = 0;
+    for (uint32_t l = 0; l < F.levels; ++l)
+        used += (unsigned long long)min(V.cell_count[l], F.cell_capacity) * F.dirs[l];
+    unsigned long long remaining = used < F.entry_capacity ? F.entry_capacity - used : 0ull;
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        unsigned long long seeded = min(V.cell_count[l], F.cell_capacity);
+        unsigned long long room = min((unsigned long long)F.cell_capacity - seeded, remaining / F.dirs[l]);
+        unsigned long long kept = 0;
+        uint32_t a = 0;
+        while (a < kRetainBins && kept + hist[l * kRetainBins + a] <= room) kept += hist[l * kRetainBins + a++];
+        V.retain_limit[l] = a;
+        remaining -= kept * F.dirs[l];
+    }
+}
+
+// Inserts the retained cell `prev` of `level` into this frame's directory
+// with a new dense id and its last-receiver frame.
+__device__ __forceinline__ void retain_cell(ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                            uint32_t level, uint32_t prev, int4 k) {
+    unsigned long long key = lux::pack_cell(k.x, k.y, k.z);
+    unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
+    uint32_t slot = lux::hash_key(k.x, k.y, k.z, (int32_t)level, F.dir_capacity);
+    // The directory is at most half full (dir_capacity >= 2 max_cells).
+    for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+        if (atomicCAS(&keys[slot], lux::kEmptyCell, key) == lux::kEmptyCell) {
+            uint32_t id = atomicAdd(&V.cell_count[level], 1u);  // below cell_capacity by retain_limit
+            V.dir_ids[(size_t)level * F.dir_capacity + slot] = id;
+            V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(k.x, k.y, k.z, (int32_t)(level << 12));
+            V.cell_last[(size_t)level * F.cell_capacity + id] = H.cell_last[(size_t)level * F.cell_capacity + prev];
+            return;
+        }
+        slot = (slot + 1u) & (F.dir_capacity - 1u);
+    }
+    atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+}
+
+__global__ void retain_insert_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        uint32_t cells = min(H.cell_count[l], F.cell_capacity);
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+            int4 key;
+            if (retain_bin(V, F, H, l, c, key) < V.retain_limit[l]) retain_cell(V, F, H, l, c, key);
+        }
+    }
 }
 
 // mergeEntry (shaders/split.slang:1624-1725) for one record: the fresh mean
@@ -1540,6 +1630,8 @@ struct LuxView {
         uint32_t *cell_count = nullptr;
         float4 *raw = nullptr;
         float2 *mass = nullptr;
+        uint32_t *cell_last = nullptr;
+        int4 *cell_keys = nullptr;
     } hist;
     bool hist_valid = false;
     uint32_t hist_levels = 0;
@@ -1586,6 +1678,11 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.raw, (size_t)d.max_entries * sizeof(float4)},
         {(void **)&D.mass, (size_t)d.max_entries * sizeof(float2)},
         {(void **)&D.hist_cell, L * (size_t)d.max_cells * sizeof(uint32_t)},
+        {(void **)&D.cell_last, L * (size_t)d.max_cells * sizeof(uint32_t)},
+        {(void **)&v->hist.cell_last, L * (size_t)d.max_cells * sizeof(uint32_t)},
+        {(void **)&v->hist.cell_keys, L * (size_t)d.max_cells * sizeof(int4)},
+        {(void **)&D.retain_hist, L * kRetainBins * sizeof(uint32_t)},
+        {(void **)&D.retain_limit, L * sizeof(uint32_t)},
         {(void **)&v->hist.dir_keys, L * v->dir_capacity * sizeof(unsigned long long)},
         {(void **)&v->hist.dir_ids, L * v->dir_capacity * sizeof(uint32_t)},
         {(void **)&v->hist.level_base, L * sizeof(unsigned long long)},
@@ -1647,10 +1744,10 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     if (!v) return LUX_OK;
     ViewDevice &D = v->dev;
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
-                    D.corner_frac, D.accum, D.count, D.merged, D.raw, D.mass, D.hist_cell, D.tables, D.error_flags,
-                    D.stats,
+                    D.corner_frac, D.accum, D.count, D.merged, D.raw, D.mass, D.hist_cell, D.cell_last,
+                    D.retain_hist, D.retain_limit, D.tables, D.error_flags, D.stats,
                     v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
-                    v->hist.mass,
+                    v->hist.mass, v->hist.cell_last, v->hist.cell_keys,
                     D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
                     D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
@@ -1765,6 +1862,11 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
 
 // seed -> layout: the receivers' cells of every level, dense ids, record
 // offsets, cleared records (clear .. prefix, shaders/split.slang:734-983).
+static HistoryDevice history_device(const LuxView *v) {
+    return HistoryDevice{v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count,
+                         v->hist.raw,      v->hist.mass,    v->hist.cell_last, v->hist.cell_keys};
+}
+
 static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, cudaStream_t st) {
     const ViewDevice &D = v->dev;
     const int grid = v->ctx->sm_count * 8;
@@ -1773,6 +1875,13 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
         seed_insert_kernel<<<grid, 256, 0, st>>>(D, F, pos);
         seed_assign_kernel<<<grid, 256, 0, st>>>(D, F);
         seed_lookup_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+    }
+    if (F.history && F.layout == LUX_LAYOUT_SPLIT) {  // retain: the previous frame's unseen cells stay
+        const HistoryDevice H = history_device(v);
+        cudaMemsetAsync(D.retain_hist, 0, (size_t)LUX_MAX_LEVELS * kRetainBins * sizeof(uint32_t), st);
+        retain_count_kernel<<<grid, 256, 0, st>>>(D, F, H);
+        retain_limit_kernel<<<1, 256, 0, st>>>(D, F);
+        retain_insert_kernel<<<grid, 256, 0, st>>>(D, F, H);
     }
     layout_kernel<<<1, 32, 0, st>>>(D, F);
     clear_entries_kernel<<<grid, 256, 0, st>>>(D, F);
@@ -1783,8 +1892,7 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
 static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     const ViewDevice &D = v->dev;
     const int grid = v->ctx->sm_count * 8;
-    HistoryDevice H{v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
-                    v->hist.mass};
+    const HistoryDevice H = history_device(v);
     for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
     if (F.history)
         for (uint32_t l = 0; l < F.levels; ++l) history_map_kernel<<<grid, 128, 0, st>>>(D, F, H, l);
@@ -1807,6 +1915,8 @@ static void begin_history(LuxView *v, FrameParams &F, const LuxSettings &s) {
         std::swap(D.cell_count, v->hist.cell_count);
         std::swap(D.raw, v->hist.raw);
         std::swap(D.mass, v->hist.mass);
+        std::swap(D.cell_last, v->hist.cell_last);
+        std::swap(D.cell_keys, v->hist.cell_keys);
         ++v->generation;
     }
     F.dirty_count = 0;

@@ -64,6 +64,7 @@ def lib():
             "orc_outgoing_radiance": (C.c_int, [P, P, P, P, P, P, P, P]),
             "orc_frame_run": (P, [P, P, P, P, U, C.c_int]),
             "orc_frame_run_history": (P, [P, P, P, P, U, C.c_int, P, P, U]),
+            "orc_frame_run_retain": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
@@ -163,18 +164,21 @@ class OracleScene:
 
 class OracleFrame:
     def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0,
-                 previous: "OracleFrame | None" = None, dirty=None):
+                 previous: "OracleFrame | None" = None, dirty=None, max_cells: int = 0xFFFFFFFF,
+                 max_entries: int = (1 << 64) - 1):
         """previous: the frame whose records serve as history; dirty: boxes
-        (n, 6) = (lo xyz, hi xyz) whose nearby records take no history."""
+        (n, 6) = (lo xyz, hi xyz) whose nearby records take no history;
+        max_cells / max_entries: the view capacities that bound the cells
+        retained from `previous`."""
         self.settings = settings_c
         pos = np.ascontiguousarray(pos, np.float32)
         nrm = np.ascontiguousarray(nrm, np.float32)
         self._previous = previous  # keeps the history frame alive
         boxes = np.ascontiguousarray(dirty if dirty is not None else np.zeros((0, 6)), np.float32).reshape(-1, 6)
-        self.handle = lib().orc_frame_run_history(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
-                                                  threads or os.cpu_count() or 1,
-                                                  previous.handle if previous is not None else None, _p(boxes),
-                                                  len(boxes))
+        self.handle = lib().orc_frame_run_retain(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
+                                                 threads or os.cpu_count() or 1,
+                                                 previous.handle if previous is not None else None, _p(boxes),
+                                                 len(boxes), max_cells, max_entries)
 
     def level(self, level: int, dirs: int):
         cells = lib().orc_frame_cells(self.handle, level)

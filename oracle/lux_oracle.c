@@ -1368,6 +1368,7 @@ typedef struct {
     float *merged;   /* float4 */
     float *raw;      /* float4 J, beta (history-blended) */
     float *mass;     /* float2 radiance mass, transmittance mass */
+    uint32_t *last;  /* frame index of each cell's last receiver */
 } Level;
 
 struct OrcFrame {
@@ -1866,12 +1867,75 @@ OrcFrame *orc_frame_run(const OrcScene *S, const LuxSettings *st_in, const float
 OrcFrame *orc_frame_run_history(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
                                 uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
                                 uint32_t dirty_count) {
+    return orc_frame_run_retain(S, st_in, pos, nrm, n, threads, previous, dirty, dirty_count, UINT32_MAX,
+                                UINT64_MAX);
+}
+
+#define RETAIN_BINS 256u
+
+/* retain (shaders/split.slang:991-1054) with a persistent world cache
+ * (persistentWorldIntervals, shaders/common.slang:82-89; set for the Split
+ * method at src/render.rs:8470): the previous frame's cells that no receiver
+ * seeded stay, unless an invalidation box voids their history.  Capacity
+ * keeps the youngest (commitCache, shaders/split.slang:1919-1961) as whole
+ * age classes, levels in order, while cells fit max_cells and records fit
+ * max_entries.  Keys carry each cell's last receiver frame in k[3] here. */
+static void retain_cells(OrcFrame *F, Key **keys, uint32_t *cells, uint32_t max_cells, uint64_t max_entries) {
+    const OrcFrame *P = F->previous;
+    uint64_t used = 0;
+    for (uint32_t l = 0; l < F->levels; ++l) used += (uint64_t)cells[l] * F->level[l].dirs;
+    uint64_t remaining = used < max_entries ? max_entries - used : 0;
+    for (uint32_t l = 0; l < F->levels; ++l) {
+        const Level *H = &P->level[l];
+        Level seeded;
+        memset(&seeded, 0, sizeof seeded);
+        seeded.cells = cells[l];
+        seeded.keys = keys[l];
+        uint32_t *bin = (uint32_t *)malloc(sizeof(uint32_t) * (H->cells ? H->cells : 1));
+        uint64_t hist[RETAIN_BINS];
+        memset(hist, 0, sizeof hist);
+        for (uint32_t c = 0; c < H->cells; ++c) {
+            bin[c] = RETAIN_BINS;
+            if (find_cell(&seeded, H->keys[c].k) >= 0 || record_dirty(F, l, H->keys[c].k)) continue;
+            uint32_t age = F->st.frame_index - H->last[c];
+            bin[c] = age < RETAIN_BINS - 1u ? age : RETAIN_BINS - 1u;
+            hist[bin[c]]++;
+        }
+        uint64_t room = max_cells > cells[l] ? (uint64_t)max_cells - cells[l] : 0;
+        uint64_t by_entries = remaining / F->level[l].dirs;
+        if (by_entries < room) room = by_entries;
+        uint64_t kept = 0;
+        uint32_t limit = 0;
+        while (limit < RETAIN_BINS && kept + hist[limit] <= room) kept += hist[limit++];
+        if (kept) {
+            Key *all = (Key *)realloc(keys[l], sizeof(Key) * (cells[l] + kept));
+            uint32_t m = cells[l];
+            for (uint32_t c = 0; c < H->cells; ++c)
+                if (bin[c] < limit) {
+                    all[m] = H->keys[c];
+                    all[m].k[3] = (int32_t)H->last[c];
+                    ++m;
+                }
+            qsort(all, m, sizeof(Key), key_cmp);
+            keys[l] = all;
+            cells[l] = m;
+        }
+        remaining -= kept * F->level[l].dirs;
+        free(bin);
+    }
+}
+
+OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
+                               uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
+                               uint32_t dirty_count, uint32_t max_cells, uint64_t max_entries) {
     OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
     F->st = *st_in;
     /* History applies with history_frames > 0, a blend above zero and a
-     * previous frame of the same cascade count. */
-    if (previous && st_in->history_frames > 0 && (st_in->temporal_blend > 0.0f || st_in->transmittance_blend > 0.0f) &&
-        previous->levels == st_in->levels) {
+     * previous frame of the same cascade shape. */
+    int same_shape = previous && previous->levels == st_in->levels;
+    for (uint32_t l = 0; same_shape && l < st_in->levels; ++l)
+        same_shape = previous->level[l].dirs == level_columns(st_in, l) * level_rows(st_in, l);
+    if (same_shape && st_in->history_frames > 0 && (st_in->temporal_blend > 0.0f || st_in->transmittance_blend > 0.0f)) {
         F->previous = previous;
         F->dirty = dirty;
         F->dirty_count = dirty ? dirty_count : 0;
@@ -1879,23 +1943,36 @@ OrcFrame *orc_frame_run_history(const OrcScene *S, const LuxSettings *st_in, con
     const LuxSettings *st = &F->st;
     F->levels = st->levels;
     /* seed: the cells of every level that hold a receiver. */
-    Key *tmp = (Key *)malloc(sizeof(Key) * (n ? n : 1));
+    Key *level_keys[LUX_MAX_LEVELS];
+    uint32_t level_cells[LUX_MAX_LEVELS];
     for (uint32_t l = 0; l < F->levels; ++l) {
         Level *L = &F->level[l];
         L->columns = level_columns(st, l);
         L->rows = level_rows(st, l);
         L->dirs = L->columns * L->rows;
+        Key *tmp = (Key *)malloc(sizeof(Key) * (n ? n : 1));
         for (uint32_t i = 0; i < n; ++i) {
             cell_key(st, l, pos + 4 * (size_t)i, tmp[i].k);
-            tmp[i].k[3] = 0;
+            tmp[i].k[3] = (int32_t)st->frame_index;
         }
         qsort(tmp, n, sizeof(Key), key_cmp);
         uint32_t cells = 0;
         for (uint32_t i = 0; i < n; ++i)
             if (cells == 0 || key_cmp(&tmp[i], &tmp[cells - 1]) != 0) tmp[cells++] = tmp[i];
+        level_keys[l] = tmp;
+        level_cells[l] = cells;
+    }
+    if (F->previous && st->layout == LUX_LAYOUT_SPLIT) retain_cells(F, level_keys, level_cells, max_cells, max_entries);
+    for (uint32_t l = 0; l < F->levels; ++l) {
+        Level *L = &F->level[l];
+        uint32_t cells = level_cells[l];
         L->cells = cells;
-        L->keys = (Key *)malloc(sizeof(Key) * (cells ? cells : 1));
-        memcpy(L->keys, tmp, sizeof(Key) * cells);
+        L->keys = level_keys[l];
+        L->last = (uint32_t *)malloc(sizeof(uint32_t) * (cells ? cells : 1));
+        for (uint32_t c = 0; c < cells; ++c) {
+            L->last[c] = (uint32_t)L->keys[c].k[3];
+            L->keys[c].k[3] = 0;
+        }
         uint64_t entries = (uint64_t)cells * L->dirs;
         L->jsum = (float *)calloc(4 * entries + 4, sizeof(float));
         L->count = (uint32_t *)calloc(entries + 1, sizeof(uint32_t));
@@ -1905,7 +1982,6 @@ OrcFrame *orc_frame_run_history(const OrcScene *S, const LuxSettings *st_in, con
         F->stats.cells[l] = cells;
         F->stats.entries[l] = entries;
     }
-    free(tmp);
     F->stats.levels = F->levels;
     uint64_t shadow = 0;
     OrcCounters cn = {0, 0, 0};
@@ -1991,6 +2067,7 @@ void orc_frame_destroy(OrcFrame *F) {
         free(F->level[l].merged);
         free(F->level[l].raw);
         free(F->level[l].mass);
+        free(F->level[l].last);
     }
     free(F->tables);
     free(F);

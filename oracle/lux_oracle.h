@@ -100,6 +100,12 @@ typedef struct OrcFrame OrcFrame;
 OrcFrame *orc_frame_run_history(const OrcScene *scene, const LuxSettings *settings, const float *receiver_position,
                                 const float *receiver_normal, uint32_t receiver_count, int threads,
                                 const OrcFrame *previous, const float *dirty, uint32_t dirty_count);
+/* orc_frame_run_history with the view capacities that bound the retained
+ * cells of the previous frame (max_cells per level, max_entries records). */
+OrcFrame *orc_frame_run_retain(const OrcScene *scene, const LuxSettings *settings, const float *receiver_position,
+                               const float *receiver_normal, uint32_t receiver_count, int threads,
+                               const OrcFrame *previous, const float *dirty, uint32_t dirty_count,
+                               uint32_t max_cells, uint64_t max_entries);
 void orc_history_blend(const LuxSettings *settings, uint32_t samples, const float fresh[4], const float *old,
                        const float *old_mass, float out[4], float mass[2]);
 OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,

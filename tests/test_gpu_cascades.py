@@ -197,3 +197,34 @@ def test_split_history_and_invalidation_match_oracle():
     view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
     compare_levels(s, [view.read_level(l) for l in range(4)], oracle.OracleFrame(oscene, s.to_c(), pos, nrm),
                    exact=False)
+
+
+def test_split_retain_matches_oracle():
+    """retain: receivers move between frames; cells of earlier frames stay in
+    the persistent world cache (their records carried, their parents merged
+    over them), and a tight max_cells keeps whole age classes youngest first."""
+    def st(frame):
+        return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   frame_index=frame).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    sets = [pos[:, 0] < 0, pos[:, 0] >= 0, np.abs(pos[:, 0]) < 0.2]
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    dirs = st(0).direction_count(0)
+    every = {tuple(k[:3]) for k in oracle_frame("cornell", st(0), pos, nrm).level(0, dirs)[0]}
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    for max_cells in (1 << 16, len(every) - 1):
+        view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=max_cells, max_entries=1 << 24,
+                            max_rays=len(pos) * 4)
+        prev = None
+        for frame, sel in enumerate(sets):
+            s = st(frame)
+            d_pos, d_nrm = to_device(pos[sel]), to_device(nrm[sel])
+            view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), int(sel.sum()))
+            assert view.stats().error_flags == 0
+            cur = oracle.OracleFrame(oscene, s.to_c(), pos[sel], nrm[sel], previous=prev, max_cells=max_cells,
+                                     max_entries=1 << 24)
+            compare_levels(s, [view.read_level(l) for l in range(4)], cur, exact=False)
+            prev = cur
+        if max_cells == 1 << 16:  # everything seen so far is still cached
+            assert {tuple(k[:3]) for k in view.read_level(0)[0]} == every

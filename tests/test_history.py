@@ -127,3 +127,54 @@ def test_oracle_frames_accumulate_history():
     kr, mr, rr, cr = reset.level(0, dirs)
     np.testing.assert_array_equal(rr, rf)
     np.testing.assert_array_equal(mr, mf)
+
+
+def keyset(keys):
+    return {tuple(k[:3]) for k in keys}
+
+
+def test_oracle_retains_unseen_cells_youngest_first():
+    """retain (shaders/split.slang:991-1054) over a persistent world cache:
+    cells of the previous frame that no receiver seeded stay with their
+    records; capacity keeps whole age classes, youngest first (commitCache's
+    youngest-kept rule, :1919-1961)."""
+    base = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=2,
+                               emissive_samples=4, temporal_blend=0.88, split_transmittance_blend=0.98,
+                               history_frames=24)
+    pos, nrm = cornell_receivers()
+    left, strip = pos[:, 0] < 0, np.abs(pos[:, 0]) < 0.2
+    scene = oracle.OracleScene.from_packed(packed("cornell"))
+    dirs = base.direction_count(0)
+
+    def st(frame):
+        s = base.sanitized()
+        s.frame_index = frame
+        return s.to_c()
+
+    f0 = oracle.OracleFrame(scene, st(0), pos[left], nrm[left])
+    f1 = oracle.OracleFrame(scene, st(1), pos[~left], nrm[~left], previous=f0)
+    seeded1 = keyset(oracle.OracleFrame(scene, st(1), pos[~left], nrm[~left]).level(0, dirs)[0])
+    k0, m0, r0, c0 = f0.level(0, dirs)
+    k1, m1, r1, c1 = f1.level(0, dirs)
+    assert keyset(k1) == keyset(k0) | seeded1
+    i0 = {key: i for i, key in enumerate(map(tuple, k0[:, :3]))}
+    kept = [(i, i0[tuple(k[:3])]) for i, k in enumerate(k1) if tuple(k[:3]) not in seeded1]
+    assert kept
+    for i, j in kept:  # no fresh samples: the record carries over unchanged
+        assert np.all(c1[i] == 0)
+        np.testing.assert_array_equal(r1[i], r0[j])
+
+    # Frame 2 seeds a strip; frame 1's own cells are one frame old, the cells
+    # only frame 0 saw are two frames old.
+    seeded2 = keyset(oracle.OracleFrame(scene, st(2), pos[strip], nrm[strip]).level(0, dirs)[0])
+    age1 = seeded1 - seeded2
+    age2 = keyset(k0) - seeded1 - seeded2
+    assert age1 and age2
+    full = len(seeded2) + len(age1) + len(age2)
+    for max_cells, expect in ((full, seeded2 | age1 | age2), (full - 1, seeded2 | age1),
+                              (len(seeded2) + len(age1) - 1, seeded2)):
+        f2 = oracle.OracleFrame(scene, st(2), pos[strip], nrm[strip], previous=f1, max_cells=max_cells)
+        assert keyset(f2.level(0, dirs)[0]) == expect, max_cells
+    # An invalidation box over the scene drops every unseen cell.
+    f2 = oracle.OracleFrame(scene, st(2), pos[strip], nrm[strip], previous=f1, dirty=[[-10, -10, -10, 10, 10, 10]])
+    assert keyset(f2.level(0, dirs)[0]) == seeded2
