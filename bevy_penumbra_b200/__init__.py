@@ -90,6 +90,7 @@ class RadianceCascades:
     temporal_blend: float = 0.88
     split_transmittance_blend: float = 0.98
     history_frames: int = 24
+    multi_bounce: bool = False
 
     @staticmethod
     def low_end() -> "RadianceCascades":
@@ -119,6 +120,7 @@ class RadianceCascades:
         s.temporal_blend = self.temporal_blend
         s.transmittance_blend = self.split_transmittance_blend
         s.history_frames = _u32(self.history_frames)
+        s.multi_bounce = 1 if self.multi_bounce else 0
         return s
 
     @staticmethod
@@ -131,7 +133,7 @@ class RadianceCascades:
             base_rows=int(s.base_rows), interval_ratio=s.interval_ratio, interval_rule=int(s.interval_rule),
             layout=int(s.layout), rays_per_receiver=int(s.rays_per_receiver), frame_index=int(s.frame_index),
             temporal_blend=s.temporal_blend, split_transmittance_blend=s.transmittance_blend,
-            history_frames=int(s.history_frames))
+            history_frames=int(s.history_frames), multi_bounce=bool(s.multi_bounce))
 
     def sanitized(self) -> "RadianceCascades":
         """RadianceCascades::sanitized() (src/lib.rs:731-759), evaluated by liblux."""
@@ -400,6 +402,7 @@ class SplitView:
         self.handle = handle
         self.desc = desc
         self.settings: RadianceCascades | None = None
+        self._owned = True
 
     def trace_merge(self, scene: GpuScene, settings: RadianceCascades, position_ptr: int, normal_ptr: int,
                     count: int) -> None:
@@ -509,10 +512,28 @@ class SplitView:
         self.ctx.check(lib().lux_view_read_hits(self.handle, _ptr(out), count))
         return out
 
+    def secondary(self) -> "SplitView | None":
+        """lux_view_secondary: the multi-bounce secondary cache of this view
+        (read-only; None before the first multi-bounce frame).  Its settings
+        are this view's with probe spacing and interval length x4."""
+        handle = C.c_void_p()
+        self.ctx.check(lib().lux_view_secondary(self.handle, C.byref(handle)))
+        if not handle.value:
+            return None
+        sec = SplitView.__new__(SplitView)
+        sec.ctx = self.ctx
+        sec.handle = handle
+        sec.desc = self.desc
+        sec.settings = replace(self.settings, multi_bounce=False, probe_spacing=self.settings.probe_spacing * 4.0,
+                               interval_length=self.settings.interval_length * 4.0) if self.settings else None
+        sec._owned = False
+        sec._owner = self  # keeps the owning view alive
+        return sec
+
     def close(self) -> None:
-        if self.handle:
+        if self.handle and getattr(self, "_owned", True):
             lib().lux_view_destroy(self.handle)
-            self.handle = None
+        self.handle = None
 
     def __del__(self):
         try:

@@ -64,7 +64,7 @@ class LuxSettings(C.Structure):
         ("base_rows", C.c_uint32), ("interval_ratio", C.c_float), ("interval_rule", C.c_uint32),
         ("layout", C.c_uint32), ("rays_per_receiver", C.c_uint32), ("frame_index", C.c_uint32),
         ("resolve_scale", C.c_uint32), ("temporal_blend", C.c_float), ("transmittance_blend", C.c_float),
-        ("history_frames", C.c_uint32),
+        ("history_frames", C.c_uint32), ("multi_bounce", C.c_uint32),
     ]
 
 
@@ -177,6 +177,7 @@ SIGNATURES = {
     "lux_view_read_probes": (C.c_int, [P, P, P]),
     "lux_view_read_hits": (C.c_int, [P, P, U32]),
     "lux_view_reset_history": (C.c_int, [P]),
+    "lux_view_secondary": (C.c_int, [P, C.POINTER(C.c_void_p)]),
     "lux_view_invalidate_bounds": (C.c_int, [P, P, P]),
     "lux_view_set_cache": (C.c_int, [P, C.POINTER(LuxCacheMode)]),
     "lux_view_cache_stats": (C.c_int, [P, C.POINTER(LuxCacheFrameStats)]),

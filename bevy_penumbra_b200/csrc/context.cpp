@@ -137,6 +137,7 @@ extern "C" void lux_settings_sanitize(LuxSettings *s) {
     s->temporal_blend = finite_clamp(s->temporal_blend, 0.88f, 0.0f, 0.99f);
     s->transmittance_blend = finite_clamp(s->transmittance_blend, 0.98f, 0.0f, 0.999f);
     s->history_frames = s->history_frames > 64u ? 64u : s->history_frames;
+    s->multi_bounce = s->multi_bounce ? 1u : 0u;
 }
 
 // splitIntervalEnd, shaders/split.slang:224-227, generalised to a ratio and

@@ -61,6 +61,7 @@ struct TraceScratch {
     float4 *ray_d;          // direction, barycentric 1
     uint4 *ray_h;           // triangle, instance, errors, barycentric 2 bits
     float4 *ray_base;       // hit emission, next-event count (kEmpty: unsupported)
+    float4 *ray_extra;      // multi-bounce term of the hit (written when the frame has feedback)
     uint32_t *slot_query;   // per (ray, sample): queue index or kEmpty
     float4 *slot_contrib;   // per (ray, sample): contribution if visible
     float4 *queue_o;        // query origin, limit

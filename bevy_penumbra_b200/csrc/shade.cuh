@@ -4,7 +4,10 @@
 //
 // Synthetic-material subset, identical to the CPU oracle: untextured opaque
 // materials (materialSample = 1), no environment map and no conventional
-// lights (rejected at upload), no secondary cache.  All source groups are
+// lights (rejected at upload).  With multi-bounce on, the secondary cache's
+// irradiance of the previous frame adds diffuse bounce light (secondaryFeedback,
+// shaders/world_resolve.slang:204-279), and the secondary cache's own hits
+// leave out their emission (environmentScale.z).  All source groups are
 // summed into one radiance.  The scattering response is the diffuse colour
 // times disneyDiffuseMultiplier / pi (shaders/common.slang:298-314 and the
 // non-full branch of scatteringResponse, shaders/environment.slang:2-6).
@@ -13,12 +16,26 @@
 
 namespace lux {
 
+// The secondary cache's cascade-0 probes of the previous frame: a directory
+// of cell keys (open addressing, lux::hash_key with level 0) and the packed
+// 6x6 irradiance table of each cell.
+struct Feedback {
+    const unsigned long long *keys;  // [capacity] packed cell keys (kEmptyCell: free)
+    const uint32_t *ids;             // [capacity] table of each slot's cell
+    const float4 *tables;            // [cells][36]
+    uint32_t capacity;               // power of two
+    float spacing;                   // the secondary cache's cascade-0 spacing
+};
+
 struct ShadeParams {
     float probe_spacing;
     float normal_bias;
     float exposure;
     uint32_t emissive_samples;
     uint32_t frame;
+    uint32_t skip_emission;  // secondary cache: no first-hit emission (next-event estimation carries it)
+    uint32_t feedback;       // 1: add diffuse x the secondary cache's irradiance at the hit
+    Feedback fb;
 };
 
 __device__ __forceinline__ uint4 sword(const SceneView &S, uint32_t i) {
@@ -119,6 +136,67 @@ __device__ __forceinline__ float disney_multiplier(f3 n, f3 l, f3 v, float pr) {
     return ls * vs;
 }
 
+// irradianceLookup + diffuseProbePage (shaders/world_resolve.slang:27-89)
+// on one packed table: rgb and coverage.
+__device__ __forceinline__ float4 probe_irradiance(const float4 *__restrict__ table, f3 normal) {
+    float ex, ey;
+    encode_normal(normal, ex, ey);
+    float gx = ex * 6.0f - 0.5f, gy = ey * 6.0f - 0.5f;
+    float bxf = floorf(gx), byf = floorf(gy);
+    float fx = gx - bxf, fy = gy - byf;
+    float cx = 1.0f - fx, cy = 1.0f - fy;
+    float weight[4] = {cx * cy, fx * cy, cx * fy, fx * fy};
+    int32_t ix = (int32_t)bxf, iy = (int32_t)byf;
+    uint32_t texel[4] = {texel_index(ix, iy), texel_index(ix + 1, iy), texel_index(ix, iy + 1),
+                         texel_index(ix + 1, iy + 1)};
+    float px = 0.0f, py = 0.0f, pz = 0.0f, obs = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float bw = weight[c];
+        if (!(bw > 0.0f)) continue;
+        float4 t = __ldg(table + texel[c]);
+        if (!(t.w > 0.0f) || !(isfinite(t.x) && isfinite(t.y) && isfinite(t.z) && isfinite(t.w))) continue;
+        float w = bw * saturate(t.w);
+        px = px + t.x * w;
+        py = py + t.y * w;
+        pz = pz + t.z * w;
+        obs += w;
+    }
+    return obs > 0.0f ? make_float4(px / obs, py / obs, pz / obs, saturate(obs)) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// secondaryFeedback (shaders/world_resolve.slang:204-279) at one LOD: the
+// previous frame's secondary probe of the cell holding `position`, looked up
+// with the shading normal; resolveLodSource with a zero LOD blend gives
+// (rgb * coverage) / coverage, and zero without coverage.
+__device__ __forceinline__ f3 feedback_irradiance(const Feedback &fb, f3 position, f3 normal) {
+    const float s = fb.spacing;
+    int32_t x = (int32_t)floorf(position.x / s), y = (int32_t)floorf(position.y / s), z = (int32_t)floorf(position.z / s);
+    if (!finite3(position) || !cell_in_range(x, y, z)) return f3{0.0f, 0.0f, 0.0f};
+    unsigned long long key = pack_cell(x, y, z);
+    uint32_t slot = hash_key(x, y, z, 0, fb.capacity);
+    for (uint32_t attempt = 0; attempt < fb.capacity; ++attempt) {
+        unsigned long long k = __ldg(fb.keys + slot);
+        if (k == key) {
+            uint32_t id = __ldg(fb.ids + slot);
+            if (id == kEmpty) break;
+            float4 e = probe_irradiance(fb.tables + (size_t)id * 36, normal);
+            if (!(e.w > 0.0f)) break;
+            return f3{(e.x * e.w) / e.w, (e.y * e.w) / e.w, (e.z * e.w) / e.w};
+        }
+        if (k == kEmptyCell) break;
+        slot = (slot + 1u) & (fb.capacity - 1u);
+    }
+    return f3{0.0f, 0.0f, 0.0f};
+}
+
+// The surface a multi-bounce secondary receiver takes from an interval-ray
+// hit (the primary trace's hit record, shaders/split.slang:1199-1211).
+struct SurfaceRecord {
+    f3 position, normal;  // hit position, geometric normal facing the ray origin
+    bool valid;
+};
+
 constexpr uint32_t kMaxNeeSamples = 16u;  // max(1, emissive_samples / 2) with emissive_samples <= 32
 
 // One next-event sample of emissiveResponseTracked whose visibility query is
@@ -215,19 +293,23 @@ __device__ void emissive_queries(const SceneView &S, const ShadeParams &P, f3 po
 }
 
 // outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, up to the
-// visibility traces.  Writes the hit's own emission to `base` and emits the
-// next-event queries; returns false when the query is unsupported (no
-// deposit).  `count` = 0 when no next-event estimate applies.
+// visibility traces.  Writes the hit's own emission to `base`, the
+// multi-bounce term (diffuse x secondary-cache irradiance) to `extra`, the
+// surface a secondary receiver would take to `rec`, and emits the next-event
+// queries; returns false when the query is unsupported (no deposit).
+// `count` = 0 when no next-event estimate applies.
 template <typename Emit>
 __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
-                                f3 &base, uint32_t &count, Emit &&emit) {
+                                f3 &base, f3 &extra, SurfaceRecord &rec, uint32_t &count, Emit &&emit) {
     base = f3{0.0f, 0.0f, 0.0f};
+    extra = f3{0.0f, 0.0f, 0.0f};
+    rec.valid = false;
     count = 0;
     if ((hit.errors & kQueryUnsupported) != 0u) return false;
     if (hit.tri == kEmpty) return true;
     float b0 = (1.0f - hit.b1) - hit.b2;
     Surface sf = surface_at(S, P, hit.inst, hit.tri, b0, hit.b1, hit.b2);
-    base = sf.emission;
+    if (!P.skip_emission) base = sf.emission;
     if ((sf.flags & 16u) != 0u) return true;
     uint32_t ibase = instance_base(S, hit.inst);
     uint4 header = gword(S, 0);
@@ -267,15 +349,31 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
     f3 diffuse{(bf ? saturate(sf.base_color.x) : 0.0f) * (1.0f - metallic),
                (bf ? saturate(sf.base_color.y) : 0.0f) * (1.0f - metallic),
                (bf ? saturate(sf.base_color.z) : 0.0f) * (1.0f - metallic)};
+    rec.position = position;
+    rec.normal = flipped;
+    rec.valid = finite3(position) && finite3(flipped) && finite3(normal) && dot(flipped, flipped) > 0.01f;
+    if (P.feedback) {
+        f3 e = feedback_irradiance(P.fb, position, normal);
+        extra = f3{e.x * diffuse.x, e.y * diffuse.y, e.z * diffuse.z};
+    }
     emissive_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
     return true;
 }
 
+template <typename Emit>
+__device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
+                                f3 &base, uint32_t &count, Emit &&emit) {
+    f3 extra;
+    SurfaceRecord rec;
+    return outgoing_record(S, P, origin, direction, hit, base, extra, rec, count, emit);
+}
+
 // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188, after the
 // next-event sum: radiance = base + sum / count.
-__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count) {
+__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count, const f3 *extra = nullptr) {
     f3 radiance = base;
     if (count) radiance = radiance + f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
+    if (extra) radiance = radiance + *extra;  // secondaryFeedback's diffuse term, added last
     if (!finite3(radiance)) return f3{0.0f, 0.0f, 0.0f};
     return f3{fmaxf(radiance.x, 0.0f), fmaxf(radiance.y, 0.0f), fmaxf(radiance.z, 0.0f)};
 }

@@ -82,6 +82,10 @@ struct FrameParams {
     uint32_t history;                           // 1: the previous frame's records may be reused
     uint32_t dirty_count;                       // boxes whose records do not reuse history
     float dirty_lo[kMaxDirty][3], dirty_hi[kMaxDirty][3];
+    // Multi-bounce: the secondary cache's receivers are the primary hits, one
+    // slot per primary receiver, and a slot with position.w == 0 holds none.
+    uint32_t sparse;       // receivers with position.w == 0 are absent
+    uint32_t record_hits;  // write each receiver's hit surface (ray frame % R) to hit_pos / hit_nrm
 };
 
 // Device state of a view (ViewBuffers, src/render.rs:5077-5160).
@@ -103,6 +107,8 @@ struct ViewDevice {
     uint32_t *cell_last;            // [levels][cell_capacity] frame index of the cell's last receiver
     uint32_t *retain_hist;          // [levels][kRetainBins] retain candidates per age class
     uint32_t *retain_limit;         // [levels] age classes below this are retained
+    float4 *hit_pos;                // [receivers] multi-bounce: hit position, 1 (0: no surface)
+    float4 *hit_nrm;                // [receivers] multi-bounce: geometric normal facing the ray
     float4 *tables;                 // [cell_capacity][36]
     uint32_t *error_flags;
     unsigned long long *stats;      // 8 counters
@@ -211,6 +217,7 @@ __global__ void seed_insert_kernel(ViewDevice V, FrameParams F, const float4 *__
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
         float4 p = pos[r];
+        if (F.sparse && p.w == 0.0f) continue;
         int32_t x, y, z;
         cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
         if (!lux::cell_in_range(x, y, z)) {
@@ -261,7 +268,8 @@ __global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__
         float4 p = pos[r];
         int32_t x, y, z;
         cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
-        V.receiver_cell[(size_t)level * F.receivers + r] = cell_id(V, F, level, x, y, z);
+        V.receiver_cell[(size_t)level * F.receivers + r] =
+            F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z);
     }
 }
 
@@ -381,14 +389,25 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
 // One Split interval ray (traceTransport, shaders/split.slang:1122-1163):
 // receiver i = ray / R, sample k = ray % R, from the biased receiver position
 // to 1e20; the hit is stored for shading.
+// Returns false for the rays of an absent receiver of a sparse set (stored
+// as unsupported, not traced).
 template <int kDepth = lux::kStack>
-__device__ __forceinline__ void closest_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
+__device__ __forceinline__ bool closest_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
                                                   const SceneView &S, const float4 *__restrict__ pos,
                                                   const float4 *__restrict__ nrm, uint32_t slot,
                                                   lux::TraceCounters &cn) {
     uint32_t ray = V.ray_order ? V.ray_order[slot] : slot;
     uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
     float4 p4 = pos[i], n4 = nrm[i];
+    if (F.sparse && p4.w == 0.0f) {
+        lux::Hit none;
+        none.t = 0.0f;
+        none.b1 = none.b2 = 0.0f;
+        none.tri = none.inst = lux::kEmpty;
+        none.errors = lux::kQueryUnsupported;
+        store_ray(V, ray, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 0.0f}, none);
+        return false;
+    }
     f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
     f3 dir;
     float u, v;
@@ -397,6 +416,7 @@ __device__ __forceinline__ void closest_split_ray(const ViewDevice &V, const Fra
     lux::Hit hit;
     lux::trace<false, kDepth>(S, origin, dir, 0.0f, 1e20f, hit, cn);
     store_ray(V, ray, origin, dir, hit);
+    return true;
 }
 
 // Persistent warps, 32 consecutive rays per fetch (one atomic per warp).
@@ -417,10 +437,8 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_ker
         uint32_t base = warp_fetch(&V.ts.work_counter[0]);
         if (base >= ray_count) break;
         uint32_t slot = base + (threadIdx.x & 31u);
-        if (slot < ray_count) {
-            closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn);
+        if (slot < ray_count && closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn))
             st[kStatInterval] += 1;
-        }
     }
     st[kStatNodes] = cn.nodes;
     st[kStatTris] = cn.triangles;
@@ -527,18 +545,26 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     uint32_t slot_of[lux::kMaxNeeSamples];
     uint32_t nq = 0, count = 0;
     bool supported = false;
-    f3 base{0.0f, 0.0f, 0.0f};
+    f3 base{0.0f, 0.0f, 0.0f}, extra;
     if (ray < rays) {
         f3 o, d;
         lux::Hit hit;
+        lux::SurfaceRecord rec;
         load_ray(V, ray, o, d, hit);
-        supported = lux::outgoing_record(S, P, o, d, hit, base, count,
+        supported = lux::outgoing_record(S, P, o, d, hit, base, extra, rec, count,
                                          [&](uint32_t sample, const lux::NeeQuery &query) {
                                              q[nq] = query;
                                              slot_of[nq] = sample;
                                              ++nq;
                                          });
         V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? count : lux::kEmpty));
+        if (P.feedback) V.ts.ray_extra[ray] = make_float4(extra.x, extra.y, extra.z, 0.0f);
+        // The multi-bounce secondary receiver of receiver i: its ray frame % R.
+        if (F.record_hits && rec.valid && ray % F.rays_per_receiver == P.frame % F.rays_per_receiver) {
+            uint32_t i = ray / F.rays_per_receiver;
+            V.hit_pos[i] = make_float4(rec.position.x, rec.position.y, rec.position.z, 1.0f);
+            V.hit_nrm[i] = make_float4(rec.normal.x, rec.normal.y, rec.normal.z, 0.0f);
+        }
     }
     // Warp-aggregated append of this warp's queries.
     uint32_t prefix = nq;
@@ -648,8 +674,9 @@ __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(View
     add_stats(V.stats, st, extra);
 }
 
-// Next-event sum in sample order; false when the ray's query is unsupported.
-__device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, f3 &radiance) {
+// Next-event sum in sample order (plus the multi-bounce term with
+// `feedback`); false when the ray's query is unsupported.
+__device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, f3 &radiance, bool feedback = false) {
     float4 b = V.ts.ray_base[ray];
     uint32_t count = lux::as_uint(b.w);
     if (count == lux::kEmpty) return false;
@@ -665,7 +692,13 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
         float4 c = V.ts.slot_contrib[slot];
         sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
     }
-    radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count);
+    if (feedback) {
+        float4 e = V.ts.ray_extra[ray];
+        f3 extra{e.x, e.y, e.z};
+        radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count, &extra);
+    } else {
+        radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count);
+    }
     return true;
 }
 
@@ -674,12 +707,13 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
 __device__ __forceinline__ void deposit_split_ray(const ViewDevice &V, const FrameParams &F, uint32_t frame,
                                                   const float4 *__restrict__ nrm, uint32_t ray,
                                                   unsigned long long st[7]) {
+    uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+    if (F.sparse && V.receiver_cell[i] == lux::kEmpty) return;  // absent receiver: no ray
     f3 radiance;
-    if (!ray_radiance(V, ray, radiance)) {
+    if (!ray_radiance(V, ray, radiance, F.shade.feedback != 0u)) {
         st[kStatUnsupported] += 1;
         return;
     }
-    uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
     float4 n4 = nrm[i];
     f3 dir;
     float u, v;
@@ -883,23 +917,35 @@ __global__ void retain_count_kernel(ViewDevice V, FrameParams F, HistoryDevice H
     }
 }
 
-__global__ void __launch_bounds__(256) retain_limit_kernel(ViewDevice V, FrameParams F) {
-    __shared__ uint32_t hist[LUX_MAX_LEVELS * kRetainBins];
-    for (uint32_t i = threadIdx.x; i < F.levels * kRetainBins; i += blockDim.x) hist[i] = V.retain_hist[i];
-    __syncthreads();
-    if (threadIdx.x != 0) return;
-    unsigned long long used = 0;
-    for (uint32_t l = 0; l < F.levels; ++l)
-        used += (unsigned long long)min(V.cell_count[l], F.cell_capacity) * F.dirs[l];
-    unsigned long long remaining = used < F.entry_capacity ? F.entry_capacity - used : 0ull;
+// One block of kRetainBins threads: per level, an inclusive scan of the age
+// histogram; the limit is the number of classes whose running total fits.
+__global__ void __launch_bounds__(kRetainBins) retain_limit_kernel(ViewDevice V, FrameParams F) {
+    __shared__ unsigned long long scan[kRetainBins];
+    __shared__ unsigned long long remaining;
+    const uint32_t t = threadIdx.x;
+    if (t == 0) {
+        unsigned long long used = 0;
+        for (uint32_t l = 0; l < F.levels; ++l)
+            used += (unsigned long long)min(V.cell_count[l], F.cell_capacity) * F.dirs[l];
+        remaining = used < F.entry_capacity ? F.entry_capacity - used : 0ull;
+    }
     for (uint32_t l = 0; l < F.levels; ++l) {
+        scan[t] = V.retain_hist[l * kRetainBins + t];
+        __syncthreads();
+        for (uint32_t off = 1; off < kRetainBins; off <<= 1) {
+            unsigned long long add = t >= off ? scan[t - off] : 0ull;
+            __syncthreads();
+            scan[t] += add;
+            __syncthreads();
+        }
         unsigned long long seeded = min(V.cell_count[l], F.cell_capacity);
         unsigned long long room = min((unsigned long long)F.cell_capacity - seeded, remaining / F.dirs[l]);
-        unsigned long long kept = 0;
-        uint32_t a = 0;
-        while (a < kRetainBins && kept + hist[l * kRetainBins + a] <= room) kept += hist[l * kRetainBins + a++];
-        V.retain_limit[l] = a;
-        remaining -= kept * F.dirs[l];
+        uint32_t fits = (uint32_t)__syncthreads_count(scan[t] <= room);  // the scan is non-decreasing
+        if (t == 0) {
+            V.retain_limit[l] = fits;
+            remaining -= (fits ? scan[fits - 1] : 0ull) * F.dirs[l];
+        }
+        __syncthreads();
     }
 }
 
@@ -1642,6 +1688,17 @@ struct LuxView {
     LuxCacheMode cache{};
     CacheDevice cdev{};
     bool cache_alloc = false;
+    // Multi-bounce (RadianceCascades::multi_bounce): the secondary cache, a
+    // second view whose receivers are this view's interval-ray hits, and the
+    // snapshot of its cascade-0 probes that hit shading reads one frame late.
+    LuxView *secondary = nullptr;
+    struct {
+        unsigned long long *keys = nullptr;
+        uint32_t *ids = nullptr;
+        float4 *tables = nullptr;
+        float spacing = 0.0f;
+        bool valid = false;
+    } fb;
 };
 
 static void cache_buffers_free(LuxView *v) {
@@ -1696,6 +1753,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.ts.ray_d, (size_t)d.max_rays * sizeof(float4)},
         {(void **)&D.ts.ray_h, (size_t)d.max_rays * sizeof(uint4)},
         {(void **)&D.ts.ray_base, (size_t)d.max_rays * sizeof(float4)},
+        {(void **)&D.ts.ray_extra, (size_t)d.max_rays * sizeof(float4)},
         {(void **)&D.ts.slot_query, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
         {(void **)&D.ts.slot_contrib, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
         {(void **)&D.ts.queue_o, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
@@ -1748,7 +1806,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
                     D.retain_hist, D.retain_limit, D.tables, D.error_flags, D.stats,
                     v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
                     v->hist.mass, v->hist.cell_last, v->hist.cell_keys,
-                    D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
+                    D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.ray_extra, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
                     D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     for (void *p : ptrs)
@@ -1756,6 +1814,10 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     for (int i = 0; i < kTimingEvents; ++i)
         if (v->ev[i]) cudaEventDestroy(v->ev[i]);
     cache_buffers_free(v);
+    void *bounce[] = {D.hit_pos, D.hit_nrm, v->fb.keys, v->fb.ids, v->fb.tables};
+    for (void *p : bounce)
+        if (p) cudaFree(p);
+    lux_view_destroy(v->secondary);
     delete v;
     return LUX_OK;
 }
@@ -1880,7 +1942,7 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
         const HistoryDevice H = history_device(v);
         cudaMemsetAsync(D.retain_hist, 0, (size_t)LUX_MAX_LEVELS * kRetainBins * sizeof(uint32_t), st);
         retain_count_kernel<<<grid, 256, 0, st>>>(D, F, H);
-        retain_limit_kernel<<<1, 256, 0, st>>>(D, F);
+        retain_limit_kernel<<<1, kRetainBins, 0, st>>>(D, F);
         retain_insert_kernel<<<grid, 256, 0, st>>>(D, F, H);
     }
     layout_kernel<<<1, 32, 0, st>>>(D, F);
@@ -1945,9 +2007,121 @@ static void enqueue_pack(LuxView *v, const FrameParams &F, cudaStream_t st) {
     pack_kernel<<<v->ctx->sm_count * 8, 64, smem, st>>>(v->dev, F);
 }
 
+// Per-frame roles of a view in a multi-bounce frame.
+struct FrameRole {
+    uint32_t sparse = 0;         // receivers with position.w == 0 are absent (the secondary cache)
+    uint32_t skip_emission = 0;  // no first-hit emission (the secondary cache)
+    uint32_t record_hits = 0;    // write the receivers' hit surfaces (the primary cache)
+    bool feedback = false;       // hit shading reads the secondary snapshot
+};
+
+static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSettings *settings, const LuxReceivers *rc,
+                             const FrameRole &role, const LuxView *fb_owner);
+
+// The secondary view, hit buffers and probe snapshot, created with the first
+// multi-bounce frame (the secondary has the primary's capacities).
+static lux_status ensure_multi_bounce(LuxView *v) {
+    if (v->secondary) return LUX_OK;
+    LuxContext *ctx = v->ctx;
+    LuxViewDesc d = v->desc;
+    LuxView *sec = nullptr;
+    lux_status s = lux_view_create(ctx, &d, &sec);
+    if (s != LUX_OK) return s;
+    ViewDevice &D = v->dev;
+    bool ok = cudaMalloc((void **)&D.hit_pos, (size_t)d.max_receivers * sizeof(float4)) == cudaSuccess &&
+              cudaMalloc((void **)&D.hit_nrm, (size_t)d.max_receivers * sizeof(float4)) == cudaSuccess &&
+              cudaMalloc((void **)&v->fb.keys, (size_t)sec->dir_capacity * 8) == cudaSuccess &&
+              cudaMalloc((void **)&v->fb.ids, (size_t)sec->dir_capacity * 4) == cudaSuccess &&
+              cudaMalloc((void **)&v->fb.tables, (size_t)d.max_cells * 36 * sizeof(float4)) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        lux_view_destroy(sec);
+        void *ptrs[] = {D.hit_pos, D.hit_nrm, v->fb.keys, v->fb.ids, v->fb.tables};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        D.hit_pos = D.hit_nrm = nullptr;
+        v->fb.keys = nullptr;
+        v->fb.ids = nullptr;
+        v->fb.tables = nullptr;
+        return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "multi_bounce: device allocation failed");
+    }
+    v->secondary = sec;
+    v->fb.valid = false;
+    return lux_view_set_timing(sec, v->timing ? 1u : 0u);
+}
+
+// Snapshot of the secondary cache's cascade-0 probes for the next frame's
+// hit shading: the level-0 directory and the tables of its live cells.
+__global__ void feedback_snapshot_kernel(ViewDevice S, uint32_t dir_capacity, unsigned long long *keys, uint32_t *ids,
+                                         float4 *tables) {
+    const size_t stride = (size_t)gridDim.x * blockDim.x;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < dir_capacity; i += stride) {
+        keys[i] = S.dir_keys[i];
+        ids[i] = S.dir_ids[i];
+    }
+    // Tables only when the secondary frame completed (pack ran).
+    const size_t n = *S.error_flags ? 0 : (size_t)S.cell_count[0] * 36;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += stride) tables[i] = S.tables[i];
+}
+
+// A multi-bounce frame (RadianceCascades::multi_bounce; the secondary
+// passes of src/render.rs:9662-9752): the primary cache traces with the
+// previous snapshot's bounce light and records each receiver's hit surface;
+// the secondary cache (LOD + 2: spacing and intervals x4) takes those
+// surfaces as receivers, leaves out first-hit emission and reads the same
+// snapshot; its cascade-0 probes then become the next frame's snapshot.
 extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, const LuxSettings *settings,
                                            const LuxReceivers *rc) {
     if (!v || !scene || !settings || !rc) return LUX_ERR_INVALID_ARGUMENT;
+    LuxSettings s = *settings;
+    lux_settings_sanitize(&s);
+    if (!s.multi_bounce || s.layout != LUX_LAYOUT_SPLIT) return view_frame(v, scene, settings, rc, FrameRole{}, nullptr);
+    lux_status st = ensure_multi_bounce(v);
+    if (st != LUX_OK) return st;
+    LuxContext *ctx = v->ctx;
+    cudaStream_t stream = ctx->stream;
+    if (rc->count > v->desc.max_receivers)
+        return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: more receivers than the view's max_receivers");
+    // Dirty boxes void the snapshot's probes for this frame (their merged
+    // values depend on the whole cascade reach) and the secondary's history.
+    const bool dirty = !v->dirty.empty();
+    for (const auto &box : v->dirty) v->secondary->dirty.push_back(box);
+    FrameRole primary;
+    primary.record_hits = 1;
+    primary.feedback = v->fb.valid && !dirty;
+    cudaMemsetAsync(v->dev.hit_pos, 0, (size_t)rc->count * sizeof(float4), stream);
+    st = view_frame(v, scene, settings, rc, primary, v);
+    if (st != LUX_OK) return st;
+    LuxView *sec = v->secondary;
+    LuxTuning t = v->tuning;
+    t.closest_mode = 0;
+    sec->tuning = t;
+    LuxSettings s2 = s;
+    s2.multi_bounce = 0;
+    s2.probe_spacing = s.probe_spacing * 4.0f;
+    s2.interval_length = s.interval_length * 4.0f;
+    LuxReceivers hits{(const float *)v->dev.hit_pos, (const float *)v->dev.hit_nrm, rc->count};
+    FrameRole secondary;
+    secondary.sparse = 1;
+    secondary.skip_emission = 1;
+    secondary.feedback = primary.feedback;
+    st = view_frame(sec, scene, &s2, &hits, secondary, v);
+    if (st != LUX_OK) return st;
+    feedback_snapshot_kernel<<<ctx->sm_count * 4, 256, 0, stream>>>(sec->dev, sec->dir_capacity, v->fb.keys,
+                                                                     v->fb.ids, v->fb.tables);
+    v->fb.spacing = s2.probe_spacing;
+    v->fb.valid = true;
+    return lux_cuda_check(ctx, (int)cudaGetLastError(), "multi_bounce launch");
+}
+
+extern "C" lux_status lux_view_secondary(LuxView *v, LuxView **secondary) {
+    if (!v || !secondary) return LUX_ERR_INVALID_ARGUMENT;
+    *secondary = v->secondary;
+    return LUX_OK;
+}
+
+static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSettings *settings, const LuxReceivers *rc,
+                             const FrameRole &role, const LuxView *fb_owner) {
     LuxContext *ctx = v->ctx;
     if (rc->count > v->desc.max_receivers)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: more receivers than the view's max_receivers");
@@ -1968,6 +2142,14 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     LuxSettings sanitized = *settings;
     lux_settings_sanitize(&sanitized);
     begin_history(v, F, sanitized);
+    F.sparse = role.sparse;
+    F.record_hits = role.record_hits;
+    F.shade.skip_emission = role.skip_emission;
+    if (role.feedback && fb_owner) {
+        F.shade.feedback = 1;
+        F.shade.fb = lux::Feedback{fb_owner->fb.keys, fb_owner->fb.ids, fb_owner->fb.tables,
+                                   fb_owner->secondary->dir_capacity, fb_owner->fb.spacing};
+    }
     mark(0);
     enqueue_setup(v, F, pos, st);
     mark(1);
@@ -2066,6 +2248,8 @@ extern "C" lux_status lux_view_reset_history(LuxView *v) {
     if (!v) return LUX_ERR_INVALID_ARGUMENT;
     v->hist_valid = false;
     v->dirty.clear();
+    v->fb.valid = false;
+    if (v->secondary) lux_view_reset_history(v->secondary);
     return LUX_OK;
 }
 
@@ -2219,7 +2403,7 @@ extern "C" lux_status lux_view_set_timing(LuxView *v, uint32_t enable) {
                 return lux_cuda_check(v->ctx, (int)cudaGetLastError(), "timing events");
     }
     v->timing = enable != 0;
-    return LUX_OK;
+    return v->secondary ? lux_view_set_timing(v->secondary, enable) : LUX_OK;
 }
 
 // Per-stage device times of the last frame in milliseconds (the reference's
@@ -2660,6 +2844,7 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
     LuxSettings s = *settings;
     lux_settings_sanitize(&s);
     if (s.layout != LUX_LAYOUT_SPLIT) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: layout must be Split");
+    if (s.multi_bounce) return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: multi_bounce runs per view");
     std::vector<FrameParams> params(n);
     for (uint32_t j = 0; j < n; ++j) {
         const LuxBatchJob &J = jobs[j];

@@ -130,6 +130,8 @@ typedef struct LuxSettings {
                                        interval radiance, 0..=0.99; mass limit 1 / (1 - blend) */
     float transmittance_blend;      /* RadianceCascades::split_transmittance_blend (intervalHistory.x), 0..=0.999 */
     uint32_t history_frames;        /* RadianceCascades::history_frames (history.w), 0..=64; 0 disables history */
+    uint32_t multi_bounce;          /* RadianceCascades::multi_bounce: 1 adds the secondary cache's diffuse bounce
+                                       light at interval-ray hits (Split layout, unbatched frames) */
 } LuxSettings;
 
 /* Receivers (Split) or the cascade-0 probe set (Dense), device pointers.
@@ -359,6 +361,12 @@ typedef struct LuxTuning {
 lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
 lux_status lux_view_get_tuning(const LuxView *view, LuxTuning *tuning);
 lux_status lux_view_timings(LuxView *view, LuxTimings *out);
+/* The view's multi-bounce secondary cache (RadianceCascades::multi_bounce;
+ * src/render.rs:5974-6118, :9662-9752): a view owned by `view`, created by
+ * its first multi-bounce frame (NULL before), whose receivers are the
+ * interval-ray hits of `view`.  Read it with lux_view_read_level /
+ * read_probes / stats / timings; do not trace or destroy it. */
+lux_status lux_view_secondary(LuxView *view, LuxView **secondary);
 /* Copies one level's records to host memory (tests): cell keys int4[cells],
  * merged float4[cells*dirs] (I.rgb, support), raw float4[cells*dirs]
  * (J.rgb, beta) and sample counts uint32[cells*dirs].  Any pointer may be NULL. */

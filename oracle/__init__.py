@@ -65,6 +65,7 @@ def lib():
             "orc_frame_run": (P, [P, P, P, P, U, C.c_int]),
             "orc_frame_run_history": (P, [P, P, P, P, U, C.c_int, P, P, U]),
             "orc_frame_run_retain": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64]),
+            "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
@@ -165,20 +166,30 @@ class OracleScene:
 class OracleFrame:
     def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0,
                  previous: "OracleFrame | None" = None, dirty=None, max_cells: int = 0xFFFFFFFF,
-                 max_entries: int = (1 << 64) - 1):
+                 max_entries: int = (1 << 64) - 1, feedback: "OracleFrame | None" = None, sparse: bool = False,
+                 skip_emission: bool = False, record_hits: bool = False):
         """previous: the frame whose records serve as history; dirty: boxes
         (n, 6) = (lo xyz, hi xyz) whose nearby records take no history;
         max_cells / max_entries: the view capacities that bound the cells
-        retained from `previous`."""
+        retained from `previous`.  Multi-bounce: feedback, the secondary frame
+        whose cascade-0 probes add bounce light at hits; sparse, receivers
+        with position.w == 0 are absent; skip_emission, hits add no emission of
+        their own; record_hits, keep each receiver's hit surface (hits())."""
         self.settings = settings_c
         pos = np.ascontiguousarray(pos, np.float32)
         nrm = np.ascontiguousarray(nrm, np.float32)
         self._previous = previous  # keeps the history frame alive
         boxes = np.ascontiguousarray(dirty if dirty is not None else np.zeros((0, 6)), np.float32).reshape(-1, 6)
-        self.handle = lib().orc_frame_run_retain(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
+        self._feedback = feedback
+        self.hit_pos = np.zeros((len(pos), 4), np.float32)
+        self.hit_nrm = np.zeros((len(pos), 4), np.float32)
+        flags = (1 if sparse else 0) | (2 if skip_emission else 0) | (4 if record_hits else 0)
+        self.handle = lib().orc_frame_run_bounce(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
                                                  threads or os.cpu_count() or 1,
                                                  previous.handle if previous is not None else None, _p(boxes),
-                                                 len(boxes), max_cells, max_entries)
+                                                 len(boxes), max_cells, max_entries,
+                                                 feedback.handle if feedback is not None else None, flags,
+                                                 _p(self.hit_pos), _p(self.hit_nrm))
 
     def level(self, level: int, dirs: int):
         cells = lib().orc_frame_cells(self.handle, level)

@@ -1276,18 +1276,32 @@ static int emissive_response(const OrcScene *S, const LuxSettings *st, const flo
     return 1;
 }
 
+/* Multi-bounce roles of a frame (RadianceCascades::multi_bounce). */
+typedef struct {
+    const OrcFrame *feedback;  /* secondary frame whose cascade-0 probes add bounce light (NULL: none) */
+    int skip_emission;         /* the secondary cache: no first-hit emission (environmentScale.z) */
+} Bounce;
+
+static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3]);
+
 /* outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, with
  * every active source group summed into one radiance (no environment, no
- * conventional lights, no secondary cache: the synthetic-scene subset). */
-int orc_outgoing_radiance(const OrcScene *S, const LuxSettings *st, const float origin[3],
-                          const float direction[3], const LuxHit *hit, float out[3], uint64_t *shadow_rays,
-                          OrcCounters *cn) {
+ * conventional lights: the synthetic-scene subset).  With a feedback frame
+ * the secondary cache's irradiance times the diffuse colour is added last
+ * (secondaryFeedback, shaders/world_resolve.slang:204-279).  `rec` receives
+ * the surface a multi-bounce secondary receiver takes from this hit:
+ * position xyz, geometric normal facing the ray xyz, valid flag. */
+static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bounce *bn, const float origin[3],
+                             const float direction[3], const LuxHit *hit, float out[3], float rec[7],
+                             uint64_t *shadow_rays, OrcCounters *cn) {
     out[0] = out[1] = out[2] = 0.0f;
+    if (rec) rec[6] = 0.0f;
     if ((hit->errors & HIT_QUERY_UNSUPPORTED) != 0u) return 0;
     if (hit->triangle == EMPTY) return 1;
     Surface sf;
     surface_at(S, st, hit->instance, hit->triangle, hit->barycentric, &sf);
     float radiance[3] = {sf.emission[0], sf.emission[1], sf.emission[2]};
+    if (bn && bn->skip_emission) radiance[0] = radiance[1] = radiance[2] = 0.0f;
     if ((sf.flags & 16u) == 0u) {
         uint32_t base = instance_base(S, hit->instance);
         U4 header = gword(S, 0);
@@ -1333,18 +1347,34 @@ int orc_outgoing_radiance(const OrcScene *S, const LuxSettings *st, const float 
             int base_finite = finite3(sf.base_color);
             for (int c = 0; c < 3; ++c)
                 diffuse[c] = (base_finite ? saturatef(sf.base_color[c]) : 0.0f) * (1.0f - metallic);
+            if (rec) {
+                memcpy(rec, position, 12);
+                memcpy(rec + 3, flipped, 12);
+                rec[6] = finite3(position) && finite3(flipped) && finite3(normal) && dot3(flipped, flipped) > 0.01f;
+            }
             float nee[3];
             if (!emissive_response(S, st, position, normal, flipped, view, roughness, diffuse, nee, shadow_rays, cn)) {
                 out[0] = out[1] = out[2] = 0.0f;
                 return 0;
             }
             for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + nee[c];
+            if (bn && bn->feedback) {
+                float e[3];
+                feedback_irradiance(bn->feedback, position, normal, e);
+                for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + e[c] * diffuse[c];
+            }
         }
     }
     /* clampOutgoingTransportRadiance, shaders/cascades.slang:179-188. */
     if (!finite3(radiance)) return 1;
     for (int c = 0; c < 3; ++c) out[c] = fmaxf(radiance[c], 0.0f);
     return 1;
+}
+
+int orc_outgoing_radiance(const OrcScene *S, const LuxSettings *st, const float origin[3],
+                          const float direction[3], const LuxHit *hit, float out[3], uint64_t *shadow_rays,
+                          OrcCounters *cn) {
+    return outgoing_radiance(S, st, NULL, origin, direction, hit, out, NULL, shadow_rays, cn);
 }
 
 /* ======================================================================
@@ -1408,6 +1438,10 @@ typedef struct {
     const LuxSettings *st;
     const float *pos, *nrm;
     uint32_t n;
+    /* multi-bounce */
+    const Bounce *bounce;
+    int sparse;               /* receivers with position.w == 0 are absent */
+    float *hit_pos, *hit_nrm; /* float4 per receiver: the surface of ray frame % R, or NULL */
     /* split: per ray outputs */
     int32_t *term_level;  /* -1 = unsupported */
     float *radiance;      /* rgb per ray */
@@ -1448,12 +1482,21 @@ static void *split_job(void *arg) {
     for (uint64_t ray = j->begin; ray < j->end; ++ray) {
         uint32_t i = (uint32_t)(ray / R), k = (uint32_t)(ray % R);
         const float *p = j->pos + 4 * (size_t)i, *n = j->nrm + 4 * (size_t)i;
+        if (j->sparse && p[3] == 0.0f) {
+            j->term_level[ray] = -2;  /* absent receiver: no ray */
+            continue;
+        }
         float uv[2], origin[3], dir[3];
         LuxHit hit;
         split_ray(j->S, st, p, n, i * R + k, uv, &hit, origin, dir);
         orc_trace_closest(j->S, origin, dir, 0.0f, 1e20f, &hit, &j->cn);
-        float rad[3];
-        int supported = orc_outgoing_radiance(j->S, st, origin, dir, &hit, rad, &j->shadow, &j->cn);
+        float rad[3], rec[7];
+        int supported = outgoing_radiance(j->S, st, j->bounce, origin, dir, &hit, rad, rec, &j->shadow, &j->cn);
+        if (j->hit_pos && rec[6] != 0.0f && k == st->frame_index % R) {
+            float *hp = j->hit_pos + 4 * (size_t)i, *hn = j->hit_nrm + 4 * (size_t)i;
+            hp[0] = rec[0]; hp[1] = rec[1]; hp[2] = rec[2]; hp[3] = 1.0f;
+            hn[0] = rec[3]; hn[1] = rec[4]; hn[2] = rec[5]; hn[3] = 0.0f;
+        }
         j->uv[2 * ray] = uv[0];
         j->uv[2 * ray + 1] = uv[1];
         memcpy(&j->radiance[3 * ray], rad, sizeof rad);
@@ -1928,6 +1971,34 @@ static void retain_cells(OrcFrame *F, Key **keys, uint32_t *cells, uint32_t max_
 OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
                                uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
                                uint32_t dirty_count, uint32_t max_cells, uint64_t max_entries) {
+    return orc_frame_run_bounce(S, st_in, pos, nrm, n, threads, previous, dirty, dirty_count, max_cells, max_entries,
+                                NULL, 0u, NULL, NULL);
+}
+
+/* secondaryFeedback at LOD 0 of the secondary frame: its cascade-0 probe of
+ * the cell holding `position`, looked up with the shading normal;
+ * resolveLodSource with a zero LOD blend gives (rgb * coverage) / coverage. */
+static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3]) {
+    out[0] = out[1] = out[2] = 0.0f;
+    if (!finite3(position)) return;
+    float s = orc_spacing(&fb->st, 0);
+    int32_t key[3] = {(int32_t)floorf(position[0] / s), (int32_t)floorf(position[1] / s),
+                      (int32_t)floorf(position[2] / s)};
+    int64_t cell = find_cell(&fb->level[0], key);
+    if (cell < 0) return;
+    Lookup lk = irradiance_lookup(normal);
+    float e[4];
+    probe_page(&fb->tables[(size_t)cell * 144], &lk, e);
+    if (!(e[3] > 0.0f)) return;
+    for (int c = 0; c < 3; ++c) out[c] = (e[c] * e[3]) / e[3];
+}
+
+OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
+                               uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
+                               uint32_t dirty_count, uint32_t max_cells, uint64_t max_entries,
+                               const OrcFrame *feedback, uint32_t flags, float *hit_pos, float *hit_nrm) {
+    const int sparse = (flags & ORC_FRAME_SPARSE) != 0u;
+    Bounce bounce = {feedback, (flags & ORC_FRAME_SKIP_EMISSION) != 0u};
     OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
     F->st = *st_in;
     /* History applies with history_frames > 0, a blend above zero and a
@@ -1951,13 +2022,15 @@ OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, cons
         L->rows = level_rows(st, l);
         L->dirs = L->columns * L->rows;
         Key *tmp = (Key *)malloc(sizeof(Key) * (n ? n : 1));
+        uint32_t present = 0;
         for (uint32_t i = 0; i < n; ++i) {
-            cell_key(st, l, pos + 4 * (size_t)i, tmp[i].k);
-            tmp[i].k[3] = (int32_t)st->frame_index;
+            if (sparse && pos[4 * (size_t)i + 3] == 0.0f) continue;
+            cell_key(st, l, pos + 4 * (size_t)i, tmp[present].k);
+            tmp[present++].k[3] = (int32_t)st->frame_index;
         }
-        qsort(tmp, n, sizeof(Key), key_cmp);
+        qsort(tmp, present, sizeof(Key), key_cmp);
         uint32_t cells = 0;
-        for (uint32_t i = 0; i < n; ++i)
+        for (uint32_t i = 0; i < present; ++i)
             if (cells == 0 || key_cmp(&tmp[i], &tmp[cells - 1]) != 0) tmp[cells++] = tmp[i];
         level_keys[l] = tmp;
         level_cells[l] = cells;
@@ -1994,14 +2067,23 @@ OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, cons
         proto.pos = pos;
         proto.nrm = nrm;
         proto.n = n;
+        proto.bounce = &bounce;
+        proto.sparse = sparse;
+        proto.hit_pos = (flags & ORC_FRAME_RECORD_HITS) ? hit_pos : NULL;
+        proto.hit_nrm = (flags & ORC_FRAME_RECORD_HITS) ? hit_nrm : NULL;
         proto.term_level = (int32_t *)malloc(sizeof(int32_t) * (rays ? rays : 1));
         proto.radiance = (float *)malloc(sizeof(float) * 3 * (rays ? rays : 1));
         proto.uv = (float *)malloc(sizeof(float) * 2 * (rays ? rays : 1));
         run_jobs(&proto, rays, threads, split_job, &shadow, &cn);
+        uint64_t present_rays = rays;
         /* deposit, shaders/split.slang:1056-1117, then the per-key mean of
          * reduce (shaders/split.slang:1386-1476), in ray order. */
         for (uint64_t ray = 0; ray < rays; ++ray) {
             int32_t term = proto.term_level[ray];
+            if (term == -2) {  /* absent receiver of a sparse set */
+                --present_rays;
+                continue;
+            }
             if (term < 0) {
                 F->stats.unsupported++;
                 continue;
@@ -2023,7 +2105,7 @@ OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, cons
                 F->stats.deposits++;
             }
         }
-        F->stats.interval_rays = rays;
+        F->stats.interval_rays = present_rays;
         free(proto.term_level);
         free(proto.radiance);
         free(proto.uv);

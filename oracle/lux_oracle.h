@@ -106,6 +106,21 @@ OrcFrame *orc_frame_run_retain(const OrcScene *scene, const LuxSettings *setting
                                const float *receiver_normal, uint32_t receiver_count, int threads,
                                const OrcFrame *previous, const float *dirty, uint32_t dirty_count,
                                uint32_t max_cells, uint64_t max_entries);
+/* Multi-bounce roles (RadianceCascades::multi_bounce): ORC_FRAME_SPARSE,
+ * receivers with position.w == 0 are absent; ORC_FRAME_SKIP_EMISSION, hits
+ * add no emission of their own (the secondary cache); ORC_FRAME_RECORD_HITS,
+ * the surface of each receiver's ray frame % R (position, 1; geometric normal
+ * facing the ray, 0) is written to hit_pos / hit_nrm (float4 per receiver,
+ * untouched where there is none).  `feedback`: the secondary frame whose
+ * cascade-0 probes add diffuse bounce light at every hit (NULL: none). */
+#define ORC_FRAME_SPARSE 1u
+#define ORC_FRAME_SKIP_EMISSION 2u
+#define ORC_FRAME_RECORD_HITS 4u
+OrcFrame *orc_frame_run_bounce(const OrcScene *scene, const LuxSettings *settings, const float *receiver_position,
+                               const float *receiver_normal, uint32_t receiver_count, int threads,
+                               const OrcFrame *previous, const float *dirty, uint32_t dirty_count,
+                               uint32_t max_cells, uint64_t max_entries, const OrcFrame *feedback, uint32_t flags,
+                               float *hit_pos, float *hit_nrm);
 void orc_history_blend(const LuxSettings *settings, uint32_t samples, const float fresh[4], const float *old,
                        const float *old_mass, float out[4], float mass[2]);
 OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,

@@ -228,3 +228,44 @@ def test_split_retain_matches_oracle():
             prev = cur
         if max_cells == 1 << 16:  # everything seen so far is still cached
             assert {tuple(k[:3]) for k in view.read_level(0)[0]} == every
+
+
+def test_multi_bounce_matches_oracle():
+    """multi_bounce: each frame the primary cache traces with the previous
+    secondary probes' bounce light and records one hit surface per receiver;
+    the secondary cache (spacing and intervals x4) traces from those surfaces
+    without first-hit emission.  Primary and secondary records follow the
+    oracle chain frame by frame."""
+    from dataclasses import replace
+
+    def st(frame):
+        return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   emissive_samples=8, frame_index=frame, multi_bounce=True).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    pos[:, 3] = 1.0
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=1 << 16, max_entries=1 << 24, max_rays=len(pos) * 4)
+    assert view.secondary() is None
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    prim = sec = None
+    caps = dict(max_cells=1 << 16, max_entries=1 << 24)
+    for frame in range(3):
+        s = st(frame)
+        s2 = replace(s, probe_spacing=s.probe_spacing * 4.0, interval_length=s.interval_length * 4.0,
+                     multi_bounce=False)
+        view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+        assert view.stats().error_flags == 0
+        p = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prim, feedback=sec, record_hits=True, **caps)
+        q = oracle.OracleFrame(oscene, s2.to_c(), p.hit_pos, p.hit_nrm, previous=sec, feedback=sec, sparse=True,
+                               skip_emission=True, **caps)
+        compare_levels(s, [view.read_level(l) for l in range(4)], p, exact=False)
+        secondary = view.secondary()
+        assert secondary is not None and secondary.stats().error_flags == 0
+        compare_levels(s2, [secondary.read_level(l) for l in range(4)], q, exact=False)
+        if sec is not None:  # the bounce light reaches the primary records
+            unfed = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prim, **caps)
+            dirs = s.direction_count(0)
+            assert np.any(p.level(0, dirs)[2][..., :3] > unfed.level(0, dirs)[2][..., :3] + 1e-4)
+        prim, sec = p, q

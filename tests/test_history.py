@@ -178,3 +178,43 @@ def test_oracle_retains_unseen_cells_youngest_first():
     # An invalidation box over the scene drops every unseen cell.
     f2 = oracle.OracleFrame(scene, st(2), pos[strip], nrm[strip], previous=f1, dirty=[[-10, -10, -10, 10, 10, 10]])
     assert keyset(f2.level(0, dirs)[0]) == seeded2
+
+
+def test_oracle_multi_bounce_roles():
+    """Multi-bounce roles of an oracle frame: the primary records one hit
+    surface per receiver (its ray frame % R), the secondary cache over those
+    sparse receivers leaves out first-hit emission, and a feedback frame adds
+    non-negative diffuse bounce light at hits."""
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=2,
+                            emissive_samples=4).sanitized()
+    s2 = bp.RadianceCascades(probe_spacing=1.0, interval_length=1.6, levels=4, rays_per_receiver=2,
+                             emissive_samples=4).sanitized()
+    pos, nrm = cornell_receivers(16)
+    pos[:, 3] = 1.0
+    scene = oracle.OracleScene.from_packed(packed("cornell"))
+    dirs = s.direction_count(0)
+    p0 = oracle.OracleFrame(scene, s.to_c(), pos, nrm, record_hits=True)
+    plain = oracle.OracleFrame(scene, s.to_c(), pos, nrm)
+    for a, b in zip(p0.level(0, dirs), plain.level(0, dirs)):
+        np.testing.assert_array_equal(a, b)  # recording changes nothing
+    have = p0.hit_pos[:, 3] == 1.0
+    assert have.mean() > 0.5
+    assert np.all(np.isfinite(p0.hit_pos[have])) and np.all(np.abs(p0.hit_pos[have, :3]) <= 2.0 + 1e-5)
+    np.testing.assert_allclose(np.linalg.norm(p0.hit_nrm[have, :3], axis=1), 1.0, rtol=1e-5)
+    assert np.all(p0.hit_pos[~have] == 0.0)
+    # Secondary cache over the sparse hit set: absent receivers seed nothing.
+    sec = oracle.OracleFrame(scene, s2.to_c(), p0.hit_pos, p0.hit_nrm, sparse=True, skip_emission=True)
+    dense = oracle.OracleFrame(scene, s2.to_c(), p0.hit_pos[have], p0.hit_nrm[have])
+    assert {tuple(k[:3]) for k in sec.level(0, dirs)[0]} == {tuple(k[:3]) for k in dense.level(0, dirs)[0]}
+    lit = oracle.OracleFrame(scene, s2.to_c(), p0.hit_pos, p0.hit_nrm, sparse=True)
+    _, _, raw_skip, _ = sec.level(0, dirs)
+    _, _, raw_lit, _ = lit.level(0, dirs)
+    assert np.all(raw_skip[..., :3] <= raw_lit[..., :3] + 1e-7)
+    assert np.any(raw_skip[..., :3] < raw_lit[..., :3] - 1e-4)  # rays that see the emitter lose it
+    # Bounce light from the secondary's probes only adds.
+    fed = oracle.OracleFrame(scene, s.to_c(), pos, nrm, feedback=sec)
+    _, _, raw_fed, samples_fed = fed.level(0, dirs)
+    _, _, raw_plain, samples_plain = plain.level(0, dirs)
+    np.testing.assert_array_equal(samples_fed, samples_plain)
+    assert np.all(raw_fed[..., :3] >= raw_plain[..., :3] - 1e-7)
+    assert np.any(raw_fed[..., :3] > raw_plain[..., :3] + 1e-4)
