@@ -321,6 +321,49 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     }
 
 
+def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device):
+    """The multi-bounce form of the same frame (RadianceCascades::multi_bounce):
+    the primary cache with the secondary probes' bounce light, then the
+    secondary cache traced from the primary hits (spacing and intervals x4).
+    Timed like the plain frame after 8 untimed frames."""
+    import dataclasses
+    import torch
+
+    bp, ctx, scene = w["bp"], w["ctx"], w["scene"]
+    settings = dataclasses.replace(w["settings"], multi_bounce=True)
+    n_recv = len(w["rpos"])
+    mview = bp.SplitView(ctx, max_receivers=n_recv, max_cells=int(w["cells_max"]),
+                         max_entries=int(w["entries"]), max_rays=n_recv * settings.rays_per_receiver)
+    mview.set_timing(True)
+
+    def frame(step):
+        settings.frame_index = step
+        mview.trace_merge(scene, settings, d_rpos.data_ptr(), d_rnrm.data_ptr(), n_recv)
+
+    for step in range(max(args.warmup, 8)):
+        frame(step)
+    torch.cuda.synchronize(device)
+    ms, sec_trace = [], []
+    for step in range(args.steps):
+        flush.fill_(float(step))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        frame(1000 + step)
+        end.record(stream)
+        torch.cuda.synchronize(device)
+        ms.append(start.elapsed_time(end))
+        sec_trace.append(mview.secondary().timings().trace_ms)
+    st, sst = mview.stats(), mview.secondary().stats()
+    if st.error_flags or sst.error_flags:
+        raise RuntimeError("multi-bounce frame reported an error")
+    mb_ms = float(np.sum(ms)) / args.steps
+    return {"ms_per_step": mb_ms, "overhead_vs_plain": mb_ms / plain_ms,
+            "secondary_trace_ms": float(np.median(sec_trace)),
+            "primary_rays": int(st.interval_rays), "secondary_rays": int(sst.interval_rays),
+            "secondary_shadow_rays": int(sst.shadow_rays), "secondary_cells_level0": int(sst.cells[0]),
+            "secondary": "spacing and intervals x4, receivers = the primary hits of ray frame % R"}
+
+
 def max_over_ranks(value, dist, device):
     """Replicas: the job's time is the slowest rank's (a MAX all-reduce;
     the identity without a process group)."""
@@ -440,6 +483,7 @@ def run_ours(args, rank, world):
 
     learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref,
                           ms_per_step, error, interval_rays, device)
+    multi_bounce = run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, ms_per_step, device)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -483,6 +527,7 @@ def run_ours(args, rank, world):
                     "d2h_bytes_per_step": int(n_pts * 16)},
             "error_vs_fp64": error,
             "learned": learned,
+            "multi_bounce": multi_bounce,
             "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
