@@ -116,13 +116,18 @@ def build_workload(device: int = 0, host_only: bool = False):
         pos[:, :3] = o[ok] + d[ok] * hits["distance"][ok, None]
         nrm = np.zeros_like(pos)
         nrm[:, :3] = world_normals(packed, hits[ok], d[ok])
-        return pos, nrm
+        # Screen attributes of the hit pixels: view depth and raster identity.
+        fwd = np.asarray(TARGET, np.float64) - np.asarray(EYE, np.float64)
+        fwd /= np.linalg.norm(fwd)
+        screen = {"hit": ok, "depth": (hits["distance"][ok] * (d[ok] @ fwd.astype(np.float32))).astype(np.float32),
+                  "identity": hits["instance"][ok].astype(np.uint32)}
+        return pos, nrm, screen
 
-    rpos, rnrm = primary(PROBE_PX)
+    rpos, rnrm, _ = primary(PROBE_PX)
     if host_only:
-        ppos, pnrm = rpos[:0], rnrm[:0]
+        ppos, pnrm, pscreen = rpos[:0], rnrm[:0], None
     else:
-        ppos, pnrm = primary(1)
+        ppos, pnrm, pscreen = primary(1)
     settings = settings_for_workload()
     # Exact record counts per level (cells holding a receiver x directions).
     entries = 0
@@ -135,7 +140,8 @@ def build_workload(device: int = 0, host_only: bool = False):
     view = None if host_only else bp.SplitView(ctx, max_receivers=len(rpos), max_cells=cells_max,
                                                max_entries=entries,
                                                max_rays=len(rpos) * settings.rays_per_receiver)
-    return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, rpos=rpos,
+    return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, pscreen=pscreen,
+                rpos=rpos,
                 rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, cells_max=cells_max, setup_s=time.time() - t0)
 
 
@@ -364,6 +370,61 @@ def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device):
             "secondary": "spacing and intervals x4, receivers = the primary hits of ray frame % R"}
 
 
+def run_screen(w, args, stream, flush, d_ppos, d_pnrm, d_out, device):
+    """Screen reconstruction of the resolved frame at WIDTH x HEIGHT (the
+    reference's temporal pass and 3 a-trous passes): the resolve output and
+    the hit pixels' attributes scattered into full-screen images, then
+    lux_screen_filter timed per frame with a static camera."""
+    import torch
+
+    bp, ctx, settings = w["bp"], w["ctx"], w["settings"]
+    sc = w["pscreen"]
+    dev = f"cuda:{device}"
+    n = WIDTH * HEIGHT
+    idx = torch.from_numpy(np.flatnonzero(sc["hit"])).to(dev)
+    irr = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    pos = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    ident = torch.zeros((n, 2), dtype=torch.int32, device=dev)
+    irr[idx] = d_out
+    pos[idx] = d_ppos
+    pos[idx, 3] = torch.from_numpy(sc["depth"]).to(dev)
+    nrm[idx] = d_pnrm
+    ident[idx, 0] = torch.from_numpy(sc["identity"].view(np.int32)).to(dev)
+    out = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    from bevy_penumbra_b200 import scenes
+    clip = scenes.clip_from_world(EYE, TARGET, 60.0, WIDTH, HEIGHT)
+    screen = bp.ScreenFilter(ctx, WIDTH, HEIGHT)
+    torch.cuda.synchronize(device)
+
+    def frame():
+        screen.filter(settings, irr.data_ptr(), pos.data_ptr(), nrm.data_ptr(), ident.data_ptr(), clip,
+                      out.data_ptr(), spatial_filter_steps=3)
+
+    for _ in range(max(args.warmup, 3)):
+        frame()
+    torch.cuda.synchronize(device)
+    ms = []
+    for step in range(args.steps):
+        flush.fill_(float(step))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        frame()
+        end.record(stream)
+        torch.cuda.synchronize(device)
+        ms.append(start.elapsed_time(end))
+    _, meta = screen.read_history()
+    t = float(np.median(ms))
+    # Compulsory bytes per frame: temporal reads the frame inputs (irradiance,
+    # position, normal 16 B, identity 8 B) and the history (72 B) and writes
+    # the history; each a-trous pass reads irradiance + mask (20 B), position,
+    # temporal metadata, normal and identity (56 B) and writes 20 B.
+    alg = n * ((56 + 72 + 72) + 3 * (76 + 20))
+    return {"ms_per_step": t, "pixels": n, "passes": "temporal + 3 a-trous (strides 1, 2, 4)",
+            "achieved_gbs": alg / (t * 1e-3) / 1e9, "algorithmic_bytes": alg,
+            "history_length_mean": float(meta[..., 0][meta[..., 3] > 0].mean())}
+
+
 def max_over_ranks(value, dist, device):
     """Replicas: the job's time is the slowest rank's (a MAX all-reduce;
     the identity without a process group)."""
@@ -484,6 +545,8 @@ def run_ours(args, rank, world):
     learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref,
                           ms_per_step, error, interval_rays, device)
     multi_bounce = run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, ms_per_step, device)
+    view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
+    screen = run_screen(w, args, stream, flush, d_ppos, d_pnrm, d_out, device)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -528,6 +591,7 @@ def run_ours(args, rank, world):
             "error_vs_fp64": error,
             "learned": learned,
             "multi_bounce": multi_bounce,
+            "screen_filter": screen,
             "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},

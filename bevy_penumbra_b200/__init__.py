@@ -595,6 +595,62 @@ CACHE_SAMPLE_DTYPE = np.dtype([("position", "<f4", 3), ("weight", "<f4"), ("dire
 CACHE_WEIGHTS = 4 * 64 * 64 + 16 * 64
 
 
+class ScreenFilter:
+    """Screen reconstruction after the world resolve (the reference's
+    temporal + denoise passes, shaders/cascades.slang:310-690): owns the
+    screen history of one view at the resolve extent."""
+
+    def __init__(self, ctx: LuxContext, width: int, height: int):
+        self.ctx = ctx
+        self.width, self.height = int(width), int(height)
+        handle = C.c_void_p()
+        ctx.check(lib().lux_screen_create(ctx.handle, self.width, self.height, C.byref(handle)))
+        self.handle = handle
+
+    def filter(self, settings: RadianceCascades, irradiance_ptr: int, position_ptr: int, normal_ptr: int,
+               identity_ptr: int, previous_clip_from_world, out_ptr: int, spatial_filter_steps: int = 3,
+               scene_changed: bool = False, dirty=None) -> None:
+        """Device pointers at the resolve extent: irradiance / position (w =
+        view depth) / normal float4, identity uint32 x 2; out float4.
+        previous_clip_from_world: 4x4 row-major; dirty: (lo xyz, hi xyz)."""
+        f = N.LuxScreenFrame()
+        f.irradiance, f.position, f.normal, f.identity = irradiance_ptr, position_ptr, normal_ptr, identity_ptr
+        m = np.asarray(previous_clip_from_world, np.float32).reshape(16)
+        for i in range(16):
+            f.previous_clip_from_world[i] = float(m[i])
+        if dirty is not None:
+            d = np.asarray(dirty, np.float32).reshape(6)
+            for a in range(3):
+                f.dirty_lo[a], f.dirty_hi[a] = float(d[a]), float(d[3 + a])
+            f.dirty = 1
+        f.scene_changed = 1 if scene_changed else 0
+        f.spatial_filter_steps = int(spatial_filter_steps)
+        s = settings.to_c()
+        self.ctx.check(lib().lux_screen_filter(self.handle, C.byref(s), C.byref(f), out_ptr))
+
+    def reset(self) -> None:
+        self.ctx.check(lib().lux_screen_reset(self.handle))
+
+    def read_history(self):
+        """(irradiance f32[h, w, 4], metadata f32[h, w, 4]: retained length,
+        variance, support mask, surface flag)."""
+        irr = np.zeros((self.height, self.width, 4), np.float32)
+        meta = np.zeros((self.height, self.width, 4), np.float32)
+        self.ctx.check(lib().lux_screen_read_history(self.handle, _ptr(irr), _ptr(meta)))
+        return irr, meta
+
+    def close(self) -> None:
+        if self.handle:
+            lib().lux_screen_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class LearnedCache:
     """lux_cache_*: hash-grid encoded MLP radiance cache (tcgen05 BF16 MLP)."""
 

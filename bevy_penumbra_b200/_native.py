@@ -130,6 +130,13 @@ class LuxBatchInfo(C.Structure):
                 ("interval_rays", C.c_uint64), ("kernels_per_frame", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class LuxScreenFrame(C.Structure):
+    _fields_ = [("irradiance", C.c_void_p), ("position", C.c_void_p), ("normal", C.c_void_p),
+                ("identity", C.c_void_p), ("previous_clip_from_world", C.c_float * 16),
+                ("dirty_lo", C.c_float * 3), ("dirty_hi", C.c_float * 3), ("dirty", C.c_uint32),
+                ("scene_changed", C.c_uint32), ("spatial_filter_steps", C.c_uint32), ("reserved", C.c_uint32)]
+
+
 P = C.c_void_p
 U32 = C.c_uint32
 SZ = C.c_size_t
@@ -200,6 +207,11 @@ SIGNATURES = {
     "lux_batch_set_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
     "lux_batch_trace_merge": (C.c_int, [P, P, U32, P]),
     "lux_batch_info": (C.c_int, [P, C.POINTER(LuxBatchInfo)]),
+    "lux_screen_create": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
+    "lux_screen_destroy": (C.c_int, [P]),
+    "lux_screen_reset": (C.c_int, [P]),
+    "lux_screen_filter": (C.c_int, [P, C.POINTER(LuxSettings), C.POINTER(LuxScreenFrame), C.c_void_p]),
+    "lux_screen_read_history": (C.c_int, [P, C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

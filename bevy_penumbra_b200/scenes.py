@@ -438,3 +438,24 @@ def camera_rays(width: int, height: int, eye, target, fov_y_deg: float = 60.0, s
     d = d.reshape(-1, 3).astype(np.float32)
     o = np.broadcast_to(eye.astype(np.float32), d.shape).copy()
     return o, d
+
+
+def clip_from_world(eye, target, fov_y_deg: float, width: int, height: int, near: float = 0.05,
+                    far: float = 1000.0) -> np.ndarray:
+    """clip_from_world (row-major float32) of the look-at perspective camera
+    camera_rays traces (view space -z forward, clip w = view depth)."""
+    eye = np.asarray(eye, np.float64)
+    fwd = np.asarray(target, np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, (0.0, 1.0, 0.0))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    view = np.eye(4)
+    view[0, :3], view[1, :3], view[2, :3] = right, up, -fwd
+    view[:3, 3] = -view[:3, :3] @ eye
+    t = math.tan(math.radians(fov_y_deg) * 0.5)
+    proj = np.zeros((4, 4))
+    proj[0, 0], proj[1, 1] = 1.0 / (t * width / height), 1.0 / t
+    proj[2, 2], proj[2, 3] = -(far + near) / (far - near), -2.0 * far * near / (far - near)
+    proj[3, 2] = -1.0
+    return (proj @ view).astype(np.float32)

@@ -557,6 +557,40 @@ lux_status lux_batch_trace_merge(LuxBatch *batch, const LuxBatchJob *jobs, uint3
                                  const LuxSettings *settings);
 lux_status lux_batch_info(const LuxBatch *batch, LuxBatchInfo *out);
 
+/* ---- Screen reconstruction after the world resolve --------------------
+ * The reference's temporal and denoise passes (shaders/cascades.slang:310-690,
+ * dispatched at src/render.rs:9836-9930) for the Split method's persistent
+ * world intervals: reprojected screen history with neighbourhood clamping,
+ * then `spatial_filter_steps` edge-stopping a-trous passes (strides 1, 2, 4,
+ * 8).  Only the temporal result becomes history.  Per-pixel inputs are at the
+ * resolve extent, row-major, device pointers. */
+typedef struct LuxScreenFrame {
+    const float *irradiance;     /* float4: lux_view_resolve output of the pixel (alpha = rawGiSupportAlpha) */
+    const float *position;       /* float4: world position xyz; w = view depth, > 0 on a surface, 0 none */
+    const float *normal;         /* float4: unit geometric normal xyz */
+    const uint32_t *identity;    /* uint32 x 2: raster identity of the pixel's surface (receiverSame) */
+    float previous_clip_from_world[16]; /* the previous frame's camera, row-major; reprojects history */
+    float dirty_lo[3], dirty_hi[3];     /* dirtyMin / dirtyMax: no history is reused inside */
+    uint32_t dirty;              /* 1: the dirty box applies */
+    uint32_t scene_changed;      /* stability.y: a global change this frame (reactive blend, radiometric steps) */
+    uint32_t spatial_filter_steps; /* RadianceCascades::spatial_filter_steps, 0..=4 */
+    uint32_t reserved;
+} LuxScreenFrame;
+typedef struct LuxScreen LuxScreen;
+lux_status lux_screen_create(LuxContext *ctx, uint32_t width, uint32_t height, LuxScreen **out);
+lux_status lux_screen_destroy(LuxScreen *screen);
+/* The next frame has no screen history (stability.x = 0). */
+lux_status lux_screen_reset(LuxScreen *screen);
+/* One frame: temporal (reads settings temporal_blend, history_frames,
+ * probe_spacing, normal_bias), then the spatial passes; `out` is a device
+ * float4[width * height] (rgb, depth or 0 without lighting support). */
+lux_status lux_screen_filter(LuxScreen *screen, const LuxSettings *settings, const LuxScreenFrame *frame,
+                             float *out);
+/* Copies the screen history to host memory (tests): irradiance float4 (rgb,
+ * depth or 0) and metadata float4 (retained length, variance, support mask,
+ * surface flag) per pixel; either pointer may be NULL. */
+lux_status lux_screen_read_history(LuxScreen *screen, float *irradiance, float *metadata);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,7 @@ def lib():
             "orc_frame_run_history": (P, [P, P, P, P, U, C.c_int, P, P, U]),
             "orc_frame_run_retain": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64]),
             "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P]),
+            "orc_screen_filter": (None, [P, U, U, P, P, P, P, P, P, U, U, U, P, P, P]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
@@ -231,6 +232,30 @@ class OracleFrame:
             self.close()
         except Exception:
             pass
+
+
+SCREEN_WORDS = 18
+
+
+def screen_filter(settings_c, irradiance, position, normal, identity, previous_clip_from_world, history=None,
+                  dirty=None, scene_changed=False, spatial_filter_steps=3):
+    """The screen temporal + denoise passes on (h, w, 4) float32 images and an
+    (h, w, 2) uint32 identity image; history: the previous call's history
+    (None: no screen history).  Returns (history, out (h, w, 4))."""
+    h, w = irradiance.shape[:2]
+    irradiance = np.ascontiguousarray(irradiance, np.float32)
+    position = np.ascontiguousarray(position, np.float32)
+    normal = np.ascontiguousarray(normal, np.float32)
+    identity = np.ascontiguousarray(identity, np.uint32)
+    prev = np.ascontiguousarray(previous_clip_from_world, np.float32).reshape(16)
+    hin = np.zeros((h, w, SCREEN_WORDS), np.float32) if history is None else np.ascontiguousarray(history)
+    hout = np.zeros((h, w, SCREEN_WORDS), np.float32)
+    out = np.zeros((h, w, 4), np.float32)
+    d = None if dirty is None else np.ascontiguousarray(dirty, np.float32).reshape(6)
+    lib().orc_screen_filter(C.byref(settings_c), w, h, _p(irradiance), _p(position), _p(normal), _p(identity),
+                            _p(prev), _p(d) if d is not None else None, 1 if scene_changed else 0,
+                            spatial_filter_steps, 0 if history is None else 1, _p(hin), _p(hout), _p(out))
+    return hout, out
 
 
 def history_blend(settings_c, samples: int, fresh, old=None, old_mass=None):

@@ -2415,3 +2415,328 @@ void orc_reference_irradiance(const OrcScene *S, const LuxSettings *settings_in,
         }
     }
 }
+
+/* ======================================================================
+ * Screen reconstruction: temporal + denoise (shaders/cascades.slang:310-690)
+ * for persistent world intervals without motion vectors; positions are the
+ * caller's (xyz, view depth in w) and the previous positions are kept in the
+ * history.  History words per pixel (ORC_SCREEN_WORDS): irradiance rgb +
+ * depth, metadata (retained length, variance, support mask, surface flag),
+ * position xyzw, normal xyzw, identity (2 words of raw bits).
+ * ==================================================================== */
+typedef struct {
+    uint32_t width, height;
+    float temporal_blend, capacity, tolerance, plane_scale;
+    uint32_t history_valid, scene_changed, dirty;
+    float dirty_lo[3], dirty_hi[3];
+    float prev[16];
+} ScreenParams;
+
+static float lum3(const float *c) { return (c[0] * 0.2126f + c[1] * 0.7152f) + c[2] * 0.0722f; }
+
+static float sdot(const float *a, const float *b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+/* surfacePlaneDistance, shaders/common.slang:585-591. */
+static float plane_distance(const float delta[3], const float *target, const float *sample) {
+    float avg[3] = {target[0] + sample[0], target[1] + sample[1], target[2] + sample[2]};
+    float len2 = sdot(avg, avg);
+    if (!(len2 > 1e-20f) || !isfinite(len2)) return fabsf(sdot(delta, target));
+    float inv = 1.0f / sqrtf(len2);
+    float n[3] = {avg[0] * inv, avg[1] * inv, avg[2] * inv};
+    return fabsf(sdot(delta, n));
+}
+
+static int screen_compatible(int a_surface, const uint32_t *a_id, const float *a_n, int b_surface,
+                             const uint32_t *b_id, const float *b_n) {
+    return a_surface && b_surface && a_id[0] == b_id[0] && a_id[1] == b_id[1] && sdot(a_n, b_n) > 0.97f;
+}
+
+static int screen_dirty(const ScreenParams *P, const float *p) {
+    return P->dirty && p[0] >= P->dirty_lo[0] && p[1] >= P->dirty_lo[1] && p[2] >= P->dirty_lo[2] &&
+           p[0] <= P->dirty_hi[0] && p[1] <= P->dirty_hi[1] && p[2] <= P->dirty_hi[2];
+}
+
+static float lerpf_(float a, float b, float t) { return a + t * (b - a); }
+
+#define HW ORC_SCREEN_WORDS
+static const float *hw_irr(const float *h, size_t p) { return h + HW * p; }
+static const float *hw_meta(const float *h, size_t p) { return h + HW * p + 4; }
+static const float *hw_pos(const float *h, size_t p) { return h + HW * p + 8; }
+static const float *hw_nrm(const float *h, size_t p) { return h + HW * p + 12; }
+static const uint32_t *hw_id(const float *h, size_t p) { return (const uint32_t *)(h + HW * p + 16); }
+
+static void screen_temporal(const ScreenParams *P, const float *irr, const float *pos, const float *nrm,
+                            const uint32_t *ids, const float *H, float *out) {
+    for (int y = 0; y < (int)P->height; ++y)
+        for (int x = 0; x < (int)P->width; ++x) {
+            size_t p = (size_t)y * P->width + x;
+            float *o = out + HW * p;
+            float center[4];
+            memcpy(center, irr + 4 * p, 16);
+            const float *position = pos + 4 * p;
+            float depth = position[3];
+            if (!(depth > 0.0f)) {
+                memset(o, 0, sizeof(float) * HW);
+                continue;
+            }
+            const float *gn = nrm + 4 * p;
+            const uint32_t *id = ids + 2 * p;
+            int current_finite = isfinite(center[3]) && finite3(center);
+            uint32_t current_mask = current_finite && center[3] > 0.0f ? ((uint32_t)floorf(center[3]) & 1u) : 0u;
+            int current_supported = current_mask != 0u && current_finite;
+            float freshness = current_supported ? saturatef((center[3] - floorf(center[3])) * 4.0f) : 0.0f;
+            if (!current_supported) center[0] = center[1] = center[2] = 0.0f;
+            uint32_t output_mask = current_mask;
+            float mean[3] = {0, 0, 0}, sq[3] = {0, 0, 0}, count = 0.0f;
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx) {
+                    int qx = x + dx, qy = y + dy;
+                    if (qx < 0 || qy < 0 || qx >= (int)P->width || qy >= (int)P->height) continue;
+                    size_t q = (size_t)qy * P->width + qx;
+                    const float *v = irr + 4 * q;
+                    if (v[3] <= 0.0f) continue;
+                    uint32_t nmask = (uint32_t)floorf(v[3]) & 1u;
+                    if (current_mask != 0u && nmask != current_mask) continue;
+                    const float *op = pos + 4 * q;
+                    if (op[3] <= 0.0f) continue;
+                    const float *on = nrm + 4 * q;
+                    if (!screen_compatible(1, id, gn, 1, ids + 2 * q, on)) continue;
+                    float delta[3] = {op[0] - position[0], op[1] - position[1], op[2] - position[2]};
+                    if (sdot(gn, on) < 0.95f || plane_distance(delta, gn, on) > P->tolerance) continue;
+                    for (int c = 0; c < 3; ++c) {
+                        mean[c] += v[c];
+                        sq[c] += v[c] * v[c];
+                    }
+                    count += 1.0f;
+                }
+            float cdiv = fmaxf(count, 1.0f);
+            float var[3], dev[3];
+            for (int c = 0; c < 3; ++c) {
+                mean[c] /= cdiv;
+                sq[c] /= cdiv;
+            }
+            for (int c = 0; c < 3; ++c) {
+                var[c] = fmaxf(0.0f, sq[c] - mean[c] * mean[c]);
+                dev[c] = sqrtf(var[c]);
+            }
+            float hist[4] = {0, 0, 0, 0}, meta[4] = {0, 0, 0, 0}, total = 0.0f;
+            uint32_t history_mask = 0u;
+            const float *M = P->prev;
+            float cx = ((M[0] * position[0] + M[1] * position[1]) + M[2] * position[2]) + M[3];
+            float cy = ((M[4] * position[0] + M[5] * position[1]) + M[6] * position[2]) + M[7];
+            float cw = ((M[12] * position[0] + M[13] * position[1]) + M[14] * position[2]) + M[15];
+            float u = (cx / cw) * 0.5f + 0.5f, v = 0.5f - (cy / cw) * 0.5f;
+            int projected = cw > 0.0f && isfinite(u) && isfinite(v);
+            float px = u * (float)P->width, py = v * (float)P->height;
+            if (projected && P->history_valid && !screen_dirty(P, position) && P->temporal_blend > 0.0f &&
+                P->capacity > 0.0f && px >= 0.0f && py >= 0.0f && px < (float)P->width && py < (float)P->height) {
+                float lx = px - 0.5f, ly = py - 0.5f;
+                int bx = (int)floorf(lx), by = (int)floorf(ly);
+                float lastx = (float)(P->width - 1u), lasty = (float)(P->height - 1u);
+                float leftx = fminf((float)bx, lastx), lefty = fminf((float)by, lasty);
+                float rightx = fminf((float)(bx + 1), lastx), righty = fminf((float)(by + 1), lasty);
+                float fx = saturatef((lx - leftx) / fmaxf(rightx - leftx, 1.0f));
+                float fy = saturatef((ly - lefty) / fmaxf(righty - lefty, 1.0f));
+                for (int corner = 0; corner < 4; ++corner) {
+                    int ox = bx + (corner & 1), oy = by + (corner >> 1);
+                    if (ox < 0 || oy < 0 || ox >= (int)P->width || oy >= (int)P->height) continue;
+                    size_t q = (size_t)oy * P->width + ox;
+                    const float *old = hw_irr(H, q), *om = hw_meta(H, q), *onrm = hw_nrm(H, q), *opos = hw_pos(H, q);
+                    if (om[0] <= 0.0f || old[3] <= 0.0f || !finite3(old) || sdot(gn, onrm) < 0.95f ||
+                        !screen_compatible(1, id, gn, om[3] > 0.0f, hw_id(H, q), onrm))
+                        continue;
+                    if (screen_dirty(P, opos)) continue;
+                    float delta[3] = {opos[0] - position[0], opos[1] - position[1], opos[2] - position[2]};
+                    if (plane_distance(delta, gn, onrm) > P->tolerance) continue;
+                    float wx = (corner & 1) ? fx : 1.0f - fx, wy = (corner >> 1) ? fy : 1.0f - fy;
+                    float weight = wx * wy;
+                    if (weight <= 0.0f) continue;
+                    if (om[2] <= 0.0f) continue;
+                    history_mask = 1u;
+                    for (int c = 0; c < 4; ++c) {
+                        hist[c] = hist[c] + old[c] * weight;
+                        meta[c] = meta[c] + om[c] * weight;
+                    }
+                    total += weight;
+                }
+            }
+            float capacity = fmaxf(P->capacity, 0.0f);
+            float retained = current_supported ? freshness : 0.0f;
+            float out_var = current_supported ? lum3(var) : 0.0f;
+            if (total > 0.00001f) {
+                for (int c = 0; c < 4; ++c) {
+                    hist[c] /= total;
+                    meta[c] /= total;
+                }
+                output_mask = history_mask;
+                float old_length = fminf(meta[0], capacity);
+                if (current_supported) {
+                    if (freshness <= 0.00001f) {
+                        memcpy(center, hist, 12);
+                        retained = old_length;
+                        out_var = meta[1];
+                    } else {
+                        int complete = freshness >= 1.0f;
+                        float clipped[3] = {hist[0], hist[1], hist[2]};
+                        if (count >= 2.0f && complete) {
+                            float d = lum3(hist) - lum3(center);
+                            float tv = fmaxf(meta[1], d * d * 0.25f);
+                            float st = sqrtf(tv);
+                            for (int c = 0; c < 3; ++c) {
+                                float r = 2.5f * fmaxf(dev[c], st) + 0.0001f;
+                                clipped[c] = fminf(fmaxf(hist[c], fmaxf(0.0f, mean[c] - r)), mean[c] + r);
+                            }
+                        }
+                        float hl = lum3(hist), cl = lum3(center);
+                        float delta = hl - cl;
+                        float ll = lum3(clipped);
+                        float change = fabsf(ll - cl) / fmaxf(fmaxf(ll, cl), 0.001f);
+                        float reactive = P->scene_changed && complete ? 1.0f - change * change : 1.0f;
+                        float ref_l = fmaxf(fmaxf(hl, cl), 0.001f);
+                        float noise = sqrtf(fmaxf(meta[1], 0.0f)) / ref_l;
+                        float threshold = fminf(fmaxf(3.0f * noise, 0.05f), 0.25f);
+                        int step = freshness > 0.0f && complete && P->scene_changed && change > threshold;
+                        if (step) old_length = 0.0f;
+                        float weight = fminf(P->temporal_blend, old_length / (old_length + 1.0f));
+                        weight = weight / fmaxf(weight + freshness * (1.0f - weight), 1e-8f);
+                        weight *= reactive;
+                        if (step) weight = 0.0f;
+                        for (int c = 0; c < 3; ++c) center[c] = lerpf_(center[c], clipped[c], weight);
+                        retained = fminf(capacity, old_length + freshness);
+                        out_var = lerpf_(lum3(var), meta[1], weight) + (weight * (1.0f - weight)) * (delta * delta);
+                    }
+                } else {
+                    memcpy(center, hist, 12);
+                    retained = old_length;
+                    out_var = meta[1];
+                }
+            }
+            center[3] = current_supported || retained > 0.0f ? depth : 0.0f;
+            memcpy(o, center, 16);
+            o[4] = retained;
+            o[5] = out_var;
+            o[6] = (float)output_mask;
+            o[7] = 1.0f;
+            memcpy(o + 8, position, 16);
+            memcpy(o + 12, gn, 16);
+            memcpy(o + 16, id, 8);
+        }
+}
+
+static void screen_denoise(const ScreenParams *P, uint32_t step, const float *pos, const float *T,
+                           const float *src, const float *src_mask, float *dst, float *dst_mask) {
+    static const float kernel[5] = {1.0f, 4.0f, 6.0f, 4.0f, 1.0f};
+    for (int y = 0; y < (int)P->height; ++y)
+        for (int x = 0; x < (int)P->width; ++x) {
+            size_t p = (size_t)y * P->width + x;
+            const float *center = src + 4 * p;
+            int has_light = center[3] > 0.0f && isfinite(center[3]) && finite3(center);
+            const float *position = pos + 4 * p;
+            float depth = has_light ? center[3] : position[3];
+            if (depth <= 0.0f || !isfinite(depth)) {
+                memset(dst + 4 * p, 0, 16);
+                dst_mask[p] = 0.0f;
+                continue;
+            }
+            const float *tm = hw_meta(T, p);
+            int surface = tm[3] > 0.0f;
+            const uint32_t *id = hw_id(T, p);
+            const float *gn = hw_nrm(T, p);
+            uint32_t center_mask = (uint32_t)src_mask[p];
+            int center_supported = tm[0] > 0.0f;
+            float variance = fmaxf(tm[1], 0.0f);
+            float cl = lum3(center);
+            float sum[3] = {0, 0, 0}, total = 0.0f;
+            for (int dy = -2; dy <= 2; ++dy) {
+                int xr = abs(dy) == 2 ? 1 : 2;
+                for (int dx = -xr; dx <= xr; ++dx) {
+                    int qx = x + dx * (int)step, qy = y + dy * (int)step;
+                    if (qx < 0 || qy < 0 || qx >= (int)P->width || qy >= (int)P->height) continue;
+                    size_t q = (size_t)qy * P->width + qx;
+                    const float *value = src + 4 * q;
+                    if (value[3] <= 0.0f) continue;
+                    const float *om = hw_meta(T, q);
+                    if (om[0] <= 0.0f) continue;
+                    const float *on = hw_nrm(T, q);
+                    if (!screen_compatible(surface, id, gn, om[3] > 0.0f, hw_id(T, q), on)) continue;
+                    uint32_t other_mask = (uint32_t)src_mask[q];
+                    if (center_mask != 0u && other_mask != center_mask) continue;
+                    if (center_mask == 0u && other_mask == 0u) continue;
+                    const float *op = pos + 4 * q;
+                    if (sdot(gn, on) < 0.95f) continue;
+                    float delta[3] = {op[0] - position[0], op[1] - position[1], op[2] - position[2]};
+                    float pd = plane_distance(delta, gn, on);
+                    if (pd > P->tolerance) continue;
+                    float c = fmaxf(0.0f, sdot(gn, on));
+                    float c2 = c * c, c4 = c2 * c2, c8 = c4 * c4, c16 = c8 * c8, c32 = c16 * c16;
+                    float weight = ((kernel[dx + 2] * kernel[dy + 2]) * c32) * expf(-pd / P->plane_scale);
+                    if (center_supported) {
+                        float scale = fmaxf(0.02f, 2.0f * sqrtf(fmaxf(variance + om[1], 0.0f)));
+                        weight *= expf(-fabsf(lum3(value) - cl) / scale);
+                    }
+                    for (int k = 0; k < 3; ++k) sum[k] += value[k] * weight;
+                    total += weight;
+                }
+            }
+            int filtered = total > 0.00001f;
+            float *o = dst + 4 * p;
+            if (filtered) {
+                for (int k = 0; k < 3; ++k) o[k] = sum[k] / total;
+            } else {
+                memcpy(o, center, 12);
+            }
+            float out_depth = has_light || center_supported || filtered ? depth : 0.0f;
+            o[3] = out_depth;
+            dst_mask[p] = out_depth > 0.0f ? 1.0f : 0.0f;
+        }
+}
+
+void orc_screen_filter(const LuxSettings *settings, uint32_t width, uint32_t height, const float *irradiance,
+                       const float *position, const float *normal, const uint32_t *identity,
+                       const float previous_clip_from_world[16], const float *dirty, uint32_t scene_changed,
+                       uint32_t spatial_filter_steps, uint32_t history_valid, const float *history_in,
+                       float *history_out, float *out) {
+    LuxSettings st = *settings;
+    ScreenParams P;
+    memset(&P, 0, sizeof P);
+    P.width = width;
+    P.height = height;
+    P.temporal_blend = st.temporal_blend;
+    P.capacity = (float)st.history_frames;
+    P.tolerance = fmaxf(st.normal_bias * 2.0f, st.probe_spacing * 0.02f);
+    P.plane_scale = fmaxf(st.normal_bias * 2.0f, st.probe_spacing * 0.05f);
+    P.history_valid = history_valid;
+    P.scene_changed = scene_changed;
+    if (dirty) {
+        P.dirty = 1;
+        memcpy(P.dirty_lo, dirty, 12);
+        memcpy(P.dirty_hi, dirty + 3, 12);
+    }
+    memcpy(P.prev, previous_clip_from_world, sizeof P.prev);
+    screen_temporal(&P, irradiance, position, normal, identity, history_in, history_out);
+    size_t n = (size_t)width * height;
+    if (spatial_filter_steps == 0) {
+        for (size_t p = 0; p < n; ++p) memcpy(out + 4 * p, hw_irr(history_out, p), 16);
+        return;
+    }
+    float *a = (float *)malloc(n * 16), *b = (float *)malloc(n * 16);
+    float *ma = (float *)malloc(n * 4), *mb = (float *)malloc(n * 4);
+    float *src = a, *src_mask = ma;
+    for (size_t p = 0; p < n; ++p) {
+        memcpy(a + 4 * p, hw_irr(history_out, p), 16);
+        ma[p] = hw_meta(history_out, p)[2];
+    }
+    for (uint32_t level = 0; level < spatial_filter_steps; ++level) {
+        uint32_t step = level == 0 ? 1u : (1u << level);
+        float *dst = src == a ? b : a, *dst_mask = src_mask == ma ? mb : ma;
+        screen_denoise(&P, step, position, history_out, src, src_mask, dst, dst_mask);
+        src = dst;
+        src_mask = dst_mask;
+    }
+    memcpy(out, src, n * 16);
+    free(a);
+    free(b);
+    free(ma);
+    free(mb);
+}
+#undef HW

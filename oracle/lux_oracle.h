@@ -121,6 +121,19 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *scene, const LuxSettings *setting
                                const OrcFrame *previous, const float *dirty, uint32_t dirty_count,
                                uint32_t max_cells, uint64_t max_entries, const OrcFrame *feedback, uint32_t flags,
                                float *hit_pos, float *hit_nrm);
+/* Screen reconstruction (temporal + denoise, shaders/cascades.slang:310-690):
+ * inputs per pixel of a width x height image (row-major): irradiance float4
+ * (resolve output), position float4 (xyz, view depth), normal float4, identity
+ * uint32 x 2; `dirty` = 6 floats (lo, hi) or NULL.  history_in / history_out:
+ * ORC_SCREEN_WORDS floats per pixel (irradiance rgb + depth; retained length,
+ * variance, support mask, surface flag; position; normal; identity bits).
+ * `out` float4 per pixel. */
+#define ORC_SCREEN_WORDS 18
+void orc_screen_filter(const LuxSettings *settings, uint32_t width, uint32_t height, const float *irradiance,
+                       const float *position, const float *normal, const uint32_t *identity,
+                       const float previous_clip_from_world[16], const float *dirty, uint32_t scene_changed,
+                       uint32_t spatial_filter_steps, uint32_t history_valid, const float *history_in,
+                       float *history_out, float *out);
 void orc_history_blend(const LuxSettings *settings, uint32_t samples, const float fresh[4], const float *old,
                        const float *old_mass, float out[4], float mass[2]);
 OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,

@@ -210,3 +210,73 @@ def cornell_dense_settings(**kw) -> bp.RadianceCascades:
                 emissive_samples=16, normal_bias=0.005)
     base.update(kw)
     return bp.RadianceCascades(**base).sanitized()
+
+
+def camera_clip(eye, target, fov_y_deg: float, width: int, height: int):
+    """scenes.clip_from_world and the camera basis of scenes.camera_rays."""
+    from bevy_penumbra_b200 import scenes
+    eye = np.asarray(eye, np.float64)
+    fwd = np.asarray(target, np.float64) - eye
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, (0.0, 1.0, 0.0))
+    right /= np.linalg.norm(right)
+    up = np.cross(right, fwd)
+    t = np.tan(np.radians(fov_y_deg) * 0.5)
+    return scenes.clip_from_world(eye, target, fov_y_deg, width, height, far=100.0), (fwd, right, up, t,
+                                                                                     width / height)
+
+
+def synthetic_screen(width: int, height: int, eye, target, seed: int = 0, fov_y_deg: float = 60.0):
+    """An analytic G-buffer for the screen filter: a floor (identity 1), a box
+    (identity 2) and a back wall (identity 3) seen through a pinhole camera;
+    irradiance is a smooth field plus seeded noise with rawGiSupportAlpha
+    (1 + 0.25 coverage; -1 unsupported; 0 without a surface).  Returns
+    (irradiance, position (w = view depth), normal, identity, clip_from_world)."""
+    clip, (fwd, right, up, t, aspect) = camera_clip(eye, target, fov_y_deg, width, height)
+    eye = np.asarray(eye, np.float64)
+    xs = (np.arange(width) + 0.5) / width * 2.0 - 1.0
+    ys = 1.0 - (np.arange(height) + 0.5) / height * 2.0
+    gx, gy = np.meshgrid(xs, ys)
+    d = fwd + gx[..., None] * (t * aspect) * right + gy[..., None] * t * up
+    d /= np.linalg.norm(d, axis=-1, keepdims=True)
+    best = np.full((height, width), np.inf)
+    nrm = np.zeros((height, width, 3))
+    ident = np.zeros((height, width), np.uint32)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tf = -eye[1] / d[..., 1]  # floor y = 0
+        hit = (tf > 1e-4) & (tf < best)
+        best[hit], nrm[hit], ident[hit] = tf[hit], (0.0, 1.0, 0.0), 1
+        tw = (-2.0 - eye[2]) / d[..., 2]  # back wall z = -2
+        hit = (tw > 1e-4) & (tw < best)
+        best[hit], nrm[hit], ident[hit] = tw[hit], (0.0, 0.0, 1.0), 3
+        lo, hi = np.array([-0.4, 0.0, -0.4]), np.array([0.4, 0.8, 0.4])
+        t0 = (lo - eye) / d
+        t1 = (hi - eye) / d
+        tn, tx = np.minimum(t0, t1), np.maximum(t0, t1)
+        near, far = tn.max(-1), tx.min(-1)
+        axis = tn.argmax(-1)
+        hit = (near <= far) & (near > 1e-4) & (near < best)
+        face = np.zeros((height, width, 3))
+        np.put_along_axis(face, axis[..., None], 1.0, axis=-1)
+        sign = -np.sign(np.take_along_axis(d, axis[..., None], -1))
+        best[hit], nrm[hit], ident[hit] = near[hit], (face * sign)[hit], 2
+    ok = np.isfinite(best)
+    p = eye + d * np.where(ok, best, 0.0)[..., None]
+    rng = np.random.default_rng(seed)
+    field = 0.5 + 0.3 * np.sin(3.0 * p[..., 0]) * np.cos(2.0 * p[..., 2]) + 0.2 * p[..., 1] + 0.1 * ident
+    noise = 1.0 + 0.1 * rng.standard_normal((height, width, 3))
+    irr = np.zeros((height, width, 4), np.float32)
+    irr[..., :3] = field[..., None] * noise * np.array([1.0, 0.9, 0.8])
+    u = rng.random((height, width))
+    coverage = np.where(u < 0.6, 1.0, rng.uniform(0.2, 1.0, (height, width)))
+    irr[..., 3] = np.where(u > 0.9, -1.0, 1.0 + 0.25 * coverage)
+    irr[~ok] = 0.0
+    pos = np.zeros((height, width, 4), np.float32)
+    pos[..., :3] = p
+    pos[..., 3] = np.where(ok, best * (d @ fwd), 0.0)
+    pos[~ok, :3] = 0.0
+    normal = np.zeros((height, width, 4), np.float32)
+    normal[..., :3] = nrm
+    identity = np.zeros((height, width, 2), np.uint32)
+    identity[..., 0] = ident
+    return irr, pos, normal, identity, clip
