@@ -802,6 +802,14 @@ __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FramePa
     float sx = 0.0f, sy = 0.0f, sz = 0.0f, total = 0.0f, potential = 0.0f;
     unsigned long long base = V.level_base[child_level];
     uint32_t dirs = F.dirs[child_level];
+    // The eight corner records are fetched before any is used (record 0
+    // stands in for a missing corner), so their latencies overlap.
+    float4 corner_value[8];
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner)
+        corner_value[corner] = __ldg(V.merged + (ids[corner] == lux::kEmpty
+                                                     ? 0ull
+                                                     : base + (unsigned long long)ids[corner] * dirs + dir));
 #pragma unroll
     for (uint32_t corner = 0; corner < 8u; ++corner) {
         float ax = (corner & 1u) == 0u ? 1.0f - frac.x : frac.x;
@@ -811,7 +819,7 @@ __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FramePa
         if (!(w > 0.0f)) continue;
         potential += w;
         if (ids[corner] == lux::kEmpty) continue;
-        float4 s = __ldg(V.merged + base + (unsigned long long)ids[corner] * dirs + dir);
+        float4 s = corner_value[corner];
         if (s.w > 0.0f && isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w)) {
             float sw = w * lux::saturate(s.w);
             sx = sx + s.x * sw;
@@ -1664,6 +1672,10 @@ struct LuxView {
     uint32_t dir_capacity = 0;
     void *stage_pos = nullptr, *stage_nrm = nullptr, *stage_ppos = nullptr, *stage_pnrm = nullptr, *stage_out = nullptr;
     uint32_t stage_receivers = 0, stage_points = 0;
+    // lux_view_frame_host: the resolve points' upload runs on this stream
+    // while the frame traces; `stage_ready` orders the resolve after it.
+    cudaStream_t stage_stream = nullptr;
+    cudaEvent_t stage_ready = nullptr;
     FrameParams last{};
     bool has_frame = false;
     // World history: the other buffer set (swapped with dev's at each
@@ -1809,8 +1821,11 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
                     D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.ray_extra, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
                     D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
+    if (v->stage_stream) cudaStreamSynchronize(v->stage_stream);
     for (void *p : ptrs)
         if (p) cudaFree(p);
+    if (v->stage_ready) cudaEventDestroy(v->stage_ready);
+    if (v->stage_stream) cudaStreamDestroy(v->stage_stream);
     for (int i = 0; i < kTimingEvents; ++i)
         if (v->ev[i]) cudaEventDestroy(v->ev[i]);
     cache_buffers_free(v);
@@ -2279,6 +2294,13 @@ extern "C" lux_status lux_view_resolve(LuxView *v, const LuxSettings *settings, 
 }
 
 static lux_status ensure_stage(LuxView *v, uint32_t receivers, uint32_t points) {
+    if (!v->stage_stream) {
+        if (cudaStreamCreateWithFlags(&v->stage_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&v->stage_ready, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return lux_fail(v->ctx, LUX_ERR_CUDA, "frame_host: staging stream creation failed");
+        }
+    }
     if (receivers > v->stage_receivers) {
         cudaFree(v->stage_pos);
         cudaFree(v->stage_nrm);
@@ -2313,16 +2335,26 @@ extern "C" lux_status lux_view_frame_host(LuxView *v, const LuxScene *scene, con
                                           const float *pnrm, uint32_t points, float *out) {
     if (!v || !scene || !settings || (receivers && (!rpos || !rnrm)) || (points && (!ppos || !pnrm || !out)))
         return LUX_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(v->ctx->device);
     lux_status s = ensure_stage(v, receivers, points);
     if (s != LUX_OK) return s;
     cudaStream_t st = v->ctx->stream;
+    // The receivers go first on the frame's stream; the resolve points (the
+    // larger upload) follow on the staging stream and overlap the trace.
+    // The previous call ended with a synchronize, so no resolve still reads
+    // the staging buffers.
     cudaMemcpyAsync(v->stage_pos, rpos, (size_t)receivers * 16, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(v->stage_nrm, rnrm, (size_t)receivers * 16, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(v->stage_ppos, ppos, (size_t)points * 16, cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(v->stage_pnrm, pnrm, (size_t)points * 16, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(v->stage_ppos, ppos, (size_t)points * 16, cudaMemcpyHostToDevice, v->stage_stream);
+    cudaMemcpyAsync(v->stage_pnrm, pnrm, (size_t)points * 16, cudaMemcpyHostToDevice, v->stage_stream);
+    cudaEventRecord(v->stage_ready, v->stage_stream);
     LuxReceivers rc{(const float *)v->stage_pos, (const float *)v->stage_nrm, receivers};
     s = lux_view_trace_merge(v, scene, settings, &rc);
-    if (s != LUX_OK) return s;
+    if (s != LUX_OK) {
+        cudaStreamSynchronize(v->stage_stream);
+        return s;
+    }
+    cudaStreamWaitEvent(st, v->stage_ready, 0);
     s = lux_view_resolve(v, settings, (const float *)v->stage_ppos, (const float *)v->stage_pnrm, points,
                          (float *)v->stage_out);
     if (s != LUX_OK) return s;
