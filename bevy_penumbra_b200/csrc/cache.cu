@@ -605,21 +605,24 @@ __global__ void adam_kernel(AdamParams P, float *__restrict__ param, float *__re
     }
 }
 
-// adam_kernel on four consecutive parameters per thread (the hash table:
-// n is a multiple of 4), with the BF16 copy written as one 8-byte store.
+// Adam on four consecutive parameters per thread (the hash table: n is a
+// multiple of 4), with the BF16 copy written as one 8-byte store.  Sparse
+// ("lazy") Adam: a parameter this step's samples did not reach (zero
+// gradient) keeps its value and moments, so a step reads only the gradients
+// of the untouched entries -- a batch reaches a quarter of a fine level's
+// entries at most.  A parameter's first update is the dense step's.
 __global__ void adam4_kernel(AdamParams P, float4 *__restrict__ param, float4 *__restrict__ grad,
                              float4 *__restrict__ m, float4 *__restrict__ v, size_t n4, uint2 *__restrict__ out) {
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
-        float4 g = grad[i], mi = m[i];
-        if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f && mi.x == 0.0f && mi.y == 0.0f &&
-            mi.z == 0.0f && mi.w == 0.0f)
-            continue;  // never touched: nothing to move
+        float4 g = grad[i];
+        if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f) continue;  // not reached this step
         grad[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float4 vi = v[i], p = param[i];
+        float4 mi = m[i], vi = v[i], p = param[i];
         float gs[4] = {g.x, g.y, g.z, g.w}, ms[4] = {mi.x, mi.y, mi.z, mi.w}, vs[4] = {vi.x, vi.y, vi.z, vi.w};
         float ps[4] = {p.x, p.y, p.z, p.w};
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
+            if (gs[k] == 0.0f) continue;
             ms[k] = P.beta1 * ms[k] + (1.0f - P.beta1) * gs[k];
             vs[k] = P.beta2 * vs[k] + (1.0f - P.beta2) * gs[k] * gs[k];
             ps[k] = ps[k] - P.lr * (ms[k] / P.correction1) / (sqrtf(vs[k] / P.correction2) + P.eps);
