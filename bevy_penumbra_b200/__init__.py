@@ -387,6 +387,21 @@ def error_stats(ctx: LuxContext, estimate_ptr: int, reference_ptr: int, count: i
             "points": int(used), "max_abs_error": mx}
 
 
+def camera_struct(clip_from_world, position, viewport_height: int, target_pixels: int = 1) -> N.LuxCamera:
+    """A LuxCamera for distance LODs (enabled)."""
+    cam = N.LuxCamera()
+    m = np.asarray(clip_from_world, np.float32).reshape(16)
+    for i in range(16):
+        cam.clip_from_world[i] = float(m[i])
+    pos = np.asarray(position, np.float32).reshape(3)
+    for a in range(3):
+        cam.position[a] = float(pos[a])
+    cam.viewport_height = int(viewport_height)
+    cam.target_pixels = int(target_pixels)
+    cam.enabled = 1
+    return cam
+
+
 class SplitView:
     """Per-view transport state (ViewBuffers) and one frame of
     seed -> trace -> deposit -> merge -> pack, then resolve."""
@@ -511,6 +526,18 @@ class SplitView:
         out = np.zeros(count, dtype=HIT_DTYPE)
         self.ctx.check(lib().lux_view_read_hits(self.handle, _ptr(out), count))
         return out
+
+    def set_camera(self, clip_from_world=None, position=None, viewport_height: int = 0,
+                   target_pixels: int = 1) -> None:
+        """lux_view_set_camera: distance LODs of later Split frames and
+        resolves from this camera (clip_from_world 4x4 row-major, world
+        position, viewport height in pixels, probe footprint in pixels);
+        None disables them."""
+        if clip_from_world is None:
+            self.ctx.check(lib().lux_view_set_camera(self.handle, None))
+            return
+        cam = camera_struct(clip_from_world, position, viewport_height, target_pixels)
+        self.ctx.check(lib().lux_view_set_camera(self.handle, C.byref(cam)))
 
     def secondary(self) -> "SplitView | None":
         """lux_view_secondary: the multi-bounce secondary cache of this view

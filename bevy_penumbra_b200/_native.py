@@ -130,6 +130,11 @@ class LuxBatchInfo(C.Structure):
                 ("interval_rays", C.c_uint64), ("kernels_per_frame", C.c_uint32), ("reserved", C.c_uint32)]
 
 
+class LuxCamera(C.Structure):
+    _fields_ = [("clip_from_world", C.c_float * 16), ("position", C.c_float * 3), ("viewport_height", C.c_uint32),
+                ("target_pixels", C.c_uint32), ("enabled", C.c_uint32)]
+
+
 class LuxScreenFrame(C.Structure):
     _fields_ = [("irradiance", C.c_void_p), ("position", C.c_void_p), ("normal", C.c_void_p),
                 ("identity", C.c_void_p), ("previous_clip_from_world", C.c_float * 16),
@@ -185,6 +190,7 @@ SIGNATURES = {
     "lux_view_read_hits": (C.c_int, [P, P, U32]),
     "lux_view_reset_history": (C.c_int, [P]),
     "lux_view_secondary": (C.c_int, [P, C.POINTER(C.c_void_p)]),
+    "lux_view_set_camera": (C.c_int, [P, C.c_void_p]),
     "lux_view_invalidate_bounds": (C.c_int, [P, P, P]),
     "lux_view_set_cache": (C.c_int, [P, C.POINTER(LuxCacheMode)]),
     "lux_view_cache_stats": (C.c_int, [P, C.POINTER(LuxCacheFrameStats)]),

@@ -221,20 +221,69 @@ LUX_HD uint32_t texel_index(int32_t x, int32_t y) {
     return (uint32_t)(y * 6 + x);
 }
 
-// Cell keys of the world grid: 21 bits per axis, biased by 2^20.
-LUX_HD uint64_t pack_cell(int32_t x, int32_t y, int32_t z) {
-    return ((uint64_t)((uint32_t)(x + (1 << 20)) & 0x1fffffu)) |
-           ((uint64_t)((uint32_t)(y + (1 << 20)) & 0x1fffffu) << 21) |
-           ((uint64_t)((uint32_t)(z + (1 << 20)) & 0x1fffffu) << 42);
+// Cell keys of the world grid: 19 bits per axis biased by 2^18, and the
+// probe LOD in bits 57-61 (cacheKey's lod field, shaders/common.slang:418-422).
+LUX_HD uint64_t pack_cell(int32_t x, int32_t y, int32_t z, uint32_t lod = 0u) {
+    return ((uint64_t)((uint32_t)(x + (1 << 18)) & 0x7ffffu)) |
+           ((uint64_t)((uint32_t)(y + (1 << 18)) & 0x7ffffu) << 19) |
+           ((uint64_t)((uint32_t)(z + (1 << 18)) & 0x7ffffu) << 38) | ((uint64_t)(lod & 31u) << 57);
 }
-LUX_HD void unpack_cell(uint64_t key, int32_t &x, int32_t &y, int32_t &z) {
-    x = (int32_t)(key & 0x1fffffull) - (1 << 20);
-    y = (int32_t)((key >> 21) & 0x1fffffull) - (1 << 20);
-    z = (int32_t)((key >> 42) & 0x1fffffull) - (1 << 20);
+LUX_HD void unpack_cell(uint64_t key, int32_t &x, int32_t &y, int32_t &z, uint32_t &lod) {
+    x = (int32_t)(key & 0x7ffffull) - (1 << 18);
+    y = (int32_t)((key >> 19) & 0x7ffffull) - (1 << 18);
+    z = (int32_t)((key >> 38) & 0x7ffffull) - (1 << 18);
+    lod = (uint32_t)(key >> 57) & 31u;
 }
 LUX_HD bool cell_in_range(int32_t x, int32_t y, int32_t z) {
-    const int32_t lim = 1 << 20;
+    const int32_t lim = 1 << 18;
     return x >= -lim && x < lim && y >= -lim && y < lim && z >= -lim && z < lim;
+}
+
+// Distance LODs (MAX_PROBE_LOD, shaders/common.slang:16).
+constexpr uint32_t kMaxLod = 24u;
+// 2^lod exactly (lod <= kMaxLod): spacing and interval ends scale by it.
+LUX_HD float lod_scale(uint32_t lod) { return as_float((127u + lod) << 23); }
+// The LOD field of a cell key's w (level << 12 | lod << 18).
+LUX_HD uint32_t key_lod(int32_t w) { return ((uint32_t)w >> 18) & 31u; }
+
+// splitLodBlendForParameters (shaders/common.slang:431-461) with the
+// camera terms precomputed per frame: perspective cameras scale by the
+// Chebyshev distance from the camera over `base` (max(focal pixels x
+// spacing / target pixels, spacing)); orthographic cameras use the fixed
+// `ortho_scale` (target pixels / projected spacing).  floor(log2(x)) for
+// x >= 1 is the float's exponent (exact), and the next boundary 2^(low+1) is
+// an exact power of two.
+LUX_HD void lod_blend(bool perspective, float cx, float cy, float cz, float base, float ortho_scale, f3 p,
+                      uint32_t &low, uint32_t &high, float &blend) {
+    float scale;
+    if (perspective) {
+        float ox = fabsf(p.x - cx), oy = fabsf(p.y - cy), oz = fabsf(p.z - cz);
+        scale = fmaxf(ox, fmaxf(oy, oz)) / base;
+    } else {
+        scale = ortho_scale;
+    }
+    float s1 = fmaxf(scale, 1.0f);
+    uint32_t e = s1 < INFINITY ? (as_uint(s1) >> 23) - 127u : kMaxLod;
+    low = e < kMaxLod ? e : kMaxLod;
+    high = low;
+    blend = 0.0f;
+    if (low < kMaxLod) {
+        float next = lod_scale(low + 1u);
+        float overlap = 0.9f * next;
+        if (scale >= overlap && scale < next) {
+            high = low + 1u;
+            blend = saturate((scale - overlap) / (next - overlap));
+        }
+    }
+}
+
+// The seeded variant of a receiver in an LOD overlap: temporal
+// low-discrepancy selection of the high LOD with probability `blend`
+// (seed, shaders/split.slang:747-752).
+LUX_HD bool lod_selects_high(uint32_t sample, uint32_t frame, float blend) {
+    uint32_t bits = transport_hash(sample ^ (frame * 0x9e3779b9u));
+    float phase = (float)(bits >> 8) * (1.0f / 16777216.0f);
+    return phase < blend;
 }
 constexpr uint64_t kEmptyCell = 0xffffffffffffffffull;
 

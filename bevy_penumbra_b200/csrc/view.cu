@@ -86,6 +86,12 @@ struct FrameParams {
     // slot per primary receiver, and a slot with position.w == 0 holds none.
     uint32_t sparse;       // receivers with position.w == 0 are absent
     uint32_t record_hits;  // write each receiver's hit surface (ray frame % R) to hit_pos / hit_nrm
+    // Distance LODs (splitLodBlendForParameters, shaders/common.slang:431-461;
+    // lod_enabled = 0: every receiver and resolve point uses LOD 0).
+    uint32_t lod_enabled, lod_perspective;
+    float lod_camera[3];
+    float lod_base;         // perspective: max(focal pixels x spacing / target pixels, spacing)
+    float lod_ortho_scale;  // orthographic: target pixels / max(focal pixels x spacing, 1e-20)
 };
 
 // Device state of a view (ViewBuffers, src/render.rs:5077-5160).
@@ -96,6 +102,7 @@ struct ViewDevice {
     uint32_t *cell_count;           // [levels]
     unsigned long long *level_base; // [levels]
     uint32_t *receiver_cell;        // [levels][max_receivers]
+    uint32_t *receiver_lod;         // [max_receivers] the LOD each receiver's rays deposit into
     uint32_t *corner_ids;           // [levels][cell_capacity][8] (level+1 ids)
     float4 *corner_frac;            // [levels][cell_capacity]
     float4 *accum;                  // [entries] J sum rgb, non-terminating count
@@ -161,21 +168,35 @@ __device__ __forceinline__ void add_stats(unsigned long long *stats, unsigned lo
     }
 }
 
+// Spacing of a level at an LOD (spacing, shaders/common.slang:414-416).
+__device__ __forceinline__ float level_spacing(const FrameParams &F, uint32_t level, uint32_t lod) {
+    return F.spacing[level] * lux::lod_scale(lod);
+}
+
 __device__ __forceinline__ void cell_of(const FrameParams &F, uint32_t level, f3 p, int32_t &x, int32_t &y,
-                                        int32_t &z) {
-    float s = F.spacing[level];
+                                        int32_t &z, uint32_t lod = 0u) {
+    float s = level_spacing(F, level, lod);
     x = (int32_t)floorf(p.x / s);
     y = (int32_t)floorf(p.y / s);
     z = (int32_t)floorf(p.z / s);
 }
 
+// A point's LOD pair and blend (0, 0, 0 without distance LODs).
+__device__ __forceinline__ void point_lod(const FrameParams &F, f3 p, uint32_t &low, uint32_t &high, float &blend) {
+    low = high = 0u;
+    blend = 0.0f;
+    if (F.lod_enabled)
+        lux::lod_blend(F.lod_perspective != 0u, F.lod_camera[0], F.lod_camera[1], F.lod_camera[2], F.lod_base,
+                       F.lod_ortho_scale, p, low, high, blend);
+}
+
 // Probe of a level directory; returns the slot or kEmpty.
 __device__ __forceinline__ uint32_t dir_find(const ViewDevice &V, const FrameParams &F, uint32_t level, int32_t x,
-                                             int32_t y, int32_t z) {
+                                             int32_t y, int32_t z, uint32_t lod = 0u) {
     if (!lux::cell_in_range(x, y, z)) return lux::kEmpty;
-    unsigned long long key = lux::pack_cell(x, y, z);
+    unsigned long long key = lux::pack_cell(x, y, z, lod);
     const unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
-    uint32_t slot = lux::hash_key(x, y, z, (int32_t)level, F.dir_capacity);
+    uint32_t slot = lux::hash_key(x, y, z, (int32_t)(level | (lod << 18)), F.dir_capacity);
     for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
         unsigned long long k = keys[slot];
         if (k == key) return slot;
@@ -186,8 +207,8 @@ __device__ __forceinline__ uint32_t dir_find(const ViewDevice &V, const FramePar
 }
 
 __device__ __forceinline__ uint32_t cell_id(const ViewDevice &V, const FrameParams &F, uint32_t level, int32_t x,
-                                            int32_t y, int32_t z) {
-    uint32_t slot = dir_find(V, F, level, x, y, z);
+                                            int32_t y, int32_t z, uint32_t lod = 0u) {
+    uint32_t slot = dir_find(V, F, level, x, y, z, lod);
     return slot == lux::kEmpty ? lux::kEmpty : V.dir_ids[(size_t)level * F.dir_capacity + slot];
 }
 
@@ -211,32 +232,39 @@ __global__ void clear_kernel(ViewDevice V, FrameParams F) {
 }
 
 // seed: insert every receiver's cell of every level (insertProbeDescriptor,
-// shaders/split.slang:292-319, with a 64-bit key compare-and-swap).
+// shaders/split.slang:292-319, with a 64-bit key compare-and-swap); in an
+// LOD overlap both LOD variants' cells are seeded (seed,
+// shaders/split.slang:758-786).
+__device__ __forceinline__ void seed_cell(ViewDevice &V, const FrameParams &F, uint32_t level, f3 p, uint32_t lod) {
+    int32_t x, y, z;
+    cell_of(F, level, p, x, y, z, lod);
+    if (!lux::cell_in_range(x, y, z)) {
+        atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+        return;
+    }
+    unsigned long long key = lux::pack_cell(x, y, z, lod);
+    unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
+    uint32_t slot = lux::hash_key(x, y, z, (int32_t)(level | (lod << 18)), F.dir_capacity);
+    for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+        unsigned long long prev = atomicCAS(&keys[slot], lux::kEmptyCell, key);
+        if (prev == lux::kEmptyCell || prev == key) return;
+        slot = (slot + 1u) & (F.dir_capacity - 1u);
+    }
+    atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+}
+
 __global__ void seed_insert_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
     size_t n = (size_t)F.receivers * F.levels;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
         float4 p = pos[r];
         if (F.sparse && p.w == 0.0f) continue;
-        int32_t x, y, z;
-        cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
-        if (!lux::cell_in_range(x, y, z)) {
-            atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
-            continue;
-        }
-        unsigned long long key = lux::pack_cell(x, y, z);
-        unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
-        uint32_t slot = lux::hash_key(x, y, z, (int32_t)level, F.dir_capacity);
-        bool placed = false;
-        for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
-            unsigned long long prev = atomicCAS(&keys[slot], lux::kEmptyCell, key);
-            if (prev == lux::kEmptyCell || prev == key) {
-                placed = true;
-                break;
-            }
-            slot = (slot + 1u) & (F.dir_capacity - 1u);
-        }
-        if (!placed) atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+        const f3 q{p.x, p.y, p.z};
+        uint32_t low, high;
+        float blend;
+        point_lod(F, q, low, high, blend);
+        seed_cell(V, F, level, q, low);
+        if (high != low) seed_cell(V, F, level, q, high);
     }
 }
 
@@ -255,8 +283,9 @@ __global__ void seed_assign_kernel(ViewDevice V, FrameParams F) {
         }
         V.dir_ids[i] = id;
         int32_t x, y, z;
-        lux::unpack_cell(key, x, y, z);
-        V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)(level << 12));
+        uint32_t lod;
+        lux::unpack_cell(key, x, y, z, lod);
+        V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)((level << 12) | (lod << 18)));
         V.cell_last[(size_t)level * F.cell_capacity + id] = F.shade.frame;
     }
 }
@@ -266,10 +295,18 @@ __global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
         float4 p = pos[r];
+        const f3 q{p.x, p.y, p.z};
+        // The variant this receiver's rays deposit into (one trace per
+        // receiver; in an LOD overlap the high LOD with probability blend).
+        uint32_t low, high;
+        float blend;
+        point_lod(F, q, low, high, blend);
+        uint32_t lod = high != low && lux::lod_selects_high(r, F.shade.frame, blend) ? high : low;
+        if (level == 0u) V.receiver_lod[r] = lod;
         int32_t x, y, z;
-        cell_of(F, level, f3{p.x, p.y, p.z}, x, y, z);
+        cell_of(F, level, q, x, y, z, lod);
         V.receiver_cell[(size_t)level * F.receivers + r] =
-            F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z);
+            F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z, lod);
     }
 }
 
@@ -719,9 +756,12 @@ __device__ __forceinline__ void deposit_split_ray(const ViewDevice &V, const Fra
     float u, v;
     split_direction(F, frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
     float t = V.ts.ray_o[ray].w;
+    // splitIntervalContainsHit at the receiver's LOD (ends scale by 2^lod,
+    // shaders/split.slang:224-236).
+    const float ls = F.lod_enabled ? lux::lod_scale(V.receiver_lod[i]) : 1.0f;
     uint32_t term = F.levels - 1u;
     for (uint32_t l = 0; l + 1u < F.levels; ++l)
-        if (t > F.start[l] && t <= F.end[l]) {
+        if (t > F.start[l] * ls && t <= F.end[l] * ls) {
             term = l;
             break;
         }
@@ -780,9 +820,11 @@ __global__ void __launch_bounds__(128) deposit_dense_kernel(ViewDevice V, FrameP
 __global__ void corners_kernel(ViewDevice V, FrameParams F, uint32_t level) {
     if (*V.error_flags) return;
     uint32_t cells = V.cell_count[level];
-    float sp = F.spacing[level], sp1 = F.spacing[level + 1];
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
         int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+        // A cell's children are the next level's cells of the same LOD.
+        const uint32_t lod = lux::key_lod(key.w);
+        const float sp = level_spacing(F, level, lod), sp1 = level_spacing(F, level + 1, lod);
         float ox = ((float)key.x + 0.5f) * sp, oy = ((float)key.y + 0.5f) * sp, oz = ((float)key.z + 0.5f) * sp;
         float gx = ox / sp1 - 0.5f, gy = oy / sp1 - 0.5f, gz = oz / sp1 - 0.5f;
         float fx = floorf(gx), fy = floorf(gy), fz = floorf(gz);
@@ -792,7 +834,7 @@ __global__ void corners_kernel(ViewDevice V, FrameParams F, uint32_t level) {
 #pragma unroll
         for (uint32_t corner = 0; corner < 8u; ++corner)
             ids[corner] = cell_id(V, F, level + 1, bx + (int32_t)(corner & 1u), by + (int32_t)((corner >> 1) & 1u),
-                                  bz + (int32_t)(corner >> 2));
+                                  bz + (int32_t)(corner >> 2), lod);
     }
 }
 
@@ -856,9 +898,10 @@ __global__ void history_map_kernel(ViewDevice V, FrameParams F, HistoryDevice H,
         uint32_t id = lux::kEmpty;
         int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
         if (lux::cell_in_range(key.x, key.y, key.z) && !record_dirty(F, level, key)) {
-            unsigned long long packed = lux::pack_cell(key.x, key.y, key.z);
+            const uint32_t lod = lux::key_lod(key.w);
+            unsigned long long packed = lux::pack_cell(key.x, key.y, key.z, lod);
             const unsigned long long *keys = H.dir_keys + (size_t)level * F.dir_capacity;
-            uint32_t slot = lux::hash_key(key.x, key.y, key.z, (int32_t)level, F.dir_capacity);
+            uint32_t slot = lux::hash_key(key.x, key.y, key.z, (int32_t)(level | (lod << 18)), F.dir_capacity);
             for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
                 unsigned long long k = keys[slot];
                 if (k == packed) {
@@ -881,7 +924,8 @@ __global__ void history_map_kernel(ViewDevice V, FrameParams F, HistoryDevice H,
 __device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t level, int4 key) {
     if (F.dirty_count == 0u) return false;
     if (level + 1u >= F.levels) return true;
-    float s = F.spacing[level], reach = F.end[level];
+    const float ls = lux::lod_scale(lux::key_lod(key.w));
+    float s = F.spacing[level] * ls, reach = F.end[level] * ls;
     float lo[3] = {(float)key.x * s - reach, (float)key.y * s - reach, (float)key.z * s - reach};
     float hi[3] = {(float)(key.x + 1) * s + reach, (float)(key.y + 1) * s + reach, (float)(key.z + 1) * s + reach};
     for (uint32_t b = 0; b < F.dirty_count && b < (uint32_t)kMaxDirty; ++b) {
@@ -908,7 +952,8 @@ __device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t leve
 __device__ __forceinline__ uint32_t retain_bin(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
                                                uint32_t level, uint32_t prev, int4 &key) {
     key = H.cell_keys[(size_t)level * F.cell_capacity + prev];
-    if (dir_find(V, F, level, key.x, key.y, key.z) != lux::kEmpty) return kRetainBins;  // seeded this frame
+    if (dir_find(V, F, level, key.x, key.y, key.z, lux::key_lod(key.w)) != lux::kEmpty)
+        return kRetainBins;  // seeded this frame
     if (record_dirty(F, level, key)) return kRetainBins;
     uint32_t age = F.shade.frame - H.cell_last[(size_t)level * F.cell_capacity + prev];
     return min(age, kRetainBins - 1u);
@@ -961,15 +1006,17 @@ __global__ void __launch_bounds__(kRetainBins) retain_limit_kernel(ViewDevice V,
 // with a new dense id and its last-receiver frame.
 __device__ __forceinline__ void retain_cell(ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
                                             uint32_t level, uint32_t prev, int4 k) {
-    unsigned long long key = lux::pack_cell(k.x, k.y, k.z);
+    const uint32_t lod = lux::key_lod(k.w);
+    unsigned long long key = lux::pack_cell(k.x, k.y, k.z, lod);
     unsigned long long *keys = V.dir_keys + (size_t)level * F.dir_capacity;
-    uint32_t slot = lux::hash_key(k.x, k.y, k.z, (int32_t)level, F.dir_capacity);
+    uint32_t slot = lux::hash_key(k.x, k.y, k.z, (int32_t)(level | (lod << 18)), F.dir_capacity);
     // The directory is at most half full (dir_capacity >= 2 max_cells).
     for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
         if (atomicCAS(&keys[slot], lux::kEmptyCell, key) == lux::kEmptyCell) {
             uint32_t id = atomicAdd(&V.cell_count[level], 1u);  // below cell_capacity by retain_limit
             V.dir_ids[(size_t)level * F.dir_capacity + slot] = id;
-            V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(k.x, k.y, k.z, (int32_t)(level << 12));
+            V.cell_keys[(size_t)level * F.cell_capacity + id] =
+                make_int4(k.x, k.y, k.z, (int32_t)((level << 12) | (lod << 18)));
             V.cell_last[(size_t)level * F.cell_capacity + id] = H.cell_last[(size_t)level * F.cell_capacity + prev];
             return;
         }
@@ -1156,7 +1203,62 @@ __global__ void __launch_bounds__(64) pack_kernel(ViewDevice V, FrameParams F) {
     }
 }
 
-// worldResolve at LOD 0, shaders/world_resolve.slang:96-196, :281-313.
+// diffuseAtLod (shaders/world_resolve.slang:96-150): trilinear over the 8
+// cascade-0 probes of LOD `lod` around p, each looked up with the
+// octahedral weights (diffuseProbePage, :51-89); rgb and coverage.
+__device__ __forceinline__ void diffuse_at_lod(const ViewDevice &V, const FrameParams &F, float4 p,
+                                               const float weight[4], const uint32_t texel[4], uint32_t lod, float &lx,
+                                               float &ly, float &lz, float &cov) {
+    float s0 = level_spacing(F, 0, lod);
+    float g[3] = {p.x / s0 - 0.5f, p.y / s0 - 0.5f, p.z / s0 - 0.5f};
+    float b[3] = {floorf(g[0]), floorf(g[1]), floorf(g[2])};
+    float fr[3] = {g[0] - b[0], g[1] - b[1], g[2] - b[2]};
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f, observed = 0.0f, potential = 0.0f;
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        float ax = (corner & 1u) == 0u ? 1.0f - fr[0] : fr[0];
+        float ay = ((corner >> 1) & 1u) == 0u ? 1.0f - fr[1] : fr[1];
+        float az = (corner >> 2) == 0u ? 1.0f - fr[2] : fr[2];
+        float w = (ax * ay) * az;
+        if (!(w > 0.0f)) continue;
+        potential += w;
+        uint32_t cell = cell_id(V, F, 0, (int32_t)b[0] + (int32_t)(corner & 1u),
+                                (int32_t)b[1] + (int32_t)((corner >> 1) & 1u), (int32_t)b[2] + (int32_t)(corner >> 2),
+                                lod);
+        if (cell == lux::kEmpty) continue;
+        float px = 0.0f, py = 0.0f, pz = 0.0f, pobs = 0.0f;
+        for (int c = 0; c < 4; ++c) {
+            float bw = weight[c];
+            if (!(bw > 0.0f)) continue;
+            float4 s = __ldg(V.tables + (size_t)cell * 36 + texel[c]);
+            if (!(s.w > 0.0f) || !(isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w))) continue;
+            float ww = bw * lux::saturate(s.w);
+            px = px + s.x * ww;
+            py = py + s.y * ww;
+            pz = pz + s.z * ww;
+            pobs += ww;
+        }
+        float qx = pobs > 0.0f ? px / pobs : 0.0f, qy = pobs > 0.0f ? py / pobs : 0.0f,
+              qz = pobs > 0.0f ? pz / pobs : 0.0f;
+        float support = lux::saturate(pobs);
+        if (!(support > 0.0f)) continue;
+        float weight_s = w * support;
+        sx = sx + qx * weight_s;
+        sy = sy + qy * weight_s;
+        sz = sz + qz * weight_s;
+        observed += weight_s;
+    }
+    lx = ly = lz = cov = 0.0f;
+    if (potential > 0.0f) {
+        cov = lux::saturate(observed / potential);
+        if (observed > 0.0f) {
+            lx = sx / observed;
+            ly = sy / observed;
+            lz = sz / observed;
+        }
+    }
+}
+
+// worldResolve, shaders/world_resolve.slang:96-196, :281-313.
 __global__ void __launch_bounds__(128) resolve_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos,
                                                       const float4 *__restrict__ nrm, uint32_t count,
                                                       float4 *__restrict__ out) {
@@ -1179,61 +1281,23 @@ __global__ void __launch_bounds__(128) resolve_kernel(ViewDevice V, FrameParams 
         int32_t ix = (int32_t)bxf, iy = (int32_t)byf;
         uint32_t texel[4] = {lux::texel_index(ix, iy), lux::texel_index(ix + 1, iy), lux::texel_index(ix, iy + 1),
                              lux::texel_index(ix + 1, iy + 1)};
-        float s0 = F.spacing[0];
-        float g[3] = {p.x / s0 - 0.5f, p.y / s0 - 0.5f, p.z / s0 - 0.5f};
-        float b[3] = {floorf(g[0]), floorf(g[1]), floorf(g[2])};
-        float fr[3] = {g[0] - b[0], g[1] - b[1], g[2] - b[2]};
-        float sx = 0.0f, sy = 0.0f, sz = 0.0f, observed = 0.0f, potential = 0.0f;
-        for (uint32_t corner = 0; corner < 8u; ++corner) {
-            float ax = (corner & 1u) == 0u ? 1.0f - fr[0] : fr[0];
-            float ay = ((corner >> 1) & 1u) == 0u ? 1.0f - fr[1] : fr[1];
-            float az = (corner >> 2) == 0u ? 1.0f - fr[2] : fr[2];
-            float w = (ax * ay) * az;
-            if (!(w > 0.0f)) continue;
-            potential += w;
-            uint32_t cell = cell_id(V, F, 0, (int32_t)b[0] + (int32_t)(corner & 1u),
-                                    (int32_t)b[1] + (int32_t)((corner >> 1) & 1u), (int32_t)b[2] + (int32_t)(corner >> 2));
-            if (cell == lux::kEmpty) continue;
-            // diffuseProbePage, shaders/world_resolve.slang:51-89.
-            float px = 0.0f, py = 0.0f, pz = 0.0f, pobs = 0.0f;
-            for (int c = 0; c < 4; ++c) {
-                float bw = weight[c];
-                if (!(bw > 0.0f)) continue;
-                float4 s = __ldg(V.tables + (size_t)cell * 36 + texel[c]);
-                if (!(s.w > 0.0f) || !(isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w))) continue;
-                float ww = bw * lux::saturate(s.w);
-                px = px + s.x * ww;
-                py = py + s.y * ww;
-                pz = pz + s.z * ww;
-                pobs += ww;
-            }
-            float qx = pobs > 0.0f ? px / pobs : 0.0f, qy = pobs > 0.0f ? py / pobs : 0.0f,
-                  qz = pobs > 0.0f ? pz / pobs : 0.0f;
-            float support = lux::saturate(pobs);
-            if (!(support > 0.0f)) continue;
-            float weight_s = w * support;
-            sx = sx + qx * weight_s;
-            sy = sy + qy * weight_s;
-            sz = sz + qz * weight_s;
-            observed += weight_s;
-        }
-        float lx = 0.0f, ly = 0.0f, lz = 0.0f, low_cov = 0.0f;
-        if (potential > 0.0f) {
-            low_cov = lux::saturate(observed / potential);
-            if (observed > 0.0f) {
-                lx = sx / observed;
-                ly = sy / observed;
-                lz = sz / observed;
-            }
-        }
-        // resolveLodSource with one LOD (blend 0, high coverage 1).
-        float low_weight = low_cov * (1.0f - 0.0f);
-        float high_weight = 1.0f * 0.0f;
+        // resolveSplitDiffuse (shaders/world_resolve.slang:163-196): the LOD
+        // pair of the point, then resolveLodSource (a single LOD takes high
+        // coverage 1 and blend 0).
+        uint32_t low, high;
+        float blend;
+        point_lod(F, f3{p.x, p.y, p.z}, low, high, blend);
+        float lx, ly, lz, low_cov;
+        diffuse_at_lod(V, F, p, weight, texel, low, lx, ly, lz, low_cov);
+        float hx = 0.0f, hy = 0.0f, hz = 0.0f, high_cov = 1.0f;
+        if (high != low) diffuse_at_lod(V, F, p, weight, texel, high, hx, hy, hz, high_cov);
+        float low_weight = low_cov * (1.0f - blend);
+        float high_weight = high_cov * blend;
         float total = low_weight + high_weight;
         coverage = lux::saturate(total);
-        dx = total > 0.0f ? (lx * low_weight + 0.0f * high_weight) / total : 0.0f;
-        dy = total > 0.0f ? (ly * low_weight + 0.0f * high_weight) / total : 0.0f;
-        dz = total > 0.0f ? (lz * low_weight + 0.0f * high_weight) / total : 0.0f;
+        dx = total > 0.0f ? (lx * low_weight + hx * high_weight) / total : 0.0f;
+        dy = total > 0.0f ? (ly * low_weight + hy * high_weight) / total : 0.0f;
+        dz = total > 0.0f ? (lz * low_weight + hz * high_weight) / total : 0.0f;
         supported = coverage > 0.0f && isfinite(dx) && isfinite(dy) && isfinite(dz);
     }
     // rawGiSupportAlpha, shaders/common.slang:323-326.
@@ -1704,6 +1768,7 @@ struct LuxView {
     // second view whose receivers are this view's interval-ray hits, and the
     // snapshot of its cascade-0 probes that hit shading reads one frame late.
     LuxView *secondary = nullptr;
+    LuxCamera camera{};  // distance LODs (enabled = 0: LOD 0)
     struct {
         unsigned long long *keys = nullptr;
         uint32_t *ids = nullptr;
@@ -1739,6 +1804,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.cell_count, L * sizeof(uint32_t)},
         {(void **)&D.level_base, L * sizeof(unsigned long long)},
         {(void **)&D.receiver_cell, L * (size_t)d.max_receivers * sizeof(uint32_t)},
+        {(void **)&D.receiver_lod, (size_t)d.max_receivers * sizeof(uint32_t)},
         {(void **)&D.corner_ids, L * (size_t)d.max_cells * 8 * sizeof(uint32_t)},
         {(void **)&D.corner_frac, L * (size_t)d.max_cells * sizeof(float4)},
         {(void **)&D.accum, (size_t)d.max_entries * sizeof(float4)},
@@ -1813,7 +1879,8 @@ extern "C" lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, 
 extern "C" lux_status lux_view_destroy(LuxView *v) {
     if (!v) return LUX_OK;
     ViewDevice &D = v->dev;
-    void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.corner_ids,
+    void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.receiver_lod,
+                    D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.mass, D.hist_cell, D.cell_last,
                     D.retain_hist, D.retain_limit, D.tables, D.error_flags, D.stats,
                     v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
@@ -1932,6 +1999,22 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
     F.transmittance_blend = s.transmittance_blend;
     F.history = 0;
     F.dirty_count = 0;
+    // Distance LODs: the camera terms of splitLodBlendForParameters
+    // (shaders/common.slang:431-461), evaluated once per frame.
+    const LuxCamera &cam = v->camera;
+    if (cam.enabled && F.layout == LUX_LAYOUT_SPLIT) {
+        const float *m = cam.clip_from_world;
+        const float px = m[12], py = m[13], pz = m[14];
+        const bool perspective = std::isfinite(px) && std::isfinite(py) && std::isfinite(pz) &&
+                                 (px * px + py * py) + pz * pz > 1e-12f;
+        const float focal = 0.5f * (float)cam.viewport_height * std::sqrt((m[4] * m[4] + m[5] * m[5]) + m[6] * m[6]);
+        const float target = (float)(cam.target_pixels > 1u ? cam.target_pixels : 1u);
+        F.lod_enabled = 1;
+        F.lod_perspective = perspective ? 1u : 0u;
+        for (int a = 0; a < 3; ++a) F.lod_camera[a] = cam.position[a];
+        F.lod_base = std::fmax(focal * s.probe_spacing / target, s.probe_spacing);
+        F.lod_ortho_scale = target / std::fmax(focal * s.probe_spacing, 1e-20f);
+    }
     if ((size_t)F.dirs[0] * 2 * sizeof(float4) > 48 * 1024)
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "trace_merge: too many cascade-0 directions");
     return LUX_OK;
@@ -2129,6 +2212,24 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "multi_bounce launch");
 }
 
+extern "C" lux_status lux_view_set_camera(LuxView *v, const LuxCamera *camera) {
+    if (!v) return LUX_ERR_INVALID_ARGUMENT;
+    if (!camera || !camera->enabled) {
+        v->camera = LuxCamera{};
+        return LUX_OK;
+    }
+    for (int i = 0; i < 16; ++i)
+        if (!std::isfinite(camera->clip_from_world[i]))
+            return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_camera: clip_from_world must be finite");
+    for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(camera->position[a]))
+            return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_camera: position must be finite");
+    if (camera->viewport_height == 0)
+        return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_camera: viewport_height must be positive");
+    v->camera = *camera;
+    return LUX_OK;
+}
+
 extern "C" lux_status lux_view_secondary(LuxView *v, LuxView **secondary) {
     if (!v || !secondary) return LUX_ERR_INVALID_ARGUMENT;
     *secondary = v->secondary;
@@ -2145,6 +2246,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
     FrameParams F;
     lux_status ps = make_params(v, settings, rc->count, F);
     if (ps != LUX_OK) return ps;
+    if (v->cache_alloc && v->cache.cutoff_level < F.levels) F.lod_enabled = 0;  // learned-cache frames: LOD 0
     if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > v->desc.max_rays)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: receivers x rays_per_receiver exceeds max_rays");
     const ViewDevice &D = v->dev;
@@ -2891,6 +2993,7 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
             return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: missing receiver buffers");
         lux_status ps = make_params(J.view, &s, rc.count, params[j]);
         if (ps != LUX_OK) return ps;
+        params[j].lod_enabled = 0;  // batched frames use LOD 0
         if ((uint64_t)rc.count * params[j].rays_per_receiver > J.view->desc.max_rays)
             return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: receivers x rays_per_receiver exceeds a view's max_rays");
     }

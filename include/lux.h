@@ -361,6 +361,25 @@ typedef struct LuxTuning {
 lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
 lux_status lux_view_get_tuning(const LuxView *view, LuxTuning *tuning);
 lux_status lux_view_timings(LuxView *view, LuxTimings *out);
+/* Camera of a view for distance LODs (splitLodBlendForParameters,
+ * shaders/common.slang:431-461; LOD keys, spacing and interval ends,
+ * shaders/common.slang:414-422, shaders/split.slang:224-236): with a camera
+ * set, each Split receiver's probes coarsen by 2^lod with its Chebyshev
+ * distance from a perspective camera (or by the projected spacing of an
+ * orthographic one); in an LOD overlap both LODs' cells are seeded and the
+ * receiver's rays deposit into one of them (seed, shaders/split.slang:
+ * 747-786); lux_view_resolve blends the two LODs (resolveSplitDiffuse).
+ * Dense, batched and learned-cache frames use LOD 0. */
+typedef struct LuxCamera {
+    float clip_from_world[16];  /* row-major */
+    float position[3];          /* camera position (world) */
+    uint32_t viewport_height;   /* pixels */
+    uint32_t target_pixels;     /* probe footprint in pixels (split_lod_target_pixels: the resolve scale); 0 = 1 */
+    uint32_t enabled;           /* 0: LOD 0 everywhere */
+} LuxCamera;
+/* NULL or enabled = 0 disables distance LODs. */
+lux_status lux_view_set_camera(LuxView *view, const LuxCamera *camera);
+
 /* The view's multi-bounce secondary cache (RadianceCascades::multi_bounce;
  * src/render.rs:5974-6118, :9662-9752): a view owned by `view`, created by
  * its first multi-bounce frame (NULL before), whose receivers are the

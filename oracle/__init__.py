@@ -65,7 +65,8 @@ def lib():
             "orc_frame_run": (P, [P, P, P, P, U, C.c_int]),
             "orc_frame_run_history": (P, [P, P, P, P, U, C.c_int, P, P, U]),
             "orc_frame_run_retain": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64]),
-            "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P]),
+            "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P, P]),
+            "orc_lod_blend": (None, [P, P, P, P, P, P]),
             "orc_screen_filter": (None, [P, U, U, P, P, P, P, P, P, U, U, U, P, P, P]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
@@ -168,20 +169,23 @@ class OracleFrame:
     def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0,
                  previous: "OracleFrame | None" = None, dirty=None, max_cells: int = 0xFFFFFFFF,
                  max_entries: int = (1 << 64) - 1, feedback: "OracleFrame | None" = None, sparse: bool = False,
-                 skip_emission: bool = False, record_hits: bool = False):
+                 skip_emission: bool = False, record_hits: bool = False, camera=None):
         """previous: the frame whose records serve as history; dirty: boxes
         (n, 6) = (lo xyz, hi xyz) whose nearby records take no history;
         max_cells / max_entries: the view capacities that bound the cells
         retained from `previous`.  Multi-bounce: feedback, the secondary frame
         whose cascade-0 probes add bounce light at hits; sparse, receivers
         with position.w == 0 are absent; skip_emission, hits add no emission of
-        their own; record_hits, keep each receiver's hit surface (hits())."""
+        their own; record_hits, keep each receiver's hit surface (hits()).
+        camera: a LuxCamera (bevy_penumbra_b200.camera_struct) for distance
+        LODs, as SplitView.set_camera."""
         self.settings = settings_c
         pos = np.ascontiguousarray(pos, np.float32)
         nrm = np.ascontiguousarray(nrm, np.float32)
         self._previous = previous  # keeps the history frame alive
         boxes = np.ascontiguousarray(dirty if dirty is not None else np.zeros((0, 6)), np.float32).reshape(-1, 6)
         self._feedback = feedback
+        self._camera = camera
         self.hit_pos = np.zeros((len(pos), 4), np.float32)
         self.hit_nrm = np.zeros((len(pos), 4), np.float32)
         flags = (1 if sparse else 0) | (2 if skip_emission else 0) | (4 if record_hits else 0)
@@ -190,7 +194,8 @@ class OracleFrame:
                                                  previous.handle if previous is not None else None, _p(boxes),
                                                  len(boxes), max_cells, max_entries,
                                                  feedback.handle if feedback is not None else None, flags,
-                                                 _p(self.hit_pos), _p(self.hit_nrm))
+                                                 _p(self.hit_pos), _p(self.hit_nrm),
+                                                 C.addressof(camera) if camera is not None else None)
 
     def level(self, level: int, dirs: int):
         cells = lib().orc_frame_cells(self.handle, level)
@@ -232,6 +237,15 @@ class OracleFrame:
             self.close()
         except Exception:
             pass
+
+
+def lod_blend(settings_c, camera, position):
+    """splitLodBlendForParameters of one point: (low, high, blend)."""
+    low, high, blend = C.c_uint32(), C.c_uint32(), C.c_float()
+    p = f32(*position)
+    lib().orc_lod_blend(C.byref(settings_c), C.byref(camera) if camera is not None else None, _p(p), C.byref(low),
+                        C.byref(high), C.byref(blend))
+    return int(low.value), int(high.value), float(blend.value)
 
 
 SCREEN_WORDS = 18

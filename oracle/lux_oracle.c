@@ -1381,13 +1381,93 @@ int orc_outgoing_radiance(const OrcScene *S, const LuxSettings *st, const float 
  * Cascade frame: deposit, reduce, merge, pack, resolve (shaders/split.slang,
  * shaders/world_resolve.slang)
  * ==================================================================== */
-typedef struct { int32_t k[4]; } Key;
+/* A cell key: x, y, z and the probe LOD (cacheKey, shaders/common.slang:
+ * 418-422); `aux` carries per-key scratch (a last-receiver frame, an index). */
+typedef struct { int32_t k[4]; uint32_t aux; } Key;
 
 static int key_cmp(const void *a, const void *b) {
     const int32_t *x = ((const Key *)a)->k, *y = ((const Key *)b)->k;
-    for (int i = 0; i < 3; ++i)
+    for (int i = 0; i < 4; ++i)
         if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
     return 0;
+}
+
+/* Distance LODs (splitLodBlendForParameters, shaders/common.slang:431-461)
+ * with the camera terms evaluated once per frame, as lux_view_trace_merge
+ * does. */
+#define MAX_LOD 24u
+typedef struct {
+    int enabled, perspective;
+    float camera[3];
+    float base, ortho_scale;
+} LodParams;
+
+static float lod_scale(uint32_t lod) {
+    uint32_t bits = (127u + lod) << 23;
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
+
+static void lod_params(const LuxSettings *st, const LuxCamera *cam, LodParams *L) {
+    memset(L, 0, sizeof *L);
+    if (!cam || !cam->enabled || st->layout != LUX_LAYOUT_SPLIT) return;
+    const float *m = cam->clip_from_world;
+    float px = m[12], py = m[13], pz = m[14];
+    int perspective = isfinite(px) && isfinite(py) && isfinite(pz) && (px * px + py * py) + pz * pz > 1e-12f;
+    float focal = 0.5f * (float)cam->viewport_height * sqrtf((m[4] * m[4] + m[5] * m[5]) + m[6] * m[6]);
+    float target = (float)(cam->target_pixels > 1u ? cam->target_pixels : 1u);
+    L->enabled = 1;
+    L->perspective = perspective;
+    for (int a = 0; a < 3; ++a) L->camera[a] = cam->position[a];
+    L->base = fmaxf(focal * st->probe_spacing / target, st->probe_spacing);
+    L->ortho_scale = target / fmaxf(focal * st->probe_spacing, 1e-20f);
+}
+
+/* floor(log2(x)) for x >= 1 is the exponent (exact); 2^(low+1) is exact. */
+static void point_lod(const LodParams *L, const float p[3], uint32_t *low, uint32_t *high, float *blend) {
+    *low = *high = 0u;
+    *blend = 0.0f;
+    if (!L || !L->enabled) return;
+    float scale;
+    if (L->perspective) {
+        float ox = fabsf(p[0] - L->camera[0]), oy = fabsf(p[1] - L->camera[1]), oz = fabsf(p[2] - L->camera[2]);
+        scale = fmaxf(ox, fmaxf(oy, oz)) / L->base;
+    } else {
+        scale = L->ortho_scale;
+    }
+    float s1 = fmaxf(scale, 1.0f);
+    uint32_t bits;
+    memcpy(&bits, &s1, 4);
+    uint32_t e = s1 < INFINITY ? (bits >> 23) - 127u : MAX_LOD;
+    *low = e < MAX_LOD ? e : MAX_LOD;
+    *high = *low;
+    if (*low < MAX_LOD) {
+        float next = lod_scale(*low + 1u);
+        float overlap = 0.9f * next;
+        if (scale >= overlap && scale < next) {
+            *high = *low + 1u;
+            *blend = saturatef((scale - overlap) / (next - overlap));
+        }
+    }
+}
+
+/* seed's variant choice in an LOD overlap (shaders/split.slang:747-752). */
+static uint32_t receiver_lod(const LodParams *L, const float p[3], uint32_t sample, uint32_t frame) {
+    uint32_t low, high;
+    float blend;
+    point_lod(L, p, &low, &high, &blend);
+    if (high == low) return low;
+    uint32_t bits = orc_transport_hash(sample ^ (frame * 0x9e3779b9u));
+    float phase = (float)(bits >> 8) * (1.0f / 16777216.0f);
+    return phase < blend ? high : low;
+}
+
+void orc_lod_blend(const LuxSettings *st, const LuxCamera *camera, const float position[3], uint32_t *low,
+                   uint32_t *high, float *blend) {
+    LodParams L;
+    lod_params(st, camera, &L);
+    point_lod(&L, position, low, high, blend);
 }
 
 typedef struct {
@@ -1403,6 +1483,7 @@ typedef struct {
 
 struct OrcFrame {
     LuxSettings st;
+    LodParams lod;
     uint32_t levels;
     Level level[LUX_MAX_LEVELS];
     float *tables;  /* c0 cells * 36 float4 */
@@ -1412,13 +1493,13 @@ struct OrcFrame {
     uint32_t dirty_count;
 };
 
-static int64_t find_cell(const Level *L, const int32_t key[3]) {
+static int64_t find_cell(const Level *L, const int32_t key[4]) {
     int64_t lo = 0, hi = (int64_t)L->cells - 1;
     while (lo <= hi) {
         int64_t mid = (lo + hi) / 2;
         const int32_t *m = L->keys[mid].k;
         int c = 0;
-        for (int i = 0; i < 3 && c == 0; ++i)
+        for (int i = 0; i < 4 && c == 0; ++i)
             if (m[i] != key[i]) c = m[i] < key[i] ? -1 : 1;
         if (c == 0) return mid;
         if (c < 0) lo = mid + 1;
@@ -1427,10 +1508,11 @@ static int64_t find_cell(const Level *L, const int32_t key[3]) {
     return -1;
 }
 
-/* cacheKey cell, shaders/common.slang:417-422 (LOD 0). */
-static void cell_key(const LuxSettings *st, uint32_t level, const float p[3], int32_t out[3]) {
-    float s = orc_spacing(st, level);
+/* cacheKey cell, shaders/common.slang:417-422: spacing x 2^lod. */
+static void cell_key(const LuxSettings *st, uint32_t level, const float p[3], uint32_t lod, int32_t out[4]) {
+    float s = orc_spacing(st, level) * lod_scale(lod);
     for (int i = 0; i < 3; ++i) out[i] = (int32_t)floorf(p[i] / s);
+    out[3] = (int32_t)lod;
 }
 
 typedef struct {
@@ -1440,6 +1522,7 @@ typedef struct {
     uint32_t n;
     /* multi-bounce */
     const Bounce *bounce;
+    const LodParams *lod;     /* distance LODs of the frame (NULL: LOD 0) */
     int sparse;               /* receivers with position.w == 0 are absent */
     float *hit_pos, *hit_nrm; /* float4 per receiver: the surface of ray frame % R, or NULL */
     /* split: per ray outputs */
@@ -1504,9 +1587,11 @@ static void *split_job(void *arg) {
             j->term_level[ray] = -1;
             continue;
         }
+        /* splitIntervalContainsHit at the receiver's LOD (ends x 2^lod). */
+        float ls = j->lod && j->lod->enabled ? lod_scale(receiver_lod(j->lod, p, i, st->frame_index)) : 1.0f;
         int32_t term = (int32_t)st->levels - 1;
         for (uint32_t l = 0; l + 1 < st->levels; ++l) {
-            if (hit.distance > interval_start(st, l) && hit.distance <= orc_interval_end(st, l)) {
+            if (hit.distance > interval_start(st, l) * ls && hit.distance <= orc_interval_end(st, l) * ls) {
                 term = (int32_t)l;
                 break;
             }
@@ -1712,10 +1797,11 @@ void orc_merge_entry(const float interval[4], uint32_t samples, const float frac
 
 /* A record's history is invalid when its cell grown by the level's
  * interval end (unbounded at the last level) meets an invalidation box. */
-static int record_dirty(const OrcFrame *F, uint32_t level, const int32_t key[3]) {
+static int record_dirty(const OrcFrame *F, uint32_t level, const int32_t key[4]) {
     if (F->dirty_count == 0) return 0;
     if (level + 1 >= F->levels) return 1;
-    float s = orc_spacing(&F->st, level), reach = orc_interval_end(&F->st, level);
+    float ls = lod_scale((uint32_t)key[3]);
+    float s = orc_spacing(&F->st, level) * ls, reach = orc_interval_end(&F->st, level) * ls;
     for (uint32_t b = 0; b < F->dirty_count; ++b) {
         const float *box = F->dirty + 6 * (size_t)b;
         int meet = 1;
@@ -1733,11 +1819,13 @@ static void merge_level(OrcFrame *F, uint32_t l) {
     Level *L = &F->level[l];
     int has_children = l + 1 < F->levels;
     Level *P = has_children ? &F->level[l + 1] : NULL;
-    float sp = orc_spacing(st, l);
-    float sp1 = has_children ? orc_spacing(st, l + 1) : 1.0f;
     for (uint32_t cell = 0; cell < L->cells; ++cell) {
         int64_t corner_cell[8];
         float fraction[3];
+        /* A cell's children are the next level's cells of the same LOD. */
+        const uint32_t lod = (uint32_t)L->keys[cell].k[3];
+        const float sp = orc_spacing(st, l) * lod_scale(lod);
+        const float sp1 = has_children ? orc_spacing(st, l + 1) * lod_scale(lod) : 1.0f;
         if (has_children) {
             int32_t base[3];
             for (int c = 0; c < 3; ++c) {
@@ -1748,8 +1836,8 @@ static void merge_level(OrcFrame *F, uint32_t l) {
                 fraction[c] = grid - fl;
             }
             for (uint32_t corner = 0; corner < 8u; ++corner) {
-                int32_t k[3] = {base[0] + (int32_t)(corner & 1u), base[1] + (int32_t)((corner >> 1) & 1u),
-                                base[2] + (int32_t)(corner >> 2)};
+                int32_t k[4] = {base[0] + (int32_t)(corner & 1u), base[1] + (int32_t)((corner >> 1) & 1u),
+                                base[2] + (int32_t)(corner >> 2), (int32_t)lod};
                 corner_cell[corner] = find_cell(P, k);
             }
         }
@@ -1922,7 +2010,7 @@ OrcFrame *orc_frame_run_history(const OrcScene *S, const LuxSettings *st_in, con
  * seeded stay, unless an invalidation box voids their history.  Capacity
  * keeps the youngest (commitCache, shaders/split.slang:1919-1961) as whole
  * age classes, levels in order, while cells fit max_cells and records fit
- * max_entries.  Keys carry each cell's last receiver frame in k[3] here. */
+ * max_entries.  Keys carry each cell's last receiver frame in aux here. */
 static void retain_cells(OrcFrame *F, Key **keys, uint32_t *cells, uint32_t max_cells, uint64_t max_entries) {
     const OrcFrame *P = F->previous;
     uint64_t used = 0;
@@ -1956,7 +2044,7 @@ static void retain_cells(OrcFrame *F, Key **keys, uint32_t *cells, uint32_t max_
             for (uint32_t c = 0; c < H->cells; ++c)
                 if (bin[c] < limit) {
                     all[m] = H->keys[c];
-                    all[m].k[3] = (int32_t)H->last[c];
+                    all[m].aux = H->last[c];
                     ++m;
                 }
             qsort(all, m, sizeof(Key), key_cmp);
@@ -1972,7 +2060,7 @@ OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, cons
                                uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
                                uint32_t dirty_count, uint32_t max_cells, uint64_t max_entries) {
     return orc_frame_run_bounce(S, st_in, pos, nrm, n, threads, previous, dirty, dirty_count, max_cells, max_entries,
-                                NULL, 0u, NULL, NULL);
+                                NULL, 0u, NULL, NULL, NULL);
 }
 
 /* secondaryFeedback at LOD 0 of the secondary frame: its cascade-0 probe of
@@ -1982,8 +2070,8 @@ static void feedback_irradiance(const OrcFrame *fb, const float position[3], con
     out[0] = out[1] = out[2] = 0.0f;
     if (!finite3(position)) return;
     float s = orc_spacing(&fb->st, 0);
-    int32_t key[3] = {(int32_t)floorf(position[0] / s), (int32_t)floorf(position[1] / s),
-                      (int32_t)floorf(position[2] / s)};
+    int32_t key[4] = {(int32_t)floorf(position[0] / s), (int32_t)floorf(position[1] / s),
+                      (int32_t)floorf(position[2] / s), 0};
     int64_t cell = find_cell(&fb->level[0], key);
     if (cell < 0) return;
     Lookup lk = irradiance_lookup(normal);
@@ -1996,11 +2084,13 @@ static void feedback_irradiance(const OrcFrame *fb, const float position[3], con
 OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, const float *pos, const float *nrm,
                                uint32_t n, int threads, const OrcFrame *previous, const float *dirty,
                                uint32_t dirty_count, uint32_t max_cells, uint64_t max_entries,
-                               const OrcFrame *feedback, uint32_t flags, float *hit_pos, float *hit_nrm) {
+                               const OrcFrame *feedback, uint32_t flags, float *hit_pos, float *hit_nrm,
+                               const LuxCamera *camera) {
     const int sparse = (flags & ORC_FRAME_SPARSE) != 0u;
     Bounce bounce = {feedback, (flags & ORC_FRAME_SKIP_EMISSION) != 0u};
     OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
     F->st = *st_in;
+    lod_params(st_in, camera, &F->lod);
     /* History applies with history_frames > 0, a blend above zero and a
      * previous frame of the same cascade shape. */
     int same_shape = previous && previous->levels == st_in->levels;
@@ -2021,12 +2111,20 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         L->columns = level_columns(st, l);
         L->rows = level_rows(st, l);
         L->dirs = L->columns * L->rows;
-        Key *tmp = (Key *)malloc(sizeof(Key) * (n ? n : 1));
+        Key *tmp = (Key *)malloc(sizeof(Key) * (2 * (size_t)n + 1));
         uint32_t present = 0;
         for (uint32_t i = 0; i < n; ++i) {
             if (sparse && pos[4 * (size_t)i + 3] == 0.0f) continue;
-            cell_key(st, l, pos + 4 * (size_t)i, tmp[present].k);
-            tmp[present++].k[3] = (int32_t)st->frame_index;
+            /* Both LOD variants' cells in an overlap (seed, shaders/split.slang:758-786). */
+            uint32_t low, high;
+            float blend;
+            point_lod(&F->lod, pos + 4 * (size_t)i, &low, &high, &blend);
+            cell_key(st, l, pos + 4 * (size_t)i, low, tmp[present].k);
+            tmp[present++].aux = st->frame_index;
+            if (high != low) {
+                cell_key(st, l, pos + 4 * (size_t)i, high, tmp[present].k);
+                tmp[present++].aux = st->frame_index;
+            }
         }
         qsort(tmp, present, sizeof(Key), key_cmp);
         uint32_t cells = 0;
@@ -2042,10 +2140,7 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         L->cells = cells;
         L->keys = level_keys[l];
         L->last = (uint32_t *)malloc(sizeof(uint32_t) * (cells ? cells : 1));
-        for (uint32_t c = 0; c < cells; ++c) {
-            L->last[c] = (uint32_t)L->keys[c].k[3];
-            L->keys[c].k[3] = 0;
-        }
+        for (uint32_t c = 0; c < cells; ++c) L->last[c] = L->keys[c].aux;
         uint64_t entries = (uint64_t)cells * L->dirs;
         L->jsum = (float *)calloc(4 * entries + 4, sizeof(float));
         L->count = (uint32_t *)calloc(entries + 1, sizeof(uint32_t));
@@ -2068,6 +2163,7 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         proto.nrm = nrm;
         proto.n = n;
         proto.bounce = &bounce;
+        proto.lod = &F->lod;
         proto.sparse = sparse;
         proto.hit_pos = (flags & ORC_FRAME_RECORD_HITS) ? hit_pos : NULL;
         proto.hit_nrm = (flags & ORC_FRAME_RECORD_HITS) ? hit_nrm : NULL;
@@ -2089,10 +2185,11 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
                 continue;
             }
             uint32_t i = (uint32_t)(ray / st->rays_per_receiver);
+            uint32_t lod = receiver_lod(&F->lod, pos + 4 * (size_t)i, i, st->frame_index);
             for (uint32_t l = 0; l <= (uint32_t)term; ++l) {
                 Level *L = &F->level[l];
-                int32_t key[3];
-                cell_key(st, l, pos + 4 * (size_t)i, key);
+                int32_t key[4];
+                cell_key(st, l, pos + 4 * (size_t)i, lod, key);
                 int64_t cell = find_cell(L, key);
                 uint32_t bin = orc_direction_index_uv(proto.uv[2 * ray], proto.uv[2 * ray + 1], L->columns, L->rows);
                 uint64_t e = (uint64_t)cell * L->dirs + bin;
@@ -2162,7 +2259,11 @@ void orc_frame_read_level(const OrcFrame *F, uint32_t level, int32_t *keys, floa
     if (level >= F->levels) return;
     const Level *L = &F->level[level];
     uint64_t entries = (uint64_t)L->cells * L->dirs;
-    if (keys) memcpy(keys, L->keys, sizeof(Key) * L->cells);
+    if (keys)
+        for (uint32_t c = 0; c < L->cells; ++c) {
+            memcpy(keys + 4 * (size_t)c, L->keys[c].k, 12);
+            keys[4 * (size_t)c + 3] = (int32_t)((level << 12) | ((uint32_t)L->keys[c].k[3] << 18));
+        }
     if (merged) memcpy(merged, L->merged, sizeof(float) * 4 * entries);
     if (raw) memcpy(raw, L->raw, sizeof(float) * 4 * entries);
     if (samples) memcpy(samples, L->count, sizeof(uint32_t) * entries);
@@ -2174,11 +2275,52 @@ void orc_frame_read_probes(const OrcFrame *F, float *tables) {
 
 void orc_frame_stats(const OrcFrame *F, LuxStats *stats) { *stats = F->stats; }
 
-/* worldResolve -> resolveSplitDiffuse -> diffuseAtLod at LOD 0
- * (shaders/world_resolve.slang:96-196, :281-313) over cascade-0 probe
- * tables: keys int4[cells] sorted ascending, tables float4[cells*36]. */
-static void resolve_tables(const Key *keys, uint32_t cells, const float *tables, float s0, const float *position,
-                           const float *normal_in, uint32_t count, float *out) {
+/* diffuseAtLod (shaders/world_resolve.slang:96-150) over cascade-0 probe
+ * tables (keys sorted ascending). */
+static void diffuse_at_lod(const Level *L0, const float *tables, float s0, const float *p, const Lookup *lk,
+                           uint32_t lod, float out[3], float *cov) {
+    float s = s0 * lod_scale(lod);
+    float grid[3], base[3], fr[3];
+    for (int c = 0; c < 3; ++c) {
+        grid[c] = p[c] / s - 0.5f;
+        base[c] = floorf(grid[c]);
+        fr[c] = grid[c] - base[c];
+    }
+    float sum[3] = {0, 0, 0}, observed = 0.0f, potential = 0.0f;
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        uint32_t bx = corner & 1u, by = (corner >> 1) & 1u, bz = corner >> 2;
+        float ax = bx == 0u ? 1.0f - fr[0] : fr[0];
+        float ay = by == 0u ? 1.0f - fr[1] : fr[1];
+        float az = bz == 0u ? 1.0f - fr[2] : fr[2];
+        float w = (ax * ay) * az;
+        if (!(w > 0.0f)) continue;
+        potential += w;
+        int32_t key[4] = {(int32_t)base[0] + (int32_t)bx, (int32_t)base[1] + (int32_t)by,
+                          (int32_t)base[2] + (int32_t)bz, (int32_t)lod};
+        int64_t cell = find_cell(L0, key);
+        if (cell < 0) continue;
+        float probe[4];
+        probe_page(&tables[(size_t)cell * 144], lk, probe);
+        float support = probe[3];
+        if (!(support > 0.0f)) continue;
+        float weight = w * support;
+        for (int c = 0; c < 3; ++c) sum[c] = sum[c] + probe[c] * weight;
+        observed += weight;
+    }
+    out[0] = out[1] = out[2] = 0.0f;
+    *cov = 0.0f;
+    if (potential > 0.0f) {
+        *cov = saturatef(observed / potential);
+        if (observed > 0.0f)
+            for (int c = 0; c < 3; ++c) out[c] = sum[c] / observed;
+    }
+}
+
+/* worldResolve -> resolveSplitDiffuse (shaders/world_resolve.slang:96-196,
+ * :281-313) over cascade-0 probe tables: keys sorted ascending, tables
+ * float4[cells*36]; the LOD pair and blend of each point from `lod`. */
+static void resolve_tables(const Key *keys, uint32_t cells, const float *tables, float s0, const LodParams *lod,
+                           const float *position, const float *normal_in, uint32_t count, float *out) {
     Level L0;
     memset(&L0, 0, sizeof L0);
     L0.cells = cells;
@@ -2193,46 +2335,19 @@ static void resolve_tables(const Key *keys, uint32_t cells, const float *tables,
             float l = length3(n3);
             float normal[3] = {n3[0] / l, n3[1] / l, n3[2] / l};
             Lookup lk = irradiance_lookup(normal);
-            float grid[3], base[3], fr[3];
-            for (int c = 0; c < 3; ++c) {
-                grid[c] = p[c] / s0 - 0.5f;
-                base[c] = floorf(grid[c]);
-                fr[c] = grid[c] - base[c];
-            }
-            float sum[3] = {0, 0, 0}, observed = 0.0f, potential = 0.0f;
-            for (uint32_t corner = 0; corner < 8u; ++corner) {
-                uint32_t bx = corner & 1u, by = (corner >> 1) & 1u, bz = corner >> 2;
-                float ax = bx == 0u ? 1.0f - fr[0] : fr[0];
-                float ay = by == 0u ? 1.0f - fr[1] : fr[1];
-                float az = bz == 0u ? 1.0f - fr[2] : fr[2];
-                float w = (ax * ay) * az;
-                if (!(w > 0.0f)) continue;
-                potential += w;
-                int32_t key[3] = {(int32_t)base[0] + (int32_t)bx, (int32_t)base[1] + (int32_t)by,
-                                  (int32_t)base[2] + (int32_t)bz};
-                int64_t cell = find_cell(&L0, key);
-                if (cell < 0) continue;
-                float probe[4];
-                probe_page(&tables[(size_t)cell * 144], &lk, probe);
-                float support = probe[3];
-                if (!(support > 0.0f)) continue;
-                float weight = w * support;
-                for (int c = 0; c < 3; ++c) sum[c] = sum[c] + probe[c] * weight;
-                observed += weight;
-            }
-            float low[3] = {0, 0, 0}, low_cov = 0.0f;
-            if (potential > 0.0f) {
-                low_cov = saturatef(observed / potential);
-                if (observed > 0.0f)
-                    for (int c = 0; c < 3; ++c) low[c] = sum[c] / observed;
-            }
-            /* resolveLodSource with one LOD (blend 0, high coverage 1). */
-            float low_weight = low_cov * (1.0f - 0.0f);
-            float high_weight = 1.0f * 0.0f;
+            uint32_t low, high;
+            float blend;
+            point_lod(lod, p, &low, &high, &blend);
+            float lo[3], low_cov, hi[3] = {0, 0, 0}, high_cov = 1.0f;
+            diffuse_at_lod(&L0, tables, s0, p, &lk, low, lo, &low_cov);
+            if (high != low) diffuse_at_lod(&L0, tables, s0, p, &lk, high, hi, &high_cov);
+            /* resolveLodSource (a single LOD takes high coverage 1, blend 0). */
+            float low_weight = low_cov * (1.0f - blend);
+            float high_weight = high_cov * blend;
             float total = low_weight + high_weight;
             coverage = saturatef(total);
             for (int c = 0; c < 3; ++c)
-                diffuse[c] = total > 0.0f ? (low[c] * low_weight + 0.0f * high_weight) / total : 0.0f;
+                diffuse[c] = total > 0.0f ? (lo[c] * low_weight + hi[c] * high_weight) / total : 0.0f;
             supported = coverage > 0.0f && finite3(diffuse);
         }
         o[0] = diffuse[0];
@@ -2244,24 +2359,26 @@ static void resolve_tables(const Key *keys, uint32_t cells, const float *tables,
 }
 
 void orc_frame_resolve(const OrcFrame *F, const float *position, const float *normal_in, uint32_t count, float *out) {
-    resolve_tables(F->level[0].keys, F->level[0].cells, F->tables, orc_spacing(&F->st, 0), position, normal_in, count,
-                   out);
+    resolve_tables(F->level[0].keys, F->level[0].cells, F->tables, orc_spacing(&F->st, 0), &F->lod, position,
+                   normal_in, count, out);
 }
 
 void orc_resolve_tables(const int32_t *keys, uint32_t cells, const float *tables, float spacing, const float *position,
                         const float *normal, uint32_t count, float *out) {
     Key *sorted = (Key *)malloc(sizeof(Key) * (cells ? cells : 1));
     uint32_t *order = (uint32_t *)malloc(sizeof(uint32_t) * (cells ? cells : 1));
-    memcpy(sorted, keys, sizeof(Key) * cells);
-    for (uint32_t i = 0; i < cells; ++i) sorted[i].k[3] = (int32_t)i;
+    for (uint32_t i = 0; i < cells; ++i) {
+        memcpy(sorted[i].k, keys + 4 * (size_t)i, 12);
+        sorted[i].k[3] = (int32_t)(((uint32_t)keys[4 * (size_t)i + 3] >> 18) & 31u);
+        sorted[i].aux = i;
+    }
     qsort(sorted, cells, sizeof(Key), key_cmp);
     float *tab = (float *)malloc(sizeof(float) * 144 * (cells ? cells : 1));
     for (uint32_t i = 0; i < cells; ++i) {
-        order[i] = (uint32_t)sorted[i].k[3];
+        order[i] = sorted[i].aux;
         memcpy(&tab[(size_t)i * 144], &tables[(size_t)order[i] * 144], sizeof(float) * 144);
-        sorted[i].k[3] = 0;
     }
-    resolve_tables(sorted, cells, tab, spacing, position, normal, count, out);
+    resolve_tables(sorted, cells, tab, spacing, NULL, position, normal, count, out);
     free(sorted);
     free(order);
     free(tab);

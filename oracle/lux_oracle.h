@@ -120,7 +120,10 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *scene, const LuxSettings *setting
                                const float *receiver_normal, uint32_t receiver_count, int threads,
                                const OrcFrame *previous, const float *dirty, uint32_t dirty_count,
                                uint32_t max_cells, uint64_t max_entries, const OrcFrame *feedback, uint32_t flags,
-                               float *hit_pos, float *hit_nrm);
+                               float *hit_pos, float *hit_nrm, const LuxCamera *camera);
+/* splitLodBlendForParameters of one point (camera NULL or disabled: 0, 0, 0). */
+void orc_lod_blend(const LuxSettings *settings, const LuxCamera *camera, const float position[3], uint32_t *low,
+                   uint32_t *high, float *blend);
 /* Screen reconstruction (temporal + denoise, shaders/cascades.slang:310-690):
  * inputs per pixel of a width x height image (row-major): irradiance float4
  * (resolve output), position float4 (xyz, view depth), normal float4, identity

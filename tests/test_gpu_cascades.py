@@ -14,8 +14,13 @@ RTOL = 1e-4   # merged cascade radiance: relative tolerance
 ATOL = 1e-6
 
 
+def key_of(k):
+    """(x, y, z, lod) of a cell key (w = level << 12 | lod << 18)."""
+    return (int(k[0]), int(k[1]), int(k[2]), (int(k[3]) >> 18) & 31)
+
+
 def by_key(keys):
-    return {tuple(k[:3]): i for i, k in enumerate(keys)}
+    return {key_of(k): i for i, k in enumerate(keys)}
 
 
 def run_frame(name, settings, pos, nrm, max_cells=1 << 16, max_entries=1 << 24, tuning=None):
@@ -44,7 +49,7 @@ def compare_levels(settings, gpu_levels, ofr, exact):
         okeys, omerged, oraw, osamples = ofr.level(level, settings.direction_count(level))
         assert len(keys) == len(okeys), f"level {level}: cell count"
         index = by_key(okeys)
-        order = np.array([index[tuple(k[:3])] for k in keys])
+        order = np.array([index[key_of(k)] for k in keys], dtype=np.int64)
         np.testing.assert_array_equal(samples, osamples[order], err_msg=f"level {level} samples")
         if exact:
             np.testing.assert_array_equal(raw.view(np.uint32), oraw[order].view(np.uint32))
@@ -69,7 +74,7 @@ def test_dense_cornell_frame_matches_oracle():
     index = by_key(levels[0][0])
     otables = ofr.probes()
     okeys = ofr.level(0, 16)[0]
-    order = np.array([by_key(pkeys)[tuple(k[:3])] for k in okeys])
+    order = np.array([by_key(pkeys)[key_of(k)] for k in okeys])
     np.testing.assert_allclose(tables[order], otables, rtol=RTOL, atol=ATOL)
     # Some probes see lit surfaces and some see the emitter.
     assert np.mean(levels[0][1][..., 3] > 0) > 0.2
@@ -127,7 +132,7 @@ def test_split_cornell_frame_matches_oracle(rays, sort, depth):
     assert st.deposits == ost.deposits and st.shadow_rays == ost.shadow_rays
     compare_levels(settings, levels, ofr, exact=False)
     okeys = ofr.level(0, 32)[0]
-    order = np.array([by_key(pkeys)[tuple(k[:3])] for k in okeys])
+    order = np.array([by_key(pkeys)[key_of(k)] for k in okeys])
     np.testing.assert_allclose(tables[order], ofr.probes(), rtol=RTOL, atol=ATOL)
 
 
@@ -269,3 +274,52 @@ def test_multi_bounce_matches_oracle():
             dirs = s.direction_count(0)
             assert np.any(p.level(0, dirs)[2][..., :3] > unfed.level(0, dirs)[2][..., :3] + 1e-4)
         prim, sec = p, q
+
+
+def test_split_lod_frames_and_resolve_match_oracle():
+    """Distance LODs: a perspective camera close to the Cornell floor puts
+    the receivers into LODs 0-2 (both variants seeded in overlaps, rays
+    deposited into the selected one with 2^lod interval ends); two frames
+    with history and retain, then the resolve's LOD blend, follow the oracle."""
+    import math
+    from tests.test_lod import perspective_infinite_reverse, view_from_world
+
+    def st(frame):
+        return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   frame_index=frame).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    eye = np.array([0.9, 0.4, 0.9])
+    clip = (perspective_infinite_reverse(math.radians(60.0), 16 / 9, 0.1)
+            @ view_from_world(eye, (0.0, 0.0, 0.0))).astype(np.float32)
+    cam = bp.camera_struct(clip, eye, 32, 16)
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=1 << 16, max_entries=1 << 24, max_rays=len(pos) * 4)
+    view.set_camera(clip, eye, 32, 16)
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    caps = dict(max_cells=1 << 16, max_entries=1 << 24)
+    prev = None
+    for frame in range(2):
+        s = st(frame)
+        view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+        assert view.stats().error_flags == 0
+        cur = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prev, camera=cam, **caps)
+        compare_levels(s, [view.read_level(l) for l in range(4)], cur, exact=False)
+        prev = cur
+    lods = {key_of(k)[3] for k in view.read_level(0)[0]}
+    assert len(lods) >= 2, lods
+    rng = np.random.default_rng(5)
+    n = 4096
+    ppos = np.zeros((n, 4), np.float32)
+    ppos[:, 0] = rng.uniform(-0.95, 0.95, n)
+    ppos[:, 2] = rng.uniform(-0.95, 0.95, n)
+    pnrm = np.zeros((n, 4), np.float32)
+    pnrm[:, 1] = 1.0
+    d_p, d_n, d_o = to_device(ppos), to_device(pnrm), empty_device(n * 16)
+    view.resolve(st(1), d_p.data_ptr(), d_n.data_ptr(), n, d_o.data_ptr())
+    ctx.synchronize()
+    out = from_device(d_o, np.float32, (n, 4))
+    np.testing.assert_allclose(out, prev.resolve(ppos, pnrm), rtol=RTOL, atol=ATOL)
+    blends = [oracle.lod_blend(st(1).to_c(), cam, p[:3])[2] for p in ppos[:512]]
+    assert any(0.0 < b < 1.0 for b in blends)  # some points blend two LODs
