@@ -140,6 +140,10 @@ def build_workload(device: int = 0, host_only: bool = False):
     view = None if host_only else bp.SplitView(ctx, max_receivers=len(rpos), max_cells=cells_max,
                                                max_entries=entries,
                                                max_rays=len(rpos) * settings.rays_per_receiver)
+    if view is not None:
+        # Distance LODs from the bench camera (resolve scale 1 = 1 target
+        # pixel); at 1280x720 and 60 degrees the LOD-0 band reaches 156 m.
+        view.set_camera(scenes.clip_from_world(EYE, TARGET, 60.0, WIDTH, HEIGHT), EYE, HEIGHT, 1)
     return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, pscreen=pscreen,
                 rpos=rpos,
                 rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, cells_max=cells_max, setup_s=time.time() - t0)
