@@ -238,6 +238,17 @@ class PackedScene:
         self.max_depth = max_depth
         self.tlas_nodes = tlas_nodes
         self.blas_nodes = blas_nodes
+        self.conventional = 0  # leading conventional (point, spot, directional) light records
+
+    def with_conventional_lights(self, records) -> "PackedScene":
+        """A copy whose light list starts with these conventional light
+        records (conventional_light / directional_light), before the emissive
+        ones, as the reference orders them (src/scene.rs:2311-2372)."""
+        recs = np.ascontiguousarray(np.asarray(records, dtype=np.uint32).reshape(-1, 24))
+        out = PackedScene(self.scene_words, self.geometry_words, np.concatenate([recs, self.lights[self.conventional:]]),
+                          self.instance_order, self.blas_cost, self.max_depth, self.tlas_nodes, self.blas_nodes)
+        out.conventional = len(recs)
+        return out
 
     @staticmethod
     def pack(positions, indices, mesh_first, mesh_count, instance_mesh, instance_transform, instance_flags,
@@ -292,6 +303,27 @@ class PackedScene:
                                 np.stack(desc.materials))
 
 
+def conventional_light(position, range_: float, color, direction=(0.0, 0.0, -1.0), spot_scale: float = 0.0,
+                       spot_offset: float = 0.0) -> np.ndarray:
+    """A point (spot_scale = 0) or spot light record (the Light layout of
+    conventionalLightResponseTracked, shaders/cascades.slang:136-176):
+    position.w = range, color.w = spot offset, direction.w = spot scale."""
+    f = np.zeros(24, np.float32)
+    f[0:3], f[3] = position, range_
+    f[4:7], f[7] = color, spot_offset
+    f[8:11], f[11] = direction, spot_scale
+    return f.view(np.uint32)
+
+
+def directional_light(direction_to_light, color) -> np.ndarray:
+    """A directional light record: the direction to the source in
+    position.xyz, position.w = 0."""
+    f = np.zeros(24, np.float32)
+    f[0:3] = direction_to_light
+    f[4:7] = color
+    return f.view(np.uint32)
+
+
 class GpuScene:
     """A scene resident on the device (lux_scene_upload)."""
 
@@ -301,7 +333,8 @@ class GpuScene:
         handle = C.c_void_p()
         ctx.check(lib().lux_scene_upload(ctx.handle, _ptr(packed.scene_words), len(packed.scene_words),
                                          _ptr(packed.geometry_words), len(packed.geometry_words),
-                                         _ptr(packed.lights), len(packed.lights), 0, C.byref(handle)))
+                                         _ptr(packed.lights), len(packed.lights), packed.conventional,
+                                         C.byref(handle)))
         self.handle = handle
 
     def layout(self) -> dict:

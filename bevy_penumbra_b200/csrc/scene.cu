@@ -318,9 +318,16 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     *out = nullptr;
     if (!sw || sn < 1 || !gw || gn < 1 || (light_count && !lights) || conventional > light_count)
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene upload: missing words or lights");
-    if (conventional != 0)
-        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
-                        "scene upload: conventional (punctual/directional) lights are not supported by this build");
+    if (conventional >= 16u)
+        return lux_fail(ctx, LUX_ERR_CAPACITY,
+                        "scene upload: at most 15 conventional lights (a hit's next-event slots are shared with the "
+                        "emissive samples)");
+    for (uint32_t l = 0; l < conventional; ++l) {
+        const LuxLight &L = lights[l];
+        for (int c = 0; c < 4; ++c)
+            if (!std::isfinite(L.position[c]) || !std::isfinite(L.color[c]) || !std::isfinite(L.direction[c]))
+                return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: conventional light with non-finite fields");
+    }
     if (sn > 0xffffffffu || gn > 0xffffffffu)
         return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: word stream exceeds 2^32 words");
     // Header (src/scene.rs:2103-2110): material end, instance base, count, stride.

@@ -3,8 +3,10 @@
 // (emissiveResponseTracked, shaders/cascades.slang:57-134).
 //
 // Synthetic-material subset, identical to the CPU oracle: untextured opaque
-// materials (materialSample = 1), no environment map and no conventional
-// lights (rejected at upload).  With multi-bounce on, the secondary cache's
+// materials (materialSample = 1), no environment map; conventional
+// (point, spot, directional) lights with visibility rays
+// (conventionalLightResponseTracked, shaders/cascades.slang:136-176).  With
+// multi-bounce on, the secondary cache's
 // irradiance of the previous frame adds diffuse bounce light (secondaryFeedback,
 // shaders/world_resolve.slang:204-279), and the secondary cache's own hits
 // leave out their emission (environmentScale.z).  All source groups are
@@ -206,6 +208,7 @@ struct NeeQuery {
     float limit;
     f3 contribution;
     uint32_t light;  // emitter record index (coherence sort key)
+    bool conventional;  // a conventional light: added as is, not averaged over the emissive samples
 };
 
 // emissiveResponseTracked, shaders/cascades.slang:57-134, up to (but not
@@ -288,7 +291,62 @@ __device__ void emissive_queries(const SceneView &S, const ShadeParams &P, f3 po
                             emission.y * (((diffuse.y * factor) * cosine) / p),
                             emission.z * (((diffuse.z * factor) * cosine) / p)};
         q.light = low;
+        q.conventional = false;
         emit(sample, q);
+    }
+}
+
+// conventionalLightResponseTracked (shaders/cascades.slang:136-176) up to the
+// visibility traces: one query per conventional light that faces the
+// surface, from the biased hit point to the light (finite lights: range fade
+// (1 - (d/range)^4)^2 / d^2, spot cone squared; directional lights: the
+// direction in position.xyz at distance 1e20), contribution color x
+// (attenuation x cos x response).  Light i takes slot first_slot + i.
+// (d/range)^4 is (x^2)^2 here and in the oracle.
+template <typename Emit>
+__device__ void conventional_queries(const SceneView &S, const ShadeParams &P, f3 position, f3 normal, f3 gnormal,
+                                     f3 view, float roughness, f3 diffuse, uint32_t first_slot, Emit &&emit) {
+    const uint32_t n = S.conventional_lights;
+    if (n == 0u) return;
+    const float bias = P.normal_bias;
+    const f3 offset = ray_offset(position, gnormal, bias);
+    for (uint32_t i = 0; i < n; ++i) {
+        const LuxLight *L = S.lights + i;
+        f3 lp{__ldg(&L->position[0]), __ldg(&L->position[1]), __ldg(&L->position[2])};
+        float range = __ldg(&L->position[3]);
+        const bool finite = range > 0.0f;
+        f3 to_light = lp;
+        float distance = 1e20f, attenuation = 1.0f;
+        if (finite) {
+            to_light = lp - position;
+            distance = length(to_light);
+            if (distance >= range || distance < bias) continue;
+            to_light = to_light / distance;
+            float x = distance / range;
+            float x2 = x * x;
+            float fade = saturate(1.0f - x2 * x2);
+            attenuation = (fade * fade) / fmaxf(distance * distance, 0.0001f);
+            float spot = __ldg(&L->direction[3]);
+            if (spot > 0.0f) {
+                f3 ldir{__ldg(&L->direction[0]), __ldg(&L->direction[1]), __ldg(&L->direction[2])};
+                float cone = saturate(dot(ldir, -to_light) * spot + __ldg(&L->color[3]));
+                attenuation *= cone * cone;
+            }
+        }
+        float cosine = fmaxf(0.0f, dot(normal, to_light));
+        if (!(cosine > 0.0f && dot(gnormal, to_light) > 0.0f && attenuation > 0.0f)) continue;
+        NeeQuery q;
+        q.origin = offset;
+        q.direction = to_light;
+        q.limit = distance - bias;
+        float factor = disney_multiplier(normal, to_light, view, roughness) / kPi;
+        float scale = attenuation * cosine;
+        q.contribution = f3{__ldg(&L->color[0]) * (scale * (diffuse.x * factor)),
+                            __ldg(&L->color[1]) * (scale * (diffuse.y * factor)),
+                            __ldg(&L->color[2]) * (scale * (diffuse.z * factor))};
+        q.light = i;
+        q.conventional = true;
+        emit(first_slot + i, q);
     }
 }
 
@@ -357,6 +415,7 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
         extra = f3{e.x * diffuse.x, e.y * diffuse.y, e.z * diffuse.z};
     }
     emissive_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
+    conventional_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
     return true;
 }
 
@@ -370,9 +429,11 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
 
 // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188, after the
 // next-event sum: radiance = base + sum / count.
-__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count, const f3 *extra = nullptr) {
+__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count, const f3 *conventional = nullptr,
+                                              const f3 *extra = nullptr) {
     f3 radiance = base;
     if (count) radiance = radiance + f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
+    if (conventional) radiance = radiance + *conventional;  // conventional lights' visible contributions
     if (extra) radiance = radiance + *extra;  // secondaryFeedback's diffuse term, added last
     if (!finite3(radiance)) return f3{0.0f, 0.0f, 0.0f};
     return f3{fmaxf(radiance.x, 0.0f), fmaxf(radiance.y, 0.0f), fmaxf(radiance.z, 0.0f)};

@@ -590,11 +590,14 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
         load_ray(V, ray, o, d, hit);
         supported = lux::outgoing_record(S, P, o, d, hit, base, extra, rec, count,
                                          [&](uint32_t sample, const lux::NeeQuery &query) {
+                                             if (nq >= lux::kMaxNeeSamples) return;  // host checks the slot count
                                              q[nq] = query;
                                              slot_of[nq] = sample;
                                              ++nq;
                                          });
-        V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? count : lux::kEmpty));
+        // w: the emissive estimator's divisor | the conventional-light slots << 16.
+        const uint32_t slots = count | (S.conventional_lights << 16);
+        V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? slots : lux::kEmpty));
         if (P.feedback) V.ts.ray_extra[ray] = make_float4(extra.x, extra.y, extra.z, 0.0f);
         // The multi-bounce secondary receiver of receiver i: its ray frame % R.
         if (F.record_hits && rec.valid && ray % F.rays_per_receiver == P.frame % F.rays_per_receiver) {
@@ -617,7 +620,8 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     uint32_t at = first + prefix - nq;
     if (ray < rays) {
         uint32_t k = 0;
-        for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
+        const uint32_t slots = count + S.conventional_lights;
+        for (uint32_t s = 0; s < slots && s < lux::kMaxNeeSamples; ++s) {
             uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
             if (k < nq && slot_of[k] == s) {
                 uint32_t qi = at + k;
@@ -626,7 +630,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
                     V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
                     V.ts.slot_query[slot] = qi;
                     V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
-                                                          q[k].contribution.z, 0.0f);
+                                                          q[k].contribution.z, q[k].conventional ? 1.0f : 0.0f);
                     if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
                 } else {
                     V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
@@ -715,10 +719,12 @@ __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(View
 // `feedback`); false when the ray's query is unsupported.
 __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, f3 &radiance, bool feedback = false) {
     float4 b = V.ts.ray_base[ray];
-    uint32_t count = lux::as_uint(b.w);
-    if (count == lux::kEmpty) return false;
-    f3 sum{0.0f, 0.0f, 0.0f};
-    for (uint32_t s = 0; s < count && s < lux::kMaxNeeSamples; ++s) {
+    const uint32_t packed = lux::as_uint(b.w);
+    if (packed == lux::kEmpty) return false;
+    // The emissive samples (averaged) then the conventional lights (summed).
+    const uint32_t count = packed & 0xffffu, conventional = packed >> 16;
+    f3 sum{0.0f, 0.0f, 0.0f}, csum{0.0f, 0.0f, 0.0f};
+    for (uint32_t s = 0; s < count + conventional && s < lux::kMaxNeeSamples; ++s) {
         size_t slot = (size_t)ray * lux::kMaxNeeSamples + s;
         uint32_t qi = V.ts.slot_query[slot];
         if (qi == lux::kEmpty) continue;
@@ -727,15 +733,15 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
         if (r == 2) return false;
         if (r == 1) continue;
         float4 c = V.ts.slot_contrib[slot];
-        sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
+        if (s < count)
+            sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
+        else
+            csum = f3{csum.x + c.x, csum.y + c.y, csum.z + c.z};
     }
-    if (feedback) {
-        float4 e = V.ts.ray_extra[ray];
-        f3 extra{e.x, e.y, e.z};
-        radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count, &extra);
-    } else {
-        radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count);
-    }
+    float4 e = feedback ? V.ts.ray_extra[ray] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    f3 extra{e.x, e.y, e.z};
+    radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count, conventional ? &csum : nullptr,
+                                    feedback ? &extra : nullptr);
     return true;
 }
 
@@ -2105,6 +2111,18 @@ static void enqueue_pack(LuxView *v, const FrameParams &F, cudaStream_t st) {
     pack_kernel<<<v->ctx->sm_count * 8, 64, smem, st>>>(v->dev, F);
 }
 
+// Next-event slots of one hit: the emissive samples (max(1, n / 2)) and one
+// per conventional light must fit the per-ray slot arrays.
+static lux_status check_nee_slots(LuxContext *ctx, const LuxSettings *settings, const LuxScene *scene) {
+    LuxSettings s = *settings;
+    lux_settings_sanitize(&s);
+    uint32_t emissive = s.emissive_samples / 2u < 1u ? 1u : s.emissive_samples / 2u;
+    if (emissive + scene->view.conventional_lights > lux::kMaxNeeSamples)
+        return lux_fail(ctx, LUX_ERR_CAPACITY,
+                        "trace: emissive samples / 2 + conventional lights exceed the 16 next-event slots of a hit");
+    return LUX_OK;
+}
+
 // Per-frame roles of a view in a multi-bounce frame.
 struct FrameRole {
     uint32_t sparse = 0;         // receivers with position.w == 0 are absent (the secondary cache)
@@ -2239,6 +2257,8 @@ extern "C" lux_status lux_view_secondary(LuxView *v, LuxView **secondary) {
 static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSettings *settings, const LuxReceivers *rc,
                              const FrameRole &role, const LuxView *fb_owner) {
     LuxContext *ctx = v->ctx;
+    lux_status slots = check_nee_slots(ctx, settings, scene);
+    if (slots != LUX_OK) return slots;
     if (rc->count > v->desc.max_receivers)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: more receivers than the view's max_receivers");
     if (rc->count && (!rc->position || (!rc->normal && settings->layout == LUX_LAYOUT_SPLIT)))
@@ -2631,6 +2651,8 @@ __global__ void radiance_out_kernel(ViewDevice V, uint32_t count, float4 *__rest
 lux_status launch_interval_radiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings_in,
                                     const LuxRay *rays, uint32_t count, float *out, const ViewDevice &V,
                                     uint32_t capacity) {
+    lux_status slots = check_nee_slots(ctx, settings_in, scene);
+    if (slots != LUX_OK) return slots;
     LuxSettings s = *settings_in;
     lux_settings_sanitize(&s);
     FrameParams F;
@@ -2992,6 +3014,8 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
         if (rc.count && (!rc.position || !rc.normal))
             return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "batch: missing receiver buffers");
         lux_status ps = make_params(J.view, &s, rc.count, params[j]);
+        if (ps != LUX_OK) return ps;
+        ps = check_nee_slots(ctx, &s, J.scene);
         if (ps != LUX_OK) return ps;
         params[j].lod_enabled = 0;  // batched frames use LOD 0
         if ((uint64_t)rc.count * params[j].rays_per_receiver > J.view->desc.max_rays)

@@ -102,15 +102,18 @@ def f32(*v) -> np.ndarray:
 class OracleScene:
     """Oracle view of the reference word streams."""
 
-    def __init__(self, scene_words: np.ndarray, geometry_words: np.ndarray, lights: np.ndarray):
+    def __init__(self, scene_words: np.ndarray, geometry_words: np.ndarray, lights: np.ndarray,
+                 conventional: int = 0):
         self._keep = (np.ascontiguousarray(scene_words, np.uint32), np.ascontiguousarray(geometry_words, np.uint32),
                       np.ascontiguousarray(lights, np.uint32))
         sw, gw, lt = self._keep
-        self.handle = lib().orc_scene_create(_p(sw), sw.size // 4, _p(gw), gw.size // 4, _p(lt), lt.size // 24, 0)
+        self.handle = lib().orc_scene_create(_p(sw), sw.size // 4, _p(gw), gw.size // 4, _p(lt), lt.size // 24,
+                                             conventional)
 
     @staticmethod
     def from_packed(packed) -> "OracleScene":
-        return OracleScene(packed.scene_words, packed.geometry_words, packed.lights)
+        return OracleScene(packed.scene_words, packed.geometry_words, packed.lights,
+                           getattr(packed, "conventional", 0))
 
     def trace_rays(self, rays: np.ndarray, any_hit: bool = False, threads: int = 0):
         """rays: structured RAY_DTYPE array -> HIT_DTYPE array, counters."""

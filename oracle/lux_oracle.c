@@ -1276,6 +1276,56 @@ static int emissive_response(const OrcScene *S, const LuxSettings *st, const flo
     return 1;
 }
 
+/* conventionalLightResponseTracked (shaders/cascades.slang:136-176): the
+ * visible contributions of the conventional lights (point, spot: range fade
+ * (1 - (d/range)^4)^2 / d^2 with (d/range)^4 as (x^2)^2, spot cone squared;
+ * directional: direction in position.xyz at distance 1e20), summed in light
+ * order; 0 when a visibility query is unsupported. */
+static int conventional_response(const OrcScene *S, const LuxSettings *st, const float position[3],
+                                 const float normal[3], const float gnormal[3], const float view[3], float roughness,
+                                 const float diffuse[3], float out[3], uint64_t *shadow_rays, OrcCounters *cn) {
+    out[0] = out[1] = out[2] = 0.0f;
+    const float bias = st->normal_bias;
+    float offset[3];
+    orc_ray_offset(position, gnormal, bias, offset);
+    for (uint32_t i = 0; i < S->conventional; ++i) {
+        const LuxLight *L = &S->lights[i];
+        float range = L->position[3];
+        int finite = range > 0.0f;
+        float to_light[3] = {L->position[0], L->position[1], L->position[2]};
+        float distance = 1e20f, attenuation = 1.0f;
+        if (finite) {
+            for (int c = 0; c < 3; ++c) to_light[c] = L->position[c] - position[c];
+            distance = length3(to_light);
+            if (distance >= range || distance < bias) continue;
+            for (int c = 0; c < 3; ++c) to_light[c] = to_light[c] / distance;
+            float x = distance / range;
+            float x2 = x * x;
+            float fade = saturatef(1.0f - x2 * x2);
+            attenuation = (fade * fade) / fmaxf(distance * distance, 0.0001f);
+            if (L->direction[3] > 0.0f) {
+                float neg[3] = {-to_light[0], -to_light[1], -to_light[2]};
+                float cone = saturatef(dot3(L->direction, neg) * L->direction[3] + L->color[3]);
+                attenuation *= cone * cone;
+            }
+        }
+        float cosine = fmaxf(0.0f, dot3(normal, to_light));
+        if (!(cosine > 0.0f && dot3(gnormal, to_light) > 0.0f && attenuation > 0.0f)) continue;
+        int supported;
+        if (shadow_rays) (*shadow_rays)++;
+        int blocked = orc_trace_occluded(S, offset, to_light, distance - bias, &supported, cn);
+        if (!supported) {
+            out[0] = out[1] = out[2] = 0.0f;
+            return 0;
+        }
+        if (blocked) continue;
+        float factor = disney_multiplier(normal, to_light, view, roughness) / PI_F;
+        float scale = attenuation * cosine;
+        for (int c = 0; c < 3; ++c) out[c] = out[c] + L->color[c] * (scale * (diffuse[c] * factor));
+    }
+    return 1;
+}
+
 /* Multi-bounce roles of a frame (RadianceCascades::multi_bounce). */
 typedef struct {
     const OrcFrame *feedback;  /* secondary frame whose cascade-0 probes add bounce light (NULL: none) */
@@ -1358,6 +1408,15 @@ static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bou
                 return 0;
             }
             for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + nee[c];
+            if (S->conventional) {
+                float conv[3];
+                if (!conventional_response(S, st, position, normal, flipped, view, roughness, diffuse, conv,
+                                           shadow_rays, cn)) {
+                    out[0] = out[1] = out[2] = 0.0f;
+                    return 0;
+                }
+                for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + conv[c];
+            }
             if (bn && bn->feedback) {
                 float e[3];
                 feedback_irradiance(bn->feedback, position, normal, e);

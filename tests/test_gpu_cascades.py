@@ -323,3 +323,21 @@ def test_split_lod_frames_and_resolve_match_oracle():
     np.testing.assert_allclose(out, prev.resolve(ppos, pnrm), rtol=RTOL, atol=ATOL)
     blends = [oracle.lod_blend(st(1).to_c(), cam, p[:3])[2] for p in ppos[:512]]
     assert any(0.0 < b < 1.0 for b in blends)  # some points blend two LODs
+
+
+def test_split_frame_with_conventional_lights_matches_oracle():
+    from tests.test_gpu_radiance import lit_cornell
+    settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   emissive_samples=8, frame_index=2).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    scene_packed = lit_cornell()
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, scene_packed)
+    view = bp.SplitView(ctx, max_receivers=len(pos), max_cells=1 << 16, max_entries=1 << 24, max_rays=len(pos) * 4)
+    d_pos, d_nrm = to_device(pos), to_device(nrm)
+    view.trace_merge(scene, settings, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
+    st = view.stats()
+    assert st.error_flags == 0
+    ofr = oracle.OracleFrame(oracle.OracleScene.from_packed(scene_packed), settings.to_c(), pos, nrm)
+    compare_levels(settings, [view.read_level(l) for l in range(4)], ofr, exact=False)
+    assert st.shadow_rays == ofr.stats().shadow_rays

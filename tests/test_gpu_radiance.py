@@ -58,3 +58,46 @@ def test_interval_radiance_bit_exact(name, lo, hi, samples):
     cpu = oracle_radiance(name, settings, rays)
     np.testing.assert_array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
     assert np.mean(gpu[:, :3].sum(1) > 0) > 0.2, "many rays must see lit surfaces or emitters"
+
+
+def lit_cornell():
+    """The Cornell scene with a point, a spot and a directional light."""
+    d = np.array([0.3, 1.0, 0.2])
+    return packed("cornell").with_conventional_lights([
+        bp.conventional_light((0.3, 1.5, 0.2), 5.0, (2.0, 2.0, 2.0)),
+        bp.conventional_light((-0.5, 1.8, -0.5), 4.0, (1.0, 0.5, 0.2), direction=(0.0, -1.0, 0.0),
+                              spot_scale=2.0, spot_offset=-1.0),
+        bp.directional_light(d / np.linalg.norm(d), (0.5, 0.5, 0.5)),
+    ])
+
+
+@pytest.mark.parametrize("samples", [16, 2])
+def test_interval_radiance_with_conventional_lights_bit_exact(samples):
+    """conventionalLightResponseTracked: point, spot and directional lights
+    with visibility rays, added after the emissive estimate."""
+    settings = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=samples, frame_index=3).sanitized()
+    rays = random_rays(4096, (-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), seed=11 + samples)
+    scene_packed = lit_cornell()
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, scene_packed)
+    d_rays = to_device(rays)
+    d_out = empty_device(len(rays) * 16)
+    bp.interval_radiance(ctx, scene, settings, d_rays.data_ptr(), len(rays), d_out.data_ptr())
+    ctx.synchronize()
+    gpu = from_device(d_out, np.float32, (len(rays), 4))
+    osc = oracle.OracleScene.from_packed(scene_packed)
+    s = settings.to_c()
+    cpu = np.zeros_like(gpu)
+    hit = np.zeros(1, dtype=bp.HIT_DTYPE)
+    rad = np.zeros(3, np.float32)
+    for i in range(len(rays)):
+        o = np.ascontiguousarray(rays["origin"][i])
+        dd = np.ascontiguousarray(rays["direction"][i])
+        oracle.lib().orc_trace_closest(osc.handle, o.ctypes.data, dd.ctypes.data, 0.0, 1e20, hit.ctypes.data, None)
+        ok = oracle.lib().orc_outgoing_radiance(osc.handle, C.byref(s), o.ctypes.data, dd.ctypes.data,
+                                                hit.ctypes.data, rad.ctypes.data, None, None)
+        cpu[i] = (*rad, hit["distance"][0]) if ok else (0, 0, 0, -1)
+    np.testing.assert_array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+    # The lights add light: brighter than the emitter-only scene on average.
+    plain = oracle_radiance("cornell", settings, rays)
+    assert gpu[:, :3].sum() > plain[:, :3].sum() * 1.05
