@@ -287,6 +287,29 @@ LUX_HD bool lod_selects_high(uint32_t sample, uint32_t frame, float blend) {
 }
 constexpr uint64_t kEmptyCell = 0xffffffffffffffffull;
 
+// transportRandom (shaders/common.slang:292-295): a decorrelated uniform in
+// (0, 1) from a seed and a lane.
+LUX_HD float transport_random(uint32_t seed, uint32_t lane) {
+    uint32_t bits = transport_hash(seed + 0x9e3779b9u * (lane + 1u));
+    return ((float)(bits >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+// cosineDirection (shaders/common.slang:407-412): tangent frame from the
+// normal and the y axis (the x axis near the poles), radius sqrt(u1) at u2
+// turns, height sqrt(1 - u1); cos/sin of the turn as sincos_turns.
+LUX_HD f3 cosine_direction_frame(f3 n, float u1, float u2) {
+    f3 axis = fabsf(n.y) < 0.99f ? f3{0.0f, 1.0f, 0.0f} : f3{1.0f, 0.0f, 0.0f};
+    f3 t = cross(axis, n);
+    float tl = sqrtf(dot(t, t));
+    t = f3{t.x / tl, t.y / tl, t.z / tl};
+    f3 b = cross(n, t);
+    float c, s;
+    sincos_turns(u2, c, s);
+    float r = sqrtf(u1), h = sqrtf(1.0f - u1);
+    float rc = r * c, rs = r * s;
+    return f3{(t.x * rc + b.x * rs) + n.x * h, (t.y * rc + b.y * rs) + n.y * h, (t.z * rc + b.z * rs) + n.z * h};
+}
+
 // Cosine-weighted direction about the unit normal n: radius sqrt(u1) at
 // u2 turns in the tangent plane, height sqrt(1 - u1), in the orthonormal
 // frame of Duff et al., "Building an Orthonormal Basis, Revisited" (2017).

@@ -3,7 +3,9 @@
 // (emissiveResponseTracked, shaders/cascades.slang:57-134).
 //
 // Synthetic-material subset, identical to the CPU oracle: untextured opaque
-// materials (materialSample = 1), no environment map; conventional
+// materials (materialSample = 1); a constant environment (no environment
+// map) with cosine-proposal visibility rays (environmentResponseTracked,
+// shaders/environment.slang:154-230); conventional
 // (point, spot, directional) lights with visibility rays
 // (conventionalLightResponseTracked, shaders/cascades.slang:136-176).  With
 // multi-bounce on, the secondary cache's
@@ -38,7 +40,13 @@ struct ShadeParams {
     uint32_t skip_emission;  // secondary cache: no first-hit emission (next-event estimation carries it)
     uint32_t feedback;       // 1: add diffuse x the secondary cache's irradiance at the hit
     Feedback fb;
+    f3 environment;          // constant environment radiance (black: no environment samples)
 };
+
+// environmentResponseTracked returns early for a black constant environment.
+__device__ __forceinline__ bool environment_on(const ShadeParams &P) {
+    return P.environment.x > 0.0f || P.environment.y > 0.0f || P.environment.z > 0.0f;
+}
 
 __device__ __forceinline__ uint4 sword(const SceneView &S, uint32_t i) {
     i = i < S.scene_word_count ? i : S.scene_word_count - 1u;
@@ -199,7 +207,12 @@ struct SurfaceRecord {
     bool valid;
 };
 
-constexpr uint32_t kMaxNeeSamples = 16u;  // max(1, emissive_samples / 2) with emissive_samples <= 32
+// Next-event slots of one hit: max(1, emissive_samples / 2) emissive samples,
+// as many environment samples with a non-black environment, one per
+// conventional light.
+constexpr uint32_t kMaxNeeSamples = 16u;
+
+enum NeeGroup : uint32_t { kNeeEmissive = 0u, kNeeEnvironment = 1u, kNeeConventional = 2u };
 
 // One next-event sample of emissiveResponseTracked whose visibility query is
 // still to be traced: the query ray and the sample's contribution if visible.
@@ -208,7 +221,7 @@ struct NeeQuery {
     float limit;
     f3 contribution;
     uint32_t light;  // emitter record index (coherence sort key)
-    bool conventional;  // a conventional light: added as is, not averaged over the emissive samples
+    NeeGroup group;  // emissive and environment samples are averaged per group, conventional lights summed
 };
 
 // emissiveResponseTracked, shaders/cascades.slang:57-134, up to (but not
@@ -291,7 +304,7 @@ __device__ void emissive_queries(const SceneView &S, const ShadeParams &P, f3 po
                             emission.y * (((diffuse.y * factor) * cosine) / p),
                             emission.z * (((diffuse.z * factor) * cosine) / p)};
         q.light = low;
-        q.conventional = false;
+        q.group = kNeeEmissive;
         emit(sample, q);
     }
 }
@@ -345,8 +358,49 @@ __device__ void conventional_queries(const SceneView &S, const ShadeParams &P, f
                             __ldg(&L->color[1]) * (scale * (diffuse.y * factor)),
                             __ldg(&L->color[2]) * (scale * (diffuse.z * factor))};
         q.light = i;
-        q.conventional = true;
+        q.group = kNeeConventional;
         emit(first_slot + i, q);
+    }
+}
+
+// environmentResponseTracked (shaders/environment.slang:154-230) for a
+// constant environment, up to the visibility traces: `count` cosine
+// proposals (no alias samples without an environment map, so pdf = cos / pi),
+// direction cosineDirection(normal, transportRandom lanes 0 and 1) of the
+// seed transportHash(seed ^ transportHash(sequence + 0x85ebca6b)),
+// sequence = sample + (frame ^ 0xE17A0002) x count, seed = hashKey of the
+// hit's cell of 0.05 probe spacings with w = 37; each a query from the biased
+// hit point to distance 1e20 with contribution environment x (response x
+// cos / pdf).  Sample i takes slot first_slot + i.
+template <typename Emit>
+__device__ void environment_queries(const ShadeParams &P, f3 position, f3 normal, f3 gnormal, f3 view,
+                                    float roughness, f3 diffuse, uint32_t count, uint32_t first_slot, Emit &&emit) {
+    if (!environment_on(P)) return;
+    const f3 env = P.environment;
+    float cell = P.probe_spacing * 0.05f;
+    uint32_t seed = hash_key((int32_t)floorf(position.x / cell), (int32_t)floorf(position.y / cell),
+                             (int32_t)floorf(position.z / cell), 37, 16777216u);
+    uint32_t sample_frame = P.frame ^ 0xE17A0002u;
+    const f3 offset = ray_offset(position, gnormal, P.normal_bias);
+    for (uint32_t sample = 0; sample < count; ++sample) {
+        uint32_t sequence = sample + sample_frame * count;
+        uint32_t sample_seed = transport_hash(seed ^ transport_hash(sequence + 0x85ebca6bu));
+        f3 d = cosine_direction_frame(normal, transport_random(sample_seed, 0u), transport_random(sample_seed, 1u));
+        float cosine = fmaxf(0.0f, dot(normal, d));
+        if (cosine <= 0.0f || dot(gnormal, d) <= 0.0f) continue;
+        float pdf = cosine / kPi;
+        if (!(pdf > 0.0f) || !isfinite(pdf)) continue;
+        NeeQuery q;
+        q.origin = offset;
+        q.direction = d;
+        q.limit = 1e20f;
+        float factor = disney_multiplier(normal, d, view, roughness) / kPi;
+        q.contribution = f3{env.x * (((diffuse.x * factor) * cosine) / pdf),
+                            env.y * (((diffuse.y * factor) * cosine) / pdf),
+                            env.z * (((diffuse.z * factor) * cosine) / pdf)};
+        q.light = 63u;
+        q.group = kNeeEnvironment;
+        emit(first_slot + sample, q);
     }
 }
 
@@ -415,7 +469,9 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
         extra = f3{e.x * diffuse.x, e.y * diffuse.y, e.z * diffuse.z};
     }
     emissive_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
-    conventional_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
+    environment_queries(P, position, normal, flipped, view, roughness, diffuse, count, count, emit);
+    conventional_queries(S, P, position, normal, flipped, view, roughness, diffuse,
+                         environment_on(P) ? 2u * count : count, emit);
     return true;
 }
 
@@ -428,11 +484,15 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
 }
 
 // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188, after the
-// next-event sum: radiance = base + sum / count.
-__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count, const f3 *conventional = nullptr,
-                                              const f3 *extra = nullptr) {
+// next-event sums: radiance = base + sum / count + environment / count
+// + conventional + extra.
+__device__ __forceinline__ f3 finish_radiance(f3 base, f3 sum, uint32_t count, const f3 *environment = nullptr,
+                                              const f3 *conventional = nullptr, const f3 *extra = nullptr) {
     f3 radiance = base;
     if (count) radiance = radiance + f3{sum.x / (float)count, sum.y / (float)count, sum.z / (float)count};
+    if (count && environment)  // the environment samples, averaged over the same count
+        radiance = radiance + f3{environment->x / (float)count, environment->y / (float)count,
+                                 environment->z / (float)count};
     if (conventional) radiance = radiance + *conventional;  // conventional lights' visible contributions
     if (extra) radiance = radiance + *extra;  // secondaryFeedback's diffuse term, added last
     if (!finite3(radiance)) return f3{0.0f, 0.0f, 0.0f};

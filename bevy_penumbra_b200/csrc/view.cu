@@ -595,8 +595,9 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
                                              slot_of[nq] = sample;
                                              ++nq;
                                          });
-        // w: the emissive estimator's divisor | the conventional-light slots << 16.
-        const uint32_t slots = count | (S.conventional_lights << 16);
+        // w: the emissive estimator's divisor | the conventional-light slots << 16
+        // | environment samples present << 24.
+        const uint32_t slots = count | (S.conventional_lights << 16) | ((lux::environment_on(P) ? 1u : 0u) << 24);
         V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? slots : lux::kEmpty));
         if (P.feedback) V.ts.ray_extra[ray] = make_float4(extra.x, extra.y, extra.z, 0.0f);
         // The multi-bounce secondary receiver of receiver i: its ray frame % R.
@@ -620,7 +621,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     uint32_t at = first + prefix - nq;
     if (ray < rays) {
         uint32_t k = 0;
-        const uint32_t slots = count + S.conventional_lights;
+        const uint32_t slots = count * (lux::environment_on(P) ? 2u : 1u) + S.conventional_lights;
         for (uint32_t s = 0; s < slots && s < lux::kMaxNeeSamples; ++s) {
             uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
             if (k < nq && slot_of[k] == s) {
@@ -630,7 +631,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
                     V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
                     V.ts.slot_query[slot] = qi;
                     V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
-                                                          q[k].contribution.z, q[k].conventional ? 1.0f : 0.0f);
+                                                          q[k].contribution.z, (float)q[k].group);
                     if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
                 } else {
                     V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
@@ -721,10 +722,12 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
     float4 b = V.ts.ray_base[ray];
     const uint32_t packed = lux::as_uint(b.w);
     if (packed == lux::kEmpty) return false;
-    // The emissive samples (averaged) then the conventional lights (summed).
-    const uint32_t count = packed & 0xffffu, conventional = packed >> 16;
-    f3 sum{0.0f, 0.0f, 0.0f}, csum{0.0f, 0.0f, 0.0f};
-    for (uint32_t s = 0; s < count + conventional && s < lux::kMaxNeeSamples; ++s) {
+    // The emissive samples (averaged), the environment samples (averaged over
+    // the same count) then the conventional lights (summed).
+    const uint32_t count = packed & 0xffffu, conventional = (packed >> 16) & 0xffu;
+    const uint32_t environment = (packed >> 24) != 0u ? count : 0u;
+    f3 sum{0.0f, 0.0f, 0.0f}, esum{0.0f, 0.0f, 0.0f}, csum{0.0f, 0.0f, 0.0f};
+    for (uint32_t s = 0; s < count + environment + conventional && s < lux::kMaxNeeSamples; ++s) {
         size_t slot = (size_t)ray * lux::kMaxNeeSamples + s;
         uint32_t qi = V.ts.slot_query[slot];
         if (qi == lux::kEmpty) continue;
@@ -735,13 +738,15 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
         float4 c = V.ts.slot_contrib[slot];
         if (s < count)
             sum = f3{sum.x + c.x, sum.y + c.y, sum.z + c.z};
+        else if (s < count + environment)
+            esum = f3{esum.x + c.x, esum.y + c.y, esum.z + c.z};
         else
             csum = f3{csum.x + c.x, csum.y + c.y, csum.z + c.z};
     }
     float4 e = feedback ? V.ts.ray_extra[ray] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     f3 extra{e.x, e.y, e.z};
-    radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count, conventional ? &csum : nullptr,
-                                    feedback ? &extra : nullptr);
+    radiance = lux::finish_radiance(f3{b.x, b.y, b.z}, sum, count, environment ? &esum : nullptr,
+                                    conventional ? &csum : nullptr, feedback ? &extra : nullptr);
     return true;
 }
 
@@ -2001,6 +2006,7 @@ static lux_status make_params(LuxView *v, const LuxSettings *settings_in, uint32
     F.shade.exposure = s.exposure;
     F.shade.emissive_samples = s.emissive_samples;
     F.shade.frame = s.frame_index;
+    F.shade.environment = f3{s.environment[0], s.environment[1], s.environment[2]};
     F.radiance_blend = s.temporal_blend;
     F.transmittance_blend = s.transmittance_blend;
     F.history = 0;
@@ -2111,15 +2117,18 @@ static void enqueue_pack(LuxView *v, const FrameParams &F, cudaStream_t st) {
     pack_kernel<<<v->ctx->sm_count * 8, 64, smem, st>>>(v->dev, F);
 }
 
-// Next-event slots of one hit: the emissive samples (max(1, n / 2)) and one
-// per conventional light must fit the per-ray slot arrays.
+// Next-event slots of one hit: the emissive samples (max(1, n / 2)), as many
+// environment samples with a non-black environment, and one per conventional
+// light must fit the per-ray slot arrays.
 static lux_status check_nee_slots(LuxContext *ctx, const LuxSettings *settings, const LuxScene *scene) {
     LuxSettings s = *settings;
     lux_settings_sanitize(&s);
     uint32_t emissive = s.emissive_samples / 2u < 1u ? 1u : s.emissive_samples / 2u;
-    if (emissive + scene->view.conventional_lights > lux::kMaxNeeSamples)
+    bool environment = s.environment[0] > 0.0f || s.environment[1] > 0.0f || s.environment[2] > 0.0f;
+    if (emissive * (environment ? 2u : 1u) + scene->view.conventional_lights > lux::kMaxNeeSamples)
         return lux_fail(ctx, LUX_ERR_CAPACITY,
-                        "trace: emissive samples / 2 + conventional lights exceed the 16 next-event slots of a hit");
+                        "trace: emissive samples / 2 (twice with a non-black environment) + conventional lights "
+                        "exceed the 16 next-event slots of a hit");
     return LUX_OK;
 }
 
@@ -2664,6 +2673,7 @@ lux_status launch_interval_radiance(LuxContext *ctx, const LuxScene *scene, cons
     F.shade.exposure = s.exposure;
     F.shade.emissive_samples = s.emissive_samples;
     F.shade.frame = s.frame_index;
+    F.shade.environment = f3{s.environment[0], s.environment[1], s.environment[2]};
     cudaStream_t st = ctx->stream;
     scratch_clear_kernel<<<1, 32, 0, st>>>(V);
     if (count) {

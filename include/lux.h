@@ -114,7 +114,9 @@ typedef struct LuxSettings {
     float interval_length;          /* RadianceCascades::interval_length (tuning.y) */
     float normal_bias;              /* RadianceCascades::normal_bias (tuning.z) */
     float intensity;                /* RadianceCascades::intensity (tuning.w) */
-    float environment[3];           /* RadianceCascades::environment (escape radiance of hit-surface NEE; primary escapes are supported zero) */
+    float environment[3];           /* RadianceCascades::environment: constant sky radiance seen by hit-surface NEE
+                                       (environmentResponseTracked, shaders/environment.slang:154-230; black: no
+                                       sky samples); escaped interval rays carry supported zero */
     float exposure;                 /* camera exposure (params.environment.w) */
     uint32_t emissive_samples;      /* RadianceCascades::emissive_samples, 1..=32; NEE draws max(1, n/2) */
     uint32_t levels;                /* extension: cascade count, 1..=LUX_MAX_LEVELS (reference 4) */

@@ -67,6 +67,9 @@ def lib():
             "orc_frame_run_retain": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64]),
             "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P, P]),
             "orc_lod_blend": (None, [P, P, P, P, P, P]),
+            "orc_transport_random": (F, [U, U]),
+            "orc_cosine_direction_frame": (None, [P, F, F, P]),
+            "orc_environment_response": (C.c_int, [P, P, F, F, U, U, P, P, P, P, F, P, C.c_int, P, P, P]),
             "orc_screen_filter": (None, [P, U, U, P, P, P, P, P, P, U, U, U, P, P, P]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
@@ -249,6 +252,33 @@ def lod_blend(settings_c, camera, position):
     lib().orc_lod_blend(C.byref(settings_c), C.byref(camera) if camera is not None else None, _p(p), C.byref(low),
                         C.byref(high), C.byref(blend))
     return int(low.value), int(high.value), float(blend.value)
+
+
+def transport_random(seed, lane):
+    """transportRandom (shaders/common.slang:292-295)."""
+    return float(lib().orc_transport_random(seed & 0xFFFFFFFF, lane & 0xFFFFFFFF))
+
+
+def cosine_direction_frame(normal, u1, u2):
+    """cosineDirection (shaders/common.slang:407-412) of a unit normal."""
+    out = np.zeros(3, np.float32)
+    n = f32(*normal)
+    lib().orc_cosine_direction_frame(_p(n), u1, u2, _p(out))
+    return out
+
+
+def environment_irradiance(environment, position, normal, roughness, count, sequence_base, visibility=0,
+                           probe_spacing=1.0, bias=0.001, geometric_normal=None, view=None, diffuse=(1.0, 1.0, 1.0)):
+    """environmentIrradiance (shaders/environment.slang:242-249) of a constant
+    environment with every visibility query stubbed (0 visible, 1 blocked,
+    2 unsupported): (rgb float32[3], supported)."""
+    out = np.zeros(3, np.float32)
+    env, p, n, dif = f32(*environment), f32(*position), f32(*normal), f32(*diffuse)
+    g = n if geometric_normal is None else f32(*geometric_normal)
+    v = n if view is None else f32(*view)
+    ok = lib().orc_environment_response(None, _p(env), probe_spacing, bias, count, sequence_base, _p(p), _p(n),
+                                        _p(g), _p(v), roughness, _p(dif), visibility, _p(out), None, None)
+    return out, bool(ok)
 
 
 SCREEN_WORDS = 18

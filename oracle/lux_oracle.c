@@ -421,7 +421,14 @@ static void local_triangle(const OrcScene *S, uint32_t triangle, U4 header, floa
  * Traversal (shaders/traversal.slang)
  * ==================================================================== */
 
-/* boxRayInterval, shaders/traversal.slang:349-369. */
+/* boxRayInterval, shaders/traversal.slang:349-369, with the slab entry
+ * padded down by 7.2e-7 relative like the GPU's child tests.  The reference
+ * pads only the exit, so once a surface is found the box of another surface
+ * within one rounding of it can be culled, and which of the two a query
+ * returns depends on the order boxes are visited in (binary here, four-wide
+ * on the GPU); with both ends padded every box holding a triangle at or
+ * before the current distance is visited and the closest hit is the
+ * smallest (distance, instance, triangle) over all triangles. */
 static int box_interval(const float o[3], const float d[3], const Node *n, float limit, float *entry,
                         float *exit) {
     float near_t = 0.0f, far_t = limit;
@@ -440,6 +447,7 @@ static int box_interval(const float o[3], const float d[3], const Node *n, float
             far_t = fminf(far_t, axis_exit + fabsf(axis_exit) * 3.5762791e-7f);
         }
     }
+    near_t = near_t - fabsf(near_t) * 7.2e-7f;
     *entry = near_t;
     *exit = far_t;
     return near_t <= far_t;
@@ -1276,6 +1284,91 @@ static int emissive_response(const OrcScene *S, const LuxSettings *st, const flo
     return 1;
 }
 
+/* transportRandom, shaders/common.slang:292-295. */
+float orc_transport_random(uint32_t seed, uint32_t lane) {
+    uint32_t bits = orc_transport_hash(seed + 0x9e3779b9u * (lane + 1u));
+    return ((float)(bits >> 8) + 0.5f) * (1.0f / 16777216.0f);
+}
+
+/* cosineDirection, shaders/common.slang:407-412: tangent
+ * normalize(cross(|n.y| < 0.99 ? +y : +x, n)), bitangent cross(n, tangent),
+ * radius sqrt(u1) at u2 turns (cosine and sine as orc_sincos_turns), height
+ * sqrt(1 - u1). */
+void orc_cosine_direction_frame(const float n[3], float u1, float u2, float out[3]) {
+    float axis[3] = {0.0f, 1.0f, 0.0f};
+    if (!(fabsf(n[1]) < 0.99f)) {
+        axis[0] = 1.0f;
+        axis[1] = 0.0f;
+    }
+    float t[3], b[3];
+    cross3(axis, n, t);
+    float tl = sqrtf(dot3(t, t));
+    for (int k = 0; k < 3; ++k) t[k] = t[k] / tl;
+    cross3(n, t, b);
+    float c, s;
+    orc_sincos_turns(u2, &c, &s);
+    float r = sqrtf(u1), h = sqrtf(1.0f - u1);
+    float rc = r * c, rs = r * s;
+    for (int k = 0; k < 3; ++k) out[k] = (t[k] * rc + b[k] * rs) + n[k] * h;
+}
+
+/* environmentResponseTracked (shaders/environment.slang:154-230) for a
+ * constant environment: `count` cosine proposals (no alias samples without
+ * an environment map: pdf = 0 x 1/(4 pi) + 1 x cos/pi = cos/pi), sample
+ * seed transportHash(seed ^ transportHash(sample + sequence_base x count +
+ * 0x85ebca6b)) with seed = hashKey(floor(position / (0.05 probe spacings)),
+ * w 37; 2^24); each sample above both normals traces a visibility query from
+ * rayOffset(position, gnormal, bias) to 1e20 and adds environment x
+ * (response x cos / pdf), response = diffuse x disneyDiffuseMultiplier / pi
+ * (diffuse = 1 for environmentIrradiance).  `visibility` (negative: trace
+ * the scene) stubs the query: 0 visible, 1 blocked, 2 unsupported.  Returns 0
+ * when a query is unsupported (out = 0). */
+int orc_environment_response(const OrcScene *S, const float environment[3], float probe_spacing, float bias,
+                             uint32_t count, uint32_t sequence_base, const float position[3], const float normal[3],
+                             const float gnormal[3], const float view[3], float roughness, const float diffuse[3],
+                             int visibility, float out[3], uint64_t *shadow_rays, OrcCounters *cn) {
+    out[0] = out[1] = out[2] = 0.0f;
+    if (count == 0u || !(environment[0] > 0.0f || environment[1] > 0.0f || environment[2] > 0.0f)) return 1;
+    float cell = probe_spacing * 0.05f;
+    int32_t k[4] = {(int32_t)floorf(position[0] / cell), (int32_t)floorf(position[1] / cell),
+                    (int32_t)floorf(position[2] / cell), 37};
+    uint32_t seed = orc_hash_key(k, 16777216u);
+    float origin[3];
+    orc_ray_offset(position, gnormal, bias, origin);
+    float sum[3] = {0, 0, 0};
+    for (uint32_t sample = 0; sample < count; ++sample) {
+        uint32_t sequence = sample + sequence_base * count;
+        uint32_t sample_seed = orc_transport_hash(seed ^ orc_transport_hash(sequence + 0x85ebca6bu));
+        float d[3];
+        orc_cosine_direction_frame(normal, orc_transport_random(sample_seed, 0u), orc_transport_random(sample_seed, 1u),
+                                   d);
+        float cosine = fmaxf(0.0f, dot3(normal, d));
+        if (cosine <= 0.0f || dot3(gnormal, d) <= 0.0f) continue;
+        float pdf = cosine / PI_F;
+        if (!(pdf > 0.0f) || !isfinite(pdf)) continue;
+        int blocked = 0, supported = 1;
+        if (shadow_rays) (*shadow_rays)++;
+        if (visibility < 0)
+            blocked = orc_trace_occluded(S, origin, d, 1e20f, &supported, cn);
+        else {
+            blocked = visibility == 1;
+            supported = visibility != 2;
+        }
+        if (!supported) {
+            out[0] = out[1] = out[2] = 0.0f;
+            return 0;
+        }
+        if (blocked) continue;
+        float factor = disney_multiplier(normal, d, view, roughness) / PI_F;
+        for (int c = 0; c < 3; ++c) {
+            float response = diffuse[c] * factor;
+            sum[c] = sum[c] + environment[c] * ((response * cosine) / pdf);
+        }
+    }
+    for (int c = 0; c < 3; ++c) out[c] = sum[c] / (float)count;
+    return 1;
+}
+
 /* conventionalLightResponseTracked (shaders/cascades.slang:136-176): the
  * visible contributions of the conventional lights (point, spot: range fade
  * (1 - (d/range)^4)^2 / d^2 with (d/range)^4 as (x^2)^2, spot cone squared;
@@ -1335,8 +1428,8 @@ typedef struct {
 static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3]);
 
 /* outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, with
- * every active source group summed into one radiance (no environment, no
- * conventional lights: the synthetic-scene subset).  With a feedback frame
+ * every active source group summed into one radiance in the order emission,
+ * emissive next-event estimate, constant environment, conventional lights.  With a feedback frame
  * the secondary cache's irradiance times the diffuse colour is added last
  * (secondaryFeedback, shaders/world_resolve.slang:204-279).  `rec` receives
  * the surface a multi-bounce secondary receiver takes from this hit:
@@ -1408,6 +1501,16 @@ static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bou
                 return 0;
             }
             for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + nee[c];
+            uint32_t count = st->emissive_samples / 2u < 1u ? 1u : st->emissive_samples / 2u;
+            float env[3];
+            if (!orc_environment_response(S, st->environment, st->probe_spacing, st->normal_bias, count,
+                                          st->frame_index ^ 0xE17A0002u, position, normal, flipped, view, roughness,
+                                          diffuse, -1, env, shadow_rays, cn)) {
+                out[0] = out[1] = out[2] = 0.0f;
+                return 0;
+            }
+            if (st->environment[0] > 0.0f || st->environment[1] > 0.0f || st->environment[2] > 0.0f)
+                for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + env[c];
             if (S->conventional) {
                 float conv[3];
                 if (!conventional_response(S, st, position, normal, flipped, view, roughness, diffuse, conv,

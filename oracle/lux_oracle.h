@@ -83,6 +83,19 @@ int orc_outgoing_radiance(const OrcScene *scene, const LuxSettings *settings,
                           const float origin[3], const float direction[3], const LuxHit *hit,
                           float out[3], uint64_t *shadow_rays, OrcCounters *counters);
 
+/* transportRandom and cosineDirection (shaders/common.slang:292-295,
+ * 407-412), and the constant-environment estimator of
+ * environmentResponseTracked (shaders/environment.slang:154-230): count
+ * samples of sequence base `sequence_base`; `visibility` negative traces the
+ * scene, 0/1/2 stub every query as visible/blocked/unsupported (scene may
+ * then be NULL).  Returns supported. */
+float orc_transport_random(uint32_t seed, uint32_t lane);
+void orc_cosine_direction_frame(const float n[3], float u1, float u2, float out[3]);
+int orc_environment_response(const OrcScene *scene, const float environment[3], float probe_spacing, float bias,
+                             uint32_t count, uint32_t sequence_base, const float position[3], const float normal[3],
+                             const float gnormal[3], const float view[3], float roughness, const float diffuse[3],
+                             int visibility, float out[3], uint64_t *shadow_rays, OrcCounters *counters);
+
 /* FP64 reference irradiance (lux_reference_irradiance restated; `round` =
  * lux_reference_round_samples(count, spp)); out double4[count]. */
 void orc_reference_sample(uint32_t p, uint32_t s, uint32_t seed, float *u1, float *u2);

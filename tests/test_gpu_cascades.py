@@ -341,3 +341,20 @@ def test_split_frame_with_conventional_lights_matches_oracle():
     ofr = oracle.OracleFrame(oracle.OracleScene.from_packed(scene_packed), settings.to_c(), pos, nrm)
     compare_levels(settings, [view.read_level(l) for l in range(4)], ofr, exact=False)
     assert st.shadow_rays == ofr.stats().shadow_rays
+
+
+def test_split_frame_with_environment_matches_oracle():
+    """A constant sky: every hit adds cosine-proposal environment samples
+    (visibility to 1e20) after its emissive estimate; the frame's levels and
+    shadow-ray count follow the oracle."""
+    settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                   emissive_samples=8, frame_index=4, environment=(1.5, 1.0, 0.5)).sanitized()
+    pos, nrm = cornell_floor_receivers()
+    ctx, scene, view, st, levels, probes = run_frame("cornell", settings, pos, nrm)
+    ofr = oracle_frame("cornell", settings, pos, nrm)
+    compare_levels(settings, levels, ofr, exact=False)
+    assert st.shadow_rays == ofr.stats().shadow_rays
+    plain = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
+                                emissive_samples=8, frame_index=4).sanitized()
+    dark = oracle_frame("cornell", plain, pos, nrm)
+    assert ofr.stats().shadow_rays > dark.stats().shadow_rays

@@ -24,7 +24,8 @@ def random_rays(n, lo, hi, seed):
 
 
 def oracle_radiance(name, settings, rays):
-    osc = oracle.OracleScene.from_packed(packed(name))
+    """name: a built-in scene name or a PackedScene."""
+    osc = oracle.OracleScene.from_packed(packed(name) if isinstance(name, str) else name)
     s = settings.to_c()
     out = np.zeros((len(rays), 4), np.float32)
     hit = np.zeros(1, dtype=bp.HIT_DTYPE)
@@ -101,3 +102,44 @@ def test_interval_radiance_with_conventional_lights_bit_exact(samples):
     # The lights add light: brighter than the emitter-only scene on average.
     plain = oracle_radiance("cornell", settings, rays)
     assert gpu[:, :3].sum() > plain[:, :3].sum() * 1.05
+
+
+@pytest.mark.parametrize("lights,samples", [(False, 8), (True, 8), (False, 2)])
+def test_interval_radiance_with_environment_bit_exact(lights, samples):
+    """environmentResponseTracked with a constant sky: max(1, samples / 2)
+    cosine proposals per hit, each a visibility query to 1e20 through the
+    Cornell box's open front, averaged and added after the emissive estimate
+    (and before the conventional lights)."""
+    settings = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=samples, frame_index=7,
+                                   environment=(4.0, 2.0, 1.0)).sanitized()
+    rays = random_rays(4096, (-0.95, 0.05, -0.95), (0.95, 1.95, 0.95), seed=21 + samples)
+    scene_packed = lit_cornell() if lights else packed("cornell")
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, scene_packed)
+    d_rays = to_device(rays)
+    d_out = empty_device(len(rays) * 16)
+    bp.interval_radiance(ctx, scene, settings, d_rays.data_ptr(), len(rays), d_out.data_ptr())
+    ctx.synchronize()
+    gpu = from_device(d_out, np.float32, (len(rays), 4))
+    cpu = oracle_radiance(scene_packed, settings, rays)
+    np.testing.assert_array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+    from dataclasses import replace
+    dark = oracle_radiance(scene_packed, replace(settings, environment=(0.0, 0.0, 0.0)), rays)
+    assert gpu[:, :3].sum() > dark[:, :3].sum() * 1.05  # sky light enters through the open front
+    assert gpu[:, 0].sum() > gpu[:, 2].sum()  # with the sky's hue
+
+
+def test_environment_next_event_slots_are_checked():
+    """Emissive and environment samples share a hit's 16 next-event slots:
+    32 emissive samples (16 per group) with a sky do not fit."""
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    rays = random_rays(32, (-0.5, 0.5, -0.5), (0.5, 1.5, 0.5), seed=1)
+    d_rays = to_device(rays)
+    d_out = empty_device(len(rays) * 16)
+    ok = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=16, environment=(1.0, 1.0, 1.0)).sanitized()
+    bp.interval_radiance(ctx, scene, ok, d_rays.data_ptr(), len(rays), d_out.data_ptr())
+    too_many = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=32, environment=(1.0, 1.0, 1.0)).sanitized()
+    with pytest.raises(bp.LuxError):
+        bp.interval_radiance(ctx, scene, too_many, d_rays.data_ptr(), len(rays), d_out.data_ptr())
+    ctx.synchronize()
