@@ -91,6 +91,7 @@ class RadianceCascades:
     split_transmittance_blend: float = 0.98
     history_frames: int = 24
     multi_bounce: bool = False
+    cached_hit_sky: bool = False
 
     @staticmethod
     def low_end() -> "RadianceCascades":
@@ -121,6 +122,7 @@ class RadianceCascades:
         s.transmittance_blend = self.split_transmittance_blend
         s.history_frames = _u32(self.history_frames)
         s.multi_bounce = 1 if self.multi_bounce else 0
+        s.cached_hit_sky = 1 if self.cached_hit_sky else 0
         return s
 
     @staticmethod
@@ -133,7 +135,8 @@ class RadianceCascades:
             base_rows=int(s.base_rows), interval_ratio=s.interval_ratio, interval_rule=int(s.interval_rule),
             layout=int(s.layout), rays_per_receiver=int(s.rays_per_receiver), frame_index=int(s.frame_index),
             temporal_blend=s.temporal_blend, split_transmittance_blend=s.transmittance_blend,
-            history_frames=int(s.history_frames), multi_bounce=bool(s.multi_bounce))
+            history_frames=int(s.history_frames), multi_bounce=bool(s.multi_bounce),
+            cached_hit_sky=bool(s.cached_hit_sky))
 
     def sanitized(self) -> "RadianceCascades":
         """RadianceCascades::sanitized() (src/lib.rs:731-759), evaluated by liblux."""
@@ -584,7 +587,8 @@ class SplitView:
         sec.ctx = self.ctx
         sec.handle = handle
         sec.desc = self.desc
-        sec.settings = replace(self.settings, multi_bounce=False, probe_spacing=self.settings.probe_spacing * 4.0,
+        sec.settings = replace(self.settings, multi_bounce=False, cached_hit_sky=False,
+                               probe_spacing=self.settings.probe_spacing * 4.0,
                                interval_length=self.settings.interval_length * 4.0) if self.settings else None
         sec._owned = False
         sec._owner = self  # keeps the owning view alive

@@ -65,6 +65,7 @@ class LuxSettings(C.Structure):
         ("layout", C.c_uint32), ("rays_per_receiver", C.c_uint32), ("frame_index", C.c_uint32),
         ("resolve_scale", C.c_uint32), ("temporal_blend", C.c_float), ("transmittance_blend", C.c_float),
         ("history_frames", C.c_uint32), ("multi_bounce", C.c_uint32),
+        ("cached_hit_sky", C.c_uint32),
     ]
 
 

@@ -138,6 +138,7 @@ extern "C" void lux_settings_sanitize(LuxSettings *s) {
     s->transmittance_blend = finite_clamp(s->transmittance_blend, 0.98f, 0.0f, 0.999f);
     s->history_frames = s->history_frames > 64u ? 64u : s->history_frames;
     s->multi_bounce = s->multi_bounce ? 1u : 0u;
+    s->cached_hit_sky = s->cached_hit_sky && s->multi_bounce ? 1u : 0u;  // ignored without multi_bounce
 }
 
 // splitIntervalEnd, shaders/split.slang:224-227, generalised to a ratio and

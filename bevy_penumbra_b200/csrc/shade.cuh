@@ -41,6 +41,8 @@ struct ShadeParams {
     uint32_t feedback;       // 1: add diffuse x the secondary cache's irradiance at the hit
     Feedback fb;
     f3 environment;          // constant environment radiance (black: no environment samples)
+    uint32_t cached_sky;     // cachedHitSky: escapes of the secondary cache carry the environment, and hits
+                             // the feedback probes cover take no environment samples
 };
 
 // environmentResponseTracked returns early for a black constant environment.
@@ -179,7 +181,8 @@ __device__ __forceinline__ float4 probe_irradiance(const float4 *__restrict__ ta
 // previous frame's secondary probe of the cell holding `position`, looked up
 // with the shading normal; resolveLodSource with a zero LOD blend gives
 // (rgb * coverage) / coverage, and zero without coverage.
-__device__ __forceinline__ f3 feedback_irradiance(const Feedback &fb, f3 position, f3 normal) {
+__device__ __forceinline__ f3 feedback_irradiance(const Feedback &fb, f3 position, f3 normal, float &coverage) {
+    coverage = 0.0f;
     const float s = fb.spacing;
     int32_t x = (int32_t)floorf(position.x / s), y = (int32_t)floorf(position.y / s), z = (int32_t)floorf(position.z / s);
     if (!finite3(position) || !cell_in_range(x, y, z)) return f3{0.0f, 0.0f, 0.0f};
@@ -192,6 +195,7 @@ __device__ __forceinline__ f3 feedback_irradiance(const Feedback &fb, f3 positio
             if (id == kEmpty) break;
             float4 e = probe_irradiance(fb.tables + (size_t)id * 36, normal);
             if (!(e.w > 0.0f)) break;
+            coverage = e.w;
             return f3{(e.x * e.w) / e.w, (e.y * e.w) / e.w, (e.z * e.w) / e.w};
         }
         if (k == kEmptyCell) break;
@@ -409,16 +413,23 @@ __device__ void environment_queries(const ShadeParams &P, f3 position, f3 normal
 // multi-bounce term (diffuse x secondary-cache irradiance) to `extra`, the
 // surface a secondary receiver would take to `rec`, and emits the next-event
 // queries; returns false when the query is unsupported (no deposit).
-// `count` = 0 when no next-event estimate applies.
+// `count` = 0 when no next-event estimate applies; `sky` is set when the
+// hit takes environment samples (slots count .. 2 count - 1).
 template <typename Emit>
 __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 origin, f3 direction, const Hit &hit,
-                                f3 &base, f3 &extra, SurfaceRecord &rec, uint32_t &count, Emit &&emit) {
+                                f3 &base, f3 &extra, SurfaceRecord &rec, uint32_t &count, bool &sky, Emit &&emit) {
     base = f3{0.0f, 0.0f, 0.0f};
     extra = f3{0.0f, 0.0f, 0.0f};
     rec.valid = false;
     count = 0;
+    sky = false;
     if ((hit.errors & kQueryUnsupported) != 0u) return false;
-    if (hit.tri == kEmpty) return true;
+    if (hit.tri == kEmpty) {
+        // outgoingEnvironmentEscape (shaders/environment.slang:145-152): the
+        // secondary cache's escapes carry the environment with cached hit sky.
+        if (P.skip_emission && P.cached_sky) base = P.environment;
+        return true;
+    }
     float b0 = (1.0f - hit.b1) - hit.b2;
     Surface sf = surface_at(S, P, hit.inst, hit.tri, b0, hit.b1, hit.b2);
     if (!P.skip_emission) base = sf.emission;
@@ -464,14 +475,17 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
     rec.position = position;
     rec.normal = flipped;
     rec.valid = finite3(position) && finite3(flipped) && finite3(normal) && dot(flipped, flipped) > 0.01f;
+    float coverage = 0.0f;
     if (P.feedback) {
-        f3 e = feedback_irradiance(P.fb, position, normal);
+        f3 e = feedback_irradiance(P.fb, position, normal, coverage);
         extra = f3{e.x * diffuse.x, e.y * diffuse.y, e.z * diffuse.z};
     }
+    // skyFromCache (shaders/cascades.slang:242): a covered hit takes its sky
+    // light from the secondary cache's probe instead of environment samples.
+    sky = environment_on(P) && !(P.cached_sky && coverage > 0.0f);
     emissive_queries(S, P, position, normal, flipped, view, roughness, diffuse, count, emit);
-    environment_queries(P, position, normal, flipped, view, roughness, diffuse, count, count, emit);
-    conventional_queries(S, P, position, normal, flipped, view, roughness, diffuse,
-                         environment_on(P) ? 2u * count : count, emit);
+    if (sky) environment_queries(P, position, normal, flipped, view, roughness, diffuse, count, count, emit);
+    conventional_queries(S, P, position, normal, flipped, view, roughness, diffuse, sky ? 2u * count : count, emit);
     return true;
 }
 
@@ -480,7 +494,8 @@ __device__ bool outgoing_record(const SceneView &S, const ShadeParams &P, f3 ori
                                 f3 &base, uint32_t &count, Emit &&emit) {
     f3 extra;
     SurfaceRecord rec;
-    return outgoing_record(S, P, origin, direction, hit, base, extra, rec, count, emit);
+    bool sky;
+    return outgoing_record(S, P, origin, direction, hit, base, extra, rec, count, sky, emit);
 }
 
 // clampOutgoingTransportRadiance, shaders/cascades.slang:179-188, after the

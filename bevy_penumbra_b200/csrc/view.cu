@@ -581,14 +581,14 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     lux::NeeQuery q[lux::kMaxNeeSamples];
     uint32_t slot_of[lux::kMaxNeeSamples];
     uint32_t nq = 0, count = 0;
-    bool supported = false;
+    bool supported = false, sky = false;
     f3 base{0.0f, 0.0f, 0.0f}, extra;
     if (ray < rays) {
         f3 o, d;
         lux::Hit hit;
         lux::SurfaceRecord rec;
         load_ray(V, ray, o, d, hit);
-        supported = lux::outgoing_record(S, P, o, d, hit, base, extra, rec, count,
+        supported = lux::outgoing_record(S, P, o, d, hit, base, extra, rec, count, sky,
                                          [&](uint32_t sample, const lux::NeeQuery &query) {
                                              if (nq >= lux::kMaxNeeSamples) return;  // host checks the slot count
                                              q[nq] = query;
@@ -597,7 +597,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
                                          });
         // w: the emissive estimator's divisor | the conventional-light slots << 16
         // | environment samples present << 24.
-        const uint32_t slots = count | (S.conventional_lights << 16) | ((lux::environment_on(P) ? 1u : 0u) << 24);
+        const uint32_t slots = count | (S.conventional_lights << 16) | ((sky ? 1u : 0u) << 24);
         V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? slots : lux::kEmpty));
         if (P.feedback) V.ts.ray_extra[ray] = make_float4(extra.x, extra.y, extra.z, 0.0f);
         // The multi-bounce secondary receiver of receiver i: its ray frame % R.
@@ -621,7 +621,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     uint32_t at = first + prefix - nq;
     if (ray < rays) {
         uint32_t k = 0;
-        const uint32_t slots = count * (lux::environment_on(P) ? 2u : 1u) + S.conventional_lights;
+        const uint32_t slots = count * (sky ? 2u : 1u) + S.conventional_lights;
         for (uint32_t s = 0; s < slots && s < lux::kMaxNeeSamples; ++s) {
             uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
             if (k < nq && slot_of[k] == s) {
@@ -2138,6 +2138,7 @@ struct FrameRole {
     uint32_t skip_emission = 0;  // no first-hit emission (the secondary cache)
     uint32_t record_hits = 0;    // write the receivers' hit surfaces (the primary cache)
     bool feedback = false;       // hit shading reads the secondary snapshot
+    uint32_t cached_sky = 0;     // cachedHitSky (both caches of a multi-bounce frame with cached_hit_sky)
 };
 
 static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSettings *settings, const LuxReceivers *rc,
@@ -2214,6 +2215,7 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     FrameRole primary;
     primary.record_hits = 1;
     primary.feedback = v->fb.valid && !dirty;
+    primary.cached_sky = s.cached_hit_sky;
     cudaMemsetAsync(v->dev.hit_pos, 0, (size_t)rc->count * sizeof(float4), stream);
     st = view_frame(v, scene, settings, rc, primary, v);
     if (st != LUX_OK) return st;
@@ -2230,6 +2232,7 @@ extern "C" lux_status lux_view_trace_merge(LuxView *v, const LuxScene *scene, co
     secondary.sparse = 1;
     secondary.skip_emission = 1;
     secondary.feedback = primary.feedback;
+    secondary.cached_sky = primary.cached_sky;
     st = view_frame(sec, scene, &s2, &hits, secondary, v);
     if (st != LUX_OK) return st;
     feedback_snapshot_kernel<<<ctx->sm_count * 4, 256, 0, stream>>>(sec->dev, sec->dir_capacity, v->fb.keys,
@@ -2291,6 +2294,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
     F.sparse = role.sparse;
     F.record_hits = role.record_hits;
     F.shade.skip_emission = role.skip_emission;
+    F.shade.cached_sky = role.cached_sky;
     if (role.feedback && fb_owner) {
         F.shade.feedback = 1;
         F.shade.fb = lux::Feedback{fb_owner->fb.keys, fb_owner->fb.ids, fb_owner->fb.tables,

@@ -134,6 +134,10 @@ typedef struct LuxSettings {
     uint32_t history_frames;        /* RadianceCascades::history_frames (history.w), 0..=64; 0 disables history */
     uint32_t multi_bounce;          /* RadianceCascades::multi_bounce: 1 adds the secondary cache's diffuse bounce
                                        light at interval-ray hits (Split layout, unbatched frames) */
+    uint32_t cached_hit_sky;        /* RadianceCascades::cached_hit_sky (lightCounts.w, src/render.rs:8495): with
+                                       multi_bounce, the secondary cache's escaped rays carry the environment and
+                                       hits its previous frame covers take their sky light from it instead of
+                                       tracing environment samples (cachedHitSky, shaders/common.slang:71-74) */
 } LuxSettings;
 
 /* Receivers (Split) or the cascade-0 probe set (Dense), device pointers.

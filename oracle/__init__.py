@@ -175,14 +175,16 @@ class OracleFrame:
     def __init__(self, scene: OracleScene, settings_c, pos: np.ndarray, nrm: np.ndarray, threads: int = 0,
                  previous: "OracleFrame | None" = None, dirty=None, max_cells: int = 0xFFFFFFFF,
                  max_entries: int = (1 << 64) - 1, feedback: "OracleFrame | None" = None, sparse: bool = False,
-                 skip_emission: bool = False, record_hits: bool = False, camera=None):
+                 skip_emission: bool = False, record_hits: bool = False, camera=None, cached_sky: bool = False):
         """previous: the frame whose records serve as history; dirty: boxes
         (n, 6) = (lo xyz, hi xyz) whose nearby records take no history;
         max_cells / max_entries: the view capacities that bound the cells
         retained from `previous`.  Multi-bounce: feedback, the secondary frame
         whose cascade-0 probes add bounce light at hits; sparse, receivers
         with position.w == 0 are absent; skip_emission, hits add no emission of
-        their own; record_hits, keep each receiver's hit surface (hits()).
+        their own; record_hits, keep each receiver's hit surface (hits());
+        cached_sky, cachedHitSky (escapes of a skip_emission frame carry the
+        environment, hits the feedback frame covers take no sky samples).
         camera: a LuxCamera (bevy_penumbra_b200.camera_struct) for distance
         LODs, as SplitView.set_camera."""
         self.settings = settings_c
@@ -194,7 +196,8 @@ class OracleFrame:
         self._camera = camera
         self.hit_pos = np.zeros((len(pos), 4), np.float32)
         self.hit_nrm = np.zeros((len(pos), 4), np.float32)
-        flags = (1 if sparse else 0) | (2 if skip_emission else 0) | (4 if record_hits else 0)
+        flags = (1 if sparse else 0) | (2 if skip_emission else 0) | (4 if record_hits else 0) | \
+            (8 if cached_sky else 0)
         self.handle = lib().orc_frame_run_bounce(scene.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos),
                                                  threads or os.cpu_count() or 1,
                                                  previous.handle if previous is not None else None, _p(boxes),

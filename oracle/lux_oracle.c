@@ -1423,9 +1423,11 @@ static int conventional_response(const OrcScene *S, const LuxSettings *st, const
 typedef struct {
     const OrcFrame *feedback;  /* secondary frame whose cascade-0 probes add bounce light (NULL: none) */
     int skip_emission;         /* the secondary cache: no first-hit emission (environmentScale.z) */
+    int cached_sky;            /* cachedHitSky: secondary escapes carry the environment, covered hits skip its samples */
 } Bounce;
 
-static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3]);
+static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3],
+                                float *coverage);
 
 /* outgoingTransportRadianceTracked, shaders/cascades.slang:196-268, with
  * every active source group summed into one radiance in the order emission,
@@ -1440,7 +1442,12 @@ static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bou
     out[0] = out[1] = out[2] = 0.0f;
     if (rec) rec[6] = 0.0f;
     if ((hit->errors & HIT_QUERY_UNSUPPORTED) != 0u) return 0;
-    if (hit->triangle == EMPTY) return 1;
+    if (hit->triangle == EMPTY) {
+        /* outgoingEnvironmentEscape (shaders/environment.slang:145-152). */
+        if (bn && bn->skip_emission && bn->cached_sky)
+            for (int c = 0; c < 3; ++c) out[c] = fmaxf(st->environment[c], 0.0f);
+        return 1;
+    }
     Surface sf;
     surface_at(S, st, hit->instance, hit->triangle, hit->barycentric, &sf);
     float radiance[3] = {sf.emission[0], sf.emission[1], sf.emission[2]};
@@ -1501,15 +1508,21 @@ static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bou
                 return 0;
             }
             for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + nee[c];
+            /* secondaryFeedback before the environment (shaders/cascades.slang:236-242):
+             * with cached hit sky a covered hit takes its sky light from the cache. */
+            float fb_e[3] = {0, 0, 0}, coverage = 0.0f;
+            if (bn && bn->feedback) feedback_irradiance(bn->feedback, position, normal, fb_e, &coverage);
+            int sky_from_cache = bn && bn->cached_sky && coverage > 0.0f;
             uint32_t count = st->emissive_samples / 2u < 1u ? 1u : st->emissive_samples / 2u;
-            float env[3];
-            if (!orc_environment_response(S, st->environment, st->probe_spacing, st->normal_bias, count,
+            float env[3] = {0, 0, 0};
+            if (!sky_from_cache &&
+                !orc_environment_response(S, st->environment, st->probe_spacing, st->normal_bias, count,
                                           st->frame_index ^ 0xE17A0002u, position, normal, flipped, view, roughness,
                                           diffuse, -1, env, shadow_rays, cn)) {
                 out[0] = out[1] = out[2] = 0.0f;
                 return 0;
             }
-            if (st->environment[0] > 0.0f || st->environment[1] > 0.0f || st->environment[2] > 0.0f)
+            if (!sky_from_cache && (st->environment[0] > 0.0f || st->environment[1] > 0.0f || st->environment[2] > 0.0f))
                 for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + env[c];
             if (S->conventional) {
                 float conv[3];
@@ -1520,11 +1533,8 @@ static int outgoing_radiance(const OrcScene *S, const LuxSettings *st, const Bou
                 }
                 for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + conv[c];
             }
-            if (bn && bn->feedback) {
-                float e[3];
-                feedback_irradiance(bn->feedback, position, normal, e);
-                for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + e[c] * diffuse[c];
-            }
+            if (bn && bn->feedback)
+                for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + fb_e[c] * diffuse[c];
         }
     }
     /* clampOutgoingTransportRadiance, shaders/cascades.slang:179-188. */
@@ -2228,8 +2238,10 @@ OrcFrame *orc_frame_run_retain(const OrcScene *S, const LuxSettings *st_in, cons
 /* secondaryFeedback at LOD 0 of the secondary frame: its cascade-0 probe of
  * the cell holding `position`, looked up with the shading normal;
  * resolveLodSource with a zero LOD blend gives (rgb * coverage) / coverage. */
-static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3]) {
+static void feedback_irradiance(const OrcFrame *fb, const float position[3], const float normal[3], float out[3],
+                                float *coverage) {
     out[0] = out[1] = out[2] = 0.0f;
+    *coverage = 0.0f;
     if (!finite3(position)) return;
     float s = orc_spacing(&fb->st, 0);
     int32_t key[4] = {(int32_t)floorf(position[0] / s), (int32_t)floorf(position[1] / s),
@@ -2240,6 +2252,7 @@ static void feedback_irradiance(const OrcFrame *fb, const float position[3], con
     float e[4];
     probe_page(&fb->tables[(size_t)cell * 144], &lk, e);
     if (!(e[3] > 0.0f)) return;
+    *coverage = e[3];
     for (int c = 0; c < 3; ++c) out[c] = (e[c] * e[3]) / e[3];
 }
 
@@ -2249,7 +2262,7 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
                                const OrcFrame *feedback, uint32_t flags, float *hit_pos, float *hit_nrm,
                                const LuxCamera *camera) {
     const int sparse = (flags & ORC_FRAME_SPARSE) != 0u;
-    Bounce bounce = {feedback, (flags & ORC_FRAME_SKIP_EMISSION) != 0u};
+    Bounce bounce = {feedback, (flags & ORC_FRAME_SKIP_EMISSION) != 0u, (flags & ORC_FRAME_CACHED_SKY) != 0u};
     OrcFrame *F = (OrcFrame *)calloc(1, sizeof(OrcFrame));
     F->st = *st_in;
     lod_params(st_in, camera, &F->lod);

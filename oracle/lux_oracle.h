@@ -129,6 +129,10 @@ OrcFrame *orc_frame_run_retain(const OrcScene *scene, const LuxSettings *setting
 #define ORC_FRAME_SPARSE 1u
 #define ORC_FRAME_SKIP_EMISSION 2u
 #define ORC_FRAME_RECORD_HITS 4u
+/* cachedHitSky (RadianceCascades::cached_hit_sky): with ORC_FRAME_SKIP_EMISSION
+ * escaped rays carry the environment; hits the feedback frame covers take no
+ * environment samples. */
+#define ORC_FRAME_CACHED_SKY 8u
 OrcFrame *orc_frame_run_bounce(const OrcScene *scene, const LuxSettings *settings, const float *receiver_position,
                                const float *receiver_normal, uint32_t receiver_count, int threads,
                                const OrcFrame *previous, const float *dirty, uint32_t dirty_count,

@@ -235,17 +235,22 @@ def test_split_retain_matches_oracle():
             assert {tuple(k[:3]) for k in view.read_level(0)[0]} == every
 
 
-def test_multi_bounce_matches_oracle():
+@pytest.mark.parametrize("cached_sky", [False, True])
+def test_multi_bounce_matches_oracle(cached_sky):
     """multi_bounce: each frame the primary cache traces with the previous
     secondary probes' bounce light and records one hit surface per receiver;
     the secondary cache (spacing and intervals x4) traces from those surfaces
     without first-hit emission.  Primary and secondary records follow the
-    oracle chain frame by frame."""
+    oracle chain frame by frame.  With cached_hit_sky (under a sky) the
+    secondary's escapes carry the sky and covered hits skip their sky
+    samples."""
     from dataclasses import replace
 
     def st(frame):
         return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=4,
-                                   emissive_samples=8, frame_index=frame, multi_bounce=True).sanitized()
+                                   emissive_samples=8, frame_index=frame, multi_bounce=True,
+                                   environment=(1.5, 1.0, 0.5) if cached_sky else (0.0, 0.0, 0.0),
+                                   cached_hit_sky=cached_sky).sanitized()
     pos, nrm = cornell_floor_receivers()
     pos[:, 3] = 1.0
     ctx = bp.LuxContext()
@@ -259,12 +264,15 @@ def test_multi_bounce_matches_oracle():
     for frame in range(3):
         s = st(frame)
         s2 = replace(s, probe_spacing=s.probe_spacing * 4.0, interval_length=s.interval_length * 4.0,
-                     multi_bounce=False)
+                     multi_bounce=False, cached_hit_sky=False)
         view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), len(pos))
-        assert view.stats().error_flags == 0
-        p = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prim, feedback=sec, record_hits=True, **caps)
+        stats = view.stats()
+        assert stats.error_flags == 0
+        p = oracle.OracleFrame(oscene, s.to_c(), pos, nrm, previous=prim, feedback=sec, record_hits=True,
+                               cached_sky=cached_sky, **caps)
         q = oracle.OracleFrame(oscene, s2.to_c(), p.hit_pos, p.hit_nrm, previous=sec, feedback=sec, sparse=True,
-                               skip_emission=True, **caps)
+                               skip_emission=True, cached_sky=cached_sky, **caps)
+        assert stats.shadow_rays == p.stats().shadow_rays
         compare_levels(s, [view.read_level(l) for l in range(4)], p, exact=False)
         secondary = view.secondary()
         assert secondary is not None and secondary.stats().error_flags == 0

@@ -218,3 +218,38 @@ def test_oracle_multi_bounce_roles():
     np.testing.assert_array_equal(samples_fed, samples_plain)
     assert np.all(raw_fed[..., :3] >= raw_plain[..., :3] - 1e-7)
     assert np.any(raw_fed[..., :3] > raw_plain[..., :3] + 1e-4)
+
+
+def test_oracle_cached_hit_sky_roles():
+    """cached_hit_sky: the secondary cache's escaped rays carry the sky
+    (outgoingEnvironmentEscape), and hits its previous frame covers take
+    their sky light from its probes instead of environment samples, so they
+    trace fewer visibility queries; without feedback nothing changes."""
+    sky = (2.0, 1.5, 1.0)
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=2,
+                            emissive_samples=4, environment=sky).sanitized()
+    s2 = bp.RadianceCascades(probe_spacing=1.0, interval_length=1.6, levels=4, rays_per_receiver=2,
+                             emissive_samples=4, environment=sky).sanitized()
+    pos, nrm = cornell_receivers(16)
+    pos[:, 3] = 1.0
+    scene = oracle.OracleScene.from_packed(packed("cornell"))
+    dirs = s.direction_count(0)
+    p0 = oracle.OracleFrame(scene, s.to_c(), pos, nrm, record_hits=True)
+    plain = oracle.OracleFrame(scene, s2.to_c(), p0.hit_pos, p0.hit_nrm, sparse=True, skip_emission=True)
+    cached = oracle.OracleFrame(scene, s2.to_c(), p0.hit_pos, p0.hit_nrm, sparse=True, skip_emission=True,
+                                cached_sky=True)
+    # First frame: no feedback, so every hit still samples the sky; escapes now carry it.
+    assert cached.stats().shadow_rays == plain.stats().shadow_rays
+    last = s2.levels - 1  # escapes deposit their radiance in the last level, which owns the tail
+    _, _, raw_c, _ = cached.level(last, s2.direction_count(last))
+    _, _, raw_p, _ = plain.level(last, s2.direction_count(last))
+    assert np.all(raw_c[..., :3] >= raw_p[..., :3] - 1e-7)
+    assert np.any(raw_c[..., :3] > raw_p[..., :3] + 1e-3)  # the open front's escapes
+    # Next frame with the secondary's probes as feedback: covered hits skip the sky samples.
+    fed = oracle.OracleFrame(scene, s.to_c(), pos, nrm, feedback=cached)
+    fed_cached = oracle.OracleFrame(scene, s.to_c(), pos, nrm, feedback=cached, cached_sky=True)
+    assert fed_cached.stats().shadow_rays < fed.stats().shadow_rays
+    _, _, raw_fc, samples_fc = fed_cached.level(0, dirs)
+    _, _, raw_f, samples_f = fed.level(0, dirs)
+    np.testing.assert_array_equal(samples_fc, samples_f)
+    assert np.all(np.isfinite(raw_fc))
