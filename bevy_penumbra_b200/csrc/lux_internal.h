@@ -62,11 +62,11 @@ struct TraceScratch {
     uint4 *ray_h;           // triangle, instance, errors, barycentric 2 bits
     float4 *ray_base;       // hit emission, next-event count (kEmpty: unsupported)
     float4 *ray_extra;      // multi-bounce term of the hit (written when the frame has feedback)
-    uint32_t *slot_query;   // per (ray, sample): queue index or kEmpty
+    uint32_t *query_slot;   // compact query list: the (ray, sample) slot of query i
     float4 *slot_contrib;   // per (ray, sample): contribution if visible
-    float4 *queue_o;        // query origin, limit
-    float4 *queue_d;        // query direction
-    uint8_t *queue_result;  // 0 visible, 1 blocked, 2 unsupported
+    float4 *queue_o;        // per (ray, sample): query origin, limit
+    float4 *queue_d;        // per (ray, sample): query direction, coherence sort key bits
+    uint8_t *queue_result;  // per (ray, sample): 0 visible, 1 blocked, 2 unsupported
     uint32_t *queue_count;
     uint32_t *work_counter; // [2] persistent-warp ray fetch: closest, shadow
 };
@@ -97,7 +97,7 @@ inline unsigned char *carve_trace_scratch(unsigned char *base, uint32_t rays, Tr
     t.ray_d = (float4 *)take(r * 16);
     t.ray_h = (uint4 *)take(r * 16);
     t.ray_base = (float4 *)take(r * 16);
-    t.slot_query = (uint32_t *)take(q * 4);
+    t.query_slot = (uint32_t *)take(q * 4);
     t.slot_contrib = (float4 *)take(q * 16);
     t.queue_o = (float4 *)take(q * 16);
     t.queue_d = (float4 *)take(q * 16);

@@ -578,27 +578,38 @@ __global__ void sort_scatter_kernel(ViewDevice V, const uint32_t *count_ptr, uin
 __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParams &F, const lux::ShadeParams &P,
                                            const SceneView &S, uint32_t ray, uint32_t rays) {
     const uint32_t lane = threadIdx.x & 31u;
-    lux::NeeQuery q[lux::kMaxNeeSamples];
-    uint32_t slot_of[lux::kMaxNeeSamples];
-    uint32_t nq = 0, count = 0;
+    // Queries are written at their slot (ray x 16 + sample) as they are
+    // emitted, so nothing is buffered per lane; the warp then appends the
+    // slots it used to the compact query list with one atomic.
+    uint32_t used = 0, nq = 0, count = 0;
     bool supported = false, sky = false;
     f3 base{0.0f, 0.0f, 0.0f}, extra;
+    const size_t slot0 = (size_t)ray * lux::kMaxNeeSamples;
     if (ray < rays) {
         f3 o, d;
         lux::Hit hit;
         lux::SurfaceRecord rec;
         load_ray(V, ray, o, d, hit);
+        const bool keys = V.sort_keys != nullptr;
         supported = lux::outgoing_record(S, P, o, d, hit, base, extra, rec, count, sky,
-                                         [&](uint32_t sample, const lux::NeeQuery &query) {
-                                             if (nq >= lux::kMaxNeeSamples) return;  // host checks the slot count
-                                             q[nq] = query;
-                                             slot_of[nq] = sample;
+                                         [&](uint32_t sample, const lux::NeeQuery &q) {
+                                             if (sample >= lux::kMaxNeeSamples) return;  // host checks the slot count
+                                             const size_t slot = slot0 + sample;
+                                             // w of the direction: the query's coherence sort key.
+                                             uint32_t key = keys ? (q.light & 63u) * kSortCells + cell16(S, q.origin)
+                                                                 : 0u;
+                                             V.ts.queue_o[slot] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.limit);
+                                             V.ts.queue_d[slot] = make_float4(q.direction.x, q.direction.y,
+                                                                              q.direction.z, lux::as_float(key));
+                                             V.ts.slot_contrib[slot] = make_float4(q.contribution.x, q.contribution.y,
+                                                                                   q.contribution.z, (float)q.group);
+                                             used |= 1u << sample;
                                              ++nq;
                                          });
-        // w: the emissive estimator's divisor | the conventional-light slots << 16
-        // | environment samples present << 24.
-        const uint32_t slots = count | (S.conventional_lights << 16) | ((sky ? 1u : 0u) << 24);
-        V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? slots : lux::kEmpty));
+        // w: the emissive estimator's divisor | conventional-light slots << 5
+        // | environment samples present << 9 | the used slots << 16.
+        const uint32_t packed = count | (S.conventional_lights << 5) | ((sky ? 1u : 0u) << 9) | (used << 16);
+        V.ts.ray_base[ray] = make_float4(base.x, base.y, base.z, lux::as_float(supported ? packed : lux::kEmpty));
         if (P.feedback) V.ts.ray_extra[ray] = make_float4(extra.x, extra.y, extra.z, 0.0f);
         // The multi-bounce secondary receiver of receiver i: its ray frame % R.
         if (F.record_hits && rec.valid && ray % F.rays_per_receiver == P.frame % F.rays_per_receiver) {
@@ -607,7 +618,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
             V.hit_nrm[i] = make_float4(rec.normal.x, rec.normal.y, rec.normal.z, 0.0f);
         }
     }
-    // Warp-aggregated append of this warp's queries.
+    // Warp-aggregated append of this warp's used slots.
     uint32_t prefix = nq;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -618,28 +629,14 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     uint32_t first = 0;
     if (lane == 31 && total) first = atomicAdd(V.ts.queue_count, total);
     first = __shfl_sync(0xffffffffu, first, 31);
-    uint32_t at = first + prefix - nq;
-    if (ray < rays) {
-        uint32_t k = 0;
-        const uint32_t slots = count * (sky ? 2u : 1u) + S.conventional_lights;
-        for (uint32_t s = 0; s < slots && s < lux::kMaxNeeSamples; ++s) {
-            uint32_t slot = (uint32_t)((size_t)ray * lux::kMaxNeeSamples + s);
-            if (k < nq && slot_of[k] == s) {
-                uint32_t qi = at + k;
-                if (qi < F.queue_capacity) {
-                    V.ts.queue_o[qi] = make_float4(q[k].origin.x, q[k].origin.y, q[k].origin.z, q[k].limit);
-                    V.ts.queue_d[qi] = make_float4(q[k].direction.x, q[k].direction.y, q[k].direction.z, 0.0f);
-                    V.ts.slot_query[slot] = qi;
-                    V.ts.slot_contrib[slot] = make_float4(q[k].contribution.x, q[k].contribution.y,
-                                                          q[k].contribution.z, (float)q[k].group);
-                    if (V.sort_keys) V.sort_keys[qi] = (q[k].light & 63u) * kSortCells + cell16(S, q[k].origin);
-                } else {
-                    V.ts.slot_query[slot] = lux::kEmpty - 1u;  // queue overflow: unsupported
-                }
-                ++k;
-            } else {
-                V.ts.slot_query[slot] = lux::kEmpty;
-            }
+    uint32_t qi = first + prefix - nq;
+    for (uint32_t m = used; m; m &= m - 1u, ++qi) {
+        const size_t slot = slot0 + (uint32_t)(__ffs(m) - 1);
+        if (qi < F.queue_capacity) {
+            V.ts.query_slot[qi] = (uint32_t)slot;
+            if (V.sort_keys) V.sort_keys[qi] = lux::as_uint(V.ts.queue_d[slot].w);
+        } else {
+            V.ts.queue_result[slot] = 2;  // list overflow: unsupported
         }
     }
 }
@@ -662,7 +659,7 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
     lux::trace_persistent<true>(
         S, &V.ts.work_counter[1], n,
         [&](uint32_t i, f3 &o, f3 &d, float &tmin, float &limit) {
-            uint32_t qi = V.query_order ? V.query_order[i] : i;
+            uint32_t qi = V.ts.query_slot[V.query_order ? V.query_order[i] : i];
             float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
             o = f3{a.x, a.y, a.z};
             d = f3{b.x, b.y, b.z};
@@ -670,7 +667,7 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
             limit = a.w;
         },
         [&](uint32_t i, const lux::Hit &sh) {
-            uint32_t qi = V.query_order ? V.query_order[i] : i;
+            uint32_t qi = V.ts.query_slot[V.query_order ? V.query_order[i] : i];
             V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
             st[kStatShadow] += 1;
         },
@@ -687,7 +684,7 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
 template <int kDepth = lux::kStack>
 __device__ __forceinline__ void shadow_query(const ViewDevice &V, const SceneView &S, uint32_t i,
                                              lux::TraceCounters &cn) {
-    uint32_t qi = V.query_order ? V.query_order[i] : i;
+    uint32_t qi = V.ts.query_slot[V.query_order ? V.query_order[i] : i];
     float4 a = V.ts.queue_o[qi], b = V.ts.queue_d[qi];
     lux::Hit sh;
     lux::trace<true, kDepth>(S, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn);
@@ -724,15 +721,14 @@ __device__ __forceinline__ bool ray_radiance(const ViewDevice &V, uint32_t ray, 
     if (packed == lux::kEmpty) return false;
     // The emissive samples (averaged), the environment samples (averaged over
     // the same count) then the conventional lights (summed).
-    const uint32_t count = packed & 0xffffu, conventional = (packed >> 16) & 0xffu;
-    const uint32_t environment = (packed >> 24) != 0u ? count : 0u;
+    const uint32_t count = packed & 31u, conventional = (packed >> 5) & 15u;
+    const uint32_t environment = ((packed >> 9) & 1u) != 0u ? count : 0u;
+    const uint32_t used = packed >> 16;
     f3 sum{0.0f, 0.0f, 0.0f}, esum{0.0f, 0.0f, 0.0f}, csum{0.0f, 0.0f, 0.0f};
     for (uint32_t s = 0; s < count + environment + conventional && s < lux::kMaxNeeSamples; ++s) {
+        if (!(used & (1u << s))) continue;
         size_t slot = (size_t)ray * lux::kMaxNeeSamples + s;
-        uint32_t qi = V.ts.slot_query[slot];
-        if (qi == lux::kEmpty) continue;
-        if (qi == lux::kEmpty - 1u) return false;
-        uint8_t r = V.ts.queue_result[qi];
+        uint8_t r = V.ts.queue_result[slot];
         if (r == 2) return false;
         if (r == 1) continue;
         float4 c = V.ts.slot_contrib[slot];
@@ -1843,7 +1839,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.ts.ray_h, (size_t)d.max_rays * sizeof(uint4)},
         {(void **)&D.ts.ray_base, (size_t)d.max_rays * sizeof(float4)},
         {(void **)&D.ts.ray_extra, (size_t)d.max_rays * sizeof(float4)},
-        {(void **)&D.ts.slot_query, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
+        {(void **)&D.ts.query_slot, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
         {(void **)&D.ts.slot_contrib, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
         {(void **)&D.ts.queue_o, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
         {(void **)&D.ts.queue_d, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(float4)},
@@ -1896,7 +1892,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
                     D.retain_hist, D.retain_limit, D.tables, D.error_flags, D.stats,
                     v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
                     v->hist.mass, v->hist.cell_last, v->hist.cell_keys,
-                    D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.ray_extra, D.ts.slot_query, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
+                    D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.ray_extra, D.ts.query_slot, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
                     D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     if (v->stage_stream) cudaStreamSynchronize(v->stage_stream);
