@@ -257,25 +257,58 @@ __global__ void __launch_bounds__(256) temporal_kernel(ScreenParams P, Input in,
 // denoise, shaders/cascades.slang:618-690: one a-trous pass at stride P.step.
 // `src` / `src_mask` are the previous stage's irradiance and support masks;
 // moments, identities and normals are the temporal output's.
+//
+// Every tap of a pixel lies on the pixel's lattice x = px + step u,
+// y = py + step v, so a block takes 16 x 16 pixels of one lattice phase
+// (px, py) and stages the lattice points they read (20 x 20 with the two-point
+// halo) in shared memory once; each pixel then evaluates its taps in the same
+// order and arithmetic as a direct read would.  Points outside the image are
+// staged with zero irradiance support (w = 0), which skips them as the bounds
+// test does.
+constexpr int kDenoiseTile = 16, kDenoiseSpan = kDenoiseTile + 4;
 __global__ void __launch_bounds__(256) denoise_kernel(ScreenParams P, Input in, History T, const float4 *src,
                                                       const float *src_mask, float4 *dst, float *dst_mask) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
+    __shared__ float4 s_value[kDenoiseSpan * kDenoiseSpan], s_meta[kDenoiseSpan * kDenoiseSpan];
+    __shared__ float4 s_nrm[kDenoiseSpan * kDenoiseSpan], s_pos[kDenoiseSpan * kDenoiseSpan];
+    __shared__ uint2 s_id[kDenoiseSpan * kDenoiseSpan];
+    __shared__ float s_mask[kDenoiseSpan * kDenoiseSpan];
+    const int step = (int)P.step;
+    const int px = (int)blockIdx.x % step, py = (int)blockIdx.y % step;  // lattice phase
+    const int u0 = ((int)blockIdx.x / step) * kDenoiseTile, v0 = ((int)blockIdx.y / step) * kDenoiseTile;
+    const int tid = threadIdx.y * kDenoiseTile + threadIdx.x;
+    for (int k = tid; k < kDenoiseSpan * kDenoiseSpan; k += kDenoiseTile * kDenoiseTile) {
+        int qx = px + step * (u0 - 2 + k % kDenoiseSpan), qy = py + step * (v0 - 2 + k / kDenoiseSpan);
+        if (qx < 0 || qy < 0 || qx >= (int)P.width || qy >= (int)P.height) {
+            s_value[k] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
+        size_t q = (size_t)qy * P.width + qx;
+        s_value[k] = src[q];
+        s_meta[k] = T.meta[q];
+        s_nrm[k] = T.nrm[q];
+        s_pos[k] = in.pos[q];
+        s_id[k] = T.id[q];
+        s_mask[k] = src_mask[q];
+    }
+    __syncthreads();
+    const int x = px + step * (u0 + (int)threadIdx.x), y = py + step * (v0 + (int)threadIdx.y);
     if (x >= (int)P.width || y >= (int)P.height) return;
     const size_t p = (size_t)y * P.width + x;
-    float4 center = src[p];
+    const int c = ((int)threadIdx.y + 2) * kDenoiseSpan + ((int)threadIdx.x + 2);
+    float4 center = s_value[c];
     bool has_light = center.w > 0.0f && isfinite(center.w) && finite3(center);
-    float4 position = in.pos[p];
+    float4 position = s_pos[c];
     float depth = has_light ? center.w : position.w;
     if (depth <= 0.0f || !isfinite(depth)) {
         dst[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         dst_mask[p] = 0.0f;
         return;
     }
-    const float4 tm = T.meta[p];
+    const float4 tm = s_meta[c];
     const bool surface = tm.w > 0.0f;
-    const uint2 id = T.id[p];
-    const float4 gn = T.nrm[p];
-    const uint32_t center_mask = (uint32_t)src_mask[p];
+    const uint2 id = s_id[c];
+    const float4 gn = s_nrm[c];
+    const uint32_t center_mask = (uint32_t)s_mask[c];
     const bool center_supported = tm.x > 0.0f;
     const float variance = fmaxf(tm.y, 0.0f);
     const float cl = luminance(make_float3(center.x, center.y, center.z));
@@ -284,25 +317,23 @@ __global__ void __launch_bounds__(256) denoise_kernel(ScreenParams P, Input in, 
     for (int dy = -2; dy <= 2; ++dy) {
         int xr = abs(dy) == 2 ? 1 : 2;
         for (int dx = -xr; dx <= xr; ++dx) {
-            int qx = x + dx * (int)P.step, qy = y + dy * (int)P.step;
-            if (qx < 0 || qy < 0 || qx >= (int)P.width || qy >= (int)P.height) continue;
-            size_t q = (size_t)qy * P.width + qx;
-            float4 value = src[q];
+            const int q = c + dy * kDenoiseSpan + dx;
+            float4 value = s_value[q];
             if (value.w <= 0.0f) continue;
-            float4 om = T.meta[q];
+            float4 om = s_meta[q];
             if (om.x <= 0.0f) continue;
-            float4 on = T.nrm[q];
-            if (!compatible(surface, id, gn, om.w > 0.0f, T.id[q], on)) continue;
-            uint32_t other_mask = (uint32_t)src_mask[q];
+            float4 on = s_nrm[q];
+            if (!compatible(surface, id, gn, om.w > 0.0f, s_id[q], on)) continue;
+            uint32_t other_mask = (uint32_t)s_mask[q];
             if (center_mask != 0u && other_mask != center_mask) continue;
             if (center_mask == 0u && other_mask == 0u) continue;
-            float4 op = in.pos[q];
+            float4 op = s_pos[q];
             if (dot3(gn, on) < 0.95f) continue;
             float4 delta = make_float4(op.x - position.x, op.y - position.y, op.z - position.z, 0.0f);
             float pd = plane_distance(delta, gn, on);
             if (pd > P.tolerance) continue;
-            float c = fmaxf(0.0f, dot3(gn, on));
-            float c2 = c * c, c4 = c2 * c2, c8 = c4 * c4, c16 = c8 * c8, c32 = c16 * c16;
+            float cs = fmaxf(0.0f, dot3(gn, on));
+            float c2 = cs * cs, c4 = c2 * c2, c8 = c4 * c4, c16 = c8 * c8, c32 = c16 * c16;
             float weight = ((kernel[dx + 2] * kernel[dy + 2]) * c32) * expf(-pd / P.plane_scale);
             if (center_supported) {
                 float scale = fmaxf(0.02f, 2.0f * sqrtf(fmaxf(variance + om.y, 0.0f)));
@@ -446,7 +477,10 @@ extern "C" lux_status lux_screen_filter(LuxScreen *s, const LuxSettings *setting
         bool last = level + 1 == f->spatial_filter_steps;
         float4 *dst = last ? (float4 *)out : (level % 2 == 0 ? s->ping : s->pong);
         float *dst_mask = src_mask == s->mask_ping ? s->mask_pong : s->mask_ping;
-        denoise_kernel<<<grid, block, 0, stream>>>(P, in, T, src, src_mask, dst, dst_mask);
+        // Blocks of 16 x 16 pixels of one lattice phase, step x step phases.
+        const uint32_t lu = (s->width + P.step - 1) / P.step, lv = (s->height + P.step - 1) / P.step;
+        dim3 lattice(P.step * ((lu + kDenoiseTile - 1) / kDenoiseTile), P.step * ((lv + kDenoiseTile - 1) / kDenoiseTile));
+        denoise_kernel<<<lattice, block, 0, stream>>>(P, in, T, src, src_mask, dst, dst_mask);
         src = dst;
         src_mask = dst_mask;
     }
