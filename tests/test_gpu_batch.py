@@ -81,14 +81,17 @@ def assert_same(a, b, settings):
             np.testing.assert_allclose(ma, mb, rtol=1e-4, atol=1e-6)
 
 
-@pytest.mark.parametrize("graph", [True, False])
-def test_batch_matches_unbatched(graph):
+@pytest.mark.parametrize("graph,sky", [(True, False), (False, False), (True, True)])
+def test_batch_matches_unbatched(graph, sky):
+    """sky: a constant environment, whose next-event samples share the
+    batched visibility pass with the emissive ones."""
     ctx = bp.LuxContext()
     jobs = make_jobs(ctx)
     batch = bp.Batch(ctx)
     batch.set_graph(graph)
+    env = (1.0, 0.8, 0.6) if sky else (0.0, 0.0, 0.0)
     for frame in (1, 2):
-        settings = bp.RadianceCascades(frame_index=frame, **SETTINGS).sanitized()
+        settings = bp.RadianceCascades(frame_index=frame, environment=env, **SETTINGS).sanitized()
         batch.trace_merge(batch_args(jobs), settings)
         got = [snapshot(j, settings) for j in jobs]
         for j, g in zip(jobs, got):
