@@ -26,6 +26,8 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include "lux_internal.h"
 #include "lux_math.cuh"
 #include "shade.cuh"
@@ -103,6 +105,11 @@ struct ViewDevice {
     unsigned long long *level_base; // [levels]
     uint32_t *receiver_cell;        // [levels][max_receivers]
     uint32_t *receiver_lod;         // [max_receivers] the LOD each receiver's rays deposit into
+    uint32_t *receiver_ordinal;     // [max_receivers] the receiver's place in the sample sequence
+    unsigned long long *order_keys; // [2][max_receivers] sequence-order sort keys (in, out)
+    uint32_t *order_vals;           // [2][max_receivers] receiver indices (in, out)
+    void *order_temp;               // radix-sort scratch
+    size_t order_temp_bytes;
     uint32_t *corner_ids;           // [levels][cell_capacity][8] (level+1 ids)
     float4 *corner_frac;            // [levels][cell_capacity]
     float4 *accum;                  // [entries] J sum rgb, non-terminating count
@@ -290,6 +297,30 @@ __global__ void seed_assign_kernel(ViewDevice V, FrameParams F) {
     }
 }
 
+// Sample sequence order (the reference's rank / parents / prefix passes,
+// shaders/split.slang:788-963): the receivers of one cascade-0 cell take
+// consecutive places and sibling cells of every coarser level adjacent runs,
+// so each probe's rays are consecutive points of the R2 sequence.  The order
+// is the LOD, then the Morton order of the cascade-0 cell (at every level
+// the octant ordinal x + 2y + 4z, as `prefix` orders siblings), then the
+// receiver index; the reference takes atomic arrival order where the index
+// and the Morton order of the roots decide here.  Absent receivers sort last.
+__device__ __forceinline__ unsigned long long sequence_key(int32_t x, int32_t y, int32_t z, uint32_t lod) {
+    const uint32_t bx = (uint32_t)x + (1u << 18), by = (uint32_t)y + (1u << 18), bz = (uint32_t)z + (1u << 18);
+    unsigned long long m = 0;
+#pragma unroll
+    for (int b = 0; b < 19; ++b)
+        m |= ((unsigned long long)((bx >> b) & 1u) << (3 * b)) | ((unsigned long long)((by >> b) & 1u) << (3 * b + 1)) |
+             ((unsigned long long)((bz >> b) & 1u) << (3 * b + 2));
+    return ((unsigned long long)(lod & 31u) << 57) | m;
+}
+
+// sorted: the receiver indices in sequence order (the sort's output half).
+__global__ void ordinal_kernel(ViewDevice V, const uint32_t *__restrict__ sorted, uint32_t receivers) {
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < receivers; j += gridDim.x * blockDim.x)
+        V.receiver_ordinal[sorted[j]] = j;
+}
+
 __global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
     size_t n = (size_t)F.receivers * F.levels;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -305,6 +336,10 @@ __global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__
         if (level == 0u) V.receiver_lod[r] = lod;
         int32_t x, y, z;
         cell_of(F, level, q, x, y, z, lod);
+        if (level == 0u) {
+            V.order_keys[r] = F.sparse && p.w == 0.0f ? ~0ull : sequence_key(x, y, z, lod);
+            V.order_vals[r] = r;
+        }
         V.receiver_cell[(size_t)level * F.receivers + r] =
             F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z, lod);
     }
@@ -353,11 +388,11 @@ __global__ void clear_entries_kernel(ViewDevice V, FrameParams F) {
 // r2(sequence + 1) + jitter)) flipped into the normal's hemisphere
 // (traceTransport, shaders/split.slang:1135-1146); (u, v) of the flipped
 // direction give its bin at every level.
-__device__ __forceinline__ void split_direction(const FrameParams &F, uint32_t frame, uint32_t i, uint32_t k, f3 n,
-                                                f3 &dir, float &u, float &v) {
+__device__ __forceinline__ void split_direction(const ViewDevice &V, const FrameParams &F, uint32_t frame, uint32_t i,
+                                                uint32_t k, f3 n, f3 &dir, float &u, float &v) {
     float jx, jy, rx, ry;
     lux::r2(lux::transport_hash(frame ^ 0x5a17c9e3u), jx, jy);
-    lux::r2(i * F.rays_per_receiver + k + 1u, rx, ry);
+    lux::r2(V.receiver_ordinal[i] * F.rays_per_receiver + k + 1u, rx, ry);
     u = lux::fracf((0.5f + rx) + jx);
     v = lux::fracf((0.5f + ry) + jy);
     dir = lux::decode_direction(u, v);
@@ -402,7 +437,7 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
             float4 p4 = pos[i], n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
             float u, v;
-            split_direction(F, F.shade.frame, i, k, n, d, u, v);
+            split_direction(V, F, F.shade.frame, i, k, n, d, u, v);
             o = lux::ray_offset(p, n, F.shade.normal_bias);
             tmin = 0.0f;
             limit = 1e20f;
@@ -448,7 +483,7 @@ __device__ __forceinline__ bool closest_split_ray(const ViewDevice &V, const Fra
     f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
     f3 dir;
     float u, v;
-    split_direction(F, frame, i, k, n, dir, u, v);
+    split_direction(V, F, frame, i, k, n, dir, u, v);
     f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
     lux::Hit hit;
     lux::trace<false, kDepth>(S, origin, dir, 0.0f, 1e20f, hit, cn);
@@ -526,7 +561,7 @@ __global__ void ray_keys_kernel(ViewDevice V, FrameParams F, SceneView S, const 
         float4 p4 = pos[i], n4 = nrm[i];
         f3 dir;
         float u, v;
-        split_direction(F, F.shade.frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+        split_direction(V, F, F.shade.frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
         uint32_t bin = lux::direction_index_uv(u, v, 8u, 4u);
         V.sort_keys[ray] = bin * kSortCells + cell16(S, f3{p4.x, p4.y, p4.z});
     }
@@ -761,7 +796,7 @@ __device__ __forceinline__ void deposit_split_ray(const ViewDevice &V, const Fra
     float4 n4 = nrm[i];
     f3 dir;
     float u, v;
-    split_direction(F, frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
+    split_direction(V, F, frame, i, k, f3{n4.x, n4.y, n4.z}, dir, u, v);
     float t = V.ts.ray_o[ray].w;
     // splitIntervalContainsHit at the receiver's LOD (ends scale by 2^lod,
     // shaders/split.slang:224-236).
@@ -1565,7 +1600,7 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
             bool full = validate || fallback;
             f3 dir;
             float u, v;
-            split_direction(F, F.shade.frame, i, k, n, dir, u, v);
+            split_direction(V, F, F.shade.frame, i, k, n, dir, u, v);
             f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
             lux::Hit hit;
             lux::trace<false>(S, origin, dir, 0.0f, full ? 1e20f : C.near_limit, hit, cn);
@@ -1795,6 +1830,15 @@ static void cache_buffers_free(LuxView *v) {
     v->cache_alloc = false;
 }
 
+// Radix-sort scratch for ordering `receivers` sequence keys.
+static size_t order_temp_bytes(uint32_t receivers) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned long long *)nullptr, (unsigned long long *)nullptr,
+                                    (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)std::max(receivers, 1u), 0,
+                                    62);
+    return std::max<size_t>(bytes, 16);
+}
+
 static lux_status view_alloc(LuxView *v) {
     LuxContext *ctx = v->ctx;
     const LuxViewDesc &d = v->desc;
@@ -1812,6 +1856,10 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.level_base, L * sizeof(unsigned long long)},
         {(void **)&D.receiver_cell, L * (size_t)d.max_receivers * sizeof(uint32_t)},
         {(void **)&D.receiver_lod, (size_t)d.max_receivers * sizeof(uint32_t)},
+        {(void **)&D.receiver_ordinal, (size_t)d.max_receivers * sizeof(uint32_t)},
+        {(void **)&D.order_keys, 2 * (size_t)d.max_receivers * sizeof(unsigned long long)},
+        {(void **)&D.order_vals, 2 * (size_t)d.max_receivers * sizeof(uint32_t)},
+        {(void **)&D.order_temp, order_temp_bytes(d.max_receivers)},
         {(void **)&D.corner_ids, L * (size_t)d.max_cells * 8 * sizeof(uint32_t)},
         {(void **)&D.corner_frac, L * (size_t)d.max_cells * sizeof(float4)},
         {(void **)&D.accum, (size_t)d.max_entries * sizeof(float4)},
@@ -1850,6 +1898,7 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.sort_perm, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
         {(void **)&D.sort_hist, (size_t)kSortBins * sizeof(uint32_t)},
     };
+    D.order_temp_bytes = order_temp_bytes(d.max_receivers);
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
             cudaGetLastError();
@@ -1887,6 +1936,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
     if (!v) return LUX_OK;
     ViewDevice &D = v->dev;
     void *ptrs[] = {D.dir_keys, D.dir_ids, D.cell_keys, D.cell_count, D.level_base, D.receiver_cell, D.receiver_lod,
+                    D.receiver_ordinal, D.order_keys, D.order_vals, D.order_temp,
                     D.corner_ids,
                     D.corner_frac, D.accum, D.count, D.merged, D.raw, D.mass, D.hist_cell, D.cell_last,
                     D.retain_hist, D.retain_limit, D.tables, D.error_flags, D.stats,
@@ -2043,6 +2093,13 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
         seed_insert_kernel<<<grid, 256, 0, st>>>(D, F, pos);
         seed_assign_kernel<<<grid, 256, 0, st>>>(D, F);
         seed_lookup_kernel<<<grid, 256, 0, st>>>(D, F, pos);
+        if (F.layout == LUX_LAYOUT_SPLIT) {  // the receivers' places in the sample sequence
+            size_t bytes = D.order_temp_bytes;
+            cub::DeviceRadixSort::SortPairs(D.order_temp, bytes, D.order_keys, D.order_keys + v->desc.max_receivers,
+                                            D.order_vals, D.order_vals + v->desc.max_receivers, (int)F.receivers, 0,
+                                            62, st);
+            ordinal_kernel<<<grid, 256, 0, st>>>(D, D.order_vals + v->desc.max_receivers, F.receivers);
+        }
     }
     if (F.history && F.layout == LUX_LAYOUT_SPLIT) {  // retain: the previous frame's unseen cells stay
         const HistoryDevice H = history_device(v);

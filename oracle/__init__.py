@@ -68,6 +68,7 @@ def lib():
             "orc_frame_run_bounce": (P, [P, P, P, P, U, C.c_int, P, P, U, U, C.c_uint64, P, U, P, P, P]),
             "orc_lod_blend": (None, [P, P, P, P, P, P]),
             "orc_transport_random": (F, [U, U]),
+            "orc_sequence_order": (None, [P, P, P, U, C.c_int, P]),
             "orc_cosine_direction_frame": (None, [P, F, F, P]),
             "orc_environment_response": (C.c_int, [P, P, F, F, U, U, P, P, P, P, F, P, C.c_int, P, P, P]),
             "orc_screen_filter": (None, [P, U, U, P, P, P, P, P, P, U, U, U, P, P, P]),
@@ -255,6 +256,15 @@ def lod_blend(settings_c, camera, position):
     lib().orc_lod_blend(C.byref(settings_c), C.byref(camera) if camera is not None else None, _p(p), C.byref(low),
                         C.byref(high), C.byref(blend))
     return int(low.value), int(high.value), float(blend.value)
+
+
+def sequence_order(settings_c, pos, sparse=False, camera=None):
+    """Each Split receiver's place in the sample sequence (uint32[n])."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    out = np.zeros(len(pos), np.uint32)
+    lib().orc_sequence_order(C.byref(settings_c), C.byref(camera) if camera is not None else None, _p(pos),
+                             len(pos), 1 if sparse else 0, _p(out))
+    return out
 
 
 def transport_random(seed, lane):

@@ -1687,6 +1687,55 @@ static void cell_key(const LuxSettings *st, uint32_t level, const float p[3], ui
     out[3] = (int32_t)lod;
 }
 
+/* Sample sequence order (rank / parents / prefix, shaders/split.slang:788-963):
+ * the receivers of one cascade-0 cell take consecutive places and sibling cells
+ * of every coarser level adjacent runs.  Key: LOD, then the Morton code of the
+ * cascade-0 cell (octant ordinal x + 2y + 4z at every level, 19 bits per axis
+ * biased by 2^18); ties by receiver index; absent receivers last. */
+static uint64_t sequence_key(const int32_t key[4]) {
+    uint32_t b[3] = {(uint32_t)key[0] + (1u << 18), (uint32_t)key[1] + (1u << 18), (uint32_t)key[2] + (1u << 18)};
+    uint64_t m = 0;
+    for (int bit = 0; bit < 19; ++bit)
+        for (int a = 0; a < 3; ++a) m |= (uint64_t)((b[a] >> bit) & 1u) << (3 * bit + a);
+    return ((uint64_t)((uint32_t)key[3] & 31u) << 57) | m;
+}
+typedef struct {
+    uint64_t key;
+    uint32_t index;
+} OrderItem;
+static int order_cmp(const void *a, const void *b) {
+    const OrderItem *x = (const OrderItem *)a, *y = (const OrderItem *)b;
+    if (x->key != y->key) return x->key < y->key ? -1 : 1;
+    return x->index < y->index ? -1 : (x->index > y->index ? 1 : 0);
+}
+
+/* Each receiver's place in the sample sequence: out[i] = rank of receiver i. */
+static void sequence_order(const LuxSettings *st, const LodParams *lod, const float *pos, uint32_t n, int sparse,
+                           uint32_t *out) {
+    OrderItem *order = (OrderItem *)malloc(sizeof(OrderItem) * (n ? n : 1));
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = pos + 4 * (size_t)i;
+        order[i].index = i;
+        if (sparse && p[3] == 0.0f) {
+            order[i].key = ~0ull;
+            continue;
+        }
+        int32_t key[4];
+        cell_key(st, 0, p, receiver_lod(lod, p, i, st->frame_index), key);
+        order[i].key = sequence_key(key);
+    }
+    qsort(order, n, sizeof(OrderItem), order_cmp);
+    for (uint32_t j = 0; j < n; ++j) out[order[j].index] = j;
+    free(order);
+}
+
+void orc_sequence_order(const LuxSettings *settings, const LuxCamera *camera, const float *pos, uint32_t n,
+                        int sparse, uint32_t *out) {
+    LodParams lod;
+    lod_params(settings, camera, &lod);
+    sequence_order(settings, &lod, pos, n, sparse, out);
+}
+
 typedef struct {
     const OrcScene *S;
     const LuxSettings *st;
@@ -1697,6 +1746,7 @@ typedef struct {
     const LodParams *lod;     /* distance LODs of the frame (NULL: LOD 0) */
     int sparse;               /* receivers with position.w == 0 are absent */
     float *hit_pos, *hit_nrm; /* float4 per receiver: the surface of ray frame % R, or NULL */
+    const uint32_t *ordinal;  /* split: each receiver's place in the sample sequence */
     /* split: per ray outputs */
     int32_t *term_level;  /* -1 = unsupported */
     float *radiance;      /* rgb per ray */
@@ -1743,7 +1793,7 @@ static void *split_job(void *arg) {
         }
         float uv[2], origin[3], dir[3];
         LuxHit hit;
-        split_ray(j->S, st, p, n, i * R + k, uv, &hit, origin, dir);
+        split_ray(j->S, st, p, n, j->ordinal[i] * R + k, uv, &hit, origin, dir);
         orc_trace_closest(j->S, origin, dir, 0.0f, 1e20f, &hit, &j->cn);
         float rad[3], rec[7];
         int supported = outgoing_radiance(j->S, st, j->bounce, origin, dir, &hit, rad, rec, &j->shadow, &j->cn);
@@ -2342,6 +2392,9 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         proto.sparse = sparse;
         proto.hit_pos = (flags & ORC_FRAME_RECORD_HITS) ? hit_pos : NULL;
         proto.hit_nrm = (flags & ORC_FRAME_RECORD_HITS) ? hit_nrm : NULL;
+        uint32_t *ordinal = (uint32_t *)malloc(sizeof(uint32_t) * (n ? n : 1));
+        sequence_order(st, &F->lod, pos, n, sparse, ordinal);
+        proto.ordinal = ordinal;
         proto.term_level = (int32_t *)malloc(sizeof(int32_t) * (rays ? rays : 1));
         proto.radiance = (float *)malloc(sizeof(float) * 3 * (rays ? rays : 1));
         proto.uv = (float *)malloc(sizeof(float) * 2 * (rays ? rays : 1));
@@ -2381,6 +2434,7 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         free(proto.term_level);
         free(proto.radiance);
         free(proto.uv);
+        free(ordinal);
     } else {
         for (uint32_t l = 0; l < F->levels; ++l) {
             FrameJob proto;

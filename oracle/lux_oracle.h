@@ -89,6 +89,12 @@ int orc_outgoing_radiance(const OrcScene *scene, const LuxSettings *settings,
  * samples of sequence base `sequence_base`; `visibility` negative traces the
  * scene, 0/1/2 stub every query as visible/blocked/unsupported (scene may
  * then be NULL).  Returns supported. */
+/* Each Split receiver's place in the sample sequence (receiver i's ray k
+ * uses R2 index out[i] x R + k): LOD, then the Morton order of the cascade-0
+ * cell, then the receiver index; absent receivers (sparse, position.w == 0)
+ * last (shaders/split.slang:788-963). */
+void orc_sequence_order(const LuxSettings *settings, const LuxCamera *camera, const float *pos, uint32_t n,
+                        int sparse, uint32_t *out);
 float orc_transport_random(uint32_t seed, uint32_t lane);
 void orc_cosine_direction_frame(const float n[3], float u1, float u2, float out[3]);
 int orc_environment_response(const OrcScene *scene, const float environment[3], float probe_spacing, float bias,
