@@ -46,7 +46,16 @@ DRAM_BYTES_PER_INTERVAL_RAY = (3.824128e6 + 0.283136e6) / 421344
 DRAM_BYTES_PER_SHADOW_RAY = (42.729216e6 + 0.481536e6) / 1236328
 LEARNED_CUTOFF = 1
 LEARNED_WARMUP = 200
-LAUNCHES_PER_FRAME_FIXED = 11  # clear, 3 seed, layout, clear entries, closest, shade, shadow, deposit, pack
+# Kernels of one plain Split frame with world history: clear, 3 seed, the
+# sample-sequence sort (radix-sort histogram, exclusive sum, 8 one-sweep passes
+# over 62-bit keys, ordinal), 3 retain, layout, clear entries, closest, shade,
+# shadow, deposit, pack; then per level a history map and a merge and per level
+# but the last a corners pass; 3 more when visibility queries are sorted.
+LAUNCHES_PER_FRAME_FIXED = 25
+
+
+def launches_per_frame(levels: int, sort_queries: bool) -> int:
+    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (3 if sort_queries else 0)
 
 
 def settings_for_workload():
@@ -651,7 +660,7 @@ def run_ours(args, rank, world):
             "learned": learned,
             "multi_bounce": multi_bounce,
             "screen_filter": screen,
-            "gpu_launches": args.steps * (LAUNCHES_PER_FRAME_FIXED + 2 * settings.levels - 1),
+            "gpu_launches": args.steps * launches_per_frame(settings.levels, bool(tuned["best"].get("sort_queries"))),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
             "clocks": clocks.summary(),
