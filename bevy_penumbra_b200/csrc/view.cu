@@ -813,13 +813,10 @@ __device__ __forceinline__ void deposit_split_ray(const ViewDevice &V, const Fra
         uint32_t bin = lux::direction_index_uv(u, v, F.columns[l], F.rows[l]);
         unsigned long long e = V.level_base[l] + (unsigned long long)cell * F.dirs[l] + bin;
         atomicAdd(&V.count[e], 1u);
-        if (l == term) {
-            atomicAdd(&V.accum[e].x, radiance.x);
-            atomicAdd(&V.accum[e].y, radiance.y);
-            atomicAdd(&V.accum[e].z, radiance.z);
-        } else {
+        if (l == term)  // one 16-byte vector atomic (w += 0 leaves the count of passes unchanged)
+            atomicAdd(&V.accum[e], make_float4(radiance.x, radiance.y, radiance.z, 0.0f));
+        else
             atomicAdd(&V.accum[e].w, 1.0f);
-        }
         st[kStatDeposits] += 1;
     }
 }
