@@ -42,8 +42,8 @@ REFERENCE_SPP = 1024
 # small atrium case (profiles/closest_split_kernel_shadow_kernel_atrium65536_640x360.md:
 # dram read + write per launch / rays of that launch); the full frame's traffic
 # is scaled from it by its ray counts.
-DRAM_BYTES_PER_INTERVAL_RAY = (3.824128e6 + 0.283136e6) / 421344
-DRAM_BYTES_PER_SHADOW_RAY = (42.729216e6 + 0.481536e6) / 1236328
+DRAM_BYTES_PER_INTERVAL_RAY = (4.247040e6 + 0.378880e6) / 421344
+DRAM_BYTES_PER_SHADOW_RAY = (54.969600e6 + 2.205952e6) / 1237295
 LEARNED_CUTOFF = 1
 LEARNED_WARMUP = 200
 # Kernels of one plain Split frame with world history: clear, 3 seed, the
