@@ -1779,6 +1779,11 @@ struct LuxView {
     // while the frame traces; `stage_ready` orders the resolve after it.
     cudaStream_t stage_stream = nullptr;
     cudaEvent_t stage_ready = nullptr;
+    // Unbatched Split frames: retain, layout and record clearing run on this
+    // stream during the closest-hit pass (`seeded` forks it after the seed,
+    // `laid_out` joins it before hit shading).
+    cudaStream_t setup_stream = nullptr;
+    cudaEvent_t seeded = nullptr, laid_out = nullptr;
     FrameParams last{};
     bool has_frame = false;
     // World history: the other buffer set (swapped with dev's at each
@@ -1947,6 +1952,10 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
         if (p) cudaFree(p);
     if (v->stage_ready) cudaEventDestroy(v->stage_ready);
     if (v->stage_stream) cudaStreamDestroy(v->stage_stream);
+    if (v->setup_stream) cudaStreamSynchronize(v->setup_stream);
+    if (v->seeded) cudaEventDestroy(v->seeded);
+    if (v->laid_out) cudaEventDestroy(v->laid_out);
+    if (v->setup_stream) cudaStreamDestroy(v->setup_stream);
     for (int i = 0; i < kTimingEvents; ++i)
         if (v->ev[i]) cudaEventDestroy(v->ev[i]);
     cache_buffers_free(v);
@@ -2082,7 +2091,8 @@ static HistoryDevice history_device(const LuxView *v) {
                          v->hist.raw,      v->hist.mass,    v->hist.cell_last, v->hist.cell_keys};
 }
 
-static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, cudaStream_t st) {
+// seed: clear, the receivers' cells and dense ids, the sample-sequence order.
+static void enqueue_seed(LuxView *v, const FrameParams &F, const float4 *pos, cudaStream_t st) {
     const ViewDevice &D = v->dev;
     const int grid = v->ctx->sm_count * 8;
     clear_kernel<<<grid, 256, 0, st>>>(D, F);
@@ -2098,6 +2108,12 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
             ordinal_kernel<<<grid, 256, 0, st>>>(D, D.order_vals + v->desc.max_receivers, F.receivers);
         }
     }
+}
+
+// layout: retained cells, record offsets, cleared records.
+static void enqueue_layout(LuxView *v, const FrameParams &F, cudaStream_t st) {
+    const ViewDevice &D = v->dev;
+    const int grid = v->ctx->sm_count * 8;
     if (F.history && F.layout == LUX_LAYOUT_SPLIT) {  // retain: the previous frame's unseen cells stay
         const HistoryDevice H = history_device(v);
         cudaMemsetAsync(D.retain_hist, 0, (size_t)LUX_MAX_LEVELS * kRetainBins * sizeof(uint32_t), st);
@@ -2107,6 +2123,11 @@ static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, c
     }
     layout_kernel<<<1, 32, 0, st>>>(D, F);
     clear_entries_kernel<<<grid, 256, 0, st>>>(D, F);
+}
+
+static void enqueue_setup(LuxView *v, const FrameParams &F, const float4 *pos, cudaStream_t st) {
+    enqueue_seed(v, F, pos, st);
+    enqueue_layout(v, F, st);
 }
 
 // Corners then the merge of every level, coarsest first (mergeEntry over
@@ -2351,7 +2372,27 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
                                    fb_owner->secondary->dir_capacity, fb_owner->fb.spacing};
     }
     mark(0);
-    enqueue_setup(v, F, pos, st);
+    const bool cached_frame = v->cache_alloc && v->cache.cutoff_level < F.levels;
+    // The closest-hit pass needs only the seed (cells, sequence order), so the
+    // rest of the setup runs beside it on the setup stream.
+    bool forked = false;
+    if (F.layout == LUX_LAYOUT_SPLIT && rc->count && !cached_frame) {
+        if (!v->setup_stream &&
+            (cudaStreamCreateWithFlags(&v->setup_stream, cudaStreamNonBlocking) != cudaSuccess ||
+             cudaEventCreateWithFlags(&v->seeded, cudaEventDisableTiming) != cudaSuccess ||
+             cudaEventCreateWithFlags(&v->laid_out, cudaEventDisableTiming) != cudaSuccess)) {
+            cudaGetLastError();
+            return lux_fail(ctx, LUX_ERR_CUDA, "trace_merge: setup stream creation failed");
+        }
+        enqueue_seed(v, F, pos, st);
+        cudaEventRecord(v->seeded, st);
+        cudaStreamWaitEvent(v->setup_stream, v->seeded, 0);
+        enqueue_layout(v, F, v->setup_stream);
+        cudaEventRecord(v->laid_out, v->setup_stream);
+        forked = true;
+    } else {
+        enqueue_setup(v, F, pos, st);
+    }
     mark(1);
     if (F.layout == LUX_LAYOUT_SPLIT) {
         uint32_t rays = rc->count * F.rays_per_receiver;
@@ -2391,6 +2432,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
             else
                 closest_split_kernel<64><<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
                     Dr, F, scene->view, pos, nrm, rays);
+            if (forked) cudaStreamWaitEvent(st, v->laid_out, 0);  // join the setup stream
             ViewDevice Dq = D;  // query pass view: keys written by shade, optional order
             if (!T.sort_queries) Dq.sort_keys = nullptr;
             shade_kernel<<<(rays + 127) / 128, 128, 0, st>>>(Dq, F, scene->view, rays, false);
