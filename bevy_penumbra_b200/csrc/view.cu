@@ -1920,6 +1920,8 @@ extern "C" lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, 
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: capacities must be positive");
     if ((uint64_t)desc->max_rays * lux::kMaxNeeSamples > 0xffffffffull)
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_rays above 2^28");
+    if (desc->max_receivers > 0x7fffffffu)  // the sample-sequence sort counts receivers in an int
+        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_receivers above 2^31 - 1");
     if (desc->max_cells > (1u << 30))
         return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "view: max_cells above 2^30");
     LuxView *v = new LuxView();
