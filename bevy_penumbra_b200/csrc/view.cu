@@ -27,6 +27,7 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "lux_internal.h"
 #include "lux_math.cuh"
@@ -131,6 +132,9 @@ struct ViewDevice {
     uint32_t *sort_keys;            // [max(rays, queries)]
     uint32_t *sort_perm;            // [max(rays, queries)] processing order -> item
     uint32_t *sort_hist;            // [kSortBins]
+    uint32_t *sort_offs;            // [kSortBins] exclusive prefix of sort_hist, then scatter cursors
+    void *scan_temp;                // device-wide scan scratch
+    size_t scan_temp_bytes;
     const uint32_t *ray_order;      // closest-hit processing order (nullptr: identity)
     const uint32_t *query_order;    // visibility processing order (nullptr: identity)
 };
@@ -596,33 +600,18 @@ __global__ void sort_hist_kernel(ViewDevice V, const uint32_t *count_ptr, uint32
         atomicAdd(&V.sort_hist[V.sort_keys[i]], 1u);
 }
 
-__global__ void __launch_bounds__(1024) sort_scan_kernel(ViewDevice V) {
-    __shared__ uint32_t part[1024];
-    constexpr uint32_t per = kSortBins / 1024;
-    uint32_t t = threadIdx.x;
-    uint32_t sum = 0;
-    for (uint32_t j = 0; j < per; ++j) sum += V.sort_hist[t * per + j];
-    part[t] = sum;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {
-        uint32_t add = t >= off ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += add;
-        __syncthreads();
-    }
-    uint32_t run = part[t] - sum;  // exclusive prefix of this thread's range
-    for (uint32_t j = 0; j < per; ++j) {
-        uint32_t c = V.sort_hist[t * per + j];
-        V.sort_hist[t * per + j] = run;
-        run += c;
-    }
-}
-
 __global__ void sort_scatter_kernel(ViewDevice V, const uint32_t *count_ptr, uint32_t cap) {
     uint32_t n = count_ptr ? min(*count_ptr, cap) : cap;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        V.sort_perm[atomicAdd(&V.sort_hist[V.sort_keys[i]], 1u)] = i;
+        V.sort_perm[atomicAdd(&V.sort_offs[V.sort_keys[i]], 1u)] = i;
 }
+
+// Exclusive prefix of the counting-sort histogram over the whole device.
+static void enqueue_sort_scan(const ViewDevice &D, cudaStream_t st) {
+    size_t bytes = D.scan_temp_bytes;
+    cub::DeviceScan::ExclusiveSum(D.scan_temp, bytes, D.sort_hist, D.sort_offs, (int)kSortBins, st);
+}
+
 
 // Hit shading up to the visibility traces; queries are appended to the
 // queue with one atomic per warp.
@@ -1852,6 +1841,13 @@ static void cache_buffers_free(LuxView *v) {
     v->cache_alloc = false;
 }
 
+// Device-wide scan scratch for the counting-sort histogram.
+static size_t scan_temp_bytes() {
+    size_t bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)kSortBins);
+    return std::max<size_t>(bytes, 16);
+}
+
 // Radix-sort scratch for ordering `receivers` sequence keys.
 static size_t order_temp_bytes(uint32_t receivers) {
     size_t bytes = 0;
@@ -1919,8 +1915,11 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.sort_keys, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
         {(void **)&D.sort_perm, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
         {(void **)&D.sort_hist, (size_t)kSortBins * sizeof(uint32_t)},
+        {(void **)&D.sort_offs, (size_t)kSortBins * sizeof(uint32_t)},
+        {(void **)&D.scan_temp, scan_temp_bytes()},
     };
     D.order_temp_bytes = order_temp_bytes(d.max_receivers);
+    D.scan_temp_bytes = scan_temp_bytes();
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
             cudaGetLastError();
@@ -1967,7 +1966,7 @@ extern "C" lux_status lux_view_destroy(LuxView *v) {
                     v->hist.dir_keys, v->hist.dir_ids, v->hist.level_base, v->hist.cell_count, v->hist.raw,
                     v->hist.mass, v->hist.cell_last, v->hist.cell_keys,
                     D.ts.ray_o, D.ts.ray_d, D.ts.ray_h, D.ts.ray_base, D.ts.ray_extra, D.ts.query_slot, D.ts.slot_contrib, D.ts.queue_o, D.ts.queue_d,
-                    D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist,
+                    D.ts.queue_result, D.ts.queue_count, D.ts.work_counter, D.sort_keys, D.sort_perm, D.sort_hist, D.sort_offs, D.scan_temp,
                     v->stage_pos, v->stage_nrm, v->stage_ppos, v->stage_pnrm, v->stage_out};
     if (v->stage_stream) cudaStreamSynchronize(v->stage_stream);
     for (void *p : ptrs)
@@ -2426,7 +2425,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
                 cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
                 ray_keys_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, F, scene->view, pos, nrm, rays);
                 sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
-                sort_scan_kernel<<<1, 1024, 0, st>>>(D);
+                enqueue_sort_scan(D, st);
                 sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
                 Dr.ray_order = D.sort_perm;
             }
@@ -2461,7 +2460,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
             if (T.sort_queries) {
                 cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
                 sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
-                sort_scan_kernel<<<1, 1024, 0, st>>>(D);
+                enqueue_sort_scan(D, st);
                 sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
                 Dq.query_order = D.sort_perm;
             }
