@@ -50,12 +50,13 @@ LEARNED_WARMUP = 200
 # sample-sequence sort (radix-sort histogram, exclusive sum, 8 one-sweep passes
 # over 62-bit keys, ordinal), 3 retain, layout, clear entries, closest, shade,
 # shadow, deposit, pack; then per level a history map and a merge and per level
-# but the last a corners pass; 3 more when visibility queries are sorted.
+# but the last a corners pass; 4 more when visibility queries are sorted
+# (histogram, scan init and scan, scatter).
 LAUNCHES_PER_FRAME_FIXED = 25
 
 
 def launches_per_frame(levels: int, sort_queries: bool) -> int:
-    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (3 if sort_queries else 0)
+    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (4 if sort_queries else 0)
 
 
 def settings_for_workload():

@@ -140,24 +140,24 @@ struct ViewDevice {
 };
 
 constexpr uint32_t kSortCells = 4096;           // 16^3 origin cells over the TLAS root box
-constexpr uint32_t kQueryCells = 262144;        // 64^3 origin cells of visibility queries
-constexpr uint32_t kSortBins = 8 * kQueryCells; // 8 emitter buckets x 64^3 origin cells of queries,
+constexpr uint32_t kQueryCells = 2097152;       // 128^3 origin cells of visibility queries
+constexpr uint32_t kSortBins = 8 * kQueryCells; // 8 emitter buckets x 128^3 origin cells of queries,
                                                 // or 32 direction bins x 16^3 cells of interval rays
 
-// Morton index of a point's cell in a 64^3 grid over the scene box.
-__device__ __forceinline__ uint32_t cell64(const SceneView &S, lux::f3 p) {
+// Morton index of a point's cell in a 128^3 grid over the scene box.
+__device__ __forceinline__ uint32_t cell128(const SceneView &S, lux::f3 p) {
     float e[3] = {p.x, p.y, p.z};
     uint32_t c[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         float span = S.root_hi[a] - S.root_lo[a];
         float t = span > 0.0f ? (e[a] - S.root_lo[a]) / span : 0.0f;
-        int q = (int)(t * 64.0f);
-        c[a] = (uint32_t)(q < 0 ? 0 : (q > 63 ? 63 : q));
+        int q = (int)(t * 128.0f);
+        c[a] = (uint32_t)(q < 0 ? 0 : (q > 127 ? 127 : q));
     }
     uint32_t m = 0;
 #pragma unroll
-    for (int b = 0; b < 6; ++b)
+    for (int b = 0; b < 7; ++b)
         m |= (((c[0] >> b) & 1u) << (3 * b)) | (((c[1] >> b) & 1u) << (3 * b + 1)) | (((c[2] >> b) & 1u) << (3 * b + 2));
     return m;
 }
@@ -640,7 +640,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
                                              if (sample >= lux::kMaxNeeSamples) return;  // host checks the slot count
                                              const size_t slot = slot0 + sample;
                                              // w of the direction: the query's coherence sort key.
-                                             uint32_t key = keys ? (q.light & 7u) * kQueryCells + cell64(S, q.origin)
+                                             uint32_t key = keys ? (q.light & 7u) * kQueryCells + cell128(S, q.origin)
                                                                  : 0u;
                                              V.ts.queue_o[slot] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.limit);
                                              V.ts.queue_d[slot] = make_float4(q.direction.x, q.direction.y,

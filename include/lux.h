@@ -358,7 +358,7 @@ typedef struct LuxTuning {
     uint32_t shadow_mode;
     uint32_t closest_blocks_per_sm;
     uint32_t shadow_blocks_per_sm;
-    uint32_t sort_queries;        /* 1: order visibility queries by (emitter bucket of 8, origin cell of a 64^3
+    uint32_t sort_queries;        /* 1: order visibility queries by (emitter bucket of 8, origin cell of a 128^3
                                      grid over the scene box) before tracing */
     uint32_t sort_rays;           /* 1: order interval rays by (direction bin, origin cell) before tracing */
     uint32_t stack_depth;         /* traversal stack entries per thread: 32 or 64 (0 = 64); an overflowing
