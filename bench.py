@@ -39,9 +39,9 @@ EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
 REFERENCE_SPP = 1024
 # DRAM bytes per ray of the traversal kernels from one ncu capture of the
-# small atrium case (profiles/closest_split_kernel_shadow_kernel_atrium65536_640x360.md:
-# dram read + write per launch / rays of that launch); the full frame's traffic
-# is scaled from it by its ray counts.
+# small atrium case (65,536 triangles at 640x360: dram read + write per launch
+# / rays of that launch); the full frame's traffic is scaled from it by its
+# ray counts.
 DRAM_BYTES_PER_INTERVAL_RAY = (4.247040e6 + 0.378880e6) / 421344
 DRAM_BYTES_PER_SHADOW_RAY = (54.969600e6 + 2.205952e6) / 1237295
 LEARNED_CUTOFF = 1

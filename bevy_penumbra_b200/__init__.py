@@ -327,6 +327,16 @@ def directional_light(direction_to_light, color) -> np.ndarray:
     return f.view(np.uint32)
 
 
+def validate_scene(packed: PackedScene) -> tuple[int, str]:
+    """lux_scene_validate: the status (and message) lux_scene_upload would
+    return for these word streams, checked on the host without a device."""
+    buf = C.create_string_buffer(512)
+    status = lib().lux_scene_validate(_ptr(packed.scene_words), len(packed.scene_words),
+                                      _ptr(packed.geometry_words), len(packed.geometry_words),
+                                      _ptr(packed.lights), len(packed.lights), packed.conventional, buf, len(buf))
+    return int(status), buf.value.decode()
+
+
 class GpuScene:
     """A scene resident on the device (lux_scene_upload)."""
 

@@ -1,7 +1,7 @@
 """ctypes binding of liblux.so (include/lux.h).
 
 This is the binding a host engine adds to call the library; the Rust FFI
-crate of bevy_lux would declare the same records.  The
+crate of bevy_lux would declare the same records and functions.  The
 library is built in-tree by ``bevy_penumbra_b200.build``; importing this
 module without it raises, so no code path silently runs without the CUDA
 kernels.
@@ -167,6 +167,7 @@ SIGNATURES = {
     "lux_packed_scene_quality": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(U32)]),
     "lux_packed_scene_destroy": (None, [P]),
     "lux_scene_upload": (C.c_int, [P, P, SZ, P, SZ, P, U32, U32, C.POINTER(P)]),
+    "lux_scene_validate": (C.c_int, [P, SZ, P, SZ, P, U32, U32, C.c_char_p, SZ]),
     "lux_scene_destroy": (C.c_int, [P]),
     "lux_scene_refit": (C.c_int, [P, P, U32, P, U32]),
     "lux_emissive_lights_at": (C.c_int, [P, SZ, P, U32, P, U32, P]),

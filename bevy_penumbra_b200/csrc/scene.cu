@@ -46,6 +46,22 @@ struct Collapser {
     // (binary node, instance) -- the instance is kEmpty unless the slot is a
     // single-instance child cut from binary leaf `x`.
     std::vector<uint2> *sources = nullptr;
+    // Binary nodes already taken into the BVH4, shared by the TLAS and every
+    // BLAS collapse of one upload: build_tree (src/scene.rs:2398-2554) emits
+    // trees, so a node reached a second time means the words hold a cycle or
+    // a shared subtree.  Rejecting it keeps the collapse linear in the node
+    // count (a shared subtree repeated at every level would otherwise double
+    // the work per level).
+    std::vector<uint8_t> *seen = nullptr;
+
+    bool visit(uint32_t index) {
+        if ((*seen)[index]) {
+            error = "BVH node reached twice (the node words do not form a tree)";
+            return false;
+        }
+        (*seen)[index] = 1;
+        return true;
+    }
 
     static double area(const BinNode &n) {
         double sx = (double)n.mx[0] - n.mn[0], sy = (double)n.mx[1] - n.mn[1], sz = (double)n.mx[2] - n.mn[2];
@@ -100,6 +116,7 @@ struct Collapser {
             error = "BVH node index out of range or cyclic";
             return lux::kEmpty;
         }
+        if (!visit(index)) return lux::kEmpty;
         const BinNode &b = bin[index];
         if (b.count > 0) {
             if ((uint64_t)b.first + b.count > leaf_limit || b.first + b.count > kLeafFirstMask) {
@@ -145,6 +162,7 @@ struct Collapser {
             }
             if (best < 0) break;
             uint32_t c = kids[best];
+            if (!visit(c)) return lux::kEmpty;
             kids.erase(kids.begin() + best);
             kids.push_back(bin[c].first);
             kids.push_back(bin[c].first + 1);
@@ -311,31 +329,48 @@ __global__ void __launch_bounds__(1024) refit_kernel(uint4 *__restrict__ sw, uin
 
 }  // namespace
 
-extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size_t sn, const uint32_t *gw, size_t gn,
-                                       const LuxLight *lights, uint32_t light_count, uint32_t conventional,
-                                       LuxScene **out) {
-    if (!ctx || !out) return LUX_ERR_INVALID_ARGUMENT;
-    *out = nullptr;
+// Host half of an upload: validation of the reference word streams, the
+// BVH4 collapse of the TLAS and every distinct BLAS, and the leaf-ordered
+// triangle positions.  Needs no device.
+struct HostScene {
+    std::vector<Bvh4Node> nodes;
+    std::vector<float4> tris;
+    std::vector<DeviceInstance> inst;
+    std::vector<uint2> slot_source;
+    std::vector<uint32_t> refit_order, depth_start;
+    uint32_t tlas_root = lux::kEmpty, inst_base = 0, inst_count = 0, tri_count = 0, tlas_slots = 0;
+    float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
+};
+
+static lux_status prepare_scene(const uint32_t *sw, size_t sn, const uint32_t *gw, size_t gn, const LuxLight *lights,
+                                uint32_t light_count, uint32_t conventional, HostScene &H, std::string &message) {
+    auto fail = [&](lux_status status, const std::string &text) {
+        message = text;
+        return status;
+    };
+    std::vector<Bvh4Node> &nodes = H.nodes;
+    std::vector<uint2> &slot_source = H.slot_source;
+    std::vector<uint32_t> &refit_order = H.refit_order, &depth_start = H.depth_start;
     if (!sw || sn < 1 || !gw || gn < 1 || (light_count && !lights) || conventional > light_count)
-        return lux_fail(ctx, LUX_ERR_INVALID_ARGUMENT, "scene upload: missing words or lights");
+        return fail(LUX_ERR_INVALID_ARGUMENT, "scene upload: missing words or lights");
     if (conventional >= 16u)
-        return lux_fail(ctx, LUX_ERR_CAPACITY,
+        return fail(LUX_ERR_CAPACITY,
                         "scene upload: at most 15 conventional lights (a hit's next-event slots are shared with the "
                         "emissive samples)");
     for (uint32_t l = 0; l < conventional; ++l) {
         const LuxLight &L = lights[l];
         for (int c = 0; c < 4; ++c)
             if (!std::isfinite(L.position[c]) || !std::isfinite(L.color[c]) || !std::isfinite(L.direction[c]))
-                return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: conventional light with non-finite fields");
+                return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: conventional light with non-finite fields");
     }
     if (sn > 0xffffffffu || gn > 0xffffffffu)
-        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: word stream exceeds 2^32 words");
+        return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: word stream exceeds 2^32 words");
     // Header (src/scene.rs:2103-2110): material end, instance base, count, stride.
     uint32_t inst_base = sw[1], inst_count = sw[2], stride = sw[3];
     if (stride != 9u || (uint64_t)inst_base + (uint64_t)inst_count * 9u > sn)
-        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance records outside the scene words");
+        return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: instance records outside the scene words");
     if (inst_count > kLeafFirstMask)
-        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: too many instances");
+        return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: too many instances");
     uint32_t node_words = inst_base - 1u;
     uint32_t node_count = node_words / 2u;
     std::vector<BinNode> bin(node_count);
@@ -351,9 +386,10 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     // Geometry header (src/scene.rs:809-823).
     uint32_t tri_word = gw[0], vertex_base = gw[1], vertex_stride = gw[2], vertex_count = gw[3];
     if (tri_word != 1u || vertex_stride != 5u || vertex_base < 1u || (uint64_t)vertex_base + (uint64_t)vertex_count * 5u > gn)
-        return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: malformed geometry header");
+        return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: malformed geometry header");
     uint32_t tri_capacity = vertex_base - 1u;
-    std::vector<DeviceInstance> inst(inst_count);
+    std::vector<DeviceInstance> &inst = H.inst;
+    inst.assign(inst_count, DeviceInstance{});
     uint32_t tri_count = 0;
     for (uint32_t i = 0; i < inst_count; ++i) {
         const uint32_t *w = sw + 4 * (size_t)(inst_base + 9 * i);
@@ -365,21 +401,21 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
         inst[i].count = w[4 * 8 + 2];
         inst[i].root = w[4 * 8 + 0];
         if ((uint64_t)inst[i].first + inst[i].count > tri_capacity)
-            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance triangle range outside geometry");
+            return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: instance triangle range outside geometry");
         if (inst[i].root >= node_count)
-            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: instance BLAS root outside the node words");
+            return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: instance BLAS root outside the node words");
         if ((uint64_t)material + 8 > sn)
-            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: material record outside the scene words");
+            return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: material record outside the scene words");
         const uint32_t *m = sw + 4 * (size_t)material;
         float cutoff;
         std::memcpy(&cutoff, &m[7], 4);
         if (cutoff != -1.0f)
-            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
+            return fail(LUX_ERR_MALFORMED_SCENE,
                             "scene upload: alpha-tested materials are not supported by this build");
         const uint32_t *tex = m + 4 * 6;
         if (tex[0] != lux::kEmpty || tex[1] != lux::kEmpty || tex[2] != lux::kEmpty || tex[3] != lux::kEmpty ||
             m[4 * 7] != lux::kEmpty)
-            return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE,
+            return fail(LUX_ERR_MALFORMED_SCENE,
                             "scene upload: textured materials are not supported by this build");
         tri_count = std::max(tri_count, inst[i].first + inst[i].count);
     }
@@ -419,17 +455,15 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
         b.count = 1;
     }
     // Collapse: TLAS from node 0, every distinct BLAS root once.
-    std::vector<Bvh4Node> nodes;
+    std::vector<uint8_t> seen(node_count, 0);
     nodes.reserve(node_count / 2 + 16);
-    uint32_t tlas_root = lux::kEmpty;
-    float root_lo[3] = {0, 0, 0}, root_hi[3] = {0, 0, 0};
-    std::vector<uint2> slot_source;
-    std::vector<uint32_t> refit_order, depth_start;
+    uint32_t &tlas_root = H.tlas_root;
+    float *root_lo = H.root_lo, *root_hi = H.root_hi;
     if (inst_count > 0) {
-        if (node_count == 0) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: no TLAS nodes");
-        Collapser tl{bin, nodes, {}, inst_count, &inst_box, &slot_source};
+        if (node_count == 0) return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: no TLAS nodes");
+        Collapser tl{bin, nodes, {}, inst_count, &inst_box, &slot_source, &seen};
         tlas_root = tl.root(0);
-        if (!tl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (TLAS): " + tl.error);
+        if (!tl.error.empty()) return fail(LUX_ERR_MALFORMED_SCENE, "scene upload (TLAS): " + tl.error);
         for (int k = 0; k < 3; ++k) {
             root_lo[k] = bin[0].mn[k];
             root_hi[k] = bin[0].mx[k];
@@ -460,20 +494,21 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     for (uint32_t i = 0; i < inst_count; ++i) {
         auto it = blas_root.find(inst[i].root);
         if (it == blas_root.end()) {
-            Collapser bl{bin, nodes, {}, tri_count};
+            Collapser bl{bin, nodes, {}, tri_count, nullptr, nullptr, &seen};
             uint32_t r = bl.root(inst[i].root);
-            if (!bl.error.empty()) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload (BLAS): " + bl.error);
+            if (!bl.error.empty()) return fail(LUX_ERR_MALFORMED_SCENE, "scene upload (BLAS): " + bl.error);
             it = blas_root.emplace(inst[i].root, r).first;
         }
         inst[i].root = it->second;
     }
     // Triangle positions in packed (leaf) order.
-    std::vector<float4> tris(3 * (size_t)std::max(tri_count, 1u));
+    std::vector<float4> &tris = H.tris;
+    tris.assign(3 * (size_t)std::max(tri_count, 1u), float4{});
     for (uint32_t t = 0; t < tri_count; ++t) {
         const uint32_t *idx = gw + 4 * (size_t)(1 + t);
         for (int v = 0; v < 3; ++v) {
             uint32_t vi = idx[v];
-            if (vi >= vertex_count) return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: vertex index out of range");
+            if (vi >= vertex_count) return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: vertex index out of range");
             const uint32_t *p = gw + 4 * ((size_t)vertex_base + (size_t)vi * 5u);
             float4 f;
             std::memcpy(&f.x, &p[0], 4);
@@ -486,8 +521,46 @@ extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size
     if (light_count > conventional) {
         for (uint32_t l = conventional; l < light_count; ++l)
             if (lights[l].source[0] >= inst_count || lights[l].source[1] >= tri_capacity)
-                return lux_fail(ctx, LUX_ERR_MALFORMED_SCENE, "scene upload: emitter record outside the scene");
+                return fail(LUX_ERR_MALFORMED_SCENE, "scene upload: emitter record outside the scene");
     }
+    H.inst_base = inst_base;
+    H.inst_count = inst_count;
+    H.tri_count = tri_count;
+    H.tlas_slots = tlas_slots;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_scene_validate(const uint32_t *sw, size_t sn, const uint32_t *gw, size_t gn,
+                                         const LuxLight *lights, uint32_t light_count, uint32_t conventional,
+                                         char *message, size_t message_size) {
+    HostScene H;
+    std::string text;
+    lux_status status = prepare_scene(sw, sn, gw, gn, lights, light_count, conventional, H, text);
+    if (message && message_size) {
+        size_t n = std::min(text.size(), message_size - 1);
+        std::memcpy(message, text.data(), n);
+        message[n] = '\0';
+    }
+    return status;
+}
+
+extern "C" lux_status lux_scene_upload(LuxContext *ctx, const uint32_t *sw, size_t sn, const uint32_t *gw, size_t gn,
+                                       const LuxLight *lights, uint32_t light_count, uint32_t conventional,
+                                       LuxScene **out) {
+    if (!ctx || !out) return LUX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    HostScene H;
+    std::string message;
+    lux_status prep = prepare_scene(sw, sn, gw, gn, lights, light_count, conventional, H, message);
+    if (prep != LUX_OK) return lux_fail(ctx, prep, message);
+    const std::vector<Bvh4Node> &nodes = H.nodes;
+    const std::vector<float4> &tris = H.tris;
+    const std::vector<DeviceInstance> &inst = H.inst;
+    const std::vector<uint2> &slot_source = H.slot_source;
+    const std::vector<uint32_t> &refit_order = H.refit_order, &depth_start = H.depth_start;
+    const uint32_t tlas_root = H.tlas_root, inst_base = H.inst_base, inst_count = H.inst_count;
+    const uint32_t tri_count = H.tri_count, tlas_slots = H.tlas_slots;
+    const float *root_lo = H.root_lo, *root_hi = H.root_hi;
     LuxScene *S = new LuxScene();
     S->ctx = ctx;
     auto alloc_copy = [&](void **dst, const void *src, size_t bytes) -> bool {

@@ -1912,14 +1912,8 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.ts.queue_result, (size_t)d.max_rays * lux::kMaxNeeSamples},
         {(void **)&D.ts.queue_count, 16},
         {(void **)&D.ts.work_counter, 16},
-        {(void **)&D.sort_keys, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
-        {(void **)&D.sort_perm, (size_t)d.max_rays * lux::kMaxNeeSamples * sizeof(uint32_t)},
-        {(void **)&D.sort_hist, (size_t)kSortBins * sizeof(uint32_t)},
-        {(void **)&D.sort_offs, (size_t)kSortBins * sizeof(uint32_t)},
-        {(void **)&D.scan_temp, scan_temp_bytes()},
     };
     D.order_temp_bytes = order_temp_bytes(d.max_receivers);
-    D.scan_temp_bytes = scan_temp_bytes();
     for (auto &a : allocs) {
         if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
             cudaGetLastError();
@@ -1930,6 +1924,36 @@ static lux_status view_alloc(LuxView *v) {
     cudaMemsetAsync(D.stats, 0, 128, ctx->stream);
     cudaMemsetAsync(D.cell_count, 0, L * 4, ctx->stream);
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "view allocation");
+}
+
+// Coherence-sort buffers (keys and permutation per ray or query, the 2^24-bin
+// histogram and its offsets, the scan scratch: about 8 x max_rays x 16 B +
+// 128 MiB), allocated when a frame of the view first runs with sort_rays or
+// sort_queries set; views that never sort do not hold them.
+static lux_status ensure_sort_buffers(LuxView *v) {
+    ViewDevice &D = v->dev;
+    if (D.sort_hist) return LUX_OK;
+    const size_t items = (size_t)v->desc.max_rays * lux::kMaxNeeSamples;
+    D.scan_temp_bytes = scan_temp_bytes();
+    struct A {
+        void **p;
+        size_t bytes;
+    } allocs[] = {
+        {(void **)&D.sort_keys, items * sizeof(uint32_t)},
+        {(void **)&D.sort_perm, items * sizeof(uint32_t)},
+        {(void **)&D.sort_offs, (size_t)kSortBins * sizeof(uint32_t)},
+        {(void **)&D.scan_temp, D.scan_temp_bytes},
+        {(void **)&D.sort_hist, (size_t)kSortBins * sizeof(uint32_t)},  // last: marks the set complete
+    };
+    for (auto &a : allocs) {
+        if (*a.p) continue;
+        if (cudaMalloc(a.p, std::max<size_t>(a.bytes, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            *a.p = nullptr;
+            return lux_fail(v->ctx, LUX_ERR_OUT_OF_MEMORY, "view: coherence-sort buffer allocation failed");
+        }
+    }
+    return LUX_OK;
 }
 
 extern "C" lux_status lux_view_create(LuxContext *ctx, const LuxViewDesc *desc, LuxView **out) {
@@ -2373,6 +2397,10 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
     if (v->cache_alloc && v->cache.cutoff_level < F.levels) F.lod_enabled = 0;  // learned-cache frames: LOD 0
     if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > v->desc.max_rays)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: receivers x rays_per_receiver exceeds max_rays");
+    if (F.layout == LUX_LAYOUT_SPLIT && (v->tuning.sort_rays || v->tuning.sort_queries)) {
+        lux_status sb = ensure_sort_buffers(v);  // before any work of the frame is queued
+        if (sb != LUX_OK) return sb;
+    }
     const ViewDevice &D = v->dev;
     cudaStream_t st = ctx->stream;
     const float4 *pos = (const float4 *)rc->position;
@@ -2713,6 +2741,7 @@ extern "C" lux_status lux_view_set_tuning(LuxView *v, const LuxTuning *t) {
         (t->stack_depth != 0 && t->stack_depth != 32 && t->stack_depth != 64))
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_tuning: value out of range");
     v->tuning = *t;
+    if (t->sort_queries || t->sort_rays) return ensure_sort_buffers(v);
     return LUX_OK;
 }
 
@@ -2868,11 +2897,17 @@ extern "C" lux_status lux_interval_radiance_noalloc(LuxContext *ctx, const LuxSc
         std::lock_guard<std::mutex> lock(g_noalloc_mutex);
         base = g_noalloc_address[ctx->device];
         if (!base) {
-            lux_status s = lux_cuda_check(ctx, (int)cudaSetDevice(ctx->device), "interval_radiance_noalloc set device");
+            // The caller's current device is put back afterwards, so a render
+            // thread working on another device does not see it change.
+            int previous = -1;
+            lux_status s = lux_cuda_check(ctx, (int)cudaGetDevice(&previous), "interval_radiance_noalloc get device");
+            if (s != LUX_OK) return s;
+            s = lux_cuda_check(ctx, (int)cudaSetDevice(ctx->device), "interval_radiance_noalloc set device");
             if (s != LUX_OK) return s;
             void *address = nullptr;
             s = lux_cuda_check(ctx, (int)cudaGetSymbolAddress(&address, g_noalloc_scratch),
                                "interval_radiance_noalloc scratch address");
+            if (previous != ctx->device) cudaSetDevice(previous);
             if (s != LUX_OK) return s;
             base = (unsigned char *)address;
             g_noalloc_address[ctx->device] = base;

@@ -255,6 +255,16 @@ lux_status lux_scene_upload(LuxContext *ctx,
                             const LuxLight *lights, uint32_t light_count,
                             uint32_t conventional_lights,
                             LuxScene **out);
+/* The host half of lux_scene_upload without a device: the same validation of
+ * the word streams and the same BVH4 collapse, returning the status the
+ * upload would return (LUX_ERR_MALFORMED_SCENE for cycles, shared subtrees,
+ * out-of-range indices or oversized leaves -- the reference's malformed BLAS
+ * fixtures, src/traversal_tests.rs:1594-1636 -- in time linear in the node
+ * count).  message: optional, receives the upload's error text. */
+lux_status lux_scene_validate(const uint32_t *scene_words, size_t scene_word_count,
+                              const uint32_t *geometry_words, size_t geometry_word_count,
+                              const LuxLight *lights, uint32_t light_count,
+                              uint32_t conventional_lights, char *message, size_t message_size);
 lux_status lux_scene_destroy(LuxScene *scene);
 /* Device BVH4 size facts: nodes (TLAS+BLAS) and node/triangle record bytes. */
 lux_status lux_scene_layout(const LuxScene *scene, uint32_t *nodes, uint32_t *node_bytes,
@@ -308,8 +318,9 @@ lux_status lux_interval_radiance(LuxContext *ctx, const LuxScene *scene, const L
  *  - At most 8192 rays per call; larger counts fail with LUX_ERR_CAPACITY
  *    before any work is queued.  Split bigger batches.
  *  - The first call on a device looks up the array's device address (with
- *    that device made current); make that first call before any stream
- *    capture on the device.
+ *    that device made current, and the caller's current device restored
+ *    afterwards); make that first call before any stream capture on the
+ *    device.
  *  - All calls share the one array.  Each call resets the counters it needs
  *    and overwrites the rest, but calls whose GPU work overlaps (different
  *    streams or contexts on the same device) race: order them. */

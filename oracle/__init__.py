@@ -75,6 +75,7 @@ def lib():
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
+            "orc_frame_read_hits": (C.c_uint64, [P, P, C.c_uint64]),
             "orc_frame_read_level": (None, [P, U, P, P, P, P]),
             "orc_frame_read_probes": (None, [P, P]),
             "orc_frame_stats": (None, [P, P]),
@@ -93,6 +94,11 @@ def lib():
             fn.argtypes = args
         _lib = h
     return _lib
+
+
+# LuxHit (include/lux.h) as a numpy record.
+HIT_DTYPE = np.dtype([("distance", "<f4"), ("triangle", "<u4"), ("instance", "<u4"), ("errors", "<u4"),
+                      ("barycentric", "<f4", (3,)), ("visited", "<u4")])
 
 
 def _p(a: np.ndarray) -> int:
@@ -121,7 +127,6 @@ class OracleScene:
 
     def trace_rays(self, rays: np.ndarray, any_hit: bool = False, threads: int = 0):
         """rays: structured RAY_DTYPE array -> HIT_DTYPE array, counters."""
-        from bevy_penumbra_b200 import HIT_DTYPE  # record layout only
         rays = np.ascontiguousarray(rays)
         hits = np.zeros(len(rays), dtype=HIT_DTYPE)
         cn = Counters()
@@ -216,6 +221,13 @@ class OracleFrame:
         if cells:
             lib().orc_frame_read_level(self.handle, level, _p(keys), _p(merged), _p(raw), _p(samples))
         return keys, merged, raw, samples
+
+    def hits(self, count: int) -> np.ndarray:
+        """Closest hits of the frame's interval rays (Split layout), as the
+        LuxHit records of lux_view_read_hits."""
+        out = np.zeros(count, dtype=HIT_DTYPE)
+        n = lib().orc_frame_read_hits(self.handle, _p(out), count)
+        return out[:n]
 
     def probes(self):
         cells = lib().orc_frame_cells(self.handle, 0)

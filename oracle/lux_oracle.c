@@ -1663,6 +1663,8 @@ struct OrcFrame {
     const struct OrcFrame *previous;  /* history source (NULL: none) */
     const float *dirty;               /* invalidation boxes, 6 floats each */
     uint32_t dirty_count;
+    LuxHit *hits;                     /* split: the closest hit of every interval ray, ray order */
+    uint64_t hit_count;
 };
 
 static int64_t find_cell(const Level *L, const int32_t key[4]) {
@@ -1750,6 +1752,7 @@ typedef struct {
     /* split: per ray outputs */
     int32_t *term_level;  /* -1 = unsupported */
     float *radiance;      /* rgb per ray */
+    LuxHit *hits;         /* closest hit per ray */
     uint32_t *ubin;       /* flipped (u, v) stored as bits */
     float *uv;
     /* dense */
@@ -1789,12 +1792,16 @@ static void *split_job(void *arg) {
         const float *p = j->pos + 4 * (size_t)i, *n = j->nrm + 4 * (size_t)i;
         if (j->sparse && p[3] == 0.0f) {
             j->term_level[ray] = -2;  /* absent receiver: no ray */
+            memset(&j->hits[ray], 0, sizeof(LuxHit));
+            j->hits[ray].triangle = j->hits[ray].instance = EMPTY;
+            j->hits[ray].errors = HIT_QUERY_UNSUPPORTED;
             continue;
         }
         float uv[2], origin[3], dir[3];
         LuxHit hit;
         split_ray(j->S, st, p, n, j->ordinal[i] * R + k, uv, &hit, origin, dir);
         orc_trace_closest(j->S, origin, dir, 0.0f, 1e20f, &hit, &j->cn);
+        j->hits[ray] = hit;
         float rad[3], rec[7];
         int supported = outgoing_radiance(j->S, st, j->bounce, origin, dir, &hit, rad, rec, &j->shadow, &j->cn);
         if (j->hit_pos && rec[6] != 0.0f && k == st->frame_index % R) {
@@ -2398,6 +2405,9 @@ OrcFrame *orc_frame_run_bounce(const OrcScene *S, const LuxSettings *st_in, cons
         proto.term_level = (int32_t *)malloc(sizeof(int32_t) * (rays ? rays : 1));
         proto.radiance = (float *)malloc(sizeof(float) * 3 * (rays ? rays : 1));
         proto.uv = (float *)malloc(sizeof(float) * 2 * (rays ? rays : 1));
+        F->hits = (LuxHit *)malloc(sizeof(LuxHit) * (rays ? rays : 1));
+        F->hit_count = rays;
+        proto.hits = F->hits;
         run_jobs(&proto, rays, threads, split_job, &shadow, &cn);
         uint64_t present_rays = rays;
         /* deposit, shaders/split.slang:1056-1117, then the per-key mean of
@@ -2478,7 +2488,14 @@ void orc_frame_destroy(OrcFrame *F) {
         free(F->level[l].last);
     }
     free(F->tables);
+    free(F->hits);
     free(F);
+}
+
+uint64_t orc_frame_read_hits(const OrcFrame *F, LuxHit *out, uint64_t count) {
+    uint64_t n = count < F->hit_count ? count : F->hit_count;
+    if (n) memcpy(out, F->hits, sizeof(LuxHit) * n);
+    return n;
 }
 
 uint32_t orc_frame_cells(const OrcFrame *F, uint32_t level) { return level < F->levels ? F->level[level].cells : 0; }

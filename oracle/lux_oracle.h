@@ -166,6 +166,9 @@ OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
                         const float *receiver_position, const float *receiver_normal,
                         uint32_t receiver_count, int threads);
 void orc_frame_destroy(OrcFrame *frame);
+/* Split frames: the closest hit of each interval ray (receiver i, ray k at
+ * index i x rays_per_receiver + k); returns the records copied. */
+uint64_t orc_frame_read_hits(const OrcFrame *frame, LuxHit *out, uint64_t count);
 uint32_t orc_frame_cells(const OrcFrame *frame, uint32_t level);
 /* cell keys int4[cells] sorted ascending; merged/raw float4[cells*dirs];
  * samples uint32[cells*dirs]; any pointer may be NULL. */

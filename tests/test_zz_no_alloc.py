@@ -68,3 +68,30 @@ def test_no_alloc_rejects_batches_above_its_capacity():
                                                    MAX_RAYS + 1, d_out.data_ptr())
     assert status == 4  # LUX_ERR_CAPACITY, refused before any launch
     assert b"8192" in N.lib().lux_last_error_message(ctx.handle)
+
+
+def test_no_alloc_calls_leave_free_device_memory_unchanged():
+    """The property the entry point exists for: once its kernels are loaded,
+    a call takes no device memory.  Every buffer the calls use is allocated
+    before the first reading; the allocating entry point is not called
+    between the readings."""
+    import torch
+
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    lib = N.lib()
+    s = bp.RadianceCascades(probe_spacing=0.25, emissive_samples=16, frame_index=7).sanitized().to_c()
+    rays = rays_in_box(MAX_RAYS, seed=11)
+    d_rays = to_device(rays)
+    d_out = empty_device(MAX_RAYS * 16)
+    # Warm-up: loads the kernels and looks up the scratch array's address.
+    ctx.check(lib.lux_interval_radiance_noalloc(ctx.handle, scene.handle, C.byref(s), d_rays.data_ptr(), 64,
+                                                d_out.data_ptr()))
+    ctx.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    for n in (MAX_RAYS, 1000):
+        ctx.check(lib.lux_interval_radiance_noalloc(ctx.handle, scene.handle, C.byref(s), d_rays.data_ptr(), n,
+                                                    d_out.data_ptr()))
+    ctx.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after == free_before
