@@ -59,12 +59,21 @@ def launches_per_frame(levels: int, sort_queries: bool) -> int:
     return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (4 if sort_queries else 0)
 
 
-def settings_for_workload():
+def settings_for_workload(sanitize: bool = True):
+    """The workload's cascade settings.  sanitize=False skips liblux's
+    RadianceCascades::sanitized() (the values are already in range; a test
+    checks both give the same record), for the CPU arm, which loads no part
+    of the library."""
     import bevy_penumbra_b200 as bp
-    return bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=8, base_columns=8, base_rows=4,
-                               interval_ratio=2.0, interval_rule=bp.INTERVAL_ENDS_GEOMETRIC,
-                               layout=bp.LAYOUT_SPLIT, rays_per_receiver=RAYS_PER_RECEIVER,
-                               emissive_samples=16).sanitized()
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=8, base_columns=8, base_rows=4,
+                            interval_ratio=2.0, interval_rule=bp.INTERVAL_ENDS_GEOMETRIC,
+                            layout=bp.LAYOUT_SPLIT, rays_per_receiver=RAYS_PER_RECEIVER, emissive_samples=16)
+    return s.sanitized() if sanitize else s
+
+
+def direction_count(settings, level: int) -> int:
+    """Directions of a level: (base_columns x base_rows) x 4^level."""
+    return (settings.base_columns * settings.base_rows) << (2 * level)
 
 
 def world_normals(packed, hits, dirs):
@@ -90,14 +99,20 @@ def world_normals(packed, hits, dirs):
 def build_workload(device: int = 0, host_only: bool = False):
     """Scene, receivers and resolve points (primary hits of the camera).
 
-    host_only: the reference arm finds the primary hits with the CPU oracle
-    and touches no GPU code (the hits are bit-identical either way)."""
+    host_only: the reference arm packs the scene with the oracle's packer and
+    finds the primary hits with the CPU oracle, so it loads nothing of
+    liblux (the words and hits are bit-identical either way)."""
     import bevy_penumbra_b200 as bp
     from bevy_penumbra_b200 import scenes
 
     t0 = time.time()
     desc = scenes.atrium(seed=2, triangles=TRIANGLES)
-    packed = bp.PackedScene.from_desc(desc)
+    if host_only:
+        import oracle
+        packed = oracle.OraclePacked.from_desc(desc)
+        oscene = oracle.OracleScene.from_packed(packed)
+    else:
+        packed = bp.PackedScene.from_desc(desc)
     ctx = scene = None
     if not host_only:
         import torch
@@ -112,8 +127,7 @@ def build_workload(device: int = 0, host_only: bool = False):
         rays["direction"] = d
         rays["limit"] = 1e20
         if host_only:
-            import oracle
-            hits, _ = oracle.OracleScene.from_packed(packed).trace_rays(rays)
+            hits, _ = oscene.trace_rays(rays)
         else:
             import torch
             d_rays = torch.from_numpy(rays.view(np.uint8).copy()).to(f"cuda:{device}")
@@ -134,11 +148,8 @@ def build_workload(device: int = 0, host_only: bool = False):
         return pos, nrm, screen
 
     rpos, rnrm, _ = primary(PROBE_PX)
-    if host_only:
-        ppos, pnrm, pscreen = rpos[:0], rnrm[:0], None
-    else:
-        ppos, pnrm, pscreen = primary(1)
-    settings = settings_for_workload()
+    ppos, pnrm, pscreen = primary(1)
+    settings = settings_for_workload(sanitize=not host_only)
     # Exact record counts per level (cells holding a receiver x directions).
     entries = 0
     cells_max = 0
@@ -146,7 +157,7 @@ def build_workload(device: int = 0, host_only: bool = False):
         s = np.float32(settings.probe_spacing * (1 << level))
         cells = np.unique(np.floor(rpos[:, :3] / s).astype(np.int64), axis=0).shape[0]
         cells_max = max(cells_max, cells)
-        entries += cells * settings.direction_count(level)
+        entries += cells * direction_count(settings, level)
     view = None if host_only else bp.SplitView(ctx, max_receivers=len(rpos), max_cells=cells_max,
                                                max_entries=entries,
                                                max_rays=len(rpos) * settings.rays_per_receiver)
@@ -279,47 +290,66 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def cpu_sample(w, fraction_receivers: int, threads: int):
-    """The oracle (CPU restatement) on every `fraction_receivers`-th receiver."""
+# The CPU sample: every CPU_STRIDE-th receiver traced and merged, and every
+# CPU_STRIDE-th resolve point resolved, by the oracle on all host threads
+# (about 1.2 s of CPU time per sample on 16 threads).
+CPU_STRIDE = 16
+
+
+def cpu_sample(w, stride: int, threads: int):
+    """One frame of the oracle (the CPU restatement of the reference's shader
+    math) on every `stride`-th receiver, then the resolve of every
+    `stride`-th resolve point from that frame's probes; timed together."""
     import oracle
 
-    rpos = np.ascontiguousarray(w["rpos"][::fraction_receivers])
-    rnrm = np.ascontiguousarray(w["rnrm"][::fraction_receivers])
-    oscene = oracle.OracleScene.from_packed(w["packed"])
+    rpos = np.ascontiguousarray(w["rpos"][::stride])
+    rnrm = np.ascontiguousarray(w["rnrm"][::stride])
+    ppos = np.ascontiguousarray(w["ppos"][::stride])
+    pnrm = np.ascontiguousarray(w["pnrm"][::stride])
+    oscene = w.get("oscene") or oracle.OracleScene.from_packed(w["packed"])
     settings = w["settings"]
     t0 = time.perf_counter()
     frame = oracle.OracleFrame(oscene, settings.to_c(), rpos, rnrm, threads=threads)
+    frame.resolve(ppos, pnrm)
     dt = time.perf_counter() - t0
-    st = frame.stats()
-    rays = int(st.interval_rays)
+    rays = int(frame.stats().interval_rays)
     frame.close()
-    return rays, dt, len(rpos)
+    return {"rays": rays, "seconds": dt, "receivers": len(rpos), "points": len(ppos)}
+
+
+def cpu_sample_text(sample, w, stride):
+    full_rays = len(w["rpos"]) * RAYS_PER_RECEIVER
+    return (f"every {stride}th receiver ({sample['receivers']} receivers, {sample['rays']} of {full_rays} "
+            f"interval rays) traced and merged, and every {stride}th resolve point ({sample['points']} of "
+            f"{len(w['ppos'])}) resolved, per step; ms_per_step is the measured sample time")
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the CPU restatement on the host cores."""
+    """--impl reference: the CPU restatement on the host cores.  Loads no
+    part of liblux: the oracle packs the scene, finds the primary hits and
+    runs every frame."""
     if rank != 0:
         return
+    import oracle
+
     w = build_workload(0, host_only=True)
+    w["oscene"] = oracle.OracleScene.from_packed(w["packed"])
     threads = os.cpu_count() or 1
-    stride = 64
-    for _ in range(max(args.warmup, 0) and 1):
-        cpu_sample(w, stride * 4, threads)
-    times, rays_done = [], 0
+    for _ in range(max(args.warmup, 0)):
+        cpu_sample(w, CPU_STRIDE, threads)
+    times, sample = [], None
     for _ in range(args.steps):
-        rays, dt, n = cpu_sample(w, stride, threads)
-        times.append(dt)
-        rays_done = rays
-    dt = float(np.median(times))
-    full_rays = len(w["rpos"]) * RAYS_PER_RECEIVER
-    mrays = rays_done / dt / 1e6
+        sample = cpu_sample(w, CPU_STRIDE, threads)
+        times.append(sample["seconds"])
+    dt = float(np.sum(times)) / max(args.steps, 1)
+    mrays = sample["rays"] / dt / 1e6
     line = {
         "impl": "reference", "metric": METRIC, "value": mrays, "unit": "Mrays/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3 * full_rays / rays_done,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(w),
         "cpu_baseline": {"value": mrays, "unit": "Mrays/s", "cores": threads, "kind": "port",
-                         "sample": f"every {stride}th receiver ({rays_done} interval rays of {full_rays}) per step"},
+                         "sample": cpu_sample_text(sample, w, CPU_STRIDE)},
         "e2e": {"value": mrays, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -624,7 +654,7 @@ def run_ours(args, rank, world):
                      + int(st.instances_visited) * 64)
         trace_s = float(np.median(trace_ms)) * 1e-3
         achieved = alg_bytes / trace_s / 1e9
-        cpu_rays, cpu_dt, cpu_recv = cpu_sample(w, 64, os.cpu_count() or 1)
+        cpu = cpu_sample(w, CPU_STRIDE, os.cpu_count() or 1)
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
@@ -651,9 +681,9 @@ def run_ours(args, rank, world):
                          "traffic_note": "ncu dram bytes of the traversal kernels per frame, scaled by rays from "
                                          "the 65,536-triangle capture; the scene stays in L2",
                          "algorithmic_bytes": alg_bytes},
-            "cpu_baseline": {"value": cpu_rays / cpu_dt / 1e6, "unit": "Mrays/s", "cores": os.cpu_count(),
-                             "kind": "port",
-                             "sample": f"every 64th receiver ({cpu_recv} receivers, {cpu_rays} interval rays)"},
+            "cpu_baseline": {"value": cpu["rays"] / cpu["seconds"] / 1e6, "unit": "Mrays/s",
+                             "cores": os.cpu_count(), "kind": "port",
+                             "sample": cpu_sample_text(cpu, w, CPU_STRIDE)},
             "e2e": {"value": e2e_value, "unit": "Mrays/s", "ms_per_step": e2e_total / args.steps,
                     "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
                     "d2h_bytes_per_step": int(n_pts * 16)},

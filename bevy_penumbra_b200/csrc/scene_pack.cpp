@@ -162,9 +162,20 @@ void build_node(std::vector<BinNode> &nodes, size_t index, BuildElement *e, size
     } else {
         float size[3] = {cmax[0] - cmin[0], cmax[1] - cmin[1], cmax[2] - cmin[2]};
         int axis = (size[0] >= size[1] && size[0] >= size[2]) ? 0 : (size[1] >= size[2] ? 1 : 2);
+        // select_nth_unstable_by(total_cmp) leaves the order inside each half
+        // unspecified; a stable sort by the same total order fixes it (equal
+        // centroids keep their current order), so the oracle's packer can
+        // restate the result exactly.  The binned search above finds a split
+        // whenever two centroids differ, so in practice this runs on
+        // coincident centroids and keeps the range as it is.
         mid = len / 2;
-        std::nth_element(e, e + mid, e + len, [axis](const BuildElement &a, const BuildElement &b) {
-            return center_of(a.box, axis) < center_of(b.box, axis);
+        auto total = [](float f) {
+            int32_t i;
+            std::memcpy(&i, &f, 4);
+            return i ^ (int32_t)((uint32_t)(i >> 31) >> 1);
+        };
+        std::stable_sort(e, e + len, [axis, &total](const BuildElement &a, const BuildElement &b) {
+            return total(center_of(a.box, axis)) < total(center_of(b.box, axis));
         });
     }
     size_t children = nodes.size();

@@ -16,9 +16,8 @@ LIB = os.path.join(HERE, "liblux_oracle.so")
 
 
 def build(force: bool = False) -> str:
-    src = os.path.join(HERE, "lux_oracle.c")
-    hdr = os.path.join(HERE, "lux_oracle.h")
-    if force or not os.path.exists(LIB) or max(os.path.getmtime(src), os.path.getmtime(hdr)) > os.path.getmtime(LIB):
+    sources = [os.path.join(HERE, n) for n in ("lux_oracle.c", "orc_pack.c", "lux_oracle.h")]
+    if force or not os.path.exists(LIB) or max(os.path.getmtime(s) for s in sources) > os.path.getmtime(LIB):
         subprocess.run(["make", "-s", "-C", HERE, "-B" if force else "liblux_oracle.so"], check=True)
     return LIB
 
@@ -75,6 +74,10 @@ def lib():
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
+            "orc_scene_pack": (C.c_int, [P, U, P, U, P, P, U, P, P, P, P, U, P, U, P]),
+            "orc_packed_sizes": (None, [P, P, P, P, P, P, P, P]),
+            "orc_packed_copy": (None, [P, P, P, P, P, U]),
+            "orc_packed_destroy": (None, [P]),
             "orc_frame_read_hits": (C.c_uint64, [P, P, C.c_uint64]),
             "orc_frame_read_level": (None, [P, U, P, P, P, P]),
             "orc_frame_read_probes": (None, [P, P]),
@@ -107,6 +110,51 @@ def _p(a: np.ndarray) -> int:
 
 def f32(*v) -> np.ndarray:
     return np.ascontiguousarray(np.array(v, dtype=np.float32).ravel())
+
+
+class OraclePacked:
+    """The oracle packer's word streams (orc_scene_pack): the attributes of
+    bevy_penumbra_b200.PackedScene, built without liblux."""
+
+    def __init__(self, positions, indices, mesh_first, mesh_count, instance_mesh, instance_transform,
+                 instance_flags, instance_material, materials):
+        a = lambda x, t: np.ascontiguousarray(x, dtype=t)
+        positions = a(positions, np.float32).reshape(-1, 3)
+        indices = a(indices, np.uint32).reshape(-1, 3)
+        mesh_first, mesh_count = a(mesh_first, np.uint32), a(mesh_count, np.uint32)
+        imesh, iflags, imat = a(instance_mesh, np.uint32), a(instance_flags, np.uint32), a(instance_material, np.uint32)
+        ixf = a(instance_transform, np.float32).reshape(-1, 12)
+        mats = a(materials, np.uint32).reshape(-1, 32)
+        handle = C.c_void_p()
+        rc = lib().orc_scene_pack(_p(positions), len(positions), _p(indices), len(indices), _p(mesh_first),
+                                  _p(mesh_count), len(mesh_first), _p(imesh), _p(ixf), _p(iflags), _p(imat),
+                                  len(imesh), _p(mats), len(mats), C.byref(handle))
+        if rc != 0:
+            raise ValueError("oracle packer: invalid scene")
+        try:
+            sw, gw = C.c_size_t(), C.c_size_t()
+            nl, tn, bn, depth = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
+            cost = C.c_double()
+            lib().orc_packed_sizes(handle, C.byref(sw), C.byref(gw), C.byref(nl), C.byref(tn), C.byref(bn),
+                                   C.byref(depth), C.byref(cost))
+            self.scene_words = np.zeros((sw.value, 4), np.uint32)
+            self.geometry_words = np.zeros((gw.value, 4), np.uint32)
+            self.lights = np.zeros((nl.value, 24), np.uint32)
+            self.instance_order = np.zeros(len(imesh), np.uint32)
+            lib().orc_packed_copy(handle, _p(self.scene_words), _p(self.geometry_words), _p(self.lights),
+                                  _p(self.instance_order), len(imesh))
+        finally:
+            lib().orc_packed_destroy(handle)
+        self.tlas_nodes, self.blas_nodes = tn.value, bn.value
+        self.max_depth, self.blas_cost = depth.value, cost.value
+        self.conventional = 0
+
+    @staticmethod
+    def from_desc(desc) -> "OraclePacked":
+        """A scene description of bevy_penumbra_b200.scenes (pure numpy)."""
+        positions, indices, first, count = desc.arrays()
+        return OraclePacked(positions, indices, first, count, desc.instance_mesh, np.stack(desc.instance_transform),
+                            desc.instance_flags, desc.instance_material, np.stack(desc.materials))
 
 
 class OracleScene:

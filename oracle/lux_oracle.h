@@ -166,6 +166,21 @@ OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
                         const float *receiver_position, const float *receiver_normal,
                         uint32_t receiver_count, int threads);
 void orc_frame_destroy(OrcFrame *frame);
+
+/* The oracle's scene packer (orc_pack.c): build_tree / node_words /
+ * pack_instances / geometry_words / build_emissive_lights restated in C.
+ * Inputs as lux_scene_pack; returns 0, or -1 for invalid input. */
+typedef struct OrcPacked OrcPacked;
+int orc_scene_pack(const float *positions, uint32_t vertex_count, const uint32_t *indices, uint32_t triangle_count,
+                   const uint32_t *mesh_first_triangle, const uint32_t *mesh_triangle_count, uint32_t mesh_count,
+                   const uint32_t *instance_mesh, const float *instance_world_from_local,
+                   const uint32_t *instance_flags, const uint32_t *instance_material, uint32_t instance_count,
+                   const uint32_t *material_words, uint32_t material_count, OrcPacked **out);
+void orc_packed_sizes(const OrcPacked *p, size_t *scene_words, size_t *geometry_words, uint32_t *lights,
+                      uint32_t *tlas_nodes, uint32_t *blas_nodes, uint32_t *max_depth, double *blas_cost);
+void orc_packed_copy(const OrcPacked *p, uint32_t *scene_words, uint32_t *geometry_words, LuxLight *lights,
+                     uint32_t *instance_order, uint32_t instance_count);
+void orc_packed_destroy(OrcPacked *p);
 /* Split frames: the closest hit of each interval ray (receiver i, ray k at
  * index i x rays_per_receiver + k); returns the records copied. */
 uint64_t orc_frame_read_hits(const OrcFrame *frame, LuxHit *out, uint64_t count);
