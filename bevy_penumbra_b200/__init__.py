@@ -769,6 +769,25 @@ class LearnedCache:
         self.ctx.check(lib().lux_cache_stats(self.handle, C.byref(out)))
         return out
 
+    def table_size(self) -> int:
+        return int(self.desc.levels) * (1 << int(self.desc.log2_table)) * 2
+
+    def gradients(self, samples_ptr: int, targets_ptr: int, count: int):
+        """lux_cache_gradients: (weight gradients as weights() layers, FP32
+        hash-table gradients [levels, 2^log2_table, 2]) of one pass, no step."""
+        w = np.zeros(CACHE_WEIGHTS, np.float32)
+        t = np.zeros(self.table_size(), np.float32)
+        self.ctx.check(lib().lux_cache_gradients(self.handle, samples_ptr, targets_ptr, count, _ptr(w), _ptr(t)))
+        layers = [w[k * 4096:(k + 1) * 4096].reshape(64, 64) for k in range(4)]
+        layers.append(w[4 * 4096:].reshape(16, 64))
+        return layers, t.reshape(int(self.desc.levels), -1, 2)
+
+    def table(self) -> np.ndarray:
+        """The FP32 master hash table [levels, 2^log2_table, 2]."""
+        t = np.zeros(self.table_size(), np.float32)
+        self.ctx.check(lib().lux_cache_read_table(self.handle, _ptr(t)))
+        return t.reshape(int(self.desc.levels), -1, 2)
+
     def close(self) -> None:
         if self.handle:
             lib().lux_cache_destroy(self.handle)

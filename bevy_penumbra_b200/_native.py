@@ -209,6 +209,8 @@ SIGNATURES = {
     "lux_cache_encode": (C.c_int, [P, P, U32, P]),
     "lux_cache_read_weights": (C.c_int, [P, P]),
     "lux_cache_forward": (C.c_int, [P, P, U32, P]),
+    "lux_cache_gradients": (C.c_int, [P, P, P, U32, P, P]),
+    "lux_cache_read_table": (C.c_int, [P, P]),
     "lux_batch_create": (C.c_int, [P, C.POINTER(P)]),
     "lux_batch_destroy": (C.c_int, [P]),
     "lux_batch_set_graph": (C.c_int, [P, U32]),

@@ -39,7 +39,13 @@ constexpr int kLevelsMax = 16;
 constexpr int kIn = 64, kHidden = 64, kOut = 16;
 constexpr int kHiddenLayers = 4;
 constexpr int kTile = 128;
-constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kTmemCols = 64;       // forward kernel: one [128][64] FP32 accumulator
+// Training kernel: the layer accumulator (columns 0-63) and the weight
+// gradients of the five layers, each an M = 64 accumulator of dW^T (rows =
+// layer inputs, columns = outputs): hidden layer l at columns 64 + 64 l, the
+// output layer (16 columns) at 320.
+constexpr uint32_t kTrainTmemCols = 512;
+constexpr uint32_t kGradCol0 = 64;
 constexpr int kWHidden = kHidden * kIn;                       // 4096 per hidden layer
 constexpr int kWTotal = kHiddenLayers * kWHidden + kOut * kIn;  // 17408
 constexpr int kPackedElems = 2 * kWTotal;                     // W and W^T packed
@@ -121,14 +127,14 @@ __device__ __forceinline__ void tmem_load16(uint32_t addr, float v[16]) {
 __device__ __forceinline__ void tmem_wait_load() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // TMEM allocation by warp 0 (address written to shared memory).
-__device__ __forceinline__ void tmem_alloc(uint32_t *slot) {
+__device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t cols = kTmemCols) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(slot)),
-                 "r"(kTmemCols)
+                 "r"(cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
 }
-__device__ __forceinline__ void tmem_free(uint32_t addr) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(addr), "r"(kTmemCols) : "memory");
+__device__ __forceinline__ void tmem_free(uint32_t addr, uint32_t cols = kTmemCols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(addr), "r"(cols) : "memory");
 }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar) {
@@ -417,38 +423,46 @@ struct SmemTrain {
     static constexpr uint32_t kBytes = kRed + 16;
 };
 
-// Weight-gradient partial sums of one layer from the shared tiles:
-// dW[o][i] += sum_b g[b][o] h[b][i], on the CUDA cores.
-template <int kOutDim>
-__device__ __forceinline__ void weight_grad(const bf16 *g, const bf16 *h, uint32_t tid, float *__restrict__ grad) {
-    constexpr int kPer = kOutDim * kIn / kTile;  // 32 (hidden) or 8 (output)
-    constexpr int kSplit = kIn / kPer;           // threads per output row
-    const uint32_t o = tid / kSplit, i0 = (tid % kSplit) * kPer;
-    float acc[kPer];
+// Weight gradient of one layer on the tensor cores: dW^T[i][o] += sum_b
+// h[b][i] g[b][o] over the tile's 128 samples, an M = 64 (inputs) x N (64 or
+// 16 outputs) x K = 128 (samples) chain.  Both operands are the activation
+// and gradient tiles as they are, read MN-major: in the packed [128][*] tiles
+// the feature index is contiguous inside an 8 x 8 core matrix, core matrices
+// along the features are kTile / 8 x 128 bytes apart (stride byte offset) and
+// along the samples 128 bytes apart (leading byte offset).  The accumulator
+// stays in TMEM across the CTA's tiles.
+__device__ __forceinline__ void issue_weight_grad(uint32_t tmem_col, uint32_t h_addr, uint32_t g_addr, uint32_t N,
+                                                  bool accumulate) {
+    const uint32_t lbo = 128u, sbo = (kTile / 8) * 128u;
+    const uint32_t idesc = idesc_bf16(64u, N) | (1u << 15) | (1u << 16);  // A and B MN-major
+    for (uint32_t ks = 0; ks < (uint32_t)kTile / 16u; ++ks)
+        mma_bf16(tmem_col, smem_desc(h_addr + ks * 2u * lbo, lbo, sbo), smem_desc(g_addr + ks * 2u * lbo, lbo, sbo),
+                 idesc, (accumulate || ks > 0u) ? 1u : 0u);
+}
+
+// Adds one layer's TMEM weight gradient to the FP32 gradient buffer.  The
+// M = 64 accumulator keeps row r in TMEM lane 32 (r / 16) + r % 16, so lanes
+// 0-15 of warp w hold rows 16 w .. 16 w + 15 (the layer inputs i).
+template <int kCols>
+__device__ __forceinline__ void flush_weight_grad(uint32_t lane_addr, uint32_t warp, uint32_t lane,
+                                                  float *__restrict__ grad) {
+    const uint32_t i = warp * 16u + lane;
 #pragma unroll
-    for (int j = 0; j < kPer; ++j) acc[j] = 0.0f;
-    for (uint32_t b = 0; b < (uint32_t)kTile; ++b) {
-        float gv = __bfloat162float(g[packed(b, o, kTile)]);
+    for (int c0 = 0; c0 < kCols; c0 += 16) {
+        float v[16];
+        tmem_load16(lane_addr + (uint32_t)c0, v);
+        tmem_wait_load();
+        if (lane < 16u) {
 #pragma unroll
-        for (int q = 0; q < kPer / 8; ++q) {
-            uint4 w = *reinterpret_cast<const uint4 *>(h + packed(b, i0 + q * 8u, kTile));
-            const __nv_bfloat162 *p = reinterpret_cast<const __nv_bfloat162 *>(&w);
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float2 f = __bfloat1622float2(p[e]);
-                acc[q * 8 + 2 * e] += gv * f.x;
-                acc[q * 8 + 2 * e + 1] += gv * f.y;
-            }
+            for (int c = 0; c < 16; ++c)
+                if (v[c] != 0.0f) atomicAdd(&grad[(uint32_t)(c0 + c) * kIn + i], v[c]);
         }
     }
-#pragma unroll
-    for (int j = 0; j < kPer; ++j)
-        if (acc[j] != 0.0f) atomicAdd(&grad[o * kIn + i0 + j], acc[j]);
 }
 
 // One training pass over `n` encoded samples: forward, relative L2 loss,
-// backward data gradients on the tensor cores, weight gradients on the CUDA
-// cores; dx = gradient of the hash features (first 32 inputs).
+// backward data gradients and weight gradients on the tensor cores; dx =
+// gradient of the hash features (first 32 inputs).
 __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restrict__ x, const float4 *__restrict__ target,
                                                            const LuxCacheSample *__restrict__ samples, uint32_t n,
                                                            float scale, const uint4 *__restrict__ weights,
@@ -463,7 +477,7 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restric
     uint32_t *slot = reinterpret_cast<uint32_t *>(smem + SmemTrain::kSlot);
     float *red = reinterpret_cast<float *>(smem + SmemTrain::kRed);
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    if (warp == 0) tmem_alloc(slot);
+    if (warp == 0) tmem_alloc(slot, kTrainTmemCols);
     if (tid == 0) mbar_init(bar);
     for (uint32_t i = tid; i < kPackedElems / 8; i += kTile) reinterpret_cast<uint4 *>(Wf)[i] = weights[i];
     sync_for_mma();
@@ -473,7 +487,7 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restric
     const uint32_t w_addr = smem_u32(Wf), h_addr = smem_u32(H), g_addr = smem_u32(G), d_addr = smem_u32(D);
     const uint32_t h_elems = kTile * kIn;
     uint32_t phase = 0;
-    bool ok = true;
+    bool ok = true, grads = false;  // grads: the TMEM weight gradients hold this CTA's sums
     float loss_sum = 0.0f;
     for (uint32_t tile = blockIdx.x; ok && tile * kTile < n; tile += gridDim.x) {
         const uint32_t row = tile * kTile + tid;
@@ -535,22 +549,21 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restric
             q.w = pack_bf16x2(gout[kg * 8 + 6], gout[kg * 8 + 7]);
             *reinterpret_cast<uint4 *>(D + packed(tid, (uint32_t)kg * 8u, kTile)) = q;
         }
-        // Backward, layer 4 down to 0: dh_l = g_l W_l (tensor cores, from the
-        // packed W_l^T), dW_l = g_l^T h_l (CUDA cores, meanwhile).
+        // Backward, layer 4 down to 0: dh_l = g_l W_l (from the packed W_l^T)
+        // and dW_l^T += h_l^T g_l, both on the tensor cores in one round.
         for (int l = kHiddenLayers; l >= 0 && ok; --l) {
             sync_for_mma();
             const bool out_layer = l == kHiddenLayers;
             if (tid == 0) {
-                issue_layer(tmem, out_layer ? d_addr : g_addr, w_addr + bwd_offset(l) * 2u, kIn,
+                const uint32_t grad_tile = out_layer ? d_addr : g_addr;
+                issue_layer(tmem, grad_tile, w_addr + bwd_offset(l) * 2u, kIn,
                             out_layer ? (uint32_t)kOut : (uint32_t)kHidden);
+                issue_weight_grad(tmem + kGradCol0 + (uint32_t)l * 64u, h_addr + (uint32_t)l * h_elems * 2u, grad_tile,
+                                  out_layer ? (uint32_t)kOut : (uint32_t)kHidden, grads);
                 mma_commit(bar_addr);
             }
             const bf16 *h = H + (uint32_t)l * h_elems;
-            if (out_layer)
-                weight_grad<kOut>(D, h, tid, grad_w + fwd_offset(l));
-            else
-                weight_grad<kHidden>(G, h, tid, grad_w + fwd_offset(l));
-            ok = wait_round(bar_addr, phase);  // also: every thread finished reading G
+            ok = wait_round(bar_addr, phase);  // both chains done: G may be overwritten
             if (!ok) break;
             tc_fence_after();
             float v[64];
@@ -568,6 +581,16 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restric
                 for (int k = 0; k < 2 * kLevelsMax; ++k) dx[(size_t)row * 2 * kLevelsMax + k] = v[k];
             }
         }
+        grads = grads || ok;
+    }
+    // This CTA's weight gradients, once, from TMEM.
+    if (ok && grads) {
+        tc_fence_after();
+        for (int l = 0; l < kHiddenLayers; ++l)
+            flush_weight_grad<kHidden>(lane_addr + kGradCol0 + (uint32_t)l * 64u, warp, tid & 31u,
+                                       grad_w + fwd_offset(l));
+        flush_weight_grad<kOut>(lane_addr + kGradCol0 + (uint32_t)kHiddenLayers * 64u, warp, tid & 31u,
+                                grad_w + fwd_offset(kHiddenLayers));
     }
     for (int off = 16; off > 0; off >>= 1) loss_sum += __shfl_down_sync(0xffffffffu, loss_sum, off);
     if ((tid & 31u) == 0u) red[warp] = loss_sum;
@@ -578,7 +601,7 @@ __global__ void __launch_bounds__(kTile) mlp_train_kernel(const uint4 *__restric
     if (tid == 0) atomicAdd(loss, red[0] + red[1] + red[2] + red[3]);
     if (warp == 0) {
         tc_fence_after();
-        tmem_free(tmem);
+        tmem_free(tmem, kTrainTmemCols);
     }
 }
 
@@ -925,6 +948,48 @@ extern "C" lux_status lux_cache_stats(LuxCache *c, LuxCacheStats *out) {
     out->last_loss = last ? loss / (3.0f * (float)last) : 0.0f;
     out->error_flags = err;
     return lux_cuda_check(c->ctx, (int)cudaGetLastError(), "cache: stats copy");
+}
+
+// One training pass without the Adam step (tests): the FP32 weight and
+// hash-table gradients of `count` <= batch samples, copied to host memory and
+// cleared on the device.
+extern "C" lux_status lux_cache_gradients(LuxCache *c, const LuxCacheSample *samples, const float *targets,
+                                          uint32_t count, float *grad_weights, float *grad_table) {
+    if (!c || !samples || !targets || !grad_weights || !grad_table) return LUX_ERR_INVALID_ARGUMENT;
+    if (count == 0 || count > c->desc.batch)
+        return lux_fail(c->ctx, LUX_ERR_INVALID_ARGUMENT, "cache: gradients take 1..batch samples");
+    LuxContext *ctx = c->ctx;
+    cudaSetDevice(ctx->device);
+    lux_status rc = ensure_rows(c, c->desc.batch);
+    if (rc != LUX_OK) return rc;
+    cudaStream_t st = ctx->stream;
+    encode_kernel<<<(count + 127) / 128, 128, 0, st>>>(c->grid, samples, count, nullptr,
+                                                       (const __nv_bfloat162 *)c->table, c->x);
+    cudaMemsetAsync(c->loss, 0, 4, st);
+    uint32_t tiles = (count + kTile - 1) / kTile;
+    mlp_train_kernel<<<std::min<uint32_t>(tiles, (uint32_t)ctx->sm_count), kTile, kTrainSmem, st>>>(
+        c->x, (const float4 *)targets, samples, count, 1.0f / (3.0f * (float)count), (const uint4 *)c->w_packed,
+        c->w_grad, c->dx, c->loss, c->error);
+    encode_backward_kernel<<<(count + 127) / 128, 128, 0, st>>>(c->grid, samples, count, c->dx,
+                                                                (float2 *)c->table_grad);
+    rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "cache: gradients");
+    if (rc != LUX_OK) return rc;
+    bool ok = cudaMemcpy(grad_weights, c->w_grad, kWTotal * 4, cudaMemcpyDeviceToHost) == cudaSuccess &&
+              cudaMemcpy(grad_table, c->table_grad, c->table_params * 4, cudaMemcpyDeviceToHost) == cudaSuccess;
+    cudaMemsetAsync(c->w_grad, 0, kWTotal * 4, st);
+    cudaMemsetAsync(c->table_grad, 0, c->table_params * 4, st);
+    if (!ok) return lux_cuda_check(ctx, (int)cudaGetLastError(), "cache: gradient copy");
+    return lux_cuda_check(ctx, (int)cudaStreamSynchronize(st), "cache: gradient clear");
+}
+
+// The FP32 master hash table (levels x 2^log2_table x 2 features) in host memory.
+extern "C" lux_status lux_cache_read_table(LuxCache *c, float *out) {
+    if (!c || !out) return LUX_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->ctx->device);
+    lux_status rc = lux_cuda_check(c->ctx, (int)cudaStreamSynchronize(c->ctx->stream), "cache: table");
+    if (rc != LUX_OK) return rc;
+    return lux_cuda_check(c->ctx, (int)cudaMemcpy(out, c->table_master, c->table_params * 4, cudaMemcpyDeviceToHost),
+                          "cache: table copy");
 }
 
 extern "C" lux_status lux_cache_read_weights(LuxCache *c, float *out) {

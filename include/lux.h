@@ -519,6 +519,14 @@ lux_status lux_cache_stats(LuxCache *cache, LuxCacheStats *out);
 lux_status lux_cache_encode(LuxCache *cache, const LuxCacheSample *samples, uint32_t count, uint16_t *out);
 lux_status lux_cache_read_weights(LuxCache *cache, float *out);
 lux_status lux_cache_forward(LuxCache *cache, const uint16_t *encoded, uint32_t count, float *out);
+/* Tests: one training pass of count (1..batch) device samples with device
+ * targets without the Adam step -- the FP32 weight gradients (host
+ * float[64*64*4 + 16*64], layout of lux_cache_read_weights) and hash-table
+ * gradients (host float[levels * 2^log2_table * 2]) -- then clears both; and
+ * the FP32 master hash table (same layout). */
+lux_status lux_cache_gradients(LuxCache *cache, const LuxCacheSample *samples, const float *targets,
+                               uint32_t count, float *grad_weights, float *grad_table);
+lux_status lux_cache_read_table(LuxCache *cache, float *out);
 
 /* Learned-cache form of a view's Split frame (no reference counterpart).
  * Interval rays of cascade-0 cells that are neither validated this frame nor
