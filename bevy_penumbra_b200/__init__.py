@@ -421,6 +421,17 @@ def reference_irradiance(ctx: LuxContext, scene: GpuScene, settings: RadianceCas
     ctx.synchronize()
 
 
+def path_reference(ctx: LuxContext, scene: GpuScene, settings: RadianceCascades, position_ptr: int, normal_ptr: int,
+                   count: int, spp: int, bounces: int, seed: int, out_ptr: int) -> None:
+    """lux_path_reference: FP64-accumulated path-traced reference (device
+    double4[count]: mean rgb, supported samples) with `bounces` diffuse
+    vertices at device float4 points / unit normals."""
+    s = settings.to_c()
+    ctx.check(lib().lux_path_reference(ctx.handle, scene.handle, C.byref(s), position_ptr, normal_ptr, count, spp,
+                                       bounces, seed, out_ptr))
+    ctx.synchronize()
+
+
 def error_stats(ctx: LuxContext, estimate_ptr: int, reference_ptr: int, count: int) -> dict:
     """lux_error_stats: FP64 error of a float4 estimate against a double4 reference."""
     out = (C.c_double * 4)()

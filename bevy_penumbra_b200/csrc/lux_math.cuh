@@ -149,6 +149,13 @@ LUX_HD void reference_sample(uint32_t p, uint32_t s, uint32_t seed, float &u1, f
     u2 = (float)(h2 >> 8) / 16777216.0f;
 }
 
+// Uniform number in [0, 1) of the path-traced reference: dimension `dim` of
+// sample `s` at point `p` (an independent hash stream per point and sample).
+LUX_HD float path_random(uint32_t p, uint32_t s, uint32_t seed, uint32_t dim) {
+    uint32_t h = transport_hash(p ^ transport_hash(s ^ transport_hash(seed + 0x7f4a7c15u + dim * 0x9e3779b9u)));
+    return (float)(h >> 8) / 16777216.0f;
+}
+
 // hashKey, shaders/common.slang:423-429.
 LUX_HD uint32_t hash_key(int32_t kx, int32_t ky, int32_t kz, int32_t kw, uint32_t buckets) {
     uint32_t h = (uint32_t)kx * 0x8da6b343u ^ (uint32_t)ky * 0xd8163841u ^ (uint32_t)kz * 0xcb1ab31fu ^

@@ -450,6 +450,21 @@ uint32_t lux_reference_round_samples(uint32_t count, uint32_t spp);
 lux_status lux_reference_irradiance(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
                                     const float *position, const float *normal, uint32_t count,
                                     uint32_t spp, uint32_t seed, double *out);
+/* The path-traced reference (no reference counterpart in the C API; it
+ * restates the reference project's offline path tracer, trace_sample,
+ * examples/pathtrace_reference.rs:724-833, from the receivers): per point
+ * (device float4 position, float4 unit normal) `spp` paths of up to `bounces`
+ * diffuse vertices (1 = direct light only; the reference's default is 3),
+ * emissive-triangle next-event estimation with power-heuristic MIS against
+ * the cosine proposal, Russian roulette from the fourth vertex; the receiver
+ * is Lambertian with unit albedo (irradiance / pi before receiver albedo, the
+ * raw output's units) and later vertices use the hit's diffuse colour and
+ * disneyDiffuseMultiplier.  FP32 rays, FP64 sums.  out: device
+ * double4[count] = (mean r, g, b, supported samples); ordered on the context
+ * stream, no allocation. */
+lux_status lux_path_reference(LuxContext *ctx, const LuxScene *scene, const LuxSettings *settings,
+                              const float *position, const float *normal, uint32_t count, uint32_t spp,
+                              uint32_t bounces, uint32_t seed, double *out);
 /* FP64 error of an FP32 estimate (device float4[count], alpha > 0 =
  * resolved) against a reference (device double4[count], w > 0 = sampled):
  * out[4] (host) = {sum of squared rgb error, sum of reference rgb, points

@@ -75,6 +75,10 @@ def lib():
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
             "orc_scene_pack": (C.c_int, [P, U, P, U, P, P, U, P, P, P, P, U, P, U, P]),
+            "orc_path_random": (F, [U, U, U, U]),
+            "orc_cosine_direction": (None, [P, F, F, P]),
+            "orc_path_sample": (C.c_int, [P, P, U, U, U, P, P, U, P]),
+            "orc_path_reference": (None, [P, P, P, P, U, U, U, U, C.c_int, P]),
             "orc_packed_sizes": (None, [P, P, P, P, P, P, P, P]),
             "orc_packed_copy": (None, [P, P, P, P, P, U]),
             "orc_packed_destroy": (None, [P]),
@@ -207,6 +211,23 @@ class OracleScene:
         lib().orc_reference_irradiance(self.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos), spp, seed,
                                        round_samples, _p(out))
         return out
+
+    def path_reference(self, settings_c, position, normal, spp: int, bounces: int, seed: int, threads: int = 0):
+        """Path-traced reference (double[count, 4]: mean rgb, supported samples)."""
+        pos = np.ascontiguousarray(position, np.float32)
+        nrm = np.ascontiguousarray(normal, np.float32)
+        out = np.zeros((len(pos), 4), np.float64)
+        lib().orc_path_reference(self.handle, C.byref(settings_c), _p(pos), _p(nrm), len(pos), spp, bounces, seed,
+                                 threads or os.cpu_count() or 1, _p(out))
+        return out
+
+    def path_sample(self, settings_c, position, normal, bounces: int, seed: int, p: int, s: int):
+        """One path's radiance (rgb), or None when a trace was unsupported."""
+        pos = np.ascontiguousarray(position, np.float32).reshape(-1)[:3].copy()
+        nrm = np.ascontiguousarray(normal, np.float32).reshape(-1)[:3].copy()
+        out = np.zeros(3, np.float32)
+        ok = lib().orc_path_sample(self.handle, C.byref(settings_c), bounces, seed, p, _p(pos), _p(nrm), s, _p(out))
+        return out if ok else None
 
     def words(self) -> np.ndarray:
         out = np.zeros(self._keep[0].shape, dtype=np.uint32).reshape(-1, 4)

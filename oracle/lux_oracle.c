@@ -2780,6 +2780,286 @@ void orc_reference_irradiance(const OrcScene *S, const LuxSettings *settings_in,
 }
 
 /* ======================================================================
+ * Path-traced reference (the reference's trace_sample,
+ * examples/pathtrace_reference.rs:724-833, from the receivers): emissive
+ * next-event estimation with power-heuristic MIS against the cosine
+ * proposal at every diffuse vertex, the last vertex's sample alone, Russian
+ * roulette from the fourth vertex; Lambertian unit-albedo receiver (the raw
+ * output's irradiance / pi), hit vertices with the diffuse colour and the
+ * Disney diffuse factor.  Each sample in FP32 as liblux's lux_path_reference,
+ * the per-point sums in FP64 in sample order.
+ * ==================================================================== */
+float orc_path_random(uint32_t p, uint32_t s, uint32_t seed, uint32_t dim) {
+    uint32_t h = orc_hash(p ^ orc_hash(s ^ orc_hash(seed + 0x7f4a7c15u + dim * 0x9e3779b9u)));
+    return (float)(h >> 8) / 16777216.0f;
+}
+
+typedef struct {
+    float position[3], normal[3], gnormal[3], view[3], diffuse[3];
+    float roughness;
+    int lambert;
+} PathVertex;
+
+static float power_heuristic(float a, float b) {
+    float aa = a * a;
+    return aa / fmaxf(aa + b * b, 1e-30f);
+}
+
+static void path_response(const PathVertex *v, const float l[3], float out[3]) {
+    if (v->lambert) {
+        out[0] = out[1] = out[2] = 1.0f / PI_F;
+        return;
+    }
+    float factor = disney_multiplier(v->normal, l, v->view, v->roughness) / PI_F;
+    for (int c = 0; c < 3; ++c) out[c] = v->diffuse[c] * factor;
+}
+
+static uint32_t light_of(const OrcScene *S, uint32_t inst, uint32_t tri) {
+    const LuxLight *L = S->lights + S->conventional;
+    uint32_t n = S->light_count - S->conventional, lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) / 2u;
+        if (L[mid].source[0] < inst || (L[mid].source[0] == inst && L[mid].source[1] < tri))
+            lo = mid + 1u;
+        else
+            hi = mid;
+    }
+    if (lo < n && L[lo].source[0] == inst && L[lo].source[1] == tri) return lo;
+    return EMPTY;
+}
+
+static int path_next_event(const OrcScene *S, const LuxSettings *st, const PathVertex *v, float u0, float u1,
+                           float u2, int competitor, float out[3]) {
+    out[0] = out[1] = out[2] = 0.0f;
+    uint32_t emissive = S->light_count - S->conventional;
+    if (emissive == 0u) return 1;
+    const LuxLight *lights = S->lights + S->conventional;
+    uint32_t low = 0, high = emissive - 1u;
+    while (low < high) {
+        uint32_t middle = (low + high) / 2u;
+        if (lights[middle].direction[3] < u0)
+            low = middle + 1u;
+        else
+            high = middle;
+    }
+    const LuxLight *L = lights + low;
+    const float bias = st->normal_bias;
+    float rel[3] = {v->position[0] - L->position[0], v->position[1] - L->position[1], v->position[2] - L->position[2]};
+    if (L->edge1[3] <= 0.0f || (L->position[3] != -2.0f && dot3(L->direction, rel) <= 0.0f)) return 1;
+    float root = sqrtf(u1);
+    float w1 = root * (1.0f - u2), w2 = root * u2;
+    float target[3];
+    for (int c = 0; c < 3; ++c) target[c] = (L->position[c] + L->edge1[c] * w1) + L->edge2[c] * w2;
+    float to_light[3] = {target[0] - v->position[0], target[1] - v->position[1], target[2] - v->position[2]};
+    float light_distance = length3(to_light);
+    if (light_distance <= bias * 0.25f) return 1;
+    float ld[3] = {to_light[0] / light_distance, to_light[1] / light_distance, to_light[2] / light_distance};
+    float cosine = fmaxf(0.0f, dot3(v->normal, ld));
+    float neg[3] = {-ld[0], -ld[1], -ld[2]};
+    float c_emit = dot3(L->direction, neg);
+    if (L->position[3] == -2.0f) c_emit = fabsf(c_emit);
+    float emitter_cosine = fmaxf(0.0f, c_emit);
+    if (cosine <= 0.0f || emitter_cosine <= 0.0f || dot3(v->gnormal, ld) <= 0.0f) return 1;
+    float bary[3] = {1.0f - root, w1, w2};
+    Surface es;
+    surface_at(S, st, L->source[0], L->source[1], bary, &es);
+    float emission[3] = {fmaxf(es.emission[0], 0.0f), fmaxf(es.emission[1], 0.0f), fmaxf(es.emission[2], 0.0f)};
+    if (!(emission[0] > 0.0f || emission[1] > 0.0f || emission[2] > 0.0f)) return 1;
+    float pdf = ((L->edge1[3] * light_distance) * light_distance) / (L->color[3] * emitter_cosine);
+    float plane = fabsf(dot3(L->direction, rel));
+    float origin[3];
+    orc_ray_offset(v->position, v->gnormal, fminf(bias, plane * 0.25f), origin);
+    float delta[3] = {target[0] - origin[0], target[1] - origin[1], target[2] - origin[2]};
+    float distance = length3(delta);
+    if (distance <= bias * 0.25f) return 1;
+    float dir[3] = {delta[0] / distance, delta[1] / distance, delta[2] / distance};
+    int supported;
+    int blocked = orc_trace_occluded(S, origin, dir, distance - fminf(bias * 0.25f, distance * 0.001f), &supported,
+                                     NULL);
+    if (blocked) return 1;
+    if (!supported) return 0;
+    float f[3];
+    path_response(v, ld, f);
+    float mis = competitor ? power_heuristic(pdf, cosine / PI_F) : 1.0f;
+    float p = fmaxf(pdf, 1e-20f);
+    for (int c = 0; c < 3; ++c) out[c] = emission[c] * (((f[c] * cosine) / p) * mis);
+    return 1;
+}
+
+static int path_hit_vertex(const OrcScene *S, const LuxSettings *st, const float origin[3], const float d[3],
+                           const LuxHit *hit, PathVertex *v, float emission[3]) {
+    Surface sf;
+    surface_at(S, st, hit->instance, hit->triangle, hit->barycentric, &sf);
+    for (int c = 0; c < 3; ++c) emission[c] = fmaxf(sf.emission[c], 0.0f);
+    if (!finite3(emission)) emission[0] = emission[1] = emission[2] = 0.0f;
+    if ((sf.flags & 16u) != 0u) return 0;
+    uint32_t base = instance_base(S, hit->instance);
+    U4 header = gword(S, 0);
+    float A[3], B[3], C[3];
+    uint32_t idx[3];
+    local_triangle(S, hit->triangle, header, A, B, C, idx);
+    float position[3];
+    for (int c = 0; c < 3; ++c) position[c] = origin[c] + d[c] * hit->distance;
+    float gn[3];
+    geometric_normal(S, base, sf.flags, A, B, C, gn);
+    float world_normal[3] = {0, 0, 0};
+    for (int i = 0; i < 3; ++i) {
+        U4 vw = gword(S, header.y + idx[i] * header.z);
+        float nrm[3] = {gn[0], gn[1], gn[2]};
+        if ((vw.w & 1u) != 0u) {
+            U4 nw = gword(S, header.y + idx[i] * header.z + 1);
+            float vn[3] = {asf(nw.x), asf(nw.y), asf(nw.z)}, tn[3];
+            transform_direction(S, base, vn, 1, tn);
+            unit_vector(tn, gn, nrm);
+        }
+        for (int c = 0; c < 3; ++c) world_normal[c] = world_normal[c] + nrm[c] * hit->barycentric[i];
+    }
+    float normal[3];
+    unit_vector(world_normal, gn, normal);
+    if (dot3(gn, d) > 0.0f && (sf.flags & 8u) != 0u) {
+        normal[0] = -normal[0]; normal[1] = -normal[1]; normal[2] = -normal[2];
+    }
+    float flipped[3] = {gn[0], gn[1], gn[2]};
+    if (dot3(gn, d) > 0.0f) {
+        flipped[0] = -flipped[0]; flipped[1] = -flipped[1]; flipped[2] = -flipped[2];
+    }
+    float neg[3] = {-d[0], -d[1], -d[2]};
+    if (dot3(normal, neg) <= 0.0f || dot3(normal, flipped) <= 0.0f) return 0;
+    float nl = length3(neg);
+    float metallic = saturatef(sf.metallic);
+    float roughness = saturatef(sf.roughness);
+    if (!isfinite(roughness)) roughness = 1.0f;
+    int bf = finite3(sf.base_color);
+    for (int c = 0; c < 3; ++c) {
+        v->position[c] = position[c];
+        v->normal[c] = normal[c];
+        v->gnormal[c] = flipped[c];
+        v->view[c] = neg[c] / nl;
+        v->diffuse[c] = (bf ? saturatef(sf.base_color[c]) : 0.0f) * (1.0f - metallic);
+    }
+    v->roughness = roughness;
+    v->lambert = 0;
+    return finite3(position) && (v->diffuse[0] > 0.0f || v->diffuse[1] > 0.0f || v->diffuse[2] > 0.0f);
+}
+
+int orc_path_sample(const OrcScene *S, const LuxSettings *st, uint32_t bounces, uint32_t seed, uint32_t p,
+                    const float pos[3], const float nrm[3], uint32_t s, float radiance[3]) {
+    radiance[0] = radiance[1] = radiance[2] = 0.0f;
+    float throughput[3] = {1.0f, 1.0f, 1.0f};
+    PathVertex v;
+    for (int c = 0; c < 3; ++c) {
+        v.position[c] = pos[c];
+        v.normal[c] = nrm[c];
+        v.gnormal[c] = nrm[c];
+        v.view[c] = nrm[c];
+        v.diffuse[c] = 1.0f;
+    }
+    v.roughness = 1.0f;
+    v.lambert = 1;
+    for (uint32_t bounce = 0; bounce < bounces; ++bounce) {
+        uint32_t dim = bounce * 6u;
+        int competitor = bounce + 1u < bounces;
+        float c3[3];
+        if (!path_next_event(S, st, &v, orc_path_random(p, s, seed, dim), orc_path_random(p, s, seed, dim + 1u),
+                             orc_path_random(p, s, seed, dim + 2u), competitor, c3))
+            return 0;
+        for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + throughput[c] * c3[c];
+        if (!competitor) break;
+        float d[3];
+        orc_cosine_direction(v.normal, orc_path_random(p, s, seed, dim + 3u), orc_path_random(p, s, seed, dim + 4u), d);
+        float cosine = dot3(v.normal, d);
+        if (!(cosine > 0.0f) || dot3(v.gnormal, d) <= 0.0f) break;
+        float pdf = cosine / PI_F;
+        float f[3];
+        path_response(&v, d, f);
+        for (int c = 0; c < 3; ++c) throughput[c] = throughput[c] * ((f[c] * cosine) / pdf);
+        if (bounce >= 3u) {
+            float survival = fminf(fmaxf(fmaxf(throughput[0], fmaxf(throughput[1], throughput[2])), 0.05f), 0.95f);
+            if (orc_path_random(p, s, seed, dim + 5u) >= survival) break;
+            for (int c = 0; c < 3; ++c) throughput[c] = throughput[c] / survival;
+        }
+        float origin[3];
+        orc_ray_offset(v.position, v.gnormal, st->normal_bias, origin);
+        LuxHit hit;
+        orc_trace_closest(S, origin, d, 0.0f, 1e20f, &hit, NULL);
+        if ((hit.errors & HIT_QUERY_UNSUPPORTED) != 0u) return 0;
+        if (hit.triangle == EMPTY) {
+            for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + throughput[c] * st->environment[c];
+            break;
+        }
+        PathVertex next;
+        float emission[3];
+        int scatters = path_hit_vertex(S, st, origin, d, &hit, &next, emission);
+        if (emission[0] > 0.0f || emission[1] > 0.0f || emission[2] > 0.0f) {
+            float mis = 1.0f;
+            uint32_t li = light_of(S, hit.instance, hit.triangle);
+            if (li != EMPTY) {
+                const LuxLight *L = S->lights + S->conventional + li;
+                float neg[3] = {-d[0], -d[1], -d[2]};
+                float c_emit = dot3(L->direction, neg);
+                if (L->position[3] == -2.0f) c_emit = fabsf(c_emit);
+                if (c_emit > 0.0f && L->color[3] > 0.0f && L->edge1[3] > 0.0f)
+                    mis = power_heuristic(pdf, ((L->edge1[3] * hit.distance) * hit.distance) / (L->color[3] * c_emit));
+            }
+            for (int c = 0; c < 3; ++c) radiance[c] = radiance[c] + (throughput[c] * emission[c]) * mis;
+        }
+        if (!scatters) break;
+        v = next;
+    }
+    if (!finite3(radiance)) radiance[0] = radiance[1] = radiance[2] = 0.0f;
+    return 1;
+}
+
+typedef struct {
+    const OrcScene *S;
+    const LuxSettings *st;
+    const float *position, *normal;
+    uint32_t spp, bounces, seed, begin, end;
+    double *out;
+} PathJob;
+
+static void *path_job(void *arg) {
+    PathJob *j = (PathJob *)arg;
+    for (uint32_t p = j->begin; p < j->end; ++p) {
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+        for (uint32_t s = 0; s < j->spp; ++s) {
+            float r[3];
+            if (!orc_path_sample(j->S, j->st, j->bounces, j->seed, p, j->position + 4 * (size_t)p,
+                                 j->normal + 4 * (size_t)p, s, r))
+                continue;
+            acc[0] += (double)r[0];
+            acc[1] += (double)r[1];
+            acc[2] += (double)r[2];
+            acc[3] += 1.0;
+        }
+        double *q = j->out + 4 * (size_t)p;
+        if (acc[3] > 0.0) {
+            q[0] = acc[0] / acc[3]; q[1] = acc[1] / acc[3]; q[2] = acc[2] / acc[3]; q[3] = acc[3];
+        } else {
+            q[0] = q[1] = q[2] = q[3] = 0.0;
+        }
+    }
+    return NULL;
+}
+
+void orc_path_reference(const OrcScene *S, const LuxSettings *settings, const float *position, const float *normal,
+                        uint32_t count, uint32_t spp, uint32_t bounces, uint32_t seed, int threads, double *out) {
+    if (threads < 1) threads = 1;
+    if ((uint32_t)threads > count) threads = count ? (int)count : 1;
+    PathJob *jobs = (PathJob *)calloc((size_t)threads, sizeof(PathJob));
+    pthread_t *tid = (pthread_t *)calloc((size_t)threads, sizeof(pthread_t));
+    for (int t = 0; t < threads; ++t) {
+        jobs[t] = (PathJob){S, settings, position, normal, spp, bounces, seed,
+                            (uint32_t)((uint64_t)count * t / threads), (uint32_t)((uint64_t)count * (t + 1) / threads),
+                            out};
+        pthread_create(&tid[t], NULL, path_job, &jobs[t]);
+    }
+    for (int t = 0; t < threads; ++t) pthread_join(tid[t], NULL);
+    free(jobs);
+    free(tid);
+}
+
+/* ======================================================================
  * Screen reconstruction: temporal + denoise (shaders/cascades.slang:310-690)
  * for persistent world intervals without motion vectors; positions are the
  * caller's (xyz, view depth in w) and the previous positions are kept in the

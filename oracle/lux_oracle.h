@@ -166,6 +166,15 @@ OrcFrame *orc_frame_run(const OrcScene *scene, const LuxSettings *settings,
                         const float *receiver_position, const float *receiver_normal,
                         uint32_t receiver_count, int threads);
 void orc_frame_destroy(OrcFrame *frame);
+/* The path-traced reference (lux_path_reference's restatement): one sample's
+ * radiance (0 when a trace is unsupported), and per point the FP64 mean over
+ * spp samples (out double4[count]: rgb, supported samples). */
+float orc_path_random(uint32_t p, uint32_t s, uint32_t seed, uint32_t dim);
+int orc_path_sample(const OrcScene *scene, const LuxSettings *settings, uint32_t bounces, uint32_t seed, uint32_t p,
+                    const float position[3], const float normal[3], uint32_t s, float radiance[3]);
+void orc_path_reference(const OrcScene *scene, const LuxSettings *settings, const float *position,
+                        const float *normal, uint32_t count, uint32_t spp, uint32_t bounces, uint32_t seed,
+                        int threads, double *out);
 
 /* The oracle's scene packer (orc_pack.c): build_tree / node_words /
  * pack_instances / geometry_words / build_emissive_lights restated in C.

@@ -137,9 +137,9 @@ def test_two_adam_steps_match_torch_optimisers():
     dg, dr = got_t - t0.reshape(-1), pt.detach().numpy() - t0.reshape(-1)
     assert np.count_nonzero(dr) > 1000
     # SparseAdam adds eps to sqrt(v) before the sqrt(1 - beta2^t) correction,
-    # the kernel after it: with eps = 1e-10 that differs only for gradients
-    # near 1e-9, so entries with every gradient above 1e-6 compare tightly.
-    big = np.isfinite(smallest) & (smallest > 1e-6)
+    # the kernel after it: a relative difference of about eps / (0.14 |g|), so
+    # entries whose every gradient is above 1e-4 compare to 1e-3.
+    big = np.isfinite(smallest) & (smallest > 1e-4)
     assert big.sum() > 1000
     np.testing.assert_allclose(dg[big], dr[big], rtol=1e-3, atol=1e-7)
     np.testing.assert_allclose(dg, dr, rtol=0, atol=2e-4)

@@ -21,6 +21,17 @@ from tests.test_gpu_cascades import compare_levels
 pytestmark = pytest.mark.gpu
 
 
+def assert_same_overflow(gpu_errors, oracle_errors):
+    """Equal error bits, except that the device may add bit 1 (its BLAS walk
+    ran out of the stack it shares with the TLAS walk) where bit 2 is set."""
+    g, o = gpu_errors.astype(np.uint32), oracle_errors.astype(np.uint32)
+    extra = g & ~o
+    assert np.all((extra & ~np.uint32(1)) == 0), np.unique(g[extra != 0])
+    assert np.all((g[extra != 0] & 2) == 2)
+    np.testing.assert_array_equal(g & ~np.uint32(1), o & ~np.uint32(1))
+    np.testing.assert_array_equal(o & ~g, 0)
+
+
 def gpu_trace(pk, rays, any_hit=False):
     ctx = bp.LuxContext()
     scene = bp.GpuScene(ctx, pk)
@@ -48,9 +59,13 @@ def test_forced_deep_traversal_matches_oracle(blas, internals):
     if internals == 64:
         assert np.all(gpu["errors"] == 0)
     else:
-        # Both walks overflow: every hit carries exactly the overflow bit.
-        np.testing.assert_array_equal(gpu["errors"], cpu["errors"])
-        assert np.all(gpu["errors"][hit] == expected)
+        # Both walks overflow: every hit carries the overflow bit of the deep
+        # tree.  The device's TLAS and BLAS walks share one stack, so an
+        # instance entered from a nearly full TLAS stack can also exhaust it
+        # in its BLAS walk (bit 1 beside bit 2); the reference's BLAS walk has
+        # a stack of its own.  Either fallback keeps every hit.
+        assert_same_overflow(gpu["errors"], cpu["errors"])
+        assert np.all((gpu["errors"][hit] & expected) == expected)
     failures, _ = check_against_f64(oscene, rays, gpu, any_hit=False, expected_errors=expected)
     assert not failures, failures[:12]
     blocked = gpu_trace(deep, rays, any_hit=True)
@@ -95,11 +110,11 @@ def test_forced_deep_split_frame_matches_oracle(blas, stack_depth):
     got, want = view.read_hits(rays), ofr.hits(rays)
     np.testing.assert_array_equal(got["triangle"], want["triangle"])
     np.testing.assert_array_equal(got["instance"], want["instance"])
-    np.testing.assert_array_equal(got["errors"], want["errors"])
+    assert_same_overflow(got["errors"], want["errors"])
     np.testing.assert_array_equal(got["distance"].view(np.uint32), want["distance"].view(np.uint32))
     hit = got["triangle"] != EMPTY
     assert hit.sum() > 100
-    assert np.all(got["errors"][hit] == (1 if blas else 2))
+    assert np.all((got["errors"][hit] & (1 if blas else 2)) == (1 if blas else 2))
     compare_levels(settings, [view.read_level(l) for l in range(settings.levels)], ofr, exact=False)
 
 
