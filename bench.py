@@ -37,7 +37,7 @@ TRIANGLES = 262_144
 RAYS_PER_RECEIVER = 36
 EYE, TARGET = (-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)
 L2_FLUSH_BYTES = 512 << 20
-REFERENCE_SPP = 1024
+REFERENCE_SPP = 4096
 # DRAM bytes per ray of the traversal kernels from one ncu capture of the
 # small atrium case (65,536 triangles at 640x360: dram read + write per launch
 # / rays of that launch); the full frame's traffic is scaled from it by its
@@ -55,8 +55,10 @@ LEARNED_WARMUP = 200
 LAUNCHES_PER_FRAME_FIXED = 25
 
 
-def launches_per_frame(levels: int, sort_queries: bool) -> int:
-    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (4 if sort_queries else 0)
+def launches_per_frame(levels: int, sort_queries: bool, sort_rays: bool = False) -> int:
+    """Kernels of one plain frame; sorting the interval rays adds the key
+    pass to the four counting-sort launches."""
+    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (4 if sort_queries else 0) + (5 if sort_rays else 0)
 
 
 def settings_for_workload(sanitize: bool = True):
@@ -168,6 +170,37 @@ def build_workload(device: int = 0, host_only: bool = False):
     return dict(bp=bp, desc=desc, packed=packed, ctx=ctx, scene=scene, view=view, settings=settings, pscreen=pscreen,
                 rpos=rpos,
                 rnrm=rnrm, ppos=ppos, pnrm=pnrm, entries=entries, cells_max=cells_max, setup_s=time.time() - t0)
+
+
+SURFACE_CLASSES = {0: "columns", 1: "arches", 2: "floor tiles", 3: "emitters", 4: "ceiling"}
+
+
+def point_classes(w, indices):
+    """Surface class of resolve points (the mesh of the instance each primary
+    hit landed on; the atrium adds columns, arches, tiles, emitters and the
+    ceiling in that order)."""
+    slot = w["pscreen"]["identity"][indices].astype(np.int64)
+    caller = w["packed"].instance_order.astype(np.int64)[slot]
+    return np.asarray(w["desc"].instance_mesh, np.int64)[caller]
+
+
+def error_report(bp, ctx, est, ref, classes):
+    """lux_error_stats of an estimate against a reference, plus the relative
+    RMSE and the ratio of means per surface class (host, FP64)."""
+    out = bp.error_stats(ctx, est.data_ptr(), ref.data_ptr(), len(est))
+    e, r = est.cpu().numpy().astype(np.float64), ref.cpu().numpy()
+    ok = (e[:, 3] > 0) & (r[:, 3] > 0)
+    per = {}
+    for k, name in SURFACE_CLASSES.items():
+        m = ok & (classes == k)
+        if m.sum() < 8:
+            continue
+        d = e[m, :3] - r[m, :3]
+        mean_ref = r[m, :3].mean()
+        per[name] = {"points": int(m.sum()), "relative_rmse": float(np.sqrt(np.mean(d * d)) / max(mean_ref, 1e-30)),
+                     "ratio_of_means": float(e[m, :3].mean() / max(mean_ref, 1e-30))}
+    out["per_surface"] = per
+    return out
 
 
 class ClockSampler:
@@ -365,8 +398,8 @@ def workload_config(w):
             "records": int(w["entries"]), "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps"}
 
 
-def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref, plain_ms,
-                plain_error, interval_rays, device):
+def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_ref, classes, plain_ms,
+                plain_error, interval_rays, device, cutoff):
     """The learned-cache form of the same frame: levels from the cutoff on
     answered by the hash-grid MLP cache (trained online inside each frame),
     1/16 of the cascade-0 cells validated per frame with per-cell fallback.
@@ -381,7 +414,7 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     lo = w["rpos"][:, :3].min(0) - 1.0
     hi = w["rpos"][:, :3].max(0) + 1.0
     cache.set_bounds(lo, hi)
-    lview.set_cache(cache, cutoff_level=args.cache_cutoff, validate_period=16, error_bound=args.cache_bound,
+    lview.set_cache(cache, cutoff_level=cutoff, validate_period=16, error_bound=args.cache_bound,
                     train_samples=65536,
                     fallback_frames=16)
     lview.set_timing(True)
@@ -409,24 +442,26 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
         raise RuntimeError("learned-cache frame reported an error")
     lview.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
     s_est = d_out[sub].contiguous()
-    err = bp.error_stats(ctx, s_est.data_ptr(), s_ref.data_ptr(), len(sub))
+    err = error_report(bp, ctx, s_est, s_ref, classes)
     return {
         "ms_per_step": learned_ms, "value": interval_rays / (learned_ms * 1e-3) / 1e6, "unit": "Mrays/s",
         "speedup_vs_plain": plain_ms / learned_ms,
         "relative_rmse": err["relative_rmse"], "plain_relative_rmse": plain_error["relative_rmse"],
         "rmse_change": err["relative_rmse"] / plain_error["relative_rmse"] - 1.0,
+        "per_surface": err["per_surface"],
         "rays": {"cached": int(cs.cached_rays), "fallback": int(cs.fallback_rays),
                  "validated": int(cs.validated_rays), "trained_samples": int(cs.trained_samples),
                  "failed_cells": int(cs.failed_cells), "validated_cells": int(cs.validated_cells),
                  "validated_bias": float(cs.validated_bias)},
         "cache": {"levels": 16, "table": "2^19 x 2 BF16 per level", "base_resolution": 16, "growth": 1.5,
                   "mlp": "64 -> 4 x 64 ReLU -> 3, BF16 tcgen05", "learning_rate": 1e-3, "batch": 16384,
-                  "samples_per_frame": 65536, "cutoff_level": args.cache_cutoff, "validate_period": 16,
+                  "samples_per_frame": 65536, "cutoff_level": cutoff, "validate_period": 16,
                   "error_bound": args.cache_bound, "fallback_frames": 16, "warmup_frames": LEARNED_WARMUP},
     }
 
 
-def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device):
+def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device, d_ppos, d_pnrm, d_out, sub, ref3,
+                     classes):
     """The multi-bounce form of the same frame (RadianceCascades::multi_bounce):
     the primary cache with the secondary probes' bounce light, then the
     secondary cache traced from the primary hits (spacing and intervals x4).
@@ -462,7 +497,10 @@ def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device):
     if st.error_flags or sst.error_flags:
         raise RuntimeError("multi-bounce frame reported an error")
     mb_ms = float(np.sum(ms)) / args.steps
+    mview.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), len(w["ppos"]), d_out.data_ptr())
+    err3 = error_report(bp, ctx, d_out[sub].contiguous(), ref3, classes)
     return {"ms_per_step": mb_ms, "overhead_vs_plain": mb_ms / plain_ms,
+            "error_vs_fp64_3_bounces": err3,
             "secondary_trace_ms": float(np.median(sec_trace)),
             "primary_rays": int(st.interval_rays), "secondary_rays": int(sst.interval_rays),
             "secondary_shadow_rays": int(sst.shadow_rays), "secondary_cells_level0": int(sst.cells[0]),
@@ -627,25 +665,51 @@ def run_ours(args, rank, world):
     e2e_value = job_mrays(world, interval_rays, args.steps, e2e_total)
 
     # FP32 error of the resolved irradiance against the FP64 path-traced
-    # reference on every 97th resolve point (not timed).
+    # reference on every 97th resolve point (not timed): two diffuse vertices
+    # (direct light + one bounce, the transport the cascades carry) and three
+    # (the reference path tracer's default depth).
     view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
     sub = torch.arange(0, n_pts, 97, device=dev)
     s_pos, s_nrm, s_est = d_ppos[sub].contiguous(), d_pnrm[sub].contiguous(), d_out[sub].contiguous()
-    s_ref = torch.zeros((len(sub), 4), dtype=torch.float64, device=dev)
-    torch.cuda.synchronize(device)
-    t0 = time.perf_counter()
-    bp.reference_irradiance(ctx, scene, settings, s_pos.data_ptr(), s_nrm.data_ptr(), len(sub), REFERENCE_SPP, 99,
-                            s_ref.data_ptr())
-    ref_s = time.perf_counter() - t0
-    error = bp.error_stats(ctx, s_est.data_ptr(), s_ref.data_ptr(), len(sub))
-    error.update({"spp": REFERENCE_SPP, "sample": f"every 97th resolve point ({len(sub)})",
-                  "reference_s": ref_s, "oracle": "FP64-accumulated path-traced interval radiance"})
+    refs = {}
+    for bounces in (2, 3):
+        r = torch.zeros((len(sub), 4), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(device)
+        t0 = time.perf_counter()
+        bp.path_reference(ctx, scene, settings, s_pos.data_ptr(), s_nrm.data_ptr(), len(sub), REFERENCE_SPP,
+                          bounces, 99, r.data_ptr())
+        refs[bounces] = (r, time.perf_counter() - t0)
+    s_ref = refs[2][0]
+    classes = point_classes(w, sub.cpu().numpy())
+    error = error_report(bp, ctx, s_est, s_ref, classes)
+    error.update({"spp": REFERENCE_SPP, "bounces": 2, "sample": f"every 97th resolve point ({len(sub)})",
+                  "reference_s": refs[2][1],
+                  "oracle": "path-traced reference (emissive NEE + MIS, FP32 rays, FP64 sums), 2 diffuse vertices"})
+    error3 = error_report(bp, ctx, s_est, refs[3][0], classes)
+    error3.update({"spp": REFERENCE_SPP, "bounces": 3, "reference_s": refs[3][1]})
 
-    learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_pos, s_nrm, s_ref,
-                          ms_per_step, error, interval_rays, device)
-    multi_bounce = run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, ms_per_step, device)
+    learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_ref, classes,
+                          ms_per_step, error, interval_rays, device, args.cache_cutoff)
+    # The operating point of the learned-cache configuration as stated:
+    # cascades from level 3 on answered by the cache.
+    learned3 = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_ref, classes,
+                           ms_per_step, error, interval_rays, device, 3)
+    multi_bounce = run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, ms_per_step, device, d_ppos, d_pnrm,
+                                    d_out, sub, refs[3][0], classes)
     view.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
     screen = run_screen(w, args, stream, flush, d_ppos, d_pnrm, d_out, device)
+
+    # The batched and full-form workloads, summarised in the same line (one
+    # GPU runs); each reports its own error instead of failing the line.
+    extras = {}
+    if world == 1 and not args.no_extras and not args.small:
+        for key, fn in (("batched", lambda: batched_line(args, world, device)),
+                        ("full", lambda: full_line(args, world, device, args.full_frames))):
+            try:
+                extras[key] = fn()
+            except Exception as exc:  # reported, not hidden: the line carries the failure
+                extras[key] = {"error": f"{type(exc).__name__}: {exc}"}
+            torch.cuda.synchronize(device)
 
     if rank == 0:
         peak, peak_kind = measured_peaks()
@@ -688,10 +752,14 @@ def run_ours(args, rank, world):
                     "h2d_bytes_per_step": int(w["rpos"].nbytes + w["rnrm"].nbytes + w["ppos"].nbytes + w["pnrm"].nbytes),
                     "d2h_bytes_per_step": int(n_pts * 16)},
             "error_vs_fp64": error,
+            "error_vs_fp64_3_bounces": error3,
             "learned": learned,
+            "learned_cutoff_3": learned3,
             "multi_bounce": multi_bounce,
             "screen_filter": screen,
-            "gpu_launches": args.steps * launches_per_frame(settings.levels, bool(tuned["best"].get("sort_queries"))),
+            **extras,
+            "gpu_launches": args.steps * launches_per_frame(settings.levels, bool(tuned["best"].get("sort_queries")),
+                                                            bool(tuned["best"].get("sort_rays"))),
             "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
             "clocks": clocks.summary(),
@@ -767,6 +835,15 @@ def run_batched(args, rank, world):
     torch.cuda.set_device(device)
     work_stream = torch.cuda.Stream(device)
     torch.cuda.set_stream(work_stream)
+    line = batched_line(args, world, device)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def batched_line(args, world, device):
+    """The batched workload's measurement (a bench line's fields)."""
+    import torch
+
     w = build_batch_workload(device)
     bp, ctx, settings, jobs = w["bp"], w["ctx"], w["settings"], w["jobs"]
     stream = torch.cuda.current_stream(device)
@@ -817,7 +894,7 @@ def run_batched(args, rank, world):
     sequential_ms = timed(one_by_one)
     rays = sum(j["n"] for j in jobs) * settings.rays_per_receiver
     info = batch.info()
-    if rank == 0:
+    if True:
         line = {
             "metric": METRIC, "value": world * rays / (batch_ms * 1e-3) / 1e6, "unit": "Mrays/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": batch_ms, "higher_is_better": True,
@@ -834,7 +911,8 @@ def run_batched(args, rank, world):
             "gpu_launches": args.steps * info.kernels_per_frame,
             "clocks": clocks.summary(), "setup_s": w["setup_s"],
         }
-        print(json.dumps(line), flush=True)
+    batch.close()
+    return line
 
 
 FULL_VIEWS = [((-17.0, 3.0, -15.0), (4.0, 4.0, 6.0)), ((17.0, 3.5, -15.0), (-4.0, 4.0, 6.0)),
@@ -883,6 +961,18 @@ def run_full(args, rank, world):
     torch.cuda.set_device(device)
     work_stream = torch.cuda.Stream(device)
     torch.cuda.set_stream(work_stream)
+    line = full_line(args, world, device, args.frames)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def full_line(args, world, device, frames):
+    """The full-form workload's measurement over `frames` frames of motion."""
+    import torch
+
+    import bevy_penumbra_b200 as bp
+    from bevy_penumbra_b200 import scenes
+
     stream = torch.cuda.current_stream(device)
     dev = f"cuda:{device}"
     t0 = time.time()
@@ -956,7 +1046,7 @@ def run_full(args, rank, world):
         scene.refit(prev, lights=packed.lights_at(prev))
         d_rec = receivers_now()
         ms, rays = [], 0
-        for frame in range(args.frames):
+        for frame in range(frames):
             cur = poses(frame)
             moved = [i for i in range(len(cur)) if not np.array_equal(cur[i], prev[i])]
             box_moved = any(int(packed.instance_order[sl]) in boxes for sl in moved)
@@ -1011,14 +1101,14 @@ def run_full(args, rank, world):
         hi = np.max([p[:, :3].max(0) for p, _ in recv], axis=0) + 1.0
         cache.set_bounds(lo, hi)
         learned = run_form(cache)
-    if rank == 0:
+    if True:
         line = {
             "metric": METRIC, "value": world * plain["value"], "unit": "Mrays/s", "n_gpus": world,
-            "steps": args.frames, "warmup": 10, "ms_per_step": plain["ms_per_frame"], "higher_is_better": True,
+            "steps": frames, "warmup": 10, "ms_per_step": plain["ms_per_frame"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "full: 1,048,576 tris, 4 emitters on circles at 0.5 m/s, 8 rigid boxes moved in "
                                    "turn every 30 frames, 4 views at 1920x1080 (receivers at 4x4 px), 8 cascades",
-                       "frames": args.frames, "fps": FULL_FPS, "views": len(views),
+                       "frames": frames, "fps": FULL_FPS, "views": len(views),
                        "interval_rays_per_frame": plain["interval_rays_per_frame"],
                        "reference": "4096-spp FP64 reference on every 64th receiver, final frame"},
             "plain": plain,
@@ -1027,7 +1117,7 @@ def run_full(args, rank, world):
                             cutoff_level=args.cache_cutoff, error_bound=args.cache_bound),
             "clocks": clocks.summary(), "setup_s": setup_s,
         }
-        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():
@@ -1040,6 +1130,10 @@ def main():
                     help="atrium: the headline frame; batched: 64 scenes per step through lux_batch_trace_merge; "
                          "full: moving emitters and boxes, 4 views at 1080p, plain and learned forms")
     ap.add_argument("--frames", type=int, default=600, help="full workload: frames of motion")
+    ap.add_argument("--full-frames", type=int, default=120,
+                    help="default line: frames of motion of its full-form summary")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default line without the batched and full-form summaries")
     ap.add_argument("--cache-cutoff", type=int, default=LEARNED_CUTOFF,
                     help="learned-cache form: first cascade answered by the cache")
     ap.add_argument("--cache-bound", type=float, default=8.0,

@@ -341,10 +341,136 @@ struct Walker {
         return true;
     }
 
-    // The next pending entry into `cur` (have = true), leaving instances and
-    // starting the ordered-scan fallbacks as needed.  Returns true when the
-    // query is complete.
-    __device__ __forceinline__ bool next_entry(const SceneView &S, uint2 *stack) {
+    // One step: inner nodes down to a leaf, that leaf, then the next pending
+    // entry.  Returns true when the query is complete.
+    // The stack lives outside the walker so the walker's fields stay in
+    // registers; only the stack itself is addressed dynamically.
+    __device__ __forceinline__ bool step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
+        while (have && (cur & kLeafBit) == 0u) {
+            bool in_tlas = blas_base < 0;
+            uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
+            if (in_tlas)
+                tlas_steps = steps;
+            else
+                blas_steps = steps;
+            if (steps > kMaxSteps) {
+                hit.errors |= kQueryUnsupported;
+                if (in_tlas) return true;  // abandon the whole query
+                sp = blas_base;            // abandon this instance
+                have = false;
+                break;
+            }
+            float entry[4];
+            uint32_t child[4];
+            cn.nodes++;
+            uint32_t mask = node_test(S.nodes, cur, r, hit.t, tmin, entry, child);
+            if (mask == 0u) {
+                have = false;
+                break;
+            }
+            uint32_t k0 = child_key(mask, entry, 0), k1 = child_key(mask, entry, 1);
+            uint32_t k2 = child_key(mask, entry, 2), k3 = child_key(mask, entry, 3);
+            key_swap(k0, k1);
+            key_swap(k2, k3);
+            key_swap(k0, k2);
+            key_swap(k1, k3);
+            key_swap(k1, k2);
+            int n = __popc(mask);
+            if (sp + n - 1 > kDepth) {
+                if (in_tlas) {
+                    hit.errors |= 2u;
+                    sp = 0;
+                    tlas_next = 0;
+                } else {
+                    hit.errors |= 1u;
+                    sp = blas_base;
+                    blas_next = inst_first;
+                }
+                have = false;
+                break;
+            }
+            if (n > 3) stack[sp++] = make_uint2(key_child(k3, child), k3 & ~3u);
+            if (n > 2) stack[sp++] = make_uint2(key_child(k2, child), k2 & ~3u);
+            if (n > 1) stack[sp++] = make_uint2(key_child(k1, child), k1 & ~3u);
+            cur = key_child(k0, child);
+            cur_t = key_entry(k0);
+        }
+        if (have) {
+            uint32_t first = cur & kLeafFirstMask;
+            uint32_t count = ((cur >> 27) & 15u) + 1u;
+            have = false;
+            if (blas_base < 0) {
+                // TLAS leaf: enter its first instance; the rest waits on the stack.
+                if (count > 1u) {
+                    if (sp < kDepth) {
+                        stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
+                                                 as_uint(cur_t));
+                    } else {
+                        // Stack exhausted: after this instance, scan every instance.
+                        hit.errors |= 2u;
+                        sp = 0;
+                        tlas_next = 0;
+                    }
+                }
+                DeviceInstance I = load_instance(S.instances, first);
+                local_ray(I, o, d, lo, ld);
+                cn.instances++;
+                // A local direction bit-identical to the world direction
+                // (translation-only instances) keeps the world constants;
+                // only the origin moves.
+                rotated = !(as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) &&
+                            as_uint(ld.z) == as_uint(d.z));
+                if (rotated) {
+                    r = slab_ray(lo, ld);
+                    tri_ray = triangle_ray(ld);
+                } else {
+                    r.ox = lo.x;
+                    r.oy = lo.y;
+                    r.oz = lo.z;
+                }
+                inst = first;
+                inst_flags = I.flags;
+                inst_first = I.first;
+                inst_count = I.count;
+                blas_base = sp;
+                blas_steps = 0;
+                cur = I.root;
+                cur_t = 0.0f;
+                have = true;
+                return false;
+            }
+            // BLAS leaf (traceTriangle / occludedTriangle).
+            if (++blas_steps > kMaxSteps) {
+                hit.errors |= kQueryUnsupported;
+                sp = blas_base;
+            } else {
+                for (uint32_t t = first; t < first + count; ++t) {
+                    f3 A, B, C;
+                    load_triangle(S.triangles, t, A, B, C);
+                    cn.triangles++;
+                    if (cull_reject(inst_flags, A, B, C, ld)) continue;
+                    float w1 = 0.0f, w2 = 0.0f;
+                    float dist = intersect_triangle(lo, ld, tri_ray, A, B, C, w1, w2);
+                    if (kAnyHit) {
+                        if (dist > 0.000025f && dist < hit.t) {
+                            // Any accepted blocker is a complete proof
+                            // (shaders/traversal.slang:786-792, :1035-1040).
+                            hit.tri = t;
+                            hit.inst = inst;
+                            hit.errors &= ~kQueryUnsupported;
+                            return true;
+                        }
+                    } else if (dist > lower && hit_better(dist, inst, t, hit)) {
+                        hit.t = dist;
+                        hit.tri = t;
+                        hit.inst = inst;
+                        hit.b1 = w1;
+                        hit.b2 = w2;
+                    }
+                }
+            }
+        }
+        // The next pending entry, leaving instances and fallbacks as needed.
         while (!have) {
             if (blas_base >= 0 && sp == blas_base) {
                 if (blas_next != kEmpty && blas_next < inst_first + inst_count) {
@@ -382,141 +508,6 @@ struct Walker {
             cur = top.x;
             cur_t = as_float(top.y);
             have = true;
-        }
-        return false;
-    }
-
-    // One step: inner nodes (and pending entries after dead ends) down to the
-    // next leaf, then that leaf.  Returns true when the query is complete.
-    // Every lane of a warp leaves the descent holding a leaf (or done), so
-    // the leaf work of a step runs with the warp's lanes together; the order
-    // in which a lane visits nodes and leaves is the plain depth-first order.
-    // The stack lives outside the walker so the walker's fields stay in
-    // registers; only the stack itself is addressed dynamically.
-    __device__ __forceinline__ bool step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
-        while (true) {
-            if (!have && next_entry(S, stack)) return true;
-            if ((cur & kLeafBit) != 0u) break;
-            bool in_tlas = blas_base < 0;
-            uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
-            if (in_tlas)
-                tlas_steps = steps;
-            else
-                blas_steps = steps;
-            if (steps > kMaxSteps) {
-                hit.errors |= kQueryUnsupported;
-                if (in_tlas) return true;  // abandon the whole query
-                sp = blas_base;            // abandon this instance
-                have = false;
-                continue;
-            }
-            float entry[4];
-            uint32_t child[4];
-            cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, r, hit.t, tmin, entry, child);
-            if (mask == 0u) {
-                have = false;
-                continue;
-            }
-            uint32_t k0 = child_key(mask, entry, 0), k1 = child_key(mask, entry, 1);
-            uint32_t k2 = child_key(mask, entry, 2), k3 = child_key(mask, entry, 3);
-            key_swap(k0, k1);
-            key_swap(k2, k3);
-            key_swap(k0, k2);
-            key_swap(k1, k3);
-            key_swap(k1, k2);
-            int n = __popc(mask);
-            if (sp + n - 1 > kDepth) {
-                if (in_tlas) {
-                    hit.errors |= 2u;
-                    sp = 0;
-                    tlas_next = 0;
-                } else {
-                    hit.errors |= 1u;
-                    sp = blas_base;
-                    blas_next = inst_first;
-                }
-                have = false;
-                continue;
-            }
-            if (n > 3) stack[sp++] = make_uint2(key_child(k3, child), k3 & ~3u);
-            if (n > 2) stack[sp++] = make_uint2(key_child(k2, child), k2 & ~3u);
-            if (n > 1) stack[sp++] = make_uint2(key_child(k1, child), k1 & ~3u);
-            cur = key_child(k0, child);
-            cur_t = key_entry(k0);
-        }
-        uint32_t first = cur & kLeafFirstMask;
-        uint32_t count = ((cur >> 27) & 15u) + 1u;
-        have = false;
-        if (blas_base < 0) {
-            // TLAS leaf: enter its first instance; the rest waits on the stack.
-            if (count > 1u) {
-                if (sp < kDepth) {
-                    stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
-                                             as_uint(cur_t));
-                } else {
-                    // Stack exhausted: after this instance, scan every instance.
-                    hit.errors |= 2u;
-                    sp = 0;
-                    tlas_next = 0;
-                }
-            }
-            DeviceInstance I = load_instance(S.instances, first);
-            local_ray(I, o, d, lo, ld);
-            cn.instances++;
-            // A local direction bit-identical to the world direction
-            // (translation-only instances) keeps the world constants;
-            // only the origin moves.
-            rotated = !(as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) &&
-                        as_uint(ld.z) == as_uint(d.z));
-            if (rotated) {
-                r = slab_ray(lo, ld);
-                tri_ray = triangle_ray(ld);
-            } else {
-                r.ox = lo.x;
-                r.oy = lo.y;
-                r.oz = lo.z;
-            }
-            inst = first;
-            inst_flags = I.flags;
-            inst_first = I.first;
-            inst_count = I.count;
-            blas_base = sp;
-            blas_steps = 0;
-            cur = I.root;
-            cur_t = 0.0f;
-            have = true;
-            return false;
-        }
-        // BLAS leaf (traceTriangle / occludedTriangle).
-        if (++blas_steps > kMaxSteps) {
-            hit.errors |= kQueryUnsupported;
-            sp = blas_base;
-            return false;
-        }
-        for (uint32_t t = first; t < first + count; ++t) {
-            f3 A, B, C;
-            load_triangle(S.triangles, t, A, B, C);
-            cn.triangles++;
-            if (cull_reject(inst_flags, A, B, C, ld)) continue;
-            float w1 = 0.0f, w2 = 0.0f;
-            float dist = intersect_triangle(lo, ld, tri_ray, A, B, C, w1, w2);
-            if (kAnyHit) {
-                if (dist > 0.000025f && dist < hit.t) {
-                    // Any accepted blocker is a complete proof
-                    // (shaders/traversal.slang:786-792, :1035-1040).
-                    hit.tri = t;
-                    hit.inst = inst;
-                    hit.errors &= ~kQueryUnsupported;
-                    return true;
-                }
-            } else if (dist > lower && hit_better(dist, inst, t, hit)) {
-                hit.t = dist;
-                hit.tri = t;
-                hit.inst = inst;
-                hit.b1 = w1;
-                hit.b2 = w2;
-            }
         }
         return false;
     }

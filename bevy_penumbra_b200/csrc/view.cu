@@ -1097,10 +1097,19 @@ __global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F,
     bool has_children = level + 1u < F.levels;
     const float jb = F.radiance_blend, tb = F.transmittance_blend;
     const float jlimit = 1.0f / (1.0f - jb), tlimit = 1.0f / (1.0f - tb);
+    // A level's records usually fit 32-bit indices: divide in 32 bits then.
+    const bool narrow = n <= 0xffffffffull;
     for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
          e += (unsigned long long)gridDim.x * blockDim.x) {
         uint32_t cnt = V.count[base + e];
-        uint32_t cell = (uint32_t)(e / dirs), d = (uint32_t)(e % dirs);
+        uint32_t cell, d;
+        if (narrow) {
+            cell = (uint32_t)e / dirs;
+            d = (uint32_t)e - cell * dirs;
+        } else {
+            cell = (uint32_t)(e / dirs);
+            d = (uint32_t)(e % dirs);
+        }
         float4 fresh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (cnt) {
             float4 acc = V.accum[base + e];
@@ -1170,8 +1179,16 @@ __global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F,
         if (transmittance > 0.0f && has_children) {
             size_t ci = (size_t)level * F.cell_capacity + cell;
             uint32_t ids[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) ids[k] = __ldg(V.corner_ids + ci * 8 + k);
+            const uint4 *cid = reinterpret_cast<const uint4 *>(V.corner_ids + ci * 8);  // 32-byte rows
+            uint4 c0 = __ldg(cid), c1 = __ldg(cid + 1);
+            ids[0] = c0.x;
+            ids[1] = c0.y;
+            ids[2] = c0.z;
+            ids[3] = c0.w;
+            ids[4] = c1.x;
+            ids[5] = c1.y;
+            ids[6] = c1.z;
+            ids[7] = c1.w;
             float4 frac = __ldg(V.corner_frac + ci);
             uint32_t x = d % F.columns[level], y = d / F.columns[level];
             uint32_t fine_columns = F.columns[level + 1];

@@ -66,7 +66,8 @@ def test_forced_deep_traversal_matches_oracle(blas, internals):
         # a stack of its own.  Either fallback keeps every hit.
         assert_same_overflow(gpu["errors"], cpu["errors"])
         assert np.all((gpu["errors"][hit] & expected) == expected)
-    failures, _ = check_against_f64(oscene, rays, gpu, any_hit=False, expected_errors=expected)
+    # The TLAS chain may also raise the BLAS bit on the device (shared stack).
+    failures, _ = check_against_f64(oscene, rays, gpu, any_hit=False, expected_errors=expected if blas else 3)
     assert not failures, failures[:12]
     blocked = gpu_trace(deep, rays, any_hit=True)
     cblocked, _ = oscene.trace_rays(rays, any_hit=True)
