@@ -860,19 +860,23 @@ def batched_line(args, world, device):
         for j in jobs:
             j["view"].trace_merge(j["scene"], settings, j["pos"].data_ptr(), j["nrm"].data_ptr(), j["n"])
 
-    # Batch launch shape: the project autotuner's blocks-per-SM axis.
+    # Batch launch shape: blocks per SM, the trace stage fused into one
+    # cooperative launch or not, and the work-queue tile (each point: one
+    # untimed frame, then one timed).
     trials = []
     for bps in (8, 16, 32):
-        batch.set_tuning(bps, bps)
-        batched(0)
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        batched(1)
-        end.record(stream)
-        torch.cuda.synchronize(device)
-        trials.append((bps, start.elapsed_time(end)))
-    best_bps = min(trials, key=lambda t: t[1])[0]
-    batch.set_tuning(best_bps, best_bps)
+        for fused in (0, 1):
+            for tile in (32, 128):
+                batch.set_tuning(bps, bps, fused, tile)
+                batched(0)
+                start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                batched(1)
+                end.record(stream)
+                torch.cuda.synchronize(device)
+                trials.append(((bps, fused, tile), start.elapsed_time(end)))
+    best = min(trials, key=lambda t: t[1])[0]
+    batch.set_tuning(best[0], best[0], best[1], best[2])
 
     def timed(fn):
         for step in range(args.warmup):
@@ -905,8 +909,9 @@ def batched_line(args, world, device):
                        "interval_rays": rays, "rays_per_receiver": settings.rays_per_receiver,
                        "l2": f"flushed ({L2_FLUSH_BYTES >> 20} MiB write) between steps"},
             "batch": {"graph_captures": info.graph_captures, "graph_launches": int(info.graph_launches),
-                      "kernels_per_frame": info.kernels_per_frame, "blocks_per_sm": best_bps,
-                      "tuning_trials_ms": [[b, round(t, 3)] for b, t in trials]},
+                      "kernels_per_frame": info.kernels_per_frame,
+                      "tuning": {"blocks_per_sm": best[0], "fused_trace": best[1], "tile_rays": best[2]},
+                      "tuning_trials_ms": [[list(b), round(t, 3)] for b, t in trials]},
             "sequential_views": {"ms_per_step": sequential_ms, "value": rays / (sequential_ms * 1e-3) / 1e6},
             "gpu_launches": args.steps * info.kernels_per_frame,
             "clocks": clocks.summary(), "setup_s": w["setup_s"],

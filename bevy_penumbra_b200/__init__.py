@@ -641,11 +641,24 @@ class Batch:
     def set_graph(self, enable: bool) -> None:
         self.ctx.check(lib().lux_batch_set_graph(self.handle, 1 if enable else 0))
 
-    def set_tuning(self, closest_blocks_per_sm: int = 16, shadow_blocks_per_sm: int = 16) -> None:
+    def set_tuning(self, closest_blocks_per_sm: int = 16, shadow_blocks_per_sm: int = 16, fused_trace: int = 0,
+                   tile_rays: int = 32) -> None:
         t = N.LuxTuning()
         t.closest_blocks_per_sm = closest_blocks_per_sm
         t.shadow_blocks_per_sm = shadow_blocks_per_sm
+        t.fused_trace = fused_trace
+        t.tile_rays = tile_rays
         self.ctx.check(lib().lux_batch_set_tuning(self.handle, C.byref(t)))
+
+    def set_wait(self, limit_ns: int, missing_arrivals: int = 0) -> None:
+        """Bound of each grid-barrier wait of the fused trace launch;
+        missing_arrivals > 0 makes the first wait run out (a test hook)."""
+        self.ctx.check(lib().lux_batch_set_wait(self.handle, int(limit_ns), int(missing_arrivals)))
+
+    def status(self) -> None:
+        """Waits for the last frame; raises LuxError(LUX_ERR_TIMEOUT) when a
+        grid-barrier wait of its fused trace launch ran out."""
+        self.ctx.check(lib().lux_batch_status(self.handle))
 
     def trace_merge(self, jobs, settings: RadianceCascades) -> None:
         """jobs: sequence of (SplitView, GpuScene, position_ptr, normal_ptr, count)."""

@@ -96,7 +96,8 @@ class LuxTimings(C.Structure):
 class LuxTuning(C.Structure):
     _fields_ = [("closest_mode", C.c_uint32), ("shadow_mode", C.c_uint32), ("closest_blocks_per_sm", C.c_uint32),
                 ("shadow_blocks_per_sm", C.c_uint32), ("sort_queries", C.c_uint32), ("sort_rays", C.c_uint32),
-                ("stack_depth", C.c_uint32), ("reserved", C.c_uint32)]
+                ("stack_depth", C.c_uint32), ("fused_trace", C.c_uint32), ("tile_rays", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class LuxCacheDesc(C.Structure):
@@ -218,6 +219,8 @@ SIGNATURES = {
     "lux_batch_set_tuning": (C.c_int, [P, C.POINTER(LuxTuning)]),
     "lux_batch_trace_merge": (C.c_int, [P, P, U32, P]),
     "lux_batch_info": (C.c_int, [P, C.POINTER(LuxBatchInfo)]),
+    "lux_batch_status": (C.c_int, [P]),
+    "lux_batch_set_wait": (C.c_int, [P, C.c_uint64, U32]),
     "lux_screen_create": (C.c_int, [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_void_p)]),
     "lux_screen_destroy": (C.c_int, [P]),
     "lux_screen_reset": (C.c_int, [P]),

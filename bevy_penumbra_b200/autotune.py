@@ -1,10 +1,11 @@
 """Launch-shape autotuner for a view's trace kernels.
 
 Times candidate LuxTunings (traversal scheduling mode of each trace kernel,
-persistent blocks per SM -- the warps-per-SM choice --, traversal stack
-depth, and whether interval rays / visibility queries are put in coherence
-order before tracing) on the caller's own frame with the library's per-stage
-CUDA-event timings, and keeps the fastest.  The winner depends on the scene,
+persistent blocks per SM -- the warps-per-SM choice --, the tile of rays a
+warp takes from the work queue per fetch, traversal stack depth, and whether
+interval rays / visibility queries are put in coherence order before
+tracing) on the caller's own frame with the library's per-stage CUDA-event
+timings, and keeps the fastest.  The winner depends on the scene,
 receivers and settings, so a host engine runs this once per view
 configuration (untimed), like a convolution-algorithm search.
 """
@@ -16,12 +17,14 @@ DEFAULT_SPACE = {
     "closest_mode": (0, 1),
     "shadow_mode": (0, 1),
     "blocks_per_sm": (8, 16, 32),
+    "tile_rays": (32, 64, 128),
     "stack_depth": (32, 64),
     "sort_rays": (0, 1),
     "sort_queries": (0, 1),
 }
 
-START = dict(closest_mode=0, shadow_mode=0, blocks_per_sm=16, stack_depth=64, sort_rays=0, sort_queries=1)
+START = dict(closest_mode=0, shadow_mode=0, blocks_per_sm=16, tile_rays=32, stack_depth=64, sort_rays=0,
+             sort_queries=1)
 
 
 def tuning_of(point: dict) -> dict:
@@ -29,7 +32,8 @@ def tuning_of(point: dict) -> dict:
     both persistent kernels)."""
     return dict(closest_mode=point["closest_mode"], shadow_mode=point["shadow_mode"],
                 closest_blocks_per_sm=point["blocks_per_sm"], shadow_blocks_per_sm=point["blocks_per_sm"],
-                stack_depth=point["stack_depth"], sort_rays=point["sort_rays"], sort_queries=point["sort_queries"])
+                tile_rays=point.get("tile_rays", 32), stack_depth=point["stack_depth"], sort_rays=point["sort_rays"],
+                sort_queries=point["sort_queries"])
 
 
 def candidates(space=None):
@@ -45,7 +49,7 @@ def autotune(view, run_frame, space=None, repeats: int = 2, sweeps: int = 2) -> 
 
     Coordinate search: starting from START, each sweep tries every value of
     one axis at a time with the others at the best point so far (the axes
-    interact little: scheduling, occupancy, stack size, ray and query order),
+    interact little: scheduling, occupancy, tile, stack size, ray and query order),
     `sweeps` times over all axes; every distinct point is timed once (its
     first frame untimed, then the minimum of `repeats` frames' trace stage).
     Returns {"best": tuning, "trace_ms": best time, "trials": [(tuning, ms), ...]}."""

@@ -27,6 +27,7 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
 #include "lux_internal.h"
@@ -46,6 +47,10 @@
 // The batched trace kernels keep a job's scene pointers per warp as well.
 #ifndef LUX_BATCH_MIN_BLOCKS
 #define LUX_BATCH_MIN_BLOCKS 6
+#endif
+// The fused batch trace kernel carries the shading phase's registers too.
+#ifndef LUX_FUSED_MIN_BLOCKS
+#define LUX_FUSED_MIN_BLOCKS 4
 #endif
 
 namespace {
@@ -138,6 +143,9 @@ struct ViewDevice {
     const uint32_t *ray_order;      // closest-hit processing order (nullptr: identity)
     const uint32_t *query_order;    // visibility processing order (nullptr: identity)
 };
+
+// Rays per work-queue fetch of a tuning (0 means 32).
+static inline uint32_t tile_of(const LuxTuning &t) { return t.tile_rays ? t.tile_rays : 32u; }
 
 constexpr uint32_t kSortCells = 4096;           // 16^3 origin cells over the TLAS root box
 constexpr uint32_t kQueryCells = 2097152;       // 128^3 origin cells of visibility queries
@@ -243,18 +251,19 @@ __device__ __forceinline__ uint32_t cell_id(const ViewDevice &V, const FramePara
     return slot == lux::kEmpty ? lux::kEmpty : V.dir_ids[(size_t)level * F.dir_capacity + slot];
 }
 
-__global__ void clear_kernel(ViewDevice V, FrameParams F) {
-    size_t n = (size_t)F.levels * F.dir_capacity;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        V.dir_keys[i] = lux::kEmptyCell;
-        V.dir_ids[i] = lux::kEmpty;
+// Item i of a frame's clear: directory slot i, and with the first items
+// the per-level counters, statistics, error word and trace counters (the
+// directory has at least 64 slots per level).
+__device__ __forceinline__ void clear_item(const ViewDevice &V, const FrameParams &F, unsigned long long i) {
+    if (i >= (unsigned long long)F.levels * F.dir_capacity) return;
+    V.dir_keys[i] = lux::kEmptyCell;
+    V.dir_ids[i] = lux::kEmpty;
+    if (i < LUX_MAX_LEVELS) {
+        V.cell_count[i] = 0;
+        V.level_base[i] = 0;
     }
-    if (blockIdx.x == 0 && threadIdx.x < LUX_MAX_LEVELS) {
-        V.cell_count[threadIdx.x] = 0;
-        V.level_base[threadIdx.x] = 0;
-    }
-    if (blockIdx.x == 0 && threadIdx.x < 16) V.stats[threadIdx.x] = 0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (i < 16) V.stats[i] = 0;
+    if (i == 0) {
         *V.error_flags = 0;
         *V.ts.queue_count = 0;
         V.ts.work_counter[0] = 0;
@@ -262,11 +271,17 @@ __global__ void clear_kernel(ViewDevice V, FrameParams F) {
     }
 }
 
+__global__ void clear_kernel(ViewDevice V, FrameParams F) {
+    size_t n = (size_t)F.levels * F.dir_capacity;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        clear_item(V, F, i);
+}
+
 // seed: insert every receiver's cell of every level (insertProbeDescriptor,
 // shaders/split.slang:292-319, with a 64-bit key compare-and-swap); in an
 // LOD overlap both LOD variants' cells are seeded (seed,
 // shaders/split.slang:758-786).
-__device__ __forceinline__ void seed_cell(ViewDevice &V, const FrameParams &F, uint32_t level, f3 p, uint32_t lod) {
+__device__ __forceinline__ void seed_cell(const ViewDevice &V, const FrameParams &F, uint32_t level, f3 p, uint32_t lod) {
     int32_t x, y, z;
     cell_of(F, level, p, x, y, z, lod);
     if (!lux::cell_in_range(x, y, z)) {
@@ -284,41 +299,51 @@ __device__ __forceinline__ void seed_cell(ViewDevice &V, const FrameParams &F, u
     atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
 }
 
+// Item i = receiver x levels + level.
+__device__ __forceinline__ void seed_insert_item(const ViewDevice &V, const FrameParams &F, const float4 *__restrict__ pos,
+                                                 unsigned long long i) {
+    if (i >= (unsigned long long)F.receivers * F.levels) return;
+    uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
+    float4 p = pos[r];
+    if (F.sparse && p.w == 0.0f) return;
+    const f3 q{p.x, p.y, p.z};
+    uint32_t low, high;
+    float blend;
+    point_lod(F, q, low, high, blend);
+    seed_cell(V, F, level, q, low);
+    if (high != low) seed_cell(V, F, level, q, high);
+}
+
 __global__ void seed_insert_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
     size_t n = (size_t)F.receivers * F.levels;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
-        float4 p = pos[r];
-        if (F.sparse && p.w == 0.0f) continue;
-        const f3 q{p.x, p.y, p.z};
-        uint32_t low, high;
-        float blend;
-        point_lod(F, q, low, high, blend);
-        seed_cell(V, F, level, q, low);
-        if (high != low) seed_cell(V, F, level, q, high);
-    }
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        seed_insert_item(V, F, pos, i);
 }
 
 // rank: dense ids for occupied directory slots.
+__device__ __forceinline__ void seed_assign_item(const ViewDevice &V, const FrameParams &F, unsigned long long i) {
+    if (i >= (unsigned long long)F.levels * F.dir_capacity) return;
+    unsigned long long key = V.dir_keys[i];
+    if (key == lux::kEmptyCell) return;
+    uint32_t level = (uint32_t)(i / F.dir_capacity);
+    uint32_t id = atomicAdd(&V.cell_count[level], 1u);
+    if (id >= F.cell_capacity) {
+        atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
+        V.dir_ids[i] = lux::kEmpty;
+        return;
+    }
+    V.dir_ids[i] = id;
+    int32_t x, y, z;
+    uint32_t lod;
+    lux::unpack_cell(key, x, y, z, lod);
+    V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)((level << 12) | (lod << 18)));
+    V.cell_last[(size_t)level * F.cell_capacity + id] = F.shade.frame;
+}
+
 __global__ void seed_assign_kernel(ViewDevice V, FrameParams F) {
     size_t n = (size_t)F.levels * F.dir_capacity;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        unsigned long long key = V.dir_keys[i];
-        if (key == lux::kEmptyCell) continue;
-        uint32_t level = (uint32_t)(i / F.dir_capacity);
-        uint32_t id = atomicAdd(&V.cell_count[level], 1u);
-        if (id >= F.cell_capacity) {
-            atomicOr(V.error_flags, LUX_VIEW_ERR_CELL_CAPACITY);
-            V.dir_ids[i] = lux::kEmpty;
-            continue;
-        }
-        V.dir_ids[i] = id;
-        int32_t x, y, z;
-        uint32_t lod;
-        lux::unpack_cell(key, x, y, z, lod);
-        V.cell_keys[(size_t)level * F.cell_capacity + id] = make_int4(x, y, z, (int32_t)((level << 12) | (lod << 18)));
-        V.cell_last[(size_t)level * F.cell_capacity + id] = F.shade.frame;
-    }
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        seed_assign_item(V, F, i);
 }
 
 // Sample sequence order (the reference's rank / parents / prefix passes,
@@ -345,33 +370,40 @@ __global__ void ordinal_kernel(ViewDevice V, const uint32_t *__restrict__ sorted
         V.receiver_ordinal[sorted[j]] = j;
 }
 
+// Item i = receiver x levels + level; the receiver's sequence key and index
+// go to keys[r], vals[r].
+__device__ __forceinline__ void seed_lookup_item(const ViewDevice &V, const FrameParams &F,
+                                                 const float4 *__restrict__ pos, unsigned long long i,
+                                                 unsigned long long *keys, uint32_t *vals) {
+    if (i >= (unsigned long long)F.receivers * F.levels) return;
+    uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
+    float4 p = pos[r];
+    const f3 q{p.x, p.y, p.z};
+    // The variant this receiver's rays deposit into (one trace per
+    // receiver; in an LOD overlap the high LOD with probability blend).
+    uint32_t low, high;
+    float blend;
+    point_lod(F, q, low, high, blend);
+    uint32_t lod = high != low && lux::lod_selects_high(r, F.shade.frame, blend) ? high : low;
+    if (level == 0u) V.receiver_lod[r] = lod;
+    int32_t x, y, z;
+    cell_of(F, level, q, x, y, z, lod);
+    if (level == 0u) {
+        keys[r] = F.sparse && p.w == 0.0f ? ~0ull : sequence_key(x, y, z, lod);
+        vals[r] = r;
+    }
+    V.receiver_cell[(size_t)level * F.receivers + r] =
+        F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z, lod);
+}
+
 __global__ void seed_lookup_kernel(ViewDevice V, FrameParams F, const float4 *__restrict__ pos) {
     size_t n = (size_t)F.receivers * F.levels;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        uint32_t r = (uint32_t)(i / F.levels), level = (uint32_t)(i % F.levels);
-        float4 p = pos[r];
-        const f3 q{p.x, p.y, p.z};
-        // The variant this receiver's rays deposit into (one trace per
-        // receiver; in an LOD overlap the high LOD with probability blend).
-        uint32_t low, high;
-        float blend;
-        point_lod(F, q, low, high, blend);
-        uint32_t lod = high != low && lux::lod_selects_high(r, F.shade.frame, blend) ? high : low;
-        if (level == 0u) V.receiver_lod[r] = lod;
-        int32_t x, y, z;
-        cell_of(F, level, q, x, y, z, lod);
-        if (level == 0u) {
-            V.order_keys[r] = F.sparse && p.w == 0.0f ? ~0ull : sequence_key(x, y, z, lod);
-            V.order_vals[r] = r;
-        }
-        V.receiver_cell[(size_t)level * F.receivers + r] =
-            F.sparse && p.w == 0.0f ? lux::kEmpty : cell_id(V, F, level, x, y, z, lod);
-    }
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        seed_lookup_item(V, F, pos, i, V.order_keys, V.order_vals);
 }
 
 // Per-level record offsets; the entry capacity bounds the whole frame.
-__global__ void layout_kernel(ViewDevice V, FrameParams F) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void layout_view(const ViewDevice &V, const FrameParams &F) {
     unsigned long long base = 0;
     for (uint32_t l = 0; l < F.levels; ++l) {
         uint32_t cells = min(V.cell_count[l], F.cell_capacity);
@@ -383,20 +415,27 @@ __global__ void layout_kernel(ViewDevice V, FrameParams F) {
     if (F.layout == LUX_LAYOUT_DENSE && base > F.ray_capacity) atomicOr(V.error_flags, LUX_VIEW_ERR_RAY_CAPACITY);
 }
 
+__global__ void layout_kernel(ViewDevice V, FrameParams F) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) layout_view(V, F);
+}
+
 __device__ __forceinline__ unsigned long long total_entries(const ViewDevice &V, const FrameParams &F) {
     unsigned long long base = 0;
     for (uint32_t l = 0; l < F.levels; ++l) base += (unsigned long long)V.cell_count[l] * F.dirs[l];
     return base;
 }
 
+__device__ __forceinline__ void clear_entry(const ViewDevice &V, unsigned long long i) {
+    V.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    V.count[i] = 0u;
+}
+
 __global__ void clear_entries_kernel(ViewDevice V, FrameParams F) {
     if (*V.error_flags) return;
     unsigned long long n = total_entries(V, F);
     for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
-         i += (unsigned long long)gridDim.x * blockDim.x) {
-        V.accum[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        V.count[i] = 0u;
-    }
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        clear_entry(V, i);
 }
 
 // ---------------------------------------------------------------------------
@@ -515,26 +554,30 @@ __device__ __forceinline__ bool closest_split_ray(const ViewDevice &V, const Fra
     return true;
 }
 
-// Persistent warps, 32 consecutive rays per fetch (one atomic per warp).
-__device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter) {
+// Persistent warps: a tile of `tile` consecutive rays per fetch (one atomic
+// per warp), taken 32 at a time.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter, uint32_t tile = 32u) {
     uint32_t base = 0;
-    if ((threadIdx.x & 31u) == 0u) base = atomicAdd(counter, 32u);
+    if ((threadIdx.x & 31u) == 0u) base = atomicAdd(counter, tile);
     return __shfl_sync(0xffffffffu, base, 0);
 }
 
 template <int kDepth>
 __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                             const float4 *__restrict__ pos,
-                                                            const float4 *__restrict__ nrm, uint32_t ray_count) {
+                                                            const float4 *__restrict__ nrm, uint32_t ray_count,
+                                                            uint32_t tile) {
     if (*V.error_flags) return;
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(&V.ts.work_counter[0]);
+        uint32_t base = warp_fetch(&V.ts.work_counter[0], tile);
         if (base >= ray_count) break;
-        uint32_t slot = base + (threadIdx.x & 31u);
-        if (slot < ray_count && closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn))
-            st[kStatInterval] += 1;
+        for (uint32_t k = 0; k < tile && base + k < ray_count; k += 32u) {
+            uint32_t slot = base + k + (threadIdx.x & 31u);
+            if (slot < ray_count && closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn))
+                st[kStatInterval] += 1;
+        }
     }
     st[kStatNodes] = cn.nodes;
     st[kStatTris] = cn.triangles;
@@ -736,18 +779,21 @@ __device__ __forceinline__ void shadow_query(const ViewDevice &V, const SceneVie
 }
 
 template <int kDepth>
-__global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S) {
+__global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S,
+                                                                             uint32_t tile) {
     if (*V.error_flags) return;
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(&V.ts.work_counter[1]);
+        uint32_t base = warp_fetch(&V.ts.work_counter[1], tile);
         if (base >= n) break;
-        uint32_t i = base + (threadIdx.x & 31u);
-        if (i < n) {
-            shadow_query<kDepth>(V, S, i, cn);
-            st[kStatShadow] += 1;
+        for (uint32_t k = 0; k < tile && base + k < n; k += 32u) {
+            uint32_t i = base + k + (threadIdx.x & 31u);
+            if (i < n) {
+                shadow_query<kDepth>(V, S, i, cn);
+                st[kStatShadow] += 1;
+            }
         }
     }
     st[kStatNodes] = cn.nodes;
@@ -865,25 +911,28 @@ __global__ void __launch_bounds__(128) deposit_dense_kernel(ViewDevice V, FrameP
 
 // Spatial corners of every cell of `level` in level + 1 (mergeRadianceGroups
 // grid, shaders/split.slang:1590-1596).
+__device__ __forceinline__ void corners_item(const ViewDevice &V, const FrameParams &F, uint32_t level, uint32_t c) {
+    int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+    // A cell's children are the next level's cells of the same LOD.
+    const uint32_t lod = lux::key_lod(key.w);
+    const float sp = level_spacing(F, level, lod), sp1 = level_spacing(F, level + 1, lod);
+    float ox = ((float)key.x + 0.5f) * sp, oy = ((float)key.y + 0.5f) * sp, oz = ((float)key.z + 0.5f) * sp;
+    float gx = ox / sp1 - 0.5f, gy = oy / sp1 - 0.5f, gz = oz / sp1 - 0.5f;
+    float fx = floorf(gx), fy = floorf(gy), fz = floorf(gz);
+    int32_t bx = (int32_t)fx, by = (int32_t)fy, bz = (int32_t)fz;
+    V.corner_frac[(size_t)level * F.cell_capacity + c] = make_float4(gx - fx, gy - fy, gz - fz, 0.0f);
+    uint32_t *ids = V.corner_ids + ((size_t)level * F.cell_capacity + c) * 8;
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner)
+        ids[corner] = cell_id(V, F, level + 1, bx + (int32_t)(corner & 1u), by + (int32_t)((corner >> 1) & 1u),
+                              bz + (int32_t)(corner >> 2), lod);
+}
+
 __global__ void corners_kernel(ViewDevice V, FrameParams F, uint32_t level) {
     if (*V.error_flags) return;
     uint32_t cells = V.cell_count[level];
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
-        int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
-        // A cell's children are the next level's cells of the same LOD.
-        const uint32_t lod = lux::key_lod(key.w);
-        const float sp = level_spacing(F, level, lod), sp1 = level_spacing(F, level + 1, lod);
-        float ox = ((float)key.x + 0.5f) * sp, oy = ((float)key.y + 0.5f) * sp, oz = ((float)key.z + 0.5f) * sp;
-        float gx = ox / sp1 - 0.5f, gy = oy / sp1 - 0.5f, gz = oz / sp1 - 0.5f;
-        float fx = floorf(gx), fy = floorf(gy), fz = floorf(gz);
-        int32_t bx = (int32_t)fx, by = (int32_t)fy, bz = (int32_t)fz;
-        V.corner_frac[(size_t)level * F.cell_capacity + c] = make_float4(gx - fx, gy - fy, gz - fz, 0.0f);
-        uint32_t *ids = V.corner_ids + ((size_t)level * F.cell_capacity + c) * 8;
-#pragma unroll
-        for (uint32_t corner = 0; corner < 8u; ++corner)
-            ids[corner] = cell_id(V, F, level + 1, bx + (int32_t)(corner & 1u), by + (int32_t)((corner >> 1) & 1u),
-                                  bz + (int32_t)(corner >> 2), lod);
-    }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x)
+        corners_item(V, F, level, c);
 }
 
 // interpolateMergedChildSources, shaders/split.slang:389-479 (one group).
@@ -1089,19 +1138,131 @@ __global__ void retain_insert_kernel(ViewDevice V, FrameParams F, HistoryDevice 
 // 1 / (1 - blend); :1478-1521) for the summed radiance group and for the
 // transmittance, then Eq. 7 with the children: I = [J (1 - beta) + beta
 // mean_4(trilerp_8(I_child) support)] / support.
-__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
-    if (*V.error_flags) return;
-    uint32_t dirs = F.dirs[level];
-    unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
-    unsigned long long base = V.level_base[level];
-    bool has_children = level + 1u < F.levels;
+// Record (cell, d) of `level`; base = the level's first record.
+__device__ __forceinline__ void merge_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                             uint32_t level, unsigned long long base, uint32_t dirs, uint32_t cell,
+                                             uint32_t d) {
+    const unsigned long long e = (unsigned long long)cell * dirs + d;
+    const bool has_children = level + 1u < F.levels;
     const float jb = F.radiance_blend, tb = F.transmittance_blend;
     const float jlimit = 1.0f / (1.0f - jb), tlimit = 1.0f / (1.0f - tb);
+    uint32_t cnt = V.count[base + e];
+    float4 fresh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (cnt) {
+        float4 acc = V.accum[base + e];
+        float fn = (float)cnt;
+        fresh = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
+    }
+    // History of this record.
+    bool reuse = false;
+    float4 old = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float2 old_mass = make_float2(0.0f, 0.0f);
+    if (F.history) {
+        uint32_t prev = V.hist_cell[(size_t)level * F.cell_capacity + cell];
+        if (prev != lux::kEmpty) {
+            unsigned long long r = H.level_base[level] + (unsigned long long)prev * dirs + d;
+            old = H.raw[r];
+            old_mass = H.mass[r];
+            reuse = true;
+        }
+    }
+    float rm = old_mass.x, tm = old_mass.y;
+    if (!isfinite(rm) || rm < 0.0f) rm = 0.0f;
+    if (!isfinite(tm) || tm < 0.0f) tm = 0.0f;
+    const bool reuse_r = reuse && jb > 0.0f, reuse_t = reuse && tb > 0.0f;
+    float jx = 0.0f, jy = 0.0f, jz = 0.0f, beta = 1.0f, rmass = 0.0f, tmass = 0.0f;
+    if (cnt) {
+        float ret = pow_count(jb, cnt);
+        rmass = (1.0f - ret) * jlimit;
+        jx = fresh.x;
+        jy = fresh.y;
+        jz = fresh.z;
+        float om = fminf(rm, jlimit) * ret;
+        if (reuse_r && om > 0.0f) {
+            jx = (jx * rmass + old.x * om) / (rmass + om);
+            jy = (jy * rmass + old.y * om) / (rmass + om);
+            jz = (jz * rmass + old.z * om) / (rmass + om);
+            rmass = rmass + om;
+        }
+        float tret = pow_count(tb, cnt);
+        tmass = (1.0f - tret) * tlimit;
+        beta = fresh.w;
+        float otm = fminf(tm, tlimit) * tret;
+        if (reuse_t && otm > 0.0f) {
+            beta = (beta * tmass + old.w * otm) / (tmass + otm);
+            tmass = tmass + otm;
+        }
+    } else {
+        if (reuse_r && rm > 0.0f) {
+            jx = old.x;
+            jy = old.y;
+            jz = old.z;
+            rmass = rm;
+        }
+        if (reuse_t && tm > 0.0f) {
+            beta = old.w;
+            tmass = tm;
+        }
+    }
+    float transmittance = tmass > 0.0f ? lux::saturate(beta) : 0.0f;
+    float support = rmass > 0.0f && tmass > 0.0f ? 1.0f - transmittance : 0.0f;
+    float rx = 0.0f, ry = 0.0f, rz = 0.0f;
+    if (support > 0.0f) {
+        rx = jx;
+        ry = jy;
+        rz = jz;
+    }
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
+    if (transmittance > 0.0f && has_children) {
+        size_t ci = (size_t)level * F.cell_capacity + cell;
+        uint32_t ids[8];
+        const uint4 *cid = reinterpret_cast<const uint4 *>(V.corner_ids + ci * 8);  // 32-byte rows
+        uint4 c0 = __ldg(cid), c1 = __ldg(cid + 1);
+        ids[0] = c0.x;
+        ids[1] = c0.y;
+        ids[2] = c0.z;
+        ids[3] = c0.w;
+        ids[4] = c1.x;
+        ids[5] = c1.y;
+        ids[6] = c1.z;
+        ids[7] = c1.w;
+        float4 frac = __ldg(V.corner_frac + ci);
+        uint32_t x = d % F.columns[level], y = d / F.columns[level];
+        uint32_t fine_columns = F.columns[level + 1];
+#pragma unroll
+        for (uint32_t child = 0; child < 4u; ++child) {
+            uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
+            float4 v = interpolate(V, F, level + 1, ids, frac, fine);
+            if (!(v.w > 0.0f)) continue;
+            cx = cx + v.x * v.w;
+            cy = cy + v.y * v.w;
+            cz = cz + v.z * v.w;
+            csup += v.w;
+        }
+    }
+    if (csup > 0.0f) {
+        rx = rx + (transmittance * cx) * 0.25f;
+        ry = ry + (transmittance * cy) * 0.25f;
+        rz = rz + (transmittance * cz) * 0.25f;
+        support = support + (transmittance * csup) * 0.25f;
+    }
+    float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
+    V.merged[base + e] = out;
+    V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
+                                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    V.mass[base + e] = make_float2(rmass, tmass);
+}
+
+__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
+    if (*V.error_flags) return;
+    const uint32_t dirs = F.dirs[level];
+    const unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
+    const unsigned long long base = V.level_base[level];
     // A level's records usually fit 32-bit indices: divide in 32 bits then.
     const bool narrow = n <= 0xffffffffull;
     for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
          e += (unsigned long long)gridDim.x * blockDim.x) {
-        uint32_t cnt = V.count[base + e];
         uint32_t cell, d;
         if (narrow) {
             cell = (uint32_t)e / dirs;
@@ -1110,162 +1271,66 @@ __global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F,
             cell = (uint32_t)(e / dirs);
             d = (uint32_t)(e % dirs);
         }
-        float4 fresh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (cnt) {
-            float4 acc = V.accum[base + e];
-            float fn = (float)cnt;
-            fresh = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
-        }
-        // History of this record.
-        bool reuse = false;
-        float4 old = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float2 old_mass = make_float2(0.0f, 0.0f);
-        if (F.history) {
-            uint32_t prev = V.hist_cell[(size_t)level * F.cell_capacity + cell];
-            if (prev != lux::kEmpty) {
-                unsigned long long r = H.level_base[level] + (unsigned long long)prev * dirs + d;
-                old = H.raw[r];
-                old_mass = H.mass[r];
-                reuse = true;
-            }
-        }
-        float rm = old_mass.x, tm = old_mass.y;
-        if (!isfinite(rm) || rm < 0.0f) rm = 0.0f;
-        if (!isfinite(tm) || tm < 0.0f) tm = 0.0f;
-        const bool reuse_r = reuse && jb > 0.0f, reuse_t = reuse && tb > 0.0f;
-        float jx = 0.0f, jy = 0.0f, jz = 0.0f, beta = 1.0f, rmass = 0.0f, tmass = 0.0f;
-        if (cnt) {
-            float ret = pow_count(jb, cnt);
-            rmass = (1.0f - ret) * jlimit;
-            jx = fresh.x;
-            jy = fresh.y;
-            jz = fresh.z;
-            float om = fminf(rm, jlimit) * ret;
-            if (reuse_r && om > 0.0f) {
-                jx = (jx * rmass + old.x * om) / (rmass + om);
-                jy = (jy * rmass + old.y * om) / (rmass + om);
-                jz = (jz * rmass + old.z * om) / (rmass + om);
-                rmass = rmass + om;
-            }
-            float tret = pow_count(tb, cnt);
-            tmass = (1.0f - tret) * tlimit;
-            beta = fresh.w;
-            float otm = fminf(tm, tlimit) * tret;
-            if (reuse_t && otm > 0.0f) {
-                beta = (beta * tmass + old.w * otm) / (tmass + otm);
-                tmass = tmass + otm;
-            }
-        } else {
-            if (reuse_r && rm > 0.0f) {
-                jx = old.x;
-                jy = old.y;
-                jz = old.z;
-                rmass = rm;
-            }
-            if (reuse_t && tm > 0.0f) {
-                beta = old.w;
-                tmass = tm;
-            }
-        }
-        float transmittance = tmass > 0.0f ? lux::saturate(beta) : 0.0f;
-        float support = rmass > 0.0f && tmass > 0.0f ? 1.0f - transmittance : 0.0f;
-        float rx = 0.0f, ry = 0.0f, rz = 0.0f;
-        if (support > 0.0f) {
-            rx = jx;
-            ry = jy;
-            rz = jz;
-        }
-        float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
-        if (transmittance > 0.0f && has_children) {
-            size_t ci = (size_t)level * F.cell_capacity + cell;
-            uint32_t ids[8];
-            const uint4 *cid = reinterpret_cast<const uint4 *>(V.corner_ids + ci * 8);  // 32-byte rows
-            uint4 c0 = __ldg(cid), c1 = __ldg(cid + 1);
-            ids[0] = c0.x;
-            ids[1] = c0.y;
-            ids[2] = c0.z;
-            ids[3] = c0.w;
-            ids[4] = c1.x;
-            ids[5] = c1.y;
-            ids[6] = c1.z;
-            ids[7] = c1.w;
-            float4 frac = __ldg(V.corner_frac + ci);
-            uint32_t x = d % F.columns[level], y = d / F.columns[level];
-            uint32_t fine_columns = F.columns[level + 1];
-#pragma unroll
-            for (uint32_t child = 0; child < 4u; ++child) {
-                uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
-                float4 v = interpolate(V, F, level + 1, ids, frac, fine);
-                if (!(v.w > 0.0f)) continue;
-                cx = cx + v.x * v.w;
-                cy = cy + v.y * v.w;
-                cz = cz + v.z * v.w;
-                csup += v.w;
-            }
-        }
-        if (csup > 0.0f) {
-            rx = rx + (transmittance * cx) * 0.25f;
-            ry = ry + (transmittance * cy) * 0.25f;
-            rz = rz + (transmittance * cz) * 0.25f;
-            support = support + (transmittance * csup) * 0.25f;
-        }
-        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
-        V.merged[base + e] = out;
-        V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
-                                                                 : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        V.mass[base + e] = make_float2(rmass, tmass);
+        merge_record(V, F, H, level, base, dirs, cell, d);
     }
 }
 
 // packProbes, shaders/split.slang:1786-1918: one block per cascade-0 cell.
-__global__ void __launch_bounds__(64) pack_kernel(ViewDevice V, FrameParams F) {
-    if (*V.error_flags) return;
-    extern __shared__ float4 smem[];
-    const uint32_t dirs = F.dirs[0];
-    float4 *val = smem;                                   // [dirs]
-    float4 *dir = smem + dirs;                            // [dirs] xyz
-    uint32_t cells = V.cell_count[0];
-    for (uint32_t d = threadIdx.x; d < dirs; d += blockDim.x) {
+// The cascade-0 bin directions of a view (the block's shared table).
+__device__ __forceinline__ void pack_directions(const FrameParams &F, float4 *dir) {
+    for (uint32_t d = threadIdx.x; d < F.dirs[0]; d += blockDim.x) {
         f3 b = lux::bin_direction(d, F.columns[0], F.rows[0]);
         dir[d] = make_float4(b.x, b.y, b.z, 0.0f);
     }
-    for (uint32_t cell = blockIdx.x; cell < cells; cell += gridDim.x) {
-        __syncthreads();
-        for (uint32_t d = threadIdx.x; d < dirs; d += blockDim.x) {
-            float4 m = V.merged[V.level_base[0] + (unsigned long long)cell * dirs + d];
-            bool ok = m.w > 0.0f && isfinite(m.x) && isfinite(m.y) && isfinite(m.z) && isfinite(m.w);
-            val[d] = ok ? m : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        }
-        __syncthreads();
-        if (threadIdx.x < 36u) {
-            uint32_t texel = threadIdx.x;
-            f3 normal = lux::decode_normal(((float)(texel % 6u) + 0.5f) / 6.0f, ((float)(texel / 6u) + 0.5f) / 6.0f);
-            float sx = 0.0f, sy = 0.0f, sz = 0.0f, nominal = 0.0f, observed = 0.0f;
-            for (uint32_t d = 0; d < dirs; ++d) {
-                float4 dv = dir[d];
-                float cosine = fmaxf(lux::dot(normal, f3{dv.x, dv.y, dv.z}), 0.0f);
-                nominal += cosine;
-                if (cosine <= 0.0f) continue;
-                float4 v = val[d];
-                if (v.w > 0.0f) {
-                    float w = cosine * lux::saturate(v.w);
-                    sx = sx + v.x * w;
-                    sy = sy + v.y * w;
-                    sz = sz + v.z * w;
-                    observed += w;
-                }
-            }
-            float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (nominal > 0.0f) {
-                float scale = nominal * (4.0f / (float)dirs);
-                if (observed > 0.0f)
-                    out = make_float4((sx / observed) * scale, (sy / observed) * scale, (sz / observed) * scale,
-                                      lux::saturate(observed / nominal));
-            }
-            V.tables[(size_t)cell * 36 + texel] = out;
-        }
+}
+
+// One cascade-0 cell's 36 texels, by the whole block (val: [dirs] shared).
+__device__ __forceinline__ void pack_cell(const ViewDevice &V, const FrameParams &F, uint32_t cell, float4 *val,
+                                          const float4 *dir) {
+    const uint32_t dirs = F.dirs[0];
+    __syncthreads();
+    for (uint32_t d = threadIdx.x; d < dirs; d += blockDim.x) {
+        float4 m = V.merged[V.level_base[0] + (unsigned long long)cell * dirs + d];
+        bool ok = m.w > 0.0f && isfinite(m.x) && isfinite(m.y) && isfinite(m.z) && isfinite(m.w);
+        val[d] = ok ? m : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
+    __syncthreads();
+    if (threadIdx.x < 36u) {
+        uint32_t texel = threadIdx.x;
+        f3 normal = lux::decode_normal(((float)(texel % 6u) + 0.5f) / 6.0f, ((float)(texel / 6u) + 0.5f) / 6.0f);
+        float sx = 0.0f, sy = 0.0f, sz = 0.0f, nominal = 0.0f, observed = 0.0f;
+        for (uint32_t d = 0; d < dirs; ++d) {
+            float4 dv = dir[d];
+            float cosine = fmaxf(lux::dot(normal, f3{dv.x, dv.y, dv.z}), 0.0f);
+            nominal += cosine;
+            if (cosine <= 0.0f) continue;
+            float4 v = val[d];
+            if (v.w > 0.0f) {
+                float w = cosine * lux::saturate(v.w);
+                sx = sx + v.x * w;
+                sy = sy + v.y * w;
+                sz = sz + v.z * w;
+                observed += w;
+            }
+        }
+        float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (nominal > 0.0f) {
+            float scale = nominal * (4.0f / (float)dirs);
+            if (observed > 0.0f)
+                out = make_float4((sx / observed) * scale, (sy / observed) * scale, (sz / observed) * scale,
+                                  lux::saturate(observed / nominal));
+        }
+        V.tables[(size_t)cell * 36 + texel] = out;
+    }
+}
+
+__global__ void __launch_bounds__(64) pack_kernel(ViewDevice V, FrameParams F) {
+    if (*V.error_flags) return;
+    extern __shared__ float4 smem[];
+    float4 *val = smem;            // [dirs]
+    float4 *dir = smem + F.dirs[0]; // [dirs] xyz
+    pack_directions(F, dir);
+    for (uint32_t cell = blockIdx.x; cell < V.cell_count[0]; cell += gridDim.x) pack_cell(V, F, cell, val, dir);
 }
 
 // diffuseAtLod (shaders/world_resolve.slang:96-150): trilinear over the 8
@@ -1416,37 +1481,40 @@ __device__ __forceinline__ void flush_stats(unsigned long long *stats, unsigned 
     cn = lux::TraceCounters{0, 0, 0};
 }
 
-__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
-    closest_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
-                         uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counter) {
-    const uint32_t fr = *frame;
+// The four trace phases over all jobs' rays and queries; each is a kernel of
+// its own or one phase of trace_batch_kernel.
+// A tile of `tile` rays may span jobs: the job is found per 32-ray chunk.
+__device__ __forceinline__ void closest_batch_phase(const BatchJob *__restrict__ jobs,
+                                                    const uint32_t *__restrict__ begin, uint32_t n, uint32_t total,
+                                                    uint32_t fr, uint32_t *counter, uint32_t tile) {
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t cur = lux::kEmpty;
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(counter);
-        if (base >= total) break;
-        uint32_t j = find_job(begin, n, base);
-        const BatchJob &J = jobs[j];
-        if (j != cur) {
-            if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
-            cur = j;
-        }
-        if (*J.V.error_flags) continue;
-        uint32_t slot = base - __ldg(begin + j) + lane;
-        if (slot < J.rays) {
-            SceneView S = J.S;
-            closest_split_ray(J.V, J.F, fr, S, J.pos, J.nrm, slot, cn);
-            st[kStatInterval] += 1;
+        const uint32_t first = warp_fetch(counter, tile);
+        if (first >= total) break;
+        for (uint32_t base = first; base < first + tile && base < total; base += 32u) {
+            uint32_t j = find_job(begin, n, base);
+            const BatchJob &J = jobs[j];
+            if (j != cur) {
+                if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
+                cur = j;
+            }
+            if (*J.V.error_flags) continue;
+            uint32_t slot = base - __ldg(begin + j) + lane;
+            if (slot < J.rays) {
+                SceneView S = J.S;
+                closest_split_ray(J.V, J.F, fr, S, J.pos, J.nrm, slot, cn);
+                st[kStatInterval] += 1;
+            }
         }
     }
     if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
 }
 
-__global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__restrict__ jobs,
-                                                          const uint32_t *__restrict__ begin, uint32_t n,
-                                                          uint32_t total, const uint32_t *__restrict__ frame) {
+__device__ __forceinline__ void shade_batch_phase(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin,
+                                                  uint32_t n, uint32_t total, uint32_t fr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total / 32u; w += warps) {
@@ -1455,7 +1523,7 @@ __global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__rest
         const BatchJob &J = jobs[j];
         if (*J.V.error_flags) continue;
         lux::ShadeParams P = J.F.shade;
-        P.frame = *frame;
+        P.frame = fr;
         SceneView S = J.S;
         shade_warp(J.V, J.F, P, S, base - __ldg(begin + j) + lane, J.rays);
     }
@@ -1466,47 +1534,83 @@ __device__ __forceinline__ uint32_t job_queries(const BatchJob &J) {
 }
 
 // Padded prefix of every job's visibility-query count (known only on the
-// device after shading); qbegin[n] is the padded total.
-__global__ void query_prefix_kernel(const BatchJob *__restrict__ jobs, uint32_t n, uint32_t *__restrict__ qbegin) {
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+// device after shading); qbegin[n] is the padded total.  One block: each
+// thread sums a run of jobs, thread 0 scans the runs.
+__device__ __forceinline__ void query_prefix_block(const BatchJob *__restrict__ jobs, uint32_t n,
+                                                   uint32_t *__restrict__ qbegin) {
+    __shared__ uint32_t run[128];
+    const uint32_t t = threadIdx.x, threads = min(blockDim.x, 128u);
+    const uint32_t chunk = (n + threads - 1u) / threads;
+    const uint32_t lo = min(n, t * chunk), hi = min(n, lo + chunk);
     uint32_t sum = 0;
-    for (uint32_t j = 0; j < n; ++j) {
-        qbegin[j] = sum;
-        sum += (job_queries(jobs[j]) + 31u) & ~31u;
+    if (t < threads)
+        for (uint32_t j = lo; j < hi; ++j) sum += (job_queries(jobs[j]) + 31u) & ~31u;
+    if (t < threads) run[t] = sum;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t acc = 0;
+        for (uint32_t k = 0; k < threads; ++k) {
+            uint32_t v = run[k];
+            run[k] = acc;
+            acc += v;
+        }
+        qbegin[n] = acc;
     }
-    qbegin[n] = sum;
+    __syncthreads();
+    if (t < threads) {
+        uint32_t acc = run[t];
+        for (uint32_t j = lo; j < hi; ++j) {
+            qbegin[j] = acc;
+            acc += (job_queries(jobs[j]) + 31u) & ~31u;
+        }
+    }
 }
 
-__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
-    shadow_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ qbegin, uint32_t n,
-                        uint32_t *counter) {
+// qbegin is written on the device in the same launch when the trace stage
+// is fused: it is read with coherent loads (no read-only path).
+__device__ __forceinline__ uint32_t find_query_job(const uint32_t *qbegin, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (qbegin[mid] <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void shadow_batch_phase(const BatchJob *__restrict__ jobs, const uint32_t *qbegin,
+                                                   uint32_t n, uint32_t *counter, uint32_t tile) {
     const uint32_t total = qbegin[n];
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t cur = lux::kEmpty;
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
-        uint32_t base = warp_fetch(counter);
-        if (base >= total) break;
-        uint32_t j = find_job(qbegin, n, base);
-        const BatchJob &J = jobs[j];
-        if (j != cur) {
-            if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
-            cur = j;
-        }
-        uint32_t i = base - qbegin[j] + lane;
-        if (i < job_queries(J)) {
-            SceneView S = J.S;
-            shadow_query(J.V, S, i, cn);
-            st[kStatShadow] += 1;
+        const uint32_t first = warp_fetch(counter, tile);
+        if (first >= total) break;
+        for (uint32_t base = first; base < first + tile && base < total; base += 32u) {
+            uint32_t j = find_query_job(qbegin, n, base);
+            const BatchJob &J = jobs[j];
+            if (j != cur) {
+                if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
+                cur = j;
+            }
+            uint32_t i = base - qbegin[j] + lane;
+            if (i < job_queries(J)) {
+                SceneView S = J.S;
+                shadow_query(J.V, S, i, cn);
+                st[kStatShadow] += 1;
+            }
         }
     }
     if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
 }
 
-__global__ void __launch_bounds__(128) deposit_batch_kernel(const BatchJob *__restrict__ jobs,
-                                                            const uint32_t *__restrict__ begin, uint32_t n,
-                                                            uint32_t total, const uint32_t *__restrict__ frame) {
+__device__ __forceinline__ void deposit_batch_phase(const BatchJob *__restrict__ jobs,
+                                                    const uint32_t *__restrict__ begin, uint32_t n, uint32_t total,
+                                                    uint32_t fr) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
     for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < total / 32u; w += warps) {
@@ -1516,8 +1620,308 @@ __global__ void __launch_bounds__(128) deposit_batch_kernel(const BatchJob *__re
         if (*J.V.error_flags) continue;
         unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
         uint32_t ray = base - __ldg(begin + j) + lane;
-        if (ray < J.rays) deposit_split_ray(J.V, J.F, *frame, J.nrm, ray, st);
+        if (ray < J.rays) deposit_split_ray(J.V, J.F, fr, J.nrm, ray, st);
         add_stats(J.V.stats, st);
+    }
+}
+
+__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
+    closest_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
+                         uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counter, uint32_t tile) {
+    closest_batch_phase(jobs, begin, n, total, *frame, counter, tile);
+}
+
+__global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__restrict__ jobs,
+                                                          const uint32_t *__restrict__ begin, uint32_t n,
+                                                          uint32_t total, const uint32_t *__restrict__ frame) {
+    shade_batch_phase(jobs, begin, n, total, *frame);
+}
+
+__global__ void __launch_bounds__(128) query_prefix_kernel(const BatchJob *__restrict__ jobs, uint32_t n,
+                                                           uint32_t *__restrict__ qbegin) {
+    if (blockIdx.x == 0) query_prefix_block(jobs, n, qbegin);
+}
+
+__global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
+    shadow_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *qbegin, uint32_t n, uint32_t *counter,
+                        uint32_t tile) {
+    shadow_batch_phase(jobs, qbegin, n, counter, tile);
+}
+
+__global__ void __launch_bounds__(128) deposit_batch_kernel(const BatchJob *__restrict__ jobs,
+                                                            const uint32_t *__restrict__ begin, uint32_t n,
+                                                            uint32_t total, const uint32_t *__restrict__ frame) {
+    deposit_batch_phase(jobs, begin, n, total, *frame);
+}
+
+// ---- the trace stage as one persistent launch --------------------------------
+// A cooperative launch (every block resident) runs the four phases with a
+// grid barrier between them.  Every barrier wait is bounded: a block that
+// waits longer than limit_ns sets the abort word, marks every job's error
+// word LUX_VIEW_ERR_TIMEOUT (the first block to give up does) and returns,
+// and so does every block that sees the abort word; the later passes skip
+// flagged views and the next frame clears the words.  `missing` arrivals
+// that never come are added to every barrier's target (a test's way to make
+// a wait run out).
+struct GridBarrier {
+    uint32_t *arrive;  // arrivals, monotonic over the frame's barriers
+    uint32_t *abort;
+    unsigned long long limit_ns;
+    uint32_t missing;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ uint32_t load_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ bool grid_sync(const GridBarrier &B, uint32_t index, const BatchJob *__restrict__ jobs, uint32_t n) {
+    __shared__ uint32_t passed;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();  // the block's writes before its arrival
+        atomicAdd(B.arrive, 1u);
+        const uint32_t target = index * gridDim.x + B.missing;
+        const unsigned long long t0 = global_ns();
+        uint32_t ok = 1;
+        while (load_acquire(B.arrive) < target) {
+            if (load_acquire(B.abort)) {
+                ok = 0;
+                break;
+            }
+            if (global_ns() - t0 > B.limit_ns) {
+                ok = 0;
+                if (atomicExch(B.abort, 1u) == 0u)
+                    for (uint32_t j = 0; j < n; ++j) atomicOr(jobs[j].V.error_flags, LUX_VIEW_ERR_TIMEOUT);
+                break;
+            }
+            __nanosleep(256);
+        }
+        __threadfence();
+        passed = ok;
+    }
+    __syncthreads();
+    return passed != 0u;
+}
+
+__global__ void __launch_bounds__(128, LUX_FUSED_MIN_BLOCKS)
+    trace_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
+                       uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counters,
+                       uint32_t *qbegin, GridBarrier B, uint32_t tile) {
+    const uint32_t fr = *frame;
+    closest_batch_phase(jobs, begin, n, total, fr, counters, tile);
+    if (!grid_sync(B, 1, jobs, n)) return;
+    shade_batch_phase(jobs, begin, n, total, fr);
+    if (!grid_sync(B, 2, jobs, n)) return;
+    if (blockIdx.x == 0) query_prefix_block(jobs, n, qbegin);
+    if (!grid_sync(B, 3, jobs, n)) return;
+    shadow_batch_phase(jobs, qbegin, n, counters + 1, tile);
+    if (!grid_sync(B, 4, jobs, n)) return;
+    deposit_batch_phase(jobs, begin, n, total, fr);
+}
+
+// ---- batched setup, merge and pack -----------------------------------------
+// Every per-view pass of a frame runs once over all jobs: a job's items
+// (directory slots, receivers x levels, records of a level, ...) form one
+// range of a concatenated domain, padded to a multiple of 32 so each warp
+// chunk lies in one job.  Row r of the domain table (rows x (n + 1) 64-bit
+// exclusive prefixes) is one such domain; the host writes the rows whose
+// sizes it knows, batch_layout_kernel the rows that depend on the seeded
+// cell counts, with the unpadded per-job sizes beside them.
+constexpr uint32_t kRowDir = 0;      // levels x directory slots (clear, assign)
+constexpr uint32_t kRowSeed = 1;     // receivers x levels (insert, lookup)
+constexpr uint32_t kRowRecv = 2;     // receivers (sequence sort, ordinals)
+constexpr uint32_t kRowEntries = 3;  // the frame's records (clear)
+constexpr uint32_t kRowCells = 4;    // + level: cells of the level (corners, pack)
+constexpr uint32_t kRowRecords = kRowCells + LUX_MAX_LEVELS;  // + level: records of the level (merge)
+constexpr uint32_t kBatchRows = kRowRecords + LUX_MAX_LEVELS;
+constexpr uint32_t kDeviceRows = kBatchRows - kRowEntries;    // rows batch_layout_kernel writes
+
+// Largest j < n with begin[j] <= x.
+__device__ __forceinline__ uint32_t find_job64(const unsigned long long *__restrict__ begin, uint32_t n,
+                                               unsigned long long x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (begin[mid] <= x)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// fn(job, item) for every item of a padded domain row, one warp chunk at a
+// time (the caller bounds item by the job's own size).
+template <typename Fn>
+__device__ __forceinline__ void for_batch_items(const unsigned long long *__restrict__ begin, uint32_t n, Fn &&fn) {
+    const unsigned long long total = begin[n];
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned long long warps = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+    for (unsigned long long w = (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5; w * 32ull < total;
+         w += warps) {
+        const unsigned long long base = w * 32ull;
+        const uint32_t j = find_job64(begin, n, base);
+        fn(j, base - begin[j] + lane);
+    }
+}
+
+__device__ __forceinline__ const unsigned long long *batch_row(const unsigned long long *dom, uint32_t n, uint32_t row) {
+    return dom + (size_t)row * (n + 1);
+}
+
+__global__ void batch_clear_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                   uint32_t n) {
+    for_batch_items(batch_row(dom, n, kRowDir), n,
+                    [&](uint32_t j, unsigned long long i) { clear_item(jobs[j].V, jobs[j].F, i); });
+}
+
+__global__ void batch_seed_insert_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                         uint32_t n) {
+    for_batch_items(batch_row(dom, n, kRowSeed), n, [&](uint32_t j, unsigned long long i) {
+        seed_insert_item(jobs[j].V, jobs[j].F, jobs[j].pos, i);
+    });
+}
+
+__global__ void batch_seed_assign_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                         uint32_t n) {
+    for_batch_items(batch_row(dom, n, kRowDir), n,
+                    [&](uint32_t j, unsigned long long i) { seed_assign_item(jobs[j].V, jobs[j].F, i); });
+}
+
+// Sequence keys of all jobs' receivers go to one array (job j's at the
+// receiver row's offset) for the segmented sort.
+__global__ void batch_seed_lookup_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                         uint32_t n, unsigned long long *keys, uint32_t *vals) {
+    const unsigned long long *recv = batch_row(dom, n, kRowRecv);
+    for_batch_items(batch_row(dom, n, kRowSeed), n, [&](uint32_t j, unsigned long long i) {
+        seed_lookup_item(jobs[j].V, jobs[j].F, jobs[j].pos, i, keys + recv[j], vals + recv[j]);
+    });
+}
+
+__global__ void batch_ordinal_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                     uint32_t n, const uint32_t *__restrict__ sorted) {
+    const unsigned long long *recv = batch_row(dom, n, kRowRecv);
+    for_batch_items(recv, n, [&](uint32_t j, unsigned long long i) {
+        if (i < jobs[j].F.receivers) jobs[j].V.receiver_ordinal[sorted[recv[j] + i]] = (uint32_t)i;
+    });
+}
+
+// Every job's record layout, then the device rows: count[r][j] the job's
+// unpadded size in row kRowEntries + r (zero for a job whose error word is
+// set), dom's rows the padded exclusive prefixes.  One block.
+__global__ void __launch_bounds__(1024) batch_layout_kernel(const BatchJob *__restrict__ jobs, uint32_t n,
+                                                            unsigned long long *__restrict__ dom,
+                                                            unsigned long long *__restrict__ count) {
+    for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
+        const ViewDevice &V = jobs[j].V;
+        const FrameParams &F = jobs[j].F;
+        layout_view(V, F);
+        const bool ok = *V.error_flags == 0u;
+        unsigned long long entries = 0;
+        for (uint32_t l = 0; l < LUX_MAX_LEVELS; ++l) {
+            const unsigned long long cells = ok && l < F.levels ? V.cell_count[l] : 0ull;
+            const unsigned long long records = cells * (l < F.levels ? F.dirs[l] : 0u);
+            count[(size_t)(kRowCells - kRowEntries + l) * n + j] = cells;
+            count[(size_t)(kRowRecords - kRowEntries + l) * n + j] = records;
+            entries += records;
+        }
+        count[j] = entries;
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t r = threadIdx.x >> 5; r < kDeviceRows; r += blockDim.x >> 5) {
+        unsigned long long *row = dom + (size_t)(kRowEntries + r) * (n + 1);
+        const unsigned long long *cnt = count + (size_t)r * n;
+        unsigned long long carry = 0;
+        for (uint32_t c = 0; c < n; c += 32u) {
+            const uint32_t j = c + lane;
+            unsigned long long v = j < n ? (cnt[j] + 31ull) & ~31ull : 0ull, incl = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                unsigned long long t = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= (uint32_t)off) incl += t;
+            }
+            if (j < n) row[j] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) row[n] = carry;
+    }
+}
+
+__global__ void batch_clear_entries_kernel(const BatchJob *__restrict__ jobs,
+                                           const unsigned long long *__restrict__ dom, uint32_t n,
+                                           const unsigned long long *__restrict__ count) {
+    for_batch_items(batch_row(dom, n, kRowEntries), n, [&](uint32_t j, unsigned long long i) {
+        if (i < count[j]) clear_entry(jobs[j].V, i);
+    });
+}
+
+// Corners of every level below the coarsest, all jobs, one launch.
+__global__ void batch_corners_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                     uint32_t n, const unsigned long long *__restrict__ count, uint32_t levels) {
+    for (uint32_t l = 0; l + 1 < levels; ++l) {
+        const unsigned long long *cells = count + (size_t)(kRowCells - kRowEntries + l) * n;
+        for_batch_items(batch_row(dom, n, kRowCells + l), n, [&](uint32_t j, unsigned long long c) {
+            const BatchJob &J = jobs[j];
+            if (c < cells[j] && l + 1 < J.F.levels && *J.V.error_flags == 0u) corners_item(J.V, J.F, l, (uint32_t)c);
+        });
+    }
+}
+
+__global__ void __launch_bounds__(256) batch_merge_kernel(const BatchJob *__restrict__ jobs,
+                                                          const unsigned long long *__restrict__ dom, uint32_t n,
+                                                          const unsigned long long *__restrict__ count,
+                                                          uint32_t level) {
+    const unsigned long long *records = count + (size_t)(kRowRecords - kRowEntries + level) * n;
+    const HistoryDevice none{};  // batched frames do not blend history
+    for_batch_items(batch_row(dom, n, kRowRecords + level), n, [&](uint32_t j, unsigned long long e) {
+        const BatchJob &J = jobs[j];
+        if (e >= records[j] || *J.V.error_flags) return;
+        const uint32_t dirs = J.F.dirs[level];
+        uint32_t cell, d;
+        if (e <= 0xffffffffull) {
+            cell = (uint32_t)e / dirs;
+            d = (uint32_t)e - cell * dirs;
+        } else {
+            cell = (uint32_t)(e / dirs);
+            d = (uint32_t)(e % dirs);
+        }
+        merge_record(J.V, J.F, none, level, J.V.level_base[level], dirs, cell, d);
+    });
+}
+
+// One block per cascade-0 cell over all jobs; the shared direction table is
+// rebuilt when the block's job changes (dynamic shared memory: 2 x the
+// largest cascade-0 direction count).
+__global__ void __launch_bounds__(64) batch_pack_kernel(const BatchJob *__restrict__ jobs,
+                                                        const unsigned long long *__restrict__ dom, uint32_t n,
+                                                        const unsigned long long *__restrict__ count,
+                                                        uint32_t max_dirs) {
+    extern __shared__ float4 smem[];
+    float4 *val = smem, *dir = smem + max_dirs;
+    const unsigned long long *begin = batch_row(dom, n, kRowCells);
+    const unsigned long long *cells = count + (size_t)(kRowCells - kRowEntries) * n;
+    const unsigned long long total = begin[n];
+    uint32_t cur = lux::kEmpty;
+    for (unsigned long long x = blockIdx.x; x < total; x += gridDim.x) {
+        const uint32_t j = find_job64(begin, n, x);
+        const unsigned long long c = x - begin[j];
+        const BatchJob &J = jobs[j];
+        if (c >= cells[j] || *J.V.error_flags) continue;
+        if (j != cur) {
+            __syncthreads();  // the previous job's table is no longer read
+            pack_directions(J.F, dir);
+            cur = j;
+        }
+        pack_cell(J.V, J.F, (uint32_t)c, val, dir);
     }
 }
 
@@ -1793,7 +2197,7 @@ constexpr int kTimingEvents = 7;
 
 struct LuxView {
     LuxContext *ctx = nullptr;
-    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0};
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0, 32, 0};
     bool timing = false;
     cudaEvent_t ev[kTimingEvents] = {};
     LuxViewDesc desc{};
@@ -2494,10 +2898,10 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
                     Dr, F, scene->view, pos, nrm, rays);
             else if (T.stack_depth == 32)
                 closest_split_kernel<32><<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
-                    Dr, F, scene->view, pos, nrm, rays);
+                    Dr, F, scene->view, pos, nrm, rays, tile_of(T));
             else
                 closest_split_kernel<64><<<ctx->sm_count * T.closest_blocks_per_sm, 128, 0, st>>>(
-                    Dr, F, scene->view, pos, nrm, rays);
+                    Dr, F, scene->view, pos, nrm, rays, tile_of(T));
             if (forked) cudaStreamWaitEvent(st, v->laid_out, 0);  // join the setup stream
             ViewDevice Dq = D;  // query pass view: keys written by shade, optional order
             if (!T.sort_queries) Dq.sort_keys = nullptr;
@@ -2512,9 +2916,11 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
             if (T.shadow_mode == 1)
                 shadow_refill_kernel<<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
             else if (T.stack_depth == 32)
-                shadow_kernel<32><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
+                shadow_kernel<32><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view,
+                                                                                         tile_of(T));
             else
-                shadow_kernel<64><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view);
+                shadow_kernel<64><<<ctx->sm_count * T.shadow_blocks_per_sm, 128, 0, st>>>(Dq, F, scene->view,
+                                                                                         tile_of(T));
             if (cached) {
                 const int g = ctx->sm_count * 8;
                 cache_queries_kernel<<<g, 256, 0, st>>>(D, nrm, rays, F.rays_per_receiver, C);
@@ -2538,7 +2944,8 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
         for (uint32_t l = 0; l < F.levels; ++l)
             closest_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, l);
         shade_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F, scene->view, F.ray_capacity, true);
-        shadow_kernel<64><<<ctx->sm_count * v->tuning.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view);
+        shadow_kernel<64><<<ctx->sm_count * v->tuning.shadow_blocks_per_sm, 128, 0, st>>>(D, F, scene->view,
+                                                                                      tile_of(v->tuning));
         deposit_dense_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(D, F);
     }
     mark(2);
@@ -2751,11 +3158,14 @@ extern "C" lux_status lux_view_timings(LuxView *v, LuxTimings *out) {
     return LUX_OK;
 }
 
+static bool tile_valid(uint32_t tile) { return tile == 0 || tile == 32 || tile == 64 || tile == 128 || tile == 256; }
+
 extern "C" lux_status lux_view_set_tuning(LuxView *v, const LuxTuning *t) {
     if (!v || !t) return LUX_ERR_INVALID_ARGUMENT;
     if (t->closest_mode > 1 || t->shadow_mode > 1 || t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 ||
         t->shadow_blocks_per_sm < 1 || t->shadow_blocks_per_sm > 64 || t->sort_queries > 1 || t->sort_rays > 1 ||
-        (t->stack_depth != 0 && t->stack_depth != 32 && t->stack_depth != 64))
+        (t->stack_depth != 0 && t->stack_depth != 32 && t->stack_depth != 64) || !tile_valid(t->tile_rays) ||
+        t->fused_trace > 1)
         return lux_fail(v->ctx, LUX_ERR_INVALID_ARGUMENT, "set_tuning: value out of range");
     v->tuning = *t;
     if (t->sort_queries || t->sort_rays) return ensure_sort_buffers(v);
@@ -2842,7 +3252,7 @@ lux_status launch_interval_radiance(LuxContext *ctx, const LuxScene *scene, cons
     if (count) {
         closest_rays_kernel<<<ctx->sm_count * 16, 128, 0, st>>>(V, scene->view, rays, count);
         shade_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, F, scene->view, count, false);
-        shadow_kernel<64><<<ctx->sm_count * 16, 128, 0, st>>>(V, F, scene->view);
+        shadow_kernel<64><<<ctx->sm_count * 16, 128, 0, st>>>(V, F, scene->view, 32u);
         radiance_out_kernel<<<(count + 127) / 128, 128, 0, st>>>(V, count, (float4 *)out);
     }
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "interval_radiance launch");
@@ -2965,7 +3375,7 @@ extern "C" lux_status lux_view_read_hits(LuxView *v, LuxHit *out, uint32_t count
 
 struct LuxBatch {
     LuxContext *ctx = nullptr;
-    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0};
+    LuxTuning tuning{0, 0, 16, 16, 0, 0, 64, 0, 32, 0};
     bool use_graph = true;
     // Configuration the device tables and graph were built for.
     std::vector<LuxBatchJob> jobs;
@@ -2978,6 +3388,21 @@ struct LuxBatch {
     BatchJob *d_jobs = nullptr;
     uint32_t *d_begin = nullptr, *d_qbegin = nullptr, *d_counters = nullptr, *d_frame = nullptr;
     size_t job_capacity = 0;
+    // Domain table (kBatchRows x (n + 1) padded prefixes) and the device
+    // rows' unpadded per-job sizes (kDeviceRows x n).
+    unsigned long long *d_dom = nullptr, *d_count = nullptr;
+    // Sequence-order sort of all jobs' receivers: keys and receiver indices
+    // (in, out halves), per-job segment bounds, scratch.
+    unsigned long long *d_keys = nullptr;
+    uint32_t *d_vals = nullptr;
+    int *d_seg = nullptr;  // [2][n] begin, end
+    void *d_sort_temp = nullptr;
+    size_t sort_temp_bytes = 0, recv_capacity = 0;
+    uint64_t recv_total = 0;  // padded receivers of all jobs
+    uint32_t levels = 0, max_dirs0 = 0;
+    int fused_per_sm = 0;                          // resident trace_batch_kernel blocks per SM
+    unsigned long long wait_limit_ns = 1000000000ull;  // grid-barrier wait bound
+    uint32_t wait_missing = 0;                     // test hook: arrivals that never come
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint32_t captures = 0;
@@ -2992,12 +3417,27 @@ static void batch_release_graph(LuxBatch *b) {
     b->graph = nullptr;
 }
 
+static void batch_release_sort(LuxBatch *b) {
+    cudaFree(b->d_keys);
+    cudaFree(b->d_vals);
+    cudaFree(b->d_sort_temp);
+    b->d_keys = nullptr;
+    b->d_vals = nullptr;
+    b->d_sort_temp = nullptr;
+    b->sort_temp_bytes = b->recv_capacity = 0;
+}
+
 static void batch_release_tables(LuxBatch *b) {
     cudaFree(b->d_jobs);
     cudaFree(b->d_begin);
     cudaFree(b->d_qbegin);
+    cudaFree(b->d_dom);
+    cudaFree(b->d_count);
+    cudaFree(b->d_seg);
     b->d_jobs = nullptr;
     b->d_begin = b->d_qbegin = nullptr;
+    b->d_dom = b->d_count = nullptr;
+    b->d_seg = nullptr;
     b->job_capacity = 0;
 }
 
@@ -3008,6 +3448,10 @@ extern "C" lux_status lux_batch_create(LuxContext *ctx, LuxBatch **out) {
     if (!b) return LUX_ERR_OUT_OF_MEMORY;
     b->ctx = ctx;
     cudaSetDevice(ctx->device);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b->fused_per_sm, trace_batch_kernel, 128, 0) != cudaSuccess) {
+        cudaGetLastError();
+        b->fused_per_sm = 0;
+    }
     if (cudaMalloc((void **)&b->d_counters, 16) != cudaSuccess || cudaMalloc((void **)&b->d_frame, 16) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(b->d_counters);
@@ -3024,6 +3468,7 @@ extern "C" lux_status lux_batch_destroy(LuxBatch *b) {
     cudaStreamSynchronize(b->ctx->stream);
     batch_release_graph(b);
     batch_release_tables(b);
+    batch_release_sort(b);
     cudaFree(b->d_counters);
     cudaFree(b->d_frame);
     delete b;
@@ -3042,8 +3487,34 @@ extern "C" lux_status lux_batch_set_tuning(LuxBatch *b, const LuxTuning *t) {
     if (t->closest_blocks_per_sm < 1 || t->closest_blocks_per_sm > 64 || t->shadow_blocks_per_sm < 1 ||
         t->shadow_blocks_per_sm > 64)
         return lux_fail(b->ctx, LUX_ERR_INVALID_ARGUMENT, "batch tuning: blocks per SM must be 1..64");
+    if (!tile_valid(t->tile_rays) || t->fused_trace > 1)
+        return lux_fail(b->ctx, LUX_ERR_INVALID_ARGUMENT, "batch tuning: tile_rays or fused_trace out of range");
     b->tuning = *t;
     b->built = false;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_set_wait(LuxBatch *b, uint64_t limit_ns, uint32_t missing_arrivals) {
+    if (!b) return LUX_ERR_INVALID_ARGUMENT;
+    if (limit_ns < 1000000ull || limit_ns > 10000000000ull)
+        return lux_fail(b->ctx, LUX_ERR_INVALID_ARGUMENT, "batch wait: limit must be 1 ms .. 10 s");
+    b->wait_limit_ns = limit_ns;
+    b->wait_missing = missing_arrivals;
+    b->built = false;
+    return LUX_OK;
+}
+
+extern "C" lux_status lux_batch_status(LuxBatch *b) {
+    if (!b) return LUX_ERR_INVALID_ARGUMENT;
+    LuxContext *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    lux_status rc = lux_cuda_check(ctx, (int)cudaStreamSynchronize(ctx->stream), "batch status: synchronize");
+    if (rc != LUX_OK) return rc;
+    uint32_t abort = 0;
+    rc = lux_cuda_check(ctx, (int)cudaMemcpy(&abort, b->d_counters + 3, 4, cudaMemcpyDeviceToHost),
+                        "batch status: read");
+    if (rc != LUX_OK) return rc;
+    if (abort) return lux_fail(ctx, LUX_ERR_TIMEOUT, "batch: a trace-stage grid barrier wait ran out");
     return LUX_OK;
 }
 
@@ -3067,31 +3538,69 @@ static bool same_jobs(const std::vector<LuxBatchJob> &a, const LuxBatchJob *b, u
     return true;
 }
 
-// Every kernel of one batched frame, in order, on `st` (captured or direct).
-static uint32_t batch_enqueue(LuxBatch *b, cudaStream_t st) {
+// Every kernel of one batched frame, in order, on `st` (captured or direct):
+// each per-view pass runs once over all jobs.
+static void batch_enqueue(LuxBatch *b, cudaStream_t st) {
     LuxContext *ctx = b->ctx;
     const uint32_t n = (uint32_t)b->jobs.size();
-    uint32_t kernels = 0;
-    for (uint32_t j = 0; j < n; ++j) {
-        enqueue_setup(b->jobs[j].view, b->params[j], (const float4 *)b->jobs[j].receivers.position, st);
-        kernels += b->params[j].receivers ? 6u : 3u;
-    }
-    cudaMemsetAsync(b->d_counters, 0, 8, st);
     const int grid = ctx->sm_count * 8;
-    if (b->total) {
-        closest_batch_kernel<<<ctx->sm_count * b->tuning.closest_blocks_per_sm, 128, 0, st>>>(
-            b->d_jobs, b->d_begin, n, b->total, b->d_frame, b->d_counters);
-        shade_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
-        query_prefix_kernel<<<1, 32, 0, st>>>(b->d_jobs, n, b->d_qbegin);
-        shadow_batch_kernel<<<ctx->sm_count * b->tuning.shadow_blocks_per_sm, 128, 0, st>>>(
-            b->d_jobs, b->d_qbegin, n, b->d_counters + 1);
-        deposit_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
-        kernels += 5;
+    cudaMemsetAsync(b->d_counters, 0, 16, st);  // work counters, barrier arrivals, abort word
+    batch_clear_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n);
+    if (b->recv_total) {
+        const size_t half = b->recv_capacity;
+        batch_seed_insert_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n);
+        batch_seed_assign_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n);
+        batch_seed_lookup_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_keys, b->d_vals);
+        size_t bytes = b->sort_temp_bytes;
+        cub::DeviceSegmentedSort::StableSortPairs(b->d_sort_temp, bytes, b->d_keys, b->d_keys + half, b->d_vals,
+                                                  b->d_vals + half, (int)b->recv_total, (int)n, b->d_seg,
+                                                  b->d_seg + n, st);
+        batch_ordinal_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_vals + half);
     }
-    for (uint32_t j = 0; j < n; ++j) {
-        enqueue_merge(b->jobs[j].view, b->params[j], st);
-        enqueue_pack(b->jobs[j].view, b->params[j], st);
-        kernels += 2u * b->params[j].levels;
+    batch_layout_kernel<<<1, 1024, 0, st>>>(b->d_jobs, n, b->d_dom, b->d_count);
+    batch_clear_entries_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
+    if (b->total && b->tuning.fused_trace) {
+        // One cooperative launch: no more blocks than can be resident.
+        const uint32_t per_sm = std::min(b->tuning.closest_blocks_per_sm, (uint32_t)std::max(b->fused_per_sm, 1));
+        GridBarrier B{b->d_counters + 2, b->d_counters + 3, b->wait_limit_ns, b->wait_missing};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(ctx->sm_count * per_sm);
+        cfg.blockDim = dim3(128);
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeCooperative;
+        attr[0].val.cooperative = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaLaunchKernelEx(&cfg, trace_batch_kernel, (const BatchJob *)b->d_jobs, (const uint32_t *)b->d_begin, n,
+                           b->total, (const uint32_t *)b->d_frame, b->d_counters, b->d_qbegin, B,
+                           tile_of(b->tuning));
+    } else if (b->total) {
+        closest_batch_kernel<<<ctx->sm_count * b->tuning.closest_blocks_per_sm, 128, 0, st>>>(
+            b->d_jobs, b->d_begin, n, b->total, b->d_frame, b->d_counters, tile_of(b->tuning));
+        shade_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
+        query_prefix_kernel<<<1, 128, 0, st>>>(b->d_jobs, n, b->d_qbegin);
+        shadow_batch_kernel<<<ctx->sm_count * b->tuning.shadow_blocks_per_sm, 128, 0, st>>>(
+            b->d_jobs, b->d_qbegin, n, b->d_counters + 1, tile_of(b->tuning));
+        deposit_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
+    }
+    if (b->levels > 1) batch_corners_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, b->levels);
+    for (int l = (int)b->levels - 1; l >= 0; --l)
+        batch_merge_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, (uint32_t)l);
+    batch_pack_kernel<<<grid, 64, (size_t)b->max_dirs0 * 2 * sizeof(float4), st>>>(b->d_jobs, b->d_dom, n,
+                                                                                 b->d_count, b->max_dirs0);
+}
+
+// Kernel nodes of a captured graph (the launches one replay makes).
+static uint32_t graph_kernels(cudaGraph_t g) {
+    size_t count = 0;
+    if (cudaGraphGetNodes(g, nullptr, &count) != cudaSuccess) return 0;
+    std::vector<cudaGraphNode_t> nodes(count);
+    if (cudaGraphGetNodes(g, nodes.data(), &count) != cudaSuccess) return 0;
+    uint32_t kernels = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        if (cudaGraphNodeGetType(node, &type) == cudaSuccess && type == cudaGraphNodeTypeKernel) ++kernels;
     }
     return kernels;
 }
@@ -3108,13 +3617,75 @@ static lux_status batch_build(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n, 
         batch_release_tables(b);
         if (cudaMalloc((void **)&b->d_jobs, n * sizeof(BatchJob)) != cudaSuccess ||
             cudaMalloc((void **)&b->d_begin, (n + 1) * 4) != cudaSuccess ||
-            cudaMalloc((void **)&b->d_qbegin, (n + 1) * 4) != cudaSuccess) {
+            cudaMalloc((void **)&b->d_qbegin, (n + 1) * 4) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_dom, (size_t)kBatchRows * (n + 1) * 8) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_count, (size_t)kDeviceRows * n * 8) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_seg, (size_t)2 * n * sizeof(int)) != cudaSuccess) {
             cudaGetLastError();
             batch_release_tables(b);
             return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
         }
         b->job_capacity = n;
     }
+    // Host-sized domain rows and the receivers' sort segments.
+    std::vector<unsigned long long> rows((size_t)kRowEntries * (n + 1), 0ull);
+    std::vector<int> seg((size_t)2 * n, 0);
+    uint32_t levels = 0, max_dirs0 = 1;
+    for (uint32_t j = 0; j < n; ++j) {
+        const FrameParams &F = params[j];
+        const unsigned long long size[kRowEntries] = {(unsigned long long)F.levels * F.dir_capacity,
+                                                      (unsigned long long)F.receivers * F.levels, F.receivers};
+        for (uint32_t r = 0; r < kRowEntries; ++r)
+            rows[(size_t)r * (n + 1) + j + 1] = rows[(size_t)r * (n + 1) + j] + ((size[r] + 31ull) & ~31ull);
+        seg[j] = (int)rows[(size_t)kRowRecv * (n + 1) + j];
+        seg[n + j] = seg[j] + (int)F.receivers;
+        levels = std::max(levels, F.levels);
+        max_dirs0 = std::max(max_dirs0, F.dirs[0]);
+    }
+    const uint64_t recv_total = rows[(size_t)kRowRecv * (n + 1) + n];
+    if (recv_total > 0x7fffffe0ull) return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: more than 2^31 receivers");
+    if (recv_total > b->recv_capacity) {
+        batch_release_sort(b);
+        size_t temp = 0;
+        cub::DeviceSegmentedSort::StableSortPairs(nullptr, temp, (const unsigned long long *)nullptr,
+                                                  (unsigned long long *)nullptr, (const uint32_t *)nullptr,
+                                                  (uint32_t *)nullptr, (int)recv_total, (int)n, (const int *)nullptr,
+                                                  (const int *)nullptr, st);
+        if (cudaMalloc((void **)&b->d_keys, recv_total * 16) != cudaSuccess ||
+            cudaMalloc((void **)&b->d_vals, recv_total * 8) != cudaSuccess ||
+            cudaMalloc(&b->d_sort_temp, std::max<size_t>(temp, 16)) != cudaSuccess) {
+            cudaGetLastError();
+            batch_release_sort(b);
+            return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
+        }
+        b->recv_capacity = recv_total;
+        b->sort_temp_bytes = std::max<size_t>(temp, 16);
+    } else {
+        size_t temp = 0;
+        cub::DeviceSegmentedSort::StableSortPairs(nullptr, temp, (const unsigned long long *)nullptr,
+                                                  (unsigned long long *)nullptr, (const uint32_t *)nullptr,
+                                                  (uint32_t *)nullptr, (int)recv_total, (int)n, (const int *)nullptr,
+                                                  (const int *)nullptr, st);
+        if (temp > b->sort_temp_bytes) {
+            cudaFree(b->d_sort_temp);
+            b->d_sort_temp = nullptr;
+            if (cudaMalloc(&b->d_sort_temp, temp) != cudaSuccess) {
+                cudaGetLastError();
+                batch_release_sort(b);
+                return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
+            }
+            b->sort_temp_bytes = temp;
+        }
+    }
+    rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_dom, rows.data(), rows.size() * 8, cudaMemcpyHostToDevice),
+                        "batch: domain rows");
+    if (rc == LUX_OK)
+        rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_seg, seg.data(), seg.size() * sizeof(int), cudaMemcpyHostToDevice),
+                            "batch: sort segments");
+    if (rc != LUX_OK) return rc;
+    b->recv_total = recv_total;
+    b->levels = levels;
+    b->max_dirs0 = max_dirs0;
     std::vector<BatchJob> h(n);
     std::vector<uint32_t> begin(n + 1, 0);
     uint64_t padded = 0, rays = 0;
@@ -3152,20 +3723,25 @@ static lux_status batch_build(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n, 
     b->params = params;
     b->total = (uint32_t)padded;
     b->rays = rays;
+    // The frame is captured once either way: the graph's kernel nodes are
+    // the launches a frame makes; without graphs the capture is discarded.
+    rc = lux_cuda_check(ctx, (int)cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "batch: capture");
+    if (rc != LUX_OK) return rc;
+    batch_enqueue(b, st);
+    cudaGraph_t g = nullptr;
+    rc = lux_cuda_check(ctx, (int)cudaStreamEndCapture(st, &g), "batch: end capture");
+    if (rc != LUX_OK) return rc;
+    b->graph = g;
+    b->kernels = graph_kernels(g);
     if (b->use_graph) {
-        rc = lux_cuda_check(ctx, (int)cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "batch: capture");
-        if (rc != LUX_OK) return rc;
-        b->kernels = batch_enqueue(b, st);
-        cudaGraph_t g = nullptr;
-        rc = lux_cuda_check(ctx, (int)cudaStreamEndCapture(st, &g), "batch: end capture");
-        if (rc != LUX_OK) return rc;
-        b->graph = g;
         rc = lux_cuda_check(ctx, (int)cudaGraphInstantiate(&b->exec, g, 0), "batch: instantiate");
         if (rc != LUX_OK) {
             batch_release_graph(b);
             return rc;
         }
         ++b->captures;
+    } else {
+        batch_release_graph(b);
     }
     b->built = true;
     return LUX_OK;
@@ -3221,7 +3797,7 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
         if (rc != LUX_OK) return rc;
         ++b->replays;
     } else {
-        b->kernels = batch_enqueue(b, st);
+        batch_enqueue(b, st);
     }
     for (uint32_t j = 0; j < n; ++j) {
         FrameParams F = b->params[j];

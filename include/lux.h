@@ -173,6 +173,7 @@ typedef struct LuxStats {
 #define LUX_VIEW_ERR_ENTRY_CAPACITY 2u
 #define LUX_VIEW_ERR_PROBE_LOOKUP 4u
 #define LUX_VIEW_ERR_RAY_CAPACITY 8u
+#define LUX_VIEW_ERR_TIMEOUT 16u   /* a batch's grid-barrier wait ran out (lux_batch_status) */
 
 /* Capacities of a view (ViewBuffers, src/render.rs:5077-5160). */
 typedef struct LuxViewDesc {
@@ -374,6 +375,11 @@ typedef struct LuxTuning {
     uint32_t sort_rays;           /* 1: order interval rays by (direction bin, origin cell) before tracing */
     uint32_t stack_depth;         /* traversal stack entries per thread: 32 or 64 (0 = 64); an overflowing
                                      walk continues with the reference's ordered scan, same answers */
+    uint32_t fused_trace;         /* batches only: 1 = the trace stage (closest hits, shading, visibility,
+                                     deposit) as one persistent cooperative launch with bounded grid
+                                     barriers between the phases; 0 = four launches */
+    uint32_t tile_rays;           /* rays (or visibility queries) a warp takes from the work queue per
+                                     fetch: 32, 64, 128 or 256 (0 = 32); the persistent walkers of modes 0 */
     uint32_t reserved;
 } LuxTuning;
 lux_status lux_view_set_tuning(LuxView *view, const LuxTuning *tuning);
@@ -609,13 +615,23 @@ lux_status lux_batch_create(LuxContext *ctx, LuxBatch **out);
 lux_status lux_batch_destroy(LuxBatch *batch);
 /* 1 (default): capture/replay a CUDA graph; 0: direct launches. */
 lux_status lux_batch_set_graph(LuxBatch *batch, uint32_t enable);
-/* closest/shadow blocks per SM of the batched persistent launches (modes and
- * sort flags are ignored). */
+/* closest/shadow blocks per SM of the batched persistent launches and
+ * fused_trace (modes, sort flags and stack depth are ignored); the fused
+ * launch takes min(closest_blocks_per_sm, resident blocks per SM). */
 lux_status lux_batch_set_tuning(LuxBatch *batch, const LuxTuning *tuning);
 /* One frame of every job with shared settings (layout must be Split). */
 lux_status lux_batch_trace_merge(LuxBatch *batch, const LuxBatchJob *jobs, uint32_t job_count,
                                  const LuxSettings *settings);
 lux_status lux_batch_info(const LuxBatch *batch, LuxBatchInfo *out);
+/* Waits for the batch's last frame; LUX_ERR_TIMEOUT when a grid-barrier
+ * wait of its fused trace launch ran out (the jobs' views then carry
+ * LUX_VIEW_ERR_TIMEOUT and their passes after the trace were skipped; the
+ * next frame starts clean). */
+lux_status lux_batch_status(LuxBatch *batch);
+/* Bound of each grid-barrier wait of the fused trace launch (1 ms .. 10 s,
+ * default 1 s).  missing_arrivals > 0 is a test hook: every barrier then
+ * waits for that many blocks that do not exist, so the first wait runs out. */
+lux_status lux_batch_set_wait(LuxBatch *batch, uint64_t limit_ns, uint32_t missing_arrivals);
 
 /* ---- Screen reconstruction after the world resolve --------------------
  * The reference's temporal and denoise passes (shaders/cascades.slang:310-690,

@@ -22,7 +22,8 @@ class FakeView:
 
 def cost(t):
     return (3.0 * (t["closest_mode"] == 1) + 1.0 * (t["shadow_mode"] == 0) + abs(t["closest_blocks_per_sm"] - 8) / 8
-            + 0.5 * (t["stack_depth"] == 64) + 2.0 * (t["sort_queries"] == 0) + 0.25 * (t["sort_rays"] == 1) + 5.0)
+            + 0.5 * (t["stack_depth"] == 64) + 2.0 * (t["sort_queries"] == 0) + 0.25 * (t["sort_rays"] == 1)
+            + 0.125 * (t["tile_rays"] != 64) + 5.0)
 
 
 def test_coordinate_search_finds_the_separable_minimum():
@@ -31,7 +32,7 @@ def test_coordinate_search_finds_the_separable_minimum():
     out = at.autotune(view, lambda: frames.append(1))
     best = out["best"]
     assert best == dict(closest_mode=0, shadow_mode=1, closest_blocks_per_sm=8, shadow_blocks_per_sm=8,
-                        stack_depth=32, sort_rays=0, sort_queries=1)
+                        tile_rays=64, stack_depth=32, sort_rays=0, sort_queries=1)
     assert out["trace_ms"] == cost(best) == 5.0
     assert view.tuning == best
     keys = [tuple(sorted(t.items())) for t, _ in out["trials"]]

@@ -81,14 +81,17 @@ def assert_same(a, b, settings):
             np.testing.assert_allclose(ma, mb, rtol=1e-4, atol=1e-6)
 
 
-@pytest.mark.parametrize("graph,sky", [(True, False), (False, False), (True, True)])
-def test_batch_matches_unbatched(graph, sky):
+@pytest.mark.parametrize("graph,sky,fused,tile", [(True, False, 0, 32), (False, False, 0, 64), (True, True, 0, 32),
+                                                  (True, False, 1, 32), (False, True, 1, 128)])
+def test_batch_matches_unbatched(graph, sky, fused, tile):
     """sky: a constant environment, whose next-event samples share the
-    batched visibility pass with the emissive ones."""
+    batched visibility pass with the emissive ones.  fused: the trace stage
+    as one cooperative launch with grid barriers between its phases."""
     ctx = bp.LuxContext()
     jobs = make_jobs(ctx)
     batch = bp.Batch(ctx)
     batch.set_graph(graph)
+    batch.set_tuning(16, 16, fused, tile)
     env = (1.0, 0.8, 0.6) if sky else (0.0, 0.0, 0.0)
     for frame in (1, 2):
         settings = bp.RadianceCascades(frame_index=frame, environment=env, **SETTINGS).sanitized()
@@ -104,7 +107,51 @@ def test_batch_matches_unbatched(graph, sky):
         assert info.graph_captures == 1 and info.graph_launches == 2
     else:
         assert info.graph_captures == 0
-    assert info.kernels_per_frame > 5
+    batch.status()
+    # Each pass runs once over all six jobs: setup, the sequence sort, the
+    # trace stage (one launch fused, five not), corners, one merge per level
+    # and the pack; the count does not grow with the job count.
+    levels = SETTINGS["levels"]
+    assert 10 + levels <= info.kernels_per_frame <= 2 * levels + (8 if fused else 12)
+
+
+def test_batch_launches_do_not_grow_with_jobs():
+    ctx = bp.LuxContext()
+    jobs = make_jobs(ctx)
+    batch = bp.Batch(ctx)
+    batch.set_tuning(16, 16, 1)
+    settings = bp.RadianceCascades(frame_index=1, **SETTINGS).sanitized()
+    batch.trace_merge(batch_args(jobs[:2]), settings)
+    two = batch.info().kernels_per_frame
+    batch.trace_merge(batch_args(jobs), settings)
+    assert batch.info().kernels_per_frame == two
+
+
+def test_fused_trace_wait_runs_out_and_recovers():
+    """A grid-barrier wait that cannot complete (one arrival short) gives up
+    after its limit: lux_batch_status reports LUX_ERR_TIMEOUT, every job's
+    view carries LUX_VIEW_ERR_TIMEOUT, and the next frame (wait restored)
+    equals an unbatched frame."""
+    ctx = bp.LuxContext()
+    jobs = make_jobs(ctx)[:3]
+    batch = bp.Batch(ctx)
+    batch.set_tuning(16, 16, 1)
+    batch.set_wait(50_000_000, missing_arrivals=1)
+    settings = bp.RadianceCascades(frame_index=1, **SETTINGS).sanitized()
+    batch.trace_merge(batch_args(jobs), settings)
+    with pytest.raises(bp.LuxError) as err:
+        batch.status()
+    assert err.value.status == 7  # LUX_ERR_TIMEOUT
+    for j in jobs:
+        assert j["view"].stats().error_flags & 16
+    batch.set_wait(1_000_000_000, 0)
+    settings = bp.RadianceCascades(frame_index=2, **SETTINGS).sanitized()
+    batch.trace_merge(batch_args(jobs), settings)
+    batch.status()
+    got = [snapshot(j, settings) for j in jobs]
+    for j, g in zip(jobs, got):
+        j["view"].trace_merge(j["scene"], settings, j["pos"].data_ptr(), j["nrm"].data_ptr(), j["n"])
+        assert_same(g, snapshot(j, settings), settings)
 
 
 def test_batch_recaptures_on_new_configuration():
