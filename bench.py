@@ -760,7 +760,7 @@ def run_ours(args, rank, world):
             **extras,
             "gpu_launches": args.steps * launches_per_frame(settings.levels, bool(tuned["best"].get("sort_queries")),
                                                             bool(tuned["best"].get("sort_rays"))),
-            "autotune": {"best": tuned["best"], "trace_ms": tuned["trace_ms"],
+            "autotune": {"best": tuned["best"], "frame_ms": tuned["frame_ms"],
                          "trials": [[t, round(ms, 3)] for t, ms in tuned["trials"]]},
             "clocks": clocks.summary(),
             "setup_s": w["setup_s"],

@@ -48,6 +48,14 @@
 #ifndef LUX_BATCH_MIN_BLOCKS
 #define LUX_BATCH_MIN_BLOCKS 6
 #endif
+// Merge launch shape: threads per block and the resident blocks the
+// register budget is sized for.
+#ifndef LUX_MERGE_THREADS
+#define LUX_MERGE_THREADS 256
+#endif
+#ifndef LUX_MERGE_MIN_BLOCKS
+#define LUX_MERGE_MIN_BLOCKS 1
+#endif
 // The fused batch trace kernel carries the shading phase's registers too.
 #ifndef LUX_FUSED_MIN_BLOCKS
 #define LUX_FUSED_MIN_BLOCKS 4
@@ -989,29 +997,33 @@ __device__ __forceinline__ float pow_count(float base, uint32_t n) {
 // cell instead of one per record.
 __device__ __forceinline__ bool record_dirty(const FrameParams &F, uint32_t level, int4 key);
 
+__device__ __forceinline__ void history_map_item(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                                 uint32_t level, uint32_t c) {
+    uint32_t id = lux::kEmpty;
+    int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+    if (lux::cell_in_range(key.x, key.y, key.z) && !record_dirty(F, level, key)) {
+        const uint32_t lod = lux::key_lod(key.w);
+        unsigned long long packed = lux::pack_cell(key.x, key.y, key.z, lod);
+        const unsigned long long *keys = H.dir_keys + (size_t)level * F.dir_capacity;
+        uint32_t slot = lux::hash_key(key.x, key.y, key.z, (int32_t)(level | (lod << 18)), F.dir_capacity);
+        for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
+            unsigned long long k = keys[slot];
+            if (k == packed) {
+                uint32_t prev = H.dir_ids[(size_t)level * F.dir_capacity + slot];
+                if (prev != lux::kEmpty && prev < H.cell_count[level]) id = prev;
+                break;
+            }
+            if (k == lux::kEmptyCell) break;
+            slot = (slot + 1u) & (F.dir_capacity - 1u);
+        }
+    }
+    V.hist_cell[(size_t)level * F.cell_capacity + c] = id;
+}
+
 __global__ void history_map_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
     uint32_t cells = min(V.cell_count[level], F.cell_capacity);
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
-        uint32_t id = lux::kEmpty;
-        int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
-        if (lux::cell_in_range(key.x, key.y, key.z) && !record_dirty(F, level, key)) {
-            const uint32_t lod = lux::key_lod(key.w);
-            unsigned long long packed = lux::pack_cell(key.x, key.y, key.z, lod);
-            const unsigned long long *keys = H.dir_keys + (size_t)level * F.dir_capacity;
-            uint32_t slot = lux::hash_key(key.x, key.y, key.z, (int32_t)(level | (lod << 18)), F.dir_capacity);
-            for (uint32_t attempt = 0; attempt < F.dir_capacity; ++attempt) {
-                unsigned long long k = keys[slot];
-                if (k == packed) {
-                    uint32_t prev = H.dir_ids[(size_t)level * F.dir_capacity + slot];
-                    if (prev != lux::kEmpty && prev < H.cell_count[level]) id = prev;
-                    break;
-                }
-                if (k == lux::kEmptyCell) break;
-                slot = (slot + 1u) & (F.dir_capacity - 1u);
-            }
-        }
-        V.hist_cell[(size_t)level * F.cell_capacity + c] = id;
-    }
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x)
+        history_map_item(V, F, H, level, c);
 }
 
 // A record's history is invalid when the region its rays may have crossed
@@ -1069,7 +1081,7 @@ __global__ void retain_count_kernel(ViewDevice V, FrameParams F, HistoryDevice H
 
 // One block of kRetainBins threads: per level, an inclusive scan of the age
 // histogram; the limit is the number of classes whose running total fits.
-__global__ void __launch_bounds__(kRetainBins) retain_limit_kernel(ViewDevice V, FrameParams F) {
+__device__ __forceinline__ void retain_limit_block(const ViewDevice &V, const FrameParams &F) {
     __shared__ unsigned long long scan[kRetainBins];
     __shared__ unsigned long long remaining;
     const uint32_t t = threadIdx.x;
@@ -1099,9 +1111,13 @@ __global__ void __launch_bounds__(kRetainBins) retain_limit_kernel(ViewDevice V,
     }
 }
 
+__global__ void __launch_bounds__(kRetainBins) retain_limit_kernel(ViewDevice V, FrameParams F) {
+    retain_limit_block(V, F);
+}
+
 // Inserts the retained cell `prev` of `level` into this frame's directory
 // with a new dense id and its last-receiver frame.
-__device__ __forceinline__ void retain_cell(ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+__device__ __forceinline__ void retain_cell(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
                                             uint32_t level, uint32_t prev, int4 k) {
     const uint32_t lod = lux::key_lod(k.w);
     unsigned long long key = lux::pack_cell(k.x, k.y, k.z, lod);
@@ -1254,7 +1270,8 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
     V.mass[base + e] = make_float2(rmass, tmass);
 }
 
-__global__ void __launch_bounds__(256) merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
+__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
+    merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
     if (*V.error_flags) return;
     const uint32_t dirs = F.dirs[level];
     const unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
@@ -1451,6 +1468,7 @@ struct BatchJob {
     ViewDevice V;
     FrameParams F;
     SceneView S;
+    HistoryDevice H;  // the view's previous frame (F.history)
     const float4 *pos, *nrm;
     uint32_t rays;
     uint32_t pad;
@@ -1777,10 +1795,18 @@ __device__ __forceinline__ const unsigned long long *batch_row(const unsigned lo
     return dom + (size_t)row * (n + 1);
 }
 
+// The directory clear, and the retain age histograms of the jobs that
+// blend history.
 __global__ void batch_clear_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
                                    uint32_t n) {
     for_batch_items(batch_row(dom, n, kRowDir), n,
                     [&](uint32_t j, unsigned long long i) { clear_item(jobs[j].V, jobs[j].F, i); });
+    const size_t bins = (size_t)LUX_MAX_LEVELS * kRetainBins;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)n * bins;
+         i += (size_t)gridDim.x * blockDim.x) {
+        const BatchJob &J = jobs[i / bins];
+        if (J.F.history) J.V.retain_hist[i % bins] = 0u;
+    }
 }
 
 __global__ void batch_seed_insert_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
@@ -1812,6 +1838,43 @@ __global__ void batch_ordinal_kernel(const BatchJob *__restrict__ jobs, const un
     for_batch_items(recv, n, [&](uint32_t j, unsigned long long i) {
         if (i < jobs[j].F.receivers) jobs[j].V.receiver_ordinal[sorted[recv[j] + i]] = (uint32_t)i;
     });
+}
+
+// retain over all jobs that blend history: the previous frame's cells of job
+// blockIdx.y (+ k gridDim.y), each level, strided over blockIdx.x.
+__global__ void batch_retain_count_kernel(const BatchJob *__restrict__ jobs, uint32_t n) {
+    for (uint32_t j = blockIdx.y; j < n; j += gridDim.y) {
+        const BatchJob &J = jobs[j];
+        if (!J.F.history) continue;
+        for (uint32_t l = 0; l < J.F.levels; ++l) {
+            const uint32_t cells = min(J.H.cell_count[l], J.F.cell_capacity);
+            for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+                int4 key;
+                uint32_t bin = retain_bin(J.V, J.F, J.H, l, c, key);
+                if (bin < kRetainBins) atomicAdd(&J.V.retain_hist[l * kRetainBins + bin], 1u);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kRetainBins) batch_retain_limit_kernel(const BatchJob *__restrict__ jobs,
+                                                                         uint32_t n) {
+    for (uint32_t j = blockIdx.x; j < n; j += gridDim.x)
+        if (jobs[j].F.history) retain_limit_block(jobs[j].V, jobs[j].F);
+}
+
+__global__ void batch_retain_insert_kernel(const BatchJob *__restrict__ jobs, uint32_t n) {
+    for (uint32_t j = blockIdx.y; j < n; j += gridDim.y) {
+        const BatchJob &J = jobs[j];
+        if (!J.F.history) continue;
+        for (uint32_t l = 0; l < J.F.levels; ++l) {
+            const uint32_t cells = min(J.H.cell_count[l], J.F.cell_capacity);
+            for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+                int4 key;
+                if (retain_bin(J.V, J.F, J.H, l, c, key) < J.V.retain_limit[l]) retain_cell(J.V, J.F, J.H, l, c, key);
+            }
+        }
+    }
 }
 
 // Every job's record layout, then the device rows: count[r][j] the job's
@@ -1864,24 +1927,26 @@ __global__ void batch_clear_entries_kernel(const BatchJob *__restrict__ jobs,
     });
 }
 
-// Corners of every level below the coarsest, all jobs, one launch.
-__global__ void batch_corners_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
-                                     uint32_t n, const unsigned long long *__restrict__ count, uint32_t levels) {
-    for (uint32_t l = 0; l + 1 < levels; ++l) {
+// Before the merge, one launch for all levels and jobs: each cell's corners
+// in the next level, and with history its previous frame's id.
+__global__ void batch_merge_prep_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                        uint32_t n, const unsigned long long *__restrict__ count, uint32_t levels) {
+    for (uint32_t l = 0; l < levels; ++l) {
         const unsigned long long *cells = count + (size_t)(kRowCells - kRowEntries + l) * n;
         for_batch_items(batch_row(dom, n, kRowCells + l), n, [&](uint32_t j, unsigned long long c) {
             const BatchJob &J = jobs[j];
-            if (c < cells[j] && l + 1 < J.F.levels && *J.V.error_flags == 0u) corners_item(J.V, J.F, l, (uint32_t)c);
+            if (c >= cells[j] || *J.V.error_flags) return;
+            if (l + 1 < J.F.levels) corners_item(J.V, J.F, l, (uint32_t)c);
+            if (J.F.history) history_map_item(J.V, J.F, J.H, l, (uint32_t)c);
         });
     }
 }
 
-__global__ void __launch_bounds__(256) batch_merge_kernel(const BatchJob *__restrict__ jobs,
+__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS) batch_merge_kernel(const BatchJob *__restrict__ jobs,
                                                           const unsigned long long *__restrict__ dom, uint32_t n,
                                                           const unsigned long long *__restrict__ count,
                                                           uint32_t level) {
     const unsigned long long *records = count + (size_t)(kRowRecords - kRowEntries + level) * n;
-    const HistoryDevice none{};  // batched frames do not blend history
     for_batch_items(batch_row(dom, n, kRowRecords + level), n, [&](uint32_t j, unsigned long long e) {
         const BatchJob &J = jobs[j];
         if (e >= records[j] || *J.V.error_flags) return;
@@ -1894,7 +1959,7 @@ __global__ void __launch_bounds__(256) batch_merge_kernel(const BatchJob *__rest
             cell = (uint32_t)(e / dirs);
             d = (uint32_t)(e % dirs);
         }
-        merge_record(J.V, J.F, none, level, J.V.level_base[level], dirs, cell, d);
+        merge_record(J.V, J.F, J.H, level, J.V.level_base[level], dirs, cell, d);
     });
 }
 
@@ -2605,7 +2670,8 @@ static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
     if (F.history)
         for (uint32_t l = 0; l < F.levels; ++l) history_map_kernel<<<grid, 128, 0, st>>>(D, F, H, l);
-    for (int l = (int)F.levels - 1; l >= 0; --l) merge_kernel<<<grid * 2, 256, 0, st>>>(D, F, H, (uint32_t)l);
+    for (int l = (int)F.levels - 1; l >= 0; --l)
+        merge_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F, H, (uint32_t)l);
 }
 
 // Start of an unbatched frame: the last frame's records become the history
@@ -3379,8 +3445,8 @@ struct LuxBatch {
     bool use_graph = true;
     // Configuration the device tables and graph were built for.
     std::vector<LuxBatchJob> jobs;
-    std::vector<uint64_t> generations;  // each view's buffer generation the job table holds
     LuxSettings settings{};  // frame_index zeroed
+    bool history = false;    // the settings blend history: retain and history mapping run
     std::vector<FrameParams> params;
     uint32_t total = 0;      // padded interval rays
     uint64_t rays = 0;
@@ -3400,6 +3466,14 @@ struct LuxBatch {
     size_t sort_temp_bytes = 0, recv_capacity = 0;
     uint64_t recv_total = 0;  // padded receivers of all jobs
     uint32_t levels = 0, max_dirs0 = 0;
+    // The job table and frame index of each frame go through two pinned
+    // host slots (the table holds the views' current buffers, swapped by
+    // history, and the frame's parameters); staged[k] marks the copy that
+    // last read slot k.
+    void *h_stage[2] = {nullptr, nullptr};
+    size_t stage_bytes = 0;
+    cudaEvent_t staged[2] = {nullptr, nullptr};
+    uint32_t stage_slot = 0;
     int fused_per_sm = 0;                          // resident trace_batch_kernel blocks per SM
     unsigned long long wait_limit_ns = 1000000000ull;  // grid-barrier wait bound
     uint32_t wait_missing = 0;                     // test hook: arrivals that never come
@@ -3452,9 +3526,13 @@ extern "C" lux_status lux_batch_create(LuxContext *ctx, LuxBatch **out) {
         cudaGetLastError();
         b->fused_per_sm = 0;
     }
-    if (cudaMalloc((void **)&b->d_counters, 16) != cudaSuccess || cudaMalloc((void **)&b->d_frame, 16) != cudaSuccess) {
+    if (cudaEventCreateWithFlags(&b->staged[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->staged[1], cudaEventDisableTiming) != cudaSuccess ||
+        cudaMalloc((void **)&b->d_counters, 16) != cudaSuccess || cudaMalloc((void **)&b->d_frame, 16) != cudaSuccess) {
         cudaGetLastError();
         cudaFree(b->d_counters);
+        for (int k = 0; k < 2; ++k)
+            if (b->staged[k]) cudaEventDestroy(b->staged[k]);
         delete b;
         return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: device allocation failed");
     }
@@ -3469,6 +3547,10 @@ extern "C" lux_status lux_batch_destroy(LuxBatch *b) {
     batch_release_graph(b);
     batch_release_tables(b);
     batch_release_sort(b);
+    for (int k = 0; k < 2; ++k) {
+        cudaFreeHost(b->h_stage[k]);
+        if (b->staged[k]) cudaEventDestroy(b->staged[k]);
+    }
     cudaFree(b->d_counters);
     cudaFree(b->d_frame);
     delete b;
@@ -3557,6 +3639,12 @@ static void batch_enqueue(LuxBatch *b, cudaStream_t st) {
                                                   b->d_seg + n, st);
         batch_ordinal_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_vals + half);
     }
+    if (b->history) {  // retain: the previous frame's unseen cells stay
+        const dim3 g2(std::max(1, grid / (int)std::min(n, 64u)), std::min(n, 65535u));
+        batch_retain_count_kernel<<<g2, 256, 0, st>>>(b->d_jobs, n);
+        batch_retain_limit_kernel<<<std::min(n, 65535u), kRetainBins, 0, st>>>(b->d_jobs, n);
+        batch_retain_insert_kernel<<<g2, 256, 0, st>>>(b->d_jobs, n);
+    }
     batch_layout_kernel<<<1, 1024, 0, st>>>(b->d_jobs, n, b->d_dom, b->d_count);
     batch_clear_entries_kernel<<<grid, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
     if (b->total && b->tuning.fused_trace) {
@@ -3584,9 +3672,11 @@ static void batch_enqueue(LuxBatch *b, cudaStream_t st) {
             b->d_jobs, b->d_qbegin, n, b->d_counters + 1, tile_of(b->tuning));
         deposit_batch_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_begin, n, b->total, b->d_frame);
     }
-    if (b->levels > 1) batch_corners_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, b->levels);
+    if (b->levels > 1 || b->history)
+        batch_merge_prep_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, b->levels);
     for (int l = (int)b->levels - 1; l >= 0; --l)
-        batch_merge_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, (uint32_t)l);
+        batch_merge_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(b->d_jobs, b->d_dom, n,
+                                                                                     b->d_count, (uint32_t)l);
     batch_pack_kernel<<<grid, 64, (size_t)b->max_dirs0 * 2 * sizeof(float4), st>>>(b->d_jobs, b->d_dom, n,
                                                                                  b->d_count, b->max_dirs0);
 }
@@ -3686,40 +3776,38 @@ static lux_status batch_build(LuxBatch *b, const LuxBatchJob *jobs, uint32_t n, 
     b->recv_total = recv_total;
     b->levels = levels;
     b->max_dirs0 = max_dirs0;
-    std::vector<BatchJob> h(n);
     std::vector<uint32_t> begin(n + 1, 0);
     uint64_t padded = 0, rays = 0;
     for (uint32_t j = 0; j < n; ++j) {
         const FrameParams &F = params[j];
         uint32_t r = F.receivers * F.rays_per_receiver;
-        BatchJob &J = h[j];
-        std::memset(&J, 0, sizeof J);
-        J.V = jobs[j].view->dev;
-        J.V.sort_keys = nullptr;
-        J.V.ray_order = nullptr;
-        J.V.query_order = nullptr;
-        J.F = F;
-        J.S = jobs[j].scene->view;
-        J.pos = (const float4 *)jobs[j].receivers.position;
-        J.nrm = (const float4 *)jobs[j].receivers.normal;
-        J.rays = r;
         begin[j] = (uint32_t)padded;
         padded += (r + 31u) & ~31u;
         rays += r;
     }
     if (padded > 0xffffffe0ull) return lux_fail(ctx, LUX_ERR_CAPACITY, "batch: more than 2^32 interval rays");
     begin[n] = (uint32_t)padded;
-    rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_jobs, h.data(), n * sizeof(BatchJob), cudaMemcpyHostToDevice),
-                        "batch: job table");
-    if (rc == LUX_OK)
-        rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_begin, begin.data(), (n + 1) * 4, cudaMemcpyHostToDevice),
-                            "batch: ray offsets");
+    rc = lux_cuda_check(ctx, (int)cudaMemcpy(b->d_begin, begin.data(), (n + 1) * 4, cudaMemcpyHostToDevice),
+                        "batch: ray offsets");
     if (rc != LUX_OK) return rc;
+    const size_t stage = n * sizeof(BatchJob) + 16;
+    if (stage > b->stage_bytes) {  // the stream is idle: no copy reads the old slots
+        for (int k = 0; k < 2; ++k) {
+            cudaFreeHost(b->h_stage[k]);
+            b->h_stage[k] = nullptr;
+        }
+        b->stage_bytes = 0;
+        if (cudaHostAlloc(&b->h_stage[0], stage, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&b->h_stage[1], stage, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return lux_fail(ctx, LUX_ERR_OUT_OF_MEMORY, "batch: pinned host allocation failed");
+        }
+        b->stage_bytes = stage;
+    }
     b->jobs.assign(jobs, jobs + n);
-    b->generations.resize(n);
-    for (uint32_t j = 0; j < n; ++j) b->generations[j] = jobs[j].view->generation;
     b->settings = s;
     b->settings.frame_index = 0;
+    b->history = s.history_frames > 0 && (s.temporal_blend > 0.0f || s.transmittance_blend > 0.0f);
     b->params = params;
     b->total = (uint32_t)padded;
     b->rays = rays;
@@ -3779,18 +3867,48 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
     cudaSetDevice(ctx->device);
     LuxSettings key = s;
     key.frame_index = 0;
+    // The graph depends on the jobs' sizes and the settings, not on the
+    // views' buffers (the job table is copied every frame).
     bool same = b->built && same_jobs(b->jobs, jobs, n) && std::memcmp(&key, &b->settings, sizeof key) == 0;
-    for (uint32_t j = 0; same && j < n; ++j) same = b->generations[j] == jobs[j].view->generation;
     if (!same) {
         lux_status rc = batch_build(b, jobs, n, s, params);
         if (rc != LUX_OK) return rc;
     }
     cudaStream_t st = ctx->stream;
-    // Pageable source: the copy is staged before the call returns, so the
-    // local may go out of scope; it orders before the frame's kernels.
-    uint32_t frame = s.frame_index;
-    lux_status rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(b->d_frame, &frame, 4, cudaMemcpyHostToDevice, st),
-                                   "batch: frame index");
+    // This frame's job table: each view's history turns over (buffer swap,
+    // invalidation boxes) as in an unbatched frame.
+    const uint32_t k = b->stage_slot;
+    b->stage_slot ^= 1u;
+    lux_status rc = lux_cuda_check(ctx, (int)cudaEventSynchronize(b->staged[k]), "batch: stage slot");
+    if (rc != LUX_OK) return rc;
+    BatchJob *h = static_cast<BatchJob *>(b->h_stage[k]);
+    uint32_t *h_frame = reinterpret_cast<uint32_t *>(h + n);
+    std::vector<FrameParams> frame_params(n);
+    for (uint32_t j = 0; j < n; ++j) {
+        FrameParams &F = frame_params[j];
+        F = b->params[j];
+        F.shade.frame = s.frame_index;
+        begin_history(jobs[j].view, F, s);
+        BatchJob &J = h[j];
+        std::memset(&J, 0, sizeof J);
+        J.V = jobs[j].view->dev;
+        J.V.sort_keys = nullptr;
+        J.V.ray_order = nullptr;
+        J.V.query_order = nullptr;
+        J.F = F;
+        J.S = jobs[j].scene->view;
+        J.H = history_device(jobs[j].view);
+        J.pos = (const float4 *)jobs[j].receivers.position;
+        J.nrm = (const float4 *)jobs[j].receivers.normal;
+        J.rays = F.receivers * F.rays_per_receiver;
+    }
+    *h_frame = s.frame_index;
+    rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(b->d_jobs, h, n * sizeof(BatchJob), cudaMemcpyHostToDevice, st),
+                        "batch: job table");
+    if (rc == LUX_OK)
+        rc = lux_cuda_check(ctx, (int)cudaMemcpyAsync(b->d_frame, h_frame, 4, cudaMemcpyHostToDevice, st),
+                            "batch: frame index");
+    if (rc == LUX_OK) rc = lux_cuda_check(ctx, (int)cudaEventRecord(b->staged[k], st), "batch: stage event");
     if (rc != LUX_OK) return rc;
     if (b->use_graph) {
         rc = lux_cuda_check(ctx, (int)cudaGraphLaunch(b->exec, st), "batch: graph launch");
@@ -3800,11 +3918,9 @@ extern "C" lux_status lux_batch_trace_merge(LuxBatch *b, const LuxBatchJob *jobs
         batch_enqueue(b, st);
     }
     for (uint32_t j = 0; j < n; ++j) {
-        FrameParams F = b->params[j];
-        F.shade.frame = s.frame_index;
-        jobs[j].view->last = F;
+        jobs[j].view->last = frame_params[j];
         jobs[j].view->has_frame = true;
-        end_history(jobs[j].view, F);
+        end_history(jobs[j].view, frame_params[j]);
     }
     return lux_cuda_check(ctx, (int)cudaGetLastError(), "batch launch");
 }

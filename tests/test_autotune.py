@@ -17,7 +17,7 @@ class FakeView:
         self.tuning = t
 
     def timings(self):
-        return SimpleNamespace(trace_ms=self.cost(self.tuning))
+        return SimpleNamespace(seed_ms=0.0, trace_ms=self.cost(self.tuning), merge_ms=0.0, pack_ms=0.0)
 
 
 def cost(t):
@@ -33,7 +33,7 @@ def test_coordinate_search_finds_the_separable_minimum():
     best = out["best"]
     assert best == dict(closest_mode=0, shadow_mode=1, closest_blocks_per_sm=8, shadow_blocks_per_sm=8,
                         tile_rays=64, stack_depth=32, sort_rays=0, sort_queries=1)
-    assert out["trace_ms"] == cost(best) == 5.0
+    assert out["frame_ms"] == cost(best) == 5.0
     assert view.tuning == best
     keys = [tuple(sorted(t.items())) for t, _ in out["trials"]]
     assert len(keys) == len(set(keys)) < len(list(at.candidates()))

@@ -154,6 +154,30 @@ def test_fused_trace_wait_runs_out_and_recovers():
         assert_same(g, snapshot(j, settings), settings)
 
 
+@pytest.mark.parametrize("fused", [0, 1])
+def test_batch_with_history_matches_unbatched(fused):
+    """History on: each frame's records blend the view's previous frame
+    (retain, history mapping, mass-weighted merge) in the batched passes as
+    in unbatched frames of twin views, also across an invalidation box, and
+    the graph is captured once."""
+    ctx = bp.LuxContext()
+    batched, single = make_jobs(ctx), make_jobs(ctx)
+    batch = bp.Batch(ctx)
+    batch.set_tuning(16, 16, fused)
+    base = dict(SETTINGS, history_frames=24)
+    for frame in (1, 2, 3, 4):
+        if frame == 3:
+            for j in batched + single:
+                j["view"].invalidate_bounds((-1.0, -0.5, -1.0), (0.5, 1.0, 0.5))
+        settings = bp.RadianceCascades(frame_index=frame, **base).sanitized()
+        batch.trace_merge(batch_args(batched), settings)
+        for j in single:
+            j["view"].trace_merge(j["scene"], settings, j["pos"].data_ptr(), j["nrm"].data_ptr(), j["n"])
+        for a, b in zip(batched, single):
+            assert_same(snapshot(a, settings), snapshot(b, settings), settings)
+    assert batch.info().graph_captures == 1
+
+
 def test_batch_recaptures_on_new_configuration():
     ctx = bp.LuxContext()
     jobs = make_jobs(ctx)

@@ -66,15 +66,19 @@ def test_two_vertex_paths_agree_with_the_one_bounce_estimator():
     pk = packed("cornell")
     settings = bp.RadianceCascades(emissive_samples=16).sanitized()
     pos, nrm = points("cornell", 32, 9)
-    path = gpu_path(pk, settings, pos, nrm, 16384, 2, 3)
+    path = gpu_path(pk, settings, pos, nrm, 65536, 2, 3)
     ctx = bp.LuxContext()
     scene = bp.GpuScene(ctx, pk)
     d_p, d_n, d_o = to_device(pos), to_device(nrm), empty_device(len(pos) * 32)
-    bp.reference_irradiance(ctx, scene, settings, d_p.data_ptr(), d_n.data_ptr(), len(pos), 65536, 3,
+    bp.reference_irradiance(ctx, scene, settings, d_p.data_ptr(), d_n.data_ptr(), len(pos), 262144, 3,
                             d_o.data_ptr())
     one = from_device(d_o, np.float64, (len(pos), 4))
     lit = one[:, :3].sum(1) > 1e-3  # points inside a box see no light at all
     assert lit.sum() >= 24
     np.testing.assert_array_equal(path[~lit, :3].sum(1) < 1e-3, True)
-    rel = np.abs(path[lit, :3].sum(1) - one[lit, :3].sum(1)) / one[lit, :3].sum(1)
-    assert np.median(rel) < 0.02 and rel.max() < 0.08, rel
+    # Both are Monte Carlo estimates (the cosine-ray one sees the small
+    # emitter only by chance, a few per cent of noise per point): the mean
+    # signed difference bounds a bias, the per-point bounds the noise.
+    rel = (path[lit, :3].sum(1) - one[lit, :3].sum(1)) / one[lit, :3].sum(1)
+    assert abs(rel.mean()) < 0.01, rel
+    assert np.median(np.abs(rel)) < 0.03 and np.abs(rel).max() < 0.15, rel
