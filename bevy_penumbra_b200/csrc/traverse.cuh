@@ -69,6 +69,10 @@ __device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, flo
 // infinite near or -inf far (miss), and a plane through the origin gives
 // NaN, which fmaxf/fminf ignore -- the reference's inside test for a zero
 // component.
+#ifndef LUX_NODE_EMPTY_CHECK
+#define LUX_NODE_EMPTY_CHECK 1
+#endif
+
 struct SlabRay {
     float ox, oy, oz;
     float ix, iy, iz;     // 1 / d, correctly rounded (+-inf on zero axes)
@@ -116,7 +120,13 @@ __device__ __forceinline__ uint32_t node_test(const Bvh4Node *__restrict__ nodes
         float far_t = fminf(fminf(bx, by), bz);
         near_t = near_t - fabsf(near_t) * 7.2e-7f;
         far_t = far_t + fabsf(far_t) * 7.2e-7f;
+#if LUX_NODE_EMPTY_CHECK
         bool h = child[i] != kEmpty && near_t <= far_t && near_t <= limit && far_t >= tmin;
+#else
+        // An empty slot's box is inverted infinities: its near and far come
+        // out NaN after the padding, and every comparison with NaN fails.
+        bool h = near_t <= far_t && near_t <= limit && far_t >= tmin;
+#endif
         entry[i] = h ? near_t : 0.0f;
         mask |= h ? (1u << i) : 0u;
     }

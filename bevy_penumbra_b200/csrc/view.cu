@@ -54,7 +54,10 @@
 #define LUX_MERGE_THREADS 256
 #endif
 #ifndef LUX_MERGE_MIN_BLOCKS
-#define LUX_MERGE_MIN_BLOCKS 1
+#define LUX_MERGE_MIN_BLOCKS 4
+#endif
+#ifndef LUX_MERGE_CORNER_OUTER
+#define LUX_MERGE_CORNER_OUTER 1
 #endif
 // The fused batch trace kernel carries the shading phase's registers too.
 #ifndef LUX_FUSED_MIN_BLOCKS
@@ -157,6 +160,7 @@ static inline uint32_t tile_of(const LuxTuning &t) { return t.tile_rays ? t.tile
 
 constexpr uint32_t kSortCells = 4096;           // 16^3 origin cells over the TLAS root box
 constexpr uint32_t kQueryCells = 2097152;       // 128^3 origin cells of visibility queries
+constexpr uint32_t kRaySortBins = 32 * kSortCells;  // 32 direction bins x 16^3 origin cells of interval rays
 constexpr uint32_t kSortBins = 8 * kQueryCells; // 8 emitter buckets x 128^3 origin cells of queries,
                                                 // or 32 direction bins x 16^3 cells of interval rays
 
@@ -657,10 +661,11 @@ __global__ void sort_scatter_kernel(ViewDevice V, const uint32_t *count_ptr, uin
         V.sort_perm[atomicAdd(&V.sort_offs[V.sort_keys[i]], 1u)] = i;
 }
 
-// Exclusive prefix of the counting-sort histogram over the whole device.
-static void enqueue_sort_scan(const ViewDevice &D, cudaStream_t st) {
+// Exclusive prefix of the first `bins` counting-sort bins over the whole
+// device (the interval-ray keys use only the first kRaySortBins).
+static void enqueue_sort_scan(const ViewDevice &D, uint32_t bins, cudaStream_t st) {
     size_t bytes = D.scan_temp_bytes;
-    cub::DeviceScan::ExclusiveSum(D.scan_temp, bytes, D.sort_hist, D.sort_offs, (int)kSortBins, st);
+    cub::DeviceScan::ExclusiveSum(D.scan_temp, bytes, D.sort_hist, D.sort_offs, (int)bins, st);
 }
 
 
@@ -979,6 +984,55 @@ __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FramePa
     return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
+// The four children of record (x, y) interpolated together: corners outer,
+// children inner, so each corner's weight and validity are worked out once
+// and its four child records (two adjacent pairs) are loaded together.  Per
+// child the corners are summed in the same order as interpolate(), and the
+// potential (the sum of positive weights) is the same for every child, so
+// every result is bit-identical to four interpolate() calls.
+__device__ __forceinline__ void interpolate_children(const ViewDevice &V, const FrameParams &F,
+                                                     uint32_t child_level, const uint32_t ids[8], float4 frac,
+                                                     uint32_t fine0, uint32_t fine_columns, float4 out[4]) {
+    float acc[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) acc[k][0] = acc[k][1] = acc[k][2] = acc[k][3] = 0.0f;
+    float potential = 0.0f;
+    const unsigned long long base = V.level_base[child_level];
+    const uint32_t dirs = F.dirs[child_level];
+    const uint32_t offset[4] = {fine0, fine0 + 1u, fine0 + fine_columns, fine0 + fine_columns + 1u};
+#pragma unroll
+    for (uint32_t corner = 0; corner < 8u; ++corner) {
+        float ax = (corner & 1u) == 0u ? 1.0f - frac.x : frac.x;
+        float ay = ((corner >> 1) & 1u) == 0u ? 1.0f - frac.y : frac.y;
+        float az = (corner >> 2) == 0u ? 1.0f - frac.z : frac.z;
+        float w = (ax * ay) * az;
+        if (!(w > 0.0f)) continue;
+        potential += w;
+        if (ids[corner] == lux::kEmpty) continue;
+        const float4 *rec = V.merged + base + (unsigned long long)ids[corner] * dirs;
+        float4 s[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) s[k] = __ldg(rec + offset[k]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            if (s[k].w > 0.0f && isfinite(s[k].x) && isfinite(s[k].y) && isfinite(s[k].z) && isfinite(s[k].w)) {
+                float sw = w * lux::saturate(s[k].w);
+                acc[k][0] = acc[k][0] + s[k].x * sw;
+                acc[k][1] = acc[k][1] + s[k].y * sw;
+                acc[k][2] = acc[k][2] + s[k].z * sw;
+                acc[k][3] += sw;
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float total = acc[k][3];
+        out[k] = total > 0.0f ? make_float4(acc[k][0] / total, acc[k][1] / total, acc[k][2] / total,
+                                            lux::saturate(total / fmaxf(potential, 1e-8f)))
+                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+}
+
 // mergeEntry without history, shaders/split.slang:1523-1725.
 // base^n by squaring and multiplying in a fixed order (the CPU restatement
 // rounds identically); pow(blend, observations) of mergeRawRadianceGroup.
@@ -1228,6 +1282,11 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
         ry = jy;
         rz = jz;
     }
+    // The raw record does not depend on the children: stored first, so its
+    // values need no registers across the child interpolation.
+    V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
+                                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    V.mass[base + e] = make_float2(rmass, tmass);
     float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
     if (transmittance > 0.0f && has_children) {
         size_t ci = (size_t)level * F.cell_capacity + cell;
@@ -1245,6 +1304,19 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
         float4 frac = __ldg(V.corner_frac + ci);
         uint32_t x = d % F.columns[level], y = d / F.columns[level];
         uint32_t fine_columns = F.columns[level + 1];
+#if LUX_MERGE_CORNER_OUTER
+        float4 child_value[4];
+        interpolate_children(V, F, level + 1, ids, frac, x * 2u + y * 2u * fine_columns, fine_columns, child_value);
+#pragma unroll
+        for (uint32_t child = 0; child < 4u; ++child) {
+            float4 v = child_value[child];
+            if (!(v.w > 0.0f)) continue;
+            cx = cx + v.x * v.w;
+            cy = cy + v.y * v.w;
+            cz = cz + v.z * v.w;
+            csup += v.w;
+        }
+#else
 #pragma unroll
         for (uint32_t child = 0; child < 4u; ++child) {
             uint32_t fine = (x * 2u + (child & 1u)) + (y * 2u + (child >> 1)) * fine_columns;
@@ -1255,6 +1327,7 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
             cz = cz + v.z * v.w;
             csup += v.w;
         }
+#endif
     }
     if (csup > 0.0f) {
         rx = rx + (transmittance * cx) * 0.25f;
@@ -1265,29 +1338,49 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
     float4 out = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
     V.merged[base + e] = out;
-    V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
-                                                             : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    V.mass[base + e] = make_float2(rmass, tmass);
+}
+
+// Processing order of a level's records: item i of cells x dirs is record
+// (cell, d) taken in direction blocks of kMergeRun consecutive directions,
+// every cell's run of a block before the next block.  A warp still covers
+// 32 consecutive records of one cell (coalesced), while the warps in flight
+// at any moment span few directions of many cells, so the child records they
+// interpolate (four fine directions per record, in the same eight corner
+// cells for neighbouring cells) are shared in cache instead of being re-read
+// once per parent cell, as a cell-major order does on the coarse levels
+// (few cells, up to 2^19 directions each).
+constexpr uint32_t kMergeRun = 32;
+
+__device__ __forceinline__ void merge_item(unsigned long long i, uint32_t cells, uint32_t dirs, uint32_t &cell,
+                                           uint32_t &d) {
+    if (dirs % kMergeRun != 0u) {  // no direction blocks: cell-major
+        cell = (uint32_t)(i / dirs);
+        d = (uint32_t)(i % dirs);
+        return;
+    }
+    const unsigned long long block = (unsigned long long)cells * kMergeRun;
+    if ((unsigned long long)cells * dirs <= 0xffffffffull) {  // 32-bit divisions
+        const uint32_t i32 = (uint32_t)i, b32 = (uint32_t)block;
+        const uint32_t run = i32 / b32, rem = i32 - run * b32;
+        cell = rem / kMergeRun;
+        d = run * kMergeRun + (rem % kMergeRun);
+    } else {
+        const unsigned long long run = i / block, rem = i - run * block;
+        cell = (uint32_t)(rem / kMergeRun);
+        d = (uint32_t)(run * kMergeRun + rem % kMergeRun);
+    }
 }
 
 __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
     merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
     if (*V.error_flags) return;
-    const uint32_t dirs = F.dirs[level];
-    const unsigned long long n = (unsigned long long)V.cell_count[level] * dirs;
+    const uint32_t dirs = F.dirs[level], cells = V.cell_count[level];
+    const unsigned long long n = (unsigned long long)cells * dirs;
     const unsigned long long base = V.level_base[level];
-    // A level's records usually fit 32-bit indices: divide in 32 bits then.
-    const bool narrow = n <= 0xffffffffull;
-    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
-         e += (unsigned long long)gridDim.x * blockDim.x) {
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
         uint32_t cell, d;
-        if (narrow) {
-            cell = (uint32_t)e / dirs;
-            d = (uint32_t)e - cell * dirs;
-        } else {
-            cell = (uint32_t)(e / dirs);
-            d = (uint32_t)(e % dirs);
-        }
+        merge_item(i, cells, dirs, cell, d);
         merge_record(V, F, H, level, base, dirs, cell, d);
     }
 }
@@ -1952,13 +2045,7 @@ __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS) batch
         if (e >= records[j] || *J.V.error_flags) return;
         const uint32_t dirs = J.F.dirs[level];
         uint32_t cell, d;
-        if (e <= 0xffffffffull) {
-            cell = (uint32_t)e / dirs;
-            d = (uint32_t)e - cell * dirs;
-        } else {
-            cell = (uint32_t)(e / dirs);
-            d = (uint32_t)(e % dirs);
-        }
+        merge_item(e, J.V.cell_count[level], dirs, cell, d);
         merge_record(J.V, J.F, J.H, level, J.V.level_base[level], dirs, cell, d);
     });
 }
@@ -2937,10 +3024,10 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
             ViewDevice Dr = D;  // ray pass view: optional coherence order of interval rays
             Dr.sort_keys = nullptr;
             if (T.sort_rays) {
-                cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
+                cudaMemsetAsync(D.sort_hist, 0, (size_t)kRaySortBins * 4, st);
                 ray_keys_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, F, scene->view, pos, nrm, rays);
                 sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
-                enqueue_sort_scan(D, st);
+                enqueue_sort_scan(D, kRaySortBins, st);
                 sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, nullptr, rays);
                 Dr.ray_order = D.sort_perm;
             }
@@ -2975,7 +3062,7 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
             if (T.sort_queries) {
                 cudaMemsetAsync(D.sort_hist, 0, (size_t)kSortBins * 4, st);
                 sort_hist_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
-                enqueue_sort_scan(D, st);
+                enqueue_sort_scan(D, kSortBins, st);
                 sort_scatter_kernel<<<ctx->sm_count * 8, 256, 0, st>>>(D, D.ts.queue_count, F.queue_capacity);
                 Dq.query_order = D.sort_perm;
             }

@@ -8,6 +8,7 @@ import pytest
 
 import bevy_penumbra_b200 as bp
 import oracle
+from bevy_penumbra_b200 import scenes
 from tests.helpers import empty_device, from_device, packed, to_device
 from tests.test_pathtrace import rectangle_irradiance, rectangle_scene
 
@@ -77,8 +78,39 @@ def test_two_vertex_paths_agree_with_the_one_bounce_estimator():
     assert lit.sum() >= 24
     np.testing.assert_array_equal(path[~lit, :3].sum(1) < 1e-3, True)
     # Both are Monte Carlo estimates (the cosine-ray one sees the small
-    # emitter only by chance, a few per cent of noise per point): the mean
-    # signed difference bounds a bias, the per-point bounds the noise.
+    # emitter only by chance, a few per cent of noise per point).  The
+    # cosine rays start normal_bias (5 mm) above the point, which raises the
+    # direct light of the emitter 2 m above by about 0.5 per cent (the
+    # next-event geometry is taken at the point itself), and the bounce term
+    # differs by about one per cent more (measured with 2^21 cosine rays per
+    # point on the oracle: -1.5 per cent in all, -1.1 with a 0.5 mm bias).
     rel = (path[lit, :3].sum(1) - one[lit, :3].sum(1)) / one[lit, :3].sum(1)
-    assert abs(rel.mean()) < 0.01, rel
-    assert np.median(np.abs(rel)) < 0.03 and np.abs(rel).max() < 0.15, rel
+    assert -0.03 < rel.mean() < 0.005, rel
+    assert np.median(np.abs(rel)) < 0.04 and np.abs(rel).max() < 0.15, rel
+
+
+def test_direct_light_agrees_with_the_cosine_estimator():
+    """Black walls leave the direct light alone: next-event estimation at
+    the receiver (one diffuse vertex) and cosine rays that see the emitter
+    estimate the same irradiance once the rays' origin offset is small."""
+    desc = scenes.cornell()
+    for words in desc.materials:
+        f = words.view(np.float32)
+        if f[4] == 0.0:
+            f[0:3] = 0.0
+    pk = bp.PackedScene.from_desc(desc)
+    settings = bp.RadianceCascades(emissive_samples=16, normal_bias=0.0005).sanitized()
+    pos, nrm = points("cornell", 32, 9)
+    path = gpu_path(pk, settings, pos, nrm, 1 << 18, 1, 3)
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, pk)
+    d_p, d_n, d_o = to_device(pos), to_device(nrm), empty_device(len(pos) * 32)
+    bp.reference_irradiance(ctx, scene, settings, d_p.data_ptr(), d_n.data_ptr(), len(pos), 1 << 23, 3,
+                            d_o.data_ptr())
+    one = from_device(d_o, np.float64, (len(pos), 4))
+    lit = one[:, :3].sum(1) > 1e-3
+    assert lit.sum() >= 24
+    # Points in deep penumbra (a few per cent of the emitter visible) keep
+    # about a per cent of noise in either estimate; the mean bounds a bias.
+    rel = (path[lit, :3].sum(1) - one[lit, :3].sum(1)) / one[lit, :3].sum(1)
+    assert abs(rel.mean()) < 0.006 and np.abs(rel).max() < 0.05, rel
