@@ -78,6 +78,35 @@ def direction_count(settings, level: int) -> int:
     return (settings.base_columns * settings.base_rows) << (2 * level)
 
 
+def merge_compulsory_bytes(settings, cells, history: bool) -> int:
+    """Bytes the merge stage must move in one frame: per record the sample
+    count and sum read (20 B) and the merged, raw and mass records written
+    (40 B), with history the previous frame's raw and mass records read
+    (24 B); per cell its corner ids, corner fractions and previous-frame id
+    (52 B); and every level below the coarsest reads each child record once
+    (16 B)."""
+    total = 0
+    for level in range(settings.levels):
+        records = int(cells[level]) * direction_count(settings, level)
+        total += records * (60 + (24 if history else 0)) + int(cells[level]) * 52
+        if level + 1 < settings.levels:
+            total += int(cells[level + 1]) * direction_count(settings, level + 1) * 16
+    return total
+
+
+def merge_roofline(settings, st, merge_ms, peak, peak_kind):
+    """The merge stage (corners, history maps, merges of every level) against
+    the HBM copy rate on its compulsory bytes."""
+    history = settings.history_frames > 0 and (settings.temporal_blend > 0 or settings.split_transmittance_blend > 0)
+    cells = list(st.cells)[:settings.levels]
+    nbytes = merge_compulsory_bytes(settings, cells, history)
+    achieved = nbytes / (merge_ms * 1e-3) / 1e9
+    return {"kernel": "merge stage (merge_prep_kernel: corners and history maps of every level, merge_kernel per level)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+            "compulsory_bytes": nbytes, "ms": merge_ms,
+            "records": sum(int(c) * direction_count(settings, l) for l, c in enumerate(cells))}
+
+
 def world_normals(packed, hits, dirs):
     """Geometric normals of hit triangles in world space, facing the ray."""
     sw = packed.scene_words
@@ -745,6 +774,7 @@ def run_ours(args, rank, world):
                          "traffic_note": "ncu dram bytes of the traversal kernels per frame, scaled by rays from "
                                          "the 65,536-triangle capture; the scene stays in L2",
                          "algorithmic_bytes": alg_bytes},
+            "merge_roofline": merge_roofline(settings, st, float(np.median(merge_ms)), peak, peak_kind),
             "cpu_baseline": {"value": cpu["rays"] / cpu["seconds"] / 1e6, "unit": "Mrays/s",
                              "cores": os.cpu_count(), "kind": "port",
                              "sample": cpu_sample_text(cpu, w, CPU_STRIDE)},
@@ -1125,6 +1155,34 @@ def full_line(args, world, device, frames):
     return line
 
 
+def run_frames(args):
+    """--frames-only: plain frames for ncu captures (a fixed launch sequence:
+    8 merge launches per frame at 8 cascades)."""
+    import torch
+
+    from bevy_penumbra_b200.autotune import START, tuning_of
+    torch.cuda.set_device(0)
+    w = build_workload(0)
+    view, scene, settings = w["view"], w["scene"], w["settings"]
+    d_rpos = torch.from_numpy(w["rpos"]).cuda()
+    d_rnrm = torch.from_numpy(w["rnrm"]).cuda()
+    view.set_tuning(**tuning_of(START))
+    view.set_timing(True)
+    stages = []
+    for step in range(args.warmup + args.steps):
+        settings.frame_index = step
+        view.trace_merge(scene, settings, d_rpos.data_ptr(), d_rnrm.data_ptr(), len(w["rpos"]))
+        torch.cuda.synchronize()
+        t = view.timings()
+        if step >= args.warmup:
+            stages.append((t.seed_ms, t.trace_ms, t.merge_ms, t.pack_ms))
+    st = view.stats()
+    m = np.median(np.array(stages), axis=0)
+    print(json.dumps({"profile": "frames-only", "width": WIDTH, "height": HEIGHT, "triangles": TRIANGLES,
+                      "tuning": tuning_of(START), "seed_ms": m[0], "trace_ms": m[1], "merge_ms": m[2], "pack_ms": m[3],
+                      "cells": list(st.cells)[:settings.levels], "error_flags": int(st.error_flags)}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1145,6 +1203,9 @@ def main():
                     help="learned-cache form: relative bias above which a validated cell falls back")
     ap.add_argument("--small", action="store_true",
                     help="profiling case: 65,536-triangle atrium at 640x360 (not a benchmark line)")
+    ap.add_argument("--frames-only", action="store_true",
+                    help="profiling target: --warmup + --steps plain frames of the atrium workload with the "
+                         "autotuner's starting tuning (no search, no other forms); prints the stage times")
     args = ap.parse_args()
     if args.small:
         global WIDTH, HEIGHT, TRIANGLES, EYE, TARGET
@@ -1152,7 +1213,9 @@ def main():
         EYE, TARGET = (-7.0, 3.0, -6.0), (2.0, 4.0, 3.0)
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    if args.impl == "reference":
+    if args.frames_only:
+        run_frames(args)
+    elif args.impl == "reference":
         run_reference(args, rank, world)
     elif args.workload == "batched":
         run_batched(args, rank, world)

@@ -70,7 +70,7 @@ __device__ __forceinline__ bool box_interval(f3 o, f3 d, float lx, float ly, flo
 // NaN, which fmaxf/fminf ignore -- the reference's inside test for a zero
 // component.
 #ifndef LUX_NODE_EMPTY_CHECK
-#define LUX_NODE_EMPTY_CHECK 1
+#define LUX_NODE_EMPTY_CHECK 0
 #endif
 
 struct SlabRay {

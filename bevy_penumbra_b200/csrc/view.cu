@@ -941,13 +941,8 @@ __device__ __forceinline__ void corners_item(const ViewDevice &V, const FramePar
                               bz + (int32_t)(corner >> 2), lod);
 }
 
-__global__ void corners_kernel(ViewDevice V, FrameParams F, uint32_t level) {
-    if (*V.error_flags) return;
-    uint32_t cells = V.cell_count[level];
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x)
-        corners_item(V, F, level, c);
-}
 
+#if !LUX_MERGE_CORNER_OUTER
 // interpolateMergedChildSources, shaders/split.slang:389-479 (one group).
 __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FrameParams &F, uint32_t child_level,
                                               const uint32_t ids[8], float4 frac, uint32_t dir) {
@@ -983,6 +978,7 @@ __device__ __forceinline__ float4 interpolate(const ViewDevice &V, const FramePa
     if (total > 0.0f) return make_float4(sx / total, sy / total, sz / total, lux::saturate(total / fmaxf(potential, 1e-8f)));
     return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
+#endif
 
 // The four children of record (x, y) interpolated together: corners outer,
 // children inner, so each corner's weight and validity are worked out once
@@ -1074,10 +1070,17 @@ __device__ __forceinline__ void history_map_item(const ViewDevice &V, const Fram
     V.hist_cell[(size_t)level * F.cell_capacity + c] = id;
 }
 
-__global__ void history_map_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
-    uint32_t cells = min(V.cell_count[level], F.cell_capacity);
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x)
-        history_map_item(V, F, H, level, c);
+// Before the merge, one launch for every level: each cell's corners in the
+// next level, and with history its previous frame's id.
+__global__ void merge_prep_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
+    if (*V.error_flags) return;
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        const uint32_t cells = min(V.cell_count[l], F.cell_capacity);
+        for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
+            if (l + 1u < F.levels) corners_item(V, F, l, c);
+            if (F.history) history_map_item(V, F, H, l, c);
+        }
+    }
 }
 
 // A record's history is invalid when the region its rays may have crossed
@@ -1209,9 +1212,16 @@ __global__ void retain_insert_kernel(ViewDevice V, FrameParams F, HistoryDevice 
 // transmittance, then Eq. 7 with the children: I = [J (1 - beta) + beta
 // mean_4(trilerp_8(I_child) support)] / support.
 // Record (cell, d) of `level`; base = the level's first record.
-__device__ __forceinline__ void merge_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
-                                             uint32_t level, unsigned long long base, uint32_t dirs, uint32_t cell,
-                                             uint32_t d) {
+// The record's own part (fresh mean, history blend, raw and mass records
+// written): its radiance, support and transmittance, and whether the
+// children must be interpolated (transmittance > 0 below the coarsest level).
+struct MergeOwn {
+    float rx, ry, rz, support, transmittance;
+};
+
+__device__ __forceinline__ bool merge_own(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                          uint32_t level, unsigned long long base, uint32_t dirs, uint32_t cell,
+                                          uint32_t d, MergeOwn &own) {
     const unsigned long long e = (unsigned long long)cell * dirs + d;
     const bool has_children = level + 1u < F.levels;
     const float jb = F.radiance_blend, tb = F.transmittance_blend;
@@ -1287,8 +1297,19 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
     V.raw[base + e] = (cnt || rmass > 0.0f || tmass > 0.0f) ? make_float4(jx, jy, jz, beta)
                                                              : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     V.mass[base + e] = make_float2(rmass, tmass);
+    own = MergeOwn{rx, ry, rz, support, transmittance};
+    return transmittance > 0.0f && has_children;
+}
+
+// The children's part (with `children`) and the merged record written.
+__device__ __forceinline__ void merge_finish(const ViewDevice &V, const FrameParams &F, uint32_t level,
+                                             unsigned long long base, uint32_t dirs, uint32_t cell, uint32_t d,
+                                             MergeOwn own, bool children) {
+    const unsigned long long e = (unsigned long long)cell * dirs + d;
+    float rx = own.rx, ry = own.ry, rz = own.rz, support = own.support;
+    const float transmittance = own.transmittance;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f, csup = 0.0f;
-    if (transmittance > 0.0f && has_children) {
+    if (children) {
         size_t ci = (size_t)level * F.cell_capacity + cell;
         uint32_t ids[8];
         const uint4 *cid = reinterpret_cast<const uint4 *>(V.corner_ids + ci * 8);  // 32-byte rows
@@ -1339,6 +1360,15 @@ __device__ __forceinline__ void merge_record(const ViewDevice &V, const FramePar
     if (support > 0.0f) out = make_float4(rx / support, ry / support, rz / support, lux::saturate(support));
     V.merged[base + e] = out;
 }
+
+__device__ __forceinline__ void merge_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                             uint32_t level, unsigned long long base, uint32_t dirs, uint32_t cell,
+                                             uint32_t d) {
+    MergeOwn own;
+    const bool children = merge_own(V, F, H, level, base, dirs, cell, d, own);
+    merge_finish(V, F, level, base, dirs, cell, d, own, children);
+}
+
 
 // Processing order of a level's records: item i of cells x dirs is record
 // (cell, d) taken in direction blocks of kMergeRun consecutive directions,
@@ -2754,9 +2784,7 @@ static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     const ViewDevice &D = v->dev;
     const int grid = v->ctx->sm_count * 8;
     const HistoryDevice H = history_device(v);
-    for (uint32_t l = 0; l + 1 < F.levels; ++l) corners_kernel<<<grid, 128, 0, st>>>(D, F, l);
-    if (F.history)
-        for (uint32_t l = 0; l < F.levels; ++l) history_map_kernel<<<grid, 128, 0, st>>>(D, F, H, l);
+    if (F.levels > 1 || F.history) merge_prep_kernel<<<grid, 128, 0, st>>>(D, F, H);
     for (int l = (int)F.levels - 1; l >= 0; --l)
         merge_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F, H, (uint32_t)l);
 }
