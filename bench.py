@@ -455,7 +455,7 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     for step in range(LEARNED_WARMUP):
         frame(step)
     torch.cuda.synchronize(device)
-    ms = []
+    ms, stages = [], []
     for step in range(args.steps):
         flush.fill_(float(step))
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -464,7 +464,10 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
         end.record(stream)
         torch.cuda.synchronize(device)
         ms.append(start.elapsed_time(end))
+        t = lview.timings()
+        stages.append((t.seed_ms, t.trace_ms, t.merge_ms, t.pack_ms))
     learned_ms = float(np.sum(ms)) / args.steps
+    stage_ms = np.median(np.array(stages), axis=0)
     cs = lview.cache_stats()
     st = lview.stats()
     if st.error_flags or cache.stats().error_flags:
@@ -475,6 +478,8 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
     return {
         "ms_per_step": learned_ms, "value": interval_rays / (learned_ms * 1e-3) / 1e6, "unit": "Mrays/s",
         "speedup_vs_plain": plain_ms / learned_ms,
+        "stages_ms": {"seed": float(stage_ms[0]), "trace_with_cache": float(stage_ms[1]),
+                      "merge": float(stage_ms[2]), "pack": float(stage_ms[3])},
         "relative_rmse": err["relative_rmse"], "plain_relative_rmse": plain_error["relative_rmse"],
         "rmse_change": err["relative_rmse"] / plain_error["relative_rmse"] - 1.0,
         "per_surface": err["per_surface"],
