@@ -187,19 +187,26 @@ struct Collapser {
     }
 };
 
-__global__ void trace_rays_kernel(SceneView S, const LuxRay *__restrict__ rays, uint32_t count, uint32_t any_hit,
-                                  LuxHit *__restrict__ hits, unsigned long long *__restrict__ counters) {
+// 128 threads per block; every lane of a warp walks together (whole-warp
+// leaf tests), lanes past `count` without a query.
+__global__ void __launch_bounds__(128) trace_rays_kernel(SceneView S, const LuxRay *__restrict__ rays, uint32_t count,
+                                                         uint32_t any_hit, LuxHit *__restrict__ hits,
+                                                         unsigned long long *__restrict__ counters) {
+    __shared__ lux::LeafScratch scratch[4];
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     lux::TraceCounters cn{0, 0, 0};
-    if (i < count) {
-        LuxRay r = rays[i];
-        lux::f3 o{r.origin[0], r.origin[1], r.origin[2]};
-        lux::f3 d{r.direction[0], r.direction[1], r.direction[2]};
-        lux::Hit h;
-        if (any_hit)
-            lux::trace<true>(S, o, d, 0.0f, r.limit, h, cn);
-        else
-            lux::trace<false>(S, o, d, r.tmin, r.limit, h, cn);
+    const bool active = i < count;
+    LuxRay r{};
+    if (active) r = rays[i];
+    lux::f3 o{r.origin[0], r.origin[1], r.origin[2]};
+    lux::f3 d{r.direction[0], r.direction[1], r.direction[2]};
+    lux::Hit h;
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
+    if (any_hit)
+        lux::trace_warp<true>(S, active, o, d, 0.0f, r.limit, h, cn, L);
+    else
+        lux::trace_warp<false>(S, active, o, d, r.tmin, r.limit, h, cn, L);
+    if (active) {
         LuxHit out;
         out.distance = h.t;
         out.triangle = h.tri;

@@ -295,6 +295,14 @@ __device__ __forceinline__ float key_entry(uint32_t key) { return as_float(key &
 // (per TLAS walk and per instance walk), 2 / 1 when the stack is exhausted in
 // the TLAS / a BLAS, after which the walk continues over every instance / every
 // triangle of the instance in order (shaders/traversal.slang:498-517, :729-745).
+// One warp's scratch for the cooperative leaf pass (shared memory).  Only
+// the owning lane writes its own slots.
+struct LeafScratch {
+    float ox[32], oy[32], oz[32], dx[32], dy[32], dz[32], sx[32], sy[32], lower[32], limit[32];
+    uint32_t axes[32], flags[32], first[32], pre[32];
+    unsigned long long best[32];
+};
+
 template <bool kAnyHit, int kDepth = kStack>
 struct Walker {
     Hit hit;
@@ -355,7 +363,14 @@ struct Walker {
     // entry.  Returns true when the query is complete.
     // The stack lives outside the walker so the walker's fields stay in
     // registers; only the stack itself is addressed dynamically.
-    __device__ __forceinline__ bool step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
+    // Inner nodes down to a leaf and that leaf's kind: a TLAS leaf enters its
+    // first instance; a BLAS leaf within the step budget is returned as
+    // (first, count) for its triangle tests (count 0: none).  Returns true
+    // when the query is complete.
+    __device__ __forceinline__ bool descend(const SceneView &S, uint2 *stack, TraceCounters &cn, uint32_t &leaf_first,
+                                            uint32_t &leaf_count) {
+        leaf_first = 0;
+        leaf_count = 0;
         while (have && (cur & kLeafBit) == 0u) {
             bool in_tlas = blas_base < 0;
             uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
@@ -454,6 +469,18 @@ struct Walker {
                 hit.errors |= kQueryUnsupported;
                 sp = blas_base;
             } else {
+                leaf_first = first;
+                leaf_count = count;
+            }
+        }
+        return false;
+    }
+
+    // The triangles of one BLAS leaf in order; true when an any-hit query is
+    // complete.
+    __device__ __forceinline__ bool test_leaf(const SceneView &S, uint32_t first, uint32_t count, TraceCounters &cn) {
+        {
+            {
                 for (uint32_t t = first; t < first + count; ++t) {
                     f3 A, B, C;
                     load_triangle(S.triangles, t, A, B, C);
@@ -480,7 +507,12 @@ struct Walker {
                 }
             }
         }
-        // The next pending entry, leaving instances and fallbacks as needed.
+        return false;
+    }
+
+    // The next pending entry, leaving instances and fallbacks as needed; true
+    // when the query is complete.
+    __device__ __forceinline__ bool next(const SceneView &S, uint2 *stack) {
         while (!have) {
             if (blas_base >= 0 && sp == blas_base) {
                 if (blas_next != kEmpty && blas_next < inst_first + inst_count) {
@@ -521,6 +553,143 @@ struct Walker {
         }
         return false;
     }
+
+    // One step: inner nodes down to a leaf, that leaf, then the next pending
+    // entry.  Returns true when the query is complete.
+    // The stack lives outside the walker so the walker's fields stay in
+    // registers; only the stack itself is addressed dynamically.
+    __device__ __forceinline__ bool step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
+        uint32_t first, count;
+        if (descend(S, stack, cn, first, count)) return true;
+        if (count && test_leaf(S, first, count, cn)) return true;
+        return next(S, stack);
+    }
+
+    // The BLAS leaves that the lanes of the warp reached in this step, tested
+    // by the whole warp: lane l owns a leaf of count(l) triangles (0: none),
+    // the warp's sum(count) (ray, triangle) pairs are dealt out to its lanes
+    // in turn, and each owner then takes the best of its candidates.  The
+    // closest candidate is the minimum of (distance bits, triangle index)
+    // over triangles of one instance, which is the order hit_better applies,
+    // so the hit is the one the in-order loop of test_leaf keeps, and the
+    // owner re-evaluates the winner for its barycentrics.  For any hit the
+    // lowest blocking triangle index is the one the in-order loop stops at,
+    // and the owner counts the triangles that loop would have tested.
+    // Returns true when the lane's any-hit query is complete.
+    __device__ bool leaf_pass(const SceneView &S, LeafScratch *L, uint32_t first, uint32_t count, TraceCounters &cn) {
+        const unsigned group = 0xffffffffu;  // every lane of the warp takes part
+        const uint32_t lane = threadIdx.x & 31u;
+        const unsigned below = (1u << lane) - 1u;
+        uint32_t pre = 0, total = 0;
+#pragma unroll
+        for (int b = 0; b < 5; ++b) {  // leaf counts are at most 16
+            const unsigned v = __ballot_sync(group, (count >> b) & 1u);
+            pre += (uint32_t)__popc(v & below) << b;
+            total += (uint32_t)__popc(v) << b;
+        }
+        if (total == 0u) return false;
+        // Every lane publishes its prefix (non-decreasing in lane order),
+        // owners their ray.
+        L->pre[lane] = pre;
+        if (count) {
+            L->ox[lane] = lo.x;
+            L->oy[lane] = lo.y;
+            L->oz[lane] = lo.z;
+            L->dx[lane] = ld.x;
+            L->dy[lane] = ld.y;
+            L->dz[lane] = ld.z;
+            L->sx[lane] = tri_ray.sx;
+            L->sy[lane] = tri_ray.sy;
+            L->axes[lane] = tri_ray.kx | (tri_ray.ky << 2) | (tri_ray.kz << 4) | (tri_ray.valid ? 64u : 0u);
+            L->flags[lane] = inst_flags;
+            L->first[lane] = first;
+            L->lower[lane] = lower;
+            L->limit[lane] = hit.t;
+            L->best[lane] = ~0ull;
+        }
+        __syncwarp(group);
+        const uint32_t workers = 32u, me = lane;
+        for (uint32_t p = me; p < total; p += workers) {
+            // The pair's owner: the highest lane whose prefix is <= p (a lane
+            // without a leaf shares its prefix with the next lane, so the
+            // highest such lane owns triangles).
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t half = 16; half >= 1u; half >>= 1)
+                if (o + half < 32u && L->pre[o + half] <= p) o += half;
+            const uint32_t t = L->first[o] + (p - L->pre[o]);
+            f3 A, B, C;
+            load_triangle(S.triangles, t, A, B, C);
+            const f3 rd{L->dx[o], L->dy[o], L->dz[o]};
+            if (cull_reject(L->flags[o], A, B, C, rd)) continue;
+            TriRay tr;
+            const uint32_t ax = L->axes[o];
+            tr.kx = ax & 3u;
+            tr.ky = (ax >> 2) & 3u;
+            tr.kz = (ax >> 4) & 3u;
+            tr.valid = (ax & 64u) != 0u;
+            tr.sx = L->sx[o];
+            tr.sy = L->sy[o];
+            float w1 = 0.0f, w2 = 0.0f;
+            const float dist = intersect_triangle(f3{L->ox[o], L->oy[o], L->oz[o]}, rd, tr, A, B, C, w1, w2);
+            if (kAnyHit) {
+                if (dist > 0.000025f && dist < L->limit[o]) atomicMin(&L->best[o], (unsigned long long)t);
+            } else if (dist > L->lower[o]) {
+                atomicMin(&L->best[o], ((unsigned long long)as_uint(dist) << 32) | t);
+            }
+        }
+        __syncwarp(group);
+        bool done = false;
+        if (count) {
+            const unsigned long long b = L->best[lane];
+            if (kAnyHit) {
+                if (b != ~0ull) {
+                    const uint32_t t = (uint32_t)b;
+                    cn.triangles += t - first + 1u;
+                    hit.tri = t;
+                    hit.inst = inst;
+                    hit.errors &= ~kQueryUnsupported;
+                    done = true;
+                } else {
+                    cn.triangles += count;
+                }
+            } else {
+                cn.triangles += count;
+                if (b != ~0ull) {
+                    const float dist = as_float((uint32_t)(b >> 32));
+                    const uint32_t t = (uint32_t)b;
+                    if (hit_better(dist, inst, t, hit)) {
+                        f3 A, B, C;
+                        load_triangle(S.triangles, t, A, B, C);
+                        float w1 = 0.0f, w2 = 0.0f;
+                        intersect_triangle(lo, ld, tri_ray, A, B, C, w1, w2);
+                        hit.t = dist;
+                        hit.tri = t;
+                        hit.inst = inst;
+                        hit.b1 = w1;
+                        hit.b2 = w2;
+                    }
+                }
+            }
+        }
+        __syncwarp(group);  // the scratch is rewritten by the next pass
+        return done;
+    }
+
+    // step() for walks of a whole warp: every lane calls it in every round
+    // (alive = the lane still has a query), so the leaf pass runs over the
+    // full warp.  Returns true when the lane's query is complete (or it has
+    // none).
+    __device__ __forceinline__ bool step_warp(const SceneView &S, uint2 *stack, TraceCounters &cn, LeafScratch *L,
+                                              bool alive) {
+        uint32_t first = 0, count = 0;
+        bool complete = !alive;
+        if (alive) complete = descend(S, stack, cn, first, count);
+        if (complete) count = 0;
+        if (leaf_pass(S, L, first, count, cn)) complete = true;
+        if (complete) return true;
+        return next(S, stack);
+    }
 };
 
 // Closest hit (kAnyHit = false) or any hit of one ray.  kDepth is the stack
@@ -533,6 +702,23 @@ __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, H
     if (w.start(S, o, d, tmin, limit))
         while (!w.step(S, stack, cn)) {
         }
+    hit = w.hit;
+}
+
+// trace() for a whole warp: every lane of the warp calls it (active: the
+// lane has a query), and the BLAS leaves reached in each round are tested
+// by the whole warp (Walker::leaf_pass).  A lane without a query returns an
+// undefined hit.
+template <bool kAnyHit, int kDepth = kStack>
+__device__ void trace_warp(const SceneView &S, bool active, f3 o, f3 d, float tmin, float limit, Hit &hit,
+                           TraceCounters &cn, LeafScratch *L) {
+    Walker<kAnyHit, kDepth> w;
+    uint2 stack[kDepth];
+    bool alive = active && w.start(S, o, d, tmin, limit);
+    while (__any_sync(0xffffffffu, alive)) {
+        const bool complete = w.step_warp(S, stack, cn, L, alive);
+        alive = alive && !complete;
+    }
     hit = w.hit;
 }
 

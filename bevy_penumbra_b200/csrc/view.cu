@@ -59,6 +59,11 @@
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
 #endif
+// Whole-warp traversal in the persistent trace kernels: the BLAS leaves the
+// lanes reach in a step are tested by the whole warp.
+#ifndef LUX_WARP_LEAVES
+#define LUX_WARP_LEAVES 1
+#endif
 // The fused batch trace kernel carries the shading phase's registers too.
 #ifndef LUX_FUSED_MIN_BLOCKS
 #define LUX_FUSED_MIN_BLOCKS 4
@@ -566,6 +571,41 @@ __device__ __forceinline__ bool closest_split_ray(const ViewDevice &V, const Fra
     return true;
 }
 
+// closest_split_ray for a whole warp (every lane calls it; `valid`: the
+// lane has a slot), with the warp's leaves tested together.
+template <int kDepth = lux::kStack>
+__device__ __forceinline__ bool closest_split_ray_warp(const ViewDevice &V, const FrameParams &F, uint32_t frame,
+                                                       const SceneView &S, const float4 *__restrict__ pos,
+                                                       const float4 *__restrict__ nrm, uint32_t slot, bool valid,
+                                                       lux::TraceCounters &cn, lux::LeafScratch *L) {
+    bool active = valid;
+    uint32_t ray = 0;
+    f3 origin{0.0f, 0.0f, 0.0f}, dir{0.0f, 0.0f, 0.0f};
+    if (valid) {
+        ray = V.ray_order ? V.ray_order[slot] : slot;
+        uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
+        float4 p4 = pos[i], n4 = nrm[i];
+        if (F.sparse && p4.w == 0.0f) {
+            lux::Hit none;
+            none.t = 0.0f;
+            none.b1 = none.b2 = 0.0f;
+            none.tri = none.inst = lux::kEmpty;
+            none.errors = lux::kQueryUnsupported;
+            store_ray(V, ray, f3{0.0f, 0.0f, 0.0f}, f3{0.0f, 0.0f, 0.0f}, none);
+            active = false;
+        } else {
+            f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
+            float u, v;
+            split_direction(V, F, frame, i, k, n, dir, u, v);
+            origin = lux::ray_offset(p, n, F.shade.normal_bias);
+        }
+    }
+    lux::Hit hit;
+    lux::trace_warp<false, kDepth>(S, active, origin, dir, 0.0f, 1e20f, hit, cn, L);
+    if (active) store_ray(V, ray, origin, dir, hit);
+    return active;
+}
+
 // Persistent warps: a tile of `tile` consecutive rays per fetch (one atomic
 // per warp), taken 32 at a time.
 __device__ __forceinline__ uint32_t warp_fetch(uint32_t *counter, uint32_t tile = 32u) {
@@ -580,6 +620,10 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_ker
                                                             const float4 *__restrict__ nrm, uint32_t ray_count,
                                                             uint32_t tile) {
     if (*V.error_flags) return;
+#if LUX_WARP_LEAVES
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
+#endif
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     while (true) {
@@ -587,8 +631,13 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS) closest_split_ker
         if (base >= ray_count) break;
         for (uint32_t k = 0; k < tile && base + k < ray_count; k += 32u) {
             uint32_t slot = base + k + (threadIdx.x & 31u);
+#if LUX_WARP_LEAVES
+            if (closest_split_ray_warp<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, slot < ray_count, cn, L))
+                st[kStatInterval] += 1;
+#else
             if (slot < ray_count && closest_split_ray<kDepth>(V, F, F.shade.frame, S, pos, nrm, slot, cn))
                 st[kStatInterval] += 1;
+#endif
         }
     }
     st[kStatNodes] = cn.nodes;
@@ -791,10 +840,31 @@ __device__ __forceinline__ void shadow_query(const ViewDevice &V, const SceneVie
     V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
 }
 
+// shadow_query for a whole warp (every lane calls it; `valid`: the lane has
+// a query).
+template <int kDepth = lux::kStack>
+__device__ __forceinline__ void shadow_query_warp(const ViewDevice &V, const SceneView &S, uint32_t i, bool valid,
+                                                  lux::TraceCounters &cn, lux::LeafScratch *L) {
+    uint32_t qi = 0;
+    float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b = a;
+    if (valid) {
+        qi = V.ts.query_slot[V.query_order ? V.query_order[i] : i];
+        a = V.ts.queue_o[qi];
+        b = V.ts.queue_d[qi];
+    }
+    lux::Hit sh;
+    lux::trace_warp<true, kDepth>(S, valid, f3{a.x, a.y, a.z}, f3{b.x, b.y, b.z}, 0.0f, a.w, sh, cn, L);
+    if (valid) V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
+}
+
 template <int kDepth>
 __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                                              uint32_t tile) {
     if (*V.error_flags) return;
+#if LUX_WARP_LEAVES
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
+#endif
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
@@ -803,10 +873,15 @@ __global__ void __launch_bounds__(128, LUX_SHADOW_MIN_BLOCKS) shadow_kernel(View
         if (base >= n) break;
         for (uint32_t k = 0; k < tile && base + k < n; k += 32u) {
             uint32_t i = base + k + (threadIdx.x & 31u);
+#if LUX_WARP_LEAVES
+            shadow_query_warp<kDepth>(V, S, i, i < n, cn, L);
+            if (i < n) st[kStatShadow] += 1;
+#else
             if (i < n) {
                 shadow_query<kDepth>(V, S, i, cn);
                 st[kStatShadow] += 1;
             }
+#endif
         }
     }
     st[kStatNodes] = cn.nodes;
