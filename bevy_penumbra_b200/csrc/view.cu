@@ -1702,7 +1702,8 @@ __device__ __forceinline__ void flush_stats(unsigned long long *stats, unsigned 
 // A tile of `tile` rays may span jobs: the job is found per 32-ray chunk.
 __device__ __forceinline__ void closest_batch_phase(const BatchJob *__restrict__ jobs,
                                                     const uint32_t *__restrict__ begin, uint32_t n, uint32_t total,
-                                                    uint32_t fr, uint32_t *counter, uint32_t tile) {
+                                                    uint32_t fr, uint32_t *counter, uint32_t tile,
+                                                    lux::LeafScratch *L) {
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t cur = lux::kEmpty;
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -1717,13 +1718,11 @@ __device__ __forceinline__ void closest_batch_phase(const BatchJob *__restrict__
                 if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
                 cur = j;
             }
-            if (*J.V.error_flags) continue;
+            if (__shfl_sync(0xffffffffu, *J.V.error_flags, 0)) continue;  // one value for the warp
             uint32_t slot = base - __ldg(begin + j) + lane;
-            if (slot < J.rays) {
-                SceneView S = J.S;
-                closest_split_ray(J.V, J.F, fr, S, J.pos, J.nrm, slot, cn);
-                st[kStatInterval] += 1;
-            }
+            SceneView S = J.S;
+            closest_split_ray_warp(J.V, J.F, fr, S, J.pos, J.nrm, slot, slot < J.rays, cn, L);
+            if (slot < J.rays) st[kStatInterval] += 1;
         }
     }
     if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, false);
@@ -1737,7 +1736,7 @@ __device__ __forceinline__ void shade_batch_phase(const BatchJob *__restrict__ j
         uint32_t base = w * 32u;
         uint32_t j = find_job(begin, n, base);
         const BatchJob &J = jobs[j];
-        if (*J.V.error_flags) continue;
+        if (__shfl_sync(0xffffffffu, *J.V.error_flags, 0)) continue;  // one value for the warp
         lux::ShadeParams P = J.F.shade;
         P.frame = fr;
         SceneView S = J.S;
@@ -1797,7 +1796,7 @@ __device__ __forceinline__ uint32_t find_query_job(const uint32_t *qbegin, uint3
 }
 
 __device__ __forceinline__ void shadow_batch_phase(const BatchJob *__restrict__ jobs, const uint32_t *qbegin,
-                                                   uint32_t n, uint32_t *counter, uint32_t tile) {
+                                                   uint32_t n, uint32_t *counter, uint32_t tile, lux::LeafScratch *L) {
     const uint32_t total = qbegin[n];
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t cur = lux::kEmpty;
@@ -1814,11 +1813,10 @@ __device__ __forceinline__ void shadow_batch_phase(const BatchJob *__restrict__ 
                 cur = j;
             }
             uint32_t i = base - qbegin[j] + lane;
-            if (i < job_queries(J)) {
-                SceneView S = J.S;
-                shadow_query(J.V, S, i, cn);
-                st[kStatShadow] += 1;
-            }
+            const bool valid = i < job_queries(J);
+            SceneView S = J.S;
+            shadow_query_warp(J.V, S, i, valid, cn, L);
+            if (valid) st[kStatShadow] += 1;
         }
     }
     if (cur != lux::kEmpty) flush_stats(jobs[cur].V.stats, st, cn, true);
@@ -1833,7 +1831,7 @@ __device__ __forceinline__ void deposit_batch_phase(const BatchJob *__restrict__
         uint32_t base = w * 32u;
         uint32_t j = find_job(begin, n, base);
         const BatchJob &J = jobs[j];
-        if (*J.V.error_flags) continue;
+        if (__shfl_sync(0xffffffffu, *J.V.error_flags, 0)) continue;  // one value for the warp
         unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
         uint32_t ray = base - __ldg(begin + j) + lane;
         if (ray < J.rays) deposit_split_ray(J.V, J.F, fr, J.nrm, ray, st);
@@ -1844,7 +1842,8 @@ __device__ __forceinline__ void deposit_batch_phase(const BatchJob *__restrict__
 __global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
     closest_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
                          uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counter, uint32_t tile) {
-    closest_batch_phase(jobs, begin, n, total, *frame, counter, tile);
+    __shared__ lux::LeafScratch scratch[4];
+    closest_batch_phase(jobs, begin, n, total, *frame, counter, tile, &scratch[threadIdx.x >> 5]);
 }
 
 __global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__restrict__ jobs,
@@ -1861,7 +1860,8 @@ __global__ void __launch_bounds__(128) query_prefix_kernel(const BatchJob *__res
 __global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
     shadow_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *qbegin, uint32_t n, uint32_t *counter,
                         uint32_t tile) {
-    shadow_batch_phase(jobs, qbegin, n, counter, tile);
+    __shared__ lux::LeafScratch scratch[4];
+    shadow_batch_phase(jobs, qbegin, n, counter, tile, &scratch[threadIdx.x >> 5]);
 }
 
 __global__ void __launch_bounds__(128) deposit_batch_kernel(const BatchJob *__restrict__ jobs,
@@ -1931,14 +1931,16 @@ __global__ void __launch_bounds__(128, LUX_FUSED_MIN_BLOCKS)
     trace_batch_kernel(const BatchJob *__restrict__ jobs, const uint32_t *__restrict__ begin, uint32_t n,
                        uint32_t total, const uint32_t *__restrict__ frame, uint32_t *counters,
                        uint32_t *qbegin, GridBarrier B, uint32_t tile) {
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
     const uint32_t fr = *frame;
-    closest_batch_phase(jobs, begin, n, total, fr, counters, tile);
+    closest_batch_phase(jobs, begin, n, total, fr, counters, tile, L);
     if (!grid_sync(B, 1, jobs, n)) return;
     shade_batch_phase(jobs, begin, n, total, fr);
     if (!grid_sync(B, 2, jobs, n)) return;
     if (blockIdx.x == 0) query_prefix_block(jobs, n, qbegin);
     if (!grid_sync(B, 3, jobs, n)) return;
-    shadow_batch_phase(jobs, qbegin, n, counters + 1, tile);
+    shadow_batch_phase(jobs, qbegin, n, counters + 1, tile, L);
     if (!grid_sync(B, 4, jobs, n)) return;
     deposit_batch_phase(jobs, begin, n, total, fr);
 }
@@ -2267,6 +2269,8 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
     closest_cache_kernel(ViewDevice V, FrameParams F, SceneView S, const float4 *__restrict__ pos,
                          const float4 *__restrict__ nrm, uint32_t ray_count, CacheDevice C) {
     if (*V.error_flags) return;
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     uint32_t fallback_rays = 0;
@@ -2274,20 +2278,24 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
         uint32_t base = warp_fetch(&V.ts.work_counter[0]);
         if (base >= ray_count) break;
         uint32_t ray = base + (threadIdx.x & 31u);
-        if (ray < ray_count) {
+        const bool active = ray < ray_count;
+        bool validate = false, fallback = false, full = false;
+        f3 dir{0.0f, 0.0f, 0.0f}, origin{0.0f, 0.0f, 0.0f};
+        if (active) {
             uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
             float4 p4 = pos[i], n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
             unsigned long long key = receiver_key(F, p);
-            bool validate = cell_hash(key) % C.period == C.frame % C.period;
-            bool fallback = !validate && fallback_active(C, key);
-            bool full = validate || fallback;
-            f3 dir;
+            validate = cell_hash(key) % C.period == C.frame % C.period;
+            fallback = !validate && fallback_active(C, key);
+            full = validate || fallback;
             float u, v;
             split_direction(V, F, F.shade.frame, i, k, n, dir, u, v);
-            f3 origin = lux::ray_offset(p, n, F.shade.normal_bias);
-            lux::Hit hit;
-            lux::trace<false>(S, origin, dir, 0.0f, full ? 1e20f : C.near_limit, hit, cn);
+            origin = lux::ray_offset(p, n, F.shade.normal_bias);
+        }
+        lux::Hit hit;
+        lux::trace_warp<false>(S, active, origin, dir, 0.0f, full ? 1e20f : C.near_limit, hit, cn, L);
+        if (active) {
             uint8_t flag = kRayPlain;
             if (!full && hit.tri == lux::kEmpty) {
                 flag = kRayCached;
