@@ -1173,17 +1173,31 @@ def run_frames(args):
     d_rnrm = torch.from_numpy(w["rnrm"]).cuda()
     view.set_tuning(**tuning_of(START))
     view.set_timing(True)
+    warm = 0
+    if args.learned_frames:
+        bp = w["bp"]
+        cache = bp.LearnedCache(w["ctx"])
+        cache.set_bounds(w["rpos"][:, :3].min(0) - 1.0, w["rpos"][:, :3].max(0) + 1.0)
+        view.set_cache(cache, cutoff_level=args.cache_cutoff, validate_period=16, error_bound=args.cache_bound,
+                       train_samples=65536, fallback_frames=16)
+        warm = LEARNED_WARMUP
     stages = []
-    for step in range(args.warmup + args.steps):
+    for step in range(warm):
+        settings.frame_index = step
+        view.trace_merge(scene, settings, d_rpos.data_ptr(), d_rnrm.data_ptr(), len(w["rpos"]))
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("frames")  # the launches a capture may select (ncu --nvtx-include frames/)
+    for step in range(warm, warm + args.warmup + args.steps):
         settings.frame_index = step
         view.trace_merge(scene, settings, d_rpos.data_ptr(), d_rnrm.data_ptr(), len(w["rpos"]))
         torch.cuda.synchronize()
         t = view.timings()
-        if step >= args.warmup:
+        if step >= warm + args.warmup:
             stages.append((t.seed_ms, t.trace_ms, t.merge_ms, t.pack_ms))
+    torch.cuda.nvtx.range_pop()
     st = view.stats()
     m = np.median(np.array(stages), axis=0)
-    print(json.dumps({"profile": "frames-only", "width": WIDTH, "height": HEIGHT, "triangles": TRIANGLES,
+    print(json.dumps({"profile": "learned-frames" if args.learned_frames else "frames-only", "width": WIDTH, "height": HEIGHT, "triangles": TRIANGLES,
                       "tuning": tuning_of(START), "seed_ms": m[0], "trace_ms": m[1], "merge_ms": m[2], "pack_ms": m[3],
                       "cells": list(st.cells)[:settings.levels], "error_flags": int(st.error_flags)}))
 
@@ -1211,6 +1225,9 @@ def main():
     ap.add_argument("--frames-only", action="store_true",
                     help="profiling target: --warmup + --steps plain frames of the atrium workload with the "
                          "autotuner's starting tuning (no search, no other forms); prints the stage times")
+    ap.add_argument("--learned-frames", action="store_true",
+                    help="with --frames-only: learned-cache frames (cutoff --cache-cutoff) after the cache's "
+                         "warm-up frames")
     args = ap.parse_args()
     if args.small:
         global WIDTH, HEIGHT, TRIANGLES, EYE, TARGET
