@@ -363,6 +363,105 @@ struct Walker {
     // entry.  Returns true when the query is complete.
     // The stack lives outside the walker so the walker's fields stay in
     // registers; only the stack itself is addressed dynamically.
+    // One inner node of the descent: its child tests, the farther hit
+    // children pushed, the nearest taken.  Clears `have` at a dead end, an
+    // instance's step budget or a stack overflow (the ordered-scan
+    // fallback); returns true when the whole query is abandoned (the TLAS
+    // step budget).
+    __device__ __forceinline__ bool node_step(const SceneView &S, uint2 *stack, TraceCounters &cn) {
+        bool in_tlas = blas_base < 0;
+        uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
+        if (in_tlas)
+            tlas_steps = steps;
+        else
+            blas_steps = steps;
+        if (steps > kMaxSteps) {
+            hit.errors |= kQueryUnsupported;
+            if (in_tlas) return true;  // abandon the whole query
+            sp = blas_base;            // abandon this instance
+            have = false;
+            return false;
+        }
+        float entry[4];
+        uint32_t child[4];
+        cn.nodes++;
+        uint32_t mask = node_test(S.nodes, cur, r, hit.t, tmin, entry, child);
+        if (mask == 0u) {
+            have = false;
+            return false;
+        }
+        uint32_t k0 = child_key(mask, entry, 0), k1 = child_key(mask, entry, 1);
+        uint32_t k2 = child_key(mask, entry, 2), k3 = child_key(mask, entry, 3);
+        key_swap(k0, k1);
+        key_swap(k2, k3);
+        key_swap(k0, k2);
+        key_swap(k1, k3);
+        key_swap(k1, k2);
+        int n = __popc(mask);
+        if (sp + n - 1 > kDepth) {
+            if (in_tlas) {
+                hit.errors |= 2u;
+                sp = 0;
+                tlas_next = 0;
+            } else {
+                hit.errors |= 1u;
+                sp = blas_base;
+                blas_next = inst_first;
+            }
+            have = false;
+            return false;
+        }
+        if (n > 3) stack[sp++] = make_uint2(key_child(k3, child), k3 & ~3u);
+        if (n > 2) stack[sp++] = make_uint2(key_child(k2, child), k2 & ~3u);
+        if (n > 1) stack[sp++] = make_uint2(key_child(k1, child), k1 & ~3u);
+        cur = key_child(k0, child);
+        cur_t = key_entry(k0);
+        return false;
+    }
+
+    // A TLAS leaf (first, count): enter its first instance (the rest of the
+    // leaf waits on the stack).
+    __device__ __forceinline__ void enter_instance(const SceneView &S, uint2 *stack, TraceCounters &cn, uint32_t first,
+                                                   uint32_t count) {
+        // TLAS leaf: enter its first instance; the rest waits on the stack.
+        if (count > 1u) {
+            if (sp < kDepth) {
+                stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
+                                         as_uint(cur_t));
+            } else {
+                // Stack exhausted: after this instance, scan every instance.
+                hit.errors |= 2u;
+                sp = 0;
+                tlas_next = 0;
+            }
+        }
+        DeviceInstance I = load_instance(S.instances, first);
+        local_ray(I, o, d, lo, ld);
+        cn.instances++;
+        // A local direction bit-identical to the world direction
+        // (translation-only instances) keeps the world constants;
+        // only the origin moves.
+        rotated = !(as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) &&
+                    as_uint(ld.z) == as_uint(d.z));
+        if (rotated) {
+            r = slab_ray(lo, ld);
+            tri_ray = triangle_ray(ld);
+        } else {
+            r.ox = lo.x;
+            r.oy = lo.y;
+            r.oz = lo.z;
+        }
+        inst = first;
+        inst_flags = I.flags;
+        inst_first = I.first;
+        inst_count = I.count;
+        blas_base = sp;
+        blas_steps = 0;
+        cur = I.root;
+        cur_t = 0.0f;
+        have = true;
+    }
+
     // Inner nodes down to a leaf and that leaf's kind: a TLAS leaf enters its
     // first instance; a BLAS leaf within the step budget is returned as
     // (first, count) for its triangle tests (count 0: none).  Returns true
@@ -371,97 +470,14 @@ struct Walker {
                                             uint32_t &leaf_count) {
         leaf_first = 0;
         leaf_count = 0;
-        while (have && (cur & kLeafBit) == 0u) {
-            bool in_tlas = blas_base < 0;
-            uint32_t steps = (in_tlas ? tlas_steps : blas_steps) + 1u;
-            if (in_tlas)
-                tlas_steps = steps;
-            else
-                blas_steps = steps;
-            if (steps > kMaxSteps) {
-                hit.errors |= kQueryUnsupported;
-                if (in_tlas) return true;  // abandon the whole query
-                sp = blas_base;            // abandon this instance
-                have = false;
-                break;
-            }
-            float entry[4];
-            uint32_t child[4];
-            cn.nodes++;
-            uint32_t mask = node_test(S.nodes, cur, r, hit.t, tmin, entry, child);
-            if (mask == 0u) {
-                have = false;
-                break;
-            }
-            uint32_t k0 = child_key(mask, entry, 0), k1 = child_key(mask, entry, 1);
-            uint32_t k2 = child_key(mask, entry, 2), k3 = child_key(mask, entry, 3);
-            key_swap(k0, k1);
-            key_swap(k2, k3);
-            key_swap(k0, k2);
-            key_swap(k1, k3);
-            key_swap(k1, k2);
-            int n = __popc(mask);
-            if (sp + n - 1 > kDepth) {
-                if (in_tlas) {
-                    hit.errors |= 2u;
-                    sp = 0;
-                    tlas_next = 0;
-                } else {
-                    hit.errors |= 1u;
-                    sp = blas_base;
-                    blas_next = inst_first;
-                }
-                have = false;
-                break;
-            }
-            if (n > 3) stack[sp++] = make_uint2(key_child(k3, child), k3 & ~3u);
-            if (n > 2) stack[sp++] = make_uint2(key_child(k2, child), k2 & ~3u);
-            if (n > 1) stack[sp++] = make_uint2(key_child(k1, child), k1 & ~3u);
-            cur = key_child(k0, child);
-            cur_t = key_entry(k0);
-        }
+        while (have && (cur & kLeafBit) == 0u)
+            if (node_step(S, stack, cn)) return true;
         if (have) {
             uint32_t first = cur & kLeafFirstMask;
             uint32_t count = ((cur >> 27) & 15u) + 1u;
             have = false;
             if (blas_base < 0) {
-                // TLAS leaf: enter its first instance; the rest waits on the stack.
-                if (count > 1u) {
-                    if (sp < kDepth) {
-                        stack[sp++] = make_uint2(kLeafBit | ((first + 1u) & kLeafFirstMask) | ((count - 2u) << 27),
-                                                 as_uint(cur_t));
-                    } else {
-                        // Stack exhausted: after this instance, scan every instance.
-                        hit.errors |= 2u;
-                        sp = 0;
-                        tlas_next = 0;
-                    }
-                }
-                DeviceInstance I = load_instance(S.instances, first);
-                local_ray(I, o, d, lo, ld);
-                cn.instances++;
-                // A local direction bit-identical to the world direction
-                // (translation-only instances) keeps the world constants;
-                // only the origin moves.
-                rotated = !(as_uint(ld.x) == as_uint(d.x) && as_uint(ld.y) == as_uint(d.y) &&
-                            as_uint(ld.z) == as_uint(d.z));
-                if (rotated) {
-                    r = slab_ray(lo, ld);
-                    tri_ray = triangle_ray(ld);
-                } else {
-                    r.ox = lo.x;
-                    r.oy = lo.y;
-                    r.oz = lo.z;
-                }
-                inst = first;
-                inst_flags = I.flags;
-                inst_first = I.first;
-                inst_count = I.count;
-                blas_base = sp;
-                blas_steps = 0;
-                cur = I.root;
-                cur_t = 0.0f;
-                have = true;
+                enter_instance(S, stack, cn, first, count);
                 return false;
             }
             // BLAS leaf (traceTriangle / occludedTriangle).
