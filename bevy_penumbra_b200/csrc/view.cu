@@ -59,6 +59,10 @@
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
 #endif
+// Hit shading's register budget (resident 128-thread blocks per SM).
+#ifndef LUX_SHADE_MIN_BLOCKS
+#define LUX_SHADE_MIN_BLOCKS 1
+#endif
 // Whole-warp traversal in the persistent trace kernels: the BLAS leaves the
 // lanes reach in a step are tested by the whole warp.
 #ifndef LUX_WARP_LEAVES
@@ -790,7 +794,7 @@ __device__ __forceinline__ void shade_warp(const ViewDevice &V, const FrameParam
     }
 }
 
-__global__ void __launch_bounds__(128) shade_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t ray_count,
+__global__ void __launch_bounds__(128, LUX_SHADE_MIN_BLOCKS) shade_kernel(ViewDevice V, FrameParams F, SceneView S, uint32_t ray_count,
                                                     bool dense) {
     if (*V.error_flags) return;
     uint32_t rays = dense ? (uint32_t)min(total_entries(V, F), (unsigned long long)ray_count) : ray_count;
@@ -1846,7 +1850,7 @@ __global__ void __launch_bounds__(128, LUX_BATCH_MIN_BLOCKS)
     closest_batch_phase(jobs, begin, n, total, *frame, counter, tile, &scratch[threadIdx.x >> 5]);
 }
 
-__global__ void __launch_bounds__(128) shade_batch_kernel(const BatchJob *__restrict__ jobs,
+__global__ void __launch_bounds__(128, LUX_SHADE_MIN_BLOCKS) shade_batch_kernel(const BatchJob *__restrict__ jobs,
                                                           const uint32_t *__restrict__ begin, uint32_t n,
                                                           uint32_t total, const uint32_t *__restrict__ frame) {
     shade_batch_phase(jobs, begin, n, total, *frame);
