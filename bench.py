@@ -49,16 +49,16 @@ LEARNED_WARMUP = 200
 # Kernels of one plain Split frame with world history: clear, 3 seed, the
 # sample-sequence sort (radix-sort histogram, exclusive sum, 8 one-sweep passes
 # over 62-bit keys, ordinal), 3 retain, layout, clear entries, closest, shade,
-# shadow, deposit, pack; then per level a history map and a merge and per level
-# but the last a corners pass; 4 more when visibility queries are sorted
-# (histogram, scan init and scan, scatter).
-LAUNCHES_PER_FRAME_FIXED = 25
+# shadow, deposit, the corners and history maps of every level, pack; then a
+# merge per level; 4 more when visibility queries are sorted (histogram, scan
+# init and scan, scatter).
+LAUNCHES_PER_FRAME_FIXED = 26
 
 
 def launches_per_frame(levels: int, sort_queries: bool, sort_rays: bool = False) -> int:
     """Kernels of one plain frame; sorting the interval rays adds the key
     pass to the four counting-sort launches."""
-    return LAUNCHES_PER_FRAME_FIXED + 3 * levels - 1 + (4 if sort_queries else 0) + (5 if sort_rays else 0)
+    return LAUNCHES_PER_FRAME_FIXED + levels + (4 if sort_queries else 0) + (5 if sort_rays else 0)
 
 
 def settings_for_workload(sanitize: bool = True):

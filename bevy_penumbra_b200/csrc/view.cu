@@ -59,9 +59,10 @@
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
 #endif
-// Hit shading's register budget (resident 128-thread blocks per SM).
+// Hit shading's register budget (resident 128-thread blocks per SM): 80
+// registers with a few spills measured faster than 112 without.
 #ifndef LUX_SHADE_MIN_BLOCKS
-#define LUX_SHADE_MIN_BLOCKS 1
+#define LUX_SHADE_MIN_BLOCKS 6
 #endif
 // Whole-warp traversal in the persistent trace kernels: the BLAS leaves the
 // lanes reach in a step are tested by the whole warp.
@@ -3083,7 +3084,14 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
     FrameParams F;
     lux_status ps = make_params(v, settings, rc->count, F);
     if (ps != LUX_OK) return ps;
-    if (v->cache_alloc && v->cache.cutoff_level < F.levels) F.lod_enabled = 0;  // learned-cache frames: LOD 0
+    if (v->cache_alloc && v->cache.cutoff_level < F.levels) {
+        // Learned-cache frames: LOD 0, and no level past the cutoff: every
+        // ray's light from beyond the cutoff (the cache's answer, or the
+        // traced hit of a validated or fallback ray) ends at level `cutoff`,
+        // which then takes the whole tail like a last level.
+        F.lod_enabled = 0;
+        F.levels = v->cache.cutoff_level + 1u;
+    }
     if (F.layout == LUX_LAYOUT_SPLIT && (uint64_t)rc->count * F.rays_per_receiver > v->desc.max_rays)
         return lux_fail(ctx, LUX_ERR_CAPACITY, "trace_merge: receivers x rays_per_receiver exceeds max_rays");
     if (F.layout == LUX_LAYOUT_SPLIT && (v->tuning.sort_rays || v->tuning.sort_queries)) {

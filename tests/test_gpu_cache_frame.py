@@ -42,10 +42,11 @@ def test_cache_frames_run_and_train():
     assert cache.stats().steps == 24 * 2
     assert cs.cached_rays > 0.3 * st.interval_rays
     # Records exist at every level up to the cutoff and the cutoff level is
-    # answered (levels past it get no deposits from cached rays).
+    # answered; no level past it is built (the cutoff level takes the tail).
     levels = [view.read_level(l) for l in range(3)]
     assert all(len(k) > 0 for k, _, _, _ in levels)
     assert levels[2][3].sum() > 0
+    assert len(view.read_level(3)[0]) == 0
 
 
 def test_cutoff_past_last_level_is_plain():
