@@ -742,9 +742,11 @@ __device__ void trace_warp(const SceneView &S, bool active, f3 o, f3 d, float tm
 // warp takes that many new rays from `counter` (one atomic per refill) and
 // keeps stepping until the counter passes `n` and every lane is done.
 // gen(id, o, d, tmin, limit) produces ray `id`; done(id, hit) consumes it.
+// With a leaf scratch (L), the warp's walks step together and the leaves of
+// each round are tested by the whole warp (Walker::step_warp).
 template <bool kAnyHit, typename Gen, typename Done>
 __device__ void trace_persistent(const SceneView &S, uint32_t *counter, uint32_t n, Gen &&gen, Done &&done,
-                                 TraceCounters &cn) {
+                                 TraceCounters &cn, LeafScratch *L = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     Walker<kAnyHit> w;
     uint2 stack[kStack];
@@ -774,7 +776,8 @@ __device__ void trace_persistent(const SceneView &S, uint32_t *counter, uint32_t
             if (exhausted) break;
             continue;
         }
-        if (active && w.step(S, stack, cn)) {
+        const bool complete = L ? w.step_warp(S, stack, cn, L, active) : (active && w.step(S, stack, cn));
+        if (active && complete) {
             done(id, w.hit);
             active = false;
         }

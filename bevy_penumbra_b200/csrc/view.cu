@@ -512,6 +512,12 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
                                                             const float4 *__restrict__ pos,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
     if (*V.error_flags) return;
+#if LUX_WARP_LEAVES
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
+#else
+    lux::LeafScratch *L = nullptr;
+#endif
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
     lux::trace_persistent<false>(
@@ -536,7 +542,7 @@ __global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V,
             V.ts.ray_h[ray] = make_uint4(h.tri, h.inst, h.errors, lux::as_uint(h.b2));
             st[kStatInterval] += 1;
         },
-        cn);
+        cn, L);
     st[kStatNodes] = cn.nodes;
     st[kStatTris] = cn.triangles;
     st[kStatInst] = cn.instances;
@@ -807,6 +813,12 @@ __global__ void __launch_bounds__(128, LUX_SHADE_MIN_BLOCKS) shade_kernel(ViewDe
 // result: 0 visible, 1 blocked, 2 unsupported.
 __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
+#if LUX_WARP_LEAVES
+    __shared__ lux::LeafScratch scratch[4];
+    lux::LeafScratch *L = &scratch[threadIdx.x >> 5];
+#else
+    lux::LeafScratch *L = nullptr;
+#endif
     uint32_t n = min(*V.ts.queue_count, F.queue_capacity);
     unsigned long long st[7] = {0, 0, 0, 0, 0, 0, 0};
     lux::TraceCounters cn{0, 0, 0};
@@ -825,7 +837,7 @@ __global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameP
             V.ts.queue_result[qi] = sh.tri != lux::kEmpty ? 1 : ((sh.errors & lux::kQueryUnsupported) ? 2 : 0);
             st[kStatShadow] += 1;
         },
-        cn);
+        cn, L);
     st[kStatNodes] = cn.nodes;
     st[kStatTris] = cn.triangles;
     st[kStatInst] = cn.instances;

@@ -118,15 +118,19 @@ def cornell_floor_receivers(n=32):
     return pos, nrm
 
 
-@pytest.mark.parametrize("rays,sort,depth,tile", [(1, 0, 64, 32), (8, 0, 64, 32), (8, 1, 64, 32), (8, 1, 32, 32),
-                                                   (8, 0, 64, 128), (8, 1, 64, 256)])
-def test_split_cornell_frame_matches_oracle(rays, sort, depth, tile):
+@pytest.mark.parametrize("rays,sort,depth,tile,mode", [(1, 0, 64, 32, 0), (8, 0, 64, 32, 0), (8, 1, 64, 32, 0),
+                                                        (8, 1, 32, 32, 0), (8, 0, 64, 128, 0), (8, 1, 64, 256, 0),
+                                                        (8, 0, 64, 32, 1), (8, 1, 64, 32, 1)])
+def test_split_cornell_frame_matches_oracle(rays, sort, depth, tile, mode):
+    """mode 1: the refill schedulers (a lane takes a new ray as soon as its
+    walk ends) for both trace passes."""
     settings = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=rays,
                                    frame_index=3).sanitized()
     pos, nrm = cornell_floor_receivers()
     ctx, scene, view, st, levels, (pkeys, tables) = run_frame("cornell", settings, pos, nrm,
                                                               tuning=dict(sort_rays=sort, sort_queries=sort,
-                                                                          stack_depth=depth, tile_rays=tile))
+                                                                          stack_depth=depth, tile_rays=tile,
+                                                                          closest_mode=mode, shadow_mode=mode))
     ofr = oracle_frame("cornell", settings, pos, nrm)
     ost = ofr.stats()
     assert st.interval_rays == len(pos) * rays
