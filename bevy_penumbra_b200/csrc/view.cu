@@ -2298,9 +2298,11 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
         const bool active = ray < ray_count;
         bool validate = false, fallback = false, full = false;
         f3 dir{0.0f, 0.0f, 0.0f}, origin{0.0f, 0.0f, 0.0f};
+        float4 n4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (active) {
             uint32_t i = ray / F.rays_per_receiver, k = ray % F.rays_per_receiver;
-            float4 p4 = pos[i], n4 = nrm[i];
+            float4 p4 = pos[i];
+            n4 = nrm[i];
             f3 p{p4.x, p4.y, p4.z}, n{n4.x, n4.y, n4.z};
             unsigned long long key = receiver_key(F, p);
             validate = cell_hash(key) % C.period == C.frame % C.period;
@@ -2312,8 +2314,8 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
         }
         lux::Hit hit;
         lux::trace_warp<false>(S, active, origin, dir, 0.0f, full ? 1e20f : C.near_limit, hit, cn, L);
+        uint8_t flag = kRayPlain;
         if (active) {
-            uint8_t flag = kRayPlain;
             if (!full && hit.tri == lux::kEmpty) {
                 flag = kRayCached;
                 hit.t = C.far_t;
@@ -2325,6 +2327,35 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
             store_ray(V, ray, origin, dir, hit);
             st[kStatInterval] += 1;
         }
+        // The cache query of every cached or validated ray, keyed by its
+        // origin and direction at its receiver's normal (albedo unknown:
+        // zero), appended to the compact query list one atomic per warp.
+        const bool want = active && flag != kRayPlain;
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t mask = __ballot_sync(0xffffffffu, want);
+        uint32_t first = 0;
+        if (lane == 0 && mask) first = atomicAdd(&C.counters[kCntQueries], (uint32_t)__popc(mask));
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (want) {
+            const uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
+            LuxCacheSample q;
+            q.position[0] = origin.x;
+            q.position[1] = origin.y;
+            q.position[2] = origin.z;
+            q.weight = 1.0f;
+            q.direction[0] = dir.x;
+            q.direction[1] = dir.y;
+            q.direction[2] = dir.z;
+            q.pad0 = 0.0f;
+            q.normal[0] = n4.x;
+            q.normal[1] = n4.y;
+            q.normal[2] = n4.z;
+            q.pad1 = 0.0f;
+            q.albedo[0] = q.albedo[1] = q.albedo[2] = 0.0f;
+            q.pad2 = 0.0f;
+            C.queries[slot] = q;
+            C.query_ray[slot] = ray;
+        }
     }
     st[kStatNodes] = cn.nodes;
     st[kStatTris] = cn.triangles;
@@ -2332,41 +2363,6 @@ __global__ void __launch_bounds__(128, LUX_CLOSEST_MIN_BLOCKS)
     add_stats(V.stats, st);
     for (int off = 16; off > 0; off >>= 1) fallback_rays += __shfl_down_sync(0xffffffffu, fallback_rays, off);
     if ((threadIdx.x & 31u) == 0u && fallback_rays) atomicAdd(&C.counters[kCntFallbackRays], fallback_rays);
-}
-
-// Compacted cache queries: every cached or validated ray, keyed by its
-// origin and direction at its receiver's normal (albedo unknown: zero).
-__global__ void cache_queries_kernel(ViewDevice V, const float4 *__restrict__ nrm, uint32_t ray_count,
-                                     uint32_t rays_per_receiver, CacheDevice C) {
-    const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t base = blockIdx.x * blockDim.x; base < ray_count; base += gridDim.x * blockDim.x) {
-        uint32_t ray = base + threadIdx.x;
-        bool want = ray < ray_count && C.flags[ray] != kRayPlain;
-        uint32_t mask = __ballot_sync(0xffffffffu, want);
-        uint32_t first = 0;
-        if (lane == 0 && mask) first = atomicAdd(&C.counters[kCntQueries], (uint32_t)__popc(mask));
-        first = __shfl_sync(0xffffffffu, first, 0);
-        if (!want) continue;
-        uint32_t slot = first + (uint32_t)__popc(mask & ((1u << lane) - 1u));
-        float4 o = V.ts.ray_o[ray], d = V.ts.ray_d[ray], n = nrm[ray / rays_per_receiver];
-        LuxCacheSample q;
-        q.position[0] = o.x;
-        q.position[1] = o.y;
-        q.position[2] = o.z;
-        q.weight = 1.0f;
-        q.direction[0] = d.x;
-        q.direction[1] = d.y;
-        q.direction[2] = d.z;
-        q.pad0 = 0.0f;
-        q.normal[0] = n.x;
-        q.normal[1] = n.y;
-        q.normal[2] = n.z;
-        q.pad1 = 0.0f;
-        q.albedo[0] = q.albedo[1] = q.albedo[2] = 0.0f;
-        q.pad2 = 0.0f;
-        C.queries[slot] = q;
-        C.query_ray[slot] = ray;
-    }
 }
 
 // Cached rays take the prediction as their hit radiance (no next-event
@@ -3211,7 +3207,6 @@ static lux_status view_frame(LuxView *v, const LuxScene *scene, const LuxSetting
                                                                                          tile_of(T));
             if (cached) {
                 const int g = ctx->sm_count * 8;
-                cache_queries_kernel<<<g, 256, 0, st>>>(D, nrm, rays, F.rays_per_receiver, C);
                 lux_status qrc = lux_cache_query_device_count(v->cache.cache, C.queries, C.counters + kCntQueries, rays,
                                                               (float *)C.pred);
                 if (qrc != LUX_OK) return qrc;
