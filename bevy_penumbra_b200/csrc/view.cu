@@ -56,8 +56,17 @@
 #ifndef LUX_MERGE_MIN_BLOCKS
 #define LUX_MERGE_MIN_BLOCKS 4
 #endif
+// The merge reads a record's sum together with its sample count (a record
+// without samples reads 16 bytes it does not use, but the two loads overlap).
+#ifndef LUX_MERGE_EAGER_SUM
+#define LUX_MERGE_EAGER_SUM 0
+#endif
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
+#endif
+// The refill schedulers' register budget (resident 128-thread blocks per SM).
+#ifndef LUX_REFILL_MIN_BLOCKS
+#define LUX_REFILL_MIN_BLOCKS 1
 #endif
 // Hit shading's register budget (resident 128-thread blocks per SM): 80
 // registers with a few spills measured faster than 112 without.
@@ -508,7 +517,7 @@ __device__ __forceinline__ void load_ray(const ViewDevice &V, uint32_t ray, f3 &
 }
 
 // Persistent warps with per-lane refill (lux::trace_persistent).
-__global__ void __launch_bounds__(128) closest_split_refill_kernel(ViewDevice V, FrameParams F, SceneView S,
+__global__ void __launch_bounds__(128, LUX_REFILL_MIN_BLOCKS) closest_split_refill_kernel(ViewDevice V, FrameParams F, SceneView S,
                                                             const float4 *__restrict__ pos,
                                                             const float4 *__restrict__ nrm, uint32_t ray_count) {
     if (*V.error_flags) return;
@@ -811,7 +820,7 @@ __global__ void __launch_bounds__(128, LUX_SHADE_MIN_BLOCKS) shade_kernel(ViewDe
 
 // Visibility queries, one per lane (traceVisibility, shaders/split.slang:1326-1339).
 // result: 0 visible, 1 blocked, 2 unsupported.
-__global__ void __launch_bounds__(128) shadow_refill_kernel(ViewDevice V, FrameParams F, SceneView S) {
+__global__ void __launch_bounds__(128, LUX_REFILL_MIN_BLOCKS) shadow_refill_kernel(ViewDevice V, FrameParams F, SceneView S) {
     if (*V.error_flags) return;
 #if LUX_WARP_LEAVES
     __shared__ lux::LeafScratch scratch[4];
@@ -1319,9 +1328,16 @@ __device__ __forceinline__ bool merge_own(const ViewDevice &V, const FrameParams
     const float jb = F.radiance_blend, tb = F.transmittance_blend;
     const float jlimit = 1.0f / (1.0f - jb), tlimit = 1.0f / (1.0f - tb);
     uint32_t cnt = V.count[base + e];
+#if LUX_MERGE_EAGER_SUM
+    const float4 acc_loaded = V.accum[base + e];  // issued with the count, not after it
+#endif
     float4 fresh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     if (cnt) {
+#if LUX_MERGE_EAGER_SUM
+        const float4 acc = acc_loaded;
+#else
         float4 acc = V.accum[base + e];
+#endif
         float fn = (float)cnt;
         fresh = make_float4(acc.x / fn, acc.y / fn, acc.z / fn, acc.w / fn);
     }
