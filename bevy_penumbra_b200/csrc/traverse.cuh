@@ -723,12 +723,13 @@ __device__ void trace(const SceneView &S, f3 o, f3 d, float tmin, float limit, H
 
 // trace() for a whole warp: every lane of the warp calls it (active: the
 // lane has a query), and the BLAS leaves reached in each round are tested
-// by the whole warp (Walker::leaf_pass).  A lane without a query returns an
-// undefined hit.
+// by the whole warp (Walker::leaf_pass).  A lane without a query returns no
+// hit.
 template <bool kAnyHit, int kDepth = kStack>
 __device__ void trace_warp(const SceneView &S, bool active, f3 o, f3 d, float tmin, float limit, Hit &hit,
                            TraceCounters &cn, LeafScratch *L) {
     Walker<kAnyHit, kDepth> w;
+    w.hit = Hit{limit, kEmpty, kEmpty, 0u, 0.0f, 0.0f};
     uint2 stack[kDepth];
     bool alive = active && w.start(S, o, d, tmin, limit);
     while (__any_sync(0xffffffffu, alive)) {
