@@ -752,6 +752,11 @@ def run_ours(args, rank, world):
                      + int(st.instances_visited) * 64)
         trace_s = float(np.median(trace_ms)) * 1e-3
         achieved = alg_bytes / trace_s / 1e9
+        # The traversal's scene stays in L2: its bytes are also set against the
+        # device's L2 read rate (32 MiB read 256 times in one launch) and the
+        # HBM read rate of the same launch over 2 GiB, both measured here.
+        l2_gbs = bp.measure_read_rate(ctx, 32 << 20, 256)
+        hbm_read_gbs = bp.measure_read_rate(ctx, 2 << 30, 4)
         cpu = cpu_sample(w, CPU_STRIDE, os.cpu_count() or 1)
         line = {
             "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
@@ -779,6 +784,11 @@ def run_ours(args, rank, world):
                          "traffic_note": "ncu dram bytes of the traversal kernels per frame, scaled by rays from "
                                          "the 65,536-triangle capture; the scene stays in L2",
                          "algorithmic_bytes": alg_bytes},
+            "roofline_l2": {"kernel": "trace stage (closest_split_kernel, shade, shadow_kernel, deposit)",
+                            "bound": "l2", "achieved": achieved, "peak": l2_gbs, "peak_kind": "measured in this run",
+                            "unit": "GB/s", "frac": achieved / l2_gbs, "hbm_read_gbs": hbm_read_gbs,
+                            "probe": "lux_measure_read_rate: 16-byte L1-bypassing loads, 32 MiB x 256 passes "
+                                     "(L2) and 2 GiB x 4 passes (HBM), shortest of five launches"},
             "merge_roofline": merge_roofline(settings, st, float(np.median(merge_ms)), peak, peak_kind),
             "cpu_baseline": {"value": cpu["rays"] / cpu["seconds"] / 1e6, "unit": "Mrays/s",
                              "cores": os.cpu_count(), "kind": "port",

@@ -29,7 +29,7 @@ from ._native import LuxError, check, lib
 
 __all__ = [
     "SamplingSettings", "RadianceCascades", "RadianceCascadesPlugin", "RadianceCascadesStatus",
-    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance", "reference_irradiance", "error_stats", "LearnedCache", "CACHE_SAMPLE_DTYPE",
+    "LuxContext", "PackedScene", "GpuScene", "SplitView", "Batch", "LuxError", "trace_rays", "interval_radiance", "reference_irradiance", "error_stats", "measure_read_rate", "LearnedCache", "CACHE_SAMPLE_DTYPE",
     "LAYOUT_SPLIT", "LAYOUT_DENSE", "INTERVAL_ENDS_GEOMETRIC", "INTERVAL_LENGTHS_GEOMETRIC",
 ]
 
@@ -442,6 +442,14 @@ def error_stats(ctx: LuxContext, estimate_ptr: int, reference_ptr: int, count: i
     mean = ref_sum / n
     return {"rmse": rmse, "mean_reference": mean, "relative_rmse": rmse / mean if mean > 0 else float("inf"),
             "points": int(used), "max_abs_error": mx}
+
+
+def measure_read_rate(ctx: LuxContext, nbytes: int, passes: int) -> float:
+    """lux_measure_read_rate: GB/s of one launch reading a device buffer of
+    `nbytes` bytes `passes` times (inside L2: the L2 read rate)."""
+    out = C.c_double(0.0)
+    ctx.check(lib().lux_measure_read_rate(ctx.handle, int(nbytes), int(passes), C.byref(out)))
+    return float(out.value)
 
 
 def camera_struct(clip_from_world, position, viewport_height: int, target_pixels: int = 1) -> N.LuxCamera:

@@ -200,6 +200,7 @@ SIGNATURES = {
     "lux_reference_round_samples": (U32, [U32, U32]),
     "lux_reference_irradiance": (C.c_int, [P, P, C.POINTER(LuxSettings), P, P, U32, U32, U32, P]),
     "lux_error_stats": (C.c_int, [P, P, P, U32, C.POINTER(C.c_double)]),
+    "lux_measure_read_rate": (C.c_int, [P, C.c_uint64, U32, C.POINTER(C.c_double)]),
     "lux_path_reference": (C.c_int, [P, P, C.POINTER(LuxSettings), P, P, U32, U32, U32, U32, P]),
     "lux_cache_desc_default": (None, [C.POINTER(LuxCacheDesc)]),
     "lux_cache_create": (C.c_int, [P, C.POINTER(LuxCacheDesc), C.POINTER(P)]),

@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "liblux.so")
 
-SOURCES = ["context.cpp", "scene_pack.cpp", "scene.cu", "view.cu", "cache.cu", "screen.cu", "pathtrace.cu"]
+SOURCES = ["context.cpp", "scene_pack.cpp", "scene.cu", "view.cu", "cache.cu", "screen.cu", "pathtrace.cu", "rate.cu"]
 HEADERS = ["lux_internal.h", "lux_math.cuh", "traverse.cuh", "shade.cuh",
            os.path.join("..", "..", "include", "lux.h")]
 

@@ -478,6 +478,16 @@ lux_status lux_path_reference(LuxContext *ctx, const LuxScene *scene, const LuxS
  * (out[1] / (3 out[2])).  Synchronises the context stream. */
 lux_status lux_error_stats(LuxContext *ctx, const float *estimate, const double *reference, uint32_t count,
                            double out[4]);
+/* Measured read rate of the context's device (no reference counterpart; the
+ * denominator of the traversal roofline): one launch reads a device buffer
+ * of `bytes` bytes (a multiple of 16 in [1 MiB, 64 GiB]) `passes` times
+ * (1..4096) with 16-byte loads that bypass L1; the shortest of five timed
+ * launches after a warm-up.  A buffer well inside L2 (126 MB on B200) gives
+ * the L2 read rate, the bound of the traversal kernels, whose scene stays in
+ * L2; one well above it gives the HBM read rate.  *gb_per_s = bytes x passes
+ * / time / 1e9.  Allocates and frees the buffer; synchronises the context
+ * stream. */
+lux_status lux_measure_read_rate(LuxContext *ctx, uint64_t bytes, uint32_t passes, double *gb_per_s);
 
 /* ---- learned radiance cache ------------------------------------------------
  * No reference counterpart (the reference's README defers neural caching).

@@ -92,3 +92,14 @@ def test_screen_filter_ragged_extent():
         ctx.synchronize()
         np.testing.assert_allclose(from_device(out, np.float32, (H, W, 4)), o_out, rtol=1e-5, atol=1e-6)
         prev_clip = clip
+
+
+def test_read_rate_probe_reports_l2_above_hbm_and_rejects_bad_sizes():
+    ctx = bp.LuxContext()
+    l2 = bp.measure_read_rate(ctx, 32 << 20, 64)
+    hbm = bp.measure_read_rate(ctx, 1 << 30, 2)
+    assert np.isfinite(l2) and np.isfinite(hbm) and hbm > 100.0
+    assert l2 > hbm
+    for nbytes, passes in ((1 << 10, 1), ((32 << 20) + 8, 1), (32 << 20, 0), (32 << 20, 5000)):
+        with pytest.raises(bp.LuxError):
+            bp.measure_read_rate(ctx, nbytes, passes)
