@@ -101,7 +101,8 @@ def merge_roofline(settings, st, merge_ms, peak, peak_kind):
     cells = list(st.cells)[:settings.levels]
     nbytes = merge_compulsory_bytes(settings, cells, history)
     achieved = nbytes / (merge_ms * 1e-3) / 1e9
-    return {"kernel": "merge stage (merge_prep_kernel: corners and history maps of every level, merge_kernel per level)", "bound": "hbm",
+    return {"kernel": ("merge stage (merge_prep_kernel: corners and history maps of every level; merge_own_kernel: the "
+                       "own part of every record of every level; merge_children_kernel per level below the coarsest)"), "bound": "hbm",
             "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
             "compulsory_bytes": nbytes, "ms": merge_ms,
             "records": sum(int(c) * direction_count(settings, l) for l, c in enumerate(cells))}

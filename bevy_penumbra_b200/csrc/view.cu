@@ -1458,15 +1458,6 @@ __device__ __forceinline__ void merge_finish(const ViewDevice &V, const FramePar
     V.merged[base + e] = out;
 }
 
-__device__ __forceinline__ void merge_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
-                                             uint32_t level, unsigned long long base, uint32_t dirs, uint32_t cell,
-                                             uint32_t d) {
-    MergeOwn own;
-    const bool children = merge_own(V, F, H, level, base, dirs, cell, d, own);
-    merge_finish(V, F, level, base, dirs, cell, d, own, children);
-}
-
-
 // Processing order of a level's records: item i of cells x dirs is record
 // (cell, d) taken in direction blocks of kMergeRun consecutive directions,
 // every cell's run of a block before the next block.  A warp still covers
@@ -1498,8 +1489,58 @@ __device__ __forceinline__ void merge_item(unsigned long long i, uint32_t cells,
     }
 }
 
+// The merge in two passes.  A record's own part (fresh mean, history blend,
+// raw and mass records) does not depend on the children, so one launch takes
+// it for the records of every level at once, in storage order, and finishes
+// the records whose merged value needs no children (no transmittance, or the
+// coarsest level).  Then, coarsest level first, one launch per level takes
+// the records that pass light on: their own part is read back from the raw
+// and mass records just written (transmittance = saturate(beta) when the
+// transmittance mass is positive; support = 1 - transmittance when the
+// radiance mass is positive too; the radiance is the raw record's), which
+// gives exactly the values merge_own returned, and adds the children.
+__device__ __forceinline__ void merge_own_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                                 unsigned long long e) {
+    uint32_t level = 0;
+    while (level + 1u < F.levels && e >= V.level_base[level + 1u]) ++level;
+    const unsigned long long base = V.level_base[level];
+    const uint32_t dirs = F.dirs[level];
+    const unsigned long long r = e - base;
+    const uint32_t cell = (uint32_t)(r / dirs), d = (uint32_t)(r - (unsigned long long)cell * dirs);
+    MergeOwn own;
+    if (!merge_own(V, F, H, level, base, dirs, cell, d, own)) merge_finish(V, F, level, base, dirs, cell, d, own, false);
+}
+
+__device__ __forceinline__ void merge_children_record(const ViewDevice &V, const FrameParams &F, uint32_t level,
+                                                      unsigned long long base, uint32_t dirs, uint32_t cell,
+                                                      uint32_t d) {
+    const unsigned long long e = base + (unsigned long long)cell * dirs + d;
+    const float2 mass = V.mass[e];
+    if (!(mass.y > 0.0f)) return;  // no transmittance: finished by the own pass
+    const float4 raw = V.raw[e];
+    const float transmittance = lux::saturate(raw.w);
+    if (!(transmittance > 0.0f)) return;
+    const float support = mass.x > 0.0f ? 1.0f - transmittance : 0.0f;
+    MergeOwn own{0.0f, 0.0f, 0.0f, support, transmittance};
+    if (support > 0.0f) {
+        own.rx = raw.x;
+        own.ry = raw.y;
+        own.rz = raw.z;
+    }
+    merge_finish(V, F, level, base, dirs, cell, d, own, true);
+}
+
+__global__ void __launch_bounds__(256) merge_own_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
+    if (*V.error_flags) return;
+    const unsigned long long n = V.level_base[F.levels - 1u] +
+                                 (unsigned long long)V.cell_count[F.levels - 1u] * F.dirs[F.levels - 1u];
+    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
+         e += (unsigned long long)gridDim.x * blockDim.x)
+        merge_own_record(V, F, H, e);
+}
+
 __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
-    merge_kernel(ViewDevice V, FrameParams F, HistoryDevice H, uint32_t level) {
+    merge_children_kernel(ViewDevice V, FrameParams F, uint32_t level) {
     if (*V.error_flags) return;
     const uint32_t dirs = F.dirs[level], cells = V.cell_count[level];
     const unsigned long long n = (unsigned long long)cells * dirs;
@@ -1508,7 +1549,7 @@ __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
          i += (unsigned long long)gridDim.x * blockDim.x) {
         uint32_t cell, d;
         merge_item(i, cells, dirs, cell, d);
-        merge_record(V, F, H, level, base, dirs, cell, d);
+        merge_children_record(V, F, level, base, dirs, cell, d);
     }
 }
 
@@ -2164,18 +2205,29 @@ __global__ void batch_merge_prep_kernel(const BatchJob *__restrict__ jobs, const
     }
 }
 
-__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS) batch_merge_kernel(const BatchJob *__restrict__ jobs,
-                                                          const unsigned long long *__restrict__ dom, uint32_t n,
-                                                          const unsigned long long *__restrict__ count,
-                                                          uint32_t level) {
+// The two-pass merge over all jobs: the own part of every record of every
+// level, then per level the records that pass light on.
+__global__ void __launch_bounds__(256) batch_merge_own_kernel(const BatchJob *__restrict__ jobs,
+                                                              const unsigned long long *__restrict__ dom, uint32_t n,
+                                                              const unsigned long long *__restrict__ count) {
+    for_batch_items(batch_row(dom, n, kRowEntries), n, [&](uint32_t j, unsigned long long e) {
+        const BatchJob &J = jobs[j];
+        if (e >= count[j] || *J.V.error_flags) return;
+        merge_own_record(J.V, J.F, J.H, e);
+    });
+}
+
+__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
+    batch_merge_children_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                uint32_t n, const unsigned long long *__restrict__ count, uint32_t level) {
     const unsigned long long *records = count + (size_t)(kRowRecords - kRowEntries + level) * n;
     for_batch_items(batch_row(dom, n, kRowRecords + level), n, [&](uint32_t j, unsigned long long e) {
         const BatchJob &J = jobs[j];
-        if (e >= records[j] || *J.V.error_flags) return;
+        if (e >= records[j] || level + 1u >= J.F.levels || *J.V.error_flags) return;
         const uint32_t dirs = J.F.dirs[level];
         uint32_t cell, d;
         merge_item(e, J.V.cell_count[level], dirs, cell, d);
-        merge_record(J.V, J.F, J.H, level, J.V.level_base[level], dirs, cell, d);
+        merge_children_record(J.V, J.F, level, J.V.level_base[level], dirs, cell, d);
     });
 }
 
@@ -2886,8 +2938,9 @@ static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     const int grid = v->ctx->sm_count * 8;
     const HistoryDevice H = history_device(v);
     if (F.levels > 1 || F.history) merge_prep_kernel<<<grid, 128, 0, st>>>(D, F, H);
-    for (int l = (int)F.levels - 1; l >= 0; --l)
-        merge_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F, H, (uint32_t)l);
+    merge_own_kernel<<<grid * 2, 256, 0, st>>>(D, F, H);
+    for (int l = (int)F.levels - 2; l >= 0; --l)
+        merge_children_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F, (uint32_t)l);
 }
 
 // Start of an unbatched frame: the last frame's records become the history
@@ -3896,9 +3949,10 @@ static void batch_enqueue(LuxBatch *b, cudaStream_t st) {
     }
     if (b->levels > 1 || b->history)
         batch_merge_prep_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, b->levels);
-    for (int l = (int)b->levels - 1; l >= 0; --l)
-        batch_merge_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(b->d_jobs, b->d_dom, n,
-                                                                                     b->d_count, (uint32_t)l);
+    batch_merge_own_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
+    for (int l = (int)b->levels - 2; l >= 0; --l)
+        batch_merge_children_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(
+            b->d_jobs, b->d_dom, n, b->d_count, (uint32_t)l);
     batch_pack_kernel<<<grid, 64, (size_t)b->max_dirs0 * 2 * sizeof(float4), st>>>(b->d_jobs, b->d_dom, n,
                                                                                  b->d_count, b->max_dirs0);
 }
