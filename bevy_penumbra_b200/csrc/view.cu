@@ -37,12 +37,13 @@
 
 // Resident 128-thread blocks per SM the trace kernels are compiled for: the
 // register cap that trades walker state kept in registers against warps in
-// flight (6 blocks = 80 registers per thread).
+// flight (6 blocks = 80 registers per thread, 7 = 72).  The visibility walk
+// keeps no child order, so it fits 7.
 #ifndef LUX_CLOSEST_MIN_BLOCKS
 #define LUX_CLOSEST_MIN_BLOCKS 6
 #endif
 #ifndef LUX_SHADOW_MIN_BLOCKS
-#define LUX_SHADOW_MIN_BLOCKS 6
+#define LUX_SHADOW_MIN_BLOCKS 7
 #endif
 // The batched trace kernels keep a job's scene pointers per warp as well.
 #ifndef LUX_BATCH_MIN_BLOCKS
@@ -55,6 +56,11 @@
 #endif
 #ifndef LUX_MERGE_MIN_BLOCKS
 #define LUX_MERGE_MIN_BLOCKS 4
+#endif
+// The own pass (every record of every level, no children): 256-thread
+// blocks, register budget for this many resident per SM.
+#ifndef LUX_MERGE_OWN_MIN_BLOCKS
+#define LUX_MERGE_OWN_MIN_BLOCKS 8
 #endif
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
@@ -1499,16 +1505,40 @@ __device__ __forceinline__ void merge_item(unsigned long long i, uint32_t cells,
 // transmittance mass is positive; support = 1 - transmittance when the
 // radiance mass is positive too; the radiance is the raw record's), which
 // gives exactly the values merge_own returned, and adds the children.
+// Record r of a level (cell-major): its cell and direction, by a shift when
+// the level's direction count is a power of two, else by a 32-bit division
+// when r fits in 32 bits (a 64-bit one otherwise).
+__device__ __forceinline__ void record_cell(unsigned long long r, uint32_t dirs, uint32_t &cell, uint32_t &d) {
+    if ((dirs & (dirs - 1u)) == 0u) {
+        const uint32_t shift = (uint32_t)__ffs(dirs) - 1u;
+        cell = (uint32_t)(r >> shift);
+        d = (uint32_t)r & (dirs - 1u);
+    } else if (r <= 0xffffffffull) {
+        cell = (uint32_t)r / dirs;
+        d = (uint32_t)r - cell * dirs;
+    } else {
+        cell = (uint32_t)(r / dirs);
+        d = (uint32_t)(r - (unsigned long long)cell * dirs);
+    }
+}
+
 __device__ __forceinline__ void merge_own_record(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
-                                                 unsigned long long e) {
+                                                 uint32_t level, unsigned long long base, uint32_t dirs,
+                                                 unsigned long long r) {
+    uint32_t cell, d;
+    record_cell(r, dirs, cell, d);
+    MergeOwn own;
+    if (!merge_own(V, F, H, level, base, dirs, cell, d, own)) merge_finish(V, F, level, base, dirs, cell, d, own, false);
+}
+
+// Record e of the frame (all levels in storage order): its level by a scan
+// of the level bases.
+__device__ __forceinline__ void merge_own_entry(const ViewDevice &V, const FrameParams &F, const HistoryDevice &H,
+                                                unsigned long long e) {
     uint32_t level = 0;
     while (level + 1u < F.levels && e >= V.level_base[level + 1u]) ++level;
     const unsigned long long base = V.level_base[level];
-    const uint32_t dirs = F.dirs[level];
-    const unsigned long long r = e - base;
-    const uint32_t cell = (uint32_t)(r / dirs), d = (uint32_t)(r - (unsigned long long)cell * dirs);
-    MergeOwn own;
-    if (!merge_own(V, F, H, level, base, dirs, cell, d, own)) merge_finish(V, F, level, base, dirs, cell, d, own, false);
+    merge_own_record(V, F, H, level, base, F.dirs[level], e - base);
 }
 
 __device__ __forceinline__ void merge_children_record(const ViewDevice &V, const FrameParams &F, uint32_t level,
@@ -1530,13 +1560,15 @@ __device__ __forceinline__ void merge_children_record(const ViewDevice &V, const
     merge_finish(V, F, level, base, dirs, cell, d, own, true);
 }
 
-__global__ void __launch_bounds__(256) merge_own_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
+__global__ void __launch_bounds__(256, LUX_MERGE_OWN_MIN_BLOCKS) merge_own_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
     if (*V.error_flags) return;
-    const unsigned long long n = V.level_base[F.levels - 1u] +
-                                 (unsigned long long)V.cell_count[F.levels - 1u] * F.dirs[F.levels - 1u];
-    for (unsigned long long e = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; e < n;
-         e += (unsigned long long)gridDim.x * blockDim.x)
-        merge_own_record(V, F, H, e);
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        const uint32_t dirs = F.dirs[l];
+        const unsigned long long n = (unsigned long long)V.cell_count[l] * dirs, base = V.level_base[l];
+        for (unsigned long long r = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; r < n;
+             r += (unsigned long long)gridDim.x * blockDim.x)
+            merge_own_record(V, F, H, l, base, dirs, r);
+    }
 }
 
 __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
@@ -2213,7 +2245,7 @@ __global__ void __launch_bounds__(256) batch_merge_own_kernel(const BatchJob *__
     for_batch_items(batch_row(dom, n, kRowEntries), n, [&](uint32_t j, unsigned long long e) {
         const BatchJob &J = jobs[j];
         if (e >= count[j] || *J.V.error_flags) return;
-        merge_own_record(J.V, J.F, J.H, e);
+        merge_own_entry(J.V, J.F, J.H, e);
     });
 }
 
