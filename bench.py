@@ -214,9 +214,41 @@ def point_classes(w, indices):
     return np.asarray(w["desc"].instance_mesh, np.int64)[caller]
 
 
-def error_report(bp, ctx, est, ref, classes):
+def emitter_distance(packed, points):
+    """Distance (m) from each point to the nearest emissive triangle (the
+    scene's emitter light records: vertex, edge1, edge2), exact in FP64: the
+    plane distance where the point projects inside the triangle, else the
+    nearest of its three edges."""
+    rec = packed.lights[packed.conventional:].view(np.float32).astype(np.float64)
+    p = np.asarray(points, np.float64)[:, :3]
+    best = np.full(len(p), np.inf)
+    for a, e1, e2 in zip(rec[:, 0:3], rec[:, 12:15], rec[:, 16:19]):
+        n = np.cross(e1, e2)
+        area2 = float(np.dot(n, n))
+        if area2 <= 0.0:
+            continue
+        q = p - a
+        # Barycentrics of the projection (solve q = u e1 + v e2 + h n).
+        u = np.einsum("ij,j->i", np.cross(q, e2), n) / area2
+        v = np.einsum("ij,j->i", np.cross(e1, q), n) / area2
+        inside = (u >= 0) & (v >= 0) & (u + v <= 1)
+        d = np.where(inside, np.abs(q @ n) / np.sqrt(area2), np.inf)
+        for s0, s1 in ((a, a + e1), (a + e1, a + e2), (a + e2, a)):
+            seg = s1 - s0
+            t = np.clip(((p - s0) @ seg) / float(np.dot(seg, seg)), 0.0, 1.0)
+            d = np.minimum(d, np.linalg.norm(p - (s0 + t[:, None] * seg), axis=1))
+        best = np.minimum(best, d)
+    return best
+
+
+EMITTER_BANDS = (0.0, 0.25, 0.5, 1.0, 2.0, 4.0, np.inf)
+
+
+def error_report(bp, ctx, est, ref, classes, distance=None):
     """lux_error_stats of an estimate against a reference, plus the relative
-    RMSE and the ratio of means per surface class (host, FP64)."""
+    RMSE and the ratio of means per surface class (host, FP64), and with the
+    points' distances to the nearest emitter the same per distance band,
+    with each band's share of the summed squared error."""
     out = bp.error_stats(ctx, est.data_ptr(), ref.data_ptr(), len(est))
     e, r = est.cpu().numpy().astype(np.float64), ref.cpu().numpy()
     ok = (e[:, 3] > 0) & (r[:, 3] > 0)
@@ -230,6 +262,21 @@ def error_report(bp, ctx, est, ref, classes):
         per[name] = {"points": int(m.sum()), "relative_rmse": float(np.sqrt(np.mean(d * d)) / max(mean_ref, 1e-30)),
                      "ratio_of_means": float(e[m, :3].mean() / max(mean_ref, 1e-30))}
     out["per_surface"] = per
+    if distance is not None:
+        m_all = ok & (classes != 3)  # emitters excluded, as in the surface classes
+        sq = np.sum((e[:, :3] - r[:, :3]) ** 2, axis=1)
+        total = float(sq[m_all].sum())
+        bands = []
+        for lo, hi in zip(EMITTER_BANDS[:-1], EMITTER_BANDS[1:]):
+            m = m_all & (distance >= lo) & (distance < hi)
+            if m.sum() == 0:
+                continue
+            mean_ref = r[m, :3].mean()
+            bands.append({"from_m": lo, "to_m": None if np.isinf(hi) else hi, "points": int(m.sum()),
+                          "relative_rmse": float(np.sqrt(sq[m].mean() / 3.0) / max(mean_ref, 1e-30)),
+                          "ratio_of_means": float(e[m, :3].mean() / max(mean_ref, 1e-30)),
+                          "share_of_squared_error": float(sq[m].sum() / max(total, 1e-300))})
+        out["by_emitter_distance"] = bands
     return out
 
 
@@ -475,7 +522,7 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
         raise RuntimeError("learned-cache frame reported an error")
     lview.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), n_pts, d_out.data_ptr())
     s_est = d_out[sub].contiguous()
-    err = error_report(bp, ctx, s_est, s_ref, classes)
+    err = error_report(bp, ctx, s_est, s_ref, classes, w.get("error_distance"))
     return {
         "ms_per_step": learned_ms, "value": interval_rays / (learned_ms * 1e-3) / 1e6, "unit": "Mrays/s",
         "speedup_vs_plain": plain_ms / learned_ms,
@@ -483,7 +530,7 @@ def run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, s
                       "merge": float(stage_ms[2]), "pack": float(stage_ms[3])},
         "relative_rmse": err["relative_rmse"], "plain_relative_rmse": plain_error["relative_rmse"],
         "rmse_change": err["relative_rmse"] / plain_error["relative_rmse"] - 1.0,
-        "per_surface": err["per_surface"],
+        "per_surface": err["per_surface"], "by_emitter_distance": err.get("by_emitter_distance"),
         "rays": {"cached": int(cs.cached_rays), "fallback": int(cs.fallback_rays),
                  "validated": int(cs.validated_rays), "trained_samples": int(cs.trained_samples),
                  "failed_cells": int(cs.failed_cells), "validated_cells": int(cs.validated_cells),
@@ -533,7 +580,7 @@ def run_multi_bounce(w, args, stream, flush, d_rpos, d_rnrm, plain_ms, device, d
         raise RuntimeError("multi-bounce frame reported an error")
     mb_ms = float(np.sum(ms)) / args.steps
     mview.resolve(settings, d_ppos.data_ptr(), d_pnrm.data_ptr(), len(w["ppos"]), d_out.data_ptr())
-    err3 = error_report(bp, ctx, d_out[sub].contiguous(), ref3, classes)
+    err3 = error_report(bp, ctx, d_out[sub].contiguous(), ref3, classes, w.get("error_distance"))
     return {"ms_per_step": mb_ms, "overhead_vs_plain": mb_ms / plain_ms,
             "error_vs_fp64_3_bounces": err3,
             "secondary_trace_ms": float(np.median(sec_trace)),
@@ -716,11 +763,13 @@ def run_ours(args, rank, world):
         refs[bounces] = (r, time.perf_counter() - t0)
     s_ref = refs[2][0]
     classes = point_classes(w, sub.cpu().numpy())
-    error = error_report(bp, ctx, s_est, s_ref, classes)
+    distance = emitter_distance(w["packed"], s_pos.cpu().numpy())
+    w["error_distance"] = distance
+    error = error_report(bp, ctx, s_est, s_ref, classes, distance)
     error.update({"spp": REFERENCE_SPP, "bounces": 2, "sample": f"every 97th resolve point ({len(sub)})",
                   "reference_s": refs[2][1],
                   "oracle": "path-traced reference (emissive NEE + MIS, FP32 rays, FP64 sums), 2 diffuse vertices"})
-    error3 = error_report(bp, ctx, s_est, refs[3][0], classes)
+    error3 = error_report(bp, ctx, s_est, refs[3][0], classes, distance)
     error3.update({"spp": REFERENCE_SPP, "bounces": 3, "reference_s": refs[3][1]})
 
     learned = run_learned(w, args, stream, flush, d_rpos, d_rnrm, d_ppos, d_pnrm, d_out, sub, s_ref, classes,
@@ -1208,8 +1257,13 @@ def run_frames(args):
     torch.cuda.nvtx.range_pop()
     st = view.stats()
     m = np.median(np.array(stages), axis=0)
+    interval_rays = max(int(st.interval_rays), 1)
     print(json.dumps({"profile": "learned-frames" if args.learned_frames else "frames-only", "width": WIDTH, "height": HEIGHT, "triangles": TRIANGLES,
                       "tuning": tuning_of(START), "seed_ms": m[0], "trace_ms": m[1], "merge_ms": m[2], "pack_ms": m[3],
+                      "per_interval_ray": {"nodes": (int(st.nodes_visited) - int(st.shadow_nodes)) / interval_rays,
+                                           "triangles": (int(st.triangles_tested) - int(st.shadow_triangles)) / interval_rays},
+                      "per_shadow_ray": {"nodes": int(st.shadow_nodes) / max(int(st.shadow_rays), 1),
+                                         "triangles": int(st.shadow_triangles) / max(int(st.shadow_rays), 1)},
                       "cells": list(st.cells)[:settings.levels], "error_flags": int(st.error_flags)}))
 
 

@@ -62,6 +62,19 @@
 #ifndef LUX_MERGE_OWN_MIN_BLOCKS
 #define LUX_MERGE_OWN_MIN_BLOCKS 8
 #endif
+// The merge's own pass lists the records that pass light on, and the
+// children pass of each level runs over that list only (full warps) instead
+// of over every record of the level.
+#ifndef LUX_MERGE_COMPACT
+#define LUX_MERGE_COMPACT 1
+#endif
+
+// The merge preparation takes one thread per (cell, corner) instead of one
+// per cell.
+#ifndef LUX_MERGE_PREP_SPLIT
+#define LUX_MERGE_PREP_SPLIT 1
+#endif
+
 #ifndef LUX_MERGE_CORNER_OUTER
 #define LUX_MERGE_CORNER_OUTER 1
 #endif
@@ -155,6 +168,8 @@ struct ViewDevice {
     float4 *merged;                 // [entries] I rgb, support
     float4 *raw;                    // [entries] J rgb, beta (history-blended)
     float2 *mass;                   // [entries] radiance mass, transmittance mass
+    uint32_t *pass_list;            // [entries] per level (at its record base): records that pass light on
+    uint32_t *pass_count;           // [levels] entries of pass_list per level
     uint32_t *hist_cell;            // [levels][cell_capacity] the previous frame's id of each cell, or kEmpty
     uint32_t *cell_last;            // [levels][cell_capacity] frame index of the cell's last receiver
     uint32_t *retain_hist;          // [levels][kRetainBins] retain candidates per age class
@@ -1027,6 +1042,23 @@ __global__ void __launch_bounds__(128) deposit_dense_kernel(ViewDevice V, FrameP
 
 // Spatial corners of every cell of `level` in level + 1 (mergeRadianceGroups
 // grid, shaders/split.slang:1590-1596).
+// One corner of cell c (corner 0 also writes the interpolation weights):
+// the eight directory probes of a cell run in eight threads.
+__device__ __forceinline__ void corner_item(const ViewDevice &V, const FrameParams &F, uint32_t level, uint32_t c,
+                                            uint32_t corner) {
+    int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
+    const uint32_t lod = lux::key_lod(key.w);
+    const float sp = level_spacing(F, level, lod), sp1 = level_spacing(F, level + 1, lod);
+    float ox = ((float)key.x + 0.5f) * sp, oy = ((float)key.y + 0.5f) * sp, oz = ((float)key.z + 0.5f) * sp;
+    float gx = ox / sp1 - 0.5f, gy = oy / sp1 - 0.5f, gz = oz / sp1 - 0.5f;
+    float fx = floorf(gx), fy = floorf(gy), fz = floorf(gz);
+    int32_t bx = (int32_t)fx, by = (int32_t)fy, bz = (int32_t)fz;
+    if (corner == 0u) V.corner_frac[(size_t)level * F.cell_capacity + c] = make_float4(gx - fx, gy - fy, gz - fz, 0.0f);
+    V.corner_ids[((size_t)level * F.cell_capacity + c) * 8 + corner] =
+        cell_id(V, F, level + 1, bx + (int32_t)(corner & 1u), by + (int32_t)((corner >> 1) & 1u),
+                bz + (int32_t)(corner >> 2), lod);
+}
+
 __device__ __forceinline__ void corners_item(const ViewDevice &V, const FrameParams &F, uint32_t level, uint32_t c) {
     int4 key = V.cell_keys[(size_t)level * F.cell_capacity + c];
     // A cell's children are the next level's cells of the same LOD.
@@ -1177,12 +1209,25 @@ __device__ __forceinline__ void history_map_item(const ViewDevice &V, const Fram
 // next level, and with history its previous frame's id.
 __global__ void merge_prep_kernel(ViewDevice V, FrameParams F, HistoryDevice H) {
     if (*V.error_flags) return;
+    if (blockIdx.x == 0 && threadIdx.x < F.levels) V.pass_count[threadIdx.x] = 0u;
     for (uint32_t l = 0; l < F.levels; ++l) {
         const uint32_t cells = min(V.cell_count[l], F.cell_capacity);
+#if LUX_MERGE_PREP_SPLIT
+        // Eight threads per cell, one corner each; the history map goes to
+        // the thread of corner 7.
+        const unsigned long long items = (unsigned long long)cells * 8u;
+        for (unsigned long long k = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; k < items;
+             k += (unsigned long long)gridDim.x * blockDim.x) {
+            const uint32_t c = (uint32_t)(k >> 3), corner = (uint32_t)k & 7u;
+            if (l + 1u < F.levels) corner_item(V, F, l, c, corner);
+            if (F.history && corner == 7u) history_map_item(V, F, H, l, c);
+        }
+#else
         for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < cells; c += gridDim.x * blockDim.x) {
             if (l + 1u < F.levels) corners_item(V, F, l, c);
             if (F.history) history_map_item(V, F, H, l, c);
         }
+#endif
     }
 }
 
@@ -1581,6 +1626,51 @@ __global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
          i += (unsigned long long)gridDim.x * blockDim.x) {
         uint32_t cell, d;
         merge_item(i, cells, dirs, cell, d);
+        merge_children_record(V, F, level, base, dirs, cell, d);
+    }
+}
+
+// The own pass that lists, level by level, the records whose merged value
+// needs the children (pass_list at the level's record base, pass_count per
+// level), taken in storage order as merge_own_kernel takes them; a warp
+// appends its records of a round together (one atomic per warp and round).
+// Levels hold fewer than 2^32 records (checked on the host).
+__global__ void __launch_bounds__(256, LUX_MERGE_OWN_MIN_BLOCKS) merge_own_list_kernel(ViewDevice V, FrameParams F,
+                                                                                      HistoryDevice H) {
+    if (*V.error_flags) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t l = 0; l < F.levels; ++l) {
+        const uint32_t dirs = F.dirs[l];
+        const unsigned long long n = (unsigned long long)V.cell_count[l] * dirs, base = V.level_base[l];
+        for (unsigned long long r = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; r < n;
+             r += (unsigned long long)gridDim.x * blockDim.x) {
+            uint32_t cell, d;
+            record_cell(r, dirs, cell, d);
+            MergeOwn own;
+            const bool children = merge_own(V, F, H, l, base, dirs, cell, d, own);
+            if (!children) merge_finish(V, F, l, base, dirs, cell, d, own, false);
+            const unsigned active = __activemask();
+            const unsigned want = __ballot_sync(active, children);
+            if (want) {
+                const uint32_t leader = (uint32_t)__ffs(want) - 1u;
+                uint32_t at = 0;
+                if (lane == leader) at = atomicAdd(&V.pass_count[l], (uint32_t)__popc(want));
+                at = __shfl_sync(active, at, leader);
+                if (children) V.pass_list[base + at + (uint32_t)__popc(want & ((1u << lane) - 1u))] = (uint32_t)r;
+            }
+        }
+    }
+}
+
+// The children pass of one level over its listed records.
+__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
+    merge_children_list_kernel(ViewDevice V, FrameParams F, uint32_t level) {
+    if (*V.error_flags) return;
+    const uint32_t dirs = F.dirs[level], n = V.pass_count[level];
+    const unsigned long long base = V.level_base[level];
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t cell, d;
+        record_cell(__ldg(V.pass_list + base + i), dirs, cell, d);
         merge_children_record(V, F, level, base, dirs, cell, d);
     }
 }
@@ -2673,6 +2763,8 @@ static lux_status view_alloc(LuxView *v) {
         {(void **)&D.merged, (size_t)d.max_entries * sizeof(float4)},
         {(void **)&D.raw, (size_t)d.max_entries * sizeof(float4)},
         {(void **)&D.mass, (size_t)d.max_entries * sizeof(float2)},
+        {(void **)&D.pass_list, LUX_MERGE_COMPACT ? (size_t)d.max_entries * sizeof(uint32_t) : 16},
+        {(void **)&D.pass_count, L * sizeof(uint32_t)},
         {(void **)&D.hist_cell, L * (size_t)d.max_cells * sizeof(uint32_t)},
         {(void **)&D.cell_last, L * (size_t)d.max_cells * sizeof(uint32_t)},
         {(void **)&v->hist.cell_last, L * (size_t)d.max_cells * sizeof(uint32_t)},
@@ -2970,6 +3062,15 @@ static void enqueue_merge(LuxView *v, const FrameParams &F, cudaStream_t st) {
     const int grid = v->ctx->sm_count * 8;
     const HistoryDevice H = history_device(v);
     if (F.levels > 1 || F.history) merge_prep_kernel<<<grid, 128, 0, st>>>(D, F, H);
+    // Record indices in the pass list are 32-bit (a level's records).
+    const bool listed = LUX_MERGE_COMPACT && F.levels > 1 && v->desc.max_entries <= 0xffffffffull;
+    if (listed) {
+        merge_own_list_kernel<<<grid * 2, 256, 0, st>>>(D, F, H);
+        for (int l = (int)F.levels - 2; l >= 0; --l)
+            merge_children_list_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F,
+                                                                                                   (uint32_t)l);
+        return;
+    }
     merge_own_kernel<<<grid * 2, 256, 0, st>>>(D, F, H);
     for (int l = (int)F.levels - 2; l >= 0; --l)
         merge_children_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(D, F, (uint32_t)l);
