@@ -611,31 +611,44 @@ struct AdamParams {
     float lr, beta1, beta2, eps, correction1, correction2;
 };
 
-__global__ void adam_kernel(AdamParams P, float *__restrict__ param, float *__restrict__ grad, float *__restrict__ m,
-                            float *__restrict__ v, size_t n, bf16 *__restrict__ out) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        float g = grad[i];
-        float mi = m[i], vi = v[i];
-        if (g == 0.0f && mi == 0.0f) continue;  // never touched: nothing to move
-        grad[i] = 0.0f;
-        mi = P.beta1 * mi + (1.0f - P.beta1) * g;
-        vi = P.beta2 * vi + (1.0f - P.beta2) * g * g;
-        m[i] = mi;
-        v[i] = vi;
-        float p = param[i] - P.lr * (mi / P.correction1) / (sqrtf(vi / P.correction2) + P.eps);
-        param[i] = p;
-        if (out) out[i] = __float2bfloat16_rn(p);
-    }
-}
-
 // Adam on four consecutive parameters per thread (the hash table: n is a
 // multiple of 4), with the BF16 copy written as one 8-byte store.  Sparse
 // ("lazy") Adam: a parameter this step's samples did not reach (zero
 // gradient) keeps its value and moments, so a step reads only the gradients
 // of the untouched entries -- a batch reaches a quarter of a fine level's
 // entries at most.  A parameter's first update is the dense step's.
+//
+// The same launch also takes the Adam step of the MLP weights (thread e of
+// the grid: weight e, dense Adam, skipping weights whose gradient and first
+// moment are both zero: never touched) and writes each weight's BF16 copy into the forward (W) and
+// backward (W^T) tile layouts, as pack_weights_kernel does: one launch per
+// training step instead of three.
 __global__ void adam4_kernel(AdamParams P, float4 *__restrict__ param, float4 *__restrict__ grad,
-                             float4 *__restrict__ m, float4 *__restrict__ v, size_t n4, uint2 *__restrict__ out) {
+                             float4 *__restrict__ m, float4 *__restrict__ v, size_t n4, uint2 *__restrict__ out,
+                             float *__restrict__ w, float *__restrict__ wg, float *__restrict__ wm,
+                             float *__restrict__ wv, bf16 *__restrict__ w_packed) {
+    const uint32_t e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w && e < (uint32_t)kWTotal) {
+        float p = w[e];
+        const float g = wg[e];
+        float mi = wm[e], vi = wv[e];
+        if (!(g == 0.0f && mi == 0.0f)) {
+            wg[e] = 0.0f;
+            mi = P.beta1 * mi + (1.0f - P.beta1) * g;
+            vi = P.beta2 * vi + (1.0f - P.beta2) * g * g;
+            wm[e] = mi;
+            wv[e] = vi;
+            p = p - P.lr * (mi / P.correction1) / (sqrtf(vi / P.correction2) + P.eps);
+            w[e] = p;
+        }
+        const uint32_t l = e < (uint32_t)(kHiddenLayers * kWHidden) ? e / kWHidden : (uint32_t)kHiddenLayers;
+        const uint32_t local = e - l * kWHidden;
+        const uint32_t o = local / kIn, i = local % kIn;
+        const uint32_t N = l < (uint32_t)kHiddenLayers ? kHidden : kOut;
+        const bf16 b = __float2bfloat16_rn(p);
+        w_packed[fwd_offset((int)l) + packed(o, i, N)] = b;
+        w_packed[bwd_offset((int)l) + packed(i, o, kIn)] = b;
+    }
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n4; i += (size_t)gridDim.x * blockDim.x) {
         float4 g = grad[i];
         if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f && g.w == 0.0f) continue;  // not reached this step
@@ -919,12 +932,9 @@ extern "C" lux_status lux_cache_train(LuxCache *c, const LuxCacheSample *samples
         P.eps = 1e-10f;
         P.correction1 = 1.0f - (float)std::pow(0.9, (double)c->steps);
         P.correction2 = 1.0f - (float)std::pow(0.99, (double)c->steps);
-        adam4_kernel<<<grid, 256, 0, st>>>(P, (float4 *)c->table_master, (float4 *)c->table_grad,
-                                           (float4 *)c->table_m, (float4 *)c->table_v, c->table_params / 4,
-                                           (uint2 *)c->table);
-        adam_kernel<<<(kWTotal + 255) / 256, 256, 0, st>>>(P, c->w_master, c->w_grad, c->w_m, c->w_v, kWTotal,
-                                                           nullptr);
-        pack_weights_kernel<<<(kWTotal + 255) / 256, 256, 0, st>>>(c->w_master, c->w_packed);
+        adam4_kernel<<<std::max(grid, (kWTotal + 255) / 256), 256, 0, st>>>(
+            P, (float4 *)c->table_master, (float4 *)c->table_grad, (float4 *)c->table_m, (float4 *)c->table_v,
+            c->table_params / 4, (uint2 *)c->table, c->w_master, c->w_grad, c->w_m, c->w_v, c->w_packed);
         c->samples += nb;
         rc = lux_cuda_check(ctx, (int)cudaGetLastError(), "cache: train launch");
         if (rc != LUX_OK) return rc;

@@ -58,9 +58,10 @@
 #define LUX_MERGE_MIN_BLOCKS 4
 #endif
 // The own pass (every record of every level, no children): 256-thread
-// blocks, register budget for this many resident per SM.
+// blocks, register budget for this many resident per SM (6: 40 registers;
+// at 8 the 32-register budget spills and the pass ran 5% longer).
 #ifndef LUX_MERGE_OWN_MIN_BLOCKS
-#define LUX_MERGE_OWN_MIN_BLOCKS 8
+#define LUX_MERGE_OWN_MIN_BLOCKS 6
 #endif
 // The merge's own pass lists the records that pass light on, and the
 // children pass of each level runs over that list only (full warps) instead
