@@ -176,7 +176,15 @@ class RadianceCascadesStatus:
 @dataclass
 class RadianceCascadesPlugin:
     """RadianceCascadesPlugin (src/lib.rs:795-900): budgets, and `build`
-    creates the device context that render() would use."""
+    creates the device context that render() would use.
+
+    The budgets keep the reference's fields and defaults.  The reference
+    spends them in its render plumbing (scene paging against
+    `scene_gpu_budget_bytes`, src/render.rs:6925-6950; view settings adapted
+    to `view_gpu_budget_bytes`, src/render.rs:416-450), which is outside this
+    library: here a scene and a view take exactly the capacities the caller
+    passes to GpuScene and SplitView, and allocation failures surface as
+    LUX_ERR_OUT_OF_MEMORY."""
     scene_gpu_budget_bytes: int = 256 * 1024 * 1024
     view_gpu_budget_bytes: int = 2 * 1024 * 1024 * 1024
     device: int = 0
