@@ -72,6 +72,7 @@ def lib():
             "orc_environment_response": (C.c_int, [P, P, F, F, U, U, P, P, P, P, F, P, C.c_int, P, P, P]),
             "orc_screen_filter": (None, [P, U, U, P, P, P, P, P, P, U, U, U, P, P, P]),
             "orc_history_blend": (None, [P, U, P, P, P, P, P]),
+            "orc_merge_history_entry": (None, [P, P, U, P, P, P, P, C.c_int, P]),
             "orc_frame_destroy": (None, [P]),
             "orc_frame_cells": (U, [P, U]),
             "orc_scene_pack": (C.c_int, [P, U, P, U, P, P, U, P, P, P, P, U, P, U, P]),
@@ -397,6 +398,18 @@ def screen_filter(settings_c, irradiance, position, normal, identity, previous_c
                             _p(prev), _p(d) if d is not None else None, 1 if scene_changed else 0,
                             spatial_filter_steps, 0 if history is None else 1, _p(hin), _p(hout), _p(out))
     return hout, out
+
+
+def merge_history_entry(settings_c, interval, samples: int, old, old_mass, fraction, children4x8):
+    """mergeEntry with history of one entry: the merged float4."""
+    out = np.zeros(4, np.float32)
+    o = f32(*old) if old is not None else None
+    om = f32(*old_mass) if old_mass is not None else None
+    ch = np.ascontiguousarray(children4x8, np.float32)
+    lib().orc_merge_history_entry(C.byref(settings_c), _p(f32(*interval)), samples,
+                                  _p(o) if o is not None else None, _p(om) if om is not None else None,
+                                  _p(f32(*fraction)), _p(ch), 1, _p(out))
+    return out
 
 
 def history_blend(settings_c, samples: int, fresh, old=None, old_mass=None):

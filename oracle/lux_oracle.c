@@ -2024,6 +2024,19 @@ void orc_merge_entry(const float interval[4], uint32_t samples, const float frac
     merge_values(&st, interval, samples, children, has_children, out);
 }
 
+/* mergeEntry with history (shaders/split.slang:1478-1521, :1624-1725) for
+ * one entry: the fresh (J, beta) of `samples` observations blended with the
+ * previous frame's record (old raw, old mass; NULL: none) under the
+ * settings' blends, then the children as orc_merge_entry takes them. */
+void orc_merge_history_entry(const LuxSettings *st, const float interval[4], uint32_t samples, const float *old,
+                             const float *old_mass, const float fraction[3], const float *child_merged,
+                             int has_children, float out[4]) {
+    float children[16], raw[4], mass[2];
+    for (int c = 0; c < 4; ++c) orc_interpolate_children(fraction, child_merged + 32 * c, children + 4 * c);
+    orc_history_blend(st, samples, interval, old, old_mass, raw, mass);
+    merge_blended(raw, mass, children, has_children, out);
+}
+
 /* A record's history is invalid when its cell grown by the level's
  * interval end (unbounded at the last level) meets an invalidation box. */
 static int record_dirty(const OrcFrame *F, uint32_t level, const int32_t key[4]) {

@@ -220,6 +220,12 @@ uint32_t orc_deposit_levels(const LuxSettings *s, float distance, int hit, int u
  * as child_merged[4][8] float4 (w <= 0 = missing) and the spatial fraction. */
 void orc_merge_entry(const float interval[4], uint32_t samples, const float fraction[3],
                      const float *child_merged, int has_children, float out[4]);
+/* mergeEntry with history for one entry: orc_history_blend of the fresh
+ * interval with the previous record (old / old_mass may be NULL), then the
+ * children as orc_merge_entry. */
+void orc_merge_history_entry(const LuxSettings *settings, const float interval[4], uint32_t samples,
+                             const float *old, const float *old_mass, const float fraction[3],
+                             const float *child_merged, int has_children, float out[4]);
 /* interpolateMergedChildSources, one source (shaders/split.slang:389-479). */
 void orc_interpolate_children(const float fraction[3], const float *corner_merged, float out[4]);
 /* packProbes texel table from base-direction merged values float4[dirs]. */

@@ -47,6 +47,29 @@ def test_ragged_and_empty_frames_match_oracle():
     assert all(view.stats().cells[l] == 0 for l in range(4))
 
 
+@pytest.mark.parametrize("count", [1, 63, 64, 65])
+def test_warp_boundary_receiver_counts_match_oracle(count):
+    """Receiver counts at the warp boundaries of the ray, query and record
+    lists (one ray per receiver: 1, 63, 64 and 65 interval rays), the analogue
+    of the reference's compaction boundary counts
+    (gpu_compact_direction_group_boundaries, src/transport_tests.rs:4109-4261):
+    every frame's records and sample counts equal the oracle's."""
+    pos, nrm = cornell_floor_receivers(16)
+    ctx = bp.LuxContext()
+    scene = bp.GpuScene(ctx, packed("cornell"))
+    oscene = oracle.OracleScene.from_packed(packed("cornell"))
+    s = bp.RadianceCascades(probe_spacing=0.25, interval_length=0.4, levels=4, rays_per_receiver=1,
+                            frame_index=0).sanitized()
+    view = bp.SplitView(ctx, max_receivers=count, max_cells=1 << 14, max_entries=1 << 22, max_rays=count)
+    d_pos, d_nrm = to_device(pos[:count]), to_device(nrm[:count])
+    view.trace_merge(scene, s, d_pos.data_ptr(), d_nrm.data_ptr(), count)
+    st = view.stats()
+    assert st.error_flags == 0 and st.interval_rays == count
+    expected = oracle.OracleFrame(oscene, s.to_c(), pos[:count], nrm[:count], max_cells=1 << 14,
+                                  max_entries=1 << 22)
+    compare_levels(s, [view.read_level(l) for l in range(4)], expected, exact=False)
+
+
 def test_multi_bounce_without_hits():
     """Receivers whose rays leave the scene record no surfaces: the secondary
     cache seeds nothing and the primary frame equals the plain one."""

@@ -253,3 +253,32 @@ def test_oracle_cached_hit_sky_roles():
     _, _, raw_f, samples_f = fed.level(0, dirs)
     np.testing.assert_array_equal(samples_fc, samples_f)
     assert np.all(np.isfinite(raw_fc))
+
+
+def support_children():
+    """The child records of supportCases stages 3-5: only child 0, corner 0
+    carries (8, support 0.25); the parent sits at fraction 0."""
+    children = np.zeros((4, 8, 4), np.float32)
+    children[0, 0] = (8, 8, 8, 0.25)
+    return children
+
+
+def test_transparent_history_passes_partial_children():
+    """supportCases result[5] (src/split_merge_tests.rs:136-142, asserted at
+    :1370-1371 under run(0, 0.9)): no fresh observation, the previous record
+    transparent (J 7, beta 1, transmittance mass 4): the radiance blend is
+    off, so the interval has no support of its own and passes the partially
+    supported child through."""
+    st = settings(0.0, 0.9)
+    r = oracle.merge_history_entry(st, (0, 0, 0, 1), 0, (7, 7, 7, 1), (0, 4), (0, 0, 0), support_children())
+    assert abs(r[0] - 8.0) < TOL
+    assert abs(r[3] - 0.0625) < TOL
+
+
+def test_opaque_history_cannot_invent_support():
+    """supportCases result[6] (src/split_merge_tests.rs:143-148, asserted at
+    :1372): the previous record's beta set to 0 (opaque) with no radiance
+    mass: nothing passes and nothing is supported."""
+    st = settings(0.0, 0.9)
+    r = oracle.merge_history_entry(st, (0, 0, 0, 1), 0, (7, 7, 7, 0), (0, 4), (0, 0, 0), support_children())
+    np.testing.assert_array_equal(r, [0, 0, 0, 0])
