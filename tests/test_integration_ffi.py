@@ -1,5 +1,6 @@
-"""The Rust FFI block a bevy_lux maintainer adds against the
-C header and the library: every function of include/lux.h is declared with
+"""The Rust FFI block a bevy_lux maintainer adds (the `extern "C"` block of the
+integration guide at the repository root) against the C header and the
+library: every function of include/lux.h is declared with
 the header's parameter count and exported by liblux.so, and every #[repr(C)]
 record has the field names, order and size of the binding's records (which
 mirror the header).  No GPU needed."""
