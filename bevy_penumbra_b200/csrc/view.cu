@@ -2145,8 +2145,9 @@ constexpr uint32_t kRowRecv = 2;     // receivers (sequence sort, ordinals)
 constexpr uint32_t kRowEntries = 3;  // the frame's records (clear)
 constexpr uint32_t kRowCells = 4;    // + level: cells of the level (corners, pack)
 constexpr uint32_t kRowRecords = kRowCells + LUX_MAX_LEVELS;  // + level: records of the level (merge)
-constexpr uint32_t kBatchRows = kRowRecords + LUX_MAX_LEVELS;
-constexpr uint32_t kDeviceRows = kBatchRows - kRowEntries;    // rows batch_layout_kernel writes
+constexpr uint32_t kRowListed = kRowRecords + LUX_MAX_LEVELS;  // + level: listed records of the level (merge)
+constexpr uint32_t kBatchRows = kRowListed + LUX_MAX_LEVELS;
+constexpr uint32_t kDeviceRows = kRowListed - kRowEntries;    // rows batch_layout_kernel writes
 
 // Largest j < n with begin[j] <= x.
 __device__ __forceinline__ uint32_t find_job64(const unsigned long long *__restrict__ begin, uint32_t n,
@@ -2317,6 +2318,9 @@ __global__ void batch_clear_entries_kernel(const BatchJob *__restrict__ jobs,
 // in the next level, and with history its previous frame's id.
 __global__ void batch_merge_prep_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
                                         uint32_t n, const unsigned long long *__restrict__ count, uint32_t levels) {
+    // Every job's list lengths start at zero (the listing own pass follows).
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n * LUX_MAX_LEVELS; k += gridDim.x * blockDim.x)
+        jobs[k / LUX_MAX_LEVELS].V.pass_count[k % LUX_MAX_LEVELS] = 0u;
     for (uint32_t l = 0; l < levels; ++l) {
         const unsigned long long *cells = count + (size_t)(kRowCells - kRowEntries + l) * n;
         for_batch_items(batch_row(dom, n, kRowCells + l), n, [&](uint32_t j, unsigned long long c) {
@@ -2337,6 +2341,81 @@ __global__ void __launch_bounds__(256) batch_merge_own_kernel(const BatchJob *__
         const BatchJob &J = jobs[j];
         if (e >= count[j] || *J.V.error_flags) return;
         merge_own_entry(J.V, J.F, J.H, e);
+    });
+}
+
+// The listing own pass over all jobs (merge_own_list_kernel's list for each
+// job's view): a warp chunk belongs to one job; lanes with records of one
+// level that pass light on append them together.
+__global__ void __launch_bounds__(256) batch_merge_own_list_kernel(const BatchJob *__restrict__ jobs,
+                                                                   const unsigned long long *__restrict__ dom,
+                                                                   uint32_t n,
+                                                                   const unsigned long long *__restrict__ count) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for_batch_items(batch_row(dom, n, kRowEntries), n, [&](uint32_t j, unsigned long long e) {
+        const BatchJob &J = jobs[j];
+        if (e >= count[j] || *J.V.error_flags) return;
+        uint32_t level = 0;
+        while (level + 1u < J.F.levels && e >= J.V.level_base[level + 1u]) ++level;
+        const unsigned long long base = J.V.level_base[level];
+        const uint32_t dirs = J.F.dirs[level];
+        const unsigned long long r = e - base;
+        uint32_t cell, d;
+        record_cell(r, dirs, cell, d);
+        MergeOwn own;
+        if (!merge_own(J.V, J.F, J.H, level, base, dirs, cell, d, own)) {
+            merge_finish(J.V, J.F, level, base, dirs, cell, d, own, false);
+            return;
+        }
+        const unsigned group = __match_any_sync(__activemask(), level);
+        const uint32_t leader = (uint32_t)__ffs(group) - 1u;
+        uint32_t at = 0;
+        if (lane == leader) at = atomicAdd(&J.V.pass_count[level], (uint32_t)__popc(group));
+        at = __shfl_sync(group, at, leader);
+        J.V.pass_list[base + at + (uint32_t)__popc(group & ((1u << lane) - 1u))] = (uint32_t)r;
+    });
+}
+
+// Domain rows of the listed records: per level, the 32-padded prefix over the
+// jobs of their list lengths (one warp per level).
+__global__ void batch_list_prefix_kernel(const BatchJob *__restrict__ jobs, unsigned long long *__restrict__ dom,
+                                         uint32_t n, uint32_t levels) {
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t l = threadIdx.x >> 5; l < levels; l += blockDim.x >> 5) {
+        unsigned long long *row = dom + (size_t)(kRowListed + l) * (n + 1);
+        unsigned long long carry = 0;
+        for (uint32_t c = 0; c < n; c += 32u) {
+            const uint32_t j = c + lane;
+            unsigned long long v = 0;
+            if (j < n) {
+                const BatchJob &J = jobs[j];
+                if (l + 1u < J.F.levels && *J.V.error_flags == 0u) v = ((unsigned long long)J.V.pass_count[l] + 31ull) & ~31ull;
+            }
+            unsigned long long incl = v;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= (uint32_t)off) incl += t;
+            }
+            if (j < n) row[j] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) row[n] = carry;
+    }
+}
+
+// The children pass of one level over every job's listed records.
+__global__ void __launch_bounds__(LUX_MERGE_THREADS, LUX_MERGE_MIN_BLOCKS)
+    batch_merge_children_list_kernel(const BatchJob *__restrict__ jobs, const unsigned long long *__restrict__ dom,
+                                     uint32_t n, uint32_t level) {
+    for_batch_items(batch_row(dom, n, kRowListed + level), n, [&](uint32_t j, unsigned long long i) {
+        const BatchJob &J = jobs[j];
+        if (level + 1u >= J.F.levels || *J.V.error_flags || i >= J.V.pass_count[level]) return;
+        const uint32_t dirs = J.F.dirs[level];
+        const unsigned long long base = J.V.level_base[level];
+        uint32_t cell, d;
+        record_cell(__ldg(J.V.pass_list + base + i), dirs, cell, d);
+        merge_children_record(J.V, J.F, level, base, dirs, cell, d);
     });
 }
 
@@ -4083,10 +4162,22 @@ static void batch_enqueue(LuxBatch *b, cudaStream_t st) {
     }
     if (b->levels > 1 || b->history)
         batch_merge_prep_kernel<<<grid, 128, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count, b->levels);
-    batch_merge_own_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
-    for (int l = (int)b->levels - 2; l >= 0; --l)
-        batch_merge_children_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(
-            b->d_jobs, b->d_dom, n, b->d_count, (uint32_t)l);
+    // The children passes over each job's list of the records that pass
+    // light on (32-bit record indices: every view's records fit them).
+    bool listed = LUX_MERGE_COMPACT && b->levels > 1;
+    for (const LuxBatchJob &job : b->jobs) listed = listed && job.view->desc.max_entries <= 0xffffffffull;
+    if (listed) {
+        batch_merge_own_list_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
+        batch_list_prefix_kernel<<<1, 32 * LUX_MAX_LEVELS, 0, st>>>(b->d_jobs, b->d_dom, n, b->levels);
+        for (int l = (int)b->levels - 2; l >= 0; --l)
+            batch_merge_children_list_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(
+                b->d_jobs, b->d_dom, n, (uint32_t)l);
+    } else {
+        batch_merge_own_kernel<<<grid * 2, 256, 0, st>>>(b->d_jobs, b->d_dom, n, b->d_count);
+        for (int l = (int)b->levels - 2; l >= 0; --l)
+            batch_merge_children_kernel<<<grid * 512 / LUX_MERGE_THREADS, LUX_MERGE_THREADS, 0, st>>>(
+                b->d_jobs, b->d_dom, n, b->d_count, (uint32_t)l);
+    }
     batch_pack_kernel<<<grid, 64, (size_t)b->max_dirs0 * 2 * sizeof(float4), st>>>(b->d_jobs, b->d_dom, n,
                                                                                  b->d_count, b->max_dirs0);
 }
