@@ -175,7 +175,10 @@ typedef struct LuxStats {
 #define LUX_VIEW_ERR_RAY_CAPACITY 8u
 #define LUX_VIEW_ERR_TIMEOUT 16u   /* a batch's grid-barrier wait ran out (lux_batch_status) */
 
-/* Capacities of a view (ViewBuffers, src/render.rs:5077-5160). */
+/* Capacities of a view (ViewBuffers, src/render.rs:5077-5160).  Device
+ * memory grows with max_entries by 88 bytes per record (sums, counts, merged,
+ * raw and mass records, the previous frame's raw and mass, the merge's list
+ * of records that pass light on). */
 typedef struct LuxViewDesc {
     uint32_t max_receivers;  /* receivers (Split) or cascade-0 probes (Dense) */
     uint32_t max_cells;      /* distinct world cells per level */
